@@ -1,0 +1,273 @@
+"""Benchmark of the MOSE explicit residual-and-update path on B200.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--precision exact|fp64|mixed]
+
+Workload (one GPU): the 2-D isentropic vortex on a periodic 2048 x 2048 block,
+MUSCL van Albada + HLLC, SSP-RK3, CFL 0.8, FP64; synthetic initial field of
+the named shape.  A "step" is one full Explicit_Step (dt pass + 3 fused RK
+stages) over the whole block.  value = cell-updates/s, one update being one
+RK3 step of one cell; N GPUs run N independent replicas (weak scaling).
+
+--impl reference times the CPU oracle (the C++/OpenMP restatement of the
+reference's Fortran algorithm; the Fortran build itself cannot be compiled
+without gfortran and the FLINT/ORION/FiNeR submodules) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+N_CELLS_SIDE = 2048
+BYTES_PER_CELL_STEP = 256          # 8 * nv * 8 B with nv = 4
+STAGE_BYTES_PER_CELL = (64 + 96 + 96) / 3.0   # stage 1 reads P^n, writes P^1; stages 2,3 also read P^n
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_case(n=N_CELLS_SIDE, steps=100):
+    from mose_b200 import cases
+    return cases.isentropic_vortex(n, steps=steps, limiter="vanalbada", riemann="HLLC", cfl=0.8)
+
+
+def workload_config(case, precision):
+    return {"workload": f"isentropic vortex 2-D, periodic {N_CELLS_SIDE}x{N_CELLS_SIDE} block on [0,10]^2, "
+                        "MUSCL van Albada + HLLC, SSP-RK3, CFL 0.8, time accurate",
+            "cells": case.ncells, "precision": precision,
+            "l2": "inputs larger than L2 (3 state buffers of 135 MB each, > 126 MB)"}
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        time.sleep(0.25)
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(seconds=15.0, n=512):
+    """The oracle's OpenMP build on a bounded sample: the same problem on a
+    512 x 512 block, steps until ~`seconds` of CPU work."""
+    from oracle import pyoracle
+    pyoracle.build()
+    cores = os.cpu_count() or 1
+    case = workload_case(n, steps=1)
+    o = pyoracle.Oracle(case, nthreads=cores, omp=True)
+    o.step()                                   # warm-up
+    t0 = time.perf_counter()
+    steps = 0
+    while time.perf_counter() - t0 < seconds or steps < 2:
+        o.step()
+        steps += 1
+    dt = time.perf_counter() - t0
+    return {"value": case.ncells * steps / dt, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": f"{n}x{n} block of the same vortex problem, {steps} RK3 steps, {dt:.1f} s wall on "
+                      f"{cores} threads (C++/OpenMP restatement of the reference Fortran)"}
+
+
+def run_reference(args):
+    world, rank, _ = dist_init()
+    if rank != 0:
+        return 0
+    from oracle import pyoracle
+    pyoracle.build()
+    cores = os.cpu_count() or 1
+    case = workload_case(N_CELLS_SIDE, steps=1)
+    o = pyoracle.Oracle(case, nthreads=cores, omp=True)
+    for _ in range(min(args.warmup, 1)):
+        o.step()
+    # each step is one full RK3 step of the 2048^2 block; bound the count so the run stays within minutes
+    t0 = time.perf_counter()
+    steps = 0
+    budget = 90.0
+    while steps < args.steps and (time.perf_counter() - t0) < budget:
+        o.step()
+        steps += 1
+    el = time.perf_counter() - t0
+    value = case.ncells * steps / el
+    line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(case, "fp64 (CPU oracle)"), "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "port",
+                             "sample": f"{steps} of the requested {args.steps} steps of the 2048^2 workload "
+                                       f"({el:.1f} s on {cores} threads)"},
+            "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_gpu(args):
+    world, rank, local = dist_init()
+    import torch
+    from mose_b200 import Solver, _lib
+    prec = {"exact": _lib.PRECISION_FP64_EXACT, "fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[
+        args.precision]
+    case = workload_case(N_CELLS_SIDE, steps=args.steps)
+    s = Solver(case, precision=prec, device=local)
+    stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
+    s.advance(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    # --- device-resident throughput (value) ---------------------------------
+    launches0 = s.launch_count
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        s.advance(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = e0.elapsed_time(e1)
+    launches = s.launch_count - launches0
+    ms = max_over_ranks(ms, world)
+    value = world * case.ncells * args.steps / (ms / 1e3)
+    # --- per-kernel timing for the roofline (same kernels, events between) --
+    kms, kn = s.time_kernels(max(3, min(20, args.steps)))
+    stage_ms = kms[2] / max(kn[2], 1)
+    cells = case.ncells
+    achieved = STAGE_BYTES_PER_CELL * cells / (stage_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    # --- end to end through the C ABI with host buffers ----------------------
+    shape = (1 + 4, N_CELLS_SIDE + 4, N_CELLS_SIDE + 4, 5)
+    host = torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    s.download_prim(1, host)
+    n_e2e = max(3, min(args.steps, 20))
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        s.upload_prim(1, host)
+        s.explicit_step()
+        s.download_prim(1, host)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, world)
+    e2e = world * cells * n_e2e / e2e_s
+    nbytes = int(np.prod(shape)) * 8
+    if rank == 0:
+        line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
+                "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f64", "data": "synthetic", "config": workload_config(case, args.precision),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None,
+                             "kernel": "k_stage2d (fused residual + RK stage)", "peak_kind": peak_kind,
+                             "stage_ms": stage_ms, "step_kernel_ms": {"dt": kms[0] / max(1, kn[0] // 3),
+                                                                      "ghost": kms[1] / max(1, kn[1]),
+                                                                      "stage": stage_ms}},
+                "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
+                        "d2h_bytes_per_step": nbytes,
+                        "call": "mose_gpu_upload_prim + mose_gpu_step + mose_gpu_download_prim (pinned host)"},
+                "gpu_launches": launches, "clocks": clk.summary(),
+                "step_bytes_per_cell": BYTES_PER_CELL_STEP,
+                "hbm_frac_whole_step": BYTES_PER_CELL_STEP * cells * args.steps / (ms / 1e3 / world) / 1e9 / peak}
+        if not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
+    ap.add_argument("--precision", default="exact", choices=["exact", "fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,185 @@
+/*
+ * mose_gpu.h -- C ABI of the B200 (sm_100a) implementation of MOSE's explicit
+ * inviscid residual-and-update path on multi-block structured grids.
+ *
+ * Plain C types only (ints, doubles, pointers and sizes), so MOSE's Fortran
+ * drivers bind it with ISO_C_BINDING (see mose_b200/fortran/mose_gpu_m.f90)
+ * and Python binds it with ctypes.  Every entry point returns a status code
+ * (MOSE_OK = 0) except the getters noted; mose_gpu_last_error() returns the
+ * message of the last failure.
+ *
+ * Each entry point names the reference routine it replaces (paths relative
+ * to the MOSE source tree, src/lib/...).
+ *
+ * Array layouts crossing this boundary are the reference's own:
+ *   node  : Fortran real(8) node(3, 0:ni, 0:nj, 0:nk)
+ *   P, R  : Fortran real(8) P(nprim, 1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc),
+ *           nprim = 5 (rho, u, v, w, p), gc = 2
+ *   bc    : one record per boundary face cell in bc.txt order (block, face
+ *           1..6, cell): int32 b,i,j,k,f,type,bs,is,js,ks,fs,d11,d12,d21,d22
+ *           (1-based), plus 6 doubles of type data
+ *           405: mach, T, p, alpha, beta, rel_fac ; 406: p_back, rel_fac
+ *
+ * State is device resident between calls: host P is stale until
+ * mose_gpu_download_prim().  A context is not thread safe and owns one
+ * CUDA stream.
+ */
+#ifndef MOSE_GPU_H
+#define MOSE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MOSE_GPU_ABI_VERSION 1
+
+/* Status codes.  The nonzero codes mirror the reference's fatal `stop`s. */
+enum {
+  MOSE_OK = 0,
+  MOSE_ERR_INVALID = 1,            /* bad argument or call order */
+  MOSE_ERR_UNSUPPORTED = 2,        /* BC type / solver / geometry not on this path */
+  MOSE_ERR_CUDA = 3,               /* CUDA runtime failure, or no sm_100 device */
+  MOSE_ERR_INTERFACE_STATE = 4,    /* Lib_Convective.f90:45-50 non-physical interface */
+  MOSE_ERR_NAN_OR_NEG_P = 5,       /* Lib_Newstate.f90:334-338 NaN or p < 0 */
+  MOSE_ERR_METRICS = 6,            /* Lib_Metrics.f90:286,353 det = 0 or volume <= 0 */
+  MOSE_ERR_TIMEOUT = 7,            /* a bounded device wait gave up */
+  MOSE_ERR_NOT_READY = 8           /* setup incomplete */
+};
+
+/* flux-limiter (Mod_Space.f90:45-70) */
+enum {
+  MOSE_LIMITER_FIRST_ORDER = 0,
+  MOSE_LIMITER_MINMOD = 1,
+  MOSE_LIMITER_VANLEER = 2,
+  MOSE_LIMITER_VANALBADA = 3,
+  MOSE_LIMITER_MC = 4,
+  MOSE_LIMITER_SUPERBEE = 5
+};
+
+/* riemann-solver (Mod_Riemann.f90:43-112) */
+enum {
+  MOSE_RIEMANN_HLLC = 0,
+  MOSE_RIEMANN_AUSMP = 1,
+  MOSE_RIEMANN_SLAU = 2,
+  MOSE_RIEMANN_SLAU2 = 3
+};
+
+/* Arithmetic of the face sweeps. */
+enum {
+  MOSE_PRECISION_FP64_EXACT = 0,   /* the reference's FP64 operation order, no FMA contraction */
+  MOSE_PRECISION_FP64 = 1,         /* FP64, FMA-contracted and reciprocal-folded */
+  MOSE_PRECISION_MIXED = 2         /* FP32 reconstruction + Riemann, FP64 state/accumulation */
+};
+
+/* integration-variables (Mod_Newstate.f90:30-44); only 'cons' is on this path */
+enum { MOSE_INTEGRATION_CONS = 0 };
+
+typedef struct mose_gpu_config {
+  int32_t abi_version;     /* MOSE_GPU_ABI_VERSION */
+  int32_t n_rk;            /* time-scheme: 1 = euler, 2 = RK2, 3 = RK3 */
+  double cfl;              /* cfl */
+  int32_t time_accurate;   /* time-accurate */
+  int32_t ramp_iter;       /* cfl-rise-threshold */
+  int32_t limiter;         /* MOSE_LIMITER_* */
+  int32_t riemann;         /* MOSE_RIEMANN_* */
+  int32_t integration;     /* MOSE_INTEGRATION_CONS */
+  int32_t precision;       /* MOSE_PRECISION_* */
+  int32_t ndir;            /* 0: derived from block 1 as Check_Mesh_Type does */
+  int32_t nsc;             /* number of species; must be 1 */
+  double gamma;            /* ratio of specific heats (calorically perfect gas) */
+  double rgas;             /* gas constant */
+  int32_t device;          /* CUDA device ordinal */
+  int32_t res_diter;       /* res-diter: residual-norm interval of mose_gpu_step */
+} mose_gpu_config;
+
+typedef struct mose_gpu_ctx mose_gpu_ctx;
+
+/* Fills cfg with the reference defaults (Register_Numerics.f90:30-72). */
+void mose_gpu_default_config(mose_gpu_config* cfg);
+
+/* Context.  Replaces the numerics state bound by Assign_Setup
+ * (config/Assign_Setup.f90:41-56). */
+int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out);
+void mose_gpu_destroy(mose_gpu_ctx* ctx);
+const char* mose_gpu_last_error(const mose_gpu_ctx* ctx);
+/* Offending (b,i,j,k) of the last device-detected failure (1-based). */
+int mose_gpu_error_location(const mose_gpu_ctx* ctx, int32_t* b, int32_t* i, int32_t* j, int32_t* k);
+
+/* Geometry and boundaries.  Blocks are added in order b = 1..nb. */
+int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int32_t nk,
+                       const double* node);
+/* Replaces Read_BCfile (io/IO_BC.f90:136-414) with the parsed records. */
+int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, int32_t nbound);
+/* Setup_Metrics (numerics/space/Mod_Metrics.f90:8-107) on the device, then the
+ * device tables.  Must follow add_block and set_bcs. */
+int mose_gpu_setup(mose_gpu_ctx* ctx);
+
+/* State transfer, reference layout (see above). */
+int mose_gpu_upload_prim(mose_gpu_ctx* ctx, int32_t b, const double* P);
+int mose_gpu_download_prim(mose_gpu_ctx* ctx, int32_t b, double* P);
+int mose_gpu_upload_prim_old(mose_gpu_ctx* ctx, int32_t b, const double* PO);
+int mose_gpu_download_residual(mose_gpu_ctx* ctx, int32_t b, double* R);
+int mose_gpu_upload_residual(mose_gpu_ctx* ctx, int32_t b, const double* R);
+/* dtlocal(1:ni,1:nj,1:nk) */
+int mose_gpu_download_dt(mose_gpu_ctx* ctx, int32_t b, double* dt);
+int mose_gpu_upload_dt(mose_gpu_ctx* ctx, int32_t b, const double* dt);
+
+/* The phases of Explicit_Step (numerics/time/explicit/Mod_Explicit.f90:40-85). */
+/* Compute_dt (numerics/time/Mod_dt.f90:10-106): local dt and global minimum.
+ * Starts the minimum from *dtglobal on entry (the reference passes 1d5). */
+int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ramp_iter,
+                        double* dtglobal);
+/* Set_Global_dt (Mod_dt.f90:110-130). */
+int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal);
+/* Copy_State (Mod_Explicit.f90:149-170): PO = P. */
+int mose_gpu_copy_state(mose_gpu_ctx* ctx);
+/* Fill_Ghost_Cell (numerics/space/Lib_Ghost.f90:11-137). */
+int mose_gpu_fill_ghosts(mose_gpu_ctx* ctx);
+/* Fluxes (numerics/fluxes/Mod_Fluxes.f90:10-209) followed by BC_Fluxes
+ * (numerics/fluxes/bc/Mod_BC_Fluxes.f90:10-218): R on the device. */
+int mose_gpu_residual(mose_gpu_ctx* ctx);
+/* RK_Newstate => Newstate_Conservative (numerics/time/explicit/Lib_Newstate.f90:13-160). */
+int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk);
+/* One whole Explicit_Step (Mod_Explicit.f90:10-113): dt, PO = P, then n_rk
+ * fused stages (ghost fill + residual + update in one kernel per stage).
+ * Returns dtglobal and the updated time. */
+int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time);
+/* nsteps Explicit_Steps enqueued back to back with dt kept on the device (no
+ * host round trip between steps; replayed from a CUDA graph).  Synchronises
+ * once at the end and returns the last dtglobal and time. */
+int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double* time);
+/* Compute_Residual (diagnostic/Mod_Diagnostic.f90:13-50): sums over all
+ * blocks of (|d rho|, |du|, |dv|, |dw|, |dp|)^2 between P and PO; total[5]. */
+int mose_gpu_residual_norms(mose_gpu_ctx* ctx, double* total);
+
+int mose_gpu_set_time(mose_gpu_ctx* ctx, double time, int32_t iter);
+int mose_gpu_get_time(mose_gpu_ctx* ctx, double* time, int32_t* iter);
+/* Waits for the context's stream and reports any device-detected failure. */
+int mose_gpu_synchronize(mose_gpu_ctx* ctx);
+
+/* Introspection for tests and the benchmark. */
+/* The context's cudaStream_t (as void*), for events or work ordered with it. */
+void* mose_gpu_stream(const mose_gpu_ctx* ctx);
+/* Runs nsteps fused Explicit_Steps without graph replay, with CUDA events
+ * between kernels, and returns the summed device time in ms per kernel class:
+ * ms[0] dt pass + step bookkeeping, ms[1] ghost fill, ms[2] stage kernels;
+ * launches[c] counts the launches of each class.  Advances the solution. */
+int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t* launches);
+/* 1 when every metric of every block is uniform and the constant-metric
+ * kernels are used. */
+int mose_gpu_uniform_metrics(const mose_gpu_ctx* ctx);
+/* Number of kernel launches this context issued since creation. */
+int64_t mose_gpu_launch_count(const mose_gpu_ctx* ctx);
+/* Device metrics of block b in the reference layout: vol(ghosted cells),
+ * dl(3, ghosted cells) along each direction's ghosted line, and face N(3), A
+ * over dir(d)%f bounds (see the reference's Mod_Allocate_Data.f90:103-108).
+ * Entries the device does not hold are left untouched. */
+int mose_gpu_download_metrics(mose_gpu_ctx* ctx, int32_t b, double* vol, double* dl);
+int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N, double* A);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MOSE_GPU_H */

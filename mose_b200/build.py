@@ -1,0 +1,86 @@
+"""Builds libmose_gpu.so (the C-ABI library) in-tree with nvcc for sm_100a.
+
+The reference-exact translation unit is compiled with --fmad=false so that no
+multiply-add contraction changes the rounding of the reference's FP64
+expressions.  Outputs go to mose_b200/lib/.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+LIBDIR = HERE / "lib"
+OBJDIR = HERE / "_build"
+LIBNAME = "libmose_gpu.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+                 "-I", str(CSRC), "-I", str(HERE.parent / "include")]
+
+# translation unit -> extra flags
+UNITS = {
+    "kernels_exact.cu": ["--fmad=false"],
+    "stage_exact_r0.cu": ["--fmad=false"],
+    "stage_exact_r1.cu": ["--fmad=false"],
+    "stage_exact_r2.cu": ["--fmad=false"],
+    "stage_exact_r3.cu": ["--fmad=false"],
+    "mose_gpu.cu": [],
+}
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _deps() -> list[Path]:
+    return sorted(CSRC.glob("*.cu*")) + sorted(CSRC.glob("*.h")) + [HERE.parent / "include" / "mose_gpu.h"]
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compiles every unit that changed and links the shared library."""
+    OBJDIR.mkdir(exist_ok=True)
+    LIBDIR.mkdir(exist_ok=True)
+    deps = _deps()
+    objs = []
+    cc = nvcc()
+    jobs = []
+    for unit, extra in UNITS.items():
+        obj = OBJDIR / (unit + ".o")
+        objs.append(obj)
+        if force or _stale(obj, deps):
+            jobs.append([cc] + COMMON + extra + ["-c", str(CSRC / unit), "-o", str(obj)])
+    # units compile independently: run them in parallel
+    procs = []
+    for cmd in jobs:
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        procs.append((cmd, subprocess.Popen(cmd)))
+    failed = [cmd for cmd, p in procs if p.wait() != 0]
+    if failed:
+        raise RuntimeError("nvcc failed: " + " ".join(failed[0]))
+    lib = LIBDIR / LIBNAME
+    if force or _stale(lib, objs):
+        cmd = [cc] + ARCH + ["-shared", "-cudart=static", "-o", str(lib)] + [str(o) for o in objs]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return lib
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)

@@ -1,0 +1,269 @@
+"""Synthetic multi-block cases in the reference's data formats.
+
+A case is the data MOSE reads at setup: block node arrays (MESH/*.tec),
+the face-by-face boundary list (INPUT/bc.txt) and an initial state
+(INPUT/ic.tec), plus the numerics of input.ini.  Arrays use the
+reference's Fortran layouts, expressed as C-contiguous numpy arrays with the
+fastest Fortran index last:
+
+  nodes[b] : (nk+1, nj+1, ni+1, 3)  == Fortran node(3, 0:ni, 0:nj, 0:nk)
+  prim[b]  : (nk,   nj,   ni,   5)  == interior P(5, 1:ni, 1:nj, 1:nk)
+  bc_rec   : (nbound, 15) int32     == b i j k f type bs is js ks fs d11 d12 d21 d22
+  bc_data  : (nbound, 6)  float64   == 405: mach T p alpha beta rel_fac ; 406: p_back rel_fac
+
+The five benchmark configurations are built from seeded synthetic inputs of
+the shapes the reference problem statement names; no external dataset is used.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+GC = 2
+NPRIM = 5
+
+# limiter / riemann names as in input.ini (Register_Numerics.f90:57-72)
+LIMITERS = {"first-order": 0, "none": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5}
+RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3}
+
+
+@dataclass
+class Case:
+    name: str
+    nodes: list
+    bc_rec: np.ndarray
+    bc_data: np.ndarray
+    prim: list
+    n_rk: int = 3
+    cfl: float = 0.5
+    time_accurate: bool = True
+    limiter: str = "minmod"
+    riemann: str = "HLLC"
+    gamma: float = 1.4
+    rgas: float = 1.0
+    steps: int = 1
+    t_end: float | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def dims(self):
+        return [(n.shape[2] - 1, n.shape[1] - 1, n.shape[0] - 1) for n in self.nodes]
+
+    @property
+    def ncells(self) -> int:
+        return int(sum(ni * nj * nk for ni, nj, nk in self.dims))
+
+
+def to_ref_layout(prim: np.ndarray) -> np.ndarray:
+    """Interior (nk,nj,ni,5) -> ghosted reference layout (nk+4,nj+4,ni+4,5), ghosts 0."""
+    nk, nj, ni, nv = prim.shape
+    out = np.zeros((nk + 2 * GC, nj + 2 * GC, ni + 2 * GC, nv), dtype=np.float64)
+    out[GC:GC + nk, GC:GC + nj, GC:GC + ni, :] = prim
+    return out
+
+
+def interior(ref: np.ndarray) -> np.ndarray:
+    """Ghosted reference layout -> interior view."""
+    return ref[GC:-GC, GC:-GC, GC:-GC, :]
+
+
+def cartesian_nodes(ni: int, nj: int, nk: int, lo=(0.0, 0.0, 0.0), hi=(1.0, 1.0, 1.0),
+                    offs=(0, 0, 0), ntot=None) -> np.ndarray:
+    """Uniform Cartesian nodes.  Coordinates are lo + (hi-lo)*(offs+i)/ntot so that
+    neighbouring blocks of a global grid share node coordinates bit for bit."""
+    ntot = ntot or (ni, nj, nk)
+    axes = []
+    for n, a, b, o, t in zip((ni, nj, nk), lo, hi, offs, ntot):
+        idx = np.arange(n + 1, dtype=np.float64) + o
+        axes.append(a + (b - a) * idx / t)
+    z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
+    return np.ascontiguousarray(np.stack([x, y, z], axis=-1))
+
+
+def _face_cells(ni, nj, nk, f):
+    """(i, j, k) 1-based of the cells of face f, in file order (k, j, i loops)."""
+    if f in (1, 2):
+        i = 1 if f == 1 else ni
+        return [(i, j, k) for k in range(1, nk + 1) for j in range(1, nj + 1)]
+    if f in (3, 4):
+        j = 1 if f == 3 else nj
+        return [(i, j, k) for k in range(1, nk + 1) for i in range(1, ni + 1)]
+    k = 1 if f == 5 else nk
+    return [(i, j, k) for j in range(1, nj + 1) for i in range(1, ni + 1)]
+
+
+def build_bcs(dims, face_spec):
+    """Boundary records in bc.txt order.
+
+    face_spec(b, f) -> ("bc", type, data6) | ("conn", type, bs, fs) with 1-based
+    blocks.  Connections map face cells with identity orientation
+    (d11=1, d12=0, d21=0, d22=1) onto the matching cell of the source face.
+    """
+    recs, data = [], []
+    for b, (ni, nj, nk) in enumerate(dims, start=1):
+        for f in range(1, 7):
+            spec = face_spec(b, f)
+            for (i, j, k) in _face_cells(ni, nj, nk, f):
+                if spec[0] == "bc":
+                    _, t, d6 = spec
+                    recs.append([b, i, j, k, f, t, 0, 0, 0, 0, 0, 0, 0, 0, 0])
+                    data.append(list(d6))
+                else:
+                    _, t, bs, fs = spec
+                    sni, snj, snk = dims[bs - 1]
+                    si, sj, sk = i, j, k
+                    if fs == 1: si = 1
+                    elif fs == 2: si = sni
+                    elif fs == 3: sj = 1
+                    elif fs == 4: sj = snj
+                    elif fs == 5: sk = 1
+                    else: sk = snk
+                    recs.append([b, i, j, k, f, t, bs, si, sj, sk, fs, 1, 0, 0, 1])
+                    data.append([0.0] * 6)
+    return np.asarray(recs, dtype=np.int32), np.asarray(data, dtype=np.float64)
+
+
+def cell_centres(nodes: np.ndarray):
+    """Cell centres (nk,nj,ni,3) as the mean of the 8 corner nodes."""
+    n = nodes
+    c = (n[:-1, :-1, :-1] + n[:-1, :-1, 1:] + n[:-1, 1:, :-1] + n[:-1, 1:, 1:] +
+         n[1:, :-1, :-1] + n[1:, :-1, 1:] + n[1:, 1:, :-1] + n[1:, 1:, 1:]) / 8.0
+    return c
+
+
+# ---------------------------------------------------------------------------
+# The five benchmark configurations
+# ---------------------------------------------------------------------------
+def sod(ncell: int = 1000, limiter="minmod", riemann="HLLC", cfl=0.5, t_end=0.2) -> Case:
+    """1-D Sod shock tube on [0,1], diaphragm at 0.5, transmissive (400) ends."""
+    nodes = cartesian_nodes(ncell, 1, 1, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0))
+    xc = cell_centres(nodes)[..., 0]
+    prim = np.zeros((1, 1, ncell, NPRIM))
+    left = xc < 0.5
+    prim[..., 0] = np.where(left, 1.0, 0.125)
+    prim[..., 4] = np.where(left, 1.0, 0.1)
+    spec = lambda b, f: ("bc", 400 if f <= 4 else 0, [0.0] * 6)
+    rec, data = build_bcs([(ncell, 1, 1)], spec)
+    return Case("sod1d", [nodes], rec, data, [prim], n_rk=3, cfl=cfl, time_accurate=True,
+                limiter=limiter, riemann=riemann, gamma=1.4, rgas=1.0, t_end=t_end)
+
+
+def isentropic_vortex(n: int = 2048, steps: int = 100, limiter="vanalbada", riemann="HLLC",
+                      cfl=0.8, L=10.0, strength=5.0, mach=0.5, gamma=1.4) -> Case:
+    """2-D isentropic vortex (strength 5, core radius 1) on a periodic [0,L]^2 block,
+    free stream rho = p = 1, Mach 0.5 at 45 degrees.  Periodic seams are 201
+    (connection with extrapolated ghost metrics)."""
+    nodes = cartesian_nodes(n, n, 1, (0.0, 0.0, 0.0), (L, L, 1.0))
+    c = cell_centres(nodes)
+    x, y = c[..., 0], c[..., 1]
+    xc = yc = L / 2
+    r2 = (x - xc) ** 2 + (y - yc) ** 2
+    ainf = np.sqrt(gamma)
+    uinf = vinf = mach * ainf / np.sqrt(2.0)
+    f = np.exp(0.5 * (1.0 - r2))
+    du = -strength / (2 * np.pi) * f * (y - yc)
+    dv = strength / (2 * np.pi) * f * (x - xc)
+    T = 1.0 - (gamma - 1.0) * strength ** 2 / (8.0 * gamma * np.pi ** 2) * np.exp(1.0 - r2)
+    rho = T ** (1.0 / (gamma - 1.0))
+    prim = np.zeros((1, n, n, NPRIM))
+    prim[..., 0] = rho
+    prim[..., 1] = uinf + du
+    prim[..., 2] = vinf + dv
+    prim[..., 4] = rho ** gamma
+
+    def spec(b, f):
+        if f >= 5:
+            return ("bc", 0, [0.0] * 6)
+        return ("conn", 201, 1, {1: 2, 2: 1, 3: 4, 4: 3}[f])
+
+    rec, data = build_bcs([(n, n, 1)], spec)
+    return Case("vortex2d", [nodes], rec, data, [prim], n_rk=3, cfl=cfl, time_accurate=True,
+                limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps)
+
+
+def four_quadrant(seed: int = 0, nbx: int = 8, nby: int = 8, nmin: int = 64, nmax: int = 1024,
+                  steps: int = 100, limiter="minmod", riemann="AUSM+", cfl=0.5, gamma=1.4,
+                  split=(0.5, 0.5)) -> Case:
+    """2-D four-quadrant Riemann problem on [0,1]^2 split into nbx x nby blocks
+    whose column widths / row heights are drawn from default_rng(seed) in
+    [nmin, nmax]; conforming 101 interfaces, transmissive (400) outer faces."""
+    rng = np.random.default_rng(seed)
+    nx = rng.integers(nmin, nmax + 1, size=nbx)
+    ny = rng.integers(nmin, nmax + 1, size=nby)
+    Nx, Ny = int(nx.sum()), int(ny.sum())
+    ox = np.concatenate([[0], np.cumsum(nx)[:-1]])
+    oy = np.concatenate([[0], np.cumsum(ny)[:-1]])
+    nodes, prims, dims = [], [], []
+    quad = {  # (rho, u, v, p)
+        "NE": (1.5, 0.0, 0.0, 1.5), "NW": (0.5323, 1.206, 0.0, 0.3),
+        "SW": (0.138, 1.206, 1.206, 0.029), "SE": (0.5323, 0.0, 1.206, 0.3)}
+    for by in range(nby):
+        for bx in range(nbx):
+            ni, nj = int(nx[bx]), int(ny[by])
+            nd = cartesian_nodes(ni, nj, 1, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0),
+                                 offs=(int(ox[bx]), int(oy[by]), 0), ntot=(Nx, Ny, 1))
+            c = cell_centres(nd)
+            east, north = c[..., 0] > split[0], c[..., 1] > split[1]
+            p = np.zeros((1, nj, ni, NPRIM))
+            for key, mask in (("NE", east & north), ("NW", ~east & north),
+                              ("SW", ~east & ~north), ("SE", east & ~north)):
+                r, u, v, pr = quad[key]
+                p[..., 0][mask] = r
+                p[..., 1][mask] = u
+                p[..., 2][mask] = v
+                p[..., 4][mask] = pr
+            nodes.append(nd)
+            prims.append(p)
+            dims.append((ni, nj, 1))
+
+    def spec(b, f):
+        bx, by = (b - 1) % nbx, (b - 1) // nbx
+        if f >= 5:
+            return ("bc", 0, [0.0] * 6)
+        nb = {1: (bx - 1, by, 2), 2: (bx + 1, by, 1), 3: (bx, by - 1, 4), 4: (bx, by + 1, 3)}[f]
+        if 0 <= nb[0] < nbx and 0 <= nb[1] < nby:
+            return ("conn", 101, nb[1] * nbx + nb[0] + 1, nb[2])
+        return ("bc", 400, [0.0] * 6)
+
+    rec, data = build_bcs(dims, spec)
+    return Case("quadrant2d", nodes, rec, data, prims, n_rk=3, cfl=cfl, time_accurate=True,
+                limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps,
+                extra={"nx": nx.tolist(), "ny": ny.tolist(), "seed": seed, "split": split})
+
+
+def curvilinear_channel(n: int = 512, steps: int = 200, mach: float = 0.8, amp: float = 0.05,
+                        limiter="vanalbada", riemann="HLLC", cfl=0.5, gamma=1.4) -> Case:
+    """2-D curvilinear block x = xi + a sin(2 pi eta), y = eta + a sin(2 pi xi) on
+    [0,1]^2; uniform Mach 0.8 flow, supersonic-static inflow (405) on the left,
+    outflow (406) at the free-stream pressure on the right, slip walls (300)."""
+    xi = np.arange(n + 1, dtype=np.float64) / n
+    eta = np.arange(n + 1, dtype=np.float64) / n
+    E, X = np.meshgrid(eta, xi, indexing="ij")
+    x = X + amp * np.sin(2 * np.pi * E)
+    y = E + amp * np.sin(2 * np.pi * X)
+    nodes = np.zeros((2, n + 1, n + 1, 3))
+    for k in range(2):
+        nodes[k, ..., 0] = x
+        nodes[k, ..., 1] = y
+        nodes[k, ..., 2] = float(k)
+    p_inf = 1.0 / gamma
+    prim = np.zeros((1, n, n, NPRIM))
+    prim[..., 0] = 1.0
+    prim[..., 1] = mach
+    prim[..., 4] = p_inf
+    T_inf = p_inf / 1.0
+
+    def spec(b, f):
+        if f == 1:
+            return ("bc", 405, [mach, T_inf, p_inf, 0.0, 0.0, 1.0])
+        if f == 2:
+            return ("bc", 406, [p_inf, 1.0, 0.0, 0.0, 0.0, 0.0])
+        if f in (3, 4):
+            return ("bc", 300, [0.0] * 6)
+        return ("bc", 0, [0.0] * 6)
+
+    rec, data = build_bcs([(n, n, 1)], spec)
+    return Case("channel2d", [nodes], rec, data, [prim], n_rk=3, cfl=cfl, time_accurate=True,
+                limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps,
+                extra={"mach": mach})

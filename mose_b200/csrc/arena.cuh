@@ -1,0 +1,37 @@
+// arena.cuh -- argument bundles shared by the host driver and the kernels.
+#pragma once
+
+#include "common.cuh"
+
+namespace mose {
+
+// Metric arenas (general-metric kernels).  Every plane has the indexing of a
+// state plane of its block (offset BlockDesc::mbase * planes).
+struct MetricArgs {
+  const double* dl;     // 3 planes per block: dl along i, j, k (ghosted along that direction)
+  const double* face;   // 12 planes per block: for dir d: nx, ny, nz, A of the low face of each cell
+  const double* vol;    // 1 plane
+  const double* vers;   // 9 planes: versor of direction d, component q at plane 3 d + q
+};
+
+struct StageArgs {
+  const BlockDesc* blk;
+  const int4* items;    // (block, first column, first row, last row + 1)
+  int nitems;
+  const double* Pc;     // current state arena
+  const double* Po;     // state at the start of the step (Copy_State's PO)
+  double* Pn;           // next state (fused mode)
+  double* R;            // residual arena (residual-only mode)
+  MetricArgs m;
+  const double* dtl;    // local dt plane arena (one plane per block), or null
+  const double* dtg;    // device scalar dtglobal (time-accurate)
+  const int* bcw;       // boundary words, see bc_code()
+  const BcParam* bcp;
+  double c_rk;          // RKcoeff(n_rk, irk)
+  int irk;
+  int time_accurate;
+  DevError* err;
+  Gas g;
+};
+
+}  // namespace mose

@@ -1,0 +1,98 @@
+// common.cuh -- device data model of the MOSE residual/update path on B200.
+//
+// HBM layout.  Every block owns, inside arenas shared by all blocks:
+//   * the state: SoA planes of primitives (rho, u, v, [w,] p), one plane per
+//     variable, each plane the block's cells plus two ghost layers in the
+//     ACTIVE directions only (i, j in 2-D; i, j, k in 3-D).  Rows are padded to
+//     a multiple of 16 doubles; block bases are 256-byte aligned.
+//   * metric planes with the same indexing as one state plane: dl along each
+//     direction, cell volume, face normal + area of the face on the low side
+//     of each cell (face i-1/2 stored at cell i), and the CFL versors.
+// In 2-D the reference carries w == 0 exactly (face normals have n_z == 0 on
+// planar meshes and the k faces are null), so the device keeps 4 variables.
+#pragma once
+
+#include <cstdint>
+
+namespace mose {
+
+constexpr int GW = 2;  // ghost layers (Global_m.f90:17 gc = 2)
+
+// Stage-kernel strip: STRIP_T threads per CTA own STRIP_W = STRIP_T - 2 cell
+// columns plus one halo column on each side.
+constexpr int STRIP_T = 128;
+constexpr int STRIP_W = STRIP_T - 2;
+
+// Internal boundary codes (reference bc.txt types in parentheses).
+enum BcCode : int {
+  BC_NONE = 0,      // (0)   null face: zero-gradient ghosts, no flux
+  BC_CONN = 1,      // (101, 201) block connection / periodic
+  BC_SYM = 2,       // (300) symmetry / slip wall
+  BC_EXTRAP = 3,    // (400) extrapolation
+  BC_SUPIN = 4,     // (405) supersonic inflow (M, T, p)
+  BC_OUTFLOW = 5,   // (406) outflow with back pressure
+};
+
+// Error word written by kernels (first offender wins).
+struct DevError {
+  int code;
+  int b, i, j, k;   // 1-based, reference indexing
+};
+
+struct Gas {
+  double gamma, R, cp, cv;
+  double cpmR;      // 0.5*(cp+cp) - R, as roe_averages forms it
+};
+
+// Per-block descriptor (device resident).
+struct BlockDesc {
+  int ni, nj, nk;       // interior cells
+  int px, py, pz;       // ghosted extents; px padded.  pz = 1 in 2-D.
+  long long plane;      // px * py
+  long long vstride;    // plane * pz: distance between SoA variable planes
+  long long sbase;      // offset of this block in the state arenas (doubles)
+  long long mbase;      // offset of this block in the one-plane arenas
+  int bcoff[6];         // offset of face f's per-cell BC words in the BC table
+  int bcn[6];           // number of face cells on face f
+  // Uniform metrics (valid when the context runs the constant-metric kernels)
+  double u_dl[3];
+  double u_n[3][3];     // face normal per direction
+  double u_A[3];        // face area per direction
+  double u_vol;
+  double u_vers[3][3];  // CFL versor per direction
+};
+
+// Cell offset inside one plane of block d (i, j, k 0-based, ghosts negative).
+__host__ __device__ inline long long cell_off2(const BlockDesc& d, int i, int j) {
+  return (long long)(j + GW) * d.px + (i + GW);
+}
+__host__ __device__ inline long long cell_off3(const BlockDesc& d, int i, int j, int k) {
+  return (long long)(k + GW) * d.plane + (long long)(j + GW) * d.px + (i + GW);
+}
+
+// BC word: low 8 bits = BcCode, high bits = parameter record index + 1.
+__host__ __device__ inline int bc_code(int w) { return w & 0xff; }
+__host__ __device__ inline int bc_param(int w) { return (w >> 8) - 1; }
+
+// Parameters of a 405 / 406 face cell, precomputed on the host.
+struct BcParam {
+  double mach, T, p, rel_fac;
+  double ca, sa, cb, sb;   // cos/sin of the inflow angles (alpha, beta)
+  double pback;
+};
+
+// One ghost-fill record (Lib_Ghost.f90 dispatch), 0-based cells.
+struct GhostRec {
+  int type;                 // BcCode of the face
+  int b, i, j, k, f;        // boundary cell and face (1..6)
+  int bs, is, js, ks, fs;   // connection source
+};
+
+// One boundary record for the ghost-metric kernel (1-based reference indices).
+struct GhostMetricRec {
+  int type;
+  int b, I, J, K, F;
+  int bs, Is, Js, Ks, Fs, d11, d12, d21, d22;
+};
+
+}  // namespace mose

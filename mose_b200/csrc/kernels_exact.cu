@@ -1,0 +1,702 @@
+// kernels_exact.cu -- the reference-exact FP64 kernels.  Built with
+// --fmad=false: no multiply-add contraction, every operation rounds once in
+// the order of the reference's Fortran expressions.
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "metrics.cuh"
+#include "stage2d.cuh"
+
+namespace mose {
+
+// ---------------------------------------------------------------------------
+// Metrics (Mod_Metrics.f90:8-107)
+// ---------------------------------------------------------------------------
+// Interior cells: Compute_Metric_Tensor -> dl, vol, CFL versors.
+__global__ void k_cell_metrics(const BlockDesc* blk, int b, NodeView nv, double* dl, double* vol,
+                               double* vers, int nd, int ndir, DevError* err) {
+  const BlockDesc& d = blk[b];
+  long long n = (long long)d.ni * d.nj * d.nk;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    int I = i + 1, J = j + 1, K = k + 1;   // reference indices
+    double M[9], l[3], v;
+    bool ok = metric_tensor(nv.at(I - 1, J - 1, K - 1), nv.at(I - 1, J - 1, K), nv.at(I - 1, J, K - 1),
+                            nv.at(I - 1, J, K), nv.at(I, J - 1, K - 1), nv.at(I, J - 1, K), nv.at(I, J, K - 1),
+                            nv.at(I, J, K), M, l, &v);
+    if (!ok) report(err, 6, b, i, j, k);
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    long long vs = d.vstride, mb = d.mbase;
+    for (int h = 0; h < 3; ++h) dl[3 * mb + h * vs + o] = l[h];
+    vol[mb + o] = v;
+    // versor = M(d,:)/norm2(M(d,:))  (Mod_dt.f90:78-80)
+    for (int dd = 0; dd < ndir; ++dd) {
+      double m0 = M[dd + 0], m1 = M[dd + 3], m2 = M[dd + 6];
+      double nrm = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+      vers[9 * mb + (3 * dd + 0) * vs + o] = m0 / nrm;
+      vers[9 * mb + (3 * dd + 1) * vs + o] = m1 / nrm;
+      vers[9 * mb + (3 * dd + 2) * vs + o] = m2 / nrm;
+    }
+  }
+}
+
+// Compute_Norm_Area (Lib_Metrics.f90:69-247).  One thread per face of the
+// direction; stored with the cell on the high side of the face.
+__global__ void k_face_metrics(const BlockDesc* blk, int b, NodeView nv, double* face, int nd, int dir) {
+  const BlockDesc& d = blk[b];
+  int ei = d.ni + (dir == 0), ej = d.nj + (dir == 1), ek = d.nk + (dir == 2);
+  long long n = (long long)ei * ej * ek;
+  double s[3];
+  face_signs(nv, s);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % ei), j = (int)((q / ei) % ej), k = (int)(q / ((long long)ei * ej));
+    // reference face indices: dir(1)%f(0:ni,1:nj,1:nk) etc.
+    int I = (dir == 0) ? i : i + 1, J = (dir == 1) ? j : j + 1, K = (dir == 2) ? k : k + 1;
+    double nrm[3], A;
+    face_metric(nv, dir, I, J, K, s[dir], nrm, &A);
+    // the face with reference index I (dir 0) is the low face of 0-based cell I
+    int ci = (dir == 0) ? I : I - 1, cj = (dir == 1) ? J : J - 1, ck = (dir == 2) ? K : K - 1;
+    if (nd == 2 && dir == 2) continue;
+    long long o = (nd == 3) ? cell_off3(d, ci, cj, ck) : cell_off2(d, ci, cj);
+    long long vs = d.vstride, mb = d.mbase;
+    double* f = face + 12 * mb + (4 * dir) * vs + o;
+    f[0] = nrm[0]; f[vs] = nrm[1]; f[2 * vs] = nrm[2]; f[3 * vs] = A;
+  }
+}
+
+// Ghost dl along the face direction for each boundary record:
+// BC_Connect_Metrics (101), BC_Symmetry_Metrics (300), BC_Extrapolate_Metrics
+// (everything else), Lib_Metrics.f90:535-1092.
+__device__ void store_ghost_dl(const BlockDesc* blk, double* dl, int b, int nd, int I, int J, int K, int dir,
+                               double val) {
+  const BlockDesc& d = blk[b];
+  long long o = (nd == 3) ? cell_off3(d, I - 1, J - 1, K - 1) : cell_off2(d, I - 1, J - 1);
+  dl[3 * d.mbase + dir * d.vstride + o] = val;
+}
+
+__global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs, int nrec,
+                                const NodeView* nodes, double* dl, int nd, int ndir, DevError* err) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrec) return;
+  const GhostMetricRec e = recs[q];
+  const int dir = (e.F - 1) / 2;
+  if (dir >= nd) return;
+  const BlockDesc& bm = blk[e.b];
+  const NodeView& nv = nodes[e.b];
+  const int Im = e.I, Jm = e.J, Km = e.K;
+  double M[9], l[3], v;
+  bool ok = true;
+  if (e.type == 300) {
+    // BC_Symmetry_Metrics: ghost g takes the metrics of the g-th interior cell
+    for (int g = 1; g <= GW; ++g) {
+      int gi = Im, gj = Jm, gk = Km, si = Im, sj = Jm, sk = Km;
+      switch (e.F) {
+        case 1: gi = Im - g; si = Im + g - 1; break;
+        case 2: gi = Im + g; si = Im - g + 1; break;
+        case 3: gj = Jm - g; sj = Jm + g - 1; break;
+        case 4: gj = Jm + g; sj = Jm - g + 1; break;
+        case 5: gk = Km - g; sk = Km + g - 1; break;
+        case 6: gk = Km + g; sk = Km - g + 1; break;
+      }
+      long long so = (nd == 3) ? cell_off3(bm, si - 1, sj - 1, sk - 1) : cell_off2(bm, si - 1, sj - 1);
+      double val = dl[3 * bm.mbase + dir * bm.vstride + so];
+      store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, val);
+    }
+    return;
+  }
+  V3 N[8][2 * GW + 1];
+  if (e.type == 101) {
+    const NodeView& ns = nodes[e.bs];
+    const int guides[6][3] = {{0, 0, 0}, {-1, 0, 0}, {0, 0, 0}, {0, -1, 0}, {0, 0, 0}, {0, 0, -1}};
+    const int guides2[6][3] = {{1, 0, 0}, {-2, 0, 0}, {0, 1, 0}, {0, -2, 0}, {0, 0, 1}, {0, 0, -2}};
+    switch (e.F) {
+      case 1: N[0][0] = nv.at(Im - 1, Jm - 1, Km - 1); N[1][0] = nv.at(Im - 1, Jm - 1, Km);
+              N[2][0] = nv.at(Im - 1, Jm, Km - 1); N[3][0] = nv.at(Im - 1, Jm, Km); break;
+      case 2: N[4][0] = nv.at(Im, Jm - 1, Km - 1); N[5][0] = nv.at(Im, Jm - 1, Km);
+              N[6][0] = nv.at(Im, Jm, Km - 1); N[7][0] = nv.at(Im, Jm, Km); break;
+      case 3: N[0][0] = nv.at(Im - 1, Jm - 1, Km - 1); N[1][0] = nv.at(Im - 1, Jm - 1, Km);
+              N[4][0] = nv.at(Im, Jm - 1, Km - 1); N[5][0] = nv.at(Im, Jm - 1, Km); break;
+      case 4: N[2][0] = nv.at(Im - 1, Jm, Km - 1); N[3][0] = nv.at(Im - 1, Jm, Km);
+              N[6][0] = nv.at(Im, Jm, Km - 1); N[7][0] = nv.at(Im, Jm, Km); break;
+      case 5: N[0][0] = nv.at(Im - 1, Jm - 1, Km - 1); N[2][0] = nv.at(Im - 1, Jm, Km - 1);
+              N[4][0] = nv.at(Im, Jm - 1, Km - 1); N[6][0] = nv.at(Im, Jm, Km - 1); break;
+      case 6: N[1][0] = nv.at(Im - 1, Jm - 1, Km); N[3][0] = nv.at(Im - 1, Jm, Km);
+              N[5][0] = nv.at(Im, Jm - 1, Km); N[7][0] = nv.at(Im, Jm, Km); break;
+    }
+    const int slotA[6] = {3, 7, 5, 7, 6, 7}, slotB[6] = {1, 5, 1, 3, 2, 3};
+    const int slotC[6] = {2, 6, 4, 6, 4, 5}, slotD[6] = {0, 4, 0, 2, 0, 1};
+    const int Fs = e.Fs;
+    for (int g = 1; g <= GW; ++g) {
+      int Is1 = e.Is + (GW - g) * guides[Fs - 1][0] + (g - 1) * guides2[Fs - 1][0];
+      int Js1 = e.Js + (GW - g) * guides[Fs - 1][1] + (g - 1) * guides2[Fs - 1][1];
+      int Ks1 = e.Ks + (GW - g) * guides[Fs - 1][2] + (g - 1) * guides2[Fs - 1][2];
+      int II, JJ, KK;
+      if (Fs <= 2) { II = Is1; JJ = (2 * Js1 + e.d11 + e.d21) / 2; KK = (2 * Ks1 + e.d12 + e.d22) / 2; }
+      else if (Fs <= 4) { II = (2 * Is1 + e.d11 + e.d21) / 2; JJ = Js1; KK = (2 * Ks1 + e.d12 + e.d22) / 2; }
+      else { II = (2 * Is1 + e.d11 + e.d21) / 2; JJ = (2 * Js1 + e.d12 + e.d22) / 2; KK = Ks1; }
+      N[slotA[e.F - 1]][g] = ns.at(II, JJ, KK);
+      int a1, a2, a3;
+      if (Fs <= 2) { a1 = II; a2 = JJ - e.d11; a3 = KK - e.d12; }
+      else if (Fs <= 4) { a1 = II - e.d11; a2 = JJ; a3 = KK - e.d12; }
+      else { a1 = II - e.d11; a2 = JJ - e.d12; a3 = KK; }
+      N[slotB[e.F - 1]][g] = ns.at(a1, a2, a3);
+      if (Fs <= 2) { a1 = II; a2 = JJ - e.d21; a3 = KK - e.d22; }
+      else if (Fs <= 4) { a1 = II - e.d21; a2 = JJ; a3 = KK - e.d22; }
+      else { a1 = II - e.d21; a2 = JJ - e.d22; a3 = KK; }
+      N[slotC[e.F - 1]][g] = ns.at(a1, a2, a3);
+      if (Fs <= 2) { a1 = II; a2 = JJ - e.d11 - e.d21; a3 = KK - e.d12 - e.d22; }
+      else if (Fs <= 4) { a1 = II - e.d11 - e.d21; a2 = JJ; a3 = KK - e.d12 - e.d22; }
+      else { a1 = II - e.d11 - e.d21; a2 = JJ - e.d12 - e.d22; a3 = KK; }
+      N[slotD[e.F - 1]][g] = ns.at(a1, a2, a3);
+      int gi = Im, gj = Jm, gk = Km;
+      switch (e.F) {
+        case 1: ok &= metric_tensor(N[0][g], N[1][g], N[2][g], N[3][g], N[0][g - 1], N[1][g - 1], N[2][g - 1], N[3][g - 1], M, l, &v); gi = Im - g; break;
+        case 2: ok &= metric_tensor(N[4][g - 1], N[5][g - 1], N[6][g - 1], N[7][g - 1], N[4][g], N[5][g], N[6][g], N[7][g], M, l, &v); gi = Im + g; break;
+        case 3: ok &= metric_tensor(N[0][g], N[1][g], N[0][g - 1], N[1][g - 1], N[4][g], N[5][g], N[4][g - 1], N[5][g - 1], M, l, &v); gj = Jm - g; break;
+        case 4: ok &= metric_tensor(N[2][g - 1], N[3][g - 1], N[2][g], N[3][g], N[6][g - 1], N[7][g - 1], N[6][g], N[7][g], M, l, &v); gj = Jm + g; break;
+        case 5: ok &= metric_tensor(N[0][g], N[0][g - 1], N[2][g], N[2][g - 1], N[4][g], N[4][g - 1], N[6][g], N[6][g - 1], M, l, &v); gk = Km - g; break;
+        case 6: ok &= metric_tensor(N[1][g - 1], N[1][g], N[3][g - 1], N[3][g], N[5][g - 1], N[5][g], N[7][g - 1], N[7][g], M, l, &v); gk = Km + g; break;
+      }
+      store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, l[dir]);
+    }
+  } else {
+    // BC_Extrapolate_Metrics (delthe = 0 branches)
+    auto at = [&](int slot, int g) -> V3& { return N[slot][g + GW]; };
+    switch (e.F) {
+      case 1:
+        for (int g = 0; g <= GW; ++g) {
+          at(0, g) = nv.at(Im + g - 1, Jm - 1, Km - 1); at(1, g) = nv.at(Im + g - 1, Jm - 1, Km);
+          at(2, g) = nv.at(Im + g - 1, Jm, Km - 1); at(3, g) = nv.at(Im + g - 1, Jm, Km);
+        }
+        for (int g = -1; g >= -GW; --g) {
+          for (int s = 0; s < 4; ++s) at(s, g) = v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3));
+          ok &= metric_tensor(at(0, g), at(1, g), at(2, g), at(3, g), at(0, g + 1), at(1, g + 1), at(2, g + 1), at(3, g + 1), M, l, &v);
+          store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir]);
+        }
+        break;
+      case 2:
+        for (int g = 0; g >= -GW; --g) {
+          at(4, g) = nv.at(Im + g, Jm - 1, Km - 1); at(5, g) = nv.at(Im + g, Jm - 1, Km);
+          at(6, g) = nv.at(Im + g, Jm, Km - 1); at(7, g) = nv.at(Im + g, Jm, Km);
+        }
+        for (int g = 1; g <= GW; ++g) {
+          for (int s = 4; s < 8; ++s) at(s, g) = v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3));
+          ok &= metric_tensor(at(4, g - 1), at(5, g - 1), at(6, g - 1), at(7, g - 1), at(4, g), at(5, g), at(6, g), at(7, g), M, l, &v);
+          store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir]);
+        }
+        break;
+      case 3: {
+        bool cubic = bm.nj > 2;
+        int gtop = cubic ? GW : 1;
+        for (int g = 0; g <= gtop; ++g) {
+          at(0, g) = nv.at(Im - 1, Jm + g - 1, Km - 1); at(1, g) = nv.at(Im - 1, Jm + g - 1, Km);
+          at(4, g) = nv.at(Im, Jm + g - 1, Km - 1); at(5, g) = nv.at(Im, Jm + g - 1, Km);
+        }
+        for (int g = -1; g >= -GW; --g) {
+          const int sl[4] = {0, 1, 4, 5};
+          for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3)) : v3lin2(at(s, g + 1), at(s, g + 2));
+          ok &= metric_tensor(at(0, g), at(1, g), at(0, g + 1), at(1, g + 1), at(4, g), at(5, g), at(4, g + 1), at(5, g + 1), M, l, &v);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir]);
+        }
+        break;
+      }
+      case 4: {
+        bool cubic = bm.nj > 2;
+        int gbot = cubic ? -GW : -1;
+        for (int g = 0; g >= gbot; --g) {
+          at(2, g) = nv.at(Im - 1, Jm + g, Km - 1); at(3, g) = nv.at(Im - 1, Jm + g, Km);
+          at(6, g) = nv.at(Im, Jm + g, Km - 1); at(7, g) = nv.at(Im, Jm + g, Km);
+        }
+        for (int g = 1; g <= GW; ++g) {
+          const int sl[4] = {2, 3, 6, 7};
+          for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3)) : v3lin2(at(s, g - 1), at(s, g - 2));
+          ok &= metric_tensor(at(2, g - 1), at(3, g - 1), at(2, g), at(3, g), at(6, g - 1), at(7, g - 1), at(6, g), at(7, g), M, l, &v);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir]);
+        }
+        break;
+      }
+      case 5: {
+        bool cubic = (ndir == 3);
+        int gtop = cubic ? GW : 1;
+        for (int g = 0; g <= gtop; ++g) {
+          at(0, g) = nv.at(Im - 1, Jm - 1, Km + g - 1); at(2, g) = nv.at(Im - 1, Jm, Km + g - 1);
+          at(4, g) = nv.at(Im, Jm - 1, Km + g - 1); at(6, g) = nv.at(Im, Jm, Km + g - 1);
+        }
+        for (int g = -1; g >= -GW; --g) {
+          const int sl[4] = {0, 2, 4, 6};
+          for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3)) : v3lin2(at(s, g + 1), at(s, g + 2));
+          ok &= metric_tensor(at(0, g), at(0, g + 1), at(2, g), at(2, g + 1), at(4, g), at(4, g + 1), at(6, g), at(6, g + 1), M, l, &v);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir]);
+        }
+        break;
+      }
+      case 6: {
+        bool cubic = (ndir == 3);
+        int gbot = cubic ? -GW : -1;
+        for (int g = 0; g >= gbot; --g) {
+          at(1, g) = nv.at(Im - 1, Jm - 1, Km + g); at(3, g) = nv.at(Im - 1, Jm, Km + g);
+          at(5, g) = nv.at(Im, Jm - 1, Km + g); at(7, g) = nv.at(Im, Jm, Km + g);
+        }
+        for (int g = 1; g <= GW; ++g) {
+          const int sl[4] = {1, 3, 5, 7};
+          for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3)) : v3lin2(at(s, g - 1), at(s, g - 2));
+          ok &= metric_tensor(at(1, g - 1), at(1, g), at(3, g - 1), at(3, g), at(5, g - 1), at(5, g), at(7, g - 1), at(7, g), M, l, &v);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir]);
+        }
+        break;
+      }
+    }
+  }
+  if (!ok) report(err, 6, e.b, Im - 1, Jm - 1, Km - 1);
+}
+
+// Uniformity check: flags[b] bit p set when plane p differs from its first
+// valid value somewhere in its valid region.
+__global__ void k_uniform_check(const BlockDesc* blk, int b, MetricArgs m, int nd, int ndir, int* flags,
+                                double* firsts) {
+  const BlockDesc& d = blk[b];
+  const long long vs = d.vstride, mb = d.mbase;
+  // reference values: cell (0,0,0) metrics; faces of cell (0,0,0)
+  long long o0 = (nd == 3) ? cell_off3(d, 0, 0, 0) : cell_off2(d, 0, 0);
+  long long n = (long long)(d.ni + 4) * (d.nj + 4) * (nd == 3 ? d.nk + 4 : 1);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % (d.ni + 4)) - GW, j = (int)((q / (d.ni + 4)) % (d.nj + 4)) - GW;
+    int k = (nd == 3) ? (int)(q / ((long long)(d.ni + 4) * (d.nj + 4))) - GW : 0;
+    bool in_i = i >= 0 && i < d.ni, in_j = j >= 0 && j < d.nj, in_k = (nd == 2) || (k >= 0 && k < d.nk);
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    int f = 0;
+    // dl along each active direction on that direction's ghosted line
+    if (in_j && in_k && m.dl[3 * mb + 0 * vs + o] != m.dl[3 * mb + 0 * vs + o0]) f |= 1;
+    if (in_i && in_k && m.dl[3 * mb + 1 * vs + o] != m.dl[3 * mb + 1 * vs + o0]) f |= 2;
+    if (nd == 3 && in_i && in_j && m.dl[3 * mb + 2 * vs + o] != m.dl[3 * mb + 2 * vs + o0]) f |= 4;
+    if (in_i && in_j && in_k) {
+      if (m.vol[mb + o] != m.vol[mb + o0]) f |= 8;
+      for (int p = 0; p < 3 * ndir; ++p)
+        if (m.vers[9 * mb + p * vs + o] != m.vers[9 * mb + p * vs + o0]) f |= 16;
+    }
+    for (int dir = 0; dir < nd; ++dir) {
+      bool in = (dir == 0 ? (i >= 0 && i <= d.ni) : in_i) && (dir == 1 ? (j >= 0 && j <= d.nj) : in_j) &&
+                (nd == 2 || (dir == 2 ? (k >= 0 && k <= d.nk) : in_k));
+      if (!in) continue;
+      for (int p = 0; p < 4; ++p)
+        if (m.face[12 * mb + (4 * dir + p) * vs + o] != m.face[12 * mb + (4 * dir + p) * vs + o0]) f |= 32 << dir;
+    }
+    if (f) atomicOr(&flags[b], f);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    for (int h = 0; h < 3; ++h) firsts[h] = m.dl[3 * mb + h * vs + o0];
+    for (int dir = 0; dir < 3; ++dir)
+      for (int p = 0; p < 4; ++p) firsts[3 + 4 * dir + p] = (dir < nd) ? m.face[12 * mb + (4 * dir + p) * vs + o0] : 0.0;
+    firsts[15] = m.vol[mb + o0];
+    for (int p = 0; p < 9; ++p) firsts[16 + p] = (p < 3 * ndir) ? m.vers[9 * mb + p * vs + o0] : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Fill_Ghost_Cell (Lib_Ghost.f90:11-137), one thread per boundary record.
+// ---------------------------------------------------------------------------
+template <int NV>
+__global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nrec, double* P, MetricArgs m,
+                              int nd) {
+  int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nrec) return;
+  const GhostRec e = recs[q];
+  const BlockDesc& d = blk[e.b];
+  const int dir = (e.f - 1) / 2;
+  if (dir >= nd) return;
+  const int gi = (e.f == 1) ? 1 : (e.f == 2) ? -1 : 0;   // guide(Fm,:) inward step
+  const int gj = (e.f == 3) ? 1 : (e.f == 4) ? -1 : 0;
+  const int gk = (e.f == 5) ? 1 : (e.f == 6) ? -1 : 0;
+  double* Pb = P + d.sbase;
+  const long long vs = d.vstride;
+  auto off = [&](const BlockDesc& bb, int i, int j, int k) {
+    return (nd == 3) ? cell_off3(bb, i, j, k) : cell_off2(bb, i, j);
+  };
+  if (e.type == BC_CONN) {     // Ghost_Connection :140-160
+    const BlockDesc& s = blk[e.bs];
+    const int si = (e.fs == 1) ? 1 : (e.fs == 2) ? -1 : 0;
+    const int sj = (e.fs == 3) ? 1 : (e.fs == 4) ? -1 : 0;
+    const int sk = (e.fs == 5) ? 1 : (e.fs == 6) ? -1 : 0;
+    const double* Ps = P + s.sbase;
+    for (int g = 1; g <= GW; ++g) {
+      long long od = off(d, e.i - gi * g, e.j - gj * g, e.k - gk * g);
+      long long os = off(s, e.is + si * (g - 1), e.js + sj * (g - 1), e.ks + sk * (g - 1));
+      for (int v = 0; v < NV; ++v) Pb[v * vs + od] = Ps[v * s.vstride + os];
+    }
+  } else if (e.type == BC_SYM) {  // Ghost_Symmetry :193-225 (first ghost only)
+    long long ob = off(d, e.i, e.j, e.k);
+    long long og = off(d, e.i - gi, e.j - gj, e.k - gk);
+    // normal of the boundary face: low face of the boundary cell (odd faces)
+    // or of the next cell (even faces)
+    int fi = e.i + (e.f == 2), fj = e.j + (e.f == 4), fk = e.k + (e.f == 6);
+    long long of = off(d, fi, fj, fk);
+    const double* fp = m.face + 12 * d.mbase + (4 * dir) * vs + of;
+    double n[3] = {fp[0], fp[vs], fp[2 * vs]};
+    double q[NV];
+    for (int v = 0; v < NV; ++v) q[v] = Pb[v * vs + ob];
+    double udotn = ex::dot_vel<NV>(q, n);
+    for (int c = 0; c < NV - 2; ++c) q[1 + c] = q[1 + c] - 2.0 * udotn * n[c];
+    for (int v = 0; v < NV; ++v) Pb[v * vs + og] = q[v];
+  } else if (e.type == BC_EXTRAP) {   // Ghost_Extrapolate :363-402
+    for (int g = 1; g <= GW; ++g) {
+      long long od = off(d, e.i - gi * g, e.j - gj * g, e.k - gk * g);
+      long long oa = off(d, e.i - gi * (g - 1), e.j - gj * (g - 1), e.k - gk * (g - 1));
+      long long oc = off(d, e.i - gi * (g - 2), e.j - gj * (g - 2), e.k - gk * (g - 2));
+      long long oe = off(d, e.i - gi * (g - 3), e.j - gj * (g - 3), e.k - gk * (g - 3));
+      for (int v = 0; v < NV; ++v)
+        Pb[v * vs + od] = 3.0 * Pb[v * vs + oa] - 3.0 * Pb[v * vs + oc] + Pb[v * vs + oe];
+    }
+  } else {                        // Ghost_ZG_Extrapolate :279-304 (0, 401-407, 420)
+    long long ob = off(d, e.i, e.j, e.k);
+    for (int g = 1; g <= GW; ++g) {
+      long long od = off(d, e.i - gi * g, e.j - gj * g, e.k - gk * g);
+      for (int v = 0; v < NV; ++v) Pb[v * vs + od] = Pb[v * vs + ob];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Compute_dt (Mod_dt.f90:10-106): local dt and a global minimum.
+// dtmin_bits holds the running minimum as the bit pattern of a positive double.
+// ---------------------------------------------------------------------------
+template <int NV, bool UNI>
+__global__ void k_compute_dt(const BlockDesc* blk, int nblk, const double* P, MetricArgs m, double* dtl,
+                             unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
+                             int ramp_iter, int store_local) {
+  // one CTA-row per (block, row) pair: blockIdx.y = block, grid-stride over cells
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  const long long ncell = (long long)d.ni * d.nj * d.nk;
+  const long long vs = d.vstride, mb = d.mbase;
+  const double* Pb = P + d.sbase;
+  double local_min = __longlong_as_double(0x7ff0000000000000LL);
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    double Q[NV];
+    for (int v = 0; v < NV; ++v) Q[v] = Pb[v * vs + o];
+    double Sound = ex::sound(g, Q[0], Q[NV - 1]);
+    double dtmin = 1e8;
+    for (int dd = 0; dd < ndir; ++dd) {
+      double ver[3];
+      double dlv;
+      if constexpr (UNI) {
+        ver[0] = d.u_vers[dd][0]; ver[1] = d.u_vers[dd][1]; ver[2] = d.u_vers[dd][2];
+        dlv = d.u_dl[dd];
+      } else {
+        for (int c = 0; c < 3; ++c) ver[c] = m.vers[9 * mb + (3 * dd + c) * vs + o];
+        dlv = m.dl[3 * mb + dd * vs + o];
+      }
+      double vel_ = fabs(ex::dot_vel<NV>(Q, ver));
+      double lambda = vel_ + Sound;
+      double dt = dlv / lambda * cfl;
+      dtmin = fmin(dt, dtmin);
+    }
+    double dtcell = dtmin;
+    if (iter < ramp_iter) dtcell = dtcell * (double)iter / (double)ramp_iter;
+    if (store_local) dtl[mb + o] = dtcell;
+    local_min = fmin(local_min, dtcell);
+  }
+  // warp + CTA min, one atomic per CTA
+  for (int s = 16; s > 0; s >>= 1) local_min = fmin(local_min, __shfl_xor_sync(0xffffffffu, local_min, s));
+  __shared__ double wmin[32];
+  if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = local_min;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = (threadIdx.x < (blockDim.x >> 5)) ? wmin[threadIdx.x] : __longlong_as_double(0x7ff0000000000000LL);
+    for (int s = 16; s > 0; s >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, s));
+    if (threadIdx.x == 0) atomicMin(dtmin_bits, (unsigned long long)__double_as_longlong(v));
+  }
+}
+
+// Set_Global_dt: every interior dtlocal = dtglobal (device scalar).
+__global__ void k_set_global_dt(const BlockDesc* blk, double* dtl, const double* dtg, int nd) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  long long ncell = (long long)d.ni * d.nj * d.nk;
+  double v = *dtg;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    dtl[d.mbase + o] = v;
+  }
+}
+
+// Device-side step bookkeeping (no host round trip between steps).
+//   begin: dtmin = dt_start ; finish: dtglobal = dtmin, time += dtglobal
+__global__ void k_step_begin(unsigned long long* dtmin_bits, double dt_start, int* iter) {
+  *dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
+  if (iter) *iter = *iter + 1;
+}
+__global__ void k_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time) {
+  double v = __longlong_as_double((long long)*dtmin_bits);
+  *dtg = v;
+  if (advance_time) *time = *time + v;
+}
+
+// ---------------------------------------------------------------------------
+// RK_Newstate pointwise (phase path): P <- update(P, PO, R)
+// ---------------------------------------------------------------------------
+template <int NV, bool UNI>
+__global__ void k_rk_stage(const BlockDesc* blk, double* P, const double* PO, const double* R, MetricArgs m,
+                           const double* dtl, Gas g, double c, int nd, DevError* err) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  long long ncell = (long long)d.ni * d.nj * d.nk;
+  const long long vs = d.vstride, mb = d.mbase;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    double Q[NV], QO[NV], Rv[NV];
+    for (int v = 0; v < NV; ++v) {
+      Q[v] = P[d.sbase + v * vs + o];
+      QO[v] = PO[d.sbase + v * vs + o];
+      Rv[v] = R[d.sbase + v * vs + o];
+    }
+    double vol;
+    if constexpr (UNI) vol = d.u_vol; else vol = m.vol[mb + o];
+    double dt = dtl[mb + o];
+    bool ok = rk_update<NV>(g, Q, QO, Rv, vol, dt, c, false);
+    if (!ok) report(err, 5, b, i, j, k);
+    for (int v = 0; v < NV; ++v) P[d.sbase + v * vs + o] = Q[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Compute_Residual (Mod_Diagnostic.f90:13-50): per-CTA partial sums of
+// (|d rho|, |du|, |dv|, |dw|, |dp|)^2, reduced in a fixed order afterwards.
+// ---------------------------------------------------------------------------
+template <int NV>
+__global__ void k_residual_norms(const BlockDesc* blk, const double* P, const double* PO, int nd,
+                                 double* partial) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  long long ncell = (long long)d.ni * d.nj * d.nk;
+  const long long vs = d.vstride;
+  double acc[5] = {0, 0, 0, 0, 0};
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    for (int v = 0; v < NV; ++v) {
+      double r = fabs(P[d.sbase + v * vs + o] - PO[d.sbase + v * vs + o]);
+      int slot = (NV == 4 && v == 3) ? 4 : v;     // 2-D: (rho,u,v,p) -> slots 0,1,2,4
+      acc[slot] = acc[slot] + r * r;
+    }
+  }
+  __shared__ double red[5][256];
+  for (int s = 0; s < 5; ++s) red[s][threadIdx.x] = acc[s];
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int s = 0; s < 5; ++s) red[s][threadIdx.x] = red[s][threadIdx.x] + red[s][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    long long slot = (long long)blockIdx.y * gridDim.x + blockIdx.x;
+    for (int s = 0; s < 5; ++s) partial[5 * slot + s] = red[s][0];
+  }
+}
+
+__global__ void k_sum_partials(const double* partial, int n, double* out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double t[5] = {0, 0, 0, 0, 0};
+  for (int q = 0; q < n; ++q)
+    for (int s = 0; s < 5; ++s) t[s] = t[s] + partial[5 * q + s];
+  for (int s = 0; s < 5; ++s) out[s] = t[s];
+}
+
+// ---------------------------------------------------------------------------
+// Layout conversion between the reference's AoS P(5, 1-gc:ni+gc, ...) and the
+// device SoA planes.  host_ref: the reference-layout array of one block.
+// ---------------------------------------------------------------------------
+__global__ void k_ref_to_soa(const BlockDesc* blk, int b, const double* ref, double* dst, int nv, int nd) {
+  const BlockDesc& d = blk[b];
+  const int ex = d.ni + 4, ey = d.nj + 4, ez = (nd == 3) ? d.nk + 4 : 1;
+  const long long n = (long long)ex * ey * ez;
+  const long long vs = d.vstride;
+  const int refz = d.nk + 4;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(q % ex), y = (int)((q / ex) % ey), z = (int)(q / ((long long)ex * ey));
+    int rz = (nd == 3) ? z : GW;  // 2-D: the k = 1 plane of the reference array
+    (void)refz;
+    const double* src = ref + 5 * ((long long)x + (long long)ex * ((long long)y + (long long)ey * rz));
+    long long o = (nd == 3) ? cell_off3(d, x - GW, y - GW, z - GW) : cell_off2(d, x - GW, y - GW);
+    if (nv == 5) {
+      for (int v = 0; v < 5; ++v) dst[d.sbase + v * vs + o] = src[v];
+    } else {
+      dst[d.sbase + 0 * vs + o] = src[0];
+      dst[d.sbase + 1 * vs + o] = src[1];
+      dst[d.sbase + 2 * vs + o] = src[2];
+      dst[d.sbase + 3 * vs + o] = src[4];
+    }
+  }
+}
+
+// Writes the reference layout; in 2-D the w slot is 0 and the k-ghost planes
+// repeat the k = 1 plane (the zero-gradient fill of null k faces).
+__global__ void k_soa_to_ref(const BlockDesc* blk, int b, const double* src, double* ref, int nv, int nd) {
+  const BlockDesc& d = blk[b];
+  const int ex = d.ni + 4, ey = d.nj + 4, ez = d.nk + 4;
+  const long long n = (long long)ex * ey * ez;
+  const long long vs = d.vstride;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(q % ex), y = (int)((q / ex) % ey), z = (int)(q / ((long long)ex * ey));
+    double* out = ref + 5 * q;
+    if (nd == 3) {
+      long long o = cell_off3(d, x - GW, y - GW, z - GW);
+      for (int v = 0; v < 5; ++v) out[v] = src[d.sbase + v * vs + o];
+    } else {
+      long long o = cell_off2(d, x - GW, y - GW);
+      out[0] = src[d.sbase + 0 * vs + o];
+      out[1] = src[d.sbase + 1 * vs + o];
+      out[2] = src[d.sbase + 2 * vs + o];
+      out[3] = 0.0;
+      out[4] = src[d.sbase + 3 * vs + o];
+    }
+  }
+}
+
+// one-plane quantity (dtlocal, interior only) <-> reference (1:ni,1:nj,1:nk)
+__global__ void k_plane_io(const BlockDesc* blk, int b, double* plane_arena, double* ref, int nd, int to_ref) {
+  const BlockDesc& d = blk[b];
+  long long n = (long long)d.ni * d.nj * d.nk;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    if (to_ref) ref[q] = plane_arena[d.mbase + o];
+    else plane_arena[d.mbase + o] = ref[q];
+  }
+}
+
+// metrics of one block -> reference-shaped vol(ghosted) and dl(3, ghosted)
+__global__ void k_metrics_to_ref(const BlockDesc* blk, int b, MetricArgs m, double* vol, double* dl, int nd) {
+  const BlockDesc& d = blk[b];
+  const int ex = d.ni + 4, ey = d.nj + 4, ez = d.nk + 4;
+  long long n = (long long)ex * ey * ez;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int x = (int)(q % ex), y = (int)((q / ex) % ey), z = (int)(q / ((long long)ex * ey));
+    if (nd == 2 && z != GW) continue;
+    long long o = (nd == 3) ? cell_off3(d, x - GW, y - GW, z - GW) : cell_off2(d, x - GW, y - GW);
+    if (vol) vol[q] = m.vol[d.mbase + o];
+    if (dl)
+      for (int h = 0; h < 3; ++h) dl[3 * q + h] = m.dl[3 * d.mbase + h * d.vstride + o];
+  }
+}
+
+__global__ void k_faces_to_ref(const BlockDesc* blk, int b, MetricArgs m, int dir, double* N, double* A, int nd) {
+  const BlockDesc& d = blk[b];
+  int ei = d.ni + (dir == 0), ej = d.nj + (dir == 1), ek = d.nk + (dir == 2);
+  long long n = (long long)ei * ej * ek;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(q % ei), j = (int)((q / ei) % ej), k = (int)(q / ((long long)ei * ej));
+    int ci = (dir == 0) ? i : i, cj = (dir == 1) ? j : j, ck = (dir == 2) ? k : k;
+    if (nd == 2 && dir == 2) continue;
+    long long o = (nd == 3) ? cell_off3(d, ci, cj, ck) : cell_off2(d, ci, cj);
+    const double* f = m.face + 12 * d.mbase + (4 * dir) * d.vstride + o;
+    if (N) { N[3 * q] = f[0]; N[3 * q + 1] = f[d.vstride]; N[3 * q + 2] = f[2 * d.vstride]; }
+    if (A) A[q] = f[3 * d.vstride];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+static inline int grid_for(long long n, int threads, int cap = 148 * 16) {
+  long long g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+void launch_cell_metrics(const BlockDesc* dblk, int b, long long ncell, NodeView nv, MetricArgs m, int nd,
+                         int ndir, DevError* err, cudaStream_t s) {
+  k_cell_metrics<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, nv, const_cast<double*>(m.dl),
+                                                       const_cast<double*>(m.vol), const_cast<double*>(m.vers),
+                                                       nd, ndir, err);
+}
+void launch_face_metrics(const BlockDesc* dblk, int b, long long nface, NodeView nv, MetricArgs m, int nd,
+                         int dir, cudaStream_t s) {
+  k_face_metrics<<<grid_for(nface, 256), 256, 0, s>>>(dblk, b, nv, const_cast<double*>(m.face), nd, dir);
+}
+void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, const NodeView* nodes, MetricArgs m,
+                          int nd, int ndir, DevError* err, cudaStream_t s) {
+  if (nrec == 0) return;
+  k_ghost_metrics<<<(nrec + 127) / 128, 128, 0, s>>>(dblk, (const GhostMetricRec*)recs, nrec, nodes,
+                                                     const_cast<double*>(m.dl), nd, ndir, err);
+}
+void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir,
+                          int* flags, double* firsts, cudaStream_t s) {
+  k_uniform_check<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, m, nd, ndir, flags, firsts);
+}
+void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, double* P, MetricArgs m, int nd,
+                        cudaStream_t s) {
+  if (nrec == 0) return;
+  if (nd == 3) k_fill_ghosts<5><<<(nrec + 127) / 128, 128, 0, s>>>(dblk, recs, nrec, P, m, nd);
+  else k_fill_ghosts<4><<<(nrec + 127) / 128, 128, 0, s>>>(dblk, recs, nrec, P, m, nd);
+}
+void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,
+                       double* dtl, unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
+                       int ramp_iter, int store_local, bool uniform, cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 8), nblk);
+  if (nd == 3) {
+    if (uniform) k_compute_dt<5, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
+    else k_compute_dt<5, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
+  } else {
+    if (uniform) k_compute_dt<4, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
+    else k_compute_dt<4, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
+  }
+}
+void launch_set_global_dt(const BlockDesc* dblk, int nblk, long long maxcell, double* dtl, const double* dtg, int nd,
+                          cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 8), nblk);
+  k_set_global_dt<<<grid, 256, 0, s>>>(dblk, dtl, dtg, nd);
+}
+void launch_step_begin(unsigned long long* dtmin_bits, double dt_start, int* iter, cudaStream_t s) {
+  k_step_begin<<<1, 1, 0, s>>>(dtmin_bits, dt_start, iter);
+}
+void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time,
+                          cudaStream_t s) {
+  k_step_dt_final<<<1, 1, 0, s>>>(dtmin_bits, dtg, time, advance_time);
+}
+void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
+                     MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
+                     cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 8), nblk);
+  if (nd == 3) {
+    if (uniform) k_rk_stage<5, true><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
+    else k_rk_stage<5, false><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
+  } else {
+    if (uniform) k_rk_stage<4, true><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
+    else k_rk_stage<4, false><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
+  }
+}
+int norms_partial_count(int nblk, long long maxcell) { return grid_for(maxcell, 256, 148 * 4) * nblk; }
+void launch_residual_norms(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, const double* PO,
+                           int nd, double* partial, double* out, cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
+  if (nd == 3) k_residual_norms<5><<<grid, 256, 0, s>>>(dblk, P, PO, nd, partial);
+  else k_residual_norms<4><<<grid, 256, 0, s>>>(dblk, P, PO, nd, partial);
+  k_sum_partials<<<1, 1, 0, s>>>(partial, grid.x * grid.y, out);
+}
+void launch_ref_to_soa(const BlockDesc* dblk, int b, long long n, const double* ref, double* dst, int nv, int nd,
+                       cudaStream_t s) {
+  k_ref_to_soa<<<grid_for(n, 256), 256, 0, s>>>(dblk, b, ref, dst, nv, nd);
+}
+void launch_soa_to_ref(const BlockDesc* dblk, int b, long long n, const double* src, double* ref, int nv, int nd,
+                       cudaStream_t s) {
+  k_soa_to_ref<<<grid_for(n, 256), 256, 0, s>>>(dblk, b, src, ref, nv, nd);
+}
+void launch_plane_io(const BlockDesc* dblk, int b, long long n, double* arena, double* ref, int nd, int to_ref,
+                     cudaStream_t s) {
+  k_plane_io<<<grid_for(n, 256), 256, 0, s>>>(dblk, b, arena, ref, nd, to_ref);
+}
+void launch_metrics_to_ref(const BlockDesc* dblk, int b, long long n, MetricArgs m, double* vol, double* dl, int nd,
+                           cudaStream_t s) {
+  k_metrics_to_ref<<<grid_for(n, 256), 256, 0, s>>>(dblk, b, m, vol, dl, nd);
+}
+void launch_faces_to_ref(const BlockDesc* dblk, int b, long long n, MetricArgs m, int dir, double* N, double* A,
+                         int nd, cudaStream_t s) {
+  k_faces_to_ref<<<grid_for(n, 256), 256, 0, s>>>(dblk, b, m, dir, N, A, nd);
+}
+
+}  // namespace mose

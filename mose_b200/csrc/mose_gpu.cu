@@ -1,0 +1,916 @@
+// mose_gpu.cu -- host side of the C ABI declared in include/mose_gpu.h.
+//
+// One context = one CUDA stream, the device arenas of all blocks, the
+// boundary tables and the step graphs.  Setup (metrics, tables) runs on the
+// device; after it every entry point only enqueues kernels, except those that
+// return values to the host.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mose_gpu.h"
+#include "kernels.h"
+
+using namespace mose;
+
+namespace {
+
+struct HostBlock {
+  int ni, nj, nk;
+  std::vector<double> node;
+};
+
+struct BcRecord {
+  int b, i, j, k, f, type, bs, is, js, ks, fs, d11, d12, d21, d22;
+  double data[6];
+};
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  ~DevBuf() { release(); }
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+    if (e == cudaSuccess) e = cudaMemset(p, 0, count * sizeof(T));
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+}  // namespace
+
+struct mose_gpu_ctx {
+  mose_gpu_config cfg;
+  Gas gas;
+  std::string err;
+  int devcode = 0, eb = 0, ei = 0, ej = 0, ek = 0;
+  cudaStream_t stream = nullptr;
+  int nsm = 148;
+  bool ready = false;
+  int ndir = 0, nd = 2, nv = 4;
+  bool uniform = false;
+  long long launches = 0;
+
+  std::vector<HostBlock> hblk;
+  std::vector<BcRecord> bc;
+  std::vector<BlockDesc> desc;
+  long long marena = 0;      // doubles per one-plane arena
+  long long maxcell = 0;
+
+  DevBuf<BlockDesc> d_desc;
+  DevBuf<double> state[3];
+  DevBuf<double> resid;
+  DevBuf<double> dl, face, vol, vers, dtl;
+  DevBuf<int> bcw;
+  DevBuf<BcParam> bcp;
+  DevBuf<GhostRec> ghosts;
+  DevBuf<int4> items;
+  DevBuf<double> scal;        // [0] dtglobal, [1] time
+  DevBuf<unsigned long long> dtmin;
+  DevBuf<int> iterdev;
+  DevBuf<DevError> derr;
+  DevBuf<double> partial, norms;
+  DevBuf<double> staging;     // reference-layout transfers
+  int nghost = 0, nitems = 0;
+  int cur = 0, po = 0;        // state arena holding P, and PO
+  int stage_grid = 0;
+
+  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
+  int graph_kernels = 0;
+
+  double h_time = 0.0;
+  int h_iter = 0;
+
+  MetricArgs margs() const { return MetricArgs{dl.p, face.p, vol.p, vers.p}; }
+};
+
+namespace {
+
+int fail(mose_gpu_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CU(call)                                                                       \
+  do {                                                                                 \
+    cudaError_t e_ = (call);                                                           \
+    if (e_ != cudaSuccess)                                                             \
+      return fail(ctx, MOSE_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                 \
+  } while (0)
+
+int check_launch(mose_gpu_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
+  return MOSE_OK;
+}
+
+// Reads the device error word; returns a status.
+int poll_device_error(mose_gpu_ctx* ctx) {
+  DevError h;
+  CU(cudaMemcpyAsync(&h, ctx->derr.p, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (h.code != 0) {
+    ctx->devcode = h.code; ctx->eb = h.b; ctx->ei = h.i; ctx->ej = h.j; ctx->ek = h.k;
+    const char* what = h.code == MOSE_ERR_INTERFACE_STATE ? "non-physical interface state"
+                       : h.code == MOSE_ERR_NAN_OR_NEG_P   ? "NaN or p<0 after the state update"
+                       : h.code == MOSE_ERR_METRICS        ? "metric tensor det=0 or non-positive volume"
+                                                           : "device failure";
+    return fail(ctx, h.code, "%s at b,i,j,k = %d %d %d %d", what, h.b, h.i, h.j, h.k);
+  }
+  return MOSE_OK;
+}
+
+int bc_code_of(int type) {
+  switch (type) {
+    case 0: return BC_NONE;
+    case 101: case 201: return BC_CONN;
+    case 300: return BC_SYM;
+    case 400: return BC_EXTRAP;
+    case 405: return BC_SUPIN;
+    case 406: return BC_OUTFLOW;
+  }
+  return -1;
+}
+
+// index of a boundary cell along its face (0-based), 2-D and 3-D
+int face_index(const HostBlock& h, int f, int i, int j, int k) {
+  if (f <= 2) return j + h.nj * k;
+  if (f <= 4) return i + h.ni * k;
+  return i + h.ni * j;
+}
+
+void destroy_graphs(mose_gpu_ctx* ctx) {
+  for (auto& g : ctx->graph)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
+}  // namespace
+
+extern "C" {
+
+void mose_gpu_default_config(mose_gpu_config* cfg) {
+  std::memset(cfg, 0, sizeof(*cfg));
+  cfg->abi_version = MOSE_GPU_ABI_VERSION;
+  cfg->n_rk = 1;            // time-scheme = euler
+  cfg->cfl = 0.5;
+  cfg->time_accurate = 0;
+  cfg->ramp_iter = 0;
+  cfg->limiter = MOSE_LIMITER_FIRST_ORDER;
+  cfg->riemann = MOSE_RIEMANN_HLLC;
+  cfg->integration = MOSE_INTEGRATION_CONS;
+  cfg->precision = MOSE_PRECISION_FP64_EXACT;
+  cfg->ndir = 0;
+  cfg->nsc = 1;
+  cfg->gamma = 1.4;
+  cfg->rgas = 1.0;
+  cfg->device = 0;
+  cfg->res_diter = 1;
+}
+
+int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
+  mose_gpu_ctx* ctx = nullptr;
+  if (!cfg || !out) return MOSE_ERR_INVALID;
+  *out = nullptr;
+  if (cfg->abi_version != MOSE_GPU_ABI_VERSION) return MOSE_ERR_INVALID;
+  if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 || cfg->integration != MOSE_INTEGRATION_CONS ||
+      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > 3 ||
+      cfg->precision < 0 || cfg->precision > 2 || !(cfg->gamma > 1.0) || !(cfg->rgas > 0.0))
+    return MOSE_ERR_UNSUPPORTED;
+  ctx = new mose_gpu_ctx();
+  ctx->cfg = *cfg;
+  if (ctx->cfg.res_diter <= 0) ctx->cfg.res_diter = 1;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device) {
+    delete ctx;
+    return MOSE_ERR_CUDA;
+  }
+  cudaDeviceProp prop;
+  if (cudaSetDevice(cfg->device) != cudaSuccess || cudaGetDeviceProperties(&prop, cfg->device) != cudaSuccess ||
+      prop.major != 10) {
+    delete ctx;
+    return MOSE_ERR_CUDA;   // built for sm_100a only
+  }
+  ctx->nsm = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete ctx;
+    return MOSE_ERR_CUDA;
+  }
+  // thermodynamic constants of the restated FLINT closure
+  ctx->gas.gamma = cfg->gamma;
+  ctx->gas.R = cfg->rgas;
+  ctx->gas.cp = cfg->gamma * cfg->rgas / (cfg->gamma - 1.0);
+  ctx->gas.cv = cfg->rgas / (cfg->gamma - 1.0);
+  ctx->gas.cpmR = 0.5 * (ctx->gas.cp + ctx->gas.cp) - ctx->gas.R;
+  *out = ctx;
+  return MOSE_OK;
+}
+
+void mose_gpu_destroy(mose_gpu_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->cfg.device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  destroy_graphs(ctx);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* mose_gpu_last_error(const mose_gpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+int mose_gpu_error_location(const mose_gpu_ctx* ctx, int32_t* b, int32_t* i, int32_t* j, int32_t* k) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (b) *b = ctx->eb;
+  if (i) *i = ctx->ei;
+  if (j) *j = ctx->ej;
+  if (k) *k = ctx->ek;
+  return ctx->devcode;
+}
+
+int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int32_t nk, const double* node) {
+  if (!ctx || !node) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "add_block after setup");
+  if (b != (int)ctx->hblk.size() + 1) return fail(ctx, MOSE_ERR_INVALID, "blocks must be added in order 1..nb");
+  if (ni < 1 || nj < 1 || nk < 1) return fail(ctx, MOSE_ERR_INVALID, "bad block dimensions");
+  HostBlock h;
+  h.ni = ni; h.nj = nj; h.nk = nk;
+  size_t n = 3 * (size_t)(ni + 1) * (nj + 1) * (nk + 1);
+  h.node.assign(node, node + n);
+  ctx->hblk.push_back(std::move(h));
+  return MOSE_OK;
+}
+
+int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, int32_t nbound) {
+  if (!ctx || !rec) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_bcs after setup");
+  int nb = (int)ctx->hblk.size();
+  long long expect = 0;
+  for (auto& h : ctx->hblk) expect += 2LL * ((long long)h.nj * h.nk + (long long)h.ni * h.nk + (long long)h.ni * h.nj);
+  if (nbound != expect)
+    return fail(ctx, MOSE_ERR_INVALID, "boundary records (%d) differ from the block faces (%lld)", nbound, expect);
+  ctx->bc.resize(nbound);
+  int lastkey = -1;
+  for (int q = 0; q < nbound; ++q) {
+    const int32_t* r = rec + 15 * (size_t)q;
+    BcRecord& e = ctx->bc[q];
+    e.b = r[0]; e.i = r[1]; e.j = r[2]; e.k = r[3]; e.f = r[4]; e.type = r[5];
+    e.bs = r[6]; e.is = r[7]; e.js = r[8]; e.ks = r[9]; e.fs = r[10];
+    e.d11 = r[11]; e.d12 = r[12]; e.d21 = r[13]; e.d22 = r[14];
+    for (int c = 0; c < 6; ++c) e.data[c] = data ? data[6 * (size_t)q + c] : 0.0;
+    if (e.b < 1 || e.b > nb || e.f < 1 || e.f > 6) return fail(ctx, MOSE_ERR_INVALID, "bad record %d", q + 1);
+    const HostBlock& h = ctx->hblk[e.b - 1];
+    if (e.i < 1 || e.i > h.ni || e.j < 1 || e.j > h.nj || e.k < 1 || e.k > h.nk)
+      return fail(ctx, MOSE_ERR_INVALID, "record %d: cell out of range", q + 1);
+    int key = (e.b - 1) * 6 + (e.f - 1);
+    if (key < lastkey) return fail(ctx, MOSE_ERR_INVALID, "records must be ordered by block and face");
+    lastkey = key;
+    if (bc_code_of(e.type) < 0)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "record %d: bc type %d is not on this path", q + 1, e.type);
+    if (e.type == 101 || e.type == 201) {
+      if (e.bs < 1 || e.bs > nb || e.fs < 1 || e.fs > 6)
+        return fail(ctx, MOSE_ERR_INVALID, "record %d: bad connection", q + 1);
+      const HostBlock& s = ctx->hblk[e.bs - 1];
+      if (e.is < 1 || e.is > s.ni || e.js < 1 || e.js > s.nj || e.ks < 1 || e.ks > s.nk)
+        return fail(ctx, MOSE_ERR_INVALID, "record %d: connection source out of range", q + 1);
+    }
+  }
+  return MOSE_OK;
+}
+
+int mose_gpu_setup(mose_gpu_ctx* ctx) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (ctx->hblk.empty() || ctx->bc.empty()) return fail(ctx, MOSE_ERR_NOT_READY, "no blocks or no boundary records");
+  CU(cudaSetDevice(ctx->cfg.device));
+  const int nb = (int)ctx->hblk.size();
+  // Check_Mesh_Type (Lib_Metrics.f90:13-66)
+  const HostBlock& b1 = ctx->hblk[0];
+  if (ctx->cfg.ndir > 0) ctx->ndir = ctx->cfg.ndir;
+  else if (b1.nk > 1) ctx->ndir = 3;
+  else if (b1.nj == 1) ctx->ndir = 1;
+  else ctx->ndir = 2;
+  ctx->nd = (ctx->ndir == 3) ? 3 : 2;
+  ctx->nv = (ctx->nd == 3) ? 5 : 4;
+  if (ctx->nd == 3) return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: not yet on this path");
+  auto nodeh = [&](const HostBlock& h, int i, int j, int k, int c) {
+    return h.node[3 * ((size_t)i + (size_t)(h.ni + 1) * ((size_t)j + (size_t)(h.nj + 1) * k)) + c];
+  };
+  if (ctx->ndir == 2) {
+    double y0 = nodeh(b1, 0, 1, 0, 1), z0 = nodeh(b1, 0, 1, 0, 2), y1 = nodeh(b1, 0, 1, 1, 1), z1 = nodeh(b1, 0, 1, 1, 2);
+    double y2 = nodeh(b1, 0, b1.nj, 0, 1), z2 = nodeh(b1, 0, b1.nj, 0, 2), y3 = nodeh(b1, 0, b1.nj, 1, 1),
+           z3 = nodeh(b1, 0, b1.nj, 1, 2);
+    double t1 = std::atan2(z1, y1) - std::atan2(z0, y0), t2 = std::atan2(z3, y3) - std::atan2(z2, y2);
+    double r0 = std::sqrt(y0 * y0 + z0 * z0), r1 = std::sqrt(y1 * y1 + z1 * z1);
+    if ((t1 - t2) < 1e-5 && r0 > 1e-10 && std::fabs(r0 - r1) < 1e-5 * r0)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "axisymmetric 2-D meshes are not on this path");
+  }
+  // 2-D: planar blocks so that n_z == 0 on i and j faces and w stays 0
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    if (h.nk != 1) return fail(ctx, MOSE_ERR_UNSUPPORTED, "mixed 2-D / 3-D blocks");
+    for (int j = 0; j <= h.nj; ++j)
+      for (int i = 0; i <= h.ni; ++i)
+        if (nodeh(h, i, j, 0, 0) != nodeh(h, i, j, 1, 0) || nodeh(h, i, j, 0, 1) != nodeh(h, i, j, 1, 1))
+          return fail(ctx, MOSE_ERR_UNSUPPORTED, "block %d is not planar in k", b + 1);
+    if (h.ni < 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "block %d: need ni >= 2", b + 1);
+  }
+  for (auto& e : ctx->bc) {
+    const HostBlock& h = ctx->hblk[e.b - 1];
+    if (e.f >= 5 && e.type != 0)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D k faces must be null (type 0), found %d", e.type);
+    bool degenerate = (e.f >= 3 && e.f <= 4 && h.nj < 3) || (e.f <= 2 && h.ni < 3);
+    if (degenerate && !(e.type == 0 || e.type == 400 || e.type == 406))
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "bc type %d on a face of a block thinner than 3 cells", e.type);
+    if (e.type == 405 && e.data[4] != 0.0)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
+  }
+
+  // ---- layout ----------------------------------------------------------------
+  ctx->desc.assign(nb, BlockDesc{});
+  long long mcur = 0;
+  ctx->maxcell = 0;
+  std::vector<int> bcwords;
+  std::vector<BcParam> params;
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    BlockDesc& d = ctx->desc[b];
+    d.ni = h.ni; d.nj = h.nj; d.nk = h.nk;
+    d.px = ((h.ni + 2 * GW) + 15) / 16 * 16;
+    d.py = h.nj + 2 * GW;
+    d.pz = (ctx->nd == 3) ? h.nk + 2 * GW : 1;
+    d.plane = (long long)d.px * d.py;
+    d.vstride = d.plane * d.pz;
+    d.vstride = (d.vstride + 31) / 32 * 32;
+    d.mbase = mcur;
+    d.sbase = (long long)ctx->nv * mcur;
+    mcur += d.vstride;
+    ctx->maxcell = std::max(ctx->maxcell, (long long)h.ni * h.nj * h.nk);
+    for (int f = 0; f < 6; ++f) {
+      d.bcn[f] = (f < 2) ? h.nj * h.nk : (f < 4) ? h.ni * h.nk : h.ni * h.nj;
+      d.bcoff[f] = (int)bcwords.size();
+      bcwords.resize(bcwords.size() + d.bcn[f], BC_NONE);
+    }
+  }
+  ctx->marena = mcur;
+  for (auto& e : ctx->bc) {
+    const BlockDesc& d = ctx->desc[e.b - 1];
+    const HostBlock& h = ctx->hblk[e.b - 1];
+    int code = bc_code_of(e.type);
+    int pidx = -1;
+    if (e.type == 405 || e.type == 406) {
+      BcParam p{};
+      if (e.type == 405) {
+        p.mach = e.data[0]; p.T = e.data[1]; p.p = e.data[2]; p.rel_fac = e.data[5];
+        double alpha = e.data[3], beta = e.data[4];
+        if (alpha >= 0.5 * 1.7976931348623157e308 || beta >= 0.5 * 1.7976931348623157e308)
+          return fail(ctx, MOSE_ERR_UNSUPPORTED, "inflow angle 'normal' is not on this path");
+        p.ca = std::cos(alpha); p.sa = std::sin(alpha); p.cb = std::cos(beta); p.sb = std::sin(beta);
+      } else {
+        p.pback = e.data[0]; p.rel_fac = e.data[1];
+      }
+      pidx = (int)params.size();
+      params.push_back(p);
+    }
+    bcwords[d.bcoff[e.f - 1] + face_index(h, e.f, e.i - 1, e.j - 1, e.k - 1)] = code | ((pidx + 1) << 8);
+  }
+
+  // ---- allocation --------------------------------------------------------------
+  for (int s = 0; s < 3; ++s)
+    if (ctx->state[s].alloc((size_t)ctx->nv * mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (state)");
+  if (ctx->resid.alloc((size_t)ctx->nv * mcur) != cudaSuccess || ctx->dl.alloc(3 * (size_t)mcur) != cudaSuccess ||
+      ctx->face.alloc(12 * (size_t)mcur) != cudaSuccess || ctx->vol.alloc((size_t)mcur) != cudaSuccess ||
+      ctx->vers.alloc(9 * (size_t)mcur) != cudaSuccess || ctx->dtl.alloc((size_t)mcur) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
+  CU(ctx->d_desc.alloc(nb));
+  CU(ctx->bcw.alloc(bcwords.size()));
+  CU(ctx->bcp.alloc(std::max<size_t>(params.size(), 1)));
+  CU(ctx->scal.alloc(4));
+  CU(ctx->dtmin.alloc(1));
+  CU(ctx->iterdev.alloc(1));
+  CU(ctx->derr.alloc(1));
+  CU(ctx->norms.alloc(5));
+  CU(ctx->partial.alloc(5 * (size_t)norms_partial_count(nb, ctx->maxcell)));
+  CU(cudaMemcpy(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ctx->bcw.p, bcwords.data(), bcwords.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!params.empty()) CU(cudaMemcpy(ctx->bcp.p, params.data(), params.size() * sizeof(BcParam), cudaMemcpyHostToDevice));
+
+  // ---- metrics on the device -------------------------------------------------
+  std::vector<DevBuf<double>> dnodes(nb);
+  std::vector<NodeView> views(nb);
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    CU(dnodes[b].alloc(h.node.size()));
+    CU(cudaMemcpy(dnodes[b].p, h.node.data(), h.node.size() * sizeof(double), cudaMemcpyHostToDevice));
+    views[b] = NodeView{dnodes[b].p, h.ni, h.nj, h.nk};
+  }
+  DevBuf<NodeView> dviews;
+  CU(dviews.alloc(nb));
+  CU(cudaMemcpy(dviews.p, views.data(), nb * sizeof(NodeView), cudaMemcpyHostToDevice));
+  MetricArgs m = ctx->margs();
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    long long ncell = (long long)h.ni * h.nj * h.nk;
+    launch_cell_metrics(ctx->d_desc.p, b, ncell, views[b], m, ctx->nd, ctx->ndir, ctx->derr.p, ctx->stream);
+    for (int dir = 0; dir < ctx->nd; ++dir) {
+      long long nf = (long long)(h.ni + (dir == 0)) * (h.nj + (dir == 1)) * (h.nk + (dir == 2));
+      launch_face_metrics(ctx->d_desc.p, b, nf, views[b], m, ctx->nd, dir, ctx->stream);
+    }
+  }
+  // ghost metrics per record, in bc order
+  std::vector<GhostMetricRec> gm;
+  for (auto& e : ctx->bc)
+    gm.push_back(GhostMetricRec{e.type, e.b - 1, e.i, e.j, e.k, e.f, e.bs - 1, e.is, e.js, e.ks, e.fs,
+                                e.d11, e.d12, e.d21, e.d22});
+  // BC_Symmetry_Metrics copies interior metrics: run the other records first
+  // is unnecessary (ghosts are never sources), but symmetric records read
+  // interior dl which is final after the cell kernel.
+  DevBuf<GhostMetricRec> dgm;
+  CU(dgm.alloc(gm.size()));
+  CU(cudaMemcpy(dgm.p, gm.data(), gm.size() * sizeof(GhostMetricRec), cudaMemcpyHostToDevice));
+  launch_ghost_metrics(ctx->d_desc.p, dgm.p, (int)gm.size(), dviews.p, m, ctx->nd, ctx->ndir, ctx->derr.p, ctx->stream);
+  {
+    int rc = check_launch(ctx, "metrics");
+    if (rc) return rc;
+  }
+  // uniformity
+  DevBuf<int> flags;
+  DevBuf<double> firsts;
+  CU(flags.alloc(nb));
+  CU(firsts.alloc(25 * (size_t)nb));
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    long long n = (long long)(h.ni + 4) * (h.nj + 4) * (ctx->nd == 3 ? h.nk + 4 : 1);
+    launch_uniform_check(ctx->d_desc.p, b, n, m, ctx->nd, ctx->ndir, flags.p, firsts.p + 25 * b, ctx->stream);
+  }
+  std::vector<int> hflags(nb);
+  std::vector<double> hfirst(25 * (size_t)nb);
+  CU(cudaMemcpyAsync(hflags.data(), flags.p, nb * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaMemcpyAsync(hfirst.data(), firsts.p, hfirst.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  {
+    int rc = poll_device_error(ctx);
+    if (rc) return rc;
+  }
+  bool uni = true;
+  for (int b = 0; b < nb; ++b) uni &= (hflags[b] == 0);
+  ctx->uniform = uni;
+  for (int b = 0; b < nb; ++b) {
+    BlockDesc& d = ctx->desc[b];
+    const double* f = &hfirst[25 * (size_t)b];
+    for (int h = 0; h < 3; ++h) d.u_dl[h] = f[h];
+    for (int dir = 0; dir < 3; ++dir) {
+      for (int q = 0; q < 3; ++q) d.u_n[dir][q] = f[3 + 4 * dir + q];
+      d.u_A[dir] = f[3 + 4 * dir + 3];
+    }
+    d.u_vol = f[15];
+    for (int dd = 0; dd < 3; ++dd)
+      for (int q = 0; q < 3; ++q) d.u_vers[dd][q] = f[16 + 3 * dd + q];
+  }
+  CU(cudaMemcpy(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice));
+
+  // ---- ghost-fill records (Fill_Ghost_Cell dispatch, Lib_Ghost.f90:50-73) ------
+  std::vector<GhostRec> gr;
+  for (auto& e : ctx->bc) {
+    if ((e.f - 1) / 2 >= ctx->nd) continue;
+    const HostBlock& h = ctx->hblk[e.b - 1];
+    // faces of degenerate directions have no ghost layer on the device
+    if ((e.f == 3 || e.f == 4) && h.nj < 3) continue;
+    int t = bc_code_of(e.type);
+    GhostRec g{t, e.b - 1, e.i - 1, e.j - 1, e.k - 1, e.f, e.bs - 1, e.is - 1, e.js - 1, e.ks - 1, e.fs};
+    gr.push_back(g);
+  }
+  ctx->nghost = (int)gr.size();
+  CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
+  if (!gr.empty()) CU(cudaMemcpy(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice));
+
+  // ---- work items for the stage kernel -----------------------------------------
+  long long strip_rows = 0;
+  for (auto& h : ctx->hblk) strip_rows += (long long)((h.ni + STRIP_W - 1) / STRIP_W) * h.nj;
+  long long target = (long long)ctx->nsm * 8;
+  int H = (int)std::max<long long>(4, std::min<long long>(256, strip_rows / std::max<long long>(1, target)));
+  std::vector<int4> items;
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    for (int j0 = 0; j0 < h.nj; j0 += H)
+      for (int c0 = 0; c0 < h.ni; c0 += STRIP_W) items.push_back(make_int4(b, c0, j0, std::min(j0 + H, h.nj)));
+  }
+  ctx->nitems = (int)items.size();
+  CU(ctx->items.alloc(items.size()));
+  CU(cudaMemcpy(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  ctx->stage_grid = std::min(ctx->nitems, ctx->nsm * 2);
+  ctx->cur = 0;
+  ctx->po = 1;
+  CU(cudaDeviceSynchronize());
+  ctx->ready = true;
+  return MOSE_OK;
+}
+
+// ---- transfers -----------------------------------------------------------------
+static int ensure_staging(mose_gpu_ctx* ctx, size_t n) {
+  if (ctx->staging.n < n)
+    if (ctx->staging.alloc(n) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (staging)");
+  return MOSE_OK;
+}
+
+static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool upload) {
+  if (!ctx || !P) return MOSE_ERR_INVALID;
+  if (!ctx->ready) return fail(ctx, MOSE_ERR_NOT_READY, "setup not done");
+  if (b < 1 || b > (int)ctx->hblk.size()) return fail(ctx, MOSE_ERR_INVALID, "bad block %d", b);
+  CU(cudaSetDevice(ctx->cfg.device));
+  const HostBlock& h = ctx->hblk[b - 1];
+  long long n = (long long)(h.ni + 4) * (h.nj + 4) * (h.nk + 4);
+  int rc = ensure_staging(ctx, 5 * (size_t)n);
+  if (rc) return rc;
+  double* dst = (arena < 0) ? ctx->resid.p : ctx->state[arena].p;
+  if (upload) {
+    CU(cudaMemcpyAsync(ctx->staging.p, P, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    launch_ref_to_soa(ctx->d_desc.p, b - 1, n, ctx->staging.p, dst, ctx->nv, ctx->nd, ctx->stream);
+    ctx->launches++;
+  } else {
+    launch_soa_to_ref(ctx->d_desc.p, b - 1, n, dst, ctx->staging.p, ctx->nv, ctx->nd, ctx->stream);
+    ctx->launches++;
+    CU(cudaMemcpyAsync(P, ctx->staging.p, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_launch(ctx, "layout conversion");
+}
+
+int mose_gpu_upload_prim(mose_gpu_ctx* ctx, int32_t b, const double* P) {
+  return prim_io(ctx, b, const_cast<double*>(P), ctx ? ctx->cur : 0, true);
+}
+int mose_gpu_download_prim(mose_gpu_ctx* ctx, int32_t b, double* P) {
+  return prim_io(ctx, b, P, ctx ? ctx->cur : 0, false);
+}
+int mose_gpu_upload_prim_old(mose_gpu_ctx* ctx, int32_t b, const double* PO) {
+  return prim_io(ctx, b, const_cast<double*>(PO), ctx ? ctx->po : 1, true);
+}
+int mose_gpu_download_residual(mose_gpu_ctx* ctx, int32_t b, double* R) { return prim_io(ctx, b, R, -1, false); }
+int mose_gpu_upload_residual(mose_gpu_ctx* ctx, int32_t b, const double* R) {
+  return prim_io(ctx, b, const_cast<double*>(R), -1, true);
+}
+
+static int dt_io(mose_gpu_ctx* ctx, int32_t b, double* dt, bool upload) {
+  if (!ctx || !dt) return MOSE_ERR_INVALID;
+  if (!ctx->ready) return fail(ctx, MOSE_ERR_NOT_READY, "setup not done");
+  if (b < 1 || b > (int)ctx->hblk.size()) return fail(ctx, MOSE_ERR_INVALID, "bad block %d", b);
+  CU(cudaSetDevice(ctx->cfg.device));
+  const HostBlock& h = ctx->hblk[b - 1];
+  long long n = (long long)h.ni * h.nj * h.nk;
+  int rc = ensure_staging(ctx, (size_t)n);
+  if (rc) return rc;
+  if (upload) {
+    CU(cudaMemcpyAsync(ctx->staging.p, dt, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    launch_plane_io(ctx->d_desc.p, b - 1, n, ctx->dtl.p, ctx->staging.p, ctx->nd, 0, ctx->stream);
+  } else {
+    launch_plane_io(ctx->d_desc.p, b - 1, n, ctx->dtl.p, ctx->staging.p, ctx->nd, 1, ctx->stream);
+    CU(cudaMemcpyAsync(dt, ctx->staging.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ctx->launches++;
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_launch(ctx, "dt transfer");
+}
+int mose_gpu_download_dt(mose_gpu_ctx* ctx, int32_t b, double* dt) { return dt_io(ctx, b, dt, false); }
+int mose_gpu_upload_dt(mose_gpu_ctx* ctx, int32_t b, const double* dt) {
+  return dt_io(ctx, b, const_cast<double*>(dt), true);
+}
+
+// ---- phases ----------------------------------------------------------------------
+static int require_ready(mose_gpu_ctx* ctx) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (!ctx->ready) return fail(ctx, MOSE_ERR_NOT_READY, "setup not done");
+  if (cudaSetDevice(ctx->cfg.device) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "cudaSetDevice");
+  return MOSE_OK;
+}
+
+int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ramp_iter, double* dtglobal) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (!dtglobal) return MOSE_ERR_INVALID;
+  launch_step_begin(ctx->dtmin.p, *dtglobal, nullptr, ctx->stream);
+  launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->margs(),
+                    ctx->dtl.p, ctx->dtmin.p, ctx->gas, cfl, ctx->ndir, ctx->nd, iter, ramp_iter, 1, ctx->uniform,
+                    ctx->stream);
+  launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, 0, ctx->stream);
+  ctx->launches += 3;
+  CU(cudaMemcpyAsync(dtglobal, ctx->scal.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_launch(ctx, "compute_dt");
+}
+
+int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(ctx->scal.p, &dtglobal, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  launch_set_global_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->dtl.p, ctx->scal.p, ctx->nd,
+                       ctx->stream);
+  ctx->launches++;
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_launch(ctx, "set_global_dt");
+}
+
+int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  ctx->po = (ctx->cur + 1) % 3;
+  CU(cudaMemcpyAsync(ctx->state[ctx->po].p, ctx->state[ctx->cur].p, ctx->state[0].n * sizeof(double),
+                     cudaMemcpyDeviceToDevice, ctx->stream));
+  return MOSE_OK;
+}
+
+int mose_gpu_fill_ghosts(mose_gpu_ctx* ctx) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[ctx->cur].p, ctx->margs(), ctx->nd,
+                     ctx->stream);
+  ctx->launches++;
+  return check_launch(ctx, "fill_ghosts");
+}
+
+static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) {
+  static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
+  StageArgs a{};
+  a.blk = ctx->d_desc.p;
+  a.items = ctx->items.p;
+  a.nitems = ctx->nitems;
+  a.Pc = ctx->state[pc].p;
+  a.Po = ctx->state[po].p;
+  a.Pn = pn >= 0 ? ctx->state[pn].p : nullptr;
+  a.R = ctx->resid.p;
+  a.m = ctx->margs();
+  a.dtl = ctx->dtl.p;
+  a.dtg = ctx->scal.p;
+  a.bcw = ctx->bcw.p;
+  a.bcp = ctx->bcp.p;
+  a.c_rk = RKcoeff[ctx->cfg.n_rk - 1][irk - 1];
+  a.irk = irk;
+  a.time_accurate = ctx->cfg.time_accurate;
+  a.err = ctx->derr.p;
+  a.g = ctx->gas;
+  return a;
+}
+
+int mose_gpu_residual(mose_gpu_ctx* ctx) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  StageArgs a = stage_args(ctx, ctx->cur, ctx->po, -1, 1);
+  if (!launch_stage2d_exact(a, ctx->stage_grid, 1, ctx->uniform, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream))
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "no kernel for this solver / limiter");
+  ctx->launches++;
+  return check_launch(ctx, "residual");
+}
+
+int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (irk < 1 || irk > ctx->cfg.n_rk) return fail(ctx, MOSE_ERR_INVALID, "irk out of range");
+  static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
+  launch_rk_stage(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->state[ctx->po].p,
+                  ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->nd,
+                  ctx->uniform, ctx->derr.p, ctx->stream);
+  ctx->launches++;
+  return check_launch(ctx, "rk_stage");
+}
+
+// Enqueues one fused Explicit_Step starting from state arena s0.  Returns the
+// number of kernels enqueued.
+static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
+  int k = 0;
+  launch_step_begin(ctx->dtmin.p, 1e5, ctx->iterdev.p, ctx->stream); ++k;
+  // Compute_dt starts its minimum from 1d5 (Mod_Explicit.f90:44)
+  launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(), ctx->dtl.p,
+                    ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, -1, 0, ctx->cfg.time_accurate ? 0 : 1,
+                    ctx->uniform, ctx->stream); ++k;
+  launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, ctx->stream); ++k;
+  int pc = s0;
+  for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
+    int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
+    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd,
+                       ctx->stream);
+    if (ctx->nghost) ++k;
+    StageArgs a = stage_args(ctx, pc, s0, pn, irk);
+    launch_stage2d_exact(a, ctx->stage_grid, 0, ctx->uniform, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream);
+    ++k;
+    pc = pn;
+  }
+  return k;
+}
+
+static int step_final_index(const mose_gpu_ctx* ctx, int s0) {
+  int pc = s0;
+  for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk)
+    pc = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
+  return pc;
+}
+
+int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
+  CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  int s0 = ctx->cur;
+  ctx->launches += enqueue_step(ctx, s0);
+  rc = check_launch(ctx, "step");
+  if (rc) return rc;
+  ctx->po = s0;
+  ctx->cur = step_final_index(ctx, s0);
+  double h[2];
+  CU(cudaMemcpyAsync(h, ctx->scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  rc = poll_device_error(ctx);
+  ctx->h_iter += 1;
+  ctx->h_time = h[1];
+  if (dtglobal) *dtglobal = h[0];
+  if (time) *time = h[1];
+  return rc;
+}
+
+int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double* time) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (nsteps < 0) return MOSE_ERR_INVALID;
+  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
+  CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  for (int n = 0; n < nsteps; ++n) {
+    int s0 = ctx->cur;
+    if (!ctx->graph[s0]) {
+      cudaGraph_t g;
+      CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      int k = enqueue_step(ctx, s0);
+      CU(cudaStreamEndCapture(ctx->stream, &g));
+      CU(cudaGraphInstantiate(&ctx->graph[s0], g, 0));
+      cudaGraphDestroy(g);
+      ctx->graph_kernels = k;
+    }
+    CU(cudaGraphLaunch(ctx->graph[s0], ctx->stream));
+    ctx->launches += ctx->graph_kernels;
+    ctx->po = s0;
+    ctx->cur = step_final_index(ctx, s0);
+  }
+  double h[2];
+  CU(cudaMemcpyAsync(h, ctx->scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  rc = poll_device_error(ctx);
+  ctx->h_iter += nsteps;
+  ctx->h_time = h[1];
+  if (dtglobal) *dtglobal = h[0];
+  if (time) *time = h[1];
+  return rc;
+}
+
+int mose_gpu_residual_norms(mose_gpu_ctx* ctx, double* total) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (!total) return MOSE_ERR_INVALID;
+  launch_residual_norms(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p,
+                        ctx->state[ctx->po].p, ctx->nd, ctx->partial.p, ctx->norms.p, ctx->stream);
+  ctx->launches += 2;
+  CU(cudaMemcpyAsync(total, ctx->norms.p, 5 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  return check_launch(ctx, "residual_norms");
+}
+
+int mose_gpu_set_time(mose_gpu_ctx* ctx, double time, int32_t iter) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  ctx->h_time = time;
+  ctx->h_iter = iter;
+  return MOSE_OK;
+}
+
+int mose_gpu_get_time(mose_gpu_ctx* ctx, double* time, int32_t* iter) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (time) *time = ctx->h_time;
+  if (iter) *iter = ctx->h_iter;
+  return MOSE_OK;
+}
+
+int mose_gpu_synchronize(mose_gpu_ctx* ctx) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  CU(cudaStreamSynchronize(ctx->stream));
+  rc = check_launch(ctx, "synchronize");
+  if (rc) return rc;
+  return poll_device_error(ctx);
+}
+
+void* mose_gpu_stream(const mose_gpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t* launches) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (!ms || !launches || nsteps < 1) return MOSE_ERR_INVALID;
+  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
+  for (int c = 0; c < 3; ++c) { ms[c] = 0.0; launches[c] = 0; }
+  CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> cls;
+  auto mark = [&](int c) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    cudaEventRecord(e, ctx->stream);
+    ev.push_back(e);
+    cls.push_back(c);
+  };
+  for (int n = 0; n < nsteps; ++n) {
+    int s0 = ctx->cur;
+    mark(-1);
+    launch_step_begin(ctx->dtmin.p, 1e5, ctx->iterdev.p, ctx->stream);
+    launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(),
+                      ctx->dtl.p, ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, -1, 0,
+                      ctx->cfg.time_accurate ? 0 : 1, ctx->uniform, ctx->stream);
+    launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, ctx->stream);
+    mark(0);
+    launches[0] += 3;
+    int pc = s0;
+    for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
+      int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
+      if (ctx->nghost) {
+        launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd,
+                           ctx->stream);
+        mark(1);
+        launches[1] += 1;
+      }
+      StageArgs a = stage_args(ctx, pc, s0, pn, irk);
+      launch_stage2d_exact(a, ctx->stage_grid, 0, ctx->uniform, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream);
+      mark(2);
+      launches[2] += 1;
+      pc = pn;
+    }
+    ctx->po = s0;
+    ctx->cur = pc;
+  }
+  ctx->launches += launches[0] + launches[1] + launches[2];
+  CU(cudaStreamSynchronize(ctx->stream));
+  rc = check_launch(ctx, "time_kernels");
+  for (size_t q = 1; q < ev.size(); ++q) {
+    if (cls[q] < 0) continue;
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ev[q - 1], ev[q]);
+    ms[cls[q]] += t;
+  }
+  for (auto e : ev) cudaEventDestroy(e);
+  double h[2];
+  CU(cudaMemcpy(h, ctx->scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost));
+  ctx->h_time = h[1];
+  ctx->h_iter += nsteps;
+  if (rc) return rc;
+  return poll_device_error(ctx);
+}
+
+int mose_gpu_uniform_metrics(const mose_gpu_ctx* ctx) { return ctx && ctx->uniform ? 1 : 0; }
+int64_t mose_gpu_launch_count(const mose_gpu_ctx* ctx) { return ctx ? ctx->launches : -1; }
+
+int mose_gpu_download_metrics(mose_gpu_ctx* ctx, int32_t b, double* vol, double* dl) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (b < 1 || b > (int)ctx->hblk.size()) return fail(ctx, MOSE_ERR_INVALID, "bad block");
+  const HostBlock& h = ctx->hblk[b - 1];
+  long long n = (long long)(h.ni + 4) * (h.nj + 4) * (h.nk + 4);
+  DevBuf<double> v, l;
+  if (vol) CU(v.alloc(n));
+  if (dl) CU(l.alloc(3 * n));
+  launch_metrics_to_ref(ctx->d_desc.p, b - 1, n, ctx->margs(), v.p, l.p, ctx->nd, ctx->stream);
+  ctx->launches++;
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (vol) CU(cudaMemcpy(vol, v.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (dl) CU(cudaMemcpy(dl, l.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  return check_launch(ctx, "download_metrics");
+}
+
+int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N, double* A) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (b < 1 || b > (int)ctx->hblk.size() || dir < 1 || dir > ctx->nd) return fail(ctx, MOSE_ERR_INVALID, "bad args");
+  const HostBlock& h = ctx->hblk[b - 1];
+  int d0 = dir - 1;
+  long long n = (long long)(h.ni + (d0 == 0)) * (h.nj + (d0 == 1)) * (h.nk + (d0 == 2));
+  DevBuf<double> nn, aa;
+  if (N) CU(nn.alloc(3 * n));
+  if (A) CU(aa.alloc(n));
+  launch_faces_to_ref(ctx->d_desc.p, b - 1, n, ctx->margs(), d0, nn.p, aa.p, ctx->nd, ctx->stream);
+  ctx->launches++;
+  CU(cudaStreamSynchronize(ctx->stream));
+  if (N) CU(cudaMemcpy(N, nn.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (A) CU(cudaMemcpy(A, aa.p, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return check_launch(ctx, "download_faces");
+}
+
+}  // extern "C"

@@ -1,0 +1,434 @@
+// physics_exact.cuh -- FP64 face physics in the reference's operation order.
+//
+// Every expression below keeps MOSE's Fortran evaluation order (left to right
+// for equal precedence, x**2 as x*x) and this header is only compiled into a
+// translation unit built with --fmad=false, so each operation rounds once
+// exactly as the Fortran source reads.  The results are bit-identical to the
+// reference algorithm's FP64 arithmetic.
+//
+// NV = 4 (2-D: rho, u, v, p) or 5 (3-D: rho, u, v, w, p).  In 2-D the w terms
+// of the reference are identically zero (w = 0, n_z = 0) and are omitted; the
+// omitted terms only ever add an exact zero.
+//
+// Thermodynamics: the reference calls FLINT (absent from its tree) for
+// rho, R, a, h, e.  This file uses FLINT's documented model for one
+// calorically perfect species: T = p/(rho R), a = sqrt(gamma R T),
+// h = cp T, e = cv T.
+#pragma once
+
+#include "common.cuh"
+
+namespace mose {
+namespace ex {
+
+template <int NV> struct V { double q[NV]; };
+
+// ---- limiters: Lib_Limiters.f90:24-105 ------------------------------------
+template <int LIM>
+__device__ __forceinline__ double limiter(double x, double y) {
+  if constexpr (LIM == 1) {            // minmod :35-45
+    double r = 0.0;
+    if (x * y < 0.0) return r;
+    r = x;
+    if (fabs(x) > fabs(y)) r = y;
+    return r;
+  } else if constexpr (LIM == 2) {     // van Leer :49-60
+    double ru = y / (x + 1e-30);
+    double phi = (ru + fabs(ru)) / (1.0 + fabs(ru));
+    return phi * x;
+  } else if constexpr (LIM == 3) {     // van Albada :64-75
+    double ru = y / (x + 1e-30);
+    double phi = (ru * ru + ru) / (1.0 + ru * ru);
+    return phi * x;
+  } else if constexpr (LIM == 4) {     // MC :79-90
+    double ru = y / (x + 1e-30);
+    double m = fmin(fmin(2.0 * ru, 0.5 * (1.0 + ru)), 2.0);
+    double phi = fmax(0.0, m);
+    return phi * x;
+  } else if constexpr (LIM == 5) {     // superbee :94-104
+    double ru = y / (x + 1e-30);
+    double phi = fmax(fmax(0.0, fmin(2.0 * ru, 1.0)), fmin(ru, 2.0));
+    return phi * x;
+  } else {                             // first order :24-31
+    return 0.0;
+  }
+}
+
+// ---- thermodynamic closure --------------------------------------------------
+// co_rotot_Rtot + f_ss for one species: R = (rho/rho) R_1 = R_1 exactly.
+__device__ __forceinline__ double sound(const Gas& g, double rho, double p) {
+  double T = p / (rho * g.R);
+  return sqrt(g.gamma * g.R * T);
+}
+// H0(p, rho_s, |u|) with |u|^2 passed squared-of-norm as the reference does.
+__device__ __forceinline__ double H0(const Gas& g, double p, double rho, double umag) {
+  double T = p / (rho * g.R);
+  double h = g.cp * T;
+  return h + 0.5 * (umag * umag);
+}
+
+template <int NV>
+__device__ __forceinline__ double dot_vel(const double* q, const double* n) {
+  if constexpr (NV == 5) return q[1] * n[0] + q[2] * n[1] + q[3] * n[2];
+  else return q[1] * n[0] + q[2] * n[1];
+}
+template <int NV>
+__device__ __forceinline__ double vel_sq(const double* q) {
+  if constexpr (NV == 5) return q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+  else return q[1] * q[1] + q[2] * q[2];
+}
+
+// ---- Riemann solvers (interface of Mod_Riemann.f90:13-28) -------------------
+// Input states q = (rho, u, v, [w,] p) with sound speed a; output per unit area
+// (F_r, F_u, F_v, [F_w,] F_E).
+template <int NV>
+__device__ __forceinline__ void hllc(const Gas& g, const double* L, double aL, const double* R,
+                                     double aR, const double* n, double* F) {
+  // riemann_HLLC, Lib_Riemann_HLL.f90:147-258, with roe_averages :550-647
+  constexpr int P = NV - 1;
+  const double rl = L[0], rr = R[0];
+  double unl = dot_vel<NV>(L, n);
+  double unr = dot_vel<NV>(R, n);
+  double inv_dltot = 1.0 / rl;
+  double inv_drtot = 1.0 / rr;
+  double Tl = L[P] * inv_dltot / g.R;
+  double Tr = R[P] * inv_drtot / g.R;
+  double srL = sqrt(rl);
+  double srR = sqrt(rr);
+  double inv_sr = 1.0 / (srL + srR);
+  double u_roe = (srR * R[1] + srL * L[1]) * inv_sr;
+  double v_roe = (srR * R[2] + srL * L[2]) * inv_sr;
+  double w_roe = 0.0;
+  if constexpr (NV == 5) w_roe = (srR * R[3] + srL * L[3]) * inv_sr;
+  double R_roe = (srR * g.R + srL * g.R) * inv_sr;
+  double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  double hl = g.cp * Tl;
+  double hr = g.cp * Tr;
+  double el = hl - g.R * Tl;
+  double er = hr - g.R * Tr;
+  double h0l = hl * rl * inv_dltot;
+  double h0r = hr * rr * inv_drtot;
+  double d_roe = (srR * rr * inv_drtot + srL * rl * inv_dltot) * inv_sr;
+  double cv_roe = d_roe * g.cpmR;
+  double sum_ei = d_roe * (srR * er + srL * el) * inv_sr;
+  h0l = h0l + 0.5 * vel_sq<NV>(L);
+  h0r = h0r + 0.5 * vel_sq<NV>(R);
+  double h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  double gam_roe = 1.0 + R_roe / cv_roe;
+  double vel2;
+  if constexpr (NV == 5) vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  else vel2 = u_roe * u_roe + v_roe * v_roe;
+  double a_roe = sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  double un_roe;
+  if constexpr (NV == 5) un_roe = u_roe * n[0] + v_roe * n[1] + w_roe * n[2];
+  else un_roe = u_roe * n[0] + v_roe * n[1];
+  double e0l = h0l - L[P] / rl;
+  double e0r = h0r - R[P] / rr;
+  double S1 = fmin(fmin(0.0, unl - aL), un_roe - a_roe);
+  double S4 = fmax(fmax(0.0, unr + aR), un_roe + a_roe);
+  double inv_denom = 1.0 / (rl * (S1 - unl) - rr * (S4 - unr));
+  double Sstar = (R[P] - L[P] + rl * unl * (S1 - unl) - rr * unr * (S4 - unr)) * inv_denom;
+  double pstar = rl * (unl - S1) * (unl - Sstar) + L[P];
+  if (S1 >= 0.0) {
+    F[0] = rl * unl;
+    for (int d = 0; d < NV - 2; ++d) F[1 + d] = F[0] * L[1 + d] + L[P] * n[d];
+    F[P] = F[0] * h0l;
+  } else if (Sstar >= 0.0) {
+    F[0] = rl * unl;
+    for (int d = 0; d < NV - 2; ++d) F[1 + d] = F[0] * L[1 + d] + L[P] * n[d];
+    F[P] = F[0] * h0l;
+    double inv = 1.0 / (S1 - Sstar);
+    double U1S = rl * (S1 - unl) * inv;
+    F[0] = F[0] + S1 * (U1S - rl);
+    for (int d = 0; d < NV - 2; ++d) {
+      double UdS = ((S1 - unl) * rl * L[1 + d] + (pstar - L[P]) * n[d]) * inv;
+      F[1 + d] = F[1 + d] + S1 * (UdS - rl * L[1 + d]);
+    }
+    double U5S = ((S1 - unl) * rl * e0l - L[P] * unl + pstar * Sstar) * inv;
+    F[P] = F[P] + S1 * (U5S - rl * e0l);
+  } else if (S4 > 0.0) {
+    F[0] = rr * unr;
+    for (int d = 0; d < NV - 2; ++d) F[1 + d] = F[0] * R[1 + d] + R[P] * n[d];
+    F[P] = F[0] * h0r;
+    double inv = 1.0 / (S4 - Sstar);
+    double U1S = rr * (S4 - unr) * inv;
+    F[0] = F[0] + S4 * (U1S - rr);
+    for (int d = 0; d < NV - 2; ++d) {
+      double UdS = ((S4 - unr) * rr * R[1 + d] + (pstar - R[P]) * n[d]) * inv;
+      F[1 + d] = F[1 + d] + S4 * (UdS - rr * R[1 + d]);
+    }
+    double U5S = ((S4 - unr) * rr * e0r - R[P] * unr + pstar * Sstar) * inv;
+    F[P] = F[P] + S4 * (U5S - rr * e0r);
+  } else {
+    F[0] = rr * unr;
+    for (int d = 0; d < NV - 2; ++d) F[1 + d] = F[0] * R[1 + d] + R[P] * n[d];
+    F[P] = F[0] * h0r;
+  }
+}
+
+template <int NV>
+__device__ __forceinline__ void ausmp(const Gas& g, const double* L, double aL, const double* R,
+                                      double aR, const double* n, double* F) {
+  // riemann_AUSMp, Lib_Riemann_AUSM.f90:150-238
+  constexpr int P = NV - 1;
+  const double beta = 0.125, alpha = 0.1875;
+  double unl = dot_vel<NV>(L, n);
+  double unr = dot_vel<NV>(R, n);
+  double H_L = H0(g, L[P], L[0], sqrt(vel_sq<NV>(L)));
+  double H_R = H0(g, R[P], R[0], sqrt(vel_sq<NV>(R)));
+  double a_half = sqrt(aL * aR);
+  double ML = unl / a_half;
+  double MR = unr / a_half;
+  double MplusL, pplusL, MminusR, pminusR;
+  if (fabs(ML) < 1.0) {
+    MplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) + beta * ((ML * ML - 1.0) * (ML * ML - 1.0));
+    pplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) * (2.0 - ML) + alpha * ML * ((ML * ML - 1.0) * (ML * ML - 1.0));
+  } else {
+    MplusL = 0.5 * (ML + fabs(ML));
+    pplusL = 0.5 * (1.0 + copysign(1.0, ML));
+  }
+  if (fabs(MR) < 1.0) {
+    MminusR = -(0.25 * ((MR - 1.0) * (MR - 1.0))) - beta * ((MR * MR - 1.0) * (MR * MR - 1.0));
+    pminusR = 0.25 * ((MR - 1.0) * (MR - 1.0)) * (2.0 + MR) - alpha * MR * ((MR * MR - 1.0) * (MR * MR - 1.0));
+  } else {
+    MminusR = 0.5 * (MR - fabs(MR));
+    pminusR = 0.5 * (1.0 - copysign(1.0, MR));
+  }
+  double Mhalf = MplusL + MminusR;
+  double phalf = pplusL * L[P] + pminusR * R[P];
+  double mdotp = L[0] * a_half * 0.5 * (Mhalf + fabs(Mhalf));
+  double mdotm = R[0] * a_half * 0.5 * (Mhalf - fabs(Mhalf));
+  F[0] = mdotp + mdotm;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = mdotp * L[1 + d] + mdotm * R[1 + d] + n[d] * phalf;
+  F[P] = mdotp * H_L + mdotm * H_R;
+}
+
+template <int NV>
+__device__ __forceinline__ void slau(const Gas& g, const double* L, double aL, const double* R,
+                                     double aR, const double* n, double* F, bool slau2) {
+  // riemann_SLAU / riemann_SLAU2, Lib_Riemann_SLAU.f90:19-141
+  constexpr int P = NV - 1;
+  const double rl = L[0], rr = R[0];
+  double unl = dot_vel<NV>(L, n);
+  double unr = dot_vel<NV>(R, n);
+  double sq_veli = vel_sq<NV>(L);
+  double sq_velj = vel_sq<NV>(R);
+  double aF = 0.5 * (aL + aR);
+  double mL = unl / aF;
+  double mR = unr / aF;
+  double Mach_tilde = fmin(1.0, sqrt(0.5 * (sq_veli + sq_velj)) / aF);
+  double Chi = (1.0 - Mach_tilde) * (1.0 - Mach_tilde);
+  double Vn_mag = (rl * fabs(unl) + rr * fabs(unr)) / (rl + rr);
+  double f_rho = -fmax(fmin(mL, 0.0), -1.0) * fmin(fmax(mR, 0.0), 1.0);
+  double Vn_magL = (1.0 - f_rho) * Vn_mag + f_rho * fabs(unl);
+  double Vn_magR = (1.0 - f_rho) * Vn_mag + f_rho * fabs(unr);
+  F[0] = 0.5 * (rl * (unl + Vn_magL) + rr * (unr - Vn_magR) - (Chi / aF) * (R[P] - L[P]));
+  double BetaL, BetaR;
+  if (fabs(mL) < 1.0) BetaL = 0.25 * (2.0 - mL) * ((mL + 1.0) * (mL + 1.0));
+  else if (mL >= 0.0) BetaL = 1.0;
+  else BetaL = 0.0;
+  if (fabs(mR) < 1.0) BetaR = 0.25 * (2.0 + mR) * ((mR - 1.0) * (mR - 1.0));
+  else if (mR >= 0.0) BetaR = 0.0;
+  else BetaR = 1.0;
+  double p_half;
+  if (!slau2)
+    p_half = 0.5 * (L[P] + R[P]) + 0.5 * (BetaL - BetaR) * (L[P] - R[P]) +
+             (1.0 - Chi) * (BetaL + BetaR - 1.0) * 0.5 * (L[P] + R[P]);
+  else
+    p_half = 0.5 * (L[P] + R[P]) + 0.5 * (BetaL - BetaR) * (L[P] - R[P]) +
+             sqrt(0.5 * (sq_veli + sq_velj)) * (BetaL + BetaR - 1.0) * aF * 0.5 * (rl + rr);
+  double H_L = H0(g, L[P], rl, sqrt(sq_veli));
+  double H_R = H0(g, R[P], rr, sqrt(sq_velj));
+  const double* S = (F[0] >= 0.0) ? L : R;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = F[0] * S[1 + d] + n[d] * p_half;
+  F[P] = F[0] * ((F[0] >= 0.0) ? H_L : H_R);
+}
+
+template <int RIE, int NV>
+__device__ __forceinline__ void riemann(const Gas& g, const double* L, double aL, const double* R,
+                                        double aR, const double* n, double* F) {
+  if constexpr (RIE == 1) ausmp<NV>(g, L, aL, R, aR, n, F);
+  else if constexpr (RIE == 2) slau<NV>(g, L, aL, R, aR, n, F, false);
+  else if constexpr (RIE == 3) slau<NV>(g, L, aL, R, aR, n, F, true);
+  else hllc<NV>(g, L, aL, R, aR, n, F);
+}
+
+// Interface flux times area, including the species upwinding of
+// Lib_Convective.f90:66-75.  For one species the species flux
+// F_r*A*(sp*(rho1/rho1) - sm*(rho4/rho4)) equals F_r*A exactly.
+// Returns false when check_gas_state rejects either state.
+template <int RIE, int NV>
+__device__ __forceinline__ bool face_flux(const Gas& g, const double* QL, const double* QR,
+                                          const double* n, double area, double* F) {
+  constexpr int P = NV - 1;
+  bool ok = (QL[0] > 0.0 && QL[P] > 0.0 && QR[0] > 0.0 && QR[P] > 0.0);
+  double aL = sound(g, QL[0], QL[P]);
+  double aR = sound(g, QR[0], QR[P]);
+  riemann<RIE, NV>(g, QL, aL, QR, aR, n, F);
+  for (int v = 0; v < NV; ++v) F[v] = F[v] * area;
+  return ok;
+}
+
+// ---- boundary-face fluxes ---------------------------------------------------
+// All return the flux oriented along the face normal (the low-to-high index
+// direction); the caller adds modfm2 * flux.
+
+// BC_Extrapolation, Lib_BC_Fluxes_Extrapolation.f90:13-47
+template <int NV>
+__device__ __forceinline__ void bc_extrapolation(const Gas& g, const double* Q, const double* n,
+                                                 double area, double* F) {
+  constexpr int P = NV - 1;
+  double Un = dot_vel<NV>(Q, n);
+  F[0] = Q[0] * Un * area;
+  double Fmass = F[0];
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = Fmass * Q[1 + d] + Q[P] * area * n[d];
+  F[P] = Fmass * H0(g, Q[P], Q[0], sqrt(vel_sq<NV>(Q)));
+}
+
+// BC_Symmetry_Eul, Lib_BC_Fluxes_Symmetry.f90:14-125 (no rotating frame).
+// Bound = boundary cell, Int = first interior cell, s = modfm2 (-1 odd faces).
+// Only the momentum components are meaningful (the caller adds only those).
+template <int RIE, int LIM, int NV>
+__device__ __forceinline__ void bc_symmetry(const Gas& g, const double* Bound, const double* Int,
+                                            double dlB, double dlI, const double* n, double area,
+                                            int face, double* F) {
+  constexpr int P = NV - 1;
+  const double fm = (double)(face % 2), fm1 = (double)(1 - face % 2), s = (double)(1 - 2 * (face % 2));
+  double Bound_Dl = 0.5 * dlB;
+  double Int_Dl = 0.5 * dlI;
+  double Un = dot_vel<NV>(Bound, n);
+  double Ghost[NV];
+  for (int v = 0; v < NV; ++v) Ghost[v] = Bound[v];
+  for (int d = 0; d < NV - 2; ++d) Ghost[1 + d] = Ghost[1 + d] - 2.0 * Un * n[d];
+  double Dist12 = 2.0 * Bound_Dl * fm + (Bound_Dl + Int_Dl) * fm1;
+  double Dist23 = (Bound_Dl + Int_Dl) * fm + 2.0 * Bound_Dl * fm1;
+  double Face[NV];
+  double Dist = Bound_Dl * s;
+  for (int v = 0; v < NV; ++v) {
+    double p1 = fm * Ghost[v] + fm1 * Int[v];
+    double p3 = fm * Int[v] + fm1 * Ghost[v];
+    double s32 = (p3 - Bound[v]) / Dist23;
+    double s21 = (Bound[v] - p1) / Dist12;
+    double sl = limiter<LIM>(s32, s21);
+    Face[v] = Bound[v] + sl * Dist;
+  }
+  double Sound = sound(g, Face[0], Face[P]);
+  double Unf = dot_vel<NV>(Face, n);
+  double Un1 = Unf * s;
+  double U1[NV], U4[NV];
+  U1[0] = U4[0] = Face[0];
+  U1[P] = U4[P] = Face[P];
+  for (int d = 0; d < NV - 2; ++d) {
+    double velt = Face[1 + d] - Unf * n[d];
+    U1[1 + d] = Un1 * n[d] + velt;
+    U4[1 + d] = -Un1 * n[d] + velt;
+  }
+  riemann<RIE, NV>(g, U1, Sound, U4, Sound, n, F);
+  for (int v = 0; v < NV; ++v) F[v] = F[v] * area;
+}
+
+// Supersonic_Inflow, Lib_BC_Fluxes_Inflow.f90:289-382 (called from
+// BC_Inlet_Supersonic_Static :244-281 once BC_Sign*Un < 0 has been checked).
+template <int RIE, int LIM, int NV>
+__device__ __forceinline__ bool bc_supersonic_inflow(const Gas& g, const double* Prim2, const double* Int,
+                                                     const BcParam& bp, const double* n, double area,
+                                                     int face, double* F) {
+  constexpr int P = NV - 1;
+  const double fm = (double)(face % 2), fm1 = (double)(1 - face % 2), s = (double)(1 - 2 * (face % 2));
+  double flow_Sound = sound(g, Prim2[0], Prim2[P]);
+  double flow_Mach = sqrt(vel_sq<NV>(Prim2)) / flow_Sound;
+  double BC_Mach_local = bp.rel_fac * bp.mach + (1.0 - bp.rel_fac) * flow_Mach;
+  double BC_p0_local = bp.rel_fac * bp.p + (1.0 - bp.rel_fac) * Prim2[P];
+  double Sup[NV];
+  Sup[P] = BC_p0_local;
+  double Sup_Rgas = 1.0 * g.R;
+  double Sup_rho = Sup[P] / (Sup_Rgas * bp.T);
+  Sup[0] = Sup_rho * 1.0;
+  double Sup_Sound = sound(g, Sup[0], Sup[P]);
+  Sup[1] = BC_Mach_local * Sup_Sound * bp.ca * bp.cb;
+  Sup[2] = BC_Mach_local * Sup_Sound * bp.sa * bp.cb;
+  if constexpr (NV == 5) Sup[3] = BC_Mach_local * Sup_Sound * bp.sb;
+  double PL[NV], PR[NV];
+  for (int v = 0; v < NV; ++v) {
+    double p1 = fm * Sup[v] + fm1 * Int[v];
+    double p3 = fm * Int[v] + fm1 * Sup[v];
+    double d32 = p3 - Prim2[v];
+    double d21 = Prim2[v] - p1;
+    double sl = limiter<LIM>(d32, d21);
+    double face_v = Prim2[v] + 0.5 * sl * s;
+    PL[v] = fm * Sup[v] + fm1 * face_v;
+    PR[v] = fm * face_v + fm1 * Sup[v];
+  }
+  double aL = sound(g, PL[0], PL[P]);
+  double aR = sound(g, PR[0], PR[P]);
+  riemann<RIE, NV>(g, PL, aL, PR, aR, n, F);
+  for (int v = 0; v < NV; ++v) F[v] = F[v] * area;
+  return true;
+}
+
+// Outflow, Lib_BC_Fluxes_Outflow.f90:59-129 (after BC_Sign*Un >= 0 was checked).
+template <int NV>
+__device__ __forceinline__ void bc_outflow(const Gas& g, const double* Bound, double Un,
+                                           const double* n, double area, double pexit_in,
+                                           int face, double* F) {
+  constexpr int P = NV - 1;
+  const double BC_Sign = (double)(1 - 2 * (face % 2));
+  double Bound_rho = Bound[0];
+  double Bound_Sound = sound(g, Bound[0], Bound[P]);
+  double Bound_Gamma = g.gamma;
+  double Riem = Bound_Sound + BC_Sign * 0.5 * (Bound_Gamma - 1.0) * Un;
+  double Mach_N = fabs(Un / Bound_Sound);
+  double Face[NV], Face_Un, Face_rho;
+  if (Mach_N < 1.0 && pexit_in > 0.0) {
+    double p_exit = pexit_in;
+    double delta = 0.5 * (Bound_Gamma - 1.0);
+    double den = 1.0 / pow(1.0 + delta, Bound_Gamma / (Bound_Gamma - 1.0));
+    double pstar = Bound[P] * den * pow(1.0 + delta * (Mach_N * Mach_N), Bound_Gamma / (Bound_Gamma - 1.0));
+    if (pstar >= p_exit) p_exit = pstar;
+    double Isentropic = (Bound_Gamma - 1.0) / (2.0 * Bound_Gamma);
+    double Face_Sound = Bound_Sound * pow(p_exit / Bound[P], Isentropic);
+    Face_Un = (Riem - Face_Sound) / (BC_Sign * 0.5 * (Bound_Gamma - 1.0));
+    Face[P] = p_exit;
+    Face_rho = Bound_Gamma * Face[P] / (Face_Sound * Face_Sound);
+    Face[0] = Bound[0] / Bound_rho * Face_rho;
+    for (int d = 0; d < NV - 2; ++d) {
+      double velt = Bound[1 + d] - Un * n[d];
+      Face[1 + d] = velt + Face_Un * n[d];
+    }
+  } else {
+    for (int v = 0; v < NV; ++v) Face[v] = Bound[v];
+    Face_Un = Un;
+    Face_rho = Bound_rho;
+  }
+  double Face_T = Face[P] / (g.R * Face_rho);
+  double Face_Enthalpy = Face[0] / Face_rho * (g.cp * Face_T);
+  F[0] = Face[0] * area * Face_Un;
+  double BC_mdot = Face_rho * area * Face_Un;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = Face[1 + d] * BC_mdot + Face[P] * area * n[d];
+  F[P] = BC_mdot * (0.5 * vel_sq<NV>(Face) + Face_Enthalpy);
+}
+
+// ---- state update: Newstate_Conservative (Lib_Newstate.f90:134-160) --------
+template <int NV>
+__device__ __forceinline__ void prim2cons(const Gas& g, const double* Q, double* U) {
+  constexpr int P = NV - 1;
+  double rho = Q[0];
+  double T = Q[P] / (rho * g.R);
+  double e = g.cv * T;
+  U[0] = rho;
+  for (int d = 0; d < NV - 2; ++d) U[1 + d] = rho * Q[1 + d];
+  U[P] = rho * (e + 0.5 * vel_sq<NV>(Q));
+}
+template <int NV>
+__device__ __forceinline__ void cons2prim(const Gas& g, const double* U, double* Q) {
+  constexpr int P = NV - 1;
+  double rho = U[0];
+  Q[0] = rho;
+  for (int d = 0; d < NV - 2; ++d) Q[1 + d] = U[1 + d] / rho;
+  double e = U[P] / rho - 0.5 * vel_sq<NV>(Q);
+  double T = e / g.cv;
+  Q[P] = rho * g.R * T;
+}
+
+}  // namespace ex
+}  // namespace mose

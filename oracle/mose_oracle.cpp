@@ -1,0 +1,1620 @@
+// mose_oracle.cpp -- CPU oracle for MOSE's explicit inviscid residual-and-update
+// path on multi-block structured grids.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the timed CPU
+// baseline.  Nothing in the product links or calls this file.
+//
+// This is a restatement, routine by routine, of the reference Fortran.  The
+// data model is the reference's own: P, PO, R are Fortran-ordered
+// (nprim, 1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc) arrays, metrics carry ghost
+// layers in every direction, the boundary list is walked in bc.txt order.
+// Each arithmetic expression keeps the Fortran evaluation order (left to
+// right for equal precedence, `x**2` as x*x) and the file is compiled with
+// -ffp-contract=off, so every operation rounds once.
+//
+// Thermodynamic closure.  MOSE calls the FLINT library (submodule lib/FLINT,
+// https://github.com/MarcoGrossi92/FLINT, pinned commit not recoverable: the
+// submodule is empty in the reference tree) for every thermodynamic quantity.
+// Its source is absent, so this oracle restates FLINT's documented model
+// (docs/theory/thermo.md) for ONE calorically perfect species, consistent
+// with the constant-cp tables the reference ships (test/common/*/thermo.dat):
+//   rho = sum(rho_s) = rho_1,  R = sum(rho_s/rho * R_s) = R_1
+//   T = p / (rho R),  a = sqrt(gamma R T),  h(T) = cp T  (table h_tab)
+//   cp = gamma R / (gamma - 1),  cv = R / (gamma - 1)
+//   H0(p, rho_s, |u|) = h(T) + 0.5 |u|^2
+//   prim2cons: (rho, rho u, rho v, rho w, rho (cv T + 0.5 |u|^2))
+//   cons2prim: u = (rho u)/rho ..., T = (E/rho - 0.5|u|^2)/cv, p = rho R T
+//   check_gas_state: error unless rho_s > 0 and p > 0
+// norm2(v) is restated as sqrt(v1*v1 + v2*v2 + v3*v3).
+// Parity at this boundary is therefore against the restated closure; the
+// FLINT table path (1 K tables, int(T) index) cannot be reproduced without
+// its source.
+
+#include "mose_oracle.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int GC = 2;                 // Global_m.f90:17
+constexpr int NPRIM = 5;              // rho, u, v, w, p (one species)
+constexpr int NU = 1, NV = 2, NW = 3, NP = 4;   // 0-based nu, nv, nw, np
+constexpr int NRES = NPRIM;           // nres = nprim - nsc + 1
+
+// Parameters_m.f90:29-34: guide(face, dir) is the inward unit step of a face.
+const int guide[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0},
+                         {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+inline int G(int f, int d) { return guide[f - 1][d - 1]; }
+
+struct Vec3 { double c[3]; };
+
+struct Thermo {
+  double gamma, R, cp, cv;
+};
+
+struct Block {
+  int ni = 0, nj = 0, nk = 0;
+  int sx = 0, sy = 0, sz = 0;           // ghosted extents
+  std::vector<double> node;             // (3, 0:ni, 0:nj, 0:nk)
+  std::vector<double> P, PO, R;         // (5, ghosted cells)
+  std::vector<double> M;                // (3,3, ghosted cells), c(r,s) at r + 3 s
+  std::vector<double> dl;               // (3, ghosted cells)
+  std::vector<double> vol;              // (ghosted cells)
+  std::vector<double> fN[3], fA[3];     // dir(d)%f : N(3), A
+  std::vector<double> dtlocal, beta;    // (1:ni, 1:nj, 1:nk)
+
+  size_t cell(int i, int j, int k) const {
+    return (size_t)(i + GC - 1) + (size_t)sx * ((size_t)(j + GC - 1) + (size_t)sy * (size_t)(k + GC - 1));
+  }
+  size_t inner(int i, int j, int k) const {
+    return (size_t)(i - 1) + (size_t)ni * ((size_t)(j - 1) + (size_t)nj * (size_t)(k - 1));
+  }
+  const double* nodep(int i, int j, int k) const {
+    return &node[3 * ((size_t)i + (size_t)(ni + 1) * ((size_t)j + (size_t)(nj + 1) * (size_t)k))];
+  }
+  Vec3 nd(int i, int j, int k) const {
+    const double* p = nodep(i, j, k);
+    return Vec3{{p[0], p[1], p[2]}};
+  }
+  // dir(1)%f(0:ni, 1:nj, 1:nk), dir(2)%f(1:ni, 0:nj, 1:nk), dir(3)%f(1:ni, 1:nj, 0:nk)
+  size_t face(int d, int i, int j, int k) const {
+    if (d == 1) return (size_t)i + (size_t)(ni + 1) * ((size_t)(j - 1) + (size_t)nj * (size_t)(k - 1));
+    if (d == 2) return (size_t)(i - 1) + (size_t)ni * ((size_t)j + (size_t)(nj + 1) * (size_t)(k - 1));
+    return (size_t)(i - 1) + (size_t)ni * ((size_t)(j - 1) + (size_t)nj * (size_t)k);
+  }
+  double* Pc(int i, int j, int k) { return &P[NPRIM * cell(i, j, k)]; }
+  double* POc(int i, int j, int k) { return &PO[NPRIM * cell(i, j, k)]; }
+  double* Rc(int i, int j, int k) { return &R[NPRIM * cell(i, j, k)]; }
+  double& M_(int r, int s, int i, int j, int k) { return M[9 * cell(i, j, k) + (r - 1) + 3 * (s - 1)]; }
+  double& dl_(int h, int i, int j, int k) { return dl[3 * cell(i, j, k) + (h - 1)]; }
+  double& vol_(int i, int j, int k) { return vol[cell(i, j, k)]; }
+};
+
+struct BCrec {
+  int b, i, j, k, f, type, bs, is, js, ks, fs, d11, d12, d21, d22;
+  double data[6];
+};
+
+}  // namespace
+
+struct orc_domain {
+  orc_config cfg;
+  Thermo th;
+  int ndir = 0;
+  double delthe = 0.0;
+  int nthreads = 1;
+  std::vector<Block> blk;
+  std::vector<BCrec> bc;
+  std::vector<int> n_bf;                // (nb, 6)
+  double time = 0.0, dtglobal = 0.0;
+  int iter = 0, iter_from_call = 0;
+  int err = 0, eb = 0, ei = 0, ej = 0, ek = 0;
+
+  void fail(int code, int b, int i, int j, int k) {
+#ifdef _OPENMP
+#pragma omp critical(orc_err)
+#endif
+    {
+      if (err == 0) { err = code; eb = b; ei = i; ej = j; ek = k; }
+    }
+  }
+};
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Thermodynamic closure (restated FLINT, see header comment)
+// ---------------------------------------------------------------------------
+inline void co_rotot_Rtot(const Thermo& t, double rhos, double& rho, double& R) {
+  rho = rhos;
+  R = (rhos / rho) * t.R;
+}
+inline double f_ss(const Thermo& t, double /*rhos*/, double p, double rho, double R) {
+  double T = p / (rho * R);
+  return std::sqrt(t.gamma * R * T);
+}
+inline double H0(const Thermo& t, double p, double rhos, double umag) {
+  double rho = rhos, R = t.R;
+  double T = p / (rho * R);
+  double h = (rhos / rho) * (t.cp * T);
+  return h + 0.5 * (umag * umag);
+}
+inline double norm2(double a, double b, double c) { return std::sqrt(a * a + b * b + c * c); }
+inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+inline int check_gas_state(double rhos, double p) { return (rhos > 0.0 && p > 0.0) ? 0 : 1; }
+
+inline void prim2cons(const Thermo& t, const double* P, double* U) {
+  double rho = P[0];
+  double T = P[NP] / (rho * t.R);
+  double e = t.cv * T;
+  U[0] = rho;
+  U[NU] = rho * P[NU];
+  U[NV] = rho * P[NV];
+  U[NW] = rho * P[NW];
+  U[NP] = rho * (e + 0.5 * (P[NU] * P[NU] + P[NV] * P[NV] + P[NW] * P[NW]));
+}
+inline void cons2prim(const Thermo& t, const double* U, double* P) {
+  double rho = U[0];
+  double u = U[NU] / rho, v = U[NV] / rho, w = U[NW] / rho;
+  double e = U[NP] / rho - 0.5 * (u * u + v * v + w * w);
+  double T = e / t.cv;
+  P[0] = rho;
+  P[NU] = u;
+  P[NV] = v;
+  P[NW] = w;
+  P[NP] = rho * t.R * T;
+}
+
+// ---------------------------------------------------------------------------
+// Limiters: Lib_Limiters.f90:24-105
+// ---------------------------------------------------------------------------
+inline double lim_minmod(double x, double y) {        // :35-45
+  double r = 0.0;
+  if (x * y < 0.0) return r;
+  r = x;
+  if (std::fabs(x) > std::fabs(y)) r = y;
+  return r;
+}
+inline double lim_vanleer(double x, double y) {       // :49-60
+  double ru = y / (x + 1e-30);
+  double phi = (ru + std::fabs(ru)) / (1.0 + std::fabs(ru));
+  return phi * x;
+}
+inline double lim_vanalbada(double x, double y) {     // :64-75
+  double ru = y / (x + 1e-30);
+  double phi = (ru * ru + ru) / (1.0 + ru * ru);
+  return phi * x;
+}
+inline double lim_mc(double x, double y) {            // :79-90
+  double ru = y / (x + 1e-30);
+  double m = std::min(std::min(2.0 * ru, 0.5 * (1.0 + ru)), 2.0);
+  double phi = std::max(0.0, m);
+  return phi * x;
+}
+inline double lim_superbee(double x, double y) {      // :94-104
+  double ru = y / (x + 1e-30);
+  double phi = std::max(std::max(0.0, std::min(2.0 * ru, 1.0)), std::min(ru, 2.0));
+  return phi * x;
+}
+inline double rlimiter(int lim, double x, double y) {
+  switch (lim) {
+    case ORC_LIM_MINMOD: return lim_minmod(x, y);
+    case ORC_LIM_VANLEER: return lim_vanleer(x, y);
+    case ORC_LIM_VANALBADA: return lim_vanalbada(x, y);
+    case ORC_LIM_MC: return lim_mc(x, y);
+    case ORC_LIM_SUPERBEE: return lim_superbee(x, y);
+    default: return 0.0;                            // rlimiter_IORD :24-31
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Riemann solvers: interface of Mod_Riemann.f90:13-28
+// ---------------------------------------------------------------------------
+struct RState { double d, u, v, w, p, a, rho; };
+struct RFlux { double r, u, v, w, E; };
+
+// roe_averages, Lib_Riemann_HLL.f90:550-647, with the table thermo restated
+// for constant cp (h_tab(T) = cp T, cp_tab = cp, Runiv/Wm = R).
+inline void roe_averages(const Thermo& t, const RState& L, const RState& Rr, double& h0l,
+                         double& h0r, double& u_roe, double& v_roe, double& w_roe,
+                         double& a_roe, double& h0_roe) {
+  double Rl = t.R, Rrr = t.R;                               // f_Rtot
+  double inv_dltot = 1.0 / L.rho;
+  double inv_drtot = 1.0 / Rr.rho;
+  double Tl = L.p * inv_dltot / Rl;
+  double Tr = Rr.p * inv_drtot / Rrr;
+  double srL = std::sqrt(L.rho);
+  double srR = std::sqrt(Rr.rho);
+  double inv_sr = 1.0 / (srL + srR);
+  u_roe = (srR * Rr.u + srL * L.u) * inv_sr;
+  v_roe = (srR * Rr.v + srL * L.v) * inv_sr;
+  w_roe = (srR * Rr.w + srL * L.w) * inv_sr;
+  double R_roe = (srR * Rrr + srL * Rl) * inv_sr;
+  double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  // species loop (one species); the leading 0 + of each accumulation is exact
+  double invW = t.R;
+  double hl = t.cp * Tl;
+  double hr = t.cp * Tr;
+  double el = hl - invW * Tl;
+  double er = hr - invW * Tr;
+  h0l = hl * L.d * inv_dltot;
+  h0r = hr * Rr.d * inv_drtot;
+  double d_roe = (srR * Rr.d * inv_drtot + srL * L.d * inv_dltot) * inv_sr;
+  double cv_roe = d_roe * (0.5 * (t.cp + t.cp) - invW);
+  double sum_ei = d_roe * (srR * er + srL * el) * inv_sr;
+  h0l = h0l + 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w);
+  h0r = h0r + 0.5 * (Rr.u * Rr.u + Rr.v * Rr.v + Rr.w * Rr.w);
+  h0_roe = (srR * h0r + srL * h0l) * inv_sr;
+  double gam_roe = 1.0 + R_roe / cv_roe;
+  double vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
+  a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+}
+
+// riemann_HLLC (Batten), Lib_Riemann_HLL.f90:147-258
+inline RFlux riemann_HLLC(const Thermo& t, const RState& L, const RState& R, double nx,
+                          double ny, double nz) {
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe;
+  roe_averages(t, L, R, h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe);
+  double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  double e0l = h0l - L.p / L.rho;
+  double e0r = h0r - R.p / R.rho;
+  double S1 = std::min(std::min(0.0, unl - L.a), un_roe - a_roe);
+  double S4 = std::max(std::max(0.0, unr + R.a), un_roe + a_roe);
+  double inv_denom = 1.0 / (L.rho * (S1 - unl) - R.rho * (S4 - unr));
+  double Sstar = (R.p - L.p + L.rho * unl * (S1 - unl) - R.rho * unr * (S4 - unr)) * inv_denom;
+  double pstar = L.rho * (unl - S1) * (unl - Sstar) + L.p;
+  if (S1 >= 0.0) {
+    F.r = L.rho * unl;
+    F.u = F.r * L.u + L.p * nx;
+    F.v = F.r * L.v + L.p * ny;
+    F.w = F.r * L.w + L.p * nz;
+    F.E = F.r * h0l;
+  } else if (Sstar >= 0.0) {
+    F.r = L.rho * unl;
+    F.u = F.r * L.u + L.p * nx;
+    F.v = F.r * L.v + L.p * ny;
+    F.w = F.r * L.w + L.p * nz;
+    F.E = F.r * h0l;
+    inv_denom = 1.0 / (S1 - Sstar);
+    double U1S = L.rho * (S1 - unl) * inv_denom;
+    double U2S = ((S1 - unl) * L.rho * L.u + (pstar - L.p) * nx) * inv_denom;
+    double U3S = ((S1 - unl) * L.rho * L.v + (pstar - L.p) * ny) * inv_denom;
+    double U4S = ((S1 - unl) * L.rho * L.w + (pstar - L.p) * nz) * inv_denom;
+    double U5S = ((S1 - unl) * L.rho * e0l - L.p * unl + pstar * Sstar) * inv_denom;
+    F.r = F.r + S1 * (U1S - L.rho);
+    F.u = F.u + S1 * (U2S - L.rho * L.u);
+    F.v = F.v + S1 * (U3S - L.rho * L.v);
+    F.w = F.w + S1 * (U4S - L.rho * L.w);
+    F.E = F.E + S1 * (U5S - L.rho * e0l);
+  } else if (S4 > 0.0) {
+    F.r = R.rho * unr;
+    F.u = F.r * R.u + R.p * nx;
+    F.v = F.r * R.v + R.p * ny;
+    F.w = F.r * R.w + R.p * nz;
+    F.E = F.r * h0r;
+    inv_denom = 1.0 / (S4 - Sstar);
+    double U1S = R.rho * (S4 - unr) * inv_denom;
+    double U2S = ((S4 - unr) * R.rho * R.u + (pstar - R.p) * nx) * inv_denom;
+    double U3S = ((S4 - unr) * R.rho * R.v + (pstar - R.p) * ny) * inv_denom;
+    double U4S = ((S4 - unr) * R.rho * R.w + (pstar - R.p) * nz) * inv_denom;
+    double U5S = ((S4 - unr) * R.rho * e0r - R.p * unr + pstar * Sstar) * inv_denom;
+    F.r = F.r + S4 * (U1S - R.rho);
+    F.u = F.u + S4 * (U2S - R.rho * R.u);
+    F.v = F.v + S4 * (U3S - R.rho * R.v);
+    F.w = F.w + S4 * (U4S - R.rho * R.w);
+    F.E = F.E + S4 * (U5S - R.rho * e0r);
+  } else {
+    F.r = R.rho * unr;
+    F.u = F.r * R.u + R.p * nx;
+    F.v = F.r * R.v + R.p * ny;
+    F.w = F.r * R.w + R.p * nz;
+    F.E = F.r * h0r;
+  }
+  return F;
+}
+
+// riemann_AUSMp, Lib_Riemann_AUSM.f90:150-238
+inline RFlux riemann_AUSMp(const Thermo& t, const RState& L, const RState& R, double nx,
+                           double ny, double nz) {
+  const double beta = 0.125, alpha = 0.1875;
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double H_L = H0(t, L.p, L.d, std::sqrt(L.u * L.u + L.v * L.v + L.w * L.w));
+  double H_R = H0(t, R.p, R.d, std::sqrt(R.u * R.u + R.v * R.v + R.w * R.w));
+  double a_half = std::sqrt(L.a * R.a);
+  double ML = unl / a_half;
+  double MR = unr / a_half;
+  double MplusL, pplusL, MminusR, pminusR;
+  if (std::fabs(ML) < 1.0) {
+    MplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) + beta * ((ML * ML - 1.0) * (ML * ML - 1.0));
+    pplusL = 0.25 * ((ML + 1.0) * (ML + 1.0)) * (2.0 - ML) + alpha * ML * ((ML * ML - 1.0) * (ML * ML - 1.0));
+  } else {
+    MplusL = 0.5 * (ML + std::fabs(ML));
+    pplusL = 0.5 * (1.0 + std::copysign(1.0, ML));
+  }
+  if (std::fabs(MR) < 1.0) {
+    MminusR = -(0.25 * ((MR - 1.0) * (MR - 1.0))) - beta * ((MR * MR - 1.0) * (MR * MR - 1.0));
+    pminusR = 0.25 * ((MR - 1.0) * (MR - 1.0)) * (2.0 + MR) - alpha * MR * ((MR * MR - 1.0) * (MR * MR - 1.0));
+  } else {
+    MminusR = 0.5 * (MR - std::fabs(MR));
+    pminusR = 0.5 * (1.0 - std::copysign(1.0, MR));
+  }
+  double Mhalf = MplusL + MminusR;
+  double phalf = pplusL * L.p + pminusR * R.p;
+  double mdotp = L.rho * a_half * 0.5 * (Mhalf + std::fabs(Mhalf));
+  double mdotm = R.rho * a_half * 0.5 * (Mhalf - std::fabs(Mhalf));
+  F.r = mdotp + mdotm;
+  F.u = mdotp * L.u + mdotm * R.u + nx * phalf;
+  F.v = mdotp * L.v + mdotm * R.v + ny * phalf;
+  F.w = mdotp * L.w + mdotm * R.w + nz * phalf;
+  F.E = mdotp * H_L + mdotm * H_R;
+  return F;
+}
+
+// riemann_SLAU / SLAU2, Lib_Riemann_SLAU.f90:19-141
+inline RFlux riemann_SLAU(const Thermo& t, const RState& L, const RState& R, double nx,
+                          double ny, double nz, bool slau2) {
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double sq_veli = L.u * L.u + L.v * L.v + L.w * L.w;
+  double sq_velj = R.u * R.u + R.v * R.v + R.w * R.w;
+  double aF = 0.5 * (L.a + R.a);
+  double mL = unl / aF;
+  double mR = unr / aF;
+  double Mach_tilde = std::min(1.0, std::sqrt(0.5 * (sq_veli + sq_velj)) / aF);
+  double Chi = (1.0 - Mach_tilde) * (1.0 - Mach_tilde);
+  double Vn_mag = (L.rho * std::fabs(unl) + R.rho * std::fabs(unr)) / (L.rho + R.rho);
+  double f_rho = -std::max(std::min(mL, 0.0), -1.0) * std::min(std::max(mR, 0.0), 1.0);
+  double Vn_magL = (1.0 - f_rho) * Vn_mag + f_rho * std::fabs(unl);
+  double Vn_magR = (1.0 - f_rho) * Vn_mag + f_rho * std::fabs(unr);
+  F.r = 0.5 * (L.rho * (unl + Vn_magL) + R.rho * (unr - Vn_magR) - (Chi / aF) * (R.p - L.p));
+  double BetaL, BetaR;
+  if (std::fabs(mL) < 1.0) BetaL = 0.25 * (2.0 - mL) * ((mL + 1.0) * (mL + 1.0));
+  else if (mL >= 0.0) BetaL = 1.0;
+  else BetaL = 0.0;
+  if (std::fabs(mR) < 1.0) BetaR = 0.25 * (2.0 + mR) * ((mR - 1.0) * (mR - 1.0));
+  else if (mR >= 0.0) BetaR = 0.0;
+  else BetaR = 1.0;
+  double p_half;
+  if (!slau2) {
+    p_half = 0.5 * (L.p + R.p) + 0.5 * (BetaL - BetaR) * (L.p - R.p) +
+             (1.0 - Chi) * (BetaL + BetaR - 1.0) * 0.5 * (L.p + R.p);
+  } else {
+    p_half = 0.5 * (L.p + R.p) + 0.5 * (BetaL - BetaR) * (L.p - R.p) +
+             std::sqrt(0.5 * (sq_veli + sq_velj)) * (BetaL + BetaR - 1.0) * aF * 0.5 * (L.rho + R.rho);
+  }
+  double H_L = H0(t, L.p, L.d, std::sqrt(sq_veli));
+  double H_R = H0(t, R.p, R.d, std::sqrt(sq_velj));
+  if (F.r >= 0.0) {
+    F.u = F.r * L.u + nx * p_half;
+    F.v = F.r * L.v + ny * p_half;
+    F.w = F.r * L.w + nz * p_half;
+    F.E = F.r * H_L;
+  } else {
+    F.u = F.r * R.u + nx * p_half;
+    F.v = F.r * R.v + ny * p_half;
+    F.w = F.r * R.w + nz * p_half;
+    F.E = F.r * H_R;
+  }
+  return F;
+}
+
+inline RFlux Riemann(const orc_domain* d, const RState& L, const RState& R, double nx,
+                     double ny, double nz) {
+  switch (d->cfg.riemann) {
+    case ORC_RIE_AUSMP: return riemann_AUSMp(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_SLAU: return riemann_SLAU(d->th, L, R, nx, ny, nz, false);
+    case ORC_RIE_SLAU2: return riemann_SLAU(d->th, L, R, nx, ny, nz, true);
+    default: return riemann_HLLC(d->th, L, R, nx, ny, nz);
+  }
+}
+
+inline RState make_state(const Thermo& t, const double* P, bool& bad) {
+  // check_gas_state, co_rotot_Rtot and f_ss as in Lib_Convective.f90:45-58
+  RState s;
+  if (check_gas_state(P[0], P[NP]) != 0) bad = true;
+  double rho, R;
+  co_rotot_Rtot(t, P[0], rho, R);
+  s.d = P[0]; s.u = P[NU]; s.v = P[NV]; s.w = P[NW]; s.p = P[NP];
+  s.rho = rho;
+  s.a = f_ss(t, P[0], P[NP], rho, R);
+  return s;
+}
+
+// Reconstruction (elemental), Lib_Reconstruction.f90:10-29, beta = 1
+inline void Reconstruction(int lim, const double* prev, const double* local, const double* next,
+                           const double* next2, double dl0, double dl1, double dl2, double dll,
+                           double dlr, double beta, double* priml, double* primr) {
+  for (int v = 0; v < NPRIM; ++v) {
+    double slope0 = (local[v] - prev[v]) / dl0;
+    double slope1 = (next[v] - local[v]) / dl1;
+    double slope2 = (next2[v] - next[v]) / dl2;
+    double slopel = rlimiter(lim, slope1, slope0);
+    double sloper = rlimiter(lim, slope2, slope1);
+    priml[v] = local[v] + beta * slopel * dll;
+    primr[v] = next[v] - beta * sloper * dlr;
+  }
+}
+
+// Species-upwinded flux times area (Lib_Convective.f90:66-75 and the
+// identical block of Lib_BC_Fluxes_Connection.f90:95-105).
+inline void face_flux(const RFlux& F, double area, const double* p1, double rho1, const double* p4,
+                      double rho4, double* Flux) {
+  double su = std::copysign(0.5, F.r);
+  double sp = 0.5 + su;
+  double sm = su - 0.5;
+  Flux[0] = F.r * area * (sp * (p1[0] / rho1) - sm * (p4[0] / rho4));
+  Flux[NU] = F.u * area;
+  Flux[NV] = F.v * area;
+  Flux[NW] = F.w * area;
+  Flux[NP] = F.E * area;
+}
+
+// Convective_Flux, Lib_Convective.f90:10-85
+inline bool Convective_Flux(const orc_domain* d, const double* dl /*-1..2*/, const double* N,
+                            double area, const double* Pm1, const double* P0, const double* P1,
+                            const double* P2, double* R0, double* R1) {
+  double l0 = 0.5 * (dl[0] + dl[1]);
+  double l1 = 0.5 * (dl[1] + dl[2]);
+  double l2 = 0.5 * (dl[2] + dl[3]);
+  double lm = 0.5 * dl[1];
+  double lp = 0.5 * dl[2];
+  double Prim1[NPRIM], Prim4[NPRIM];
+  Reconstruction(d->cfg.limiter, Pm1, P0, P1, P2, l0, l1, l2, lm, lp, 1.0, Prim1, Prim4);
+  bool bad = false;
+  RState L = make_state(d->th, Prim1, bad);
+  RState R = make_state(d->th, Prim4, bad);
+  RFlux F = Riemann(d, L, R, N[0], N[1], N[2]);
+  double Flux[NPRIM];
+  face_flux(F, area, Prim1, L.rho, Prim4, R.rho, Flux);
+  for (int v = 0; v < NPRIM; ++v) R0[v] = R0[v] + Flux[v];
+  for (int v = 0; v < NPRIM; ++v) R1[v] = R1[v] - Flux[v];
+  return !bad;
+}
+
+// ---------------------------------------------------------------------------
+// Metrics: Lib_Metrics.f90
+// ---------------------------------------------------------------------------
+inline double tvol(const double* vx, const double* vy, const double* vz, int i1, int i2, int i3,
+                   int i4) {
+  --i1; --i2; --i3; --i4;
+  return std::fabs(((vx[i2] - vx[i1]) * ((vy[i3] - vy[i1]) * (vz[i4] - vz[i1]) - (vy[i4] - vy[i1]) * (vz[i3] - vz[i1])) +
+                    (vy[i2] - vy[i1]) * ((vx[i4] - vx[i1]) * (vz[i3] - vz[i1]) - (vx[i3] - vx[i1]) * (vz[i4] - vz[i1])) +
+                    (vz[i2] - vz[i1]) * ((vx[i3] - vx[i1]) * (vy[i4] - vy[i1]) - (vx[i4] - vx[i1]) * (vy[i3] - vy[i1]))) /
+                   6.0);
+}
+
+// Compute_Metric_Tensor, Lib_Metrics.f90:250-376.  Mout: c(3,3) column-major.
+inline bool Compute_Metric_Tensor(const Vec3& N1, const Vec3& N2, const Vec3& N3, const Vec3& N4,
+                                  const Vec3& N5, const Vec3& N6, const Vec3& N7, const Vec3& N8,
+                                  double* Mout, double* dlout, double* volout) {
+  double A[3][3];
+  for (int c = 0; c < 3; ++c) {
+    A[0][c] = N5.c[c] - N1.c[c] + N6.c[c] - N2.c[c] + N7.c[c] - N3.c[c] + N8.c[c] - N4.c[c];
+    A[1][c] = N3.c[c] - N1.c[c] + N4.c[c] - N2.c[c] + N7.c[c] - N5.c[c] + N8.c[c] - N6.c[c];
+    A[2][c] = N2.c[c] - N1.c[c] + N4.c[c] - N3.c[c] + N6.c[c] - N5.c[c] + N8.c[c] - N7.c[c];
+  }
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) A[r][c] = 0.25 * A[r][c];
+  double det = A[0][0] * A[1][1] * A[2][2] - A[0][0] * A[1][2] * A[2][1] -
+               A[0][1] * A[1][0] * A[2][2] + A[0][1] * A[1][2] * A[2][0] +
+               A[0][2] * A[1][0] * A[2][1] - A[0][2] * A[1][1] * A[2][0];
+  bool ok = true;
+  if (std::fabs(det) == 0.0) {
+    ok = false;
+    for (int q = 0; q < 9; ++q) Mout[q] = 0.0;
+    Mout[0] = Mout[4] = Mout[8] = 1.0;
+  } else {
+    double cof[3][3];
+    cof[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]);
+    cof[0][1] = -(A[1][0] * A[2][2] - A[1][2] * A[2][0]);
+    cof[0][2] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+    cof[1][0] = -(A[0][1] * A[2][2] - A[0][2] * A[2][1]);
+    cof[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]);
+    cof[1][2] = -(A[0][0] * A[2][1] - A[0][1] * A[2][0]);
+    cof[2][0] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]);
+    cof[2][1] = -(A[0][0] * A[1][2] - A[0][2] * A[1][0]);
+    cof[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) Mout[r + 3 * c] = cof[r][c] / det;
+  }
+  for (int h = 0; h < 3; ++h) dlout[h] = std::sqrt(A[h][0] * A[h][0] + A[h][1] * A[h][1] + A[h][2] * A[h][2]);
+  double vx[8], vy[8], vz[8];
+  const Vec3* order[8] = {&N1, &N5, &N3, &N7, &N2, &N6, &N4, &N8};
+  for (int q = 0; q < 8; ++q) { vx[q] = order[q]->c[0]; vy[q] = order[q]->c[1]; vz[q] = order[q]->c[2]; }
+  double v = tvol(vx, vy, vz, 1, 2, 3, 5) + tvol(vx, vy, vz, 2, 4, 3, 8) + tvol(vx, vy, vz, 5, 8, 6, 2) +
+             tvol(vx, vy, vz, 5, 7, 8, 3) + tvol(vx, vy, vz, 5, 8, 2, 3);
+  *volout = v;
+  if (v <= 0.0) ok = false;
+  return ok;
+}
+
+inline Vec3 sub(const Vec3& a, const Vec3& b) { return Vec3{{a.c[0] - b.c[0], a.c[1] - b.c[1], a.c[2] - b.c[2]}}; }
+inline Vec3 lin3(const Vec3& a, const Vec3& b, const Vec3& c) {   // 3a - 3b + c
+  Vec3 r;
+  for (int q = 0; q < 3; ++q) r.c[q] = 3.0 * a.c[q] - 3.0 * b.c[q] + c.c[q];
+  return r;
+}
+inline Vec3 lin2(const Vec3& a, const Vec3& b) {                  // 2a - b
+  Vec3 r;
+  for (int q = 0; q < 3; ++q) r.c[q] = 2.0 * a.c[q] - b.c[q];
+  return r;
+}
+
+bool cmt_store(Block& B, int i, int j, int k, const Vec3& N1, const Vec3& N2, const Vec3& N3,
+               const Vec3& N4, const Vec3& N5, const Vec3& N6, const Vec3& N7, const Vec3& N8) {
+  return Compute_Metric_Tensor(N1, N2, N3, N4, N5, N6, N7, N8, &B.M[9 * B.cell(i, j, k)],
+                               &B.dl[3 * B.cell(i, j, k)], &B.vol[B.cell(i, j, k)]);
+}
+
+// Compute_Norm_Area, Lib_Metrics.f90:69-247
+void Compute_Norm_Area(Block& b) {
+  int im = b.ni, jm = b.nj, km = b.nk;
+  auto cross = [](const Vec3& d1, const Vec3& d2, double* d3) {
+    d3[0] = (d1.c[1] * d2.c[2] - d1.c[2] * d2.c[1]);
+    d3[1] = (d1.c[2] * d2.c[0] - d1.c[0] * d2.c[2]);
+    d3[2] = (d1.c[0] * d2.c[1] - d1.c[1] * d2.c[0]);
+  };
+  auto avg4 = [](const Vec3& a, const Vec3& bb, const Vec3& c, const Vec3& d) {
+    Vec3 r;
+    for (int q = 0; q < 3; ++q) r.c[q] = 0.25 * (a.c[q] + bb.c[q] + c.c[q] + d.c[q]);
+    return r;
+  };
+  double d3[3], sn[3];
+  // i direction sign
+  cross(sub(b.nd(1, 1, 1), b.nd(1, 0, 0)), sub(b.nd(1, 0, 1), b.nd(1, 1, 0)), sn);
+  Vec3 c1 = avg4(b.nd(1, 1, 1), b.nd(1, 0, 1), b.nd(1, 0, 0), b.nd(1, 1, 0));
+  Vec3 c2 = avg4(b.nd(0, 1, 1), b.nd(0, 0, 1), b.nd(0, 0, 0), b.nd(0, 1, 0));
+  Vec3 dd = sub(c1, c2);
+  double signi = std::copysign(1.0, dd.c[0] * sn[0] + dd.c[1] * sn[1] + dd.c[2] * sn[2]);
+  // j direction sign
+  cross(sub(b.nd(0, 1, 1), b.nd(1, 1, 0)), sub(b.nd(1, 1, 1), b.nd(0, 1, 0)), sn);
+  c1 = avg4(b.nd(1, 1, 1), b.nd(0, 1, 1), b.nd(0, 1, 0), b.nd(1, 1, 0));
+  c2 = avg4(b.nd(1, 0, 1), b.nd(0, 0, 1), b.nd(0, 0, 0), b.nd(1, 0, 0));
+  dd = sub(c1, c2);
+  double signj = std::copysign(1.0, dd.c[0] * sn[0] + dd.c[1] * sn[1] + dd.c[2] * sn[2]);
+  // k direction sign
+  cross(sub(b.nd(0, 1, 1), b.nd(1, 0, 1)), sub(b.nd(0, 0, 1), b.nd(1, 1, 1)), sn);
+  c1 = avg4(b.nd(1, 1, 1), b.nd(0, 1, 1), b.nd(0, 0, 1), b.nd(1, 0, 1));
+  c2 = avg4(b.nd(1, 1, 0), b.nd(0, 1, 0), b.nd(0, 0, 0), b.nd(1, 0, 0));
+  dd = sub(c1, c2);
+  double signk = std::copysign(1.0, dd.c[0] * sn[0] + dd.c[1] * sn[1] + dd.c[2] * sn[2]);
+
+  auto store = [&](int dir, size_t f, double sgn) {
+    for (int q = 0; q < 3; ++q) d3[q] = d3[q] * 0.5;
+    double A = std::sqrt(d3[0] * d3[0] + d3[1] * d3[1] + d3[2] * d3[2]);
+    double n[3];
+    if (A == 0.0) { n[0] = n[1] = n[2] = 0.0; }
+    else for (int q = 0; q < 3; ++q) n[q] = d3[q] / A * sgn;
+    b.fA[dir][f] = A;
+    for (int q = 0; q < 3; ++q) b.fN[dir][3 * f + q] = n[q];
+  };
+  for (int k = 1; k <= km; ++k)
+    for (int j = 1; j <= jm; ++j)
+      for (int i = 0; i <= im; ++i) {
+        cross(sub(b.nd(i, j, k), b.nd(i, j - 1, k - 1)), sub(b.nd(i, j - 1, k), b.nd(i, j, k - 1)), d3);
+        store(0, b.face(1, i, j, k), signi);
+      }
+  for (int k = 1; k <= km; ++k)
+    for (int j = 0; j <= jm; ++j)
+      for (int i = 1; i <= im; ++i) {
+        cross(sub(b.nd(i - 1, j, k), b.nd(i, j, k - 1)), sub(b.nd(i, j, k), b.nd(i - 1, j, k - 1)), d3);
+        store(1, b.face(2, i, j, k), signj);
+      }
+  for (int k = 0; k <= km; ++k)
+    for (int j = 1; j <= jm; ++j)
+      for (int i = 1; i <= im; ++i) {
+        cross(sub(b.nd(i - 1, j, k), b.nd(i, j - 1, k)), sub(b.nd(i - 1, j - 1, k), b.nd(i, j, k)), d3);
+        store(2, b.face(3, i, j, k), signk);
+      }
+}
+
+// BC_Extrapolate_Metrics, Lib_Metrics.f90:535-797 (delthe == 0 branches)
+bool BC_Extrapolate_Metrics(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& b) {
+  const int gc = GC;
+  Vec3 N[8][2 * GC + 1];   // N[q][g + gc], q = 0..7 for N1..N8
+  auto at = [&](int q, int g) -> Vec3& { return N[q][g + gc]; };
+  bool ok = true;
+  switch (Fm) {
+    case 1:
+      for (int g = 0; g <= gc; ++g) {
+        at(0, g) = b.nd(Im + g - 1, Jm - 1, Km - 1);
+        at(1, g) = b.nd(Im + g - 1, Jm - 1, Km);
+        at(2, g) = b.nd(Im + g - 1, Jm, Km - 1);
+        at(3, g) = b.nd(Im + g - 1, Jm, Km);
+      }
+      for (int g = -1; g >= -gc; --g) {
+        for (int q = 0; q < 4; ++q) at(q, g) = lin3(at(q, g + 1), at(q, g + 2), at(q, g + 3));
+        ok &= cmt_store(b, Im + g, Jm, Km, at(0, g), at(1, g), at(2, g), at(3, g), at(0, g + 1), at(1, g + 1),
+                        at(2, g + 1), at(3, g + 1));
+      }
+      break;
+    case 2:
+      for (int g = 0; g >= -gc; --g) {
+        at(4, g) = b.nd(Im + g, Jm - 1, Km - 1);
+        at(5, g) = b.nd(Im + g, Jm - 1, Km);
+        at(6, g) = b.nd(Im + g, Jm, Km - 1);
+        at(7, g) = b.nd(Im + g, Jm, Km);
+      }
+      for (int g = 1; g <= gc; ++g) {
+        for (int q = 4; q < 8; ++q) at(q, g) = lin3(at(q, g - 1), at(q, g - 2), at(q, g - 3));
+        ok &= cmt_store(b, Im + g, Jm, Km, at(4, g - 1), at(5, g - 1), at(6, g - 1), at(7, g - 1), at(4, g), at(5, g),
+                        at(6, g), at(7, g));
+      }
+      break;
+    case 3: {
+      bool cubic = b.nj > 2;
+      int gtop = cubic ? gc : 1;
+      for (int g = 0; g <= gtop; ++g) {
+        at(0, g) = b.nd(Im - 1, Jm + g - 1, Km - 1);
+        at(1, g) = b.nd(Im - 1, Jm + g - 1, Km);
+        at(4, g) = b.nd(Im, Jm + g - 1, Km - 1);
+        at(5, g) = b.nd(Im, Jm + g - 1, Km);
+      }
+      for (int g = -1; g >= -gc; --g) {
+        for (int q : {0, 1, 4, 5})
+          at(q, g) = cubic ? lin3(at(q, g + 1), at(q, g + 2), at(q, g + 3)) : lin2(at(q, g + 1), at(q, g + 2));
+        ok &= cmt_store(b, Im, Jm + g, Km, at(0, g), at(1, g), at(0, g + 1), at(1, g + 1), at(4, g), at(5, g),
+                        at(4, g + 1), at(5, g + 1));
+      }
+      break;
+    }
+    case 4: {
+      bool cubic = b.nj > 2;
+      int gbot = cubic ? -gc : -1;
+      for (int g = 0; g >= gbot; --g) {
+        at(2, g) = b.nd(Im - 1, Jm + g, Km - 1);
+        at(3, g) = b.nd(Im - 1, Jm + g, Km);
+        at(6, g) = b.nd(Im, Jm + g, Km - 1);
+        at(7, g) = b.nd(Im, Jm + g, Km);
+      }
+      for (int g = 1; g <= gc; ++g) {
+        for (int q : {2, 3, 6, 7})
+          at(q, g) = cubic ? lin3(at(q, g - 1), at(q, g - 2), at(q, g - 3)) : lin2(at(q, g - 1), at(q, g - 2));
+        ok &= cmt_store(b, Im, Jm + g, Km, at(2, g - 1), at(3, g - 1), at(2, g), at(3, g), at(6, g - 1), at(7, g - 1),
+                        at(6, g), at(7, g));
+      }
+      break;
+    }
+    case 5: {
+      bool cubic = (D->ndir == 3);
+      int gtop = cubic ? gc : 1;
+      for (int g = 0; g <= gtop; ++g) {
+        at(0, g) = b.nd(Im - 1, Jm - 1, Km + g - 1);
+        at(2, g) = b.nd(Im - 1, Jm, Km + g - 1);
+        at(4, g) = b.nd(Im, Jm - 1, Km + g - 1);
+        at(6, g) = b.nd(Im, Jm, Km + g - 1);
+      }
+      for (int g = -1; g >= -gc; --g) {
+        for (int q : {0, 2, 4, 6})
+          at(q, g) = cubic ? lin3(at(q, g + 1), at(q, g + 2), at(q, g + 3)) : lin2(at(q, g + 1), at(q, g + 2));
+        ok &= cmt_store(b, Im, Jm, Km + g, at(0, g), at(0, g + 1), at(2, g), at(2, g + 1), at(4, g), at(4, g + 1),
+                        at(6, g), at(6, g + 1));
+      }
+      break;
+    }
+    case 6: {
+      bool cubic = (D->ndir == 3);
+      int gbot = cubic ? -gc : -1;
+      for (int g = 0; g >= gbot; --g) {
+        at(1, g) = b.nd(Im - 1, Jm - 1, Km + g);
+        at(3, g) = b.nd(Im - 1, Jm, Km + g);
+        at(5, g) = b.nd(Im, Jm - 1, Km + g);
+        at(7, g) = b.nd(Im, Jm, Km + g);
+      }
+      for (int g = 1; g <= gc; ++g) {
+        for (int q : {1, 3, 5, 7})
+          at(q, g) = cubic ? lin3(at(q, g - 1), at(q, g - 2), at(q, g - 3)) : lin2(at(q, g - 1), at(q, g - 2));
+        ok &= cmt_store(b, Im, Jm, Km + g, at(1, g - 1), at(1, g), at(3, g - 1), at(3, g), at(5, g - 1), at(5, g),
+                        at(7, g - 1), at(7, g));
+      }
+      break;
+    }
+  }
+  return ok;
+}
+
+// BC_Symmetry_Metrics, Lib_Metrics.f90:800-857
+void BC_Symmetry_Metrics(int Im, int Jm, int Km, int Fm, Block& b) {
+  for (int g = 1; g <= GC; ++g) {
+    int gi = Im, gj = Jm, gk = Km, si = Im, sj = Jm, sk = Km;
+    switch (Fm) {
+      case 1: gi = Im - g; si = Im + g - 1; break;
+      case 2: gi = Im + g; si = Im - g + 1; break;
+      case 3: gj = Jm - g; sj = Jm + g - 1; break;
+      case 4: gj = Jm + g; sj = Jm - g + 1; break;
+      case 5: gk = Km - g; sk = Km + g - 1; break;
+      case 6: gk = Km + g; sk = Km - g + 1; break;
+    }
+    size_t dst = b.cell(gi, gj, gk), src = b.cell(si, sj, sk);
+    for (int q = 0; q < 9; ++q) b.M[9 * dst + q] = b.M[9 * src + q];
+    for (int q = 0; q < 3; ++q) b.dl[3 * dst + q] = b.dl[3 * src + q];
+    b.vol[dst] = b.vol[src];
+  }
+}
+
+// BC_Connect_Metrics, Lib_Metrics.f90:860-1092
+bool BC_Connect_Metrics(int Im, int Jm, int Km, int Fm, Block& bm, int Is, int Js, int Ks, int Fs,
+                        const Block& bs, int d11s, int d12s, int d21s, int d22s) {
+  const int guides[6][3] = {{0, 0, 0}, {-1, 0, 0}, {0, 0, 0}, {0, -1, 0}, {0, 0, 0}, {0, 0, -1}};
+  const int guides2[6][3] = {{1, 0, 0}, {-2, 0, 0}, {0, 1, 0}, {0, -2, 0}, {0, 0, 1}, {0, 0, -2}};
+  Vec3 N[8][GC + 1];
+  switch (Fm) {
+    case 1: N[0][0] = bm.nd(Im - 1, Jm - 1, Km - 1); N[1][0] = bm.nd(Im - 1, Jm - 1, Km);
+            N[2][0] = bm.nd(Im - 1, Jm, Km - 1); N[3][0] = bm.nd(Im - 1, Jm, Km); break;
+    case 2: N[4][0] = bm.nd(Im, Jm - 1, Km - 1); N[5][0] = bm.nd(Im, Jm - 1, Km);
+            N[6][0] = bm.nd(Im, Jm, Km - 1); N[7][0] = bm.nd(Im, Jm, Km); break;
+    case 3: N[0][0] = bm.nd(Im - 1, Jm - 1, Km - 1); N[1][0] = bm.nd(Im - 1, Jm - 1, Km);
+            N[4][0] = bm.nd(Im, Jm - 1, Km - 1); N[5][0] = bm.nd(Im, Jm - 1, Km); break;
+    case 4: N[2][0] = bm.nd(Im - 1, Jm, Km - 1); N[3][0] = bm.nd(Im - 1, Jm, Km);
+            N[6][0] = bm.nd(Im, Jm, Km - 1); N[7][0] = bm.nd(Im, Jm, Km); break;
+    case 5: N[0][0] = bm.nd(Im - 1, Jm - 1, Km - 1); N[2][0] = bm.nd(Im - 1, Jm, Km - 1);
+            N[4][0] = bm.nd(Im, Jm - 1, Km - 1); N[6][0] = bm.nd(Im, Jm, Km - 1); break;
+    case 6: N[1][0] = bm.nd(Im - 1, Jm - 1, Km); N[3][0] = bm.nd(Im - 1, Jm, Km);
+            N[5][0] = bm.nd(Im, Jm - 1, Km); N[7][0] = bm.nd(Im, Jm, Km); break;
+  }
+  bool ok = true;
+  for (int g = 1; g <= GC; ++g) {
+    int Is1 = Is + (GC - g) * guides[Fs - 1][0] + (g - 1) * guides2[Fs - 1][0];
+    int Js1 = Js + (GC - g) * guides[Fs - 1][1] + (g - 1) * guides2[Fs - 1][1];
+    int Ks1 = Ks + (GC - g) * guides[Fs - 1][2] + (g - 1) * guides2[Fs - 1][2];
+    int II, JJ, KK;
+    if (Fs <= 2) { II = Is1; JJ = (2 * Js1 + d11s + d21s) / 2; KK = (2 * Ks1 + d12s + d22s) / 2; }
+    else if (Fs <= 4) { II = (2 * Is1 + d11s + d21s) / 2; JJ = Js1; KK = (2 * Ks1 + d12s + d22s) / 2; }
+    else { II = (2 * Is1 + d11s + d21s) / 2; JJ = (2 * Js1 + d12s + d22s) / 2; KK = Ks1; }
+    const int slotA[6] = {3, 7, 5, 7, 6, 7};   // N4, N8, N6, N8, N7, N8
+    N[slotA[Fm - 1]][g] = bs.nd(II, JJ, KK);
+    int III, JJJ, KKK;
+    if (Fs <= 2) { III = II; JJJ = JJ - d11s; KKK = KK - d12s; }
+    else if (Fs <= 4) { III = II - d11s; JJJ = JJ; KKK = KK - d12s; }
+    else { III = II - d11s; JJJ = JJ - d12s; KKK = KK; }
+    const int slotB[6] = {1, 5, 1, 3, 2, 3};   // N2, N6, N2, N4, N3, N4
+    N[slotB[Fm - 1]][g] = bs.nd(III, JJJ, KKK);
+    if (Fs <= 2) { III = II; JJJ = JJ - d21s; KKK = KK - d22s; }
+    else if (Fs <= 4) { III = II - d21s; JJJ = JJ; KKK = KK - d22s; }
+    else { III = II - d21s; JJJ = JJ - d22s; KKK = KK; }
+    const int slotC[6] = {2, 6, 4, 6, 4, 5};   // N3, N7, N5, N7, N5, N6
+    N[slotC[Fm - 1]][g] = bs.nd(III, JJJ, KKK);
+    if (Fs <= 2) { III = II; JJJ = JJ - d11s - d21s; KKK = KK - d12s - d22s; }
+    else if (Fs <= 4) { III = II - d11s - d21s; JJJ = JJ; KKK = KK - d12s - d22s; }
+    else { III = II - d11s - d21s; JJJ = JJ - d12s - d22s; KKK = KK; }
+    const int slotD[6] = {0, 4, 0, 2, 0, 1};   // N1, N5, N1, N3, N1, N2
+    N[slotD[Fm - 1]][g] = bs.nd(III, JJJ, KKK);
+    switch (Fm) {
+      case 1: ok &= cmt_store(bm, Im - g, Jm, Km, N[0][g], N[1][g], N[2][g], N[3][g], N[0][g - 1], N[1][g - 1], N[2][g - 1], N[3][g - 1]); break;
+      case 2: ok &= cmt_store(bm, Im + g, Jm, Km, N[4][g - 1], N[5][g - 1], N[6][g - 1], N[7][g - 1], N[4][g], N[5][g], N[6][g], N[7][g]); break;
+      case 3: ok &= cmt_store(bm, Im, Jm - g, Km, N[0][g], N[1][g], N[0][g - 1], N[1][g - 1], N[4][g], N[5][g], N[4][g - 1], N[5][g - 1]); break;
+      case 4: ok &= cmt_store(bm, Im, Jm + g, Km, N[2][g - 1], N[3][g - 1], N[2][g], N[3][g], N[6][g - 1], N[7][g - 1], N[6][g], N[7][g]); break;
+      case 5: ok &= cmt_store(bm, Im, Jm, Km - g, N[0][g], N[0][g - 1], N[2][g], N[2][g - 1], N[4][g], N[4][g - 1], N[6][g], N[6][g - 1]); break;
+      case 6: ok &= cmt_store(bm, Im, Jm, Km + g, N[1][g - 1], N[1][g], N[3][g - 1], N[3][g], N[5][g - 1], N[5][g], N[7][g - 1], N[7][g]); break;
+    }
+  }
+  return ok;
+}
+
+// Face_Index, Lib_BC_Fluxes.f90:22-45
+inline void Face_Index(int face, int ci, int cj, int ck, int& dir, int& fi, int& fj, int& fk) {
+  fi = ci; fj = cj; fk = ck;
+  if (face <= 2) { dir = 1; fi = ci - face % 2; }
+  else if (face <= 4) { dir = 2; fj = cj - face % 2; }
+  else { dir = 3; fk = ck - face % 2; }
+}
+
+// ---------------------------------------------------------------------------
+// Ghost cells: Lib_Ghost.f90
+// ---------------------------------------------------------------------------
+void Ghost_Connection(int Im, int Jm, int Km, int Fm, Block& bm, int Is, int Js, int Ks, int Fs,
+                      const Block& bs) {                     // :140-160
+  for (int g = 1; g <= GC; ++g) {
+    int Ig = Im - G(Fm, 1) * g, Jg = Jm - G(Fm, 2) * g, Kg = Km - G(Fm, 3) * g;
+    const double* src = &bs.P[NPRIM * bs.cell(Is + G(Fs, 1) * (g - 1), Js + G(Fs, 2) * (g - 1),
+                                              Ks + G(Fs, 3) * (g - 1))];
+    double* dst = bm.Pc(Ig, Jg, Kg);
+    for (int v = 0; v < NPRIM; ++v) dst[v] = src[v];
+  }
+}
+
+void Ghost_Symmetry(int Im, int Jm, int Km, int Fm, Block& b) {   // :193-225
+  int Ig = Im - G(Fm, 1), Jg = Jm - G(Fm, 2), Kg = Km - G(Fm, 3);
+  const double* normal;
+  if (Fm <= 2) normal = &b.fN[0][3 * b.face(1, Im - Fm % 2, Jm, Km)];
+  else if (Fm <= 4) normal = &b.fN[1][3 * b.face(2, Im, Jm - Fm % 2, Km)];
+  else normal = &b.fN[2][3 * b.face(3, Im, Jm, Km - Fm % 2)];
+  double* pm = b.Pc(Im, Jm, Km);
+  double* pg = b.Pc(Ig, Jg, Kg);
+  double vel[3] = {pm[NU], pm[NV], pm[NW]};
+  double udotn = dot3(vel, normal);
+  for (int q = 0; q < 3; ++q) vel[q] = vel[q] - 2.0 * udotn * normal[q];
+  pg[NU] = vel[0]; pg[NV] = vel[1]; pg[NW] = vel[2];
+  pg[0] = pm[0];
+  pg[NP] = pm[NP];
+}
+
+void Ghost_ZG_Extrapolate(int Im, int Jm, int Km, int Fm, Block& b) {   // :279-304
+  for (int g = 1; g <= GC; ++g) {
+    double* dst = nullptr;
+    switch (Fm) {
+      case 1: dst = b.Pc(Im - g, Jm, Km); break;
+      case 2: dst = b.Pc(Im + g, Jm, Km); break;
+      case 3: dst = b.Pc(Im, Jm - g, Km); break;
+      case 4: dst = b.Pc(Im, Jm + g, Km); break;
+      case 5: dst = b.Pc(Im, Jm, Km - g); break;
+      case 6: dst = b.Pc(Im, Jm, Km + g); break;
+    }
+    const double* src = b.Pc(Im, Jm, Km);
+    for (int v = 0; v < NPRIM; ++v) dst[v] = src[v];
+  }
+}
+
+void Ghost_Extrapolate(int Im, int Jm, int Km, int Fm, Block& b) {   // :363-402
+  for (int g = 1; g <= GC; ++g) {
+    int di = -G(Fm, 1), dj = -G(Fm, 2), dk = -G(Fm, 3);   // outward step
+    double* dst = b.Pc(Im + di * g, Jm + dj * g, Km + dk * g);
+    const double* a = b.Pc(Im + di * (g - 1), Jm + dj * (g - 1), Km + dk * (g - 1));
+    const double* c = b.Pc(Im + di * (g - 2), Jm + dj * (g - 2), Km + dk * (g - 2));
+    const double* e = b.Pc(Im + di * (g - 3), Jm + dj * (g - 3), Km + dk * (g - 3));
+    for (int v = 0; v < NPRIM; ++v) dst[v] = 3.0 * a[v] - 3.0 * c[v] + e[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Boundary fluxes
+// ---------------------------------------------------------------------------
+inline void compute_modfm(int fm, int& modfm, int& modfm1, int& modfm2) {   // Lib_BC_Fluxes.f90:9-19
+  modfm = fm % 2;
+  modfm1 = 1 - modfm;
+  modfm2 = 1 - 2 * modfm;
+}
+
+bool BC_Connection_Eul(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk) {
+  // Lib_BC_Fluxes_Connection.f90:13-114
+  int modfm, modfm1, modfm2, dir, fi, fj, fk;
+  compute_modfm(Fm, modfm, modfm1, modfm2);
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  int I1 = modfm * (Im - G(Fm, 1) * GC) + modfm1 * (Im + G(Fm, 1));
+  int J1 = modfm * (Jm - G(Fm, 2) * GC) + modfm1 * (Jm + G(Fm, 2));
+  int K1 = modfm * (Km - G(Fm, 3) * GC) + modfm1 * (Km + G(Fm, 3));
+  int I2 = modfm1 * Im + modfm * (Im - G(Fm, 1));
+  int J2 = modfm1 * Jm + modfm * (Jm - G(Fm, 2));
+  int K2 = modfm1 * Km + modfm * (Km - G(Fm, 3));
+  int I3 = modfm1 * (Im - G(Fm, 1)) + modfm * Im;
+  int J3 = modfm1 * (Jm - G(Fm, 2)) + modfm * Jm;
+  int K3 = modfm1 * (Km - G(Fm, 3)) + modfm * Km;
+  int I4 = modfm1 * (Im - G(Fm, 1) * GC) + modfm * (Im + G(Fm, 1));
+  int J4 = modfm1 * (Jm - G(Fm, 2) * GC) + modfm * (Jm + G(Fm, 2));
+  int K4 = modfm1 * (Km - G(Fm, 3) * GC) + modfm * (Km + G(Fm, 3));
+  const double* Prim1 = blk.Pc(I1, J1, K1);
+  const double* Prim2 = blk.Pc(I2, J2, K2);
+  const double* Prim3 = blk.Pc(I3, J3, K3);
+  const double* Prim4 = blk.Pc(I4, J4, K4);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  double Dl1 = blk.dl_(dir, I1, J1, K1) * 0.5;
+  double Dl2 = blk.dl_(dir, I2, J2, K2) * 0.5;
+  double Dl3 = blk.dl_(dir, I3, J3, K3) * 0.5;
+  double Dl4 = blk.dl_(dir, I4, J4, K4) * 0.5;
+  double Dist23 = Dl2 + Dl3;
+  double Dist12 = Dl1 + Dl2;
+  double Dist34 = Dl3 + Dl4;
+  double PL[NPRIM], PR[NPRIM];
+  Reconstruction(D->cfg.limiter, Prim1, Prim2, Prim3, Prim4, Dist12, Dist23, Dist34, Dl2, Dl3, 1.0, PL, PR);
+  bool bad = false;   // the connection flux does not call check_gas_state
+  RState L = make_state(D->th, PL, bad);
+  RState R = make_state(D->th, PR, bad);
+  RFlux F = Riemann(D, L, R, Normal[0], Normal[1], Normal[2]);
+  double su = std::copysign(0.5, F.r);
+  double sel_L = 0.5 + su, sel_R = su - 0.5;
+  double Fmass = F.r * Area;
+  double Flux[NPRIM];
+  Flux[0] = Fmass * (sel_L * PL[0] / L.rho - sel_R * PR[0] / R.rho);
+  Flux[NU] = F.u * Area;
+  Flux[NV] = F.v * Area;
+  Flux[NW] = F.w * Area;
+  Flux[NP] = F.E * Area;
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + Flux[v] * (double)modfm2;
+  return true;
+}
+
+void BC_Extrapolation(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk) {
+  // Lib_BC_Fluxes_Extrapolation.f90:13-47
+  int dir, fi, fj, fk;
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  const double* Prim = blk.Pc(Im, Jm, Km);
+  double vel[3] = {Prim[NU], Prim[NV], Prim[NW]};
+  double Un = dot3(vel, Normal);
+  double Flux[NPRIM];
+  Flux[0] = Prim[0] * Un * Area;
+  double Fmass = Flux[0];
+  for (int q = 0; q < 3; ++q) Flux[NU + q] = Fmass * vel[q] + Prim[NP] * Area * Normal[q];
+  Flux[NP] = Fmass * H0(D->th, Prim[NP], Prim[0], norm2(vel[0], vel[1], vel[2]));
+  int FluxSign = 1 - 2 * (Fm % 2);
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + (double)FluxSign * Flux[v];
+}
+
+void BC_Symmetry_Eul(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk) {
+  // Lib_BC_Fluxes_Symmetry.f90:14-125 (Un_wall = 0: no rotating frame)
+  int modfm, modfm1, modfm2, dir, fi, fj, fk;
+  compute_modfm(Fm, modfm, modfm1, modfm2);
+  int Ii = Im + G(Fm, 1), Ij = Jm + G(Fm, 2), Ik = Km + G(Fm, 3);
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const double* normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  double area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  double Bound_Dl = 0.5 * blk.dl_(dir, Im, Jm, Km);
+  double Int_Dl = 0.5 * blk.dl_(dir, Ii, Ij, Ik);
+  const double* Bound = blk.Pc(Im, Jm, Km);
+  const double* Int = blk.Pc(Ii, Ij, Ik);
+  double bvel[3] = {Bound[NU], Bound[NV], Bound[NW]};
+  double Un = dot3(bvel, normal);
+  double Ghost[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) Ghost[v] = Bound[v];
+  for (int q = 0; q < 3; ++q) Ghost[NU + q] = Ghost[NU + q] - 2.0 * Un * normal[q];
+  double fm = (double)modfm, fm1 = (double)modfm1;
+  double Prim1[NPRIM], Prim3[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) Prim1[v] = fm * Ghost[v] + fm1 * Int[v];
+  double Dist12 = 2.0 * Bound_Dl * fm + (Bound_Dl + Int_Dl) * fm1;
+  for (int v = 0; v < NPRIM; ++v) Prim3[v] = fm * Int[v] + fm1 * Ghost[v];
+  double Dist23 = (Bound_Dl + Int_Dl) * fm + 2.0 * Bound_Dl * fm1;
+  double Slope[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) {
+    double s32 = (Prim3[v] - Bound[v]) / Dist23;
+    double s21 = (Bound[v] - Prim1[v]) / Dist12;
+    Slope[v] = rlimiter(D->cfg.limiter, s32, s21);
+  }
+  double Dist = Bound_Dl * (double)modfm2;
+  double Face[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) Face[v] = Bound[v] + Slope[v] * Dist;
+  double rotot, Rtot;
+  co_rotot_Rtot(D->th, Face[0], rotot, Rtot);
+  double Sound = f_ss(D->th, Face[0], Face[NP], rotot, Rtot);
+  double fvel[3] = {Face[NU], Face[NV], Face[NW]};
+  Un = dot3(fvel, normal);
+  double Velt[3];
+  for (int q = 0; q < 3; ++q) Velt[q] = fvel[q] - Un * normal[q];
+  double Un1 = Un * (double)modfm2;
+  double U1[3], U4[3];
+  for (int q = 0; q < 3; ++q) { U1[q] = Un1 * normal[q] + Velt[q]; U4[q] = -Un1 * normal[q] + Velt[q]; }
+  RState L{Face[0], U1[0], U1[1], U1[2], Face[NP], Sound, rotot};
+  RState R{Face[0], U4[0], U4[1], U4[2], Face[NP], Sound, rotot};
+  RFlux F = Riemann(D, L, R, normal[0], normal[1], normal[2]);
+  double Flux[3] = {F.u * area, F.v * area, F.w * area};
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int q = 0; q < 3; ++q) r[NU + q] = r[NU + q] + (double)modfm2 * Flux[q];
+}
+
+// BC_Inlet_Supersonic_Static + Supersonic_Inflow, Lib_BC_Fluxes_Inflow.f90:244-382.
+// Returns false when BC_Sign*Un >= 0 (the caller falls back to symmetry).
+bool BC_Inlet_Supersonic(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk,
+                         const double* data) {
+  const Thermo& t = D->th;
+  double BC_Mach = data[0], BC_T0 = data[1], BC_p0 = data[2], BC_alpha = data[3],
+         BC_beta = data[4], BC_rel_fac = data[5];
+  int modfm, modfm1, modfm2, dir, fi, fj, fk;
+  compute_modfm(Fm, modfm, modfm1, modfm2);
+  int Ii = Im + G(Fm, 1), Ij = Jm + G(Fm, 2), Ik = Km + G(Fm, 3);
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const double* Prim2 = blk.Pc(Im, Jm, Km);
+  const double* Int = blk.Pc(Ii, Ij, Ik);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  double BC_Sign = (double)modfm2;
+  double vel2[3] = {Prim2[NU], Prim2[NV], Prim2[NW]};
+  double Un = dot3(vel2, Normal);
+  if (BC_Sign * Un >= 0.0) return false;
+  // Supersonic_Inflow
+  double flow_Rgas = t.R;
+  double flow_Sound = f_ss(t, Prim2[0], Prim2[NP], Prim2[0], flow_Rgas);
+  double flow_Mach = norm2(vel2[0], vel2[1], vel2[2]) / flow_Sound;
+  double BC_Mach_local = BC_rel_fac * BC_Mach + (1.0 - BC_rel_fac) * flow_Mach;
+  double BC_p0_local = BC_rel_fac * BC_p0 + (1.0 - BC_rel_fac) * Prim2[NP];
+  double alpha_eff = BC_alpha, beta_eff = BC_beta;   // Compute_Inflow_Direction :477-495
+  if (BC_alpha >= 0.5 * 1.7976931348623157e308) alpha_eff = std::atan(Normal[1] / (Normal[0] + 1e-20));
+  if (BC_beta >= 0.5 * 1.7976931348623157e308) beta_eff = std::atan(Normal[2] / (Normal[0] + 1e-20));
+  double Sup[NPRIM];
+  Sup[NP] = BC_p0_local;
+  double Sup_T = BC_T0;
+  double Sup_Rgas = 1.0 * t.R;                       // sum(BC_ci*Ri_Tab), ci = 1
+  double Sup_rho = Sup[NP] / (Sup_Rgas * Sup_T);
+  Sup[0] = Sup_rho * 1.0;
+  double Sup_Sound = f_ss(t, Sup[0], Sup[NP], Sup_rho, Sup_Rgas);
+  Sup[NU] = BC_Mach_local * Sup_Sound * std::cos(alpha_eff) * std::cos(beta_eff);
+  Sup[NV] = BC_Mach_local * Sup_Sound * std::sin(alpha_eff) * std::cos(beta_eff);
+  Sup[NW] = BC_Mach_local * Sup_Sound * std::sin(beta_eff);
+  double fm = (double)modfm, fm1 = (double)modfm1;
+  double Prim1[NPRIM], Prim3[NPRIM], Slope[NPRIM], Face[NPRIM], PL[NPRIM], PR[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) {
+    Prim1[v] = fm * Sup[v] + fm1 * Int[v];
+    Prim3[v] = fm * Int[v] + fm1 * Sup[v];
+  }
+  for (int v = 0; v < NPRIM; ++v) {
+    double d32 = Prim3[v] - Prim2[v];
+    double d21 = Prim2[v] - Prim1[v];
+    Slope[v] = rlimiter(D->cfg.limiter, d32, d21);
+  }
+  for (int v = 0; v < NPRIM; ++v) Face[v] = Prim2[v] + 0.5 * Slope[v] * (double)modfm2;
+  for (int v = 0; v < NPRIM; ++v) {
+    PL[v] = fm * Sup[v] + fm1 * Face[v];
+    PR[v] = fm * Face[v] + fm1 * Sup[v];
+  }
+  bool bad = false;
+  RState L = make_state(t, PL, bad);
+  RState R = make_state(t, PR, bad);
+  RFlux F = Riemann(D, L, R, Normal[0], Normal[1], Normal[2]);
+  double su = std::copysign(1.0, F.r);
+  double Sel_L = (1.0 + su) / 2.0, Sel_R = (su - 1.0) / 2.0;
+  double Fmass = F.r * Area;
+  double Flux[NPRIM];
+  Flux[0] = Fmass * (Sel_L * PL[0] / L.rho - Sel_R * PR[0] / R.rho);
+  Flux[NU] = F.u * Area;
+  Flux[NV] = F.v * Area;
+  Flux[NW] = F.w * Area;
+  Flux[NP] = F.E * Area;
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + (double)modfm2 * Flux[v];
+  return true;
+}
+
+// BC_Outflow + Outflow, Lib_BC_Fluxes_Outflow.f90:12-129.
+bool BC_Outflow(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const double* data) {
+  const Thermo& t = D->th;
+  double BC_pexit = data[0];
+  int modfm, modfm1, modfm2, dir, fi, fj, fk;
+  compute_modfm(Fm, modfm, modfm1, modfm2);
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const double* Bound = blk.Pc(Im, Jm, Km);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  double BC_Sign = (double)modfm2;
+  double bvel[3] = {Bound[NU], Bound[NV], Bound[NW]};
+  double Un = dot3(bvel, Normal);
+  if (BC_Sign * Un < 0.0) return false;
+  double Bound_rho, Bound_Rgas;
+  co_rotot_Rtot(t, Bound[0], Bound_rho, Bound_Rgas);
+  double Bound_Sound = f_ss(t, Bound[0], Bound[NP], Bound_rho, Bound_Rgas);
+  double Bound_Gamma = t.gamma;
+  double Riem = Bound_Sound + BC_Sign * 0.5 * (Bound_Gamma - 1.0) * Un;
+  double Vel_N[3], Vel_T[3];
+  for (int q = 0; q < 3; ++q) { Vel_N[q] = Un * Normal[q]; Vel_T[q] = bvel[q] - Vel_N[q]; }
+  double Mach_N = std::fabs(Un / Bound_Sound);
+  double Face[NPRIM], Face_Un, Face_Sound, Face_rho, Face_Rgas;
+  if (Mach_N < 1.0 && BC_pexit > 0.0) {
+    double p_exit = BC_pexit;
+    double delta = 0.5 * (Bound_Gamma - 1.0);
+    double den = 1.0 / std::pow(1.0 + delta, Bound_Gamma / (Bound_Gamma - 1.0));
+    double pstar = Bound[NP] * den * std::pow(1.0 + delta * (Mach_N * Mach_N), Bound_Gamma / (Bound_Gamma - 1.0));
+    if (pstar >= p_exit) p_exit = pstar;
+    double Isentropic = (Bound_Gamma - 1.0) / (2.0 * Bound_Gamma);
+    Face_Sound = Bound_Sound * std::pow(p_exit / Bound[NP], Isentropic);
+    Face_Un = (Riem - Face_Sound) / (BC_Sign * 0.5 * (Bound_Gamma - 1.0));
+    Face[NP] = p_exit;
+    Face_rho = Bound_Gamma * Face[NP] / (Face_Sound * Face_Sound);
+    Face[0] = Bound[0] / Bound_rho * Face_rho;
+    for (int q = 0; q < 3; ++q) Face[NU + q] = Vel_T[q] + Face_Un * Normal[q];
+    Face_Rgas = Bound_Rgas;
+  } else {
+    for (int v = 0; v < NPRIM; ++v) Face[v] = Bound[v];
+    Face_Un = Un;
+    Face_Sound = Bound_Sound;
+    Face_rho = Bound_rho;
+    Face_Rgas = Bound_Rgas;
+  }
+  (void)Face_Sound;
+  double Face_T = Face[NP] / (Face_Rgas * Face_rho);
+  double Face_Enthalpy = Face[0] / Face_rho * (t.cp * Face_T);
+  double Flux[NPRIM];
+  Flux[0] = Face[0] * Area * Face_Un;
+  double BC_mdot = Face_rho * Area * Face_Un;
+  for (int q = 0; q < 3; ++q) Flux[NU + q] = Face[NU + q] * BC_mdot + Face[NP] * Area * Normal[q];
+  Flux[NP] = BC_mdot * (0.5 * (Face[NU] * Face[NU] + Face[NV] * Face[NV] + Face[NW] * Face[NW]) + Face_Enthalpy);
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + (double)modfm2 * Flux[v];
+  return true;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C API
+// ===========================================================================
+extern "C" {
+
+orc_domain* orc_create(const orc_config* cfg, int nthreads) {
+  orc_domain* d = new orc_domain();
+  d->cfg = *cfg;
+  d->th.gamma = cfg->gamma;
+  d->th.R = cfg->rgas;
+  d->th.cp = cfg->gamma * cfg->rgas / (cfg->gamma - 1.0);
+  d->th.cv = cfg->rgas / (cfg->gamma - 1.0);
+  d->nthreads = nthreads > 0 ? nthreads : 1;
+  if (d->cfg.res_diter <= 0) d->cfg.res_diter = 1;
+  return d;
+}
+
+void orc_destroy(orc_domain* d) { delete d; }
+
+int orc_add_block(orc_domain* d, int ni, int nj, int nk, const double* node) {
+  if (ni < 1 || nj < 1 || nk < 1 || !node) return ORC_ERR_INVALID;
+  Block b;
+  b.ni = ni; b.nj = nj; b.nk = nk;
+  b.sx = ni + 2 * GC; b.sy = nj + 2 * GC; b.sz = nk + 2 * GC;
+  size_t nc = (size_t)b.sx * b.sy * b.sz;
+  b.node.assign(node, node + 3 * (size_t)(ni + 1) * (nj + 1) * (nk + 1));
+  b.P.assign(NPRIM * nc, 0.0);
+  b.PO.assign(NPRIM * nc, 0.0);
+  b.R.assign(NPRIM * nc, 0.0);
+  b.M.assign(9 * nc, 0.0);
+  b.dl.assign(3 * nc, 0.0);
+  b.vol.assign(nc, 0.0);
+  b.fN[0].assign(3 * (size_t)(ni + 1) * nj * nk, 0.0); b.fA[0].assign((size_t)(ni + 1) * nj * nk, 0.0);
+  b.fN[1].assign(3 * (size_t)ni * (nj + 1) * nk, 0.0); b.fA[1].assign((size_t)ni * (nj + 1) * nk, 0.0);
+  b.fN[2].assign(3 * (size_t)ni * nj * (nk + 1), 0.0); b.fA[2].assign((size_t)ni * nj * (nk + 1), 0.0);
+  b.dtlocal.assign((size_t)ni * nj * nk, 0.0);
+  b.beta.assign((size_t)ni * nj * nk, 1.0);
+  d->blk.push_back(std::move(b));
+  return ORC_OK;
+}
+
+int orc_set_bcs(orc_domain* d, const int32_t* rec, const double* data, int nbound) {
+  int nb = (int)d->blk.size();
+  size_t expect = 0;
+  for (auto& b : d->blk) expect += 2 * ((size_t)b.nj * b.nk + (size_t)b.ni * b.nk + (size_t)b.ni * b.nj);
+  if ((size_t)nbound != expect) return ORC_ERR_INVALID;                  // Check_BC, IO_BC.f90:123
+  d->bc.resize(nbound);
+  d->n_bf.assign(6 * nb, 0);
+  int lastkey = -1;
+  for (int q = 0; q < nbound; ++q) {
+    const int32_t* r = rec + 15 * (size_t)q;
+    BCrec& e = d->bc[q];
+    e.b = r[0]; e.i = r[1]; e.j = r[2]; e.k = r[3]; e.f = r[4]; e.type = r[5];
+    e.bs = r[6]; e.is = r[7]; e.js = r[8]; e.ks = r[9]; e.fs = r[10];
+    e.d11 = r[11]; e.d12 = r[12]; e.d21 = r[13]; e.d22 = r[14];
+    for (int c = 0; c < 6; ++c) e.data[c] = data ? data[6 * (size_t)q + c] : 0.0;
+    if (e.b < 1 || e.b > nb || e.f < 1 || e.f > 6) return ORC_ERR_INVALID;
+    int key = (e.b - 1) * 6 + (e.f - 1);
+    if (key < lastkey) return ORC_ERR_INVALID;     // BC_Fluxes relies on (block, face) order
+    lastkey = key;
+    d->n_bf[key] += 1;
+    switch (e.type) {
+      case 0: case 101: case 201: case 300: case 400: case 405: case 406: break;
+      default: return ORC_ERR_UNSUPPORTED;
+    }
+    if (e.type == 101 || e.type == 201) {
+      if (e.bs < 1 || e.bs > nb || e.fs < 1 || e.fs > 6) return ORC_ERR_INVALID;
+    }
+  }
+  return ORC_OK;
+}
+
+int orc_setup_metrics(orc_domain* d) {
+  if (d->blk.empty()) return ORC_ERR_INVALID;
+  // Check_Mesh_Type, Lib_Metrics.f90:13-66
+  Block& b1 = d->blk[0];
+  if (d->cfg.ndir > 0) d->ndir = d->cfg.ndir;
+  else if (b1.nk > 1) d->ndir = 3;
+  else if (b1.nj == 1) d->ndir = 1;
+  else d->ndir = 2;
+  d->delthe = 0.0;
+  if (d->ndir == 2 && b1.nj >= 1) {
+    Vec3 a = b1.nd(0, 1, 0), bb = b1.nd(0, 1, 1), c = b1.nd(0, b1.nj, 0), e = b1.nd(0, b1.nj, 1);
+    double t1 = std::atan2(bb.c[2], bb.c[1]) - std::atan2(a.c[2], a.c[1]);
+    double t2 = std::atan2(e.c[2], e.c[1]) - std::atan2(c.c[2], c.c[1]);
+    double r0 = std::sqrt(a.c[1] * a.c[1] + a.c[2] * a.c[2]);
+    double r1 = std::sqrt(bb.c[1] * bb.c[1] + bb.c[2] * bb.c[2]);
+    if ((t1 - t2) < 1e-5 && r0 > 1e-10 && std::fabs(r0 - r1) < 1e-5 * r0) d->delthe = t1;
+  }
+  if (d->delthe != 0.0) return ORC_ERR_UNSUPPORTED;   // axisymmetric meshes: out of scope
+  bool ok = true;
+  for (auto& b : d->blk) {
+    for (int k = 1; k <= b.nk; ++k)
+      for (int j = 1; j <= b.nj; ++j)
+        for (int i = 1; i <= b.ni; ++i)
+          ok &= cmt_store(b, i, j, k, b.nd(i - 1, j - 1, k - 1), b.nd(i - 1, j - 1, k), b.nd(i - 1, j, k - 1),
+                          b.nd(i - 1, j, k), b.nd(i, j - 1, k - 1), b.nd(i, j - 1, k), b.nd(i, j, k - 1),
+                          b.nd(i, j, k));
+    Compute_Norm_Area(b);
+  }
+  for (auto& e : d->bc) {
+    Block& bm = d->blk[e.b - 1];
+    switch (e.type) {
+      case 101:
+        ok &= BC_Connect_Metrics(e.i, e.j, e.k, e.f, bm, e.is, e.js, e.ks, e.fs, d->blk[e.bs - 1], e.d11, e.d12,
+                                 e.d21, e.d22);
+        break;
+      case 300: BC_Symmetry_Metrics(e.i, e.j, e.k, e.f, bm); break;
+      default: ok &= BC_Extrapolate_Metrics(d, e.i, e.j, e.k, e.f, bm); break;
+    }
+  }
+  return ok ? ORC_OK : ORC_ERR_METRICS;
+}
+
+static int check_block(const orc_domain* d, int b) {
+  return (b >= 1 && b <= (int)d->blk.size()) ? ORC_OK : ORC_ERR_INVALID;
+}
+
+int orc_set_prim(orc_domain* d, int b, const double* P) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  Block& B = d->blk[b - 1];
+  std::memcpy(B.P.data(), P, B.P.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_get_prim(const orc_domain* d, int b, double* P) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  const Block& B = d->blk[b - 1];
+  std::memcpy(P, B.P.data(), B.P.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_set_prim_old(orc_domain* d, int b, const double* PO) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  Block& B = d->blk[b - 1];
+  std::memcpy(B.PO.data(), PO, B.PO.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_get_residual(const orc_domain* d, int b, double* R) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  const Block& B = d->blk[b - 1];
+  std::memcpy(R, B.R.data(), B.R.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_get_dtlocal(const orc_domain* d, int b, double* dt) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  const Block& B = d->blk[b - 1];
+  std::memcpy(dt, B.dtlocal.data(), B.dtlocal.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_set_dtlocal(orc_domain* d, int b, const double* dt) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  Block& B = d->blk[b - 1];
+  std::memcpy(B.dtlocal.data(), dt, B.dtlocal.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_get_metrics(const orc_domain* d, int b, double* vol, double* dl, double* M) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  const Block& B = d->blk[b - 1];
+  if (vol) std::memcpy(vol, B.vol.data(), B.vol.size() * sizeof(double));
+  if (dl) std::memcpy(dl, B.dl.data(), B.dl.size() * sizeof(double));
+  if (M) std::memcpy(M, B.M.data(), B.M.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_get_faces(const orc_domain* d, int b, int dir, double* N, double* A) {
+  if (check_block(d, b) || dir < 1 || dir > 3) return ORC_ERR_INVALID;
+  const Block& B = d->blk[b - 1];
+  if (N) std::memcpy(N, B.fN[dir - 1].data(), B.fN[dir - 1].size() * sizeof(double));
+  if (A) std::memcpy(A, B.fA[dir - 1].data(), B.fA[dir - 1].size() * sizeof(double));
+  return ORC_OK;
+}
+
+// Fill_Ghost_Cell, Lib_Ghost.f90:11-137 (single rank: every block is local).
+int orc_fill_ghost_cell(orc_domain* d) {
+  int n = (int)d->bc.size();
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(d->nthreads)
+#endif
+  for (int q = 0; q < n; ++q) {
+    const BCrec& e = d->bc[q];
+    Block& bm = d->blk[e.b - 1];
+    switch (e.type) {
+      case 101: case 201:
+        Ghost_Connection(e.i, e.j, e.k, e.f, bm, e.is, e.js, e.ks, e.fs, d->blk[e.bs - 1]);
+        break;
+      case 300: Ghost_Symmetry(e.i, e.j, e.k, e.f, bm); break;
+      case 0: case 401: case 402: case 403: case 404: case 405: case 406: case 407: case 420:
+        Ghost_ZG_Extrapolate(e.i, e.j, e.k, e.f, bm);
+        break;
+      default: Ghost_Extrapolate(e.i, e.j, e.k, e.f, bm); break;
+    }
+  }
+  return ORC_OK;
+}
+
+// Fluxes / Fluxes_blk, Mod_Fluxes.f90:10-209 (convective part, SD off).
+int orc_fluxes(orc_domain* d) {
+  for (int bi = 0; bi < (int)d->blk.size(); ++bi) {
+    Block& B = d->blk[bi];
+    const int n1 = B.ni, n2 = B.nj, n3 = B.nk;
+#ifdef _OPENMP
+#pragma omp parallel num_threads(d->nthreads)
+#endif
+    {
+#ifdef _OPENMP
+#pragma omp for collapse(3)
+#endif
+      for (int k = 1; k <= n3; ++k)
+        for (int j = 1; j <= n2; ++j)
+          for (int i = 1; i <= n1; ++i) {
+            double* r = B.Rc(i, j, k);
+            for (int v = 0; v < NPRIM; ++v) r[v] = 0.0;
+            B.beta[B.inner(i, j, k)] = 1.0;
+          }
+      // i faces (:89-99)
+#ifdef _OPENMP
+#pragma omp for collapse(2)
+#endif
+      for (int k = 1; k <= n3; ++k)
+        for (int j = 1; j <= n2; ++j)
+          for (int i = 1; i <= n1 - 1; ++i) {
+            double dls[4] = {B.dl_(1, i - 1, j, k), B.dl_(1, i, j, k), B.dl_(1, i + 1, j, k), B.dl_(1, i + 2, j, k)};
+            size_t f = B.face(1, i, j, k);
+            if (!Convective_Flux(d, dls, &B.fN[0][3 * f], B.fA[0][f], B.Pc(i - 1, j, k), B.Pc(i, j, k),
+                                 B.Pc(i + 1, j, k), B.Pc(i + 2, j, k), B.Rc(i, j, k), B.Rc(i + 1, j, k)))
+              d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
+          }
+      // j faces (:129-139)
+#ifdef _OPENMP
+#pragma omp for collapse(2)
+#endif
+      for (int k = 1; k <= n3; ++k)
+        for (int i = 1; i <= n1; ++i)
+          for (int j = 1; j <= n2 - 1; ++j) {
+            double dls[4] = {B.dl_(2, i, j - 1, k), B.dl_(2, i, j, k), B.dl_(2, i, j + 1, k), B.dl_(2, i, j + 2, k)};
+            size_t f = B.face(2, i, j, k);
+            if (!Convective_Flux(d, dls, &B.fN[1][3 * f], B.fA[1][f], B.Pc(i, j - 1, k), B.Pc(i, j, k),
+                                 B.Pc(i, j + 1, k), B.Pc(i, j + 2, k), B.Rc(i, j, k), B.Rc(i, j + 1, k)))
+              d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
+          }
+      // k faces (:169-179)
+#ifdef _OPENMP
+#pragma omp for collapse(2)
+#endif
+      for (int j = 1; j <= n2; ++j)
+        for (int i = 1; i <= n1; ++i)
+          for (int k = 1; k <= n3 - 1; ++k) {
+            double dls[4] = {B.dl_(3, i, j, k - 1), B.dl_(3, i, j, k), B.dl_(3, i, j, k + 1), B.dl_(3, i, j, k + 2)};
+            size_t f = B.face(3, i, j, k);
+            if (!Convective_Flux(d, dls, &B.fN[2][3 * f], B.fA[2][f], B.Pc(i, j, k - 1), B.Pc(i, j, k),
+                                 B.Pc(i, j, k + 1), B.Pc(i, j, k + 2), B.Rc(i, j, k), B.Rc(i, j, k + 1)))
+              d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
+          }
+    }
+  }
+  return d->err;
+}
+
+// BC_Fluxes, Mod_BC_Fluxes.f90:10-218: in order of block and face.
+int orc_bc_fluxes(orc_domain* d) {
+  int upper = 0;
+  int nb = (int)d->blk.size();
+  for (int b = 1; b <= nb; ++b)
+    for (int f = 1; f <= 6; ++f) {
+      int lower = upper;
+      upper = upper + d->n_bf[(b - 1) * 6 + (f - 1)];
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 64) num_threads(d->nthreads)
+#endif
+      for (int q = lower; q < upper; ++q) {
+        const BCrec& e = d->bc[q];
+        Block& bm = d->blk[e.b - 1];
+        switch (e.type) {
+          case 101: case 201: BC_Connection_Eul(d, e.i, e.j, e.k, e.f, bm); break;
+          case 300: BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm); break;
+          case 400: BC_Extrapolation(d, e.i, e.j, e.k, e.f, bm); break;
+          case 405:
+            if (!BC_Inlet_Supersonic(d, e.i, e.j, e.k, e.f, bm, e.data)) BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            break;
+          case 406:
+            if (!BC_Outflow(d, e.i, e.j, e.k, e.f, bm, e.data)) BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            break;
+          default: break;
+        }
+      }
+    }
+  return d->err;
+}
+
+// RK_Newstate => Newstate_Conservative / Newstate_Primitive, Lib_Newstate.f90
+int orc_rk_newstate(orc_domain* d, int irk) {
+  static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};  // Lib_RK.f90:8-11
+  const int n_rk = d->cfg.n_rk;
+  const double c = RKcoeff[n_rk - 1][irk - 1];
+  const double strangcoeff = 1.0;
+  const Thermo& t = d->th;
+  const bool prim_mode = d->cfg.integration == ORC_INT_PRIM;
+  for (int bi = 0; bi < (int)d->blk.size(); ++bi) {
+    Block& B = d->blk[bi];
+#ifdef _OPENMP
+#pragma omp parallel for collapse(3) schedule(static) num_threads(d->nthreads)
+#endif
+    for (int k = 1; k <= B.nk; ++k)
+      for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i) {
+          double* prim = B.Pc(i, j, k);
+          const double* primold = B.POc(i, j, k);
+          double* res = B.Rc(i, j, k);
+          double dt = B.dtlocal[B.inner(i, j, k)];
+          double volume = B.vol_(i, j, k);
+          if (!prim_mode) {
+            // Compute_Cons_NoIRS :134-160
+            for (int v = 0; v < NPRIM; ++v) res[v] = -(res[v] / volume * dt * strangcoeff);
+            double consold[NPRIM], cons[NPRIM];
+            prim2cons(t, primold, consold);
+            prim2cons(t, prim, cons);
+            for (int v = 0; v < NPRIM; ++v) {        // RK_stage, Lib_RK.f90:15-27
+              double r_ = (cons[v] - consold[v] + res[v]) * c;
+              cons[v] = consold[v] + r_;
+            }
+            double rho, Rgas;
+            co_rotot_Rtot(t, prim[0], rho, Rgas);
+            double temperature = prim[NP] / (rho * Rgas);
+            (void)temperature;                        // T_guess: closed-form cons2prim
+            cons2prim(t, cons, prim);
+          } else {
+            // Compute_Prim_Residual :255-302 + RK_Stage (one calorically perfect species)
+            double rho, Rgas;
+            co_rotot_Rtot(t, prim[0], rho, Rgas);
+            double temperature = prim[NP] / (rho * Rgas);
+            double inv_volume = 1.0 / volume;
+            double inv_rhovolume = inv_volume / rho;
+            double velocity[3] = {prim[NU], prim[NV], prim[NW]};
+            res[0] = -res[0] * inv_volume;
+            double dwrotot = res[0];
+            for (int q = 0; q < 3; ++q) res[NU + q] = -res[NU + q] * inv_rhovolume - velocity[q] / rho * dwrotot;
+            double dwE = -res[NP] * inv_volume;
+            double dwroe = dwE - rho * (velocity[0] * res[NU] + velocity[1] * res[NV] + velocity[2] * res[NW]) -
+                           0.5 * dwrotot * (velocity[0] * velocity[0] + velocity[1] * velocity[1] + velocity[2] * velocity[2]);
+            double eiroi = (t.cp * temperature - t.R * temperature) * res[0];
+            double cv = prim[0] * (t.cp - t.R);
+            double dwTemp = (dwroe - eiroi) / cv;
+            res[NP] = t.R * (temperature * res[0] + prim[0] * dwTemp);
+            for (int v = 0; v < NPRIM; ++v) res[v] = res[v] * dt * strangcoeff;
+            for (int v = 0; v < NPRIM; ++v) {
+              double r_ = (prim[v] - primold[v] + res[v]) * c;
+              prim[v] = primold[v] + r_;
+            }
+          }
+          // Check_And_Fix_State :323-356
+          bool nan = false;
+          for (int v = 0; v < NPRIM; ++v) nan |= std::isnan(prim[v]);
+          if (nan || prim[NP] < 0.0) d->fail(ORC_ERR_NAN_OR_NEG_P, bi + 1, i, j, k);
+          if (prim[0] < 1e-20) prim[0] = 1e-20;
+        }
+  }
+  return d->err;
+}
+
+int orc_copy_state(orc_domain* d) {   // Copy_State, Mod_Explicit.f90:149-170
+  for (auto& B : d->blk) {
+#ifdef _OPENMP
+#pragma omp parallel for collapse(3) num_threads(d->nthreads)
+#endif
+    for (int k = 1; k <= B.nk; ++k)
+      for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i) {
+          const double* p = B.Pc(i, j, k);
+          double* po = B.POc(i, j, k);
+          for (int v = 0; v < NPRIM; ++v) po[v] = p[v];
+        }
+  }
+  return ORC_OK;
+}
+
+// Compute_dt, Mod_dt.f90:10-106 (Euler: CFL only).
+int orc_compute_dt(orc_domain* d, double* dtglobal_out) {
+  double dtglobal = d->dtglobal;
+  const Thermo& t = d->th;
+  const double cfl = d->cfg.cfl;
+  const int ndir = d->ndir;
+  for (auto& B : d->blk) {
+    double dtg = dtglobal;
+#ifdef _OPENMP
+#pragma omp parallel for collapse(3) reduction(min : dtg) num_threads(d->nthreads)
+#endif
+    for (int k = 1; k <= B.nk; ++k)
+      for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i) {
+          const double* p = B.Pc(i, j, k);
+          double rho, Rgas;
+          co_rotot_Rtot(t, p[0], rho, Rgas);
+          double Sound = f_ss(t, p[0], p[NP], rho, Rgas);
+          double dtmin = 1e8;
+          double vel[3] = {p[NU], p[NV], p[NW]};
+          for (int dd = 1; dd <= ndir; ++dd) {
+            double met[3] = {B.M_(dd, 1, i, j, k), B.M_(dd, 2, i, j, k), B.M_(dd, 3, i, j, k)};
+            double nrm = norm2(met[0], met[1], met[2]);
+            double versor[3] = {met[0] / nrm, met[1] / nrm, met[2] / nrm};
+            double vel_ = std::fabs(dot3(vel, versor));
+            double lambda = vel_ + Sound;
+            double dt = B.dl_(dd, i, j, k) / lambda * cfl;
+            dtmin = std::min(dt, dtmin);
+          }
+          double dtcell = dtmin;
+          if (d->iter < d->cfg.ramp_iter) dtcell = dtcell * (double)d->iter / (double)d->cfg.ramp_iter;
+          B.dtlocal[B.inner(i, j, k)] = dtcell;
+          dtg = std::min(dtcell, dtg);
+        }
+    dtglobal = dtg;
+  }
+  d->dtglobal = dtglobal;
+  if (dtglobal_out) *dtglobal_out = dtglobal;
+  return ORC_OK;
+}
+
+int orc_set_global_dt(orc_domain* d) {   // Set_Global_dt, Mod_dt.f90:110-130
+  for (auto& B : d->blk) std::fill(B.dtlocal.begin(), B.dtlocal.end(), d->dtglobal);
+  return ORC_OK;
+}
+
+// Explicit_Step, Mod_Explicit.f90:10-97 (no Strang, no sources, no coupling hook).
+int orc_explicit_step(orc_domain* d, double* dtglobal, double* time) {
+  d->iter = d->iter + 1;
+  d->iter_from_call = d->iter_from_call + 1;
+  d->dtglobal = 1e5;
+  orc_compute_dt(d, nullptr);
+  if (d->cfg.time_accurate) {
+    orc_set_global_dt(d);
+    d->time = d->time + d->dtglobal;
+  }
+  orc_copy_state(d);
+  for (int i_rk = 1; i_rk <= d->cfg.n_rk; ++i_rk) {
+    orc_fill_ghost_cell(d);
+    orc_fluxes(d);
+    orc_bc_fluxes(d);
+    orc_rk_newstate(d, i_rk);
+    if (d->err) break;
+  }
+  if (dtglobal) *dtglobal = d->dtglobal;
+  if (time) *time = d->time;
+  return d->err;
+}
+
+// Compute_Residual, Mod_Diagnostic.f90:13-50, summed over blocks.
+int orc_compute_residual(const orc_domain* d, double* total) {
+  for (int q = 0; q < NRES; ++q) total[q] = 0.0;
+  for (const auto& B : d->blk) {
+    double residuo[NRES] = {0, 0, 0, 0, 0};
+    for (int k = 1; k <= B.nk; ++k)
+      for (int j = 1; j <= B.nj; ++j)
+        for (int i = 1; i <= B.ni; ++i) {
+          const double* pn = &B.P[NPRIM * B.cell(i, j, k)];
+          const double* po = &B.PO[NPRIM * B.cell(i, j, k)];
+          double resn[NRES];
+          resn[0] = std::fabs(pn[0] - po[0]);
+          for (int v = 1; v < NRES; ++v) resn[v] = std::fabs(pn[v] - po[v]);
+          for (int v = 0; v < NRES; ++v) residuo[v] = residuo[v] + resn[v] * resn[v];
+        }
+    for (int v = 0; v < NRES; ++v) total[v] = total[v] + residuo[v];
+  }
+  return ORC_OK;
+}
+
+void orc_set_time(orc_domain* d, double time, int iter) {
+  d->time = time;
+  d->iter = iter;
+}
+double orc_get_time(const orc_domain* d) { return d->time; }
+void orc_set_dtglobal(orc_domain* d, double dtglobal) { d->dtglobal = dtglobal; }
+
+int orc_last_error(const orc_domain* d, int* b, int* i, int* j, int* k) {
+  if (b) *b = d->eb;
+  if (i) *i = d->ei;
+  if (j) *j = d->ej;
+  if (k) *k = d->ek;
+  return d->err;
+}
+
+double orc_limiter(int limiter, double x, double y) { return rlimiter(limiter, x, y); }
+
+void orc_riemann(const orc_domain* d, const double* left, const double* right, const double* normal,
+                 double* flux) {
+  bool bad = false;
+  RState L = make_state(d->th, left, bad);
+  RState R = make_state(d->th, right, bad);
+  RFlux F = Riemann(d, L, R, normal[0], normal[1], normal[2]);
+  flux[0] = F.r; flux[1] = F.u; flux[2] = F.v; flux[3] = F.w; flux[4] = F.E;
+}
+
+}  // extern "C"

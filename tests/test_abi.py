@@ -1,0 +1,75 @@
+"""The C-ABI library loads and exports every entry point include/*.h declares
+(no compute calls: runs without a GPU)."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def declared_functions():
+    names = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        names += re.findall(r"\b(mose_gpu_\w+)\s*\(", text)
+    return sorted(set(names))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from mose_b200 import _lib, build
+    build.build()
+    return _lib.load()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 30
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_binding_covers_the_header(lib):
+    from mose_b200 import _lib
+    assert set(_lib.SIGNATURES) == set(declared_functions())
+
+
+def test_default_config_matches_reference_defaults(lib):
+    from mose_b200 import _lib
+    cfg = _lib.Config()
+    lib.mose_gpu_default_config(C.byref(cfg))
+    # Register_Numerics.f90: time-scheme euler, cfl 0.5, time-accurate false, HLLC
+    assert cfg.abi_version == _lib.ABI_VERSION
+    assert cfg.n_rk == 1 and cfg.cfl == 0.5 and cfg.time_accurate == 0 and cfg.riemann == 0
+    assert cfg.nsc == 1 and cfg.gamma == 1.4
+
+
+def test_create_rejects_bad_configs_without_touching_the_gpu(lib):
+    from mose_b200 import _lib
+    cfg = _lib.Config()
+    lib.mose_gpu_default_config(C.byref(cfg))
+    h = C.c_void_p()
+    cfg.nsc = 2          # multi-species is off this path
+    assert lib.mose_gpu_create(C.byref(cfg), C.byref(h)) == _lib.ERR_UNSUPPORTED
+    cfg.nsc = 1
+    cfg.abi_version = 99
+    assert lib.mose_gpu_create(C.byref(cfg), C.byref(h)) == _lib.ERR_INVALID
+    assert not h.value
+
+
+def test_library_has_no_cpu_fallback():
+    """The package fails loudly when the CUDA library is absent."""
+    import importlib
+    from mose_b200 import _lib
+    saved = _lib.LIB_PATH
+    try:
+        _lib.LIB_PATH = Path("/nonexistent/libmose_gpu.so")
+        _lib._lib = None
+        with pytest.raises(RuntimeError, match="no CPU fallback"):
+            _lib.load()
+    finally:
+        _lib.LIB_PATH = saved
+        _lib._lib = None
+        importlib.reload(_lib)

@@ -1,0 +1,191 @@
+"""GPU parity: the CUDA path (through the C ABI) against the CPU oracle on
+the same seeded inputs.  The reference-exact FP64 mode must agree bit for bit
+(max |difference| == 0) except where a transcendental library call (pow in
+the 406 outflow) may differ by an ulp between glibc and CUDA; those cases use
+the normwise relative L-infinity bar of 1e-12."""
+import numpy as np
+import pytest
+
+from mose_b200 import cases
+from mose_b200.cases import GC
+
+pytestmark = pytest.mark.gpu
+
+
+def solver(case, **kw):
+    from mose_b200 import Solver
+    return Solver(case, **kw)
+
+
+def interior(P):
+    """Interior cells of a reference-layout array (nk+4, nj+4, ni+4, 5)."""
+    return P[GC:-GC, GC:-GC, GC:-GC]
+
+
+def rel_linf(a, b):
+    den = np.abs(b).max()
+    return np.abs(a - b).max() / (den if den > 0 else 1.0)
+
+
+def compare_state(s, o, nblk, exact=True, tol=1e-12, vars_=(0, 1, 2, 4)):
+    worst = 0.0
+    for b in range(1, nblk + 1):
+        g = interior(s.download_prim(b))[..., list(vars_)]
+        r = interior(o.get_prim(b))[..., list(vars_)]
+        if exact:
+            assert np.array_equal(g, r), f"block {b}: max diff {np.abs(g - r).max()}"
+        else:
+            worst = max(worst, rel_linf(g, r))
+    if not exact:
+        assert worst <= tol, worst
+    return worst
+
+
+SMALL = {
+    "sod": lambda: cases.sod(200),
+    "vortex": lambda: cases.isentropic_vortex(64, steps=3),
+    "vortex_minmod_ausm": lambda: cases.isentropic_vortex(40, steps=3, limiter="minmod", riemann="AUSM+"),
+    "quadrant": lambda: cases.four_quadrant(seed=2, nbx=3, nby=2, nmin=20, nmax=70, steps=3),
+    "quadrant_vanleer_slau": lambda: cases.four_quadrant(seed=5, nbx=2, nby=2, nmin=17, nmax=40, steps=3,
+                                                        limiter="vanleer", riemann="SLAU"),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_metrics_bitwise(oracle_mod, name):
+    case = SMALL[name]()
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for b in range(1, len(case.nodes) + 1):
+        vol_o, dl_o, _ = o.get_metrics(b)
+        vol_g, dl_g = s.download_metrics(b)
+        assert np.array_equal(vol_g[2, 2:-2, 2:-2], vol_o[2, 2:-2, 2:-2])
+        ni, nj, _ = s.dims[b - 1]
+        # dl along i on the i-ghosted rows, along j on the j-ghosted columns
+        assert np.array_equal(dl_g[2, 2:-2, :, 0], dl_o[2, 2:-2, :, 0])
+        if nj >= 3:
+            assert np.array_equal(dl_g[2, :, 2:-2, 1], dl_o[2, :, 2:-2, 1])
+        for d in (1, 2):
+            Ng, Ag = s.download_faces(b, d)
+            No, Ao = o.get_faces(b, d)
+            assert np.array_equal(Ag, Ao) and np.array_equal(Ng, No)
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_residual_phase_path_bitwise(oracle_mod, name):
+    """One residual evaluation (Fill_Ghost_Cell + Fluxes + BC_Fluxes) through
+    the phase entry points: R identical to the oracle's."""
+    case = SMALL[name]()
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    o.fill_ghost_cell()
+    o.fluxes()
+    o.bc_fluxes()
+    s.fill_ghost_cell()
+    s.fluxes_and_bc_fluxes()
+    for b in range(1, len(case.nodes) + 1):
+        rg = interior(s.download_residual(b))[..., [0, 1, 2, 4]]
+        ro = interior(o.get_residual(b))[..., [0, 1, 2, 4]]
+        assert np.array_equal(rg, ro), f"block {b}: rel {rel_linf(rg, ro):.3e}"
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_phase_step_bitwise(oracle_mod, name):
+    """A whole Explicit_Step through the separate phases (compute_dt,
+    set_global_dt, copy_state, then per stage ghost fill, residual, newstate)."""
+    case = SMALL[name]()
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(2):
+        dto, _ = o.step()
+        dtg = s.run_phases()
+        assert dtg == dto
+        compare_state(s, o, len(case.nodes))
+
+
+@pytest.mark.parametrize("name", sorted(SMALL))
+def test_fused_steps_bitwise(oracle_mod, name):
+    """The fused step (one kernel per RK stage, dt on the device) over several
+    steps, and the graph-replayed advance()."""
+    case = SMALL[name]()
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(2):
+        dto, to = o.step()
+        dtg, tg = s.explicit_step()
+        assert dtg == dto and tg == to
+    compare_state(s, o, len(case.nodes))
+    for _ in range(3):
+        o.step()
+    dtg, tg = s.advance(3)
+    assert tg == o.time
+    compare_state(s, o, len(case.nodes))
+    ng, no = s.compute_residual(), o.residual_norms()
+    np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0)
+
+
+def test_sod_to_final_time_bitwise(oracle_mod):
+    """Configuration 1 at 1000 cells integrated to t >= 0.2."""
+    case = cases.sod(1000)
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    n = 0
+    while o.time < case.t_end:
+        o.step()
+        s.explicit_step()
+        n += 1
+    assert s.time == o.time
+    compare_state(s, o, 1)
+
+
+def test_sod79_reference_inputs_bitwise(oracle_mod):
+    from tests.test_oracle import sod79_case
+    case, _ = sod79_case()
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    while o.time < case.t_end:
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, 1)
+
+
+def test_curvilinear_walls_inflow_outflow(oracle_mod):
+    """Configuration 5 geometry (small): curvilinear metrics, 405 inflow, 406
+    outflow (pow: ulp-level library differences allowed), 300 slip walls."""
+    case = cases.curvilinear_channel(48, steps=1)
+    # a perturbation so every boundary branch sees non-trivial states
+    rng = np.random.default_rng(0)
+    case.prim[0][..., 0] *= 1 + 0.05 * rng.standard_normal(case.prim[0].shape[:-1])
+    case.prim[0][..., 2] = 0.05 * rng.standard_normal(case.prim[0].shape[:-1])
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(3):
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, 1, exact=False, tol=1e-12)
+
+
+def test_local_time_stepping(oracle_mod):
+    case = cases.four_quadrant(seed=3, nbx=2, nby=2, nmin=16, nmax=30, steps=1)
+    case.time_accurate = False
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(2):
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, 4)
+    for b in range(1, 5):
+        assert np.array_equal(s.download_dt(b), o.get_dtlocal(b))
+
+
+def test_device_error_reports_location(oracle_mod):
+    """A negative pressure planted in the initial state is reported like the
+    reference's stop (code 4/5 with the offending cell), and the context stays
+    usable."""
+    from mose_b200 import MoseError
+    case = cases.isentropic_vortex(32, steps=1)
+    case.prim[0][0, 10, 7, 4] = -1.0
+    s = solver(case)
+    with pytest.raises(MoseError) as ei:
+        s.explicit_step()
+    assert ei.value.code in (4, 5)
