@@ -22,7 +22,9 @@
  *
  * State is device resident between calls: host P is stale until
  * mose_gpu_download_prim().  A context is not thread safe and owns one
- * CUDA stream.
+ * CUDA stream.  On 2-D domains (nk = 1) the transfers of P and R read and
+ * write only the k = 1 plane of the reference array: the reference never
+ * reads its k ghost planes on this path, and w is identically zero there.
  */
 #ifndef MOSE_GPU_H
 #define MOSE_GPU_H

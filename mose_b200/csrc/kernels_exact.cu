@@ -393,7 +393,7 @@ __global__ void k_compute_dt(const BlockDesc* blk, int nblk, const double* P, Me
       dtmin = fmin(dt, dtmin);
     }
     double dtcell = dtmin;
-    if (iter < ramp_iter) dtcell = dtcell * (double)iter / (double)ramp_iter;
+    if (ramp_iter > 0 && iter < ramp_iter) dtcell = dtcell * (double)iter / (double)ramp_iter;
     if (store_local) dtl[mb + o] = dtcell;
     local_min = fmin(local_min, dtcell);
   }
@@ -507,19 +507,18 @@ __global__ void k_sum_partials(const double* partial, int n, double* out) {
 
 // ---------------------------------------------------------------------------
 // Layout conversion between the reference's AoS P(5, 1-gc:ni+gc, ...) and the
-// device SoA planes.  host_ref: the reference-layout array of one block.
+// device SoA planes.  ref: the transferred slab of one block's reference
+// array -- the whole array in 3-D, the k = 1 plane in 2-D (the only plane the
+// 2-D path reads or writes).
 // ---------------------------------------------------------------------------
 __global__ void k_ref_to_soa(const BlockDesc* blk, int b, const double* ref, double* dst, int nv, int nd) {
   const BlockDesc& d = blk[b];
   const int ex = d.ni + 4, ey = d.nj + 4, ez = (nd == 3) ? d.nk + 4 : 1;
   const long long n = (long long)ex * ey * ez;
   const long long vs = d.vstride;
-  const int refz = d.nk + 4;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     int x = (int)(q % ex), y = (int)((q / ex) % ey), z = (int)(q / ((long long)ex * ey));
-    int rz = (nd == 3) ? z : GW;  // 2-D: the k = 1 plane of the reference array
-    (void)refz;
-    const double* src = ref + 5 * ((long long)x + (long long)ex * ((long long)y + (long long)ey * rz));
+    const double* src = ref + 5 * q;
     long long o = (nd == 3) ? cell_off3(d, x - GW, y - GW, z - GW) : cell_off2(d, x - GW, y - GW);
     if (nv == 5) {
       for (int v = 0; v < 5; ++v) dst[d.sbase + v * vs + o] = src[v];
@@ -532,11 +531,11 @@ __global__ void k_ref_to_soa(const BlockDesc* blk, int b, const double* ref, dou
   }
 }
 
-// Writes the reference layout; in 2-D the w slot is 0 and the k-ghost planes
-// repeat the k = 1 plane (the zero-gradient fill of null k faces).
+// Writes the slab of the reference layout (see k_ref_to_soa); in 2-D the w
+// slot is 0.
 __global__ void k_soa_to_ref(const BlockDesc* blk, int b, const double* src, double* ref, int nv, int nd) {
   const BlockDesc& d = blk[b];
-  const int ex = d.ni + 4, ey = d.nj + 4, ez = d.nk + 4;
+  const int ex = d.ni + 4, ey = d.nj + 4, ez = (nd == 3) ? d.nk + 4 : 1;
   const long long n = (long long)ex * ey * ez;
   const long long vs = d.vstride;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {

@@ -539,7 +539,10 @@ static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool uplo
   if (b < 1 || b > (int)ctx->hblk.size()) return fail(ctx, MOSE_ERR_INVALID, "bad block %d", b);
   CU(cudaSetDevice(ctx->cfg.device));
   const HostBlock& h = ctx->hblk[b - 1];
-  long long n = (long long)(h.ni + 4) * (h.nj + 4) * (h.nk + 4);
+  // the transferred slab: the whole array in 3-D, the k = 1 plane in 2-D
+  long long plane = (long long)(h.ni + 4) * (h.nj + 4);
+  long long n = (ctx->nd == 3) ? plane * (h.nk + 4) : plane;
+  if (ctx->nd == 2) P += 5 * GW * plane;
   int rc = ensure_staging(ctx, 5 * (size_t)n);
   if (rc) return rc;
   double* dst = (arena < 0) ? ctx->resid.p : ctx->state[arena].p;
@@ -699,7 +702,7 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
   launch_step_begin(ctx->dtmin.p, 1e5, ctx->iterdev.p, ctx->stream); ++k;
   // Compute_dt starts its minimum from 1d5 (Mod_Explicit.f90:44)
   launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(), ctx->dtl.p,
-                    ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, -1, 0, ctx->cfg.time_accurate ? 0 : 1,
+                    ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0, ctx->cfg.time_accurate ? 0 : 1,
                     ctx->uniform, ctx->stream); ++k;
   launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, ctx->stream); ++k;
   int pc = s0;
@@ -834,7 +837,7 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
     mark(-1);
     launch_step_begin(ctx->dtmin.p, 1e5, ctx->iterdev.p, ctx->stream);
     launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(),
-                      ctx->dtl.p, ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, -1, 0,
+                      ctx->dtl.p, ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0,
                       ctx->cfg.time_accurate ? 0 : 1, ctx->uniform, ctx->stream);
     launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, ctx->stream);
     mark(0);
