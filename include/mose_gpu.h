@@ -156,6 +156,31 @@ int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double
  * blocks of (|d rho|, |du|, |dv|, |dw|, |dp|)^2 between P and PO; total[5]. */
 int mose_gpu_residual_norms(mose_gpu_ctx* ctx, double* total);
 
+/* Compute_Residual on caller-owned device arrays, allocating nothing.
+ * No counterpart in the reference: it exists for callers that keep P and PO
+ * in their own device memory (the reference layout of one block) and cannot
+ * let a library call cudaMalloc, because their device memory belongs to
+ * another allocator or to a budget fixed at start-up.
+ *   P, PO : device pointers, P(5, 1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc)
+ *   total : device pointer to 5 doubles; total += sums of squares of
+ *           (|d rho|, |du|, |dv|, |dw|, |dp|) over the interior cells, like
+ *           the reference's `total = total + residuo` across blocks
+ *   stream: a cudaStream_t (NULL: the legacy default stream)
+ * Scratch: a fixed device array of MOSE_NOALLOC_MAX_CHUNKS x 5 doubles
+ * (160 KB, held by every GPU that loads the library until exit); a block
+ * may hold at most MOSE_NOALLOC_MAX_CHUNKS * MOSE_NOALLOC_CHUNK_CELLS
+ * (268,435,456) cells, larger blocks return MOSE_ERR_INVALID with a message
+ * in mose_gpu_noalloc_last_error().  The first call on a device looks up the
+ * array's address (cudaGetSymbolAddress) with that device current, so make
+ * the first call before any stream capture.  Every call shares the array:
+ * calls that overlap on the GPU (other streams, other threads) race.  Calls
+ * on one stream are ordered and each overwrites what it reads. */
+#define MOSE_NOALLOC_MAX_CHUNKS 4096
+#define MOSE_NOALLOC_CHUNK_CELLS 65536
+int mose_gpu_residual_norms_noalloc(const double* P, const double* PO, int32_t ni, int32_t nj, int32_t nk,
+                                    double* total, void* stream);
+const char* mose_gpu_noalloc_last_error(void);
+
 int mose_gpu_set_time(mose_gpu_ctx* ctx, double time, int32_t iter);
 int mose_gpu_get_time(mose_gpu_ctx* ctx, double* time, int32_t* iter);
 /* Waits for the context's stream and reports any device-detected failure. */

@@ -61,6 +61,8 @@ SIGNATURES = {
     "mose_gpu_synchronize": (C.c_int, [_D]),
     "mose_gpu_uniform_metrics": (C.c_int, [_D]),
     "mose_gpu_stream": (C.c_void_p, [_D]),
+    "mose_gpu_residual_norms_noalloc": (C.c_int, [_D, _D, C.c_int32, C.c_int32, C.c_int32, _D, _D]),
+    "mose_gpu_noalloc_last_error": (C.c_char_p, []),
     "mose_gpu_time_kernels": (C.c_int, [_D, C.c_int32, _dp, _ip]),
     "mose_gpu_launch_count": (C.c_int64, [_D]),
     "mose_gpu_download_metrics": (C.c_int, [_D, C.c_int32, _dp, _dp]),

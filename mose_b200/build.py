@@ -30,6 +30,7 @@ UNITS = {
     "stage_exact_r2.cu": ["--fmad=false"],
     "stage_exact_r3.cu": ["--fmad=false"],
     "mose_gpu.cu": [],
+    "norms_noalloc.cu": [],
 }
 
 
