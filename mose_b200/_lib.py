@@ -5,10 +5,12 @@ Loading fails loudly when the library is missing: there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "lib" / "libmose_gpu.so"
+# MOSE_GPU_LIB selects another build of the same library (e.g. a tuning variant)
+LIB_PATH = Path(os.environ.get("MOSE_GPU_LIB", _HERE / "lib" / "libmose_gpu.so"))
 
 ABI_VERSION = 1
 

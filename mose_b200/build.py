@@ -25,10 +25,9 @@ COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--exp
 # translation unit -> extra flags
 UNITS = {
     "kernels_exact.cu": ["--fmad=false"],
-    "stage_exact_r0.cu": ["--fmad=false"],
-    "stage_exact_r1.cu": ["--fmad=false"],
-    "stage_exact_r2.cu": ["--fmad=false"],
-    "stage_exact_r3.cu": ["--fmad=false"],
+    **{f"stage_exact_r{r}.cu": ["--fmad=false"] for r in range(4)},
+    **{f"stage_fp64_r{r}.cu": [] for r in range(4)},
+    **{f"stage_mixed_r{r}.cu": [] for r in range(4)},
     "mose_gpu.cu": [],
     "norms_noalloc.cu": [],
 }
@@ -52,10 +51,16 @@ def _stale(target: Path, deps: list[Path]) -> bool:
     return any(d.stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    """Compiles every unit that changed and links the shared library."""
-    OBJDIR.mkdir(exist_ok=True)
-    LIBDIR.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, out_dir: Path | None = None,
+          defines: tuple = ()) -> Path:
+    """Compiles every unit that changed and links the shared library.
+    out_dir/defines build a variant elsewhere (objects and library in out_dir)."""
+    global OBJDIR, LIBDIR
+    if out_dir is not None:
+        OBJDIR = LIBDIR = Path(out_dir)
+    OBJDIR.mkdir(parents=True, exist_ok=True)
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    extra_defs = [f"-D{d}" for d in defines]
     deps = _deps()
     objs = []
     cc = nvcc()
@@ -64,7 +69,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         obj = OBJDIR / (unit + ".o")
         objs.append(obj)
         if force or _stale(obj, deps):
-            jobs.append([cc] + COMMON + extra + ["-c", str(CSRC / unit), "-o", str(obj)])
+            jobs.append([cc] + COMMON + extra + extra_defs + ["-c", str(CSRC / unit), "-o", str(obj)])
     # units compile independently: run them in parallel
     procs = []
     for cmd in jobs:

@@ -46,17 +46,23 @@ void launch_faces_to_ref(const BlockDesc* dblk, int b, long long n, MetricArgs m
 }  // namespace mose
 
 namespace mose {
-bool launch_stage2d_exact_r0(const StageArgs& a, int grid, int mode, bool uni, int lim, cudaStream_t s);
-bool launch_stage2d_exact_r1(const StageArgs& a, int grid, int mode, bool uni, int lim, cudaStream_t s);
-bool launch_stage2d_exact_r2(const StageArgs& a, int grid, int mode, bool uni, int lim, cudaStream_t s);
-bool launch_stage2d_exact_r3(const StageArgs& a, int grid, int mode, bool uni, int lim, cudaStream_t s);
-inline bool launch_stage2d_exact(const StageArgs& a, int grid, int mode, bool uni, int rie, int lim, cudaStream_t s) {
-  switch (rie) {
-    case 0: return launch_stage2d_exact_r0(a, grid, mode, uni, lim, s);
-    case 1: return launch_stage2d_exact_r1(a, grid, mode, uni, lim, s);
-    case 2: return launch_stage2d_exact_r2(a, grid, mode, uni, lim, s);
-    case 3: return launch_stage2d_exact_r3(a, grid, mode, uni, lim, s);
-  }
-  return false;
+// Stage kernels: one launcher per (precision p, Riemann solver r) unit.
+#define MOSE_STAGE_DECL(p, r) \
+  bool launch_stage2d_p##p##_r##r(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s);
+MOSE_STAGE_DECL(0, 0) MOSE_STAGE_DECL(0, 1) MOSE_STAGE_DECL(0, 2) MOSE_STAGE_DECL(0, 3)
+MOSE_STAGE_DECL(1, 0) MOSE_STAGE_DECL(1, 1) MOSE_STAGE_DECL(1, 2) MOSE_STAGE_DECL(1, 3)
+MOSE_STAGE_DECL(2, 0) MOSE_STAGE_DECL(2, 1) MOSE_STAGE_DECL(2, 2) MOSE_STAGE_DECL(2, 3)
+#undef MOSE_STAGE_DECL
+
+// mode 0: fused residual + RK update; mode 1: residual only (exact precision).
+inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int prec, int rie, int lim,
+                           cudaStream_t s) {
+  using L = bool (*)(const StageArgs&, int, int, bool, int, cudaStream_t);
+  static const L table[3][4] = {
+      {launch_stage2d_p0_r0, launch_stage2d_p0_r1, launch_stage2d_p0_r2, launch_stage2d_p0_r3},
+      {launch_stage2d_p1_r0, launch_stage2d_p1_r1, launch_stage2d_p1_r2, launch_stage2d_p1_r3},
+      {launch_stage2d_p2_r0, launch_stage2d_p2_r1, launch_stage2d_p2_r2, launch_stage2d_p2_r3}};
+  if (prec < 0 || prec > 2 || rie < 0 || rie > 3) return false;
+  return table[prec][rie](a, nsm, mode, uni, lim, s);
 }
 }  // namespace mose

@@ -40,12 +40,16 @@ struct DevBuf {
   DevBuf& operator=(const DevBuf&) = delete;
   DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
   ~DevBuf() { release(); }
+  // Zero-filled allocation.  The context's stream does not synchronise with
+  // the legacy default stream that cudaMemset uses, so wait for the fill
+  // before any work on the context's stream can touch the buffer.
   cudaError_t alloc(size_t count) {
     release();
     n = count;
     if (count == 0) return cudaSuccess;
     cudaError_t e = cudaMalloc(&p, count * sizeof(T));
     if (e == cudaSuccess) e = cudaMemset(p, 0, count * sizeof(T));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return e;
   }
   void release() {
@@ -91,7 +95,6 @@ struct mose_gpu_ctx {
   DevBuf<double> staging;     // reference-layout transfers
   int nghost = 0, nitems = 0;
   int cur = 0, po = 0;        // state arena holding P, and PO
-  int stage_grid = 0;
 
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_kernels = 0;
@@ -518,7 +521,6 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   ctx->nitems = (int)items.size();
   CU(ctx->items.alloc(items.size()));
   CU(cudaMemcpy(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
-  ctx->stage_grid = std::min(ctx->nitems, ctx->nsm * 2);
   ctx->cur = 0;
   ctx->po = 1;
   CU(cudaDeviceSynchronize());
@@ -676,8 +678,10 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
 int mose_gpu_residual(mose_gpu_ctx* ctx) {
   int rc = require_ready(ctx);
   if (rc) return rc;
+  // the phase-by-phase path always runs the reference-exact arithmetic
   StageArgs a = stage_args(ctx, ctx->cur, ctx->po, -1, 1);
-  if (!launch_stage2d_exact(a, ctx->stage_grid, 1, ctx->uniform, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream))
+  if (!launch_stage2d(a, ctx->nsm, 1, false, MOSE_PRECISION_FP64_EXACT, ctx->cfg.riemann, ctx->cfg.limiter,
+                      ctx->stream))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "no kernel for this solver / limiter");
   ctx->launches++;
   return check_launch(ctx, "residual");
@@ -712,7 +716,8 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
                        ctx->stream);
     if (ctx->nghost) ++k;
     StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-    launch_stage2d_exact(a, ctx->stage_grid, 0, ctx->uniform, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream);
+    launch_stage2d(a, ctx->nsm, 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
+                   ctx->stream);
     ++k;
     pc = pn;
   }
@@ -852,7 +857,8 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
         launches[1] += 1;
       }
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-      launch_stage2d_exact(a, ctx->stage_grid, 0, ctx->uniform, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream);
+      launch_stage2d(a, ctx->nsm, 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
+                     ctx->stream);
       mark(2);
       launches[2] += 1;
       pc = pn;

@@ -1,0 +1,346 @@
+// physics_fast.cuh -- FP64 and mixed FP32/FP64 face physics: the same
+// algorithm as physics_exact.cuh, restated for speed.
+//
+// FP64 ("fp64" precision): the single-species calorically perfect algebra is
+// simplified where it is an identity in exact arithmetic (rho_s/rho = 1,
+// R_roe = R, gamma_roe = gamma, cv_roe T_roe - sum_ei = 0, h = gamma/(gamma-1)
+// p/rho), divisions and square roots become reciprocals / reciprocal square
+// roots refined by Newton-Raphson from the hardware seed, and the compiler
+// contracts multiply-adds.  Branch-free, so independent faces interleave.
+// Results stay within ~1e-14 relative of the reference arithmetic; the
+// tests hold them to the 1e-12 normwise bar.
+//
+// Mixed ("mixed" precision): the limited slopes and the Riemann solver's wave
+// structure (sound speeds, Roe averages, signal speeds, star state) run in
+// FP32 with single-instruction reciprocals; the upwind physical flux and the
+// interface states stay FP64, so the FP32 rounding only touches the small
+// dissipative part of each face flux.
+#pragma once
+
+#include "common.cuh"
+
+namespace mose {
+namespace fast {
+
+// ---- reciprocal / reciprocal square root by Newton-Raphson ------------------
+// Seed from the hardware approximation of the leading bits (about 2^-23
+// relative error), two Newton-Raphson steps (error squares per step: 2^-46,
+// then below one ulp).  Markstein, IBM J. Res. Dev. 34 (1990); Muller et al.,
+// Handbook of Floating-Point Arithmetic, ch. 4.  Valid for normal, finite x.
+__device__ __forceinline__ double rcp(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  double e = fma(-x, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-x, r, 1.0);
+  return fma(r, e, r);
+}
+__device__ __forceinline__ double rsqrt_(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  // y <- y + y (1 - x y^2) / 2
+  double e = fma(-x * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-x * y, y, 1.0);
+  return fma(0.5 * y, e, y);
+}
+// sqrt(x) = x rsqrt(x) with one residual correction; sqrt(0) = 0.
+__device__ __forceinline__ double sqrt_(double x) {
+  double y = rsqrt_(x);
+  double s = x * y;
+  double e = fma(-s, s, x);          // x - s^2
+  s = fma(0.5 * y, e, s);
+  return x > 0.0 ? s : 0.0;
+}
+__device__ __forceinline__ double div_(double a, double b) { return a * rcp(b); }
+
+// ---- limiters: phi(r) x with r = y/(x + 1e-30), one division each ----------
+template <int LIM>
+__device__ __forceinline__ double limiter(double x, double y) {
+  if constexpr (LIM == 1) {            // minmod
+    double r = (fabs(x) > fabs(y)) ? y : x;
+    return (x * y < 0.0) ? 0.0 : r;
+  } else if constexpr (LIM == 2) {     // van Leer: x (y sgn(x') + |y|) / (|x'| + |y|)
+    double xp = x + 1e-30;
+    double num = y * copysign(1.0, xp) + fabs(y);
+    double den = fabs(xp) + fabs(y);
+    return x * num / den;
+  } else if constexpr (LIM == 3) {     // van Albada: x (y^2 + y x') / (x'^2 + y^2)
+    double xp = x + 1e-30;
+    double num = y * (y + xp);
+    double den = fma(xp, xp, y * y);
+    return x * num / den;
+  } else if constexpr (LIM == 4) {     // MC
+    double ru = y / (x + 1e-30);
+    return fmax(0.0, fmin(fmin(2.0 * ru, 0.5 * (1.0 + ru)), 2.0)) * x;
+  } else if constexpr (LIM == 5) {     // superbee
+    double ru = y / (x + 1e-30);
+    return fmax(fmax(0.0, fmin(2.0 * ru, 1.0)), fmin(ru, 2.0)) * x;
+  } else {
+    return 0.0;
+  }
+}
+template <int LIM>
+__device__ __forceinline__ float limiter32(float x, float y) {
+  if constexpr (LIM == 1) {
+    float r = (fabsf(x) > fabsf(y)) ? y : x;
+    return (x * y < 0.0f) ? 0.0f : r;
+  } else if constexpr (LIM == 2) {
+    float xp = x + 1e-30f;
+    float num = y * copysignf(1.0f, xp) + fabsf(y);
+    float den = fabsf(xp) + fabsf(y);
+    return den > 0.0f ? __fdividef(x * num, den) : 0.0f;
+  } else if constexpr (LIM == 3) {
+    float xp = x + 1e-30f;
+    float num = y * (y + xp);
+    float den = fmaf(xp, xp, y * y);
+    return den > 0.0f ? __fdividef(x * num, den) : 0.0f;
+  } else if constexpr (LIM == 4) {
+    float ru = __fdividef(y, x + 1e-30f);
+    return fmaxf(0.0f, fminf(fminf(2.0f * ru, 0.5f * (1.0f + ru)), 2.0f)) * x;
+  } else if constexpr (LIM == 5) {
+    float ru = __fdividef(y, x + 1e-30f);
+    return fmaxf(fmaxf(0.0f, fminf(2.0f * ru, 1.0f)), fminf(ru, 2.0f)) * x;
+  } else {
+    return 0.0f;
+  }
+}
+
+struct GasF {
+  double gamma, gm1, gcp;       // gamma, gamma - 1, gamma / (gamma - 1)
+  double igm1;                  // 1 / (gamma - 1)
+};
+__device__ __forceinline__ GasF gasf(const Gas& g) {
+  GasF f;
+  f.gamma = g.gamma;
+  f.gm1 = g.gamma - 1.0;
+  f.gcp = g.gamma / (g.gamma - 1.0);
+  f.igm1 = 1.0 / (g.gamma - 1.0);
+  return f;
+}
+
+template <int NV>
+__device__ __forceinline__ double un(const double* q, const double* n) {
+  if constexpr (NV == 5) return q[1] * n[0] + q[2] * n[1] + q[3] * n[2];
+  else return q[1] * n[0] + q[2] * n[1];
+}
+template <int NV>
+__device__ __forceinline__ double v2(const double* q) {
+  if constexpr (NV == 5) return q[1] * q[1] + q[2] * q[2] + q[3] * q[3];
+  else return q[1] * q[1] + q[2] * q[2];
+}
+
+// Batten HLLC (Lib_Riemann_HLL.f90:147-258) in FP64, branch free: the side
+// and the star correction are selected, not branched to.
+template <int NV>
+__device__ __forceinline__ void hllc(const GasF& g, const double* L, const double* R, const double* n, double* F) {
+  constexpr int P = NV - 1;
+  const double rl = L[0], rr = R[0];
+  const double rsl = rsqrt_(rl), rsr = rsqrt_(rr);
+  const double srL = rl * rsl, srR = rr * rsr;          // sqrt(rho)
+  const double irl = rsl * rsl, irr = rsr * rsr;        // 1/rho
+  const double unl = un<NV>(L, n), unr = un<NV>(R, n);
+  const double pol = L[P] * irl, por = R[P] * irr;      // p/rho
+  const double aL = sqrt_(g.gamma * pol), aR = sqrt_(g.gamma * por);
+  const double h0l = fma(g.gcp, pol, 0.5 * v2<NV>(L));
+  const double h0r = fma(g.gcp, por, 0.5 * v2<NV>(R));
+  const double isr = rcp(srL + srR);
+  const double wl = srL * isr, wr = srR * isr;
+  double ur[3];
+  ur[0] = fma(wr, R[1], wl * L[1]);
+  ur[1] = fma(wr, R[2], wl * L[2]);
+  ur[2] = 0.0;
+  if constexpr (NV == 5) ur[2] = fma(wr, R[3], wl * L[3]);
+  const double h0_roe = fma(wr, h0r, wl * h0l);
+  const double vel2 = ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2];
+  const double a_roe = sqrt_(g.gm1 * fma(-0.5, vel2, h0_roe));
+  const double un_roe = (NV == 5) ? ur[0] * n[0] + ur[1] * n[1] + ur[2] * n[2] : ur[0] * n[0] + ur[1] * n[1];
+  const double S1 = fmin(fmin(0.0, unl - aL), un_roe - a_roe);
+  const double S4 = fmax(fmax(0.0, unr + aR), un_roe + a_roe);
+  const double ml = rl * (S1 - unl), mr = rr * (S4 - unr);
+  const double idn = rcp(ml - mr);
+  const double Sstar = (R[P] - L[P] + ml * unl - mr * unr) * idn;
+  // upwind side K: left when S1 >= 0 or Sstar >= 0
+  const bool left = (S1 >= 0.0) || (Sstar >= 0.0);
+  const double* K = left ? L : R;
+  const double rk = left ? rl : rr, unk = left ? unl : unr, h0k = left ? h0l : h0r;
+  const double SK = left ? S1 : S4;
+  const double pk = K[P];
+  const double e0k = h0k - pk * (left ? irl : irr);
+  F[0] = rk * unk;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = fma(F[0], K[1 + d], pk * n[d]);
+  F[P] = F[0] * h0k;
+  // star correction, applied when K's outer wave is subsonic in the face frame
+  const bool corr = left ? (S1 < 0.0) : (S4 > 0.0);
+  const double mk = left ? ml : mr;                        // rho_K (S_K - un_K)
+  const double pstar = fma(rl * (unl - S1), unl - Sstar, L[P]);
+  const double inv = rcp(SK - Sstar);
+  const double dp = pstar - pk;
+  const double c0 = SK * (mk * inv - rk);                  // S_K (U*_1 - rho_K)
+  double c[5];
+  c[0] = c0;
+  for (int d = 0; d < NV - 2; ++d) c[1 + d] = SK * (fma(mk, K[1 + d], dp * n[d]) * inv - rk * K[1 + d]);
+  c[P] = SK * ((mk * e0k - pk * unk + pstar * Sstar) * inv - rk * e0k);
+  for (int v = 0; v < NV; ++v) F[v] = corr ? F[v] + c[v] : F[v];
+}
+
+// AUSM+ (Lib_Riemann_AUSM.f90:150-238) in FP64.
+template <int NV>
+__device__ __forceinline__ void ausmp(const GasF& g, const double* L, const double* R, const double* n, double* F) {
+  constexpr int P = NV - 1;
+  const double beta = 0.125, alpha = 0.1875;
+  const double irl = rcp(L[0]), irr = rcp(R[0]);
+  const double unl = un<NV>(L, n), unr = un<NV>(R, n);
+  const double pol = L[P] * irl, por = R[P] * irr;
+  const double H_L = fma(g.gcp, pol, 0.5 * v2<NV>(L));
+  const double H_R = fma(g.gcp, por, 0.5 * v2<NV>(R));
+  const double a_half = sqrt_(g.gamma * sqrt_(pol * por));   // sqrt(aL aR)
+  const double ia = rcp(a_half);
+  const double ML = unl * ia, MR = unr * ia;
+  const double mL2 = (ML * ML - 1.0), mR2 = (MR * MR - 1.0);
+  const double sub_Mp = fma(0.25 * (ML + 1.0), ML + 1.0, beta * mL2 * mL2);
+  const double sub_pp = fma(0.25 * (ML + 1.0) * (ML + 1.0), 2.0 - ML, alpha * ML * mL2 * mL2);
+  const double sub_Mm = -fma(0.25 * (MR - 1.0), MR - 1.0, beta * mR2 * mR2);
+  const double sub_pm = fma(0.25 * (MR - 1.0) * (MR - 1.0), 2.0 + MR, -alpha * MR * mR2 * mR2);
+  const bool sl = fabs(ML) < 1.0, sr = fabs(MR) < 1.0;
+  const double MplusL = sl ? sub_Mp : 0.5 * (ML + fabs(ML));
+  const double pplusL = sl ? sub_pp : 0.5 * (1.0 + copysign(1.0, ML));
+  const double MminusR = sr ? sub_Mm : 0.5 * (MR - fabs(MR));
+  const double pminusR = sr ? sub_pm : 0.5 * (1.0 - copysign(1.0, MR));
+  const double Mhalf = MplusL + MminusR;
+  const double phalf = fma(pplusL, L[P], pminusR * R[P]);
+  const double mdotp = L[0] * a_half * 0.5 * (Mhalf + fabs(Mhalf));
+  const double mdotm = R[0] * a_half * 0.5 * (Mhalf - fabs(Mhalf));
+  F[0] = mdotp + mdotm;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = fma(mdotp, L[1 + d], fma(mdotm, R[1 + d], n[d] * phalf));
+  F[P] = fma(mdotp, H_L, mdotm * H_R);
+}
+
+// ---- mixed: FP32 wave structure, FP64 upwind flux ----------------------------
+template <int NV>
+__device__ __forceinline__ void hllc_mixed(const GasF& g, const double* L, const double* R, const double* n,
+                                           double* F) {
+  constexpr int P = NV - 1;
+  const float gam = (float)g.gamma, gm1 = (float)g.gm1;
+  float l[5], r[5], nf[3];
+  for (int v = 0; v < NV; ++v) { l[v] = (float)L[v]; r[v] = (float)R[v]; }
+  for (int d = 0; d < 3; ++d) nf[d] = (float)n[d];
+  const float rsl = rsqrtf(l[0]), rsr = rsqrtf(r[0]);
+  const float srL = l[0] * rsl, srR = r[0] * rsr;
+  const float irl = rsl * rsl, irr = rsr * rsr;
+  float unl = l[1] * nf[0] + l[2] * nf[1], unr = r[1] * nf[0] + r[2] * nf[1];
+  float vl2 = l[1] * l[1] + l[2] * l[2], vr2 = r[1] * r[1] + r[2] * r[2];
+  if constexpr (NV == 5) {
+    unl += l[3] * nf[2]; unr += r[3] * nf[2];
+    vl2 += l[3] * l[3]; vr2 += r[3] * r[3];
+  }
+  const float pol = l[P] * irl, por = r[P] * irr;
+  const float aL = sqrtf(gam * pol), aR = sqrtf(gam * por);
+  const float gcp = (float)g.gcp;
+  const float h0l = fmaf(gcp, pol, 0.5f * vl2), h0r = fmaf(gcp, por, 0.5f * vr2);
+  const float isr = __frcp_rn(srL + srR);
+  const float wl = srL * isr, wr = srR * isr;
+  float ur0 = fmaf(wr, r[1], wl * l[1]), ur1 = fmaf(wr, r[2], wl * l[2]), ur2 = 0.0f;
+  if constexpr (NV == 5) ur2 = fmaf(wr, r[3], wl * l[3]);
+  const float h0_roe = fmaf(wr, h0r, wl * h0l);
+  const float a_roe = sqrtf(fmaxf(gm1 * fmaf(-0.5f, ur0 * ur0 + ur1 * ur1 + ur2 * ur2, h0_roe), 0.0f));
+  const float un_roe = ur0 * nf[0] + ur1 * nf[1] + ur2 * nf[2];
+  const float S1 = fminf(fminf(0.0f, unl - aL), un_roe - a_roe);
+  const float S4 = fmaxf(fmaxf(0.0f, unr + aR), un_roe + a_roe);
+  const float ml = l[0] * (S1 - unl), mr = r[0] * (S4 - unr);
+  const float Sstar = __fdividef(r[P] - l[P] + ml * unl - mr * unr, ml - mr);
+  const bool left = (S1 >= 0.0f) || (Sstar >= 0.0f);
+  // FP64 physical flux of the upwind state
+  const double* K = left ? L : R;
+  const double unK = (NV == 5) ? K[1] * n[0] + K[2] * n[1] + K[3] * n[2] : K[1] * n[0] + K[2] * n[1];
+  const double iK = 1.0 / K[0];
+  const double pK = K[P];
+  const double h0K = fma(g.gcp, pK * iK, 0.5 * v2<NV>(K));
+  F[0] = K[0] * unK;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = fma(F[0], K[1 + d], pK * n[d]);
+  F[P] = F[0] * h0K;
+  // FP32 star correction S_K (U*_K - U_K)
+  const bool corr = left ? (S1 < 0.0f) : (S4 > 0.0f);
+  const float SK = left ? S1 : S4;
+  const float* k = left ? l : r;
+  const float mk = left ? ml : mr, unk = left ? unl : unr, rk = k[0];
+  const float pstar = fmaf(l[0] * (unl - S1), unl - Sstar, l[P]);
+  const float inv = __frcp_rn(SK - Sstar);
+  const float dp = pstar - k[P];
+  const float e0k = (left ? h0l : h0r) - k[P] * (left ? irl : irr);
+  float c[5];
+  c[0] = SK * (mk * inv - rk);
+  for (int d = 0; d < NV - 2; ++d) c[1 + d] = SK * (fmaf(mk, k[1 + d], dp * nf[d]) * inv - rk * k[1 + d]);
+  c[P] = SK * ((mk * e0k - k[P] * unk + pstar * Sstar) * inv - rk * e0k);
+  for (int v = 0; v < NV; ++v) F[v] = corr ? F[v] + (double)c[v] : F[v];
+}
+
+template <int NV>
+__device__ __forceinline__ void ausmp_mixed(const GasF& g, const double* L, const double* R, const double* n,
+                                            double* F) {
+  constexpr int P = NV - 1;
+  const float beta = 0.125f, alpha = 0.1875f;
+  float l[5], r[5], nf[3];
+  for (int v = 0; v < NV; ++v) { l[v] = (float)L[v]; r[v] = (float)R[v]; }
+  for (int d = 0; d < 3; ++d) nf[d] = (float)n[d];
+  const float irl = __frcp_rn(l[0]), irr = __frcp_rn(r[0]);
+  float unl = l[1] * nf[0] + l[2] * nf[1], unr = r[1] * nf[0] + r[2] * nf[1];
+  if constexpr (NV == 5) { unl += l[3] * nf[2]; unr += r[3] * nf[2]; }
+  const float a_half = sqrtf((float)g.gamma * sqrtf(l[P] * irl * r[P] * irr));
+  const float ia = __frcp_rn(a_half);
+  const float ML = unl * ia, MR = unr * ia;
+  const float mL2 = ML * ML - 1.0f, mR2 = MR * MR - 1.0f;
+  const bool sl = fabsf(ML) < 1.0f, sr = fabsf(MR) < 1.0f;
+  const float MplusL = sl ? fmaf(0.25f * (ML + 1.0f), ML + 1.0f, beta * mL2 * mL2) : 0.5f * (ML + fabsf(ML));
+  const float pplusL = sl ? fmaf(0.25f * (ML + 1.0f) * (ML + 1.0f), 2.0f - ML, alpha * ML * mL2 * mL2)
+                          : 0.5f * (1.0f + copysignf(1.0f, ML));
+  const float MminusR = sr ? -fmaf(0.25f * (MR - 1.0f), MR - 1.0f, beta * mR2 * mR2) : 0.5f * (MR - fabsf(MR));
+  const float pminusR = sr ? fmaf(0.25f * (MR - 1.0f) * (MR - 1.0f), 2.0f + MR, -alpha * MR * mR2 * mR2)
+                           : 0.5f * (1.0f - copysignf(1.0f, MR));
+  const float Mhalf = MplusL + MminusR;
+  // mass fluxes and pressure in FP32, the transported quantities in FP64
+  const double mdotp = (double)(l[0] * a_half * 0.5f * (Mhalf + fabsf(Mhalf)));
+  const double mdotm = (double)(r[0] * a_half * 0.5f * (Mhalf - fabsf(Mhalf)));
+  const double phalf = (double)pplusL * L[P] + (double)pminusR * R[P];
+  const double H_L = fma(g.gcp, L[P] / L[0], 0.5 * v2<NV>(L));
+  const double H_R = fma(g.gcp, R[P] / R[0], 0.5 * v2<NV>(R));
+  F[0] = mdotp + mdotm;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = fma(mdotp, L[1 + d], fma(mdotm, R[1 + d], n[d] * phalf));
+  F[P] = fma(mdotp, H_L, mdotm * H_R);
+}
+
+// ---- state update (Newstate_Conservative restated, one species) -----------
+// U = (rho, rho u, ..., p/(gamma-1) + rho |u|^2 / 2); p = (gamma-1)(E - rho |u|^2 / 2)
+template <int NV>
+__device__ __forceinline__ bool rk_update(const GasF& g, double* Q, const double* QO, const double* R, double dtv,
+                                          double c, bool first_stage) {
+  constexpr int P = NV - 1;
+  double U[NV], U0[NV];
+  U[0] = Q[0];
+  for (int d = 0; d < NV - 2; ++d) U[1 + d] = Q[0] * Q[1 + d];
+  U[P] = fma(Q[P], g.igm1, 0.5 * Q[0] * v2<NV>(Q));
+  if (first_stage) {
+    for (int v = 0; v < NV; ++v) U[v] = fma(-R[v] * dtv, c, U[v]);
+  } else {
+    U0[0] = QO[0];
+    for (int d = 0; d < NV - 2; ++d) U0[1 + d] = QO[0] * QO[1 + d];
+    U0[P] = fma(QO[P], g.igm1, 0.5 * QO[0] * v2<NV>(QO));
+    for (int v = 0; v < NV; ++v) U[v] = fma(fma(-R[v], dtv, U[v] - U0[v]), c, U0[v]);
+  }
+  const double ir = rcp(U[0]);
+  Q[0] = U[0];
+  double ke = 0.0;
+  for (int d = 0; d < NV - 2; ++d) {
+    Q[1 + d] = U[1 + d] * ir;
+    ke = fma(U[1 + d], Q[1 + d], ke);
+  }
+  Q[P] = g.gm1 * fma(-0.5, ke, U[P]);
+  bool bad = false;
+  for (int v = 0; v < NV; ++v) bad |= isnan(Q[v]);
+  bad |= (Q[P] < 0.0);
+  if (Q[0] < 1e-20) Q[0] = 1e-20;
+  return !bad;
+}
+
+}  // namespace fast
+}  // namespace mose

@@ -1,0 +1,9 @@
+// stage_fp64_r3.cu -- 2-D stage kernels, precision fp64 (MOSE_PRECISION_* = 1),
+// Riemann solver 3 (MOSE_RIEMANN_*).
+#include "stage_inst.cuh"
+
+namespace mose {
+bool launch_stage2d_p1_r3(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s) {
+  return stage2d_dispatch_lim<1, 3>(a, nsm, mode, uni, lim, s);
+}
+}  // namespace mose

@@ -1,0 +1,63 @@
+// stage_inst.cuh -- launch dispatch of the 2-D stage kernel over arithmetic
+// policy, limiter, metric mode and kernel mode.  Each translation unit
+// stage_<precision>_r<solver>.cu instantiates one (precision, Riemann solver)
+// pair.  The residual-only mode (the phase-by-phase C-ABI path) exists for the
+// reference-exact policy with metric arrays; the fused mode has
+// constant-metric variants for uniform grids.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <type_traits>
+
+#include "stage2d.cuh"
+
+namespace mose {
+
+template <int PREC, int RIE, int LIM>
+using StagePolicy = typename std::conditional<PREC == 0, PolExact<RIE, LIM>, PolFast<RIE, LIM, PREC == 2>>::type;
+
+// Persistent grid: as many CTAs as the SMs hold at once (the kernel's
+// register budget decides), never more than there are work items.
+template <int PREC, int RIE, int LIM, bool UNI, int MODE>
+static void launch_persistent(const StageArgs& a, int nsm, cudaStream_t s) {
+  using PH = StagePolicy<PREC, RIE, LIM>;
+  static int occ = 0;   // one per kernel instance
+  if (occ == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage2d<PH, RIE, LIM, UNI, MODE>, STRIP_T, 0) !=
+            cudaSuccess ||
+        occ < 1)
+      occ = 1;
+  }
+  const int grid = a.nitems < occ * nsm ? a.nitems : occ * nsm;
+  k_stage2d<PH, RIE, LIM, UNI, MODE><<<grid, STRIP_T, 0, s>>>(a);
+}
+
+template <int PREC, int RIE, int LIM>
+static bool stage2d_dispatch_uni(const StageArgs& a, int nsm, int mode, bool uni, cudaStream_t s) {
+  if (mode == 1) {
+    if constexpr (PREC == 0) {
+      launch_persistent<PREC, RIE, LIM, false, 1>(a, nsm, s);
+      return true;
+    }
+    return false;
+  }
+  if (uni) launch_persistent<PREC, RIE, LIM, true, 0>(a, nsm, s);
+  else launch_persistent<PREC, RIE, LIM, false, 0>(a, nsm, s);
+  return true;
+}
+
+template <int PREC, int RIE>
+static bool stage2d_dispatch_lim(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s) {
+  switch (lim) {
+    case 0: return stage2d_dispatch_uni<PREC, RIE, 0>(a, nsm, mode, uni, s);
+    case 1: return stage2d_dispatch_uni<PREC, RIE, 1>(a, nsm, mode, uni, s);
+    case 2: return stage2d_dispatch_uni<PREC, RIE, 2>(a, nsm, mode, uni, s);
+    case 3: return stage2d_dispatch_uni<PREC, RIE, 3>(a, nsm, mode, uni, s);
+    case 4: return stage2d_dispatch_uni<PREC, RIE, 4>(a, nsm, mode, uni, s);
+    case 5: return stage2d_dispatch_uni<PREC, RIE, 5>(a, nsm, mode, uni, s);
+  }
+  return false;
+}
+
+}  // namespace mose
