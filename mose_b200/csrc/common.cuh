@@ -18,10 +18,13 @@ namespace mose {
 
 constexpr int GW = 2;  // ghost layers (Global_m.f90:17 gc = 2)
 
-// Stage-kernel strip: STRIP_T threads per CTA own STRIP_W = STRIP_T - 2 cell
-// columns plus one halo column on each side.
-constexpr int STRIP_T = 128;
-constexpr int STRIP_W = STRIP_T - 2;
+// Stage-kernel tiling: a CTA of SB_T threads is SB_X thread columns by SB_Y
+// thread rows.  It owns a strip of at most SB_W = SB_X - 2 cell columns (one
+// halo column each side) and marches up the strip SB_Y rows per batch.
+constexpr int SB_X = 64;
+constexpr int SB_Y = 4;
+constexpr int SB_T = SB_X * SB_Y;
+constexpr int SB_W = SB_X - 2;
 
 // Internal boundary codes (reference bc.txt types in parentheses).
 enum BcCode : int {

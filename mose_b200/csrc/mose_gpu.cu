@@ -59,6 +59,61 @@ struct DevBuf {
   }
 };
 
+// Splits n into parts of nearly equal size, each a multiple of q except the
+// last; returns the part boundaries (parts + 1 values).
+std::vector<int> split_even(int n, int parts, int q) {
+  const int units = (n + q - 1) / q;
+  std::vector<int> cut(parts + 1, 0);
+  for (int p = 0; p < parts; ++p) {
+    const int u = units / parts + (p < units % parts ? 1 : 0);
+    cut[p + 1] = std::min(n, cut[p] + u * q);
+  }
+  cut[parts] = n;
+  return cut;
+}
+
+// Work items of the 2-D stage kernel: (block, c0 | c1 << 16, j0, j1).
+// Every block's columns split into ceil(ni / SB_W) strips of nearly equal
+// width starting on even columns (16-byte aligned row copies); its rows into
+// runs of about H rows in whole batches.  H is the candidate whose
+// round-robin assignment over the persistent grid has the smallest makespan,
+// an item costing its batches plus about two for the prologue and the first
+// copies.
+std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int grid) {
+  auto build = [&](int H) {
+    std::vector<int4> items;
+    for (int b = 0; b < (int)blocks.size(); ++b) {
+      const HostBlock& h = blocks[b];
+      const int ns = (h.ni + SB_W - 1) / SB_W;
+      const std::vector<int> cc = split_even(h.ni, ns, 2);
+      const int nr = std::max(1, (h.nj + H / 2) / H);
+      const std::vector<int> rc = split_even(h.nj, std::min(nr, (h.nj + SB_Y - 1) / SB_Y), SB_Y);
+      for (size_t r = 0; r + 1 < rc.size(); ++r)
+        for (int s = 0; s < ns; ++s)
+          if (rc[r + 1] > rc[r] && cc[s + 1] > cc[s])
+            items.push_back(make_int4(b, cc[s] | (cc[s + 1] << 16), rc[r], rc[r + 1]));
+    }
+    return items;
+  };
+  auto makespan = [&](const std::vector<int4>& items) {
+    std::vector<long long> load(std::max(1, grid), 0);
+    for (size_t i = 0; i < items.size(); ++i)
+      load[i % load.size()] += (items[i].w - items[i].z + SB_Y - 1) / SB_Y + 2;
+    return *std::max_element(load.begin(), load.end());
+  };
+  std::vector<int4> best;
+  long long best_t = -1;
+  for (int H = 16; H <= 512; H += SB_Y) {
+    std::vector<int4> items = build(H);
+    const long long tm = makespan(items);
+    if (best_t < 0 || tm < best_t || (tm == best_t && items.size() < best.size())) {
+      best_t = tm;
+      best.swap(items);
+    }
+  }
+  return best;
+}
+
 }  // namespace
 
 struct mose_gpu_ctx {
@@ -508,16 +563,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if (!gr.empty()) CU(cudaMemcpy(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice));
 
   // ---- work items for the stage kernel -----------------------------------------
-  long long strip_rows = 0;
-  for (auto& h : ctx->hblk) strip_rows += (long long)((h.ni + STRIP_W - 1) / STRIP_W) * h.nj;
-  long long target = (long long)ctx->nsm * 8;
-  int H = (int)std::max<long long>(4, std::min<long long>(256, strip_rows / std::max<long long>(1, target)));
-  std::vector<int4> items;
-  for (int b = 0; b < nb; ++b) {
-    const HostBlock& h = ctx->hblk[b];
-    for (int j0 = 0; j0 < h.nj; j0 += H)
-      for (int c0 = 0; c0 < h.ni; c0 += STRIP_W) items.push_back(make_int4(b, c0, j0, std::min(j0 + H, h.nj)));
-  }
+  std::vector<int4> items = plan_stage_items(ctx->hblk, 2 * ctx->nsm);
   ctx->nitems = (int)items.size();
   CU(ctx->items.alloc(items.size()));
   CU(cudaMemcpy(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));

@@ -1,20 +1,28 @@
 // stage2d.cuh -- fused residual + RK-stage kernel for 2-D blocks (and 1-D run
 // as 2-D with nj = 1), one launch per RK stage over every block.
 //
-// Work decomposition: an item is a strip of STRIP_W = T-2 cell columns of one
-// block and a run of rows.  Thread t owns column c = c0 - 1 + t (one column of
-// halo on each side), so per row:
-//   * every thread forms the limited i-slope of its cell (T-2 cells + 2 halo);
-//   * threads 0..T-2 each form ONE i-face flux F(c+1/2);
-//   * threads 1..T-2 update their cell.
-// The j direction is marched: each thread keeps its column's last j-slope,
-// limited slope and lower j-face flux in registers, so every j-face flux is
-// formed once per strip.  Each interior face flux is therefore computed once
-// (plus one halo face per strip side); the reference computes the same flux
-// with the same operations (Mod_Fluxes.f90:89-139), so results match it
-// bit for bit, and do not depend on the decomposition.  The i-face and
-// j-face Riemann solves of a row are issued together, without a barrier or a
-// branch between them, so the two independent FP64 chains overlap.
+// Work decomposition.  An item is a strip of cell columns [c0, c1) of one
+// block (at most SB_W = 62 columns) and a run of rows [j0, j1).  The CTA is
+// SB_X = 64 thread columns by SB_Y = 4 thread rows; thread (tx, ty) sits on
+// column c = c0 - 1 + tx (one halo column each side) and on row j0 + 4k + ty
+// of batch k.  The CTA marches up the strip one batch of 4 rows at a time:
+//   phase A: the limited i-slope of every cell of the batch (halo columns
+//            included) and the limited j-slope of the row above each cell;
+//   phase B: one i-face flux F(c+1/2) per thread and the j-face flux
+//            G(c, j+1/2) above each owned cell;
+//   phase C: residual assembly and the RK update of the owned cells.
+// The j-slope and the j-face flux of the batch's top row carry into the next
+// batch, so every interior face flux is formed once per strip (plus one halo
+// face per strip side); the reference forms the same flux with the same
+// operations (Mod_Fluxes.f90:89-139), so the exact policy matches it bit for
+// bit whatever the decomposition.
+//
+// Data movement.  State rows stream through a 12-row ring in shared memory
+// (three units of 4 rows: two in use, one in flight) with 16-byte cp.async
+// copies issued one batch ahead, so DRAM latency overlaps the arithmetic and
+// no registers hold prefetched data.  The state at the start of the step (PO)
+// for the next batch is prefetched the same way.  Slopes and face fluxes live
+// in shared memory; one face solve is live per thread at a time.
 //
 // Residual accumulation keeps the reference order per cell: the interior
 // face sweeps first (i-, i+, j-, j+: Mod_Fluxes.f90:89-179), then the
@@ -22,8 +30,8 @@
 // bc list by block and face, Mod_BC_Fluxes.f90:52-216).
 //
 // The arithmetic is a policy: PolExact (the reference's operation order),
-// PolFast (FP64 restated for speed) or PolMixed (FP32 wave structure).
-// Boundary-face fluxes always use the reference-exact formulas.
+// PolFast (FP64 restated for speed) or PolFast<..., true> (FP32 wave
+// structure).  Boundary-face fluxes always use the reference-exact formulas.
 #pragma once
 
 #include "arena.cuh"
@@ -194,39 +202,68 @@ __device__ __forceinline__ void add_bc(ResAcc<NV, COMP>& R, const double* F, dou
   }
 }
 
+// ---- shared memory of the batched march --------------------------------------
+constexpr int SB_RING = 3 * SB_Y;   // ring rows: three units of SB_Y rows
+constexpr int SB_RS = 68;           // ring row stride (doubles): cells c0-2 .. c0+63, 16-byte rows
+constexpr int SB_CH = 33;           // 16-byte chunks per ring row (66 cells)
+constexpr int SB_OCH = SB_W / 2;    // 16-byte chunks of the owned columns of a PO row
+
+// NVR ring planes: the NV state variables, plus dl along i and j with metric arrays.
+template <int NV, int NVR>
+struct StageSmem {
+  double ring[NVR][SB_RING][SB_RS];
+  double po[2][NV][SB_Y][SB_X];       // PO of the owned cells (column c - c0), double buffered
+  double sx[NV][SB_Y][SB_X];          // limited i-slope of cell (c, j)
+  double sy[NV][SB_Y + 1][SB_X];      // limited j-slope of row r: 0 = batch base row (carried)
+  double f[NV][SB_Y][SB_X];           // F(c + 1/2, j)
+  double g[NV][SB_Y + 1][SB_X];       // G(c, j0 + r - 1/2): row 0 carried from the previous batch
+  int fm[SB_Y][SB_X];                 // add masks of F / G
+  int gm[SB_Y + 1][SB_X];
+};
+
+template <bool UNI>
+constexpr size_t stage_smem_bytes() {
+  return sizeof(StageSmem<4, UNI ? 4 : 6>);
+}
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(sdst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // Minimum resident CTAs per SM the register allocation is sized for.
 #ifndef MOSE_STAGE_MIN_CTAS
-#define MOSE_STAGE_MIN_CTAS 3
+#define MOSE_STAGE_MIN_CTAS 2
 #endif
 
 // MODE: 0 = fused (residual + RK update, writes Pn), 1 = residual only (writes R).
 template <class PH, int RIE, int LIM, bool UNI, int MODE>
-__global__ void __launch_bounds__(STRIP_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs a) {
+__global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs a) {
   constexpr int NV = 4;
-  constexpr int T = STRIP_T;
-  __shared__ double sP[NV][T + 2];
-  __shared__ double sDL[T + 2];
-  __shared__ double sSig[NV][T];
-  __shared__ double sF[NV][T];
-  __shared__ int sMask[T];
+  constexpr int NVR = UNI ? NV : NV + 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  StageSmem<NV, NVR>& S = *reinterpret_cast<StageSmem<NV, NVR>*>(smem_raw);
   const int t = threadIdx.x;
+  const int tx = t % SB_X, ty = t / SB_X;
+  const bool need_po = (MODE == 0) && (a.irk != 1);
 
+#pragma unroll 1
   for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
     const int4 item = a.items[it];
-    const int b = item.x, c0 = item.y, j0 = item.z, j1 = item.w;
+    const int b = item.x, c0 = item.y & 0xffff, c1 = item.y >> 16, j0 = item.z, j1 = item.w;
     const BlockDesc& d = a.blk[b];
     const int ni = d.ni, nj = d.nj, px = d.px;
     const long long vs = d.vstride;
     const double* Pc = a.Pc + d.sbase;
     const long long mb = d.mbase;
-    const int c = c0 - 1 + t;
-    const int cend = min(c0 + STRIP_W, ni);
-    const bool colok = (c <= ni + 1);
-    const bool has_face = (t < T - 1) && (c <= cend - 1);
-    const bool has_cell = (t >= 1) && (c < cend);
-    // column used for this thread's loads (threads past the block read its last ghost column)
-    const int cl = min(c, ni + 1);
+    const int c = c0 - 1 + tx;
+    const bool has_face = (tx < SB_X - 1) && (c <= c1 - 1);   // F(c + 1/2)
+    const bool owns = (tx >= 1) && (c < c1);
+    const int nbatch = (j1 - j0 + SB_Y - 1) / SB_Y;
     auto off = [&](int cc, int jj) -> long long { return (long long)(jj + GW) * px + (cc + GW); };
+
     // uniform metric constants
     double u_dlx = 0, u_dly = 0, u_nx[3] = {0, 0, 0}, u_ny[3] = {0, 0, 0}, u_Ax = 0, u_Ay = 0, u_vol = 0;
     double u_ilx = 0, u_ily = 0;
@@ -237,18 +274,6 @@ __global__ void __launch_bounds__(STRIP_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageA
       u_ilx = PH::inv_len(0.5 * (u_dlx + u_dlx));
       u_ily = PH::inv_len(0.5 * (u_dly + u_dly));
     }
-    auto dlx_at = [&](int cc, int jj) -> double {
-      if constexpr (UNI) return u_dlx; else return a.m.dl[3 * mb + 0 * vs + off(cc, jj)];
-    };
-    auto dly_at = [&](int cc, int jj) -> double {
-      if constexpr (UNI) return u_dly; else return a.m.dl[3 * mb + 1 * vs + off(cc, jj)];
-    };
-    // 1/l for l = 0.5 (dl_a + dl_b)
-    auto ilen = [&](double l, double u_il) -> double {
-      if constexpr (!PH::kFast) return 0.0;
-      else if constexpr (UNI) return u_il;
-      else return PH::inv_len(l);
-    };
     auto face_at = [&](int dir, int cc, int jj, double* n) -> double {
       if constexpr (UNI) {
         const double* un = dir == 0 ? u_nx : u_ny;
@@ -260,180 +285,245 @@ __global__ void __launch_bounds__(STRIP_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageA
         return f[3 * vs];
       }
     };
-    auto loadQ = [&](int cc, int jj, double* q) {
-      const long long o = off(cc, jj);
+    // ring access: ring row rr, ring column (cell c0 - 2 + col)
+    auto ringQ = [&](int rr, int col, double* q) {
 #pragma unroll
-      for (int v = 0; v < NV; ++v) q[v] = Pc[v * vs + o];
+      for (int v = 0; v < NV; ++v) q[v] = S.ring[v][rr][col];
     };
-    const bool jwork = has_cell;   // columns that own cells march in j
-    const int cj = jwork ? c : max(0, min(c, ni - 1));   // in-block column for the march of idle threads
+    auto ring_dlx = [&](int rr, int col) -> double {
+      if constexpr (UNI) return u_dlx; else return S.ring[NV][rr][col];
+    };
+    auto ring_dly = [&](int rr, int col) -> double {
+      if constexpr (UNI) return u_dly; else return S.ring[NV + 1][rr][col];
+    };
+    // 1/l for l = 0.5 (dl_a + dl_b)
+    auto ilen = [&](double l, double u_il) -> double {
+      if constexpr (!PH::kFast) return 0.0;
+      else if constexpr (UNI) return u_il;
+      else return PH::inv_len(l);
+    };
+    // limited j-slope of the cell at ring row rr (rows rr-1, rr, rr+1), ring column col
+    auto slope_j = [&](int rm, int rr, int rp, int col, double* s) {
+      const double la = 0.5 * (ring_dly(rm, col) + ring_dly(rr, col));
+      const double lb = 0.5 * (ring_dly(rr, col) + ring_dly(rp, col));
+      const double ila = ilen(la, u_ily), ilb = ilen(lb, u_ily);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) {
+        const double q = S.ring[v][rr][col];
+        const double sa = PH::slope(q - S.ring[v][rm][col], la, ila);
+        const double sb = PH::slope(S.ring[v][rp][col] - q, lb, ilb);
+        s[v] = PH::lim(sb, sa);
+      }
+    };
 
-    // ---- j-march preamble: slopes and the j-face below the first row -------
-    double q0[NV], q1[NV], sig0[NV], shalf[NV], Gm[NV];
-    int Gmask = ADD_ALL;
-    double dy0 = 0, dy1 = 0;
-    {
-      double qm2[NV], qm1[NV];
-      loadQ(cj, j0 - 2, qm2);
-      loadQ(cj, j0 - 1, qm1);
-      loadQ(cj, j0, q0);
-      loadQ(cj, j0 + 1, q1);
-      double dym2 = dly_at(cj, j0 - 2), dym1 = dly_at(cj, j0 - 1);
-      dy0 = dly_at(cj, j0); dy1 = dly_at(cj, j0 + 1);
-      double la = 0.5 * (dym2 + dym1), lb = 0.5 * (dym1 + dy0), lc = 0.5 * (dy0 + dy1);
-      double ila = ilen(la, u_ily), ilb = ilen(lb, u_ily), ilc = ilen(lc, u_ily);
-      double sigm1[NV];
+    // unit u = rows j0 - 2 + 4u .. + 3 into ring rows 4 (u % 3) ..
+    auto load_unit = [&](int u) {
+      const int slot = (u % 3) * SB_Y;
+      const int rbase = j0 - 2 + SB_Y * u;
+      constexpr int n = NVR * SB_Y * SB_CH;
+      for (int e = t; e < n; e += SB_T) {
+        const int pv = e / (SB_Y * SB_CH);
+        const int rem = e - pv * (SB_Y * SB_CH);
+        const int i = rem / SB_CH;
+        const int q = rem - i * SB_CH;
+        const int r = rbase + i;
+        const int x = c0 + 2 * q;   // padded column of cell c0 - 2 + 2q
+        if (r > nj + 1 || x >= px) continue;
+        const double* plane;
+        if (pv < NV) plane = Pc + pv * vs;
+        else plane = a.m.dl + 3 * mb + (pv - NV) * vs;
+        cp_async16(&S.ring[pv][slot + i][2 * q], plane + (long long)(r + GW) * px + x);
+      }
+    };
+    // PO of batch kk (rows j0 + 4 kk .., owned columns) into po[kk & 1]
+    auto load_po = [&](int kk) {
+      const double* Po = a.Po + d.sbase;
+      const int rbase = j0 + SB_Y * kk;
+      constexpr int n = NV * SB_Y * SB_OCH;
+      for (int e = t; e < n; e += SB_T) {
+        const int v = e / (SB_Y * SB_OCH);
+        const int rem = e - v * (SB_Y * SB_OCH);
+        const int i = rem / SB_OCH;
+        const int q = rem - i * SB_OCH;
+        const int r = rbase + i;
+        const int x = c0 + GW + 2 * q;   // padded column of cell c0 + 2q
+        if (r >= j1 || x >= px) continue;
+        cp_async16(&S.po[kk & 1][v][i][2 * q], Po + v * vs + (long long)(r + GW) * px + x);
+      }
+    };
+
+    // ---- prologue: j-slopes of rows j0-1, j0 and the j-face below row j0 --------
+    load_unit(0);
+    load_unit(1);
+    if (need_po) load_po(0);
+    cp_async_commit();
+    cp_async_wait_all();
+    __syncthreads();
+    if (ty < 2 && owns) {
+      // ty 0: row j0 - 1 (ring row 1) -> sy[1]; ty 1: row j0 (ring row 2) -> sy[0]
+      double s[NV];
+      slope_j(ty, ty + 1, ty + 2, tx + 1, s);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) S.sy[v][1 - ty][tx] = s[v];
+    }
+    __syncthreads();
+    if (ty == 0 && owns) {
+      double qm[NV], q0[NV], QL[NV], QR[NV], G[NV], n[3];
+      ringQ(1, tx + 1, qm);
+      ringQ(2, tx + 1, q0);
+      const double lm = 0.5 * ring_dly(1, tx + 1), lp = 0.5 * ring_dly(2, tx + 1);
 #pragma unroll
       for (int v = 0; v < NV; ++v) {
-        double sa = PH::slope(qm1[v] - qm2[v], la, ila);
-        double sb = PH::slope(q0[v] - qm1[v], lb, ilb);
-        double sc = PH::slope(q1[v] - q0[v], lc, ilc);
-        sigm1[v] = PH::lim(sb, sa);
-        sig0[v] = PH::lim(sc, sb);
-        shalf[v] = sc;
+        QL[v] = qm[v] + S.sy[v][1][tx] * lm;
+        QR[v] = q0[v] - S.sy[v][0][tx] * lp;
       }
-      double n[3];
-      double A = face_at(1, cj, j0, n);
-      double QL[NV], QR[NV];
-      double lm = 0.5 * dym1, lp = 0.5 * dy0;
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        QL[v] = qm1[v] + sigm1[v] * lm;
-        QR[v] = q0[v] - sig0[v] * lp;
-      }
-      bool ok = PH::template face<NV>(a.g, QL, QR, n, A, Gm);
-      if (!ok && jwork && j0 > 0) report(a.err, 4, b, c, j0, 0);
-      if (j0 == 0 && jwork) {
-        int w = a.bcw[d.bcoff[2] + c];
+      const double A = face_at(1, c, j0, n);
+      const bool ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+      if (!ok && j0 > 0) report(a.err, 4, b, c, j0, 0);
+      int mask = ADD_ALL;
+      if (j0 == 0) {
+        const int w = a.bcw[d.bcoff[2] + c];
         if (bc_code(w) == BC_NONE) {
-          for (int v = 0; v < NV; ++v) Gm[v] = 0.0;
-          Gmask = ADD_NONE;
+          for (int v = 0; v < NV; ++v) G[v] = 0.0;
+          mask = ADD_NONE;
         } else if (bc_code(w) != BC_CONN) {
-          Gmask = boundary_flux<RIE, LIM, NV>(a, w, q0, q1, dy0, dy1, n, A, 3, Gm);
+          double q1[NV];
+          ringQ(3, tx + 1, q1);
+          mask = boundary_flux<RIE, LIM, NV>(a, w, q0, q1, ring_dly(2, tx + 1), ring_dly(3, tx + 1), n, A, 3, G);
         }
       }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) S.g[v][SB_Y][tx] = G[v];
+      S.gm[SB_Y][tx] = mask;
     }
 
-    for (int j = j0; j < j1; ++j) {
-      // ---- rows in: own column of row j+2 (march), row j into shared memory --
-      double q2[NV];
-      loadQ(cj, j + 2, q2);
-      const double dy2 = dly_at(cj, j + 2);
-      __syncthreads();   // previous row's readers of sP / sSig / sF are done
-      if (colok) {
-        if (jwork) {
+#pragma unroll 1
+    for (int k = 0; k < nbatch; ++k) {
+      cp_async_wait_all();
+      __syncthreads();   // ring units k, k+1 and po[k & 1] visible; batch k-1 done with everything
+      if (k + 2 <= nbatch) load_unit(k + 2);
+      if (need_po && k + 1 < nbatch) load_po(k + 1);
+      cp_async_commit();
+      const int j = j0 + SB_Y * k + ty;
+      const bool rowok = j < j1;
+      const int rr = (SB_Y * k + ty + 2) % SB_RING;   // ring row of row j
+      const int rm = (rr + SB_RING - 1) % SB_RING;
+      const int rp = (rr + 1) % SB_RING, rp2 = (rr + 2) % SB_RING;
+      const int col = tx + 1;                         // ring column of cell c
+
+      // ---- phase A: limited slopes ------------------------------------------------
+      if (ty == 0 && owns) {   // carry the previous batch's top j-face
 #pragma unroll
-          for (int v = 0; v < NV; ++v) sP[v][t + 1] = q0[v];
-        } else {
-          double q[NV];
-          loadQ(cl, j, q);
-#pragma unroll
-          for (int v = 0; v < NV; ++v) sP[v][t + 1] = q[v];
-        }
-        sDL[t + 1] = dlx_at(cl, j);
+        for (int v = 0; v < NV; ++v) S.g[v][0][tx] = S.g[v][SB_Y][tx];
+        S.gm[0][tx] = S.gm[SB_Y][tx];
       }
-      if (t == 0) {
-        double q[NV];
-        loadQ(c0 - 2, j, q);
+      if (rowok) {
+        {
+          const double dm = ring_dlx(rr, col - 1), d0 = ring_dlx(rr, col), dp = ring_dlx(rr, col + 1);
+          const double la = 0.5 * (dm + d0), lb = 0.5 * (d0 + dp);
+          const double ila = ilen(la, u_ilx), ilb = ilen(lb, u_ilx);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sP[v][0] = q[v];
-        sDL[0] = dlx_at(c0 - 2, j);
-      }
-      if (t == T - 1 && c0 + T - 1 <= ni + 1) {
-        double q[NV];
-        loadQ(c0 + T - 1, j, q);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) sP[v][T + 1] = q[v];
-        sDL[T + 1] = dlx_at(c0 + T - 1, j);
-      }
-      __syncthreads();
-      // ---- limited slopes: i of row j (shared), j of row j+1 (marched) -------
-      double sig1[NV], sup[NV];
-      {
-        const double lu = 0.5 * (dy1 + dy2);
-        const double ilu = ilen(lu, u_ily);
-        const double lmn = 0.5 * (sDL[t] + sDL[t + 1]);
-        const double lpl = 0.5 * (sDL[t + 1] + sDL[t + 2]);
-        const double ilmn = ilen(lmn, u_ilx), ilpl = ilen(lpl, u_ilx);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          sup[v] = PH::slope(q2[v] - q1[v], lu, ilu);
-          sig1[v] = PH::lim(sup[v], shalf[v]);
-          double sm = PH::slope(sP[v][t + 1] - sP[v][t], lmn, ilmn);
-          double sp = PH::slope(sP[v][t + 2] - sP[v][t + 1], lpl, ilpl);
-          sSig[v][t] = PH::lim(sp, sm);
-        }
-      }
-      __syncthreads();
-      // ---- face fluxes: F(c+1/2, j) and G(c, j+1/2), issued together ---------
-      double F[NV], Gp[NV];
-      int mask = ADD_ALL, Gpmask = ADD_ALL;
-      {
-        double nf[3], ng[3];
-        const double Af = face_at(0, min(c + 1, ni + 1), j, nf);
-        const double Ag = face_at(1, cj, j + 1, ng);
-        double QLf[NV], QRf[NV], QLg[NV], QRg[NV];
-        const double lmf = 0.5 * sDL[t + 1], lpf = 0.5 * sDL[min(t + 2, T + 1)];
-        const double lmg = 0.5 * dy0, lpg = 0.5 * dy1;
-        const int tn = min(t + 1, T - 1);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          QLf[v] = sP[v][t + 1] + sSig[v][t] * lmf;
-          QRf[v] = sP[v][min(t + 2, T + 1)] - sSig[v][tn] * lpf;
-          QLg[v] = q0[v] + sig0[v] * lmg;
-          QRg[v] = q1[v] - sig1[v] * lpg;
-        }
-        const bool okf = PH::template face<NV>(a.g, QLf, QRf, nf, Af, F);
-        const bool okg = PH::template face<NV>(a.g, QLg, QRg, ng, Ag, Gp);
-        const bool lowb = (c == -1), highb = (c == ni - 1);
-        if (!okf && has_face && !lowb && !highb) report(a.err, 4, b, c, j, 0);
-        if (!okg && jwork && j < nj - 1) report(a.err, 4, b, c, j, 0);
-        // boundary faces: the reference's BC_Fluxes formulas override
-        if (has_face && (lowb || highb)) {
-          const int w = a.bcw[d.bcoff[lowb ? 0 : 1] + j];
-          if (bc_code(w) == BC_NONE) {
-            for (int v = 0; v < NV; ++v) F[v] = 0.0;
-            mask = ADD_NONE;
-          } else if (bc_code(w) != BC_CONN) {
-            double Q[NV], Qi[NV];
-            const int tb = lowb ? t + 2 : t + 1, ti = lowb ? t + 3 : t;   // boundary / interior column
-            for (int v = 0; v < NV; ++v) { Q[v] = sP[v][tb]; Qi[v] = sP[v][ti]; }
-            mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, sDL[tb], sDL[ti], nf, Af, lowb ? 1 : 2, F);
+          for (int v = 0; v < NV; ++v) {
+            const double q = S.ring[v][rr][col];
+            const double sa = PH::slope(q - S.ring[v][rr][col - 1], la, ila);
+            const double sb = PH::slope(S.ring[v][rr][col + 1] - q, lb, ilb);
+            S.sx[v][ty][tx] = PH::lim(sb, sa);
           }
         }
-        if (jwork && j == nj - 1) {
-          const int w = a.bcw[d.bcoff[3] + c];
-          if (bc_code(w) == BC_NONE) {
-            for (int v = 0; v < NV; ++v) Gp[v] = 0.0;
-            Gpmask = ADD_NONE;
-          } else if (bc_code(w) != BC_CONN) {
-            double qin[NV];
-            loadQ(c, j - 1, qin);
-            Gpmask = boundary_flux<RIE, LIM, NV>(a, w, q0, qin, dy0, dly_at(c, j - 1), ng, Ag, 4, Gp);
-          }
+        if (owns) {
+          double s[NV];
+          slope_j(rr, rp, rp2, col, s);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) S.sy[v][ty + 1][tx] = s[v];
         }
       }
-      if (has_face) {
+      __syncthreads();
+
+      // ---- phase B: face fluxes -----------------------------------------------------
+      if (rowok) {
+        if (has_face) {
+          double QL[NV], QR[NV], F[NV], n[3];
+          const double lm = 0.5 * ring_dlx(rr, col), lp = 0.5 * ring_dlx(rr, col + 1);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) sF[v][t] = F[v];
-        sMask[t] = mask;
+          for (int v = 0; v < NV; ++v) {
+            QL[v] = S.ring[v][rr][col] + S.sx[v][ty][tx] * lm;
+            QR[v] = S.ring[v][rr][col + 1] - S.sx[v][ty][tx + 1] * lp;
+          }
+          const double A = face_at(0, c + 1, j, n);
+          const bool ok = PH::template face<NV>(a.g, QL, QR, n, A, F);
+          const bool lowb = (c == -1), highb = (c == ni - 1);
+          int mask = ADD_ALL;
+          if (!ok && !lowb && !highb) report(a.err, 4, b, c, j, 0);
+          if (lowb || highb) {
+            const int w = a.bcw[d.bcoff[lowb ? 0 : 1] + j];
+            if (bc_code(w) == BC_NONE) {
+              for (int v = 0; v < NV; ++v) F[v] = 0.0;
+              mask = ADD_NONE;
+            } else if (bc_code(w) != BC_CONN) {
+              double Q[NV], Qi[NV];
+              const int cb = lowb ? col + 1 : col, ci = lowb ? col + 2 : col - 1;   // boundary / interior cell
+              ringQ(rr, cb, Q);
+              ringQ(rr, ci, Qi);
+              mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, ring_dlx(rr, cb), ring_dlx(rr, ci), n, A,
+                                                 lowb ? 1 : 2, F);
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) S.f[v][ty][tx] = F[v];
+          S.fm[ty][tx] = mask;
+        }
+        if (owns) {
+          double QL[NV], QR[NV], G[NV], n[3];
+          const double lm = 0.5 * ring_dly(rr, col), lp = 0.5 * ring_dly(rp, col);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            QL[v] = S.ring[v][rr][col] + S.sy[v][ty][tx] * lm;
+            QR[v] = S.ring[v][rp][col] - S.sy[v][ty + 1][tx] * lp;
+          }
+          const double A = face_at(1, c, j + 1, n);
+          const bool ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+          int mask = ADD_ALL;
+          if (!ok && j < nj - 1) report(a.err, 4, b, c, j, 0);
+          if (j == nj - 1) {
+            const int w = a.bcw[d.bcoff[3] + c];
+            if (bc_code(w) == BC_NONE) {
+              for (int v = 0; v < NV; ++v) G[v] = 0.0;
+              mask = ADD_NONE;
+            } else if (bc_code(w) != BC_CONN) {
+              double Q[NV], Qi[NV];
+              ringQ(rr, col, Q);
+              ringQ(rm, col, Qi);
+              mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, ring_dly(rr, col), ring_dly(rm, col), n, A, 4, G);
+            }
+          }
+#pragma unroll
+          for (int v = 0; v < NV; ++v) S.g[v][ty + 1][tx] = G[v];
+          S.gm[ty + 1][tx] = mask;
+        }
       }
       __syncthreads();
-      if (has_cell) {
+
+      // ---- phase C: residual and update ---------------------------------------------
+      if (rowok && owns) {
         ResAcc<NV, PH::kCompensated> R;
         R.init();
         const bool bi0 = (c == 0), bi1 = (c == ni - 1), bj0 = (j == 0), bj1 = (j == nj - 1);
-        double Fm[NV];
+        double Fm[NV], Fp[NV], Gm[NV], Gp[NV];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Fm[v] = sF[v][t - 1];
+        for (int v = 0; v < NV; ++v) {
+          Fm[v] = S.f[v][ty][tx - 1];
+          Fp[v] = S.f[v][ty][tx];
+          Gm[v] = S.g[v][ty][tx];
+          Gp[v] = S.g[v][ty + 1][tx];
+        }
         if (!bi0) for (int v = 0; v < NV; ++v) R.add(v, -Fm[v]);
-        if (!bi1) for (int v = 0; v < NV; ++v) R.add(v, F[v]);
+        if (!bi1) for (int v = 0; v < NV; ++v) R.add(v, Fp[v]);
         if (!bj0) for (int v = 0; v < NV; ++v) R.add(v, -Gm[v]);
         if (!bj1) for (int v = 0; v < NV; ++v) R.add(v, Gp[v]);
-        if (bi0) add_bc<NV>(R, Fm, -1.0, sMask[t - 1]);
-        if (bi1) add_bc<NV>(R, F, 1.0, mask);
-        if (bj0) add_bc<NV>(R, Gm, -1.0, Gmask);
-        if (bj1) add_bc<NV>(R, Gp, 1.0, Gpmask);
+        if (bi0) add_bc<NV>(R, Fm, -1.0, S.fm[ty][tx - 1]);
+        if (bi1) add_bc<NV>(R, Fp, 1.0, S.fm[ty][tx]);
+        if (bj0) add_bc<NV>(R, Gm, -1.0, S.gm[ty][tx]);
+        if (bj1) add_bc<NV>(R, Gp, 1.0, S.gm[ty + 1][tx]);
         double Rv[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
@@ -445,33 +535,28 @@ __global__ void __launch_bounds__(STRIP_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageA
         } else {
           double vol;
           if constexpr (UNI) vol = u_vol; else vol = a.m.vol[mb + o];
-          double dt = a.time_accurate ? *a.dtg : a.dtl[mb + o];
+          const double dt = a.time_accurate ? *a.dtg : a.dtl[mb + o];
           double Q[NV], QO[NV];
-#pragma unroll
-          for (int v = 0; v < NV; ++v) Q[v] = q0[v];
+          ringQ(rr, col, Q);
           const bool first = (a.irk == 1);
           if (!first) {
-            const double* Po = a.Po + d.sbase;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) QO[v] = Po[v * vs + o];
+            for (int v = 0; v < NV; ++v) QO[v] = S.po[k & 1][v][ty][tx - 1];
           }
-          bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
+          const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
           if (!ok) report(a.err, 5, b, c, j, 0);
           double* Pn = a.Pn + d.sbase;
 #pragma unroll
           for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
         }
       }
-      // ---- advance the j-march ----------------------------------------------
+      if (ty == SB_Y - 1 && owns) {   // carry the top row's j-slope
 #pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        q0[v] = q1[v]; q1[v] = q2[v];
-        sig0[v] = sig1[v]; shalf[v] = sup[v]; Gm[v] = Gp[v];
+        for (int v = 0; v < NV; ++v) S.sy[v][0][tx] = S.sy[v][SB_Y][tx];
       }
-      Gmask = Gpmask;
-      dy0 = dy1; dy1 = dy2;
     }
-    __syncthreads();
+    cp_async_wait_all();
+    __syncthreads();   // the next item refills the ring
   }
 }
 

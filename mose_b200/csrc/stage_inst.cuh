@@ -17,20 +17,22 @@ namespace mose {
 template <int PREC, int RIE, int LIM>
 using StagePolicy = typename std::conditional<PREC == 0, PolExact<RIE, LIM>, PolFast<RIE, LIM, PREC == 2>>::type;
 
-// Persistent grid: as many CTAs as the SMs hold at once (the kernel's
-// register budget decides), never more than there are work items.
+// Persistent grid: as many CTAs as the SMs hold at once (registers and the
+// shared-memory ring decide), never more than there are work items.
 template <int PREC, int RIE, int LIM, bool UNI, int MODE>
 static void launch_persistent(const StageArgs& a, int nsm, cudaStream_t s) {
   using PH = StagePolicy<PREC, RIE, LIM>;
+  constexpr size_t smem = stage_smem_bytes<UNI>();
   static int occ = 0;   // one per kernel instance
   if (occ == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage2d<PH, RIE, LIM, UNI, MODE>, STRIP_T, 0) !=
+    cudaFuncSetAttribute(k_stage2d<PH, RIE, LIM, UNI, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage2d<PH, RIE, LIM, UNI, MODE>, SB_T, smem) !=
             cudaSuccess ||
         occ < 1)
       occ = 1;
   }
   const int grid = a.nitems < occ * nsm ? a.nitems : occ * nsm;
-  k_stage2d<PH, RIE, LIM, UNI, MODE><<<grid, STRIP_T, 0, s>>>(a);
+  k_stage2d<PH, RIE, LIM, UNI, MODE><<<grid, SB_T, smem, s>>>(a);
 }
 
 template <int PREC, int RIE, int LIM>
