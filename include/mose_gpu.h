@@ -206,6 +206,15 @@ int64_t mose_gpu_launch_count(const mose_gpu_ctx* ctx);
 int mose_gpu_download_metrics(mose_gpu_ctx* ctx, int32_t b, double* vol, double* dl);
 int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N, double* A);
 
+/* Self-check of the restated FP64 reciprocal, reciprocal square root and
+ * square root of the "fp64" and "mixed" precisions over n seeded inputs
+ * spread over [2^-60, 2^60) on the current device.  out[0..2]: the largest
+ * relative error of 1/x, 1/sqrt(x), sqrt(x) in units of 2^-53 (half an ulp
+ * at the top of a binade), measured through exact FMA residuals; out[3]: the
+ * largest distance in ulps between the restated sqrt(x) and the correctly
+ * rounded one.  No context needed; synchronous. */
+int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
+
 #ifdef __cplusplus
 }
 #endif

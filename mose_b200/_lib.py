@@ -69,6 +69,7 @@ SIGNATURES = {
     "mose_gpu_launch_count": (C.c_int64, [_D]),
     "mose_gpu_download_metrics": (C.c_int, [_D, C.c_int32, _dp, _dp]),
     "mose_gpu_download_faces": (C.c_int, [_D, C.c_int32, C.c_int32, _dp, _dp]),
+    "mose_gpu_check_fast_math": (C.c_int, [C.c_int64, C.c_uint64, _dp]),
 }
 
 

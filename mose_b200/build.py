@@ -30,6 +30,7 @@ UNITS = {
     **{f"stage_mixed_r{r}.cu": [] for r in range(4)},
     "mose_gpu.cu": [],
     "norms_noalloc.cu": [],
+    "fastmath_check.cu": [],
 }
 
 

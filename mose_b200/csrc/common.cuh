@@ -45,6 +45,10 @@ struct DevError {
 struct Gas {
   double gamma, R, cp, cv;
   double cpmR;      // 0.5*(cp+cp) - R, as roe_averages forms it
+  // constants of the restated (fast) arithmetic, formed once on the host
+  double gm1;       // gamma - 1
+  double gcp;       // gamma / (gamma - 1)
+  double igm1;      // 1 / (gamma - 1)
 };
 
 // Per-block descriptor (device resident).

@@ -283,6 +283,9 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   ctx->gas.cp = cfg->gamma * cfg->rgas / (cfg->gamma - 1.0);
   ctx->gas.cv = cfg->rgas / (cfg->gamma - 1.0);
   ctx->gas.cpmR = 0.5 * (ctx->gas.cp + ctx->gas.cp) - ctx->gas.R;
+  ctx->gas.gm1 = cfg->gamma - 1.0;
+  ctx->gas.gcp = cfg->gamma / (cfg->gamma - 1.0);
+  ctx->gas.igm1 = 1.0 / (cfg->gamma - 1.0);
   *out = ctx;
   return MOSE_OK;
 }

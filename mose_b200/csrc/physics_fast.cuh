@@ -22,27 +22,29 @@
 namespace mose {
 namespace fast {
 
-// ---- reciprocal / reciprocal square root by Newton-Raphson ------------------
-// Seed from the hardware approximation of the leading bits (about 2^-23
-// relative error), two Newton-Raphson steps (error squares per step: 2^-46,
-// then below one ulp).  Markstein, IBM J. Res. Dev. 34 (1990); Muller et al.,
-// Handbook of Floating-Point Arithmetic, ch. 4.  Valid for normal, finite x.
+// ---- reciprocal / reciprocal square root ------------------------------------
+// Seed from the hardware approximation of the leading bits, then ONE
+// third-order (Householder) correction, which cubes the seed's relative
+// error d: with e = 1 - x r (= d),
+//   1/x       = r (1 + e + e^2 + ...)          -> r + r (e + e^2)
+//   1/sqrt(x) = y (1 + e/2 + 3 e^2 / 8 + ...)  with e = 1 - x y^2
+// (Householder, The Numerical Treatment of a Single Nonlinear Equation,
+// 1970; Muller et al., Handbook of Floating-Point Arithmetic, ch. 4).  A seed
+// good to 2^-18 or better leaves the cubic term below 2^-54, so the result is
+// within about one ulp; the accuracy is checked on the device against IEEE
+// division and square root.  Valid for normal, finite, positive x (rcp: any
+// normal x).
 __device__ __forceinline__ double rcp(double x) {
   double r;
   asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-  double e = fma(-x, r, 1.0);
-  r = fma(r, e, r);
-  e = fma(-x, r, 1.0);
-  return fma(r, e, r);
+  const double e = fma(-x, r, 1.0);
+  return fma(r, fma(e, e, e), r);
 }
 __device__ __forceinline__ double rsqrt_(double x) {
   double y;
   asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-  // y <- y + y (1 - x y^2) / 2
-  double e = fma(-x * y, y, 1.0);
-  y = fma(0.5 * y, e, y);
-  e = fma(-x * y, y, 1.0);
-  return fma(0.5 * y, e, y);
+  const double e = fma(-x * y, y, 1.0);
+  return fma(y * e, fma(0.375, e, 0.5), y);
 }
 // sqrt(x) = x rsqrt(x) with one residual correction; sqrt(0) = 0.
 __device__ __forceinline__ double sqrt_(double x) {
@@ -54,56 +56,80 @@ __device__ __forceinline__ double sqrt_(double x) {
 }
 __device__ __forceinline__ double div_(double a, double b) { return a * rcp(b); }
 
-// ---- limiters: phi(r) x with r = y/(x + 1e-30), one division each ----------
+// ---- limiters: phi(r) x with r = y/(x + 1e-30), one reciprocal each --------
+// The rational limiters are rewritten over a common denominator, which is
+// positive whenever x + 1e-30 != 0 (the only x the reference divides by).
 template <int LIM>
 __device__ __forceinline__ double limiter(double x, double y) {
   if constexpr (LIM == 1) {            // minmod
     double r = (fabs(x) > fabs(y)) ? y : x;
     return (x * y < 0.0) ? 0.0 : r;
   } else if constexpr (LIM == 2) {     // van Leer: x (y sgn(x') + |y|) / (|x'| + |y|)
-    double xp = x + 1e-30;
-    double num = y * copysign(1.0, xp) + fabs(y);
-    double den = fabs(xp) + fabs(y);
-    return x * num / den;
+    const double xp = x + 1e-30;
+    const double num = y * copysign(1.0, xp) + fabs(y);
+    return (x * num) * rcp(fabs(xp) + fabs(y));
   } else if constexpr (LIM == 3) {     // van Albada: x (y^2 + y x') / (x'^2 + y^2)
-    double xp = x + 1e-30;
-    double num = y * (y + xp);
-    double den = fma(xp, xp, y * y);
-    return x * num / den;
+    const double xp = x + 1e-30;
+    const double num = y * (y + xp);
+    return (x * num) * rcp(fma(xp, xp, y * y));
   } else if constexpr (LIM == 4) {     // MC
-    double ru = y / (x + 1e-30);
+    const double ru = y * rcp(x + 1e-30);
     return fmax(0.0, fmin(fmin(2.0 * ru, 0.5 * (1.0 + ru)), 2.0)) * x;
   } else if constexpr (LIM == 5) {     // superbee
-    double ru = y / (x + 1e-30);
+    const double ru = y * rcp(x + 1e-30);
     return fmax(fmax(0.0, fmin(2.0 * ru, 1.0)), fmin(ru, 2.0)) * x;
   } else {
     return 0.0;
   }
 }
+
+// ---- FP32 building blocks ---------------------------------------------------
+// Single-instruction approximations (relative error about 2^-22 / 2^-23):
+// the FP32 Riemann solve is an approximation of the FP64 one by design, and
+// its error against the FP64 oracle is measured, not assumed.
+__device__ __forceinline__ float frcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ float frsq(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+// sqrt(x) for x > 0 (x rsqrt(x))
+__device__ __forceinline__ float fsqrtp(float x) { return x * frsq(x); }
+
+// FP32 limiters.  The denominator is floored at FLT_MIN: where it would be
+// zero the numerator is zero too, and 0 * (1 / FLT_MIN) = 0.
 template <int LIM>
 __device__ __forceinline__ float limiter32(float x, float y) {
+  constexpr float kMin = 1.17549435e-38f;
   if constexpr (LIM == 1) {
     float r = (fabsf(x) > fabsf(y)) ? y : x;
     return (x * y < 0.0f) ? 0.0f : r;
   } else if constexpr (LIM == 2) {
-    float xp = x + 1e-30f;
-    float num = y * copysignf(1.0f, xp) + fabsf(y);
-    float den = fabsf(xp) + fabsf(y);
-    return den > 0.0f ? __fdividef(x * num, den) : 0.0f;
+    const float xp = x + 1e-30f;
+    const float num = y * copysignf(1.0f, xp) + fabsf(y);
+    return (x * num) * frcp(fmaxf(fabsf(xp) + fabsf(y), kMin));
   } else if constexpr (LIM == 3) {
-    float xp = x + 1e-30f;
-    float num = y * (y + xp);
-    float den = fmaf(xp, xp, y * y);
-    return den > 0.0f ? __fdividef(x * num, den) : 0.0f;
+    const float xp = x + 1e-30f;
+    const float num = y * (y + xp);
+    return (x * num) * frcp(fmaxf(fmaf(xp, xp, y * y), kMin));
   } else if constexpr (LIM == 4) {
-    float ru = __fdividef(y, x + 1e-30f);
+    const float ru = y * frcp(x + 1e-30f);
     return fmaxf(0.0f, fminf(fminf(2.0f * ru, 0.5f * (1.0f + ru)), 2.0f)) * x;
   } else if constexpr (LIM == 5) {
-    float ru = __fdividef(y, x + 1e-30f);
+    const float ru = y * frcp(x + 1e-30f);
     return fmaxf(fmaxf(0.0f, fminf(2.0f * ru, 1.0f)), fminf(ru, 2.0f)) * x;
   } else {
     return 0.0f;
   }
+}
+template <int LIM>
+__device__ __forceinline__ float4 limiter32x4(float4 x, float4 y) {
+  return make_float4(limiter32<LIM>(x.x, y.x), limiter32<LIM>(x.y, y.y), limiter32<LIM>(x.z, y.z),
+                     limiter32<LIM>(x.w, y.w));
 }
 
 struct GasF {
@@ -113,9 +139,9 @@ struct GasF {
 __device__ __forceinline__ GasF gasf(const Gas& g) {
   GasF f;
   f.gamma = g.gamma;
-  f.gm1 = g.gamma - 1.0;
-  f.gcp = g.gamma / (g.gamma - 1.0);
-  f.igm1 = 1.0 / (g.gamma - 1.0);
+  f.gm1 = g.gm1;
+  f.gcp = g.gcp;
+  f.igm1 = g.igm1;
   return f;
 }
 
@@ -309,6 +335,93 @@ __device__ __forceinline__ void ausmp_mixed(const GasF& g, const double* L, cons
   F[P] = fma(mdotp, H_L, mdotm * H_R);
 }
 
+// ---- complete FP32 face solves (2-D: states (rho, u, v, p), normal (nx, ny)) --
+struct GasF32 {
+  float gamma, gm1, gcp;   // gamma, gamma - 1, gamma / (gamma - 1)
+};
+__device__ __forceinline__ GasF32 gasf32(const Gas& g) {
+  GasF32 f;
+  f.gamma = (float)g.gamma;
+  f.gm1 = (float)g.gm1;
+  f.gcp = (float)g.gcp;
+  return f;
+}
+
+// Batten HLLC (Lib_Riemann_HLL.f90:147-258) in FP32, flux per unit area.
+// The star correction S_K (U*_K - U_K) is added with the factor S_K folded
+// into a select, so the solve is branch free.
+__device__ __forceinline__ void hllc32(const GasF32& g, float4 L, float4 R, float nx, float ny, float* F) {
+  const float rsl = frsq(L.x), rsr = frsq(R.x);
+  const float srL = L.x * rsl, srR = R.x * rsr;            // sqrt(rho)
+  const float irl = rsl * rsl, irr = rsr * rsr;            // 1 / rho
+  const float unl = fmaf(L.y, nx, L.z * ny), unr = fmaf(R.y, nx, R.z * ny);
+  const float pol = L.w * irl, por = R.w * irr;            // p / rho
+  const float aL = fsqrtp(g.gamma * pol), aR = fsqrtp(g.gamma * por);
+  const float h0l = fmaf(g.gcp, pol, 0.5f * fmaf(L.y, L.y, L.z * L.z));
+  const float h0r = fmaf(g.gcp, por, 0.5f * fmaf(R.y, R.y, R.z * R.z));
+  const float isr = frcp(srL + srR);
+  const float wl = srL * isr, wr = srR * isr;
+  const float ur0 = fmaf(wr, R.y, wl * L.y), ur1 = fmaf(wr, R.z, wl * L.z);
+  const float h0_roe = fmaf(wr, h0r, wl * h0l);
+  const float a2 = g.gm1 * fmaf(-0.5f, fmaf(ur0, ur0, ur1 * ur1), h0_roe);
+  const float a_roe = fsqrtp(fmaxf(a2, 1.17549435e-38f));
+  const float un_roe = fmaf(ur0, nx, ur1 * ny);
+  const float S1 = fminf(fminf(0.0f, unl - aL), un_roe - a_roe);
+  const float S4 = fmaxf(fmaxf(0.0f, unr + aR), un_roe + a_roe);
+  const float ml = L.x * (S1 - unl), mr = R.x * (S4 - unr);
+  const float Sstar = (R.w - L.w + ml * unl - mr * unr) * frcp(ml - mr);
+  const bool left = (S1 >= 0.0f) || (Sstar >= 0.0f);
+  const float rk = left ? L.x : R.x, uk = left ? L.y : R.y, vk = left ? L.z : R.z, pk = left ? L.w : R.w;
+  const float unk = left ? unl : unr, h0k = left ? h0l : h0r, irk = left ? irl : irr;
+  const float SK = left ? S1 : S4, mk = left ? ml : mr;
+  const float m = rk * unk;
+  F[0] = m;
+  F[1] = fmaf(m, uk, pk * nx);
+  F[2] = fmaf(m, vk, pk * ny);
+  F[3] = m * h0k;
+  // star correction, applied when K's outer wave is subsonic in the face frame
+  const bool corr = left ? (S1 < 0.0f) : (S4 > 0.0f);
+  const float sc = corr ? SK : 0.0f;
+  const float pstar = fmaf(L.x * (unl - S1), unl - Sstar, L.w);
+  const float inv = frcp(SK - Sstar);
+  const float dp = pstar - pk;
+  const float e0k = h0k - pk * irk;
+  F[0] = fmaf(sc, fmaf(mk, inv, -rk), F[0]);
+  F[1] = fmaf(sc, fmaf(fmaf(mk, uk, dp * nx), inv, -rk * uk), F[1]);
+  F[2] = fmaf(sc, fmaf(fmaf(mk, vk, dp * ny), inv, -rk * vk), F[2]);
+  F[3] = fmaf(sc, fmaf(fmaf(mk, e0k, fmaf(-pk, unk, pstar * Sstar)), inv, -rk * e0k), F[3]);
+}
+
+// AUSM+ (Lib_Riemann_AUSM.f90:150-238) in FP32, flux per unit area.
+__device__ __forceinline__ void ausmp32(const GasF32& g, float4 L, float4 R, float nx, float ny, float* F) {
+  const float beta = 0.125f, alpha = 0.1875f;
+  const float irl = frcp(L.x), irr = frcp(R.x);
+  const float unl = fmaf(L.y, nx, L.z * ny), unr = fmaf(R.y, nx, R.z * ny);
+  const float pol = L.w * irl, por = R.w * irr;
+  const float a_half = fsqrtp(g.gamma * fsqrtp(pol * por));   // sqrt(aL aR)
+  const float ia = frcp(a_half);
+  const float ML = unl * ia, MR = unr * ia;
+  const float mL2 = fmaf(ML, ML, -1.0f), mR2 = fmaf(MR, MR, -1.0f);
+  const bool sl = fabsf(ML) < 1.0f, sr = fabsf(MR) < 1.0f;
+  const float lp1 = ML + 1.0f, rm1 = MR - 1.0f;
+  const float MplusL = sl ? fmaf(0.25f * lp1, lp1, beta * mL2 * mL2) : 0.5f * (ML + fabsf(ML));
+  const float pplusL = sl ? fmaf(0.25f * lp1 * lp1, 2.0f - ML, alpha * ML * mL2 * mL2)
+                          : 0.5f * (1.0f + copysignf(1.0f, ML));
+  const float MminusR = sr ? -fmaf(0.25f * rm1, rm1, beta * mR2 * mR2) : 0.5f * (MR - fabsf(MR));
+  const float pminusR = sr ? fmaf(0.25f * rm1 * rm1, 2.0f + MR, -alpha * MR * mR2 * mR2)
+                           : 0.5f * (1.0f - copysignf(1.0f, MR));
+  const float Mhalf = MplusL + MminusR;
+  const float phalf = fmaf(pplusL, L.w, pminusR * R.w);
+  const float mp = L.x * a_half * 0.5f * (Mhalf + fabsf(Mhalf));
+  const float mm = R.x * a_half * 0.5f * (Mhalf - fabsf(Mhalf));
+  const float HL = fmaf(g.gcp, pol, 0.5f * fmaf(L.y, L.y, L.z * L.z));
+  const float HR = fmaf(g.gcp, por, 0.5f * fmaf(R.y, R.y, R.z * R.z));
+  F[0] = mp + mm;
+  F[1] = fmaf(mp, L.y, fmaf(mm, R.y, nx * phalf));
+  F[2] = fmaf(mp, L.z, fmaf(mm, R.z, ny * phalf));
+  F[3] = fmaf(mp, HL, mm * HR);
+}
+
 // ---- state update (Newstate_Conservative restated, one species) -----------
 // U = (rho, rho u, ..., p/(gamma-1) + rho |u|^2 / 2); p = (gamma-1)(E - rho |u|^2 / 2)
 template <int NV>
@@ -335,9 +448,9 @@ __device__ __forceinline__ bool rk_update(const GasF& g, double* Q, const double
     ke = fma(U[1 + d], Q[1 + d], ke);
   }
   Q[P] = g.gm1 * fma(-0.5, ke, U[P]);
-  bool bad = false;
-  for (int v = 0; v < NV; ++v) bad |= isnan(Q[v]);
-  bad |= (Q[P] < 0.0);
+  // A NaN in any conserved variable reaches p (through 1/rho, the velocities
+  // or E), so one ordered compare finds NaN or p < 0 (Lib_Newstate.f90:334-338).
+  const bool bad = !(Q[P] >= 0.0);
   if (Q[0] < 1e-20) Q[0] = 1e-20;
   return !bad;
 }

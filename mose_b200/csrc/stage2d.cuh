@@ -30,8 +30,18 @@
 // bc list by block and face, Mod_BC_Fluxes.f90:52-216).
 //
 // The arithmetic is a policy: PolExact (the reference's operation order),
-// PolFast (FP64 restated for speed) or PolFast<..., true> (FP32 wave
-// structure).  Boundary-face fluxes always use the reference-exact formulas.
+// PolFast (FP64 restated for speed) or PolFast<..., true> (mixed).  Boundary
+// -face fluxes always use the reference-exact formulas.
+//
+// Mixed precision on uniform grids (HLLC, AUSM+) runs an FP32 pipeline: each
+// staged FP64 row is converted once into an FP32 ring of (rho, u, v, p)
+// vectors, and the slopes, limiters, face states and the whole Riemann solve
+// are FP32.  The FP32 face fluxes are exact FP64 numbers, so the per-
+// direction flux differences F(c+1/2) - F(c-1/2) are formed in FP64 without
+// rounding (the difference of two FP32 values is exact in FP64 unless their
+// exponents differ by more than 28, where the error is below 2^-53 of the
+// larger); the residual is A_i dF + A_j dG, and the RK update runs in FP64
+// from the FP64 state.
 #pragma once
 
 #include "arena.cuh"
@@ -119,6 +129,7 @@ template <int RIE, int LIM>
 struct PolExact {
   static constexpr bool kFast = false;
   static constexpr bool kCompensated = false;
+  static constexpr bool kMixed = false;
   __device__ static double inv_len(double l) { return 0.0; }
   __device__ static double slope(double dq, double l, double) { return dq / l; }
   __device__ static double lim(double x, double y) { return ex::limiter<LIM>(x, y); }
@@ -138,6 +149,7 @@ template <int RIE, int LIM, bool MIXED>
 struct PolFast {
   static constexpr bool kFast = true;
   static constexpr bool kCompensated = MIXED;
+  static constexpr bool kMixed = MIXED;
   __device__ static double inv_len(double l) { return fast::rcp(l); }
   __device__ static double slope(double dq, double, double il) { return dq * il; }
   __device__ static double lim(double x, double y) {
@@ -208,22 +220,32 @@ constexpr int SB_RS = 68;           // ring row stride (doubles): cells c0-2 .. 
 constexpr int SB_CH = 33;           // 16-byte chunks per ring row (66 cells)
 constexpr int SB_OCH = SB_W / 2;    // 16-byte chunks of the owned columns of a PO row
 
-// NVR ring planes: the NV state variables, plus dl along i and j with metric arrays.
-template <int NV, int NVR>
+// FP32 pipeline: mixed policy, uniform metrics, a solver with an FP32 form.
+template <class PH, int RIE, bool UNI>
+constexpr bool stage_fp32_pipeline() {
+  return PH::kMixed && UNI && RIE <= 1;
+}
+
+// NVR ring planes: the NV state variables, plus dl along i and j with metric
+// arrays.  MX: the FP32 pipeline's arrays replace the FP64 slope arrays.
+template <int NV, int NVR, bool MX>
 struct StageSmem {
   double ring[NVR][SB_RING][SB_RS];
   double po[2][NV][SB_Y][SB_X];       // PO of the owned cells (column c - c0), double buffered
-  double sx[NV][SB_Y][SB_X];          // limited i-slope of cell (c, j)
-  double sy[NV][SB_Y + 1][SB_X];      // limited j-slope of row r: 0 = batch base row (carried)
   double f[NV][SB_Y][SB_X];           // F(c + 1/2, j)
   double g[NV][SB_Y + 1][SB_X];       // G(c, j0 + r - 1/2): row 0 carried from the previous batch
   int fm[SB_Y][SB_X];                 // add masks of F / G
   int gm[SB_Y + 1][SB_X];
+  double sx[MX ? 1 : NV][SB_Y][SB_X];       // limited i-slope of cell (c, j)
+  double sy[MX ? 1 : NV][SB_Y + 1][SB_X];   // limited j-slope of row r: 0 = batch base row (carried)
+  float4 r32[MX ? SB_RING : 1][SB_RS];      // FP32 ring of (rho, u, v, p)
+  float4 sx32[MX ? SB_Y : 1][SB_X];
+  float4 sy32[MX ? SB_Y + 1 : 1][SB_X];
 };
 
-template <bool UNI>
+template <bool UNI, bool MX>
 constexpr size_t stage_smem_bytes() {
-  return sizeof(StageSmem<4, UNI ? 4 : 6>);
+  return sizeof(StageSmem<4, UNI ? 4 : 6, MX>);
 }
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
@@ -232,6 +254,17 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
+  return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 f4_sub(float4 a, float4 b) {
+  return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+// a + s b
+__device__ __forceinline__ float4 f4_fma(float s, float4 b, float4 a) {
+  return make_float4(fmaf(s, b.x, a.x), fmaf(s, b.y, a.y), fmaf(s, b.z, a.z), fmaf(s, b.w, a.w));
+}
 
 // Minimum resident CTAs per SM the register allocation is sized for.
 #ifndef MOSE_STAGE_MIN_CTAS
@@ -243,8 +276,12 @@ template <class PH, int RIE, int LIM, bool UNI, int MODE>
 __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs a) {
   constexpr int NV = 4;
   constexpr int NVR = UNI ? NV : NV + 2;
+  constexpr bool MX = stage_fp32_pipeline<PH, RIE, UNI>();
+  // uniform grid, fast arithmetic: the limiters are homogeneous of degree 1,
+  // so slopes stay in difference units and the half-cell factor is 1/2
+  constexpr bool FU = UNI && PH::kFast;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  StageSmem<NV, NVR>& S = *reinterpret_cast<StageSmem<NV, NVR>*>(smem_raw);
+  StageSmem<NV, NVR, MX>& S = *reinterpret_cast<StageSmem<NV, NVR, MX>*>(smem_raw);
   const int t = threadIdx.x;
   const int tx = t % SB_X, ty = t / SB_X;
   const bool need_po = (MODE == 0) && (a.irk != 1);
@@ -285,7 +322,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
         return f[3 * vs];
       }
     };
-    // ring access: ring row rr, ring column (cell c0 - 2 + col)
+    // ring access: ring row rr, ring column col (cell c0 - 2 + col)
     auto ringQ = [&](int rr, int col, double* q) {
 #pragma unroll
       for (int v = 0; v < NV; ++v) q[v] = S.ring[v][rr][col];
@@ -302,37 +339,79 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
       else if constexpr (UNI) return u_il;
       else return PH::inv_len(l);
     };
-    // limited j-slope of the cell at ring row rr (rows rr-1, rr, rr+1), ring column col
+    // limited slope of q between qa (low side) and qb (high side), cell-centre
+    // distances la, lb
+    auto lslope = [&](double qa, double q, double qb, double la, double lb, double ila, double ilb) -> double {
+      if constexpr (FU) return PH::lim(qb - q, q - qa);
+      else return PH::lim(PH::slope(qb - q, lb, ilb), PH::slope(q - qa, la, ila));
+    };
+    // half-cell factor of a face state: 0.5 dl (reference) or 0.5 (difference units)
+    auto half = [&](double dl) -> double {
+      if constexpr (FU) return 0.5; else return 0.5 * dl;
+    };
+    // limited j-slope of the cell at ring row rr (rows rm, rr, rp), ring column col
     auto slope_j = [&](int rm, int rr, int rp, int col, double* s) {
       const double la = 0.5 * (ring_dly(rm, col) + ring_dly(rr, col));
       const double lb = 0.5 * (ring_dly(rr, col) + ring_dly(rp, col));
       const double ila = ilen(la, u_ily), ilb = ilen(lb, u_ily);
 #pragma unroll
+      for (int v = 0; v < NV; ++v)
+        s[v] = lslope(S.ring[v][rm][col], S.ring[v][rr][col], S.ring[v][rp][col], la, lb, ila, ilb);
+    };
+    // FP32 pipeline: face normals of the uniform block
+    const float fnx0 = (float)u_nx[0], fnx1 = (float)u_nx[1], fny0 = (float)u_ny[0], fny1 = (float)u_ny[1];
+    const fast::GasF32 g32 = fast::gasf32(a.g);
+    auto solve32 = [&](float4 L, float4 R, float nx, float ny, double* F) -> bool {
+      float f[4];
+      if constexpr (RIE == 0) fast::hllc32(g32, L, R, nx, ny, f);
+      else fast::ausmp32(g32, L, R, nx, ny, f);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) F[v] = (double)f[v];
+      return L.x > 0.0f && L.w > 0.0f && R.x > 0.0f && R.w > 0.0f;
+    };
+    // boundary override in the FP32 pipeline: flux per unit area, mask applied
+    auto per_area = [&](double* F, int mask, double iA) {
+#pragma unroll
       for (int v = 0; v < NV; ++v) {
-        const double q = S.ring[v][rr][col];
-        const double sa = PH::slope(q - S.ring[v][rm][col], la, ila);
-        const double sb = PH::slope(S.ring[v][rp][col] - q, lb, ilb);
-        s[v] = PH::lim(sb, sa);
+        const bool keep = (mask == ADD_ALL) || (mask == ADD_MOMENTUM && v >= 1 && v < NV - 1);
+        F[v] = keep ? F[v] * iA : 0.0;
       }
     };
 
-    // unit u = rows j0 - 2 + 4u .. + 3 into ring rows 4 (u % 3) ..
+    // unit u = rows j0 - 2 + 4u .. + 3 into ring rows 4 (u % 3) ..; each
+    // thread copies all planes of its (row, 2-cell chunk) pairs
     auto load_unit = [&](int u) {
       const int slot = (u % 3) * SB_Y;
       const int rbase = j0 - 2 + SB_Y * u;
-      constexpr int n = NVR * SB_Y * SB_CH;
-      for (int e = t; e < n; e += SB_T) {
-        const int pv = e / (SB_Y * SB_CH);
-        const int rem = e - pv * (SB_Y * SB_CH);
-        const int i = rem / SB_CH;
-        const int q = rem - i * SB_CH;
+      for (int e = t; e < SB_Y * SB_CH; e += SB_T) {
+        const int i = e / SB_CH, q = e - i * SB_CH;
         const int r = rbase + i;
         const int x = c0 + 2 * q;   // padded column of cell c0 - 2 + 2q
         if (r > nj + 1 || x >= px) continue;
-        const double* plane;
-        if (pv < NV) plane = Pc + pv * vs;
-        else plane = a.m.dl + 3 * mb + (pv - NV) * vs;
-        cp_async16(&S.ring[pv][slot + i][2 * q], plane + (long long)(r + GW) * px + x);
+        const long long o = (long long)(r + GW) * px + x;
+#pragma unroll
+        for (int pv = 0; pv < NVR; ++pv) {
+          const double* plane = pv < NV ? Pc + pv * vs : a.m.dl + 3 * mb + (pv - NV) * vs;
+          cp_async16(&S.ring[pv][slot + i][2 * q], plane + o);
+        }
+      }
+    };
+    // FP32 copy of the chunks this thread copied for unit u (after its wait)
+    auto convert_unit = [&](int u) {
+      if constexpr (MX) {
+        const int slot = (u % 3) * SB_Y;
+        const int rbase = j0 - 2 + SB_Y * u;
+        for (int e = t; e < SB_Y * SB_CH; e += SB_T) {
+          const int i = e / SB_CH, q = e - i * SB_CH;
+          if (rbase + i > nj + 1 || c0 + 2 * q >= px) continue;
+          const int rr = slot + i;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int col = 2 * q + h;
+            S.r32[rr][col] = make_float4((float)S.ring[0][rr][col], (float)S.ring[1][rr][col],
+                                         (float)S.ring[2][rr][col], (float)S.ring[3][rr][col]);
+          }
+        }
       }
     };
     // PO of batch kk (rows j0 + 4 kk .., owned columns) into po[kk & 1]
@@ -358,27 +437,42 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
     if (need_po) load_po(0);
     cp_async_commit();
     cp_async_wait_all();
+    convert_unit(0);
+    convert_unit(1);
     __syncthreads();
     if (ty < 2 && owns) {
-      // ty 0: row j0 - 1 (ring row 1) -> sy[1]; ty 1: row j0 (ring row 2) -> sy[0]
-      double s[NV];
-      slope_j(ty, ty + 1, ty + 2, tx + 1, s);
+      // ty 0: row j0 - 1 (ring row 1) -> slot 1; ty 1: row j0 (ring row 2) -> slot 0
+      if constexpr (MX) {
+        const float4 qa = S.r32[ty][tx + 1], q = S.r32[ty + 1][tx + 1], qb = S.r32[ty + 2][tx + 1];
+        S.sy32[1 - ty][tx] = fast::limiter32x4<LIM>(f4_sub(qb, q), f4_sub(q, qa));
+      } else {
+        double s[NV];
+        slope_j(ty, ty + 1, ty + 2, tx + 1, s);
 #pragma unroll
-      for (int v = 0; v < NV; ++v) S.sy[v][1 - ty][tx] = s[v];
+        for (int v = 0; v < NV; ++v) S.sy[v][1 - ty][tx] = s[v];
+      }
     }
     __syncthreads();
     if (ty == 0 && owns) {
-      double qm[NV], q0[NV], QL[NV], QR[NV], G[NV], n[3];
-      ringQ(1, tx + 1, qm);
+      double q0[NV], G[NV], n[3];
       ringQ(2, tx + 1, q0);
-      const double lm = 0.5 * ring_dly(1, tx + 1), lp = 0.5 * ring_dly(2, tx + 1);
-#pragma unroll
-      for (int v = 0; v < NV; ++v) {
-        QL[v] = qm[v] + S.sy[v][1][tx] * lm;
-        QR[v] = q0[v] - S.sy[v][0][tx] * lp;
-      }
       const double A = face_at(1, c, j0, n);
-      const bool ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+      bool ok;
+      if constexpr (MX) {
+        const float4 L = f4_fma(0.5f, S.sy32[1][tx], S.r32[1][tx + 1]);
+        const float4 R = f4_fma(-0.5f, S.sy32[0][tx], S.r32[2][tx + 1]);
+        ok = solve32(L, R, fny0, fny1, G);
+      } else {
+        double qm[NV], QL[NV], QR[NV];
+        ringQ(1, tx + 1, qm);
+        const double lm = half(ring_dly(1, tx + 1)), lp = half(ring_dly(2, tx + 1));
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          QL[v] = qm[v] + S.sy[v][1][tx] * lm;
+          QR[v] = q0[v] - S.sy[v][0][tx] * lp;
+        }
+        ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+      }
       if (!ok && j0 > 0) report(a.err, 4, b, c, j0, 0);
       int mask = ADD_ALL;
       if (j0 == 0) {
@@ -390,6 +484,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           double q1[NV];
           ringQ(3, tx + 1, q1);
           mask = boundary_flux<RIE, LIM, NV>(a, w, q0, q1, ring_dly(2, tx + 1), ring_dly(3, tx + 1), n, A, 3, G);
+          if constexpr (MX) per_area(G, mask, 1.0 / A);
         }
       }
 #pragma unroll
@@ -399,7 +494,6 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
 
 #pragma unroll 1
     for (int k = 0; k < nbatch; ++k) {
-      cp_async_wait_all();
       __syncthreads();   // ring units k, k+1 and po[k & 1] visible; batch k-1 done with everything
       if (k + 2 <= nbatch) load_unit(k + 2);
       if (need_po && k + 1 < nbatch) load_po(k + 1);
@@ -418,23 +512,27 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
         S.gm[0][tx] = S.gm[SB_Y][tx];
       }
       if (rowok) {
-        {
+        if constexpr (MX) {
+          const float4 qa = S.r32[rr][col - 1], q = S.r32[rr][col], qb = S.r32[rr][col + 1];
+          S.sx32[ty][tx] = fast::limiter32x4<LIM>(f4_sub(qb, q), f4_sub(q, qa));
+          if (owns) {
+            const float4 q1 = S.r32[rp][col], q2 = S.r32[rp2][col];
+            S.sy32[ty + 1][tx] = fast::limiter32x4<LIM>(f4_sub(q2, q1), f4_sub(q1, q));
+          }
+        } else {
           const double dm = ring_dlx(rr, col - 1), d0 = ring_dlx(rr, col), dp = ring_dlx(rr, col + 1);
           const double la = 0.5 * (dm + d0), lb = 0.5 * (d0 + dp);
           const double ila = ilen(la, u_ilx), ilb = ilen(lb, u_ilx);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            const double q = S.ring[v][rr][col];
-            const double sa = PH::slope(q - S.ring[v][rr][col - 1], la, ila);
-            const double sb = PH::slope(S.ring[v][rr][col + 1] - q, lb, ilb);
-            S.sx[v][ty][tx] = PH::lim(sb, sa);
-          }
-        }
-        if (owns) {
-          double s[NV];
-          slope_j(rr, rp, rp2, col, s);
+          for (int v = 0; v < NV; ++v)
+            S.sx[v][ty][tx] = lslope(S.ring[v][rr][col - 1], S.ring[v][rr][col], S.ring[v][rr][col + 1], la, lb,
+                                     ila, ilb);
+          if (owns) {
+            double s[NV];
+            slope_j(rr, rp, rp2, col, s);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) S.sy[v][ty + 1][tx] = s[v];
+            for (int v = 0; v < NV; ++v) S.sy[v][ty + 1][tx] = s[v];
+          }
         }
       }
       __syncthreads();
@@ -442,15 +540,23 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
       // ---- phase B: face fluxes -----------------------------------------------------
       if (rowok) {
         if (has_face) {
-          double QL[NV], QR[NV], F[NV], n[3];
-          const double lm = 0.5 * ring_dlx(rr, col), lp = 0.5 * ring_dlx(rr, col + 1);
-#pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            QL[v] = S.ring[v][rr][col] + S.sx[v][ty][tx] * lm;
-            QR[v] = S.ring[v][rr][col + 1] - S.sx[v][ty][tx + 1] * lp;
-          }
+          double F[NV], n[3];
           const double A = face_at(0, c + 1, j, n);
-          const bool ok = PH::template face<NV>(a.g, QL, QR, n, A, F);
+          bool ok;
+          if constexpr (MX) {
+            const float4 L = f4_fma(0.5f, S.sx32[ty][tx], S.r32[rr][col]);
+            const float4 R = f4_fma(-0.5f, S.sx32[ty][tx + 1], S.r32[rr][col + 1]);
+            ok = solve32(L, R, fnx0, fnx1, F);
+          } else {
+            double QL[NV], QR[NV];
+            const double lm = half(ring_dlx(rr, col)), lp = half(ring_dlx(rr, col + 1));
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              QL[v] = S.ring[v][rr][col] + S.sx[v][ty][tx] * lm;
+              QR[v] = S.ring[v][rr][col + 1] - S.sx[v][ty][tx + 1] * lp;
+            }
+            ok = PH::template face<NV>(a.g, QL, QR, n, A, F);
+          }
           const bool lowb = (c == -1), highb = (c == ni - 1);
           int mask = ADD_ALL;
           if (!ok && !lowb && !highb) report(a.err, 4, b, c, j, 0);
@@ -466,6 +572,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
               ringQ(rr, ci, Qi);
               mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, ring_dlx(rr, cb), ring_dlx(rr, ci), n, A,
                                                  lowb ? 1 : 2, F);
+              if constexpr (MX) per_area(F, mask, 1.0 / A);
             }
           }
 #pragma unroll
@@ -473,15 +580,23 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           S.fm[ty][tx] = mask;
         }
         if (owns) {
-          double QL[NV], QR[NV], G[NV], n[3];
-          const double lm = 0.5 * ring_dly(rr, col), lp = 0.5 * ring_dly(rp, col);
-#pragma unroll
-          for (int v = 0; v < NV; ++v) {
-            QL[v] = S.ring[v][rr][col] + S.sy[v][ty][tx] * lm;
-            QR[v] = S.ring[v][rp][col] - S.sy[v][ty + 1][tx] * lp;
-          }
+          double G[NV], n[3];
           const double A = face_at(1, c, j + 1, n);
-          const bool ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+          bool ok;
+          if constexpr (MX) {
+            const float4 L = f4_fma(0.5f, S.sy32[ty][tx], S.r32[rr][col]);
+            const float4 R = f4_fma(-0.5f, S.sy32[ty + 1][tx], S.r32[rp][col]);
+            ok = solve32(L, R, fny0, fny1, G);
+          } else {
+            double QL[NV], QR[NV];
+            const double lm = half(ring_dly(rr, col)), lp = half(ring_dly(rp, col));
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+              QL[v] = S.ring[v][rr][col] + S.sy[v][ty][tx] * lm;
+              QR[v] = S.ring[v][rp][col] - S.sy[v][ty + 1][tx] * lp;
+            }
+            ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+          }
           int mask = ADD_ALL;
           if (!ok && j < nj - 1) report(a.err, 4, b, c, j, 0);
           if (j == nj - 1) {
@@ -494,6 +609,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
               ringQ(rr, col, Q);
               ringQ(rm, col, Qi);
               mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, ring_dly(rr, col), ring_dly(rm, col), n, A, 4, G);
+              if constexpr (MX) per_area(G, mask, 1.0 / A);
             }
           }
 #pragma unroll
@@ -505,28 +621,38 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
 
       // ---- phase C: residual and update ---------------------------------------------
       if (rowok && owns) {
-        ResAcc<NV, PH::kCompensated> R;
-        R.init();
-        const bool bi0 = (c == 0), bi1 = (c == ni - 1), bj0 = (j == 0), bj1 = (j == nj - 1);
-        double Fm[NV], Fp[NV], Gm[NV], Gp[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          Fm[v] = S.f[v][ty][tx - 1];
-          Fp[v] = S.f[v][ty][tx];
-          Gm[v] = S.g[v][ty][tx];
-          Gp[v] = S.g[v][ty + 1][tx];
-        }
-        if (!bi0) for (int v = 0; v < NV; ++v) R.add(v, -Fm[v]);
-        if (!bi1) for (int v = 0; v < NV; ++v) R.add(v, Fp[v]);
-        if (!bj0) for (int v = 0; v < NV; ++v) R.add(v, -Gm[v]);
-        if (!bj1) for (int v = 0; v < NV; ++v) R.add(v, Gp[v]);
-        if (bi0) add_bc<NV>(R, Fm, -1.0, S.fm[ty][tx - 1]);
-        if (bi1) add_bc<NV>(R, Fp, 1.0, S.fm[ty][tx]);
-        if (bj0) add_bc<NV>(R, Gm, -1.0, S.gm[ty][tx]);
-        if (bj1) add_bc<NV>(R, Gp, 1.0, S.gm[ty + 1][tx]);
         double Rv[NV];
+        if constexpr (MX) {
+          // exact FP64 differences of the FP32 face fluxes, scaled by the areas
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
+          for (int v = 0; v < NV; ++v) {
+            const double dF = S.f[v][ty][tx] - S.f[v][ty][tx - 1];
+            const double dG = S.g[v][ty + 1][tx] - S.g[v][ty][tx];
+            Rv[v] = fma(u_Ax, dF, u_Ay * dG);
+          }
+        } else {
+          ResAcc<NV, PH::kCompensated> R;
+          R.init();
+          const bool bi0 = (c == 0), bi1 = (c == ni - 1), bj0 = (j == 0), bj1 = (j == nj - 1);
+          double Fm[NV], Fp[NV], Gm[NV], Gp[NV];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            Fm[v] = S.f[v][ty][tx - 1];
+            Fp[v] = S.f[v][ty][tx];
+            Gm[v] = S.g[v][ty][tx];
+            Gp[v] = S.g[v][ty + 1][tx];
+          }
+          if (!bi0) for (int v = 0; v < NV; ++v) R.add(v, -Fm[v]);
+          if (!bi1) for (int v = 0; v < NV; ++v) R.add(v, Fp[v]);
+          if (!bj0) for (int v = 0; v < NV; ++v) R.add(v, -Gm[v]);
+          if (!bj1) for (int v = 0; v < NV; ++v) R.add(v, Gp[v]);
+          if (bi0) add_bc<NV>(R, Fm, -1.0, S.fm[ty][tx - 1]);
+          if (bi1) add_bc<NV>(R, Fp, 1.0, S.fm[ty][tx]);
+          if (bj0) add_bc<NV>(R, Gm, -1.0, S.gm[ty][tx]);
+          if (bj1) add_bc<NV>(R, Gp, 1.0, S.gm[ty + 1][tx]);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
+        }
         const long long o = off(c, j);
         if constexpr (MODE == 1) {
           double* Rb = a.R + d.sbase;
@@ -551,11 +677,16 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
         }
       }
       if (ty == SB_Y - 1 && owns) {   // carry the top row's j-slope
+        if constexpr (MX) {
+          S.sy32[0][tx] = S.sy32[SB_Y][tx];
+        } else {
 #pragma unroll
-        for (int v = 0; v < NV; ++v) S.sy[v][0][tx] = S.sy[v][SB_Y][tx];
+          for (int v = 0; v < NV; ++v) S.sy[v][0][tx] = S.sy[v][SB_Y][tx];
+        }
       }
+      cp_async_wait_all();   // this thread's copies of unit k+2 and po[k+1 & 1]
+      if (k + 2 <= nbatch) convert_unit(k + 2);
     }
-    cp_async_wait_all();
     __syncthreads();   // the next item refills the ring
   }
 }
