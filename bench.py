@@ -8,6 +8,12 @@ the named shape.  A "step" is one full Explicit_Step (dt pass + 3 fused RK
 stages) over the whole block.  value = cell-updates/s, one update being one
 RK3 step of one cell; N GPUs run N independent replicas (weak scaling).
 
+Precisions: value is the "fp64" path (the reference algorithm in restated
+FP64 arithmetic, within 1e-12 of the reference arithmetic per step); the
+reference-exact path and the mixed FP32/FP64 path are timed in the same run
+under "variants", with the mixed path's density error after 100 steps
+against the reference-exact path.
+
 --impl reference times the CPU oracle (the C++/OpenMP restatement of the
 reference's Fortran algorithm; the Fortran build itself cannot be compiled
 without gfortran and the FLINT/ORION/FiNeR submodules) on the host cores.
@@ -180,14 +186,69 @@ def run_reference(args):
     return 0
 
 
+PRECISIONS = ("exact", "fp64", "mixed")
+
+
+def precision_code(name):
+    from mose_b200 import _lib
+    return {"exact": _lib.PRECISION_FP64_EXACT, "fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[name]
+
+
+def time_advance(s, stream, steps, world, clk=None):
+    """Device time (ms, max over ranks) of `steps` graph-replayed fused steps."""
+    import torch
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if clk is not None:
+        clk.__enter__()
+    e0.record(stream)
+    s.advance(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if clk is not None:
+        clk.__exit__(None, None, None)
+    barrier(world)
+    return max_over_ranks(e0.elapsed_time(e1), world)
+
+
+def stage_roofline(s, steps, cells):
+    """Per-kernel-class device times (CUDA events between launches) and the
+    stage kernel's achieved HBM GB/s on the algorithmic bytes."""
+    kms, kn = s.time_kernels(max(3, min(20, steps)))
+    stage_ms = kms[2] / max(kn[2], 1)
+    achieved = STAGE_BYTES_PER_CELL * cells / (stage_ms / 1e3) / 1e9
+    return stage_ms, achieved, {"dt": kms[0] / max(1, kn[0] // 3), "ghost": kms[1] / max(1, kn[1]),
+                                "stage": stage_ms}
+
+
+def mixed_error(local, steps=100):
+    """Density error of the mixed precision against the reference-exact
+    path (bit-identical to the FP64 oracle) after `steps` RK3 steps of the
+    workload."""
+    from mose_b200 import Solver
+    from mose_b200.cases import GC
+    case = workload_case(N_CELLS_SIDE, steps=steps)
+    out = {}
+    for name in ("exact", "mixed"):
+        s = Solver(case, precision=precision_code(name), device=local)
+        s.advance(steps)
+        out[name] = s.download_prim(1)[GC:-GC, GC:-GC, GC:-GC, 0].copy()
+        s.close()
+    r, g = out["exact"], out["mixed"]
+    return {"density_l2": float(np.sqrt(((g - r) ** 2).sum() / (r ** 2).sum())),
+            "density_linf": float(np.abs(g - r).max() / np.abs(r).max()), "steps": steps,
+            "against": "reference-exact GPU path (bit-identical to the FP64 oracle)"}
+
+
 def run_gpu(args):
     world, rank, local = dist_init()
     import torch
-    from mose_b200 import Solver, _lib
-    prec = {"exact": _lib.PRECISION_FP64_EXACT, "fp64": _lib.PRECISION_FP64, "mixed": _lib.PRECISION_MIXED}[
-        args.precision]
+    from mose_b200 import Solver
     case = workload_case(N_CELLS_SIDE, steps=args.steps)
-    s = Solver(case, precision=prec, device=local)
+    cells = case.ncells
+    peak, peak_kind = peaks()
+    s = Solver(case, precision=precision_code(args.precision), device=local)
     stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
     s.advance(max(args.warmup, 3))
     torch.cuda.synchronize()
@@ -200,25 +261,11 @@ def run_gpu(args):
         return 0
     # --- device-resident throughput (value) ---------------------------------
     launches0 = s.launch_count
-    barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        s.advance(args.steps)
-        e1.record(stream)
-        torch.cuda.synchronize()
-    barrier(world)
-    ms = e0.elapsed_time(e1)
+    clk = ClockSampler(local)
+    ms = time_advance(s, stream, args.steps, world, clk)
     launches = s.launch_count - launches0
-    ms = max_over_ranks(ms, world)
-    value = world * case.ncells * args.steps / (ms / 1e3)
-    # --- per-kernel timing for the roofline (same kernels, events between) --
-    kms, kn = s.time_kernels(max(3, min(20, args.steps)))
-    stage_ms = kms[2] / max(kn[2], 1)
-    cells = case.ncells
-    achieved = STAGE_BYTES_PER_CELL * cells / (stage_ms / 1e3) / 1e9
-    peak, peak_kind = peaks()
+    value = world * cells * args.steps / (ms / 1e3)
+    stage_ms, achieved, step_ms = stage_roofline(s, args.steps, cells)
     # --- end to end through the C ABI with host buffers ----------------------
     shape = (1 + 4, N_CELLS_SIDE + 4, N_CELLS_SIDE + 4, 5)
     host = torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -231,11 +278,26 @@ def run_gpu(args):
         s.upload_prim(1, host)
         s.explicit_step()
         s.download_prim(1, host)
-    e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, world)
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
     e2e = world * cells * n_e2e / e2e_s
     nbytes = int(np.prod(shape[1:])) * 8      # 2-D: the k = 1 plane of the reference array crosses the bus
+    s.close()
+    # --- the other precisions on the same workload ---------------------------
+    variants = {}
+    for name in PRECISIONS:
+        if name == args.precision:
+            continue
+        v = Solver(case, precision=precision_code(name), device=local)
+        vstream = torch.cuda.ExternalStream(v.stream_handle, device=torch.device("cuda", local))
+        v.advance(3)
+        vms = time_advance(v, vstream, args.steps, world)
+        v_stage_ms, v_ach, v_step = stage_roofline(v, args.steps, cells)
+        variants[name] = {"value": world * cells * args.steps / (vms / 1e3), "ms_per_step": vms / args.steps,
+                          "stage_ms": v_stage_ms, "roofline_frac": v_ach / peak, "step_kernel_ms": v_step}
+        v.close()
+    err = mixed_error(local) if rank == 0 else None
     if rank == 0:
+        variants.setdefault("mixed", {})["error_vs_fp64_oracle"] = err
         line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -243,19 +305,17 @@ def run_gpu(args):
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None,
                              "kernel": "k_stage2d (fused residual + RK stage)", "peak_kind": peak_kind,
-                             "stage_ms": stage_ms, "step_kernel_ms": {"dt": kms[0] / max(1, kn[0] // 3),
-                                                                      "ghost": kms[1] / max(1, kn[1]),
-                                                                      "stage": stage_ms}},
+                             "stage_ms": stage_ms, "step_kernel_ms": step_ms},
                 "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
                         "d2h_bytes_per_step": nbytes,
                         "call": "mose_gpu_upload_prim + mose_gpu_step + mose_gpu_download_prim (pinned host)"},
                 "gpu_launches": launches, "clocks": clk.summary(),
                 "step_bytes_per_cell": BYTES_PER_CELL_STEP,
-                "hbm_frac_whole_step": BYTES_PER_CELL_STEP * cells * args.steps / (ms / 1e3 / world) / 1e9 / peak}
+                "hbm_frac_whole_step": BYTES_PER_CELL_STEP * cells * args.steps / (ms / 1e3 / world) / 1e9 / peak,
+                "variants": variants}
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
-    s.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -268,7 +328,8 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="gpu", choices=["gpu", "reference"])
-    ap.add_argument("--precision", default="exact", choices=["exact", "fp64", "mixed"])
+    ap.add_argument("--precision", default="fp64", choices=list(PRECISIONS),
+                    help="precision of the headline value; the others are reported under variants")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + K fused steps (the command profiled by ncu); prints nothing")

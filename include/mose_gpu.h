@@ -68,7 +68,11 @@ enum {
   MOSE_RIEMANN_SLAU2 = 3
 };
 
-/* Arithmetic of the face sweeps. */
+/* Arithmetic of the face sweeps and of the fused steps' CFL pass.  In the
+ * fused step (mose_gpu_step / mose_gpu_advance) the last RK stage also forms
+ * the next step's Compute_dt on the state it writes; the first fused step
+ * after any call that changes the state runs the standalone (reference
+ * arithmetic) pass instead. */
 enum {
   MOSE_PRECISION_FP64_EXACT = 0,   /* the reference's FP64 operation order, no FMA contraction */
   MOSE_PRECISION_FP64 = 1,         /* FP64, FMA-contracted and reciprocal-folded */

@@ -23,7 +23,7 @@ struct StageArgs {
   double* Pn;           // next state (fused mode)
   double* R;            // residual arena (residual-only mode)
   MetricArgs m;
-  const double* dtl;    // local dt plane arena (one plane per block), or null
+  double* dtl;          // local dt plane arena (one plane per block), or null
   const double* dtg;    // device scalar dtglobal (time-accurate)
   const int* bcw;       // boundary words, see bc_code()
   const BcParam* bcp;
@@ -32,6 +32,13 @@ struct StageArgs {
   int time_accurate;
   DevError* err;
   Gas g;
+  // Fused Compute_dt of the NEXT step (last RK stage only, else dtmin = null):
+  // the CFL dt of every updated cell folds into *dtmin (bit pattern of a
+  // positive double); with dt_local each cell's dt is also stored in dtl.
+  unsigned long long* dtmin;
+  double cfl;
+  int ndir;
+  int dt_local;
 };
 
 }  // namespace mose

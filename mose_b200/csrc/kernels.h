@@ -26,6 +26,8 @@ void launch_set_global_dt(const BlockDesc* dblk, int nblk, long long maxcell, do
 void launch_step_begin(unsigned long long* dtmin_bits, double dt_start, int* iter, cudaStream_t s);
 void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time,
                           cudaStream_t s);
+void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time, double dt_start,
+                         int* iter, cudaStream_t s);
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
                      cudaStream_t s);
@@ -54,7 +56,8 @@ MOSE_STAGE_DECL(1, 0) MOSE_STAGE_DECL(1, 1) MOSE_STAGE_DECL(1, 2) MOSE_STAGE_DEC
 MOSE_STAGE_DECL(2, 0) MOSE_STAGE_DECL(2, 1) MOSE_STAGE_DECL(2, 2) MOSE_STAGE_DECL(2, 3)
 #undef MOSE_STAGE_DECL
 
-// mode 0: fused residual + RK update; mode 1: residual only (exact precision).
+// mode 0: fused residual + RK update; 1: residual only (exact precision);
+// 2: fused, plus the next step's Compute_dt (last RK stage of a fused step).
 inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int prec, int rie, int lim,
                            cudaStream_t s) {
   using L = bool (*)(const StageArgs&, int, int, bool, int, cudaStream_t);

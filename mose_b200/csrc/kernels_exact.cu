@@ -3,6 +3,8 @@
 // the order of the reference's Fortran expressions.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "kernels.h"
 #include "metrics.cuh"
 #include "stage2d.cuh"
@@ -363,36 +365,21 @@ template <int NV, bool UNI>
 __global__ void k_compute_dt(const BlockDesc* blk, int nblk, const double* P, MetricArgs m, double* dtl,
                              unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
                              int ramp_iter, int store_local) {
-  // one CTA-row per (block, row) pair: blockIdx.y = block, grid-stride over cells
+  // blockIdx.y = block; CTAs stride over the block's cell rows (j, k), threads
+  // over the cells of a row, so no per-cell index division
   const int b = blockIdx.y;
   const BlockDesc& d = blk[b];
-  const long long ncell = (long long)d.ni * d.nj * d.nk;
+  const int rows = d.nj * d.nk;
   const long long vs = d.vstride, mb = d.mbase;
   const double* Pb = P + d.sbase;
   double local_min = __longlong_as_double(0x7ff0000000000000LL);
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
-    int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+  for (int row = blockIdx.x; row < rows; row += gridDim.x)
+  for (int i = threadIdx.x; i < d.ni; i += blockDim.x) {
+    const int j = row % d.nj, k = row / d.nj;
     long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
     double Q[NV];
     for (int v = 0; v < NV; ++v) Q[v] = Pb[v * vs + o];
-    double Sound = ex::sound(g, Q[0], Q[NV - 1]);
-    double dtmin = 1e8;
-    for (int dd = 0; dd < ndir; ++dd) {
-      double ver[3];
-      double dlv;
-      if constexpr (UNI) {
-        ver[0] = d.u_vers[dd][0]; ver[1] = d.u_vers[dd][1]; ver[2] = d.u_vers[dd][2];
-        dlv = d.u_dl[dd];
-      } else {
-        for (int c = 0; c < 3; ++c) ver[c] = m.vers[9 * mb + (3 * dd + c) * vs + o];
-        dlv = m.dl[3 * mb + dd * vs + o];
-      }
-      double vel_ = fabs(ex::dot_vel<NV>(Q, ver));
-      double lambda = vel_ + Sound;
-      double dt = dlv / lambda * cfl;
-      dtmin = fmin(dt, dtmin);
-    }
-    double dtcell = dtmin;
+    double dtcell = cfl_dt<NV, UNI, false>(g, Q, d, m, o, ndir, cfl);
     if (ramp_iter > 0 && iter < ramp_iter) dtcell = dtcell * (double)iter / (double)ramp_iter;
     if (store_local) dtl[mb + o] = dtcell;
     local_min = fmin(local_min, dtcell);
@@ -432,6 +419,17 @@ __global__ void k_step_dt_final(const unsigned long long* dtmin_bits, double* dt
   double v = __longlong_as_double((long long)*dtmin_bits);
   *dtg = v;
   if (advance_time) *time = *time + v;
+}
+// Fused-step bookkeeping: dtglobal = the running minimum (from the standalone
+// pass, or from the previous step's last RK stage), time += dtglobal, then
+// the minimum restarts from dt_start for this step's last stage.
+__global__ void k_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time,
+                               double dt_start, int* iter) {
+  const double v = __longlong_as_double((long long)*dtmin_bits);
+  *dtg = v;
+  if (advance_time) *time = *time + v;
+  *dtmin_bits = (unsigned long long)__double_as_longlong(dt_start);
+  if (iter) *iter = *iter + 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -636,7 +634,8 @@ void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, d
 void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,
                        double* dtl, unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
                        int ramp_iter, int store_local, bool uniform, cudaStream_t s) {
-  dim3 grid(grid_for(maxcell, 256, 148 * 8), nblk);
+  // one CTA per cell row (rows <= cells), at most 16 per SM
+  dim3 grid((unsigned)std::min<long long>(maxcell, 148 * 16), nblk);
   if (nd == 3) {
     if (uniform) k_compute_dt<5, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
     else k_compute_dt<5, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
@@ -656,6 +655,10 @@ void launch_step_begin(unsigned long long* dtmin_bits, double dt_start, int* ite
 void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time,
                           cudaStream_t s) {
   k_step_dt_final<<<1, 1, 0, s>>>(dtmin_bits, dtg, time, advance_time);
+}
+void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time, double dt_start,
+                         int* iter, cudaStream_t s) {
+  k_step_dt_take<<<1, 1, 0, s>>>(dtmin_bits, dtg, time, advance_time, dt_start, iter);
 }
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,

@@ -153,6 +153,9 @@ struct mose_gpu_ctx {
 
   cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
   int graph_kernels = 0;
+  // dtmin holds the CFL minimum of state[cur], folded in by the last RK stage
+  // of the previous fused step; cleared by every call that changes the state
+  bool dt_valid = false;
 
   double h_time = 0.0;
   int h_iter = 0;
@@ -598,6 +601,7 @@ static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool uplo
   if (rc) return rc;
   double* dst = (arena < 0) ? ctx->resid.p : ctx->state[arena].p;
   if (upload) {
+    ctx->dt_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, P, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_ref_to_soa(ctx->d_desc.p, b - 1, n, ctx->staging.p, dst, ctx->nv, ctx->nd, ctx->stream);
     ctx->launches++;
@@ -634,6 +638,7 @@ static int dt_io(mose_gpu_ctx* ctx, int32_t b, double* dt, bool upload) {
   int rc = ensure_staging(ctx, (size_t)n);
   if (rc) return rc;
   if (upload) {
+    ctx->dt_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, dt, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_plane_io(ctx->d_desc.p, b - 1, n, ctx->dtl.p, ctx->staging.p, ctx->nd, 0, ctx->stream);
   } else {
@@ -661,6 +666,7 @@ int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ram
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!dtglobal) return MOSE_ERR_INVALID;
+  ctx->dt_valid = false;
   launch_step_begin(ctx->dtmin.p, *dtglobal, nullptr, ctx->stream);
   launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->margs(),
                     ctx->dtl.p, ctx->dtmin.p, ctx->gas, cfl, ctx->ndir, ctx->nd, iter, ramp_iter, 1, ctx->uniform,
@@ -675,6 +681,7 @@ int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ram
 int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
   int rc = require_ready(ctx);
   if (rc) return rc;
+  ctx->dt_valid = false;
   CU(cudaMemcpyAsync(ctx->scal.p, &dtglobal, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   launch_set_global_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->dtl.p, ctx->scal.p, ctx->nd,
                        ctx->stream);
@@ -686,6 +693,7 @@ int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
 int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
   int rc = require_ready(ctx);
   if (rc) return rc;
+  ctx->dt_valid = false;
   ctx->po = (ctx->cur + 1) % 3;
   CU(cudaMemcpyAsync(ctx->state[ctx->po].p, ctx->state[ctx->cur].p, ctx->state[0].n * sizeof(double),
                      cudaMemcpyDeviceToDevice, ctx->stream));
@@ -741,6 +749,7 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
   if (rc) return rc;
   if (irk < 1 || irk > ctx->cfg.n_rk) return fail(ctx, MOSE_ERR_INVALID, "irk out of range");
   static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
+  ctx->dt_valid = false;
   launch_rk_stage(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->state[ctx->po].p,
                   ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->nd,
                   ctx->uniform, ctx->derr.p, ctx->stream);
@@ -748,16 +757,39 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
   return check_launch(ctx, "rk_stage");
 }
 
-// Enqueues one fused Explicit_Step starting from state arena s0.  Returns the
-// number of kernels enqueued.
-static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
-  int k = 0;
-  launch_step_begin(ctx->dtmin.p, 1e5, ctx->iterdev.p, ctx->stream); ++k;
-  // Compute_dt starts its minimum from 1d5 (Mod_Explicit.f90:44)
+// Time-accurate runs fold the next step's Compute_dt (the CFL minimum) into
+// the last RK stage, which holds the new state anyway.  With local time
+// stepping each step keeps its standalone pass, so dtlocal always holds the
+// dt of the step that used it, as in the reference.
+static bool fused_dt(const mose_gpu_ctx* ctx) { return ctx->cfg.time_accurate != 0; }
+static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
+  a.dtmin = ctx->dtmin.p;
+  a.cfl = ctx->cfg.cfl;
+  a.ndir = ctx->ndir;
+  a.dt_local = 0;
+}
+
+// The standalone Compute_dt pass over state arena s0: dtmin = min over cells,
+// starting from 1d5 (Mod_Explicit.f90:44); local dt stored when not time
+// accurate.  Returns the number of kernels enqueued.
+static int enqueue_dt_pass(mose_gpu_ctx* ctx, int s0) {
+  launch_step_begin(ctx->dtmin.p, 1e5, nullptr, ctx->stream);
   launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(), ctx->dtl.p,
                     ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0, ctx->cfg.time_accurate ? 0 : 1,
-                    ctx->uniform, ctx->stream); ++k;
-  launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, ctx->stream); ++k;
+                    ctx->uniform, ctx->stream);
+  return 2;
+}
+
+// Enqueues one fused Explicit_Step starting from state arena s0, whose CFL
+// minimum is already in dtmin (the dt pass, or the previous step's last
+// stage): publish dtglobal and advance time, then the RK stages; the last
+// stage folds in the CFL minimum of the new state for the next step.
+// Returns the number of kernels enqueued.
+static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
+  int k = 0;
+  if (!fused_dt(ctx)) k += enqueue_dt_pass(ctx, s0);
+  launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
+                      ctx->stream); ++k;
   int pc = s0;
   for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
     int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
@@ -765,7 +797,8 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
                        ctx->stream);
     if (ctx->nghost) ++k;
     StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-    launch_stage2d(a, ctx->nsm, 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
+    if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
+    launch_stage2d(a, ctx->nsm, a.dtmin ? 2 : 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
                    ctx->stream);
     ++k;
     pc = pn;
@@ -786,9 +819,11 @@ int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
   if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
   CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   int s0 = ctx->cur;
+  if (fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, s0);
   ctx->launches += enqueue_step(ctx, s0);
   rc = check_launch(ctx, "step");
   if (rc) return rc;
+  ctx->dt_valid = fused_dt(ctx);
   ctx->po = s0;
   ctx->cur = step_final_index(ctx, s0);
   double h[2];
@@ -807,6 +842,7 @@ int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double
   if (nsteps < 0) return MOSE_ERR_INVALID;
   if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
   CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  if (nsteps > 0 && fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, ctx->cur);
   for (int n = 0; n < nsteps; ++n) {
     int s0 = ctx->cur;
     if (!ctx->graph[s0]) {
@@ -820,6 +856,7 @@ int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double
     }
     CU(cudaGraphLaunch(ctx->graph[s0], ctx->stream));
     ctx->launches += ctx->graph_kernels;
+    ctx->dt_valid = fused_dt(ctx);
     ctx->po = s0;
     ctx->cur = step_final_index(ctx, s0);
   }
@@ -889,13 +926,11 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
   for (int n = 0; n < nsteps; ++n) {
     int s0 = ctx->cur;
     mark(-1);
-    launch_step_begin(ctx->dtmin.p, 1e5, ctx->iterdev.p, ctx->stream);
-    launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(),
-                      ctx->dtl.p, ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0,
-                      ctx->cfg.time_accurate ? 0 : 1, ctx->uniform, ctx->stream);
-    launch_step_dt_final(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, ctx->stream);
+    if (!fused_dt(ctx) || !ctx->dt_valid) launches[0] += enqueue_dt_pass(ctx, s0);
+    launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
+                        ctx->stream);
     mark(0);
-    launches[0] += 3;
+    launches[0] += 1;
     int pc = s0;
     for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
       int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
@@ -906,12 +941,14 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
         launches[1] += 1;
       }
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-      launch_stage2d(a, ctx->nsm, 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
+      if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
+      launch_stage2d(a, ctx->nsm, a.dtmin ? 2 : 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
                      ctx->stream);
       mark(2);
       launches[2] += 1;
       pc = pn;
     }
+    ctx->dt_valid = fused_dt(ctx);
     ctx->po = s0;
     ctx->cur = pc;
   }

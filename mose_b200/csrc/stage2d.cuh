@@ -120,6 +120,38 @@ __device__ __forceinline__ bool rk_update(const Gas& g, double* Q, const double*
   return !bad;
 }
 
+// CFL time step of one cell (Mod_dt.f90:71-85): the minimum over the ndir
+// directions of dl_d CFL / (|u . versor_d| + a).  FAST: the restated FP64
+// arithmetic (a^2 = gamma p / rho, reciprocals); otherwise the reference's
+// operations, so the standalone pass and the fused one agree bit for bit.
+template <int NV, bool UNI, bool FAST>
+__device__ __forceinline__ double cfl_dt(const Gas& g, const double* Q, const BlockDesc& d, const MetricArgs& m,
+                                         long long o, int ndir, double cfl) {
+  const long long vs = d.vstride, mb = d.mbase;
+  double Sound;
+  if constexpr (FAST) Sound = fast::sqrt_(g.gamma * Q[NV - 1] * fast::rcp(Q[0]));
+  else Sound = ex::sound(g, Q[0], Q[NV - 1]);
+  double dtmin = 1e8;
+  for (int dd = 0; dd < ndir; ++dd) {
+    double ver[3];
+    double dlv;
+    if constexpr (UNI) {
+      ver[0] = d.u_vers[dd][0]; ver[1] = d.u_vers[dd][1]; ver[2] = d.u_vers[dd][2];
+      dlv = d.u_dl[dd];
+    } else {
+      for (int c = 0; c < 3; ++c) ver[c] = m.vers[9 * mb + (3 * dd + c) * vs + o];
+      dlv = m.dl[3 * mb + dd * vs + o];
+    }
+    const double vel_ = fabs(ex::dot_vel<NV>(Q, ver));
+    const double lambda = vel_ + Sound;
+    double dt;
+    if constexpr (FAST) dt = (dlv * cfl) * fast::rcp(lambda);
+    else dt = dlv / lambda * cfl;
+    dtmin = fmin(dt, dtmin);
+  }
+  return dtmin;
+}
+
 // ---- arithmetic policies ---------------------------------------------------
 // slope(dq, l, il): first difference over the cell-centre distance l (il = 1/l)
 // lim(x, y): limited slope phi(y/x) x
@@ -271,7 +303,22 @@ __device__ __forceinline__ float4 f4_fma(float s, float4 b, float4 a) {
 #define MOSE_STAGE_MIN_CTAS 2
 #endif
 
-// MODE: 0 = fused (residual + RK update, writes Pn), 1 = residual only (writes R).
+// FP32 CFL dt of one cell of a uniform 2-D block (the FP32 pipeline's fused
+// Compute_dt): a relative error near 1e-7 in the global dt moves the solution
+// far less than the pipeline's own FP32 flux error.
+__device__ __forceinline__ double cfl_dt32(const Gas& g, const double* Q, const BlockDesc& d, int ndir, double cfl) {
+  const float r = (float)Q[0], u = (float)Q[1], v = (float)Q[2], p = (float)Q[3];
+  const float a = fast::fsqrtp((float)g.gamma * p * fast::frcp(r));
+  float dtmin = 1e8f;
+  for (int dd = 0; dd < ndir; ++dd) {
+    const float lam = fabsf(fmaf(u, (float)d.u_vers[dd][0], v * (float)d.u_vers[dd][1])) + a;
+    dtmin = fminf(dtmin, (float)(d.u_dl[dd] * cfl) * fast::frcp(lam));
+  }
+  return (double)dtmin;
+}
+
+// MODE: 0 = fused (residual + RK update, writes Pn), 1 = residual only (writes
+// R), 2 = fused and the next step's Compute_dt on the new state (last stage).
 template <class PH, int RIE, int LIM, bool UNI, int MODE>
 __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs a) {
   constexpr int NV = 4;
@@ -284,7 +331,8 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
   StageSmem<NV, NVR, MX>& S = *reinterpret_cast<StageSmem<NV, NVR, MX>*>(smem_raw);
   const int t = threadIdx.x;
   const int tx = t % SB_X, ty = t / SB_X;
-  const bool need_po = (MODE == 0) && (a.irk != 1);
+  const bool need_po = (MODE != 1) && (a.irk != 1);
+  double dtrun = __longlong_as_double(0x7ff0000000000000LL);   // fused dt: running minimum
 
 #pragma unroll 1
   for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
@@ -674,6 +722,13 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           double* Pn = a.Pn + d.sbase;
 #pragma unroll
           for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
+          if constexpr (MODE == 2) {   // Compute_dt of the next step on the new state
+            double dtc;
+            if constexpr (MX) dtc = cfl_dt32(a.g, Q, d, a.ndir, a.cfl);
+            else dtc = cfl_dt<NV, UNI, PH::kFast>(a.g, Q, d, a.m, o, a.ndir, a.cfl);
+            if (a.dt_local) a.dtl[mb + o] = dtc;
+            dtrun = fmin(dtrun, dtc);
+          }
         }
       }
       if (ty == SB_Y - 1 && owns) {   // carry the top row's j-slope
@@ -688,6 +743,17 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
       if (k + 2 <= nbatch) convert_unit(k + 2);
     }
     __syncthreads();   // the next item refills the ring
+  }
+  if constexpr (MODE == 2) {   // CTA minimum, one atomic
+    __shared__ double red[SB_T / 32];
+    for (int s = 16; s > 0; s >>= 1) dtrun = fmin(dtrun, __shfl_xor_sync(0xffffffffu, dtrun, s));
+    if ((t & 31) == 0) red[t >> 5] = dtrun;
+    __syncthreads();
+    if (t == 0) {
+      double v = red[0];
+      for (int w = 1; w < SB_T / 32; ++w) v = fmin(v, red[w]);
+      atomicMin(a.dtmin, (unsigned long long)__double_as_longlong(v));
+    }
   }
 }
 

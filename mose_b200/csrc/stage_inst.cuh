@@ -44,6 +44,11 @@ static bool stage2d_dispatch_uni(const StageArgs& a, int nsm, int mode, bool uni
     }
     return false;
   }
+  if (mode == 2) {
+    if (uni) launch_persistent<PREC, RIE, LIM, true, 2>(a, nsm, s);
+    else launch_persistent<PREC, RIE, LIM, false, 2>(a, nsm, s);
+    return true;
+  }
   if (uni) launch_persistent<PREC, RIE, LIM, true, 0>(a, nsm, s);
   else launch_persistent<PREC, RIE, LIM, false, 0>(a, nsm, s);
   return true;
