@@ -267,3 +267,96 @@ def curvilinear_channel(n: int = 512, steps: int = 200, mach: float = 0.8, amp: 
     return Case("channel2d", [nodes], rec, data, [prim], n_rk=3, cfl=cfl, time_accurate=True,
                 limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps,
                 extra={"mach": mach})
+
+
+def periodic_box_3d(n: int = 128, nb=(2, 2, 2), sizes=None, steps: int = 50, seed: int = 0,
+                    limiter="vanleer", riemann="HLLC", cfl=0.3, gamma=1.4, mach=0.3, amp=1e-2,
+                    nmodes: int = 16, kmax: int = 8) -> Case:
+    """3-D periodic box [0,1]^3 of nb[0] x nb[1] x nb[2] blocks (n^3 cells each, or
+    per-direction block sizes `sizes`), uniform state rho = 1, p = 1/gamma
+    (sound speed 1), Mach 0.3 along x, plus `nmodes` seeded Fourier modes with
+    integer wavevectors of norm in [1, kmax] and random phases on rho, u, v, w,
+    their sum scaled to amplitude `amp`.  Block interfaces are 101 connections,
+    the periodic wrap is 201 (connection with extrapolated ghost metrics).
+    [0,1] with a power-of-two cell count gives dyadic, exactly uniform metrics."""
+    rng = np.random.default_rng(seed)
+    sizes = sizes or [[n] * nb[0], [n] * nb[1], [n] * nb[2]]
+    N = [int(sum(s)) for s in sizes]
+    offs = [np.concatenate([[0], np.cumsum(s)[:-1]]).astype(int) for s in sizes]
+    modes = []
+    while len(modes) < nmodes:
+        kv = rng.integers(-kmax, kmax + 1, size=3)
+        kn = float(np.sqrt((kv ** 2).sum()))
+        if 1.0 <= kn <= kmax:
+            modes.append((kv.astype(np.float64), rng.uniform(0.0, 2.0 * np.pi, size=4)))
+    nodes, prims, dims, index = [], [], [], {}
+    for bz in range(nb[2]):
+        for by in range(nb[1]):
+            for bx in range(nb[0]):
+                ni, nj, nk = int(sizes[0][bx]), int(sizes[1][by]), int(sizes[2][bz])
+                nd = cartesian_nodes(ni, nj, nk, (0.0, 0.0, 0.0), (1.0, 1.0, 1.0),
+                                     offs=(int(offs[0][bx]), int(offs[1][by]), int(offs[2][bz])), ntot=tuple(N))
+                c = cell_centres(nd)
+                pert = np.zeros(c.shape[:-1] + (4,))
+                for kv, ph in modes:
+                    arg = 2.0 * np.pi * (c[..., 0] * kv[0] + c[..., 1] * kv[1] + c[..., 2] * kv[2])
+                    for q in range(4):
+                        pert[..., q] += np.cos(arg + ph[q])
+                pert *= amp / nmodes
+                p = np.zeros((nk, nj, ni, NPRIM))
+                p[..., 0] = 1.0 + pert[..., 0]
+                p[..., 1] = mach + pert[..., 1]
+                p[..., 2] = pert[..., 2]
+                p[..., 3] = pert[..., 3]
+                p[..., 4] = 1.0 / gamma
+                index[(bx, by, bz)] = len(nodes) + 1
+                nodes.append(nd)
+                prims.append(p)
+                dims.append((ni, nj, nk))
+
+    def spec(b, f):
+        key = [k for k, v in index.items() if v == b][0]
+        d = (f - 1) // 2
+        step = -1 if f % 2 == 1 else 1
+        nbk = list(key)
+        nbk[d] += step
+        wrap = not (0 <= nbk[d] < nb[d])
+        nbk[d] %= nb[d]
+        fs = f + 1 if f % 2 == 1 else f - 1
+        return ("conn", 201 if wrap else 101, index[tuple(nbk)], fs)
+
+    rec, data = build_bcs(dims, spec)
+    return Case("box3d", nodes, rec, data, prims, n_rk=3, cfl=cfl, time_accurate=True,
+                limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps,
+                extra={"sizes": sizes, "seed": seed, "amp": amp, "nmodes": nmodes})
+
+
+def channel_3d(n: int = 16, steps: int = 10, mach: float = 0.8, amp: float = 0.04,
+               limiter="vanalbada", riemann="HLLC", cfl=0.3, gamma=1.4) -> Case:
+    """3-D curvilinear channel block on [0,1]^3 (x = xi + a sin(2 pi eta),
+    y = eta + a sin(2 pi zeta), z = zeta + a sin(2 pi xi)): supersonic-static
+    inflow (405) on face 1, outflow (406) on face 2, slip walls (300) on
+    faces 3-4, extrapolation (400) on faces 5-6; uniform Mach-0.8 state."""
+    t = np.arange(n + 1, dtype=np.float64) / n
+    Z, E, X = np.meshgrid(t, t, t, indexing="ij")
+    nodes = np.stack([X + amp * np.sin(2 * np.pi * E), E + amp * np.sin(2 * np.pi * Z),
+                      Z + amp * np.sin(2 * np.pi * X)], axis=-1)
+    p_inf = 1.0 / gamma
+    prim = np.zeros((n, n, n, NPRIM))
+    prim[..., 0] = 1.0
+    prim[..., 1] = mach
+    prim[..., 4] = p_inf
+
+    def spec(b, f):
+        if f == 1:
+            return ("bc", 405, [mach, p_inf, p_inf, 0.0, 0.0, 1.0])
+        if f == 2:
+            return ("bc", 406, [p_inf, 1.0, 0.0, 0.0, 0.0, 0.0])
+        if f in (3, 4):
+            return ("bc", 300, [0.0] * 6)
+        return ("bc", 400, [0.0] * 6)
+
+    rec, data = build_bcs([(n, n, n)], spec)
+    return Case("channel3d", [np.ascontiguousarray(nodes)], rec, data, [prim], n_rk=3, cfl=cfl,
+                time_accurate=True, limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps,
+                extra={"mach": mach})

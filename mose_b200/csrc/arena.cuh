@@ -39,6 +39,9 @@ struct StageArgs {
   double cfl;
   int ndir;
   int dt_local;
+  // 3-D work lists: [0] i-sweep rows, [1] j-march columns, [2] k-march columns
+  const int4* items3[3];
+  int nitems3[3];
 };
 
 }  // namespace mose

@@ -114,6 +114,33 @@ std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int gri
   return best;
 }
 
+// Work items of the 3-D sweeps.  [0] i-sweep: (block, c0 | c1 << 16, r0, r1)
+// over rows r = j + nj k, strips as in 2-D, runs of up to 64 rows; [1] j-march
+// and [2] k-march: (block, q0, m0, m1), 256 consecutive columns q of the
+// block's (i, k) or (i, j) plane marching m over runs of at most 64 cells.
+void plan_3d_items(const std::vector<HostBlock>& blocks, std::vector<int4> out[3]) {
+  for (int q = 0; q < 3; ++q) out[q].clear();
+  for (int b = 0; b < (int)blocks.size(); ++b) {
+    const HostBlock& h = blocks[b];
+    const int ns = (h.ni + SB_W - 1) / SB_W;
+    const std::vector<int> cc = split_even(h.ni, ns, 2);
+    const int rows = h.nj * h.nk;
+    const std::vector<int> rc = split_even(rows, (rows + 63) / 64, SB_Y);
+    for (size_t r = 0; r + 1 < rc.size(); ++r)
+      for (int s = 0; s < ns; ++s)
+        if (rc[r + 1] > rc[r] && cc[s + 1] > cc[s])
+          out[0].push_back(make_int4(b, cc[s] | (cc[s + 1] << 16), rc[r], rc[r + 1]));
+    for (int dir = 1; dir <= 2; ++dir) {
+      const int nl = dir == 1 ? h.nj : h.nk, nother = dir == 1 ? h.nk : h.nj;
+      const int ncol = h.ni * nother;
+      const std::vector<int> mc = split_even(nl, (nl + 63) / 64, 1);
+      for (size_t r = 0; r + 1 < mc.size(); ++r)
+        for (int q0 = 0; q0 < ncol; q0 += SB_T)
+          if (mc[r + 1] > mc[r]) out[dir].push_back(make_int4(b, q0, mc[r], mc[r + 1]));
+    }
+  }
+}
+
 }  // namespace
 
 struct mose_gpu_ctx {
@@ -142,6 +169,8 @@ struct mose_gpu_ctx {
   DevBuf<BcParam> bcp;
   DevBuf<GhostRec> ghosts;
   DevBuf<int4> items;
+  DevBuf<int4> items3[3];     // 3-D sweeps
+  int nitems3[3] = {0, 0, 0};
   DevBuf<double> scal;        // [0] dtglobal, [1] time
   DevBuf<unsigned long long> dtmin;
   DevBuf<int> iterdev;
@@ -376,7 +405,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   else ctx->ndir = 2;
   ctx->nd = (ctx->ndir == 3) ? 3 : 2;
   ctx->nv = (ctx->nd == 3) ? 5 : 4;
-  if (ctx->nd == 3) return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: not yet on this path");
+  if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: HLLC or AUSM+ with minmod, van Leer or van Albada");
   auto nodeh = [&](const HostBlock& h, int i, int j, int k, int c) {
     return h.node[3 * ((size_t)i + (size_t)(h.ni + 1) * ((size_t)j + (size_t)(h.nj + 1) * k)) + c];
   };
@@ -390,7 +420,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "axisymmetric 2-D meshes are not on this path");
   }
   // 2-D: planar blocks so that n_z == 0 on i and j faces and w stays 0
-  for (int b = 0; b < nb; ++b) {
+  for (int b = 0; b < nb && ctx->nd == 2; ++b) {
     const HostBlock& h = ctx->hblk[b];
     if (h.nk != 1) return fail(ctx, MOSE_ERR_UNSUPPORTED, "mixed 2-D / 3-D blocks");
     for (int j = 0; j <= h.nj; ++j)
@@ -401,14 +431,18 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   }
   for (auto& e : ctx->bc) {
     const HostBlock& h = ctx->hblk[e.b - 1];
-    if (e.f >= 5 && e.type != 0)
+    if (ctx->nd == 2 && e.f >= 5 && e.type != 0)
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D k faces must be null (type 0), found %d", e.type);
-    bool degenerate = (e.f >= 3 && e.f <= 4 && h.nj < 3) || (e.f <= 2 && h.ni < 3);
+    bool degenerate = (e.f >= 3 && e.f <= 4 && h.nj < 3) || (e.f <= 2 && h.ni < 3) ||
+                      (ctx->nd == 3 && e.f >= 5 && h.nk < 3);
     if (degenerate && !(e.type == 0 || e.type == 400 || e.type == 406))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "bc type %d on a face of a block thinner than 3 cells", e.type);
-    if (e.type == 405 && e.data[4] != 0.0)
+    if (ctx->nd == 2 && e.type == 405 && e.data[4] != 0.0)
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
   }
+  for (int b = 0; b < nb && ctx->nd == 3; ++b)
+    if (ctx->hblk[b].nk < 1 || ctx->hblk[b].ni >= 65536)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "block %d: 3-D extents out of range", b + 1);
 
   // ---- layout ----------------------------------------------------------------
   ctx->desc.assign(nb, BlockDesc{});
@@ -573,6 +607,16 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   ctx->nitems = (int)items.size();
   CU(ctx->items.alloc(items.size()));
   CU(cudaMemcpy(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  if (ctx->nd == 3) {
+    std::vector<int4> it3[3];
+    plan_3d_items(ctx->hblk, it3);
+    for (int q = 0; q < 3; ++q) {
+      ctx->nitems3[q] = (int)it3[q].size();
+      CU(ctx->items3[q].alloc(std::max<size_t>(it3[q].size(), 1)));
+      if (!it3[q].empty())
+        CU(cudaMemcpy(ctx->items3[q].p, it3[q].data(), it3[q].size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+  }
   ctx->cur = 0;
   ctx->po = 1;
   CU(cudaDeviceSynchronize());
@@ -729,7 +773,22 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   a.time_accurate = ctx->cfg.time_accurate;
   a.err = ctx->derr.p;
   a.g = ctx->gas;
+  for (int q = 0; q < 3; ++q) {
+    a.items3[q] = ctx->items3[q].p;
+    a.nitems3[q] = ctx->nitems3[q];
+  }
   return a;
+}
+
+// One RK stage (mode 0 / 2) or one residual evaluation (mode 1) on every
+// block: the 2-D kernel, or the three 3-D sweeps.  Returns the kernel count
+// (0: no kernel for this configuration).
+static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int prec, bool uni) {
+  if (ctx->nd == 3)
+    return launch_stage3d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
+               ? (ctx->nitems3[0] > 0 ? 3 : 2)
+               : 0;
+  return launch_stage2d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream) ? 1 : 0;
 }
 
 int mose_gpu_residual(mose_gpu_ctx* ctx) {
@@ -737,10 +796,10 @@ int mose_gpu_residual(mose_gpu_ctx* ctx) {
   if (rc) return rc;
   // the phase-by-phase path always runs the reference-exact arithmetic
   StageArgs a = stage_args(ctx, ctx->cur, ctx->po, -1, 1);
-  if (!launch_stage2d(a, ctx->nsm, 1, false, MOSE_PRECISION_FP64_EXACT, ctx->cfg.riemann, ctx->cfg.limiter,
-                      ctx->stream))
-    return fail(ctx, MOSE_ERR_UNSUPPORTED, "no kernel for this solver / limiter");
-  ctx->launches++;
+  // the residual-only kernels read the metric arrays
+  const int nk = launch_stage(ctx, a, 1, MOSE_PRECISION_FP64_EXACT, false);
+  if (!nk) return fail(ctx, MOSE_ERR_UNSUPPORTED, "no kernel for this solver / limiter");
+  ctx->launches += nk;
   return check_launch(ctx, "residual");
 }
 
@@ -798,9 +857,7 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
     if (ctx->nghost) ++k;
     StageArgs a = stage_args(ctx, pc, s0, pn, irk);
     if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
-    launch_stage2d(a, ctx->nsm, a.dtmin ? 2 : 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
-                   ctx->stream);
-    ++k;
+    k += launch_stage(ctx, a, a.dtmin ? 2 : 0, ctx->cfg.precision, ctx->uniform);
     pc = pn;
   }
   return k;
@@ -942,10 +999,8 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
       }
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
       if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
-      launch_stage2d(a, ctx->nsm, a.dtmin ? 2 : 0, ctx->uniform, ctx->cfg.precision, ctx->cfg.riemann, ctx->cfg.limiter,
-                     ctx->stream);
+      launches[2] += launch_stage(ctx, a, a.dtmin ? 2 : 0, ctx->cfg.precision, ctx->uniform);
       mark(2);
-      launches[2] += 1;
       pc = pn;
     }
     ctx->dt_valid = fused_dt(ctx);

@@ -1,0 +1,337 @@
+// stage3d.cuh -- residual + RK-stage kernels for 3-D blocks: three directional
+// sweeps per RK stage over every block.
+//
+// The reference accumulates a cell's residual in a fixed order: the interior
+// i-faces (low then high), the interior j-faces, the interior k-faces
+// (Mod_Fluxes.f90:89-179), then the boundary faces in face order 1..6
+// (BC_Fluxes walks the bc list, Mod_BC_Fluxes.f90:52-216).  The 3-D path keeps
+// that order with one kernel per direction and the residual in HBM between
+// them (FP64, so the round trip is exact):
+//   k_sweep3d_i:  R  = -F(i-1/2) + F(i+1/2)     (interior i-faces)
+//   k_march3d<1>: R += -G(j-1/2) + G(j+1/2)     (interior j-faces)
+//   k_march3d<2>: R += -H(k-1/2) + H(k+1/2), then the boundary-face terms of
+//                 faces 1..6, then Newstate (or R itself in residual mode) and
+//                 the next step's CFL dt on the new state.
+// The i-sweep exchanges slopes and face fluxes through shared memory along
+// rows of 62 cells (one halo column each side).  The j- and k-sweeps march:
+// each thread walks one column along j (or k) with the three-cell stencil, the
+// limited slope and the lower face flux in registers, so every interior face
+// flux is formed once and loads are coalesced across threads in i.
+// Boundary faces are formed only for boundary cells, in the last sweep: the
+// interior formula with the ghosts for connections (101/201, as
+// BC_Connection_Eul does), boundary_flux() for the other types.
+#pragma once
+
+#include "stage2d.cuh"
+
+namespace mose {
+namespace s3 {
+
+constexpr int NV = 5;
+
+__device__ __forceinline__ long long off3(const BlockDesc& d, int i, int j, int k) { return cell_off3(d, i, j, k); }
+
+// dl of cell o along direction dir
+template <bool UNI>
+__device__ __forceinline__ double dl_at(const StageArgs& a, const BlockDesc& d, int dir, long long o) {
+  if constexpr (UNI) return d.u_dl[dir];
+  else return a.m.dl[3 * d.mbase + dir * d.vstride + o];
+}
+// normal and area of the low face along dir of cell o
+template <bool UNI>
+__device__ __forceinline__ double face_at(const StageArgs& a, const BlockDesc& d, int dir, long long o, double* n) {
+  if constexpr (UNI) {
+    n[0] = d.u_n[dir][0]; n[1] = d.u_n[dir][1]; n[2] = d.u_n[dir][2];
+    return d.u_A[dir];
+  } else {
+    const long long vs = d.vstride;
+    const double* f = a.m.face + 12 * d.mbase + (4 * dir) * vs + o;
+    n[0] = f[0]; n[1] = f[vs]; n[2] = f[2 * vs];
+    return f[3 * vs];
+  }
+}
+__device__ __forceinline__ void loadQ(const double* P, long long vs, long long o, double* q) {
+#pragma unroll
+  for (int v = 0; v < NV; ++v) q[v] = P[v * vs + o];
+}
+
+// Limited slope of q between qa (low side) and qb (high side) with dl da, d0,
+// db along the line (Lib_Reconstruction.f90:10-29 with l = (dl_a + dl_b) / 2).
+template <class PH, bool UNI>
+__device__ __forceinline__ void lslope(const double* qa, const double* q, const double* qb, double da, double d0,
+                                       double db, double* s) {
+  constexpr bool FU = UNI && PH::kFast;
+  if constexpr (FU) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = PH::lim(qb[v] - q[v], q[v] - qa[v]);
+  } else {
+    const double la = 0.5 * (da + d0), lb = 0.5 * (d0 + db);
+    double ila = 0.0, ilb = 0.0;
+    if constexpr (PH::kFast) { ila = PH::inv_len(la); ilb = PH::inv_len(lb); }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) s[v] = PH::lim(PH::slope(qb[v] - q[v], lb, ilb), PH::slope(q[v] - qa[v], la, ila));
+  }
+}
+
+// Face flux between cells L (state PL, slope sL, dl dL) and R from the
+// reconstructed states; n, A the face metric.  false: check_gas_state rejects.
+template <class PH, bool UNI>
+__device__ __forceinline__ bool face(const Gas& g, const double* PL, const double* sL, double dL, const double* PR,
+                                     const double* sR, double dR, const double* n, double A, double* F) {
+  constexpr bool FU = UNI && PH::kFast;
+  const double hm = FU ? 0.5 : 0.5 * dL, hp = FU ? 0.5 : 0.5 * dR;
+  double QL[NV], QR[NV];
+#pragma unroll
+  for (int v = 0; v < NV; ++v) {
+    QL[v] = PL[v] + sL[v] * hm;
+    QR[v] = PR[v] - sR[v] * hp;
+  }
+  return PH::template face<NV>(g, QL, QR, n, A, F);
+}
+
+// Boundary-face term of face f (1..6) of boundary cell (i, j, k) of block b:
+// returns the add mask and the flux in F (per the reference's BC_Fluxes).
+template <class PH, int RIE, int LIM, bool UNI>
+__device__ __noinline__ int bc_face(const StageArgs& a, int b, int f, int i, int j, int k, double* F) {
+  const BlockDesc& d = a.blk[b];
+  const int dir = (f - 1) / 2;
+  const bool high = (f % 2) == 0;
+  const int idx = (f <= 2) ? j + d.nj * k : (f <= 4) ? i + d.ni * k : i + d.ni * j;
+  const int w = a.bcw[d.bcoff[f - 1] + idx];
+  const int code = bc_code(w);
+  if (code == BC_NONE) return ADD_NONE;
+  const double* P = a.Pc + d.sbase;
+  const long long vs = d.vstride;
+  const int di = dir == 0, dj = dir == 1, dk = dir == 2;
+  // cells along the face normal, m = 0 the boundary cell, m > 0 inward
+  const int sgn = high ? -1 : 1;
+  auto cell = [&](int m) { return off3(d, i + sgn * m * di, j + sgn * m * dj, k + sgn * m * dk); };
+  double n[3];
+  // the boundary face is the low face of the boundary cell, or of the next cell
+  const double A = face_at<UNI>(a, d, dir, high ? off3(d, i + di, j + dj, k + dk) : cell(0), n);
+  if (code == BC_CONN) {
+    // interior formula across the face with the ghost cells: stencil
+    // (-2, -1 | 0, 1) on the low side, (n-2, n-1 | n, n+1) on the high side
+    double q[4][NV], dl[4];
+    for (int s = 0; s < 4; ++s) {
+      // offset from the boundary cell along +dir, low index first: the face
+      // lies between stencil cells 1 and 2
+      const int t = high ? s - 1 : s - 2;
+      const long long o = off3(d, i + di * t, j + dj * t, k + dk * t);
+      loadQ(P, vs, o, q[s]);
+      dl[s] = dl_at<UNI>(a, d, dir, o);
+    }
+    double sL[NV], sR[NV];
+    lslope<PH, UNI>(q[0], q[1], q[2], dl[0], dl[1], dl[2], sL);
+    lslope<PH, UNI>(q[1], q[2], q[3], dl[1], dl[2], dl[3], sR);
+    face<PH, UNI>(a.g, q[1], sL, dl[1], q[2], sR, dl[2], n, A, F);
+    return ADD_ALL;
+  }
+  double Q[NV], Qi[NV];
+  loadQ(P, vs, cell(0), Q);
+  loadQ(P, vs, cell(1), Qi);
+  return boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dl_at<UNI>(a, d, dir, cell(0)), dl_at<UNI>(a, d, dir, cell(1)), n,
+                                     A, f, F);
+}
+
+}  // namespace s3
+
+// ---- i-sweep ------------------------------------------------------------------
+// Items: (block, c0 | c1 << 16, r0, r1) with rows r = j + nj k.  A CTA takes
+// SB_Y rows at a time, SB_X thread columns on cells c0 - 1 .. c0 + 62.
+template <class PH, int RIE, int LIM, bool UNI>
+__global__ void __launch_bounds__(SB_T, 2) k_sweep3d_i(StageArgs a, const int4* items, int nitems) {
+  using namespace s3;
+  __shared__ double sP[NV][SB_Y][SB_X + 2];
+  __shared__ double sD[SB_Y][SB_X + 2];
+  __shared__ double sS[NV][SB_Y][SB_X];
+  __shared__ double sF[NV][SB_Y][SB_X];
+  const int t = threadIdx.x, tx = t % SB_X, ty = t / SB_X;
+#pragma unroll 1
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 item = items[it];
+    const int b = item.x, c0 = item.y & 0xffff, c1 = item.y >> 16, r0 = item.z, r1 = item.w;
+    const BlockDesc& d = a.blk[b];
+    const int ni = d.ni, nj = d.nj;
+    const long long vs = d.vstride;
+    const double* P = a.Pc + d.sbase;
+    const int c = c0 - 1 + tx;
+#pragma unroll 1
+    for (int rb = r0; rb < r1; rb += SB_Y) {
+      const int r = rb + ty;
+      const bool rowok = r < r1;
+      const int j = rowok ? r % nj : 0, k = rowok ? r / nj : 0;
+      __syncthreads();
+      if (rowok) {
+        auto put = [&](int cc, int col) {
+          if (cc > ni + 1) return;
+          const long long o = off3(d, cc, j, k);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) sP[v][ty][col] = P[v * vs + o];
+          sD[ty][col] = dl_at<UNI>(a, d, 0, o);
+        };
+        put(c, tx + 1);
+        if (tx == 0) put(c0 - 2, 0);
+        if (tx == SB_X - 1) put(c0 + SB_X - 1, SB_X + 1);
+      }
+      __syncthreads();
+      if (rowok && c <= ni) {
+        double qa[NV], q[NV], qb[NV], s[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { qa[v] = sP[v][ty][tx]; q[v] = sP[v][ty][tx + 1]; qb[v] = sP[v][ty][tx + 2]; }
+        lslope<PH, UNI>(qa, q, qb, sD[ty][tx], sD[ty][tx + 1], sD[ty][tx + 2], s);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sS[v][ty][tx] = s[v];
+      }
+      __syncthreads();
+      // interior face c + 1/2, 0 <= c <= ni - 2
+      if (rowok && tx < SB_X - 1 && c >= 0 && c <= ni - 2 && c <= c1 - 1) {
+        double PL[NV], PR[NV], sL[NV], sR[NV], F[NV], n[3];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          PL[v] = sP[v][ty][tx + 1]; PR[v] = sP[v][ty][tx + 2];
+          sL[v] = sS[v][ty][tx]; sR[v] = sS[v][ty][tx + 1];
+        }
+        const double A = face_at<UNI>(a, d, 0, off3(d, c + 1, j, k), n);
+        const bool ok = face<PH, UNI>(a.g, PL, sL, sD[ty][tx + 1], PR, sR, sD[ty][tx + 2], n, A, F);
+        if (!ok) report(a.err, 4, b, c, j, k);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) sF[v][ty][tx] = F[v];
+      }
+      __syncthreads();
+      if (rowok && tx >= 1 && c < c1) {
+        ResAcc<NV, PH::kCompensated> R;
+        R.init();
+        if (c > 0) for (int v = 0; v < NV; ++v) R.add(v, -sF[v][ty][tx - 1]);
+        if (c < ni - 1) for (int v = 0; v < NV; ++v) R.add(v, sF[v][ty][tx]);
+        const long long o = off3(d, c, j, k);
+        double* Rb = a.R + d.sbase;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Rb[v * vs + o] = R.get(v);
+      }
+    }
+  }
+}
+
+// ---- j- and k-sweeps ------------------------------------------------------------
+// DIR = 1 (j) or 2 (k).  Items: (block, q0, m0, m1): threads q0 .. q0 + 255 of
+// the block's columns q = i + ni * other (other = k for DIR 1, j for DIR 2)
+// march m = j (or k) over [m0, m1).  MODE: 3 = add the interior faces to R
+// (j-sweep); 0 = last sweep, fused Newstate; 1 = last sweep, residual only;
+// 2 = last sweep, fused Newstate and the next step's CFL dt.
+template <class PH, int RIE, int LIM, bool UNI, int DIR, int MODE>
+__global__ void __launch_bounds__(SB_T, 2) k_march3d(StageArgs a, const int4* items, int nitems) {
+  using namespace s3;
+  double dtrun = __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll 1
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 item = items[it];
+    const int b = item.x, m0 = item.z, m1 = item.w;
+    const BlockDesc& d = a.blk[b];
+    const int ni = d.ni, nj = d.nj, nk = d.nk;
+    const int nl = (DIR == 1) ? nj : nk, nother = (DIR == 1) ? nk : nj;
+    const int q = item.y + threadIdx.x;
+    if (q >= ni * nother) continue;
+    const int i = q % ni, other = q / ni;
+    const long long vs = d.vstride;
+    const long long S = (DIR == 1) ? (long long)d.px : d.plane;   // stride along the march
+    const double* P = a.Pc + d.sbase;
+    double* Rb = a.R + d.sbase;
+    const long long obase = (DIR == 1) ? off3(d, i, 0, other) : off3(d, i, other, 0);   // cell m = 0
+    auto om = [&](int m) { return obase + (long long)m * S; };
+    // march state: P(m), P(m+1), slope(m), lower face flux G(m-1/2)
+    double p0[NV], p1[NV], p2[NV], s0[NV], s1[NV], Gm[NV], Gp[NV];
+    double d0, d1, d2;
+    {
+      double pm2[NV], pm1[NV], sm1[NV];
+      loadQ(P, vs, om(m0 - 2), pm2);
+      loadQ(P, vs, om(m0 - 1), pm1);
+      loadQ(P, vs, om(m0), p0);
+      loadQ(P, vs, om(m0 + 1), p1);
+      const double dm2 = dl_at<UNI>(a, d, DIR, om(m0 - 2)), dm1 = dl_at<UNI>(a, d, DIR, om(m0 - 1));
+      d0 = dl_at<UNI>(a, d, DIR, om(m0));
+      d1 = dl_at<UNI>(a, d, DIR, om(m0 + 1));
+      lslope<PH, UNI>(pm2, pm1, p0, dm2, dm1, d0, sm1);
+      lslope<PH, UNI>(pm1, p0, p1, dm1, d0, d1, s0);
+      if (m0 > 0) {
+        double n[3];
+        const double A = face_at<UNI>(a, d, DIR, om(m0), n);
+        const bool ok = face<PH, UNI>(a.g, pm1, sm1, dm1, p0, s0, d0, n, A, Gm);
+        const int jj = (DIR == 1) ? m0 : other, kk = (DIR == 1) ? other : m0;
+        if (!ok) report(a.err, 4, b, i, jj, kk);
+      }
+    }
+#pragma unroll 1
+    for (int m = m0; m < m1; ++m) {
+      loadQ(P, vs, om(m + 2), p2);
+      d2 = dl_at<UNI>(a, d, DIR, om(m + 2));
+      lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
+      const int j = (DIR == 1) ? m : other, k = (DIR == 1) ? other : m;
+      if (m <= nl - 2) {
+        double n[3];
+        const double A = face_at<UNI>(a, d, DIR, om(m + 1), n);
+        const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Gp);
+        if (!ok) report(a.err, 4, b, i, j, k);
+      }
+      const long long o = om(m);
+      ResAcc<NV, PH::kCompensated> R;
+      R.init();
+#pragma unroll
+      for (int v = 0; v < NV; ++v) R.s[v] = Rb[v * vs + o];
+      if (m > 0) for (int v = 0; v < NV; ++v) R.add(v, -Gm[v]);
+      if (m < nl - 1) for (int v = 0; v < NV; ++v) R.add(v, Gp[v]);
+      if constexpr (MODE == 3) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Rb[v * vs + o] = R.get(v);
+      } else {
+        // boundary faces in face order 1..6
+        const bool on[6] = {i == 0, i == ni - 1, j == 0, j == nj - 1, k == 0, k == nk - 1};
+        for (int f = 1; f <= 6; ++f) {
+          if (!on[f - 1]) continue;
+          double F[NV];
+          const int mask = bc_face<PH, RIE, LIM, UNI>(a, b, f, i, j, k, F);
+          add_bc<NV>(R, F, (f % 2) ? -1.0 : 1.0, mask);
+        }
+        double Rv[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
+        if constexpr (MODE == 1) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) Rb[v * vs + o] = Rv[v];
+        } else {
+          double vol;
+          if constexpr (UNI) vol = d.u_vol; else vol = a.m.vol[d.mbase + o];
+          const double dt = a.time_accurate ? *a.dtg : a.dtl[d.mbase + o];
+          double Q[NV], QO[NV];
+#pragma unroll
+          for (int v = 0; v < NV; ++v) Q[v] = p0[v];
+          const bool first = (a.irk == 1);
+          if (!first) loadQ(a.Po + d.sbase, vs, o, QO);
+          const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
+          if (!ok) report(a.err, 5, b, i, j, k);
+          double* Pn = a.Pn + d.sbase;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
+          if constexpr (MODE == 2) dtrun = fmin(dtrun, cfl_dt<NV, UNI, PH::kFast>(a.g, Q, d, a.m, o, a.ndir, a.cfl));
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) { p0[v] = p1[v]; p1[v] = p2[v]; s0[v] = s1[v]; Gm[v] = Gp[v]; }
+      d0 = d1; d1 = d2;
+    }
+  }
+  if constexpr (MODE == 2) {
+    __shared__ double red[SB_T / 32];
+    const int t = threadIdx.x;
+    for (int s = 16; s > 0; s >>= 1) dtrun = fmin(dtrun, __shfl_xor_sync(0xffffffffu, dtrun, s));
+    if ((t & 31) == 0) red[t >> 5] = dtrun;
+    __syncthreads();
+    if (t == 0) {
+      double v = red[0];
+      for (int w = 1; w < SB_T / 32; ++w) v = fmin(v, red[w]);
+      atomicMin(a.dtmin, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
+}  // namespace mose
