@@ -241,6 +241,53 @@ def mixed_error(local, steps=100):
             "against": "reference-exact GPU path (bit-identical to the FP64 oracle)"}
 
 
+def config_report(name, make_case, local, steps, precisions=PRECISIONS):
+    """Throughput of each precision (graph-replayed steps, CUDA events) on one
+    configuration, and the mixed precision's density error against the
+    reference-exact path (bit-identical to the FP64 oracle) after `steps`."""
+    import torch
+    from mose_b200 import Solver
+    from mose_b200.cases import GC
+    case = make_case()
+    out = {"cells": case.ncells, "blocks": len(case.nodes), "steps": steps, "limiter": case.limiter,
+           "riemann": case.riemann, "cfl": case.cfl}
+    dens = {}
+    for prec in precisions:
+        s = Solver(case, precision=precision_code(prec), device=local)
+        stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
+        s.advance(2)
+        ms = time_advance(s, stream, steps, 1)
+        out[prec] = {"value": case.ncells * steps / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / steps}
+        s.close()
+        # error run from the initial state
+        s = Solver(case, precision=precision_code(prec), device=local)
+        s.advance(steps)
+        dens[prec] = [s.download_prim(b)[GC:-GC, GC:-GC, GC:-GC, 0].copy() for b in range(1, len(case.nodes) + 1)]
+        s.close()
+    for prec in precisions:
+        if prec == "exact":
+            continue
+        num = sum(float(((g - r) ** 2).sum()) for g, r in zip(dens[prec], dens["exact"]))
+        den = sum(float((r ** 2).sum()) for r in dens["exact"])
+        li = max(float(np.abs(g - r).max()) for g, r in zip(dens[prec], dens["exact"])) / \
+            max(float(np.abs(r).max()) for r in dens["exact"])
+        out[prec]["density_error_vs_exact"] = {"l2": float(np.sqrt(num / den)), "linf": li, "steps": steps}
+    return {name: out}
+
+
+def extra_configs(local):
+    """The other benchmark configurations at their full sizes: the 64-block
+    four-quadrant problem (one persistent kernel per stage over all blocks,
+    graph-replayed steps) and the 3-D periodic box of 8 blocks of 128^3."""
+    from mose_b200 import cases
+    rep = {}
+    rep.update(config_report("quadrant2d_64_blocks_ausm_minmod",
+                             lambda: cases.four_quadrant(seed=0, steps=100), local, 100))
+    rep.update(config_report("box3d_8x128^3_hllc_vanleer",
+                             lambda: cases.periodic_box_3d(128, steps=50, seed=0), local, 50))
+    return rep
+
+
 def run_gpu(args):
     world, rank, local = dist_init()
     import torch
@@ -296,6 +343,7 @@ def run_gpu(args):
                           "stage_ms": v_stage_ms, "roofline_frac": v_ach / peak, "step_kernel_ms": v_step}
         v.close()
     err = mixed_error(local) if rank == 0 else None
+    extra = extra_configs(local) if (rank == 0 and not args.no_extra_configs) else None
     if rank == 0:
         variants.setdefault("mixed", {})["error_vs_fp64_oracle"] = err
         line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
@@ -313,6 +361,8 @@ def run_gpu(args):
                 "step_bytes_per_cell": BYTES_PER_CELL_STEP,
                 "hbm_frac_whole_step": BYTES_PER_CELL_STEP * cells * args.steps / (ms / 1e3 / world) / 1e9 / peak,
                 "variants": variants}
+        if extra is not None:
+            line["configs"] = extra
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
@@ -331,6 +381,8 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=list(PRECISIONS),
                     help="precision of the headline value; the others are reported under variants")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra-configs", action="store_true",
+                    help="skip the four-quadrant and 3-D configuration reports")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + K fused steps (the command profiled by ncu); prints nothing")
     args = ap.parse_args()

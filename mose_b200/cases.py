@@ -93,6 +93,21 @@ def _face_cells(ni, nj, nk, f):
     return [(i, j, k) for j in range(1, nj + 1) for i in range(1, ni + 1)]
 
 
+def _face_cells_np(ni, nj, nk, f):
+    """(n, 3) int array of the 1-based (i, j, k) of face f's cells, in file
+    order (k, j, i loops, the last index fastest as _face_cells lists them)."""
+    if f in (1, 2):
+        k, j = np.meshgrid(np.arange(1, nk + 1), np.arange(1, nj + 1), indexing="ij")
+        i = np.full_like(k, 1 if f == 1 else ni)
+    elif f in (3, 4):
+        k, i = np.meshgrid(np.arange(1, nk + 1), np.arange(1, ni + 1), indexing="ij")
+        j = np.full_like(k, 1 if f == 3 else nj)
+    else:
+        j, i = np.meshgrid(np.arange(1, nj + 1), np.arange(1, ni + 1), indexing="ij")
+        k = np.full_like(j, 1 if f == 5 else nk)
+    return np.stack([i.ravel(), j.ravel(), k.ravel()], axis=1)
+
+
 def build_bcs(dims, face_spec):
     """Boundary records in bc.txt order.
 
@@ -104,24 +119,33 @@ def build_bcs(dims, face_spec):
     for b, (ni, nj, nk) in enumerate(dims, start=1):
         for f in range(1, 7):
             spec = face_spec(b, f)
-            for (i, j, k) in _face_cells(ni, nj, nk, f):
-                if spec[0] == "bc":
-                    _, t, d6 = spec
-                    recs.append([b, i, j, k, f, t, 0, 0, 0, 0, 0, 0, 0, 0, 0])
-                    data.append(list(d6))
+            ijk = _face_cells_np(ni, nj, nk, f)
+            r = np.zeros((len(ijk), 15), dtype=np.int32)
+            r[:, 0] = b
+            r[:, 1:4] = ijk
+            r[:, 4] = f
+            r[:, 5] = spec[1]
+            dd = np.zeros((len(ijk), 6))
+            if spec[0] == "bc":
+                dd[:] = np.asarray(spec[2], dtype=np.float64)
+            else:
+                _, t, bs, fs = spec
+                sni, snj, snk = dims[bs - 1]
+                src = ijk.copy()
+                if fs in (1, 2):
+                    src[:, 0] = 1 if fs == 1 else sni
+                elif fs in (3, 4):
+                    src[:, 1] = 1 if fs == 3 else snj
                 else:
-                    _, t, bs, fs = spec
-                    sni, snj, snk = dims[bs - 1]
-                    si, sj, sk = i, j, k
-                    if fs == 1: si = 1
-                    elif fs == 2: si = sni
-                    elif fs == 3: sj = 1
-                    elif fs == 4: sj = snj
-                    elif fs == 5: sk = 1
-                    else: sk = snk
-                    recs.append([b, i, j, k, f, t, bs, si, sj, sk, fs, 1, 0, 0, 1])
-                    data.append([0.0] * 6)
-    return np.asarray(recs, dtype=np.int32), np.asarray(data, dtype=np.float64)
+                    src[:, 2] = 1 if fs == 5 else snk
+                r[:, 6] = bs
+                r[:, 7:10] = src
+                r[:, 10] = fs
+                r[:, 11] = 1
+                r[:, 14] = 1
+            recs.append(r)
+            data.append(dd)
+    return np.concatenate(recs, axis=0), np.concatenate(data, axis=0)
 
 
 def cell_centres(nodes: np.ndarray):

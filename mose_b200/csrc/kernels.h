@@ -17,7 +17,7 @@ void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, con
 void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir, int* flags,
                           double* firsts, cudaStream_t s);
 void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, double* P, MetricArgs m, int nd,
-                        cudaStream_t s);
+                        DevError* err, cudaStream_t s);
 void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,
                        double* dtl, unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
                        int ramp_iter, int store_local, bool uniform, cudaStream_t s);

@@ -70,8 +70,15 @@ __global__ void k_face_metrics(const BlockDesc* blk, int b, NodeView nv, double*
 // BC_Connect_Metrics (101), BC_Symmetry_Metrics (300), BC_Extrapolate_Metrics
 // (everything else), Lib_Metrics.f90:535-1092.
 __device__ void store_ghost_dl(const BlockDesc* blk, double* dl, int b, int nd, int I, int J, int K, int dir,
-                               double val) {
+                               double val, DevError* err) {
   const BlockDesc& d = blk[b];
+  // bounds self-check: the cell must lie inside the ghosted extents
+  const bool in = I - 1 >= -GW && I - 1 < d.ni + GW && J - 1 >= -GW && J - 1 < d.nj + GW &&
+                  (nd == 2 || (K - 1 >= -GW && K - 1 < d.nk + GW));
+  if (!in) {
+    if (atomicCAS(&err->code, 0, 1) == 0) { err->b = b + 1; err->i = I; err->j = J; err->k = K; }
+    return;
+  }
   long long o = (nd == 3) ? cell_off3(d, I - 1, J - 1, K - 1) : cell_off2(d, I - 1, J - 1);
   dl[3 * d.mbase + dir * d.vstride + o] = val;
 }
@@ -86,6 +93,12 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
   const BlockDesc& bm = blk[e.b];
   const NodeView& nv = nodes[e.b];
   const int Im = e.I, Jm = e.J, Km = e.K;
+  // self-check: the node view must describe this record's block (and source)
+  if (nv.p == nullptr || nv.ni != bm.ni || nv.nj != bm.nj || nv.nk != bm.nk ||
+      (e.type == 101 && (nodes[e.bs].p == nullptr || nodes[e.bs].ni != blk[e.bs].ni))) {
+    if (atomicCAS(&err->code, 0, 1) == 0) { err->b = -2; err->i = q; err->j = e.b; err->k = e.bs; }
+    return;
+  }
   double M[9], l[3], v;
   bool ok = true;
   if (e.type == 300) {
@@ -102,7 +115,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
       }
       long long so = (nd == 3) ? cell_off3(bm, si - 1, sj - 1, sk - 1) : cell_off2(bm, si - 1, sj - 1);
       double val = dl[3 * bm.mbase + dir * bm.vstride + so];
-      store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, val);
+      store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, val, err);
     }
     return;
   }
@@ -159,7 +172,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
         case 5: ok &= metric_tensor(N[0][g], N[0][g - 1], N[2][g], N[2][g - 1], N[4][g], N[4][g - 1], N[6][g], N[6][g - 1], M, l, &v); gk = Km - g; break;
         case 6: ok &= metric_tensor(N[1][g - 1], N[1][g], N[3][g - 1], N[3][g], N[5][g - 1], N[5][g], N[7][g - 1], N[7][g], M, l, &v); gk = Km + g; break;
       }
-      store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, l[dir]);
+      store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, l[dir], err);
     }
   } else {
     // BC_Extrapolate_Metrics (delthe = 0 branches)
@@ -173,7 +186,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
         for (int g = -1; g >= -GW; --g) {
           for (int s = 0; s < 4; ++s) at(s, g) = v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3));
           ok &= metric_tensor(at(0, g), at(1, g), at(2, g), at(3, g), at(0, g + 1), at(1, g + 1), at(2, g + 1), at(3, g + 1), M, l, &v);
-          store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir]);
+          store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir], err);
         }
         break;
       case 2:
@@ -184,7 +197,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
         for (int g = 1; g <= GW; ++g) {
           for (int s = 4; s < 8; ++s) at(s, g) = v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3));
           ok &= metric_tensor(at(4, g - 1), at(5, g - 1), at(6, g - 1), at(7, g - 1), at(4, g), at(5, g), at(6, g), at(7, g), M, l, &v);
-          store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir]);
+          store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir], err);
         }
         break;
       case 3: {
@@ -198,7 +211,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           const int sl[4] = {0, 1, 4, 5};
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3)) : v3lin2(at(s, g + 1), at(s, g + 2));
           ok &= metric_tensor(at(0, g), at(1, g), at(0, g + 1), at(1, g + 1), at(4, g), at(5, g), at(4, g + 1), at(5, g + 1), M, l, &v);
-          store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir]);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir], err);
         }
         break;
       }
@@ -213,7 +226,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           const int sl[4] = {2, 3, 6, 7};
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3)) : v3lin2(at(s, g - 1), at(s, g - 2));
           ok &= metric_tensor(at(2, g - 1), at(3, g - 1), at(2, g), at(3, g), at(6, g - 1), at(7, g - 1), at(6, g), at(7, g), M, l, &v);
-          store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir]);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir], err);
         }
         break;
       }
@@ -228,7 +241,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           const int sl[4] = {0, 2, 4, 6};
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3)) : v3lin2(at(s, g + 1), at(s, g + 2));
           ok &= metric_tensor(at(0, g), at(0, g + 1), at(2, g), at(2, g + 1), at(4, g), at(4, g + 1), at(6, g), at(6, g + 1), M, l, &v);
-          store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir]);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir], err);
         }
         break;
       }
@@ -243,7 +256,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           const int sl[4] = {1, 3, 5, 7};
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3)) : v3lin2(at(s, g - 1), at(s, g - 2));
           ok &= metric_tensor(at(1, g - 1), at(1, g), at(3, g - 1), at(3, g), at(5, g - 1), at(5, g), at(7, g - 1), at(7, g), M, l, &v);
-          store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir]);
+          store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir], err);
         }
         break;
       }
@@ -299,7 +312,7 @@ __global__ void k_uniform_check(const BlockDesc* blk, int b, MetricArgs m, int n
 // ---------------------------------------------------------------------------
 template <int NV>
 __global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nrec, double* P, MetricArgs m,
-                              int nd) {
+                              int nd, DevError* err) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nrec) return;
   const GhostRec e = recs[q];
@@ -311,7 +324,15 @@ __global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nr
   const int gk = (e.f == 5) ? 1 : (e.f == 6) ? -1 : 0;
   double* Pb = P + d.sbase;
   const long long vs = d.vstride;
-  auto off = [&](const BlockDesc& bb, int i, int j, int k) {
+  // offset of a cell; self-check: -1 (and the access is skipped) for a cell
+  // outside the ghosted extents of its block
+  auto off = [&](const BlockDesc& bb, int i, int j, int k) -> long long {
+    const bool in = i >= -GW && i < bb.ni + GW && j >= -GW && j < bb.nj + GW &&
+                    (nd == 2 || (k >= -GW && k < bb.nk + GW));
+    if (!in) {
+      if (atomicCAS(&err->code, 0, 1) == 0) { err->b = -3; err->i = i; err->j = j; err->k = k; }
+      return -1;
+    }
     return (nd == 3) ? cell_off3(bb, i, j, k) : cell_off2(bb, i, j);
   };
   if (e.type == BC_CONN) {     // Ghost_Connection :140-160
@@ -323,6 +344,7 @@ __global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nr
     for (int g = 1; g <= GW; ++g) {
       long long od = off(d, e.i - gi * g, e.j - gj * g, e.k - gk * g);
       long long os = off(s, e.is + si * (g - 1), e.js + sj * (g - 1), e.ks + sk * (g - 1));
+      if (od < 0 || os < 0) continue;
       for (int v = 0; v < NV; ++v) Pb[v * vs + od] = Ps[v * s.vstride + os];
     }
   } else if (e.type == BC_SYM) {  // Ghost_Symmetry :193-225 (first ghost only)
@@ -332,6 +354,7 @@ __global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nr
     // or of the next cell (even faces)
     int fi = e.i + (e.f == 2), fj = e.j + (e.f == 4), fk = e.k + (e.f == 6);
     long long of = off(d, fi, fj, fk);
+    if (ob < 0 || og < 0 || of < 0) return;
     const double* fp = m.face + 12 * d.mbase + (4 * dir) * vs + of;
     double n[3] = {fp[0], fp[vs], fp[2 * vs]};
     double q[NV];
@@ -345,13 +368,16 @@ __global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nr
       long long oa = off(d, e.i - gi * (g - 1), e.j - gj * (g - 1), e.k - gk * (g - 1));
       long long oc = off(d, e.i - gi * (g - 2), e.j - gj * (g - 2), e.k - gk * (g - 2));
       long long oe = off(d, e.i - gi * (g - 3), e.j - gj * (g - 3), e.k - gk * (g - 3));
+      if (od < 0 || oa < 0 || oc < 0 || oe < 0) continue;
       for (int v = 0; v < NV; ++v)
         Pb[v * vs + od] = 3.0 * Pb[v * vs + oa] - 3.0 * Pb[v * vs + oc] + Pb[v * vs + oe];
     }
   } else {                        // Ghost_ZG_Extrapolate :279-304 (0, 401-407, 420)
     long long ob = off(d, e.i, e.j, e.k);
+    if (ob < 0) return;
     for (int g = 1; g <= GW; ++g) {
       long long od = off(d, e.i - gi * g, e.j - gj * g, e.k - gk * g);
+      if (od < 0) continue;
       for (int v = 0; v < NV; ++v) Pb[v * vs + od] = Pb[v * vs + ob];
     }
   }
@@ -626,10 +652,10 @@ void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricA
   k_uniform_check<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, m, nd, ndir, flags, firsts);
 }
 void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, double* P, MetricArgs m, int nd,
-                        cudaStream_t s) {
+                        DevError* err, cudaStream_t s) {
   if (nrec == 0) return;
-  if (nd == 3) k_fill_ghosts<5><<<(nrec + 127) / 128, 128, 0, s>>>(dblk, recs, nrec, P, m, nd);
-  else k_fill_ghosts<4><<<(nrec + 127) / 128, 128, 0, s>>>(dblk, recs, nrec, P, m, nd);
+  if (nd == 3) k_fill_ghosts<5><<<(nrec + 127) / 128, 128, 0, s>>>(dblk, recs, nrec, P, m, nd, err);
+  else k_fill_ghosts<4><<<(nrec + 127) / 128, 128, 0, s>>>(dblk, recs, nrec, P, m, nd, err);
 }
 void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,
                        double* dtl, unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,

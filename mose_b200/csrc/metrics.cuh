@@ -27,7 +27,14 @@ __device__ __forceinline__ V3 v3lin2(const V3& a, const V3& b) {                
 struct NodeView {
   const double* p;
   int ni, nj, nk;
+  DevError* err;   // bounds self-check: an index outside 0..n is recorded here and clamped
   __device__ __forceinline__ V3 at(int i, int j, int k) const {
+    if (i < 0 || i > ni || j < 0 || j > nj || k < 0 || k > nk) {
+      if (err && atomicCAS(&err->code, 0, 1) == 0) { err->b = -1; err->i = i; err->j = j; err->k = k; }
+      i = i < 0 ? 0 : (i > ni ? ni : i);
+      j = j < 0 ? 0 : (j > nj ? nj : j);
+      k = k < 0 ? 0 : (k > nk ? nk : k);
+    }
     const double* q = p + 3 * ((long long)i + (long long)(ni + 1) * ((long long)j + (long long)(nj + 1) * k));
     return V3{{q[0], q[1], q[2]}};
   }

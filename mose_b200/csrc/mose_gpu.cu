@@ -363,11 +363,15 @@ int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, 
   for (auto& h : ctx->hblk) expect += 2LL * ((long long)h.nj * h.nk + (long long)h.ni * h.nk + (long long)h.ni * h.nj);
   if (nbound != expect)
     return fail(ctx, MOSE_ERR_INVALID, "boundary records (%d) differ from the block faces (%lld)", nbound, expect);
-  ctx->bc.resize(nbound);
+  // Null (type 0) records of the k faces of single-plane blocks are kept out
+  // of the list: such faces are never active (a 3-D domain needs nk > 1 in
+  // every block) and a 2-D domain has ni * nj of them per face.
+  ctx->bc.clear();
+  ctx->bc.reserve(std::min<long long>(nbound, 1LL << 20));
   int lastkey = -1;
   for (int q = 0; q < nbound; ++q) {
     const int32_t* r = rec + 15 * (size_t)q;
-    BcRecord& e = ctx->bc[q];
+    BcRecord e;
     e.b = r[0]; e.i = r[1]; e.j = r[2]; e.k = r[3]; e.f = r[4]; e.type = r[5];
     e.bs = r[6]; e.is = r[7]; e.js = r[8]; e.ks = r[9]; e.fs = r[10];
     e.d11 = r[11]; e.d12 = r[12]; e.d21 = r[13]; e.d22 = r[14];
@@ -388,6 +392,8 @@ int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, 
       if (e.is < 1 || e.is > s.ni || e.js < 1 || e.js > s.nj || e.ks < 1 || e.ks > s.nk)
         return fail(ctx, MOSE_ERR_INVALID, "record %d: connection source out of range", q + 1);
     }
+    if (e.type == 0 && e.f >= 5 && h.nk == 1) continue;
+    ctx->bc.push_back(e);
   }
   return MOSE_OK;
 }
@@ -494,6 +500,11 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   }
 
   // ---- allocation --------------------------------------------------------------
+  // Every upload below is a cudaMemcpyAsync on the context's stream: a plain
+  // cudaMemcpy from pageable memory may return before its DMA has landed and
+  // runs on the legacy default stream, which the context's non-blocking
+  // stream does not wait for, so the kernels enqueued next could read the
+  // buffer before it is written.
   for (int s = 0; s < 3; ++s)
     if (ctx->state[s].alloc((size_t)ctx->nv * mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (state)");
   if (ctx->resid.alloc((size_t)ctx->nv * mcur) != cudaSuccess || ctx->dl.alloc(3 * (size_t)mcur) != cudaSuccess ||
@@ -509,9 +520,9 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   CU(ctx->derr.alloc(1));
   CU(ctx->norms.alloc(5));
   CU(ctx->partial.alloc(5 * (size_t)norms_partial_count(nb, ctx->maxcell)));
-  CU(cudaMemcpy(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ctx->bcw.p, bcwords.data(), bcwords.size() * sizeof(int), cudaMemcpyHostToDevice));
-  if (!params.empty()) CU(cudaMemcpy(ctx->bcp.p, params.data(), params.size() * sizeof(BcParam), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->bcw.p, bcwords.data(), bcwords.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  if (!params.empty()) CU(cudaMemcpyAsync(ctx->bcp.p, params.data(), params.size() * sizeof(BcParam), cudaMemcpyHostToDevice, ctx->stream));
 
   // ---- metrics on the device -------------------------------------------------
   std::vector<DevBuf<double>> dnodes(nb);
@@ -519,12 +530,12 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   for (int b = 0; b < nb; ++b) {
     const HostBlock& h = ctx->hblk[b];
     CU(dnodes[b].alloc(h.node.size()));
-    CU(cudaMemcpy(dnodes[b].p, h.node.data(), h.node.size() * sizeof(double), cudaMemcpyHostToDevice));
-    views[b] = NodeView{dnodes[b].p, h.ni, h.nj, h.nk};
+    CU(cudaMemcpyAsync(dnodes[b].p, h.node.data(), h.node.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    views[b] = NodeView{dnodes[b].p, h.ni, h.nj, h.nk, ctx->derr.p};
   }
   DevBuf<NodeView> dviews;
   CU(dviews.alloc(nb));
-  CU(cudaMemcpy(dviews.p, views.data(), nb * sizeof(NodeView), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(dviews.p, views.data(), nb * sizeof(NodeView), cudaMemcpyHostToDevice, ctx->stream));
   MetricArgs m = ctx->margs();
   for (int b = 0; b < nb; ++b) {
     const HostBlock& h = ctx->hblk[b];
@@ -545,10 +556,12 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   // interior dl which is final after the cell kernel.
   DevBuf<GhostMetricRec> dgm;
   CU(dgm.alloc(gm.size()));
-  CU(cudaMemcpy(dgm.p, gm.data(), gm.size() * sizeof(GhostMetricRec), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(dgm.p, gm.data(), gm.size() * sizeof(GhostMetricRec), cudaMemcpyHostToDevice, ctx->stream));
   launch_ghost_metrics(ctx->d_desc.p, dgm.p, (int)gm.size(), dviews.p, m, ctx->nd, ctx->ndir, ctx->derr.p, ctx->stream);
   {
     int rc = check_launch(ctx, "metrics");
+    if (rc) return rc;
+    rc = poll_device_error(ctx);   // metric failures and index self-checks
     if (rc) return rc;
   }
   // uniformity
@@ -585,7 +598,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     for (int dd = 0; dd < 3; ++dd)
       for (int q = 0; q < 3; ++q) d.u_vers[dd][q] = f[16 + 3 * dd + q];
   }
-  CU(cudaMemcpy(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
 
   // ---- ghost-fill records (Fill_Ghost_Cell dispatch, Lib_Ghost.f90:50-73) ------
   std::vector<GhostRec> gr;
@@ -600,13 +613,13 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   }
   ctx->nghost = (int)gr.size();
   CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
-  if (!gr.empty()) CU(cudaMemcpy(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice));
+  if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
 
   // ---- work items for the stage kernel -----------------------------------------
   std::vector<int4> items = plan_stage_items(ctx->hblk, 2 * ctx->nsm);
   ctx->nitems = (int)items.size();
   CU(ctx->items.alloc(items.size()));
-  CU(cudaMemcpy(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  CU(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
   if (ctx->nd == 3) {
     std::vector<int4> it3[3];
     plan_3d_items(ctx->hblk, it3);
@@ -614,7 +627,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       ctx->nitems3[q] = (int)it3[q].size();
       CU(ctx->items3[q].alloc(std::max<size_t>(it3[q].size(), 1)));
       if (!it3[q].empty())
-        CU(cudaMemcpy(ctx->items3[q].p, it3[q].data(), it3[q].size() * sizeof(int4), cudaMemcpyHostToDevice));
+        CU(cudaMemcpyAsync(ctx->items3[q].p, it3[q].data(), it3[q].size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
     }
   }
   ctx->cur = 0;
@@ -747,7 +760,7 @@ int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
 int mose_gpu_fill_ghosts(mose_gpu_ctx* ctx) {
   int rc = require_ready(ctx);
   if (rc) return rc;
-  launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[ctx->cur].p, ctx->margs(), ctx->nd,
+  launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[ctx->cur].p, ctx->margs(), ctx->nd, ctx->derr.p,
                      ctx->stream);
   ctx->launches++;
   return check_launch(ctx, "fill_ghosts");
@@ -852,7 +865,7 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
   int pc = s0;
   for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
     int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
-    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd,
+    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
                        ctx->stream);
     if (ctx->nghost) ++k;
     StageArgs a = stage_args(ctx, pc, s0, pn, irk);
@@ -992,7 +1005,7 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
     for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
       int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
       if (ctx->nghost) {
-        launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd,
+        launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
                            ctx->stream);
         mark(1);
         launches[1] += 1;
