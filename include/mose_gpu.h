@@ -219,6 +219,34 @@ int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N
  * rounded one.  No context needed; synchronous. */
 int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
 
+/* ---- Discrete adjoint (2-D, HLLC with minmod / van Leer / van Albada,
+ * time-accurate SSP-RK).  The objective is the pressure integral over one
+ * block face, J = sum over the face cells of p * A (the wall-pressure
+ * convention of Lib_BC_Fluxes.f90:48-72).  The adjoint differentiates the
+ * whole Explicit_Step: every RK stage, the boundary fluxes (405 also in the
+ * inflow Mach), the ghost fill and the global CFL dt (through its argmin
+ * cell). */
+/* Sets the Mach number of every 405 supersonic-inflow face. */
+int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach);
+/* Runs nsteps fused steps from the current state keeping a checkpoint of the
+ * state every `interval` steps (sqrt(nsteps) is the usual choice), and
+ * returns J on face `face` (1..4) of block `block` of the final state. */
+int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval, int32_t block, int32_t face,
+                             double* J);
+/* Reverse sweep of the preceding mose_gpu_adjoint_forward: each checkpoint
+ * segment is recomputed (recording its stage inputs) and differentiated
+ * back.  Leaves dJ/dP of the initial state in the context's adjoint state
+ * (mose_gpu_download_adjoint) and returns dJ/dMach; the state returns to the
+ * forward run's final state. */
+int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach);
+/* One step of the adjoint at the current state P^n: the adjoint state goes
+ * from lambda^{n+1} (uploaded) to lambda^n = (dP^{n+1}/dP^n)^T lambda^{n+1};
+ * *dJ_dmach = lambda^{n+1} . dP^{n+1}/dMach.  The state stays P^n. */
+int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach);
+/* The adjoint state of block b in the reference layout of P (w entries 0). */
+int mose_gpu_upload_adjoint(mose_gpu_ctx* ctx, int32_t b, const double* lam);
+int mose_gpu_download_adjoint(mose_gpu_ctx* ctx, int32_t b, double* lam);
+
 #ifdef __cplusplus
 }
 #endif

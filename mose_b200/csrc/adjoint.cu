@@ -1,0 +1,530 @@
+// adjoint.cu -- discrete adjoint of the 2-D explicit step (HLLC with minmod,
+// van Leer or van Albada; time-accurate SSP-RK; general metrics).
+//
+// One RK stage is P_s = U2P(U0 + c ((U(P_{s-1}) - U0) - R(P_{s-1}) dt / vol))
+// with U0 = U(P^n) (Lib_Newstate.f90:134-160, Lib_RK.f90:15-27).  Its
+// adjoint, given lam = dJ/dP_s:
+//   lam_V = J_U2P(P_s)^T lam                         (k_adj_pre)
+//   dJ/dP_{s-1} += J_P2U(P_{s-1})^T (c lam_V)          (k_adj_pre)
+//   dJ/dP^n     += J_P2U(P^n)^T ((1 - c) lam_V)        (k_adj_pre)
+//   lam_R = -(dt / vol) c lam_V ;  dJ/ddt += sum R . (-(c / vol) lam_V)
+//   dJ/dP_{s-1} += (dR/dP_{s-1})^T lam_R               (faces, gather, ghosts)
+// The residual's transpose is face-local: every face recomputes its flux
+// from its four-cell stencil, runs the reverse sweep of HLLC, the limiter
+// and the reconstruction with the face-flux adjoint lam_R(left) -
+// lam_R(right), and stores the four stencil cells' contributions; a per-cell
+// gather then sums the (up to eight) contributions of a cell, so nothing is
+// accumulated with atomics and the result does not depend on scheduling.
+// Boundary faces (a few per thousand) use central-difference Jacobians of
+// the reference boundary formulas (405 also in the inflow Mach); connection
+// faces run the interior face's reverse sweep over the ghost stencil.  The
+// ghost fill (Lib_Ghost.f90) is transposed face by face.  The global CFL dt
+// of the step (Mod_dt.f90) contributes through its argmin cell.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels.h"
+#include "physics_adjoint.cuh"
+#include "stage2d.cuh"
+
+namespace mose {
+
+namespace {
+
+constexpr int NV = 4;
+
+__device__ __forceinline__ long long off(const BlockDesc& d, int i, int j) { return cell_off2(d, i, j); }
+
+// dl along dir of cell o (metric arrays)
+__device__ __forceinline__ double dl_at(const MetricArgs& m, const BlockDesc& d, int dir, long long o) {
+  return m.dl[3 * d.mbase + dir * d.vstride + o];
+}
+__device__ __forceinline__ double face_at(const MetricArgs& m, const BlockDesc& d, int dir, long long o, double* n) {
+  const long long vs = d.vstride;
+  const double* f = m.face + 12 * d.mbase + (4 * dir) * vs + o;
+  n[0] = f[0]; n[1] = f[vs]; n[2] = f[2 * vs];
+  return f[3 * vs];
+}
+
+// Reverse sweep of one face: stencil q[0..3] (cells c-1 .. c+2 along the
+// direction, the face between q[1] and q[2]), dl[0..3], face normal n, area
+// A; Fb the adjoint of the area-scaled face flux.  Returns the flux (area
+// scaled) in F and the stencil cells' adjoint contributions in C[4][NV].
+template <int LIM>
+__device__ __forceinline__ void face_vjp(const Gas& g, const double q[4][NV], const double* dl, const double* n,
+                                         double A, const double* Fb, double* F, double C[4][NV]) {
+  const double la = 0.5 * (dl[0] + dl[1]), lb = 0.5 * (dl[1] + dl[2]), lc = 0.5 * (dl[2] + dl[3]);
+  double QL[NV], QR[NV], dsLx[NV], dsLy[NV], dsRx[NV], dsRy[NV];
+  for (int v = 0; v < NV; ++v) {
+    const double sa = (q[1][v] - q[0][v]) / la, sb = (q[2][v] - q[1][v]) / lb, sc = (q[3][v] - q[2][v]) / lc;
+    const double sL = adj::limiter_grad<LIM>(sb, sa, &dsLx[v], &dsLy[v]);
+    const double sR = adj::limiter_grad<LIM>(sc, sb, &dsRx[v], &dsRy[v]);
+    QL[v] = q[1][v] + sL * (0.5 * dl[1]);
+    QR[v] = q[2][v] - sR * (0.5 * dl[2]);
+  }
+  double Fa[NV], Fu[NV], QLb[NV] = {0, 0, 0, 0}, QRb[NV] = {0, 0, 0, 0};
+  for (int v = 0; v < NV; ++v) Fa[v] = Fb[v] * A;
+  adj::hllc_vjp(g.gamma, g.gcp, g.gm1, QL, QR, n[0], n[1], Fa, Fu, QLb, QRb);
+  for (int v = 0; v < NV; ++v) F[v] = Fu[v] * A;
+  for (int v = 0; v < NV; ++v) {
+    for (int s = 0; s < 4; ++s) C[s][v] = 0.0;
+    C[1][v] += QLb[v];
+    C[2][v] += QRb[v];
+    const double sLb = QLb[v] * (0.5 * dl[1]), sRb = -QRb[v] * (0.5 * dl[2]);
+    // sL = phi(sb, sa): sb = (q2 - q1) / lb, sa = (q1 - q0) / la
+    const double sbb = sLb * dsLx[v] + sRb * dsRy[v];   // sb also feeds sR as its upwind slope
+    const double sab = sLb * dsLy[v];
+    const double scb = sRb * dsRx[v];
+    C[2][v] += sbb / lb; C[1][v] -= sbb / lb;
+    C[1][v] += sab / la; C[0][v] -= sab / la;
+    C[3][v] += scb / lc; C[2][v] -= scb / lc;
+  }
+}
+
+}  // namespace
+
+// ---- per-cell pre-step ---------------------------------------------------------
+// lam (adjoint of P_s) -> lamR = -(dt/vol) c lam_V, wdt = -(c/vol) lam_V,
+// lam_loc = J_P2U(P_{s-1})^T c lam_V, lam_n += J_P2U(P^n)^T (1-c) lam_V.
+__global__ void k_adj_pre(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* Ps, const double* Pprev,
+                          const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc,
+                          double* lam_n, double c, const double* dtg) {
+  const BlockDesc& d = blk[b];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= d.ni || j >= d.nj) return;
+  const long long vs = d.vstride, o = d.sbase + off(d, i, j), om = d.mbase + off(d, i, j);
+  double P[NV], L[NV], V[NV];
+  for (int v = 0; v < NV; ++v) { P[v] = Ps[o + v * vs]; L[v] = lam[o + v * vs]; }
+  adj::u2p_vjp(g.gm1, P, L, V);
+  const double vol = m.vol[om], dt = *dtg;
+  double Q[NV], Ub[NV], loc[NV] = {0, 0, 0, 0}, acc[NV] = {0, 0, 0, 0};
+  for (int v = 0; v < NV; ++v) {
+    Ub[v] = c * V[v];
+    lamR[o + v * vs] = -(dt / vol) * Ub[v];
+    wdt[o + v * vs] = -Ub[v] / vol;
+  }
+  for (int v = 0; v < NV; ++v) Q[v] = Pprev[o + v * vs];
+  adj::p2u_vjp(g.igm1, Q, Ub, loc);
+  for (int v = 0; v < NV; ++v) { Q[v] = Pn[o + v * vs]; Ub[v] = (1.0 - c) * V[v]; }
+  adj::p2u_vjp(g.igm1, Q, Ub, acc);
+  for (int v = 0; v < NV; ++v) {
+    lam_loc[o + v * vs] = loc[v];
+    lam_n[o + v * vs] += acc[v];
+  }
+}
+
+// ---- interior faces along dir ----------------------------------------------------
+// Face between cells (i, j) and its dir-neighbour, stored at (i, j): the four
+// stencil contributions in C (16 planes per direction) and the flux in F.
+template <int LIM>
+__global__ void k_adj_faces(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* P, const double* lamR,
+                            double* C, double* F, int dir) {
+  const BlockDesc& d = blk[b];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  const int di = dir == 0, dj = dir == 1;
+  if (i >= d.ni - di || j >= d.nj - dj) return;   // interior faces only
+  const long long vs = d.vstride;
+  double q[4][NV], dl[4];
+  for (int s = 0; s < 4; ++s) {
+    const long long o = off(d, i + di * (s - 1), j + dj * (s - 1));
+    for (int v = 0; v < NV; ++v) q[s][v] = P[d.sbase + o + v * vs];
+    dl[s] = dl_at(m, d, dir, o);
+  }
+  const long long oc = off(d, i, j), on = off(d, i + di, j + dj);
+  double n[3], Fb[NV], Fv[NV], Cc[4][NV];
+  const double A = face_at(m, d, dir, on, n);
+  for (int v = 0; v < NV; ++v) Fb[v] = lamR[d.sbase + oc + v * vs] - lamR[d.sbase + on + v * vs];
+  face_vjp<LIM>(g, q, dl, n, A, Fb, Fv, Cc);
+  const long long base = 16 * d.mbase + oc;
+  for (int s = 0; s < 4; ++s)
+    for (int v = 0; v < NV; ++v) C[base + (4 * s + v) * vs] = Cc[s][v];
+  for (int v = 0; v < NV; ++v) F[4 * d.mbase + oc + v * vs] = Fv[v];
+}
+
+// ---- boundary faces ------------------------------------------------------------
+// One thread per boundary face cell of faces 1..4 (list: block, face, cell
+// index along the face, bc-table entry).  Stores the face term's adjoint
+// contributions to the four cells along the face normal (slots in increasing
+// index: -2..1 on a low face, n-2..n+1 on a high face), the face term itself
+// (already signed and masked, as added to the boundary cell's residual) and
+// dJ/dMach of a 405 face.
+template <int RIE, int LIM>
+__global__ void k_adj_bc(StageArgs a, const int4* list, int nlist, const double* lamR, double* Cb, double* Fbc,
+                         double* dmach) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nlist) return;
+  const int4 e = list[q];
+  const int b = e.x, f = e.y, idx = e.z, ent = e.w;
+  const BlockDesc& d = a.blk[b];
+  const int dir = (f - 1) / 2;
+  const bool high = (f % 2) == 0;
+  const int i = dir == 0 ? (high ? d.ni - 1 : 0) : idx, j = dir == 1 ? (high ? d.nj - 1 : 0) : idx;
+  const int di = dir == 0, dj = dir == 1;
+  const long long vs = d.vstride;
+  const double sgn = high ? 1.0 : -1.0;
+  const int w = a.bcw[d.bcoff[f - 1] + idx];
+  const int code = bc_code(w);
+  double out[4][NV], Fout[NV];
+  for (int s = 0; s < 4; ++s)
+    for (int v = 0; v < NV; ++v) out[s][v] = 0.0;
+  for (int v = 0; v < NV; ++v) Fout[v] = 0.0;
+  double dm = 0.0;
+  const long long ob = off(d, i, j);
+  double Lr[NV];
+  for (int v = 0; v < NV; ++v) Lr[v] = lamR[d.sbase + ob + v * vs];
+  // stencil cells along the normal, increasing index: t = -2..1 (low) or -1..2 (high) from the boundary cell
+  auto cell = [&](int s) { const int t = high ? s - 1 : s - 2; return off(d, i + di * t, j + dj * t); };
+  double n[3];
+  const double A = face_at(a.m, d, dir, high ? off(d, i + di, j + dj) : ob, n);
+  if (code == BC_CONN) {
+    double qq[4][NV], dl[4], Fb[NV], Fv[NV];
+    for (int s = 0; s < 4; ++s) {
+      const long long o = cell(s);
+      for (int v = 0; v < NV; ++v) qq[s][v] = a.Pc[d.sbase + o + v * vs];
+      dl[s] = dl_at(a.m, d, dir, o);
+    }
+    for (int v = 0; v < NV; ++v) Fb[v] = sgn * Lr[v];
+    face_vjp<LIM>(a.g, qq, dl, n, A, Fb, Fv, out);
+    for (int v = 0; v < NV; ++v) Fout[v] = sgn * Fv[v];
+  } else if (code != BC_NONE) {
+    // central-difference Jacobian of the reference boundary formula in
+    // (Q, Qi) = (boundary cell, first interior cell), and in the inflow Mach
+    const int sb = high ? 1 : 2, si = high ? 0 : 3;   // slots of the boundary / interior cell
+    double Q[NV], Qi[NV], Fv[NV];
+    for (int v = 0; v < NV; ++v) { Q[v] = a.Pc[d.sbase + cell(sb) + v * vs]; Qi[v] = a.Pc[d.sbase + cell(si) + v * vs]; }
+    const double dlB = dl_at(a.m, d, dir, cell(sb)), dlI = dl_at(a.m, d, dir, cell(si));
+    const int mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fv);
+    double keep[NV];
+    for (int v = 0; v < NV; ++v) {
+      keep[v] = (mask == ADD_ALL || (mask == ADD_MOMENTUM && v >= 1 && v < NV - 1)) ? 1.0 : 0.0;
+      Fout[v] = sgn * keep[v] * Fv[v];
+    }
+    double Fb[NV];
+    for (int v = 0; v < NV; ++v) Fb[v] = sgn * keep[v] * Lr[v];
+    for (int side = 0; side < 2; ++side) {
+      double* X = side == 0 ? Q : Qi;
+      for (int k = 0; k < NV; ++k) {
+        const double x0 = X[k], h = 1e-6 * fmax(fabs(x0), 1e-3);
+        double Fp[NV], Fm[NV];
+        X[k] = x0 + h;
+        boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fp);
+        X[k] = x0 - h;
+        boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fm);
+        X[k] = x0;
+        double s = 0.0;
+        for (int v = 0; v < NV; ++v) s += Fb[v] * (Fp[v] - Fm[v]) / (2.0 * h);
+        out[side == 0 ? sb : si][k] = s;
+      }
+    }
+    if (code == BC_SUPIN) {
+      BcParam p = a.bcp[bc_param(w)];
+      const double M0 = p.mach, h = 1e-6 * fmax(fabs(M0), 1e-3);
+      double Fp[NV], Fm[NV];
+      p.mach = M0 + h;
+      ex::bc_supersonic_inflow<RIE, LIM, NV>(a.g, Q, Qi, p, n, A, f, Fp);
+      p.mach = M0 - h;
+      ex::bc_supersonic_inflow<RIE, LIM, NV>(a.g, Q, Qi, p, n, A, f, Fm);
+      // only where boundary_flux takes the inflow branch (its test !(s Un >= 0))
+      const double Un = ex::dot_vel<NV>(Q, n), s405 = (double)(1 - 2 * (f % 2));
+      if (!(s405 * Un >= 0.0))
+        for (int v = 0; v < NV; ++v) dm += Fb[v] * (Fp[v] - Fm[v]) / (2.0 * h);
+    }
+  }
+  for (int s = 0; s < 4; ++s)
+    for (int v = 0; v < NV; ++v) Cb[(size_t)ent * 16 + 4 * s + v] = out[s][v];
+  for (int v = 0; v < NV; ++v) Fbc[(size_t)ent * 4 + v] = Fout[v];
+  dmach[ent] = dm;
+}
+
+// ---- gather ------------------------------------------------------------------------
+// Ghosted cells: lamG = sum of the interior-face contributions that reach the
+// cell; interior cells also form R . wdt of the interior faces (dt partial).
+__global__ void k_adj_gather(const BlockDesc* blk, int b, const double* Cx, const double* Cy, const double* Fx,
+                             const double* Fy, const double* wdt, double* lamG, double* dtpart) {
+  const BlockDesc& d = blk[b];
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - GW, j = (int)blockIdx.y - GW;
+  if (i >= d.ni + GW || j >= d.nj + GW) return;
+  const long long vs = d.vstride, oc = off(d, i, j);
+  double acc[NV] = {0, 0, 0, 0};
+  // x faces between (f, j) and (f + 1, j), f = 0..ni-2: cell i is slot s = i - f + 1
+  if (j >= 0 && j < d.nj)
+    for (int s = 0; s < 4; ++s) {
+      const int f = i - s + 1;
+      if (f < 0 || f > d.ni - 2) continue;
+      const long long base = 16 * d.mbase + off(d, f, j);
+      for (int v = 0; v < NV; ++v) acc[v] += Cx[base + (4 * s + v) * vs];
+    }
+  if (i >= 0 && i < d.ni)
+    for (int s = 0; s < 4; ++s) {
+      const int f = j - s + 1;
+      if (f < 0 || f > d.nj - 2) continue;
+      const long long base = 16 * d.mbase + off(d, i, f);
+      for (int v = 0; v < NV; ++v) acc[v] += Cy[base + (4 * s + v) * vs];
+    }
+  for (int v = 0; v < NV; ++v) lamG[d.sbase + oc + v * vs] = acc[v];
+  if (i >= 0 && i < d.ni && j >= 0 && j < d.nj) {
+    double R[NV] = {0, 0, 0, 0};
+    const long long o4 = 4 * d.mbase;
+    if (i > 0) for (int v = 0; v < NV; ++v) R[v] -= Fx[o4 + off(d, i - 1, j) + v * vs];
+    if (i < d.ni - 1) for (int v = 0; v < NV; ++v) R[v] += Fx[o4 + oc + v * vs];
+    if (j > 0) for (int v = 0; v < NV; ++v) R[v] -= Fy[o4 + off(d, i, j - 1) + v * vs];
+    if (j < d.nj - 1) for (int v = 0; v < NV; ++v) R[v] += Fy[o4 + oc + v * vs];
+    double s = 0.0;
+    for (int v = 0; v < NV; ++v) s += R[v] * wdt[d.sbase + oc + v * vs];
+    dtpart[d.mbase + oc] = s;
+  }
+}
+
+// Boundary-face contributions of face f (entries of one face touch distinct cells).
+__global__ void k_adj_bc_gather(const BlockDesc* blk, const int4* list, int first, int n, const double* Cb,
+                                const double* Fbc, const double* wdt, double* lamG, double* dtpart) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int4 e = list[first + q];
+  const int b = e.x, f = e.y, idx = e.z, ent = e.w;
+  const BlockDesc& d = blk[b];
+  const int dir = (f - 1) / 2;
+  const bool high = (f % 2) == 0;
+  const int i = dir == 0 ? (high ? d.ni - 1 : 0) : idx, j = dir == 1 ? (high ? d.nj - 1 : 0) : idx;
+  const int di = dir == 0, dj = dir == 1;
+  const long long vs = d.vstride;
+  for (int s = 0; s < 4; ++s) {
+    const int t = high ? s - 1 : s - 2;
+    const long long o = off(d, i + di * t, j + dj * t);
+    for (int v = 0; v < NV; ++v) lamG[d.sbase + o + v * vs] += Cb[(size_t)ent * 16 + 4 * s + v];
+  }
+  const long long ob = off(d, i, j);
+  double s = 0.0;
+  for (int v = 0; v < NV; ++v) s += Fbc[(size_t)ent * 4 + v] * wdt[d.sbase + ob + v * vs];
+  dtpart[d.mbase + ob] += s;
+}
+
+// Transpose of Fill_Ghost_Cell for the ghost records of one face.
+__global__ void k_adj_ghostT(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
+                             double* lamG) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const GhostRec e = recs[ids[q]];
+  const BlockDesc& d = blk[e.b];
+  const int dir = (e.f - 1) / 2;
+  const int gi = (e.f == 1) ? 1 : (e.f == 2) ? -1 : 0;
+  const int gj = (e.f == 3) ? 1 : (e.f == 4) ? -1 : 0;
+  const long long vs = d.vstride;
+  double* Lb = lamG + d.sbase;
+  auto at = [&](int g) { return off(d, e.i - gi * g, e.j - gj * g); };   // g > 0 ghost, g <= 0 interior
+  if (e.type == BC_CONN) {
+    const BlockDesc& s = blk[e.bs];
+    const int si = (e.fs == 1) ? 1 : (e.fs == 2) ? -1 : 0;
+    const int sj = (e.fs == 3) ? 1 : (e.fs == 4) ? -1 : 0;
+    double* Ls = lamG + s.sbase;
+    for (int g = 1; g <= GW; ++g) {
+      const long long od = at(g), os = off(s, e.is + si * (g - 1), e.js + sj * (g - 1));
+      for (int v = 0; v < NV; ++v) {
+        Ls[v * s.vstride + os] += Lb[v * vs + od];
+        Lb[v * vs + od] = 0.0;
+      }
+    }
+  } else if (e.type == BC_SYM) {
+    // first ghost = the boundary cell with its velocity mirrored in the wall
+    const int fi = e.i + (e.f == 2), fj = e.j + (e.f == 4);
+    const double* fp = m.face + 12 * d.mbase + (4 * dir) * vs + off(d, fi, fj);
+    const double nx = fp[0], ny = fp[vs];
+    const long long og = at(1), ob = at(0);
+    const double lr = Lb[og], lu = Lb[vs + og], lv = Lb[2 * vs + og], lp = Lb[3 * vs + og];
+    // u' = u - 2 (u.n) n  (transpose of I - 2 n n^T is itself)
+    const double dotl = lu * nx + lv * ny;
+    Lb[ob] += lr;
+    Lb[vs + ob] += lu - 2.0 * dotl * nx;
+    Lb[2 * vs + ob] += lv - 2.0 * dotl * ny;
+    Lb[3 * vs + ob] += lp;
+    for (int g = 1; g <= GW; ++g)
+      for (int v = 0; v < NV; ++v) Lb[v * vs + at(g)] = 0.0;
+  } else if (e.type == BC_EXTRAP) {
+    // forward: P(g) = 3 P(g-1) - 3 P(g-2) + P(g-3), g = 1, 2 in order
+    for (int g = GW; g >= 1; --g) {
+      const long long od = at(g), oa = at(g - 1), oc = at(g - 2), oe = at(g - 3);
+      for (int v = 0; v < NV; ++v) {
+        const double l = Lb[v * vs + od];
+        Lb[v * vs + od] = 0.0;
+        Lb[v * vs + oa] += 3.0 * l;
+        Lb[v * vs + oc] -= 3.0 * l;
+        Lb[v * vs + oe] += l;
+      }
+    }
+  } else {   // zero gradient (0, 405, 406, ...)
+    const long long ob = at(0);
+    for (int g = 1; g <= GW; ++g)
+      for (int v = 0; v < NV; ++v) {
+        Lb[v * vs + ob] += Lb[v * vs + at(g)];
+        Lb[v * vs + at(g)] = 0.0;
+      }
+  }
+}
+
+// lam_out = lam_loc + lamG on interior cells, 0 on ghosts.
+__global__ void k_adj_combine(const BlockDesc* blk, int b, const double* lam_loc, const double* lamG, double* lam_out) {
+  const BlockDesc& d = blk[b];
+  const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - GW, j = (int)blockIdx.y - GW;
+  if (i >= d.ni + GW || j >= d.nj + GW) return;
+  const long long vs = d.vstride, o = d.sbase + off(d, i, j);
+  const bool in = i >= 0 && i < d.ni && j >= 0 && j < d.nj;
+  for (int v = 0; v < NV; ++v) lam_out[o + v * vs] = in ? lam_loc[o + v * vs] + lamG[o + v * vs] : 0.0;
+}
+
+// Deterministic sum of n values into *out (+= when accumulate), one CTA.
+__global__ void k_sum(const double* x, long long n, double* out, int accumulate) {
+  __shared__ double s[256];
+  double acc = 0.0;
+  for (long long q = threadIdx.x; q < n; q += blockDim.x) acc += x[q];
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = accumulate ? *out + s[0] : s[0];
+}
+
+// The cell attaining the step's global dt, in two passes with this
+// kernel's own arithmetic (pass 0: the minimum's bit pattern into arg[1];
+// pass 1: the smallest flat index attaining it into arg[0]), so the choice
+// does not hinge on last-bit agreement with the forward pass's arithmetic.
+template <bool UNI>
+__global__ void k_dt_argmin(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* P, double cfl, int ndir,
+                            unsigned long long* arg, int pass) {
+  const BlockDesc& d = blk[b];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= d.ni || j >= d.nj) return;
+  const long long o = off(d, i, j);
+  double Q[NV];
+  for (int v = 0; v < NV; ++v) Q[v] = P[d.sbase + o + v * d.vstride];
+  const double dt = cfl_dt<NV, UNI, false>(g, Q, d, m, o, ndir, cfl);
+  const unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
+  if (pass == 0) atomicMin(arg + 1, bits);
+  else if (bits == arg[1]) atomicMin(arg, ((unsigned long long)b << 40) | (unsigned long long)o);
+}
+
+// lam_n[argmin] += (dJ/ddt) d(dt_cell)/dP at the argmin cell.
+__global__ void k_adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
+                         const double* lam_dt, double cfl, int ndir, double* lam_n) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const unsigned long long a = *arg;
+  if (a == ~0ull) return;
+  const int b = (int)(a >> 40);
+  const long long o = (long long)(a & ((1ull << 40) - 1));
+  const BlockDesc& d = blk[b];
+  const long long vs = d.vstride;
+  double Q[NV];
+  for (int v = 0; v < NV; ++v) Q[v] = P[d.sbase + o + v * vs];
+  const double a0 = sqrt(g.gamma * Q[3] / Q[0]);
+  double dtmin = 1e300, lam = 1.0, K = 0.0, sdot = 0.0, vx = 0.0, vy = 0.0;
+  for (int dd = 0; dd < ndir; ++dd) {
+    const double ux = m.vers[9 * d.mbase + (3 * dd + 0) * vs + o], uy = m.vers[9 * d.mbase + (3 * dd + 1) * vs + o];
+    const double dot = Q[1] * ux + Q[2] * uy;
+    const double l = fabs(dot) + a0, k = m.dl[3 * d.mbase + dd * vs + o] * cfl;
+    if (k / l < dtmin) { dtmin = k / l; lam = l; K = k; sdot = copysign(1.0, dot); vx = ux; vy = uy; }
+  }
+  const double f = -(*lam_dt) * K / (lam * lam);   // dJ/dlambda
+  lam_n[d.sbase + o + 0 * vs] += f * (-0.5 * a0 / Q[0]);
+  lam_n[d.sbase + o + 1 * vs] += f * sdot * vx;
+  lam_n[d.sbase + o + 2 * vs] += f * sdot * vy;
+  lam_n[d.sbase + o + 3 * vs] += f * (0.5 * a0 / Q[3]);
+}
+
+// Objective J = sum over the face cells of face f of block b of p A, and its
+// adjoint (dJ/dp = A on those cells) written into lam (zeroed elsewhere).
+__global__ void k_adj_objective(const BlockDesc* blk, int b, int f, MetricArgs m, const double* P, double* terms,
+                                double* lam) {
+  const BlockDesc& d = blk[b];
+  const int dir = (f - 1) / 2;
+  const bool high = (f % 2) == 0;
+  const int n = dir == 0 ? d.nj : d.ni;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const int i = dir == 0 ? (high ? d.ni - 1 : 0) : q, j = dir == 1 ? (high ? d.nj - 1 : 0) : q;
+  const long long o = off(d, i, j), vs = d.vstride;
+  double nn[3];
+  const double A = face_at(m, d, dir, high ? off(d, i + (dir == 0), j + (dir == 1)) : o, nn);
+  terms[q] = P[d.sbase + o + 3 * vs] * A;
+  lam[d.sbase + o + 3 * vs] = A;
+}
+
+// ---- launchers -----------------------------------------------------------------------
+namespace adjl {
+
+static dim3 cells(int ni, int nj, bool ghosted) {
+  const int nx = ni + (ghosted ? 2 * GW : 0), ny = nj + (ghosted ? 2 * GW : 0);
+  return dim3((nx + 127) / 128, ny);
+}
+
+}  // namespace adjl
+
+void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* Ps,
+             const double* Pprev, const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc,
+             double* lam_n, double c, const double* dtg, cudaStream_t s) {
+  k_adj_pre<<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, Ps, Pprev, Pn, lam, lamR, wdt, lam_loc, lam_n, c, dtg);
+}
+void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, int lim, const double* P,
+               const double* lamR, double* C, double* F, int dir, cudaStream_t s) {
+  const dim3 grid = adjl::cells(ni, nj, false);
+  switch (lim) {
+    case 1: k_adj_faces<1><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, C, F, dir); break;
+    case 2: k_adj_faces<2><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, C, F, dir); break;
+    default: k_adj_faces<3><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, C, F, dir); break;
+  }
+}
+void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,
+            double* dmach, cudaStream_t s) {
+  if (n == 0) return;
+  const int grid = (n + 127) / 128;
+  switch (lim) {
+    case 1: k_adj_bc<0, 1><<<grid, 128, 0, s>>>(a, list, n, lamR, Cb, Fbc, dmach); break;
+    case 2: k_adj_bc<0, 2><<<grid, 128, 0, s>>>(a, list, n, lamR, Cb, Fbc, dmach); break;
+    default: k_adj_bc<0, 3><<<grid, 128, 0, s>>>(a, list, n, lamR, Cb, Fbc, dmach); break;
+  }
+}
+void adj_gather(const BlockDesc* blk, int b, int ni, int nj, const double* Cx, const double* Cy,
+                const double* Fx, const double* Fy, const double* wdt, double* lamG, double* dtpart, cudaStream_t s) {
+  k_adj_gather<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, Cx, Cy, Fx, Fy, wdt, lamG, dtpart);
+}
+void adj_bc_gather(const BlockDesc* blk, const int4* list, int first, int n, const double* Cb, const double* Fbc,
+                   const double* wdt, double* lamG, double* dtpart, cudaStream_t s) {
+  if (n == 0) return;
+  k_adj_bc_gather<<<(n + 127) / 128, 128, 0, s>>>(blk, list, first, n, Cb, Fbc, wdt, lamG, dtpart);
+}
+void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
+                         double* lamG, cudaStream_t s) {
+  if (n == 0) return;
+  k_adj_ghostT<<<(n + 127) / 128, 128, 0, s>>>(blk, recs, ids, n, m, lamG);
+}
+void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,
+                 double* lam_out, cudaStream_t s) {
+  k_adj_combine<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, lam_loc, lamG, lam_out);
+}
+void adj_sum(const double* x, long long n, double* out, int accumulate, cudaStream_t s) {
+  k_sum<<<1, 256, 0, s>>>(x, n, out, accumulate);
+}
+void adj_dt_argmin(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P, double cfl,
+                   int ndir, bool uniform, unsigned long long* arg, int pass, cudaStream_t s) {
+  if (uniform) k_dt_argmin<true><<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, P, cfl, ndir, arg, pass);
+  else k_dt_argmin<false><<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, P, cfl, ndir, arg, pass);
+}
+void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
+            const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s) {
+  k_adj_dt<<<1, 32, 0, s>>>(blk, m, g, P, arg, lam_dt, cfl, ndir, lam_n);
+}
+__global__ void k_axpy(double* y, const double* x, long long n) {
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
+    y[q] += x[q];
+}
+void adj_axpy(double* y, const double* x, long long n, cudaStream_t s) {
+  const long long g = (n + 255) / 256;
+  k_axpy<<<(unsigned)(g < 148 * 8 ? g : 148 * 8), 256, 0, s>>>(y, x, n);
+}
+void adj_objective(const BlockDesc* blk, int b, int f, int n, MetricArgs m, const double* P, double* terms,
+                   double* lam, cudaStream_t s) {
+  k_adj_objective<<<(n + 127) / 128, 128, 0, s>>>(blk, b, f, m, P, terms, lam);
+}
+
+}  // namespace mose

@@ -31,6 +31,31 @@ void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* ti
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
                      cudaStream_t s);
+// Discrete adjoint (2-D, HLLC; adjoint.cu).
+void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* Ps, const double* Pprev,
+             const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc, double* lam_n, double c,
+             const double* dtg, cudaStream_t s);
+void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, int lim, const double* P,
+               const double* lamR, double* C, double* F, int dir, cudaStream_t s);
+void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,
+            double* dmach, cudaStream_t s);
+void adj_gather(const BlockDesc* blk, int b, int ni, int nj, const double* Cx, const double* Cy, const double* Fx,
+                const double* Fy, const double* wdt, double* lamG, double* dtpart, cudaStream_t s);
+void adj_bc_gather(const BlockDesc* blk, const int4* list, int first, int n, const double* Cb, const double* Fbc,
+                   const double* wdt, double* lamG, double* dtpart, cudaStream_t s);
+void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
+                         double* lamG, cudaStream_t s);
+void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,
+                 double* lam_out, cudaStream_t s);
+void adj_sum(const double* x, long long n, double* out, int accumulate, cudaStream_t s);
+void adj_dt_argmin(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P, double cfl,
+                   int ndir, bool uniform, unsigned long long* arg, int pass, cudaStream_t s);
+void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
+            const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s);
+void adj_objective(const BlockDesc* blk, int b, int f, int n, MetricArgs m, const double* P, double* terms,
+                   double* lam, cudaStream_t s);
+void adj_axpy(double* y, const double* x, long long n, cudaStream_t s);
+
 int norms_partial_count(int nblk, long long maxcell);
 void launch_residual_norms(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, const double* PO,
                            int nd, double* partial, double* out, cudaStream_t s);

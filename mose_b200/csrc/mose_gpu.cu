@@ -189,6 +189,23 @@ struct mose_gpu_ctx {
   double h_time = 0.0;
   int h_iter = 0;
 
+  // ---- discrete adjoint (adjoint.cu) ----
+  std::vector<GhostRec> hghost;          // ghost-fill records (host copy)
+  bool adj_init = false;
+  int adj_nsteps = 0, adj_interval = 0, adj_block = 0, adj_face = 0;
+  std::vector<DevBuf<double>> adj_ckpt;  // P^n at steps 0, K, 2K, ...
+  std::vector<DevBuf<double>> adj_seg;   // stage inputs (ghosts filled) of one segment, [step * 3 + stage]
+  DevBuf<double> adj_segend;             // the state after the segment's last step
+  DevBuf<double> adj_dts;                // dt of each step of the segment
+  DevBuf<double> lam, lam_loc, lam_n, lamR, wdt, lamG, Cx, Cy, Fx, Fy, dtpart, adj_scal, Cb, Fbc, dmach, objt;
+  DevBuf<unsigned long long> adj_arg;
+  DevBuf<int4> adj_bclist;               // boundary face cells of faces 1..4, grouped by face
+  int adj_bcfirst[5] = {0, 0, 0, 0, 0};  // face f's entries: [adj_bcfirst[f-1], adj_bcfirst[f])
+  DevBuf<int> adj_gids;                  // ghost records grouped by face
+  int adj_gfirst[5] = {0, 0, 0, 0, 0};
+  bool adj_recorded = false;
+  std::vector<BcParam> hbcp;             // 405 / 406 parameters (host copy)
+
   MetricArgs margs() const { return MetricArgs{dl.p, face.p, vol.p, vers.p}; }
 };
 
@@ -523,6 +540,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
   CU(cudaMemcpyAsync(ctx->bcw.p, bcwords.data(), bcwords.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   if (!params.empty()) CU(cudaMemcpyAsync(ctx->bcp.p, params.data(), params.size() * sizeof(BcParam), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->hbcp = params;
 
   // ---- metrics on the device -------------------------------------------------
   std::vector<DevBuf<double>> dnodes(nb);
@@ -612,6 +630,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     gr.push_back(g);
   }
   ctx->nghost = (int)gr.size();
+  ctx->hghost = gr;
   CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
   if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
 
@@ -656,7 +675,8 @@ static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool uplo
   if (ctx->nd == 2) P += 5 * GW * plane;
   int rc = ensure_staging(ctx, 5 * (size_t)n);
   if (rc) return rc;
-  double* dst = (arena < 0) ? ctx->resid.p : ctx->state[arena].p;
+  double* dst = (arena == -2) ? ctx->lam.p : (arena < 0) ? ctx->resid.p : ctx->state[arena].p;
+  if (arena == -2 && !ctx->lam.p) return fail(ctx, MOSE_ERR_NOT_READY, "no adjoint state yet");
   if (upload) {
     ctx->dt_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, P, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -1075,5 +1095,293 @@ int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N
   if (A) CU(cudaMemcpy(A, aa.p, n * sizeof(double), cudaMemcpyDeviceToHost));
   return check_launch(ctx, "download_faces");
 }
+
+
+// ---- discrete adjoint (kernels in adjoint.cu) -------------------------------------
+static double rk_coeff(const mose_gpu_ctx* ctx, int irk) {
+  static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
+  return RKcoeff[ctx->cfg.n_rk - 1][irk - 1];
+}
+
+// Buffers and work lists of the adjoint, made on first use.
+static int adj_prepare(mose_gpu_ctx* ctx) {
+  if (ctx->adj_init) return MOSE_OK;
+  if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: 2-D domains only");
+  if (ctx->cfg.riemann != MOSE_RIEMANN_HLLC || ctx->cfg.limiter < 1 || ctx->cfg.limiter > 3)
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: HLLC with minmod, van Leer or van Albada");
+  if (!ctx->cfg.time_accurate) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: time-accurate runs only");
+  const size_t ns = (size_t)ctx->nv * ctx->marena, m = (size_t)ctx->marena;
+  for (DevBuf<double>* b : {&ctx->lam, &ctx->lam_loc, &ctx->lam_n, &ctx->lamR, &ctx->wdt, &ctx->lamG})
+    if (b->alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
+  if (ctx->Cx.alloc(16 * m) != cudaSuccess || ctx->Cy.alloc(16 * m) != cudaSuccess || ctx->Fx.alloc(4 * m) != cudaSuccess ||
+      ctx->Fy.alloc(4 * m) != cudaSuccess || ctx->dtpart.alloc(m) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
+  CU(ctx->adj_scal.alloc(4));
+  CU(ctx->adj_arg.alloc(2));
+  // boundary face cells of faces 1..4, grouped by face (one launch per face
+  // touches each cell at most once)
+  std::vector<int4> list;
+  size_t nent = 0, maxface = 1;
+  for (const BlockDesc& d : ctx->desc) {
+    for (int f = 0; f < 6; ++f) nent = std::max(nent, (size_t)(d.bcoff[f] + d.bcn[f]));
+    maxface = std::max(maxface, (size_t)std::max(d.ni, d.nj));
+  }
+  for (int f = 1; f <= 4; ++f) {
+    ctx->adj_bcfirst[f - 1] = (int)list.size();
+    for (int b = 0; b < (int)ctx->desc.size(); ++b) {
+      const BlockDesc& d = ctx->desc[b];
+      for (int idx = 0; idx < d.bcn[f - 1]; ++idx) list.push_back(make_int4(b, f, idx, d.bcoff[f - 1] + idx));
+    }
+  }
+  ctx->adj_bcfirst[4] = (int)list.size();
+  CU(ctx->adj_bclist.alloc(std::max<size_t>(list.size(), 1)));
+  if (!list.empty())
+    CU(cudaMemcpyAsync(ctx->adj_bclist.p, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->Cb.alloc(16 * std::max<size_t>(nent, 1)) != cudaSuccess || ctx->Fbc.alloc(4 * std::max<size_t>(nent, 1)) != cudaSuccess ||
+      ctx->dmach.alloc(std::max<size_t>(nent, 1)) != cudaSuccess || ctx->objt.alloc(maxface) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
+  std::vector<int> gids;
+  for (int f = 1; f <= 4; ++f) {
+    ctx->adj_gfirst[f - 1] = (int)gids.size();
+    for (int q = 0; q < (int)ctx->hghost.size(); ++q)
+      if (ctx->hghost[q].f == f) gids.push_back(q);
+  }
+  ctx->adj_gfirst[4] = (int)gids.size();
+  CU(ctx->adj_gids.alloc(std::max<size_t>(gids.size(), 1)));
+  if (!gids.empty())
+    CU(cudaMemcpyAsync(ctx->adj_gids.p, gids.data(), gids.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  ctx->adj_init = true;
+  return MOSE_OK;
+}
+
+static int adj_segment_buffers(mose_gpu_ctx* ctx, int K) {
+  const size_t ns = (size_t)ctx->nv * ctx->marena;
+  if ((int)ctx->adj_seg.size() < 3 * K) {
+    const size_t old = ctx->adj_seg.size();
+    ctx->adj_seg.resize(3 * (size_t)K);
+    for (size_t q = old; q < ctx->adj_seg.size(); ++q)
+      if (ctx->adj_seg[q].alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
+  }
+  if (ctx->adj_segend.n < ns && ctx->adj_segend.alloc(ns) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
+  if ((int)ctx->adj_dts.n < K && ctx->adj_dts.alloc(K) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
+  return MOSE_OK;
+}
+
+// One Explicit_Step from arena s0 with the standalone Compute_dt, recording
+// every RK stage's input (ghosts filled) in adj_seg[3 k + stage] and the
+// step's dt in adj_dts[k].  Returns the arena of the new state.
+static int record_step(mose_gpu_ctx* ctx, int s0, int k) {
+  const size_t bytes = (size_t)ctx->nv * ctx->marena * sizeof(double);
+  enqueue_dt_pass(ctx, s0);
+  launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
+                      ctx->stream);
+  cudaMemcpyAsync(ctx->adj_dts.p + k, ctx->scal.p, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+  int pc = s0;
+  for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
+    const int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
+    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd,
+                       ctx->derr.p, ctx->stream);
+    cudaMemcpyAsync(ctx->adj_seg[3 * (size_t)k + irk - 1].p, ctx->state[pc].p, bytes, cudaMemcpyDeviceToDevice,
+                    ctx->stream);
+    StageArgs a = stage_args(ctx, pc, s0, pn, irk);
+    launch_stage(ctx, a, 0, ctx->cfg.precision, ctx->uniform);
+    pc = pn;
+  }
+  ctx->launches += 3 + 2 * ctx->cfg.n_rk;
+  return pc;
+}
+
+// The adjoint of recorded step k: ctx->lam holds dJ/dP^{k+1} on entry and
+// dJ/dP^k on exit; Pnext is P^{k+1}.  dJ/dMach accumulates in adj_scal[1].
+static void adj_reverse_step(mose_gpu_ctx* ctx, int k, const double* Pnext) {
+  cudaStream_t st = ctx->stream;
+  const size_t ns = (size_t)ctx->nv * ctx->marena;
+  const double* S[3] = {ctx->adj_seg[3 * (size_t)k].p, ctx->adj_seg[3 * (size_t)k + 1].p,
+                        ctx->adj_seg[3 * (size_t)k + 2].p};
+  const double* dtg = ctx->adj_dts.p + k;
+  const int nb = (int)ctx->hblk.size(), lim = ctx->cfg.limiter;
+  const MetricArgs m = ctx->margs();
+  cudaMemsetAsync(ctx->lam_n.p, 0, ns * sizeof(double), st);
+  cudaMemsetAsync(ctx->adj_scal.p, 0, sizeof(double), st);   // dJ/ddt of this step
+  const int nlist = ctx->adj_bcfirst[4];
+  for (int irk = ctx->cfg.n_rk; irk >= 1; --irk) {
+    const double* Ps = (irk == ctx->cfg.n_rk) ? Pnext : S[irk];
+    const double* Pprev = S[irk - 1];
+    const double c = rk_coeff(ctx, irk);
+    for (int b = 0; b < nb; ++b)
+      adj_pre(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, Ps, Pprev, S[0], ctx->lam.p,
+              ctx->lamR.p, ctx->wdt.p, ctx->lam_loc.p, ctx->lam_n.p, c, dtg, st);
+    for (int b = 0; b < nb; ++b) {
+      adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cx.p,
+                ctx->Fx.p, 0, st);
+      adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cy.p,
+                ctx->Fy.p, 1, st);
+    }
+    StageArgs a = stage_args(ctx, 0, 0, -1, irk);
+    a.Pc = Pprev;
+    adj_bc(a, lim, ctx->adj_bclist.p, nlist, ctx->lamR.p, ctx->Cb.p, ctx->Fbc.p, ctx->dmach.p, st);
+    cudaMemsetAsync(ctx->dtpart.p, 0, ctx->marena * sizeof(double), st);
+    for (int b = 0; b < nb; ++b)
+      adj_gather(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->Cx.p, ctx->Cy.p, ctx->Fx.p, ctx->Fy.p,
+                 ctx->wdt.p, ctx->lamG.p, ctx->dtpart.p, st);
+    for (int f = 1; f <= 4; ++f)
+      adj_bc_gather(ctx->d_desc.p, ctx->adj_bclist.p, ctx->adj_bcfirst[f - 1],
+                    ctx->adj_bcfirst[f] - ctx->adj_bcfirst[f - 1], ctx->Cb.p, ctx->Fbc.p, ctx->wdt.p, ctx->lamG.p,
+                    ctx->dtpart.p, st);
+    for (int f = 1; f <= 4; ++f)
+      adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gfirst[f - 1],
+                          ctx->adj_gfirst[f] - ctx->adj_gfirst[f - 1], m, ctx->lamG.p, st);
+    for (int b = 0; b < nb; ++b)
+      adj_combine(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->lam_loc.p, ctx->lamG.p, ctx->lam.p, st);
+    adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 1, st);
+    adj_sum(ctx->dmach.p, (long long)ctx->dmach.n, ctx->adj_scal.p + 1, 1, st);
+  }
+  // the step's dt = min over cells of the CFL dt of P^k
+  cudaMemsetAsync(ctx->adj_arg.p, 0xff, 2 * sizeof(unsigned long long), st);
+  for (int pass = 0; pass < 2; ++pass)
+    for (int b = 0; b < nb; ++b)
+      adj_dt_argmin(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, S[0], ctx->cfg.cfl, ctx->ndir,
+                    ctx->uniform, ctx->adj_arg.p, pass, st);
+  adj_dt(ctx->d_desc.p, m, ctx->gas, S[0], ctx->adj_arg.p, ctx->adj_scal.p, ctx->cfg.cfl, ctx->ndir, ctx->lam_n.p, st);
+  adj_axpy(ctx->lam.p, ctx->lam_n.p, (long long)ns, st);
+  ctx->launches += ctx->cfg.n_rk * (5 * nb + 11) + nb + 2;
+}
+
+int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  bool any = false;
+  for (auto& e : ctx->bc)
+    if (e.type == 405) any = true;
+  if (!any) return fail(ctx, MOSE_ERR_INVALID, "no 405 inflow faces");
+  // 405 records keep their parameter slots in bc order; 406 records have rel_fac but no mach
+  size_t q = 0;
+  for (auto& e : ctx->bc) {
+    if (e.type == 405) ctx->hbcp[q].mach = mach;
+    if (e.type == 405 || e.type == 406) ++q;
+  }
+  CU(cudaMemcpyAsync(ctx->bcp.p, ctx->hbcp.data(), ctx->hbcp.size() * sizeof(BcParam), cudaMemcpyHostToDevice,
+                     ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  ctx->dt_valid = false;
+  return MOSE_OK;
+}
+
+int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval, int32_t block, int32_t face,
+                             double* J) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (nsteps < 1 || interval < 1 || !J) return fail(ctx, MOSE_ERR_INVALID, "adjoint_forward: bad arguments");
+  if (block < 1 || block > (int)ctx->hblk.size() || face < 1 || face > 4)
+    return fail(ctx, MOSE_ERR_INVALID, "adjoint_forward: objective face must be face 1..4 of a block");
+  rc = adj_prepare(ctx);
+  if (rc) return rc;
+  const size_t ns = (size_t)ctx->nv * ctx->marena;
+  const int nck = (nsteps + interval - 1) / interval;
+  if ((int)ctx->adj_ckpt.size() < nck + 1) {
+    const size_t old = ctx->adj_ckpt.size();
+    ctx->adj_ckpt.resize(nck + 1);
+    for (size_t q = old; q < ctx->adj_ckpt.size(); ++q)
+      if (ctx->adj_ckpt[q].alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (checkpoints)");
+  }
+  rc = adj_segment_buffers(ctx, interval);
+  if (rc) return rc;
+  for (int mck = 0; mck < nck; ++mck) {
+    CU(cudaMemcpyAsync(ctx->adj_ckpt[mck].p, ctx->state[ctx->cur].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    const int cnt = std::min(interval, nsteps - mck * interval);
+    rc = mose_gpu_advance(ctx, cnt, nullptr, nullptr);
+    if (rc) return rc;
+  }
+  // the final state (restored after the backward sweep) and the objective
+  CU(cudaMemcpyAsync(ctx->adj_ckpt[nck].p, ctx->state[ctx->cur].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+                     ctx->stream));
+  const BlockDesc& d = ctx->desc[block - 1];
+  const int nf = (face <= 2) ? d.nj : d.ni;
+  CU(cudaMemsetAsync(ctx->lam.p, 0, ns * sizeof(double), ctx->stream));
+  adj_objective(ctx->d_desc.p, block - 1, face, nf, ctx->margs(), ctx->state[ctx->cur].p, ctx->objt.p, ctx->lam.p,
+                ctx->stream);
+  adj_sum(ctx->objt.p, nf, ctx->adj_scal.p + 2, 0, ctx->stream);
+  CU(cudaMemcpyAsync(J, ctx->adj_scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
+  ctx->adj_nsteps = nsteps;
+  ctx->adj_interval = interval;
+  ctx->adj_block = block;
+  ctx->adj_face = face;
+  ctx->adj_recorded = true;
+  return check_launch(ctx, "adjoint_forward");
+}
+
+int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (!ctx->adj_recorded) return fail(ctx, MOSE_ERR_INVALID, "adjoint_backward needs a preceding adjoint_forward");
+  const size_t ns = (size_t)ctx->nv * ctx->marena;
+  const int N = ctx->adj_nsteps, K = ctx->adj_interval, nck = (N + K - 1) / K;
+  const double h_time = ctx->h_time;
+  CU(cudaMemsetAsync(ctx->adj_scal.p + 1, 0, sizeof(double), ctx->stream));
+  for (int mck = nck - 1; mck >= 0; --mck) {
+    const int cnt = std::min(K, N - mck * K);
+    // recompute the segment from its checkpoint, recording the stage inputs
+    CU(cudaMemcpyAsync(ctx->state[ctx->cur].p, ctx->adj_ckpt[mck].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    int pc = ctx->cur;
+    for (int k = 0; k < cnt; ++k) pc = record_step(ctx, pc, k);
+    CU(cudaMemcpyAsync(ctx->adj_segend.p, ctx->state[pc].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+                       ctx->stream));
+    for (int k = cnt - 1; k >= 0; --k)
+      adj_reverse_step(ctx, k, k == cnt - 1 ? ctx->adj_segend.p : ctx->adj_seg[3 * (size_t)(k + 1)].p);
+    rc = check_launch(ctx, "adjoint_backward");
+    if (rc) return rc;
+  }
+  // back to the forward run's final state and time
+  CU(cudaMemcpyAsync(ctx->state[ctx->cur].p, ctx->adj_ckpt[nck].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+                     ctx->stream));
+  ctx->h_time = h_time;
+  ctx->dt_valid = false;
+  double h = 0.0;
+  CU(cudaMemcpyAsync(&h, ctx->adj_scal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  rc = poll_device_error(ctx);
+  if (dJ_dmach) *dJ_dmach = h;
+  ctx->adj_recorded = false;
+  return rc;
+}
+
+int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  rc = adj_prepare(ctx);
+  if (rc) return rc;
+  rc = adj_segment_buffers(ctx, 1);
+  if (rc) return rc;
+  const size_t ns = (size_t)ctx->nv * ctx->marena;
+  const double h_time = ctx->h_time;
+  CU(cudaMemsetAsync(ctx->adj_scal.p + 1, 0, sizeof(double), ctx->stream));
+  const int pc = record_step(ctx, ctx->cur, 0);
+  CU(cudaMemcpyAsync(ctx->adj_segend.p, ctx->state[pc].p, ns * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  adj_reverse_step(ctx, 0, ctx->adj_segend.p);
+  // the state stays P^n (the recorded first-stage input)
+  CU(cudaMemcpyAsync(ctx->state[ctx->cur].p, ctx->adj_seg[0].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+                     ctx->stream));
+  ctx->h_time = h_time;
+  ctx->dt_valid = false;
+  double h = 0.0;
+  CU(cudaMemcpyAsync(&h, ctx->adj_scal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  rc = poll_device_error(ctx);
+  if (dJ_dmach) *dJ_dmach = h;
+  return rc ? rc : check_launch(ctx, "adjoint_step");
+}
+
+int mose_gpu_upload_adjoint(mose_gpu_ctx* ctx, int32_t b, const double* lam) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  rc = adj_prepare(ctx);
+  if (rc) return rc;
+  return prim_io(ctx, b, const_cast<double*>(lam), -2, true);
+}
+int mose_gpu_download_adjoint(mose_gpu_ctx* ctx, int32_t b, double* lam) { return prim_io(ctx, b, lam, -2, false); }
 
 }  // extern "C"

@@ -121,6 +121,43 @@ class Solver:
         self._check(self.lib.mose_gpu_download_prim(self.h, b, _dp(out)))
         return out
 
+    # ---- discrete adjoint (2-D, HLLC) -------------------------------------------
+    def set_inflow_mach(self, mach: float):
+        """Mach number of every 405 supersonic-inflow face."""
+        self._check(self.lib.mose_gpu_set_inflow_mach(self.h, float(mach)))
+
+    def adjoint_forward(self, nsteps: int, interval: int, block: int = 1, face: int = 3) -> float:
+        """nsteps fused steps with a checkpoint every `interval` steps; returns
+        J = sum over the cells of face `face` of block `block` of p * A."""
+        J = C.c_double()
+        self._check(self.lib.mose_gpu_adjoint_forward(self.h, nsteps, interval, block, face, C.byref(J)))
+        return J.value
+
+    def adjoint_backward(self) -> float:
+        """Reverse sweep of the last adjoint_forward: dJ/dP0 stays in the
+        adjoint state (download_adjoint); returns dJ/dMach."""
+        d = C.c_double()
+        self._check(self.lib.mose_gpu_adjoint_backward(self.h, C.byref(d)))
+        return d.value
+
+    def adjoint_step(self) -> float:
+        """lambda <- (dP^{n+1}/dP^n)^T lambda at the current state; returns
+        lambda . dP^{n+1}/dMach."""
+        d = C.c_double()
+        self._check(self.lib.mose_gpu_adjoint_step(self.h, C.byref(d)))
+        return d.value
+
+    def upload_adjoint(self, b: int, lam: np.ndarray):
+        lam = np.ascontiguousarray(lam, dtype=np.float64)
+        if lam.shape != self._shape(b):
+            raise ValueError(f"block {b}: expected {self._shape(b)}, got {lam.shape}")
+        self._check(self.lib.mose_gpu_upload_adjoint(self.h, b, _dp(lam)))
+
+    def download_adjoint(self, b: int) -> np.ndarray:
+        out = np.empty(self._shape(b))
+        self._check(self.lib.mose_gpu_download_adjoint(self.h, b, _dp(out)))
+        return out
+
     def download_residual(self, b: int) -> np.ndarray:
         out = np.empty(self._shape(b))
         self._check(self.lib.mose_gpu_download_residual(self.h, b, _dp(out)))

@@ -1,0 +1,149 @@
+"""Discrete adjoint of the explicit step (C ABI mose_gpu_adjoint_*) against
+central finite differences (step 1e-6) of the forward: one step, a
+checkpointed multi-step objective, the CPU oracle's forward (the reference
+gradient), and the torch.autograd.Function.  Curvilinear channel: 405
+inflow (Mach derivative too), 406 outflow, 300 slip walls; van Albada +
+HLLC, SSP-RK3.  Bar: relative error 1e-5."""
+import numpy as np
+import pytest
+
+from mose_b200 import cases
+from mose_b200.cases import GC, to_ref_layout
+
+pytestmark = pytest.mark.gpu
+
+H = 1e-6
+
+
+def channel(n=16, seed=0):
+    case = cases.curvilinear_channel(n, steps=1)
+    rng = np.random.default_rng(seed)
+    p = case.prim[0]
+    p[..., 0] *= 1 + 0.05 * rng.standard_normal(p.shape[:-1])
+    p[..., 1] *= 1 + 0.05 * rng.standard_normal(p.shape[:-1])
+    p[..., 2] = 0.05 * rng.standard_normal(p.shape[:-1])
+    p[..., 4] *= 1 + 0.05 * rng.standard_normal(p.shape[:-1])
+    return case
+
+
+def interior(P):
+    return P[GC:-GC, GC:-GC, GC:-GC]
+
+
+def direction(shape, rng):
+    d = rng.standard_normal(shape)
+    d[..., 3] = 0.0      # w is not a state of the 2-D path
+    return d
+
+
+def solver(case):
+    from mose_b200 import Solver
+    return Solver(case)
+
+
+def step_state(s, P0, mach, nsteps):
+    s.upload_prim(1, to_ref_layout(P0))
+    s.set_time(0.0, 0)
+    s.set_inflow_mach(mach)
+    for _ in range(nsteps):
+        s.explicit_step()
+    return interior(s.download_prim(1))
+
+
+def test_adjoint_step_matches_fd():
+    case = channel()
+    mach = case.extra["mach"]
+    s = solver(case)
+    P0 = case.prim[0].copy()
+    rng = np.random.default_rng(1)
+    lam1 = direction(P0.shape, rng)
+    s.upload_prim(1, to_ref_layout(P0))
+    s.upload_adjoint(1, to_ref_layout(lam1))
+    dM = s.adjoint_step()
+    lam0 = interior(s.download_adjoint(1))
+    g = lambda P, M: float((lam1 * step_state(s, P, M, 1)).sum())
+    for q in range(3):
+        d = direction(P0.shape, rng)
+        fd = (g(P0 + H * d, mach) - g(P0 - H * d, mach)) / (2 * H)
+        adj = float((lam0 * d).sum())
+        assert abs(adj - fd) <= 1e-5 * abs(fd), (q, adj, fd)
+    fdm = (g(P0, mach + H) - g(P0, mach - H)) / (2 * H)
+    assert abs(dM - fdm) <= 1e-5 * max(abs(fdm), 1e-12), (dM, fdm)
+
+
+def objective(s, P0, mach, nsteps):
+    s.upload_prim(1, to_ref_layout(P0))
+    s.set_time(0.0, 0)
+    s.set_inflow_mach(mach)
+    return s.adjoint_forward(nsteps, 4, 1, 3)
+
+
+def test_checkpointed_gradient_matches_fd():
+    case = channel(seed=2)
+    mach = case.extra["mach"]
+    s = solver(case)
+    P0 = case.prim[0].copy()
+    n = 12
+    J = objective(s, P0, mach, n)
+    dM = s.adjoint_backward()
+    grad = interior(s.download_adjoint(1))
+    assert np.isfinite(J) and np.isfinite(grad).all()
+    rng = np.random.default_rng(3)
+    for q in range(4):
+        d = direction(P0.shape, rng)
+        fd = (objective(s, P0 + H * d, mach, n) - objective(s, P0 - H * d, mach, n)) / (2 * H)
+        adj = float((grad * d).sum())
+        assert abs(adj - fd) <= 1e-5 * abs(fd), (q, adj, fd)
+    fdm = (objective(s, P0, mach + H, n) - objective(s, P0, mach - H, n)) / (2 * H)
+    assert abs(dM - fdm) <= 1e-5 * abs(fdm), (dM, fdm)
+
+
+def test_gradient_matches_oracle_fd(oracle_mod):
+    """The reference gradient: central differences of the CPU oracle."""
+    case = channel(12, seed=4)
+    mach = case.extra["mach"]
+    n = 8
+    s = solver(case)
+    P0 = case.prim[0].copy()
+    objective(s, P0, mach, n)
+    dM = s.adjoint_backward()
+    grad = interior(s.download_adjoint(1))
+
+    def J_oracle(P, M):
+        c = cases.curvilinear_channel(12, steps=1)
+        c.prim[0][...] = P
+        c.bc_data[c.bc_rec[:, 5] == 405, 0] = M
+        o = oracle_mod.Oracle(c)
+        for _ in range(n):
+            o.step()
+        _, A = o.get_faces(1, 2)                     # j-faces: A[k, j, i], j = 0 is face 3
+        p = interior(o.get_prim(1))[0, 0, :, 4]
+        return float((p * A[0, 0, :]).sum())
+
+    rng = np.random.default_rng(5)
+    for q in range(2):
+        d = direction(P0.shape, rng)
+        fd = (J_oracle(P0 + H * d, mach) - J_oracle(P0 - H * d, mach)) / (2 * H)
+        adj = float((grad * d).sum())
+        assert abs(adj - fd) <= 1e-5 * abs(fd), (q, adj, fd)
+    fdm = (J_oracle(P0, mach + H) - J_oracle(P0, mach - H)) / (2 * H)
+    assert abs(dM - fdm) <= 1e-5 * abs(fdm), (dM, fdm)
+
+
+def test_autograd_function_matches_direct_api():
+    import torch
+    from mose_b200.adjoint import wall_pressure
+    case = channel(seed=6)
+    mach = case.extra["mach"]
+    s = solver(case)
+    P0 = case.prim[0].copy()
+    J_direct = objective(s, P0, mach, 12)
+    dM_direct = s.adjoint_backward()
+    g_direct = interior(s.download_adjoint(1))
+    p = torch.tensor(P0, requires_grad=True)
+    m = torch.tensor(mach, dtype=torch.float64, requires_grad=True)
+    J = wall_pressure(p, m, s, 12, 4, 1, 3)
+    J.backward()
+    assert J.item() == J_direct
+    assert np.array_equal(p.grad.numpy(), g_direct)
+    assert float(m.grad) == dM_direct
