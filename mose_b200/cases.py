@@ -293,6 +293,24 @@ def curvilinear_channel(n: int = 512, steps: int = 200, mach: float = 0.8, amp: 
                 extra={"mach": mach})
 
 
+def perturbed_channel(n: int = 512, steps: int = 200, amp: float = 0.05, seed: int = 0, **kw) -> Case:
+    """The curvilinear channel with its uniform Mach-0.8 state carrying seeded
+    cell-wise perturbations: relative amplitude `amp` on rho, u and p, and
+    v = amp * Mach * N(0, 1).  The wall-pressure objective has no gradient at
+    the exactly uniform state: every limited slope is zero there, and the
+    limiters (homogeneous of degree 1) have one-sided directional derivatives
+    that are not linear in the direction.  The perturbation also breaks the
+    ties of the CFL minimum."""
+    case = curvilinear_channel(n, steps=steps, **kw)
+    rng = np.random.default_rng(seed)
+    p = case.prim[0]
+    shape = p.shape[:-1]
+    for v in (0, 1, 4):
+        p[..., v] *= 1 + amp * rng.standard_normal(shape)
+    p[..., 2] = amp * case.extra["mach"] * rng.standard_normal(shape)
+    return case
+
+
 def periodic_box_3d(n: int = 128, nb=(2, 2, 2), sizes=None, steps: int = 50, seed: int = 0,
                     limiter="vanleer", riemann="HLLC", cfl=0.3, gamma=1.4, mach=0.3, amp=1e-2,
                     nmodes: int = 16, kmax: int = 8) -> Case:

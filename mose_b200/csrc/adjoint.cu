@@ -152,7 +152,11 @@ __global__ void k_adj_faces(const BlockDesc* blk, int b, MetricArgs m, Gas g, co
 template <int RIE, int LIM>
 __global__ void k_adj_bc(StageArgs a, const int4* list, int nlist, const double* lamR, double* Cb, double* Fbc,
                          double* dmach) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  // thread (q, col): entry q of the list; col 0..7 the input (Q then Qi, 4
+  // each) of a finite-difference column, col 8 the face term itself, the
+  // inflow Mach column and the connection faces
+  const long long tq = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const int q = (int)(tq / 9), col = (int)(tq % 9);
   if (q >= nlist) return;
   const int4 e = list[q];
   const int b = e.x, f = e.y, idx = e.z, ent = e.w;
@@ -165,11 +169,6 @@ __global__ void k_adj_bc(StageArgs a, const int4* list, int nlist, const double*
   const double sgn = high ? 1.0 : -1.0;
   const int w = a.bcw[d.bcoff[f - 1] + idx];
   const int code = bc_code(w);
-  double out[4][NV], Fout[NV];
-  for (int s = 0; s < 4; ++s)
-    for (int v = 0; v < NV; ++v) out[s][v] = 0.0;
-  for (int v = 0; v < NV; ++v) Fout[v] = 0.0;
-  double dm = 0.0;
   const long long ob = off(d, i, j);
   double Lr[NV];
   for (int v = 0; v < NV; ++v) Lr[v] = lamR[d.sbase + ob + v * vs];
@@ -177,64 +176,78 @@ __global__ void k_adj_bc(StageArgs a, const int4* list, int nlist, const double*
   auto cell = [&](int s) { const int t = high ? s - 1 : s - 2; return off(d, i + di * t, j + dj * t); };
   double n[3];
   const double A = face_at(a.m, d, dir, high ? off(d, i + di, j + dj) : ob, n);
-  if (code == BC_CONN) {
-    double qq[4][NV], dl[4], Fb[NV], Fv[NV];
-    for (int s = 0; s < 4; ++s) {
-      const long long o = cell(s);
-      for (int v = 0; v < NV; ++v) qq[s][v] = a.Pc[d.sbase + o + v * vs];
-      dl[s] = dl_at(a.m, d, dir, o);
-    }
-    for (int v = 0; v < NV; ++v) Fb[v] = sgn * Lr[v];
-    face_vjp<LIM>(a.g, qq, dl, n, A, Fb, Fv, out);
-    for (int v = 0; v < NV; ++v) Fout[v] = sgn * Fv[v];
-  } else if (code != BC_NONE) {
-    // central-difference Jacobian of the reference boundary formula in
-    // (Q, Qi) = (boundary cell, first interior cell), and in the inflow Mach
-    const int sb = high ? 1 : 2, si = high ? 0 : 3;   // slots of the boundary / interior cell
-    double Q[NV], Qi[NV], Fv[NV];
-    for (int v = 0; v < NV; ++v) { Q[v] = a.Pc[d.sbase + cell(sb) + v * vs]; Qi[v] = a.Pc[d.sbase + cell(si) + v * vs]; }
-    const double dlB = dl_at(a.m, d, dir, cell(sb)), dlI = dl_at(a.m, d, dir, cell(si));
-    const int mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fv);
-    double keep[NV];
-    for (int v = 0; v < NV; ++v) {
-      keep[v] = (mask == ADD_ALL || (mask == ADD_MOMENTUM && v >= 1 && v < NV - 1)) ? 1.0 : 0.0;
-      Fout[v] = sgn * keep[v] * Fv[v];
-    }
-    double Fb[NV];
-    for (int v = 0; v < NV; ++v) Fb[v] = sgn * keep[v] * Lr[v];
-    for (int side = 0; side < 2; ++side) {
-      double* X = side == 0 ? Q : Qi;
-      for (int k = 0; k < NV; ++k) {
-        const double x0 = X[k], h = 1e-6 * fmax(fabs(x0), 1e-3);
-        double Fp[NV], Fm[NV];
-        X[k] = x0 + h;
-        boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fp);
-        X[k] = x0 - h;
-        boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fm);
-        X[k] = x0;
-        double s = 0.0;
-        for (int v = 0; v < NV; ++v) s += Fb[v] * (Fp[v] - Fm[v]) / (2.0 * h);
-        out[side == 0 ? sb : si][k] = s;
+  double* Cq = Cb + (size_t)ent * 16;
+  if (code == BC_NONE || code == BC_CONN) {
+    if (col != 8) return;
+    double out[4][NV], Fout[NV];
+    for (int s = 0; s < 4; ++s)
+      for (int v = 0; v < NV; ++v) out[s][v] = 0.0;
+    for (int v = 0; v < NV; ++v) Fout[v] = 0.0;
+    if (code == BC_CONN) {
+      double qq[4][NV], dl[4], Fb[NV], Fv[NV];
+      for (int s = 0; s < 4; ++s) {
+        const long long o = cell(s);
+        for (int v = 0; v < NV; ++v) qq[s][v] = a.Pc[d.sbase + o + v * vs];
+        dl[s] = dl_at(a.m, d, dir, o);
       }
+      for (int v = 0; v < NV; ++v) Fb[v] = sgn * Lr[v];
+      face_vjp<LIM>(a.g, qq, dl, n, A, Fb, Fv, out);
+      for (int v = 0; v < NV; ++v) Fout[v] = sgn * Fv[v];
     }
-    if (code == BC_SUPIN) {
-      BcParam p = a.bcp[bc_param(w)];
-      const double M0 = p.mach, h = 1e-6 * fmax(fabs(M0), 1e-3);
-      double Fp[NV], Fm[NV];
-      p.mach = M0 + h;
-      ex::bc_supersonic_inflow<RIE, LIM, NV>(a.g, Q, Qi, p, n, A, f, Fp);
-      p.mach = M0 - h;
-      ex::bc_supersonic_inflow<RIE, LIM, NV>(a.g, Q, Qi, p, n, A, f, Fm);
-      // only where boundary_flux takes the inflow branch (its test !(s Un >= 0))
-      const double Un = ex::dot_vel<NV>(Q, n), s405 = (double)(1 - 2 * (f % 2));
-      if (!(s405 * Un >= 0.0))
-        for (int v = 0; v < NV; ++v) dm += Fb[v] * (Fp[v] - Fm[v]) / (2.0 * h);
-    }
+    for (int s = 0; s < 4; ++s)
+      for (int v = 0; v < NV; ++v) Cq[4 * s + v] = out[s][v];
+    for (int v = 0; v < NV; ++v) Fbc[(size_t)ent * 4 + v] = Fout[v];
+    return;
   }
-  for (int s = 0; s < 4; ++s)
-    for (int v = 0; v < NV; ++v) Cb[(size_t)ent * 16 + 4 * s + v] = out[s][v];
-  for (int v = 0; v < NV; ++v) Fbc[(size_t)ent * 4 + v] = Fout[v];
-  dmach[ent] = dm;
+  // central-difference Jacobian of the reference boundary formula in
+  // (Q, Qi) = (boundary cell, first interior cell), and in the inflow Mach
+  const int sb = high ? 1 : 2, si = high ? 0 : 3;   // slots of the boundary / interior cell
+  double Q[NV], Qi[NV], Fv[NV];
+  for (int v = 0; v < NV; ++v) { Q[v] = a.Pc[d.sbase + cell(sb) + v * vs]; Qi[v] = a.Pc[d.sbase + cell(si) + v * vs]; }
+  const double dlB = dl_at(a.m, d, dir, cell(sb)), dlI = dl_at(a.m, d, dir, cell(si));
+  const int mask = boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fv);
+  double Fb[NV];
+  for (int v = 0; v < NV; ++v) {
+    const double keep = (mask == ADD_ALL || (mask == ADD_MOMENTUM && v >= 1 && v < NV - 1)) ? 1.0 : 0.0;
+    Fb[v] = sgn * keep * Lr[v];
+    if (col == 8) Fbc[(size_t)ent * 4 + v] = sgn * keep * Fv[v];
+  }
+  if (col < 8) {
+    const int side = col / NV, k = col % NV;
+    double* X = side == 0 ? Q : Qi;
+    const double x0 = X[k], h = 1e-6 * fmax(fabs(x0), 1e-3);
+    double Fp[NV], Fm[NV];
+    X[k] = x0 + h;
+    boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fp);
+    X[k] = x0 - h;
+    boundary_flux<RIE, LIM, NV>(a, w, Q, Qi, dlB, dlI, n, A, f, Fm);
+    double sacc = 0.0;
+    for (int v = 0; v < NV; ++v) sacc += Fb[v] * (Fp[v] - Fm[v]) / (2.0 * h);
+    // slots: the boundary cell's column k, the interior cell's column k; the
+    // other two slots are zero
+    Cq[4 * (side == 0 ? sb : si) + k] = sacc;
+    if (side == 0) {
+      const int z0 = high ? 2 : 0, z1 = high ? 3 : 1;   // the two cells off this face's stencil
+      Cq[4 * z0 + k] = 0.0;
+      Cq[4 * z1 + k] = 0.0;
+    }
+    return;
+  }
+  double dm = 0.0;
+  if (code == BC_SUPIN) {
+    BcParam p = a.bcp[bc_param(w)];
+    const double M0 = p.mach, h = 1e-6 * fmax(fabs(M0), 1e-3);
+    double Fp[NV], Fm[NV];
+    p.mach = M0 + h;
+    ex::bc_supersonic_inflow<RIE, LIM, NV>(a.g, Q, Qi, p, n, A, f, Fp);
+    p.mach = M0 - h;
+    ex::bc_supersonic_inflow<RIE, LIM, NV>(a.g, Q, Qi, p, n, A, f, Fm);
+    // only where boundary_flux takes the inflow branch (its test !(s Un >= 0))
+    const double Un = ex::dot_vel<NV>(Q, n), s405 = (double)(1 - 2 * (f % 2));
+    if (!(s405 * Un >= 0.0))
+      for (int v = 0; v < NV; ++v) dm += Fb[v] * (Fp[v] - Fm[v]) / (2.0 * h);
+  }
+  dmach[ent] += dm;
 }
 
 // ---- gather ------------------------------------------------------------------------
@@ -272,13 +285,15 @@ __global__ void k_adj_gather(const BlockDesc* blk, int b, const double* Cx, cons
     if (j < d.nj - 1) for (int v = 0; v < NV; ++v) R[v] += Fy[o4 + oc + v * vs];
     double s = 0.0;
     for (int v = 0; v < NV; ++v) s += R[v] * wdt[d.sbase + oc + v * vs];
-    dtpart[d.mbase + oc] = s;
+    dtpart[d.mbase + oc] += s;
   }
 }
 
 // Boundary-face contributions of face f (entries of one face touch distinct cells).
-__global__ void k_adj_bc_gather(const BlockDesc* blk, const int4* list, int first, int n, const double* Cb,
-                                const double* Fbc, const double* wdt, double* lamG, double* dtpart) {
+__global__ void k_adj_bc_gather(const BlockDesc* blk, const int4* __restrict__ list, int first, int n,
+                                const double* __restrict__ Cb, const double* __restrict__ Fbc,
+                                const double* __restrict__ wdt, double* __restrict__ lamG,
+                                double* __restrict__ dtpart) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const int4 e = list[first + q];
@@ -289,20 +304,31 @@ __global__ void k_adj_bc_gather(const BlockDesc* blk, const int4* list, int firs
   const int i = dir == 0 ? (high ? d.ni - 1 : 0) : idx, j = dir == 1 ? (high ? d.nj - 1 : 0) : idx;
   const int di = dir == 0, dj = dir == 1;
   const long long vs = d.vstride;
+  // all loads first: the sixteen read-modify-writes are independent
+  long long o[4];
+  double l[4][NV], c[4][NV];
   for (int s = 0; s < 4; ++s) {
     const int t = high ? s - 1 : s - 2;
-    const long long o = off(d, i + di * t, j + dj * t);
-    for (int v = 0; v < NV; ++v) lamG[d.sbase + o + v * vs] += Cb[(size_t)ent * 16 + 4 * s + v];
+    o[s] = d.sbase + off(d, i + di * t, j + dj * t);
+    for (int v = 0; v < NV; ++v) {
+      l[s][v] = lamG[o[s] + v * vs];
+      c[s][v] = Cb[(size_t)ent * 16 + 4 * s + v];
+    }
   }
   const long long ob = off(d, i, j);
-  double s = 0.0;
-  for (int v = 0; v < NV; ++v) s += Fbc[(size_t)ent * 4 + v] * wdt[d.sbase + ob + v * vs];
-  dtpart[d.mbase + ob] += s;
+  double w[NV], F[NV];
+  for (int v = 0; v < NV; ++v) { w[v] = wdt[d.sbase + ob + v * vs]; F[v] = Fbc[(size_t)ent * 4 + v]; }
+  const double dp = dtpart[d.mbase + ob];
+  for (int s = 0; s < 4; ++s)
+    for (int v = 0; v < NV; ++v) lamG[o[s] + v * vs] = l[s][v] + c[s][v];
+  double sum = 0.0;
+  for (int v = 0; v < NV; ++v) sum += F[v] * w[v];
+  dtpart[d.mbase + ob] = dp + sum;
 }
 
 // Transpose of Fill_Ghost_Cell for the ghost records of one face.
-__global__ void k_adj_ghostT(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
-                             double* lamG) {
+__global__ void k_adj_ghostT(const BlockDesc* blk, const GhostRec* __restrict__ recs, const int* __restrict__ ids,
+                             int n, MetricArgs m, double* lamG) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const GhostRec e = recs[ids[q]];
@@ -313,18 +339,28 @@ __global__ void k_adj_ghostT(const BlockDesc* blk, const GhostRec* recs, const i
   const long long vs = d.vstride;
   double* Lb = lamG + d.sbase;
   auto at = [&](int g) { return off(d, e.i - gi * g, e.j - gj * g); };   // g > 0 ghost, g <= 0 interior
+  // every branch loads what it reads before it stores: the ghost cells and
+  // the cells they feed are distinct, so the accesses are independent
   if (e.type == BC_CONN) {
     const BlockDesc& s = blk[e.bs];
     const int si = (e.fs == 1) ? 1 : (e.fs == 2) ? -1 : 0;
     const int sj = (e.fs == 3) ? 1 : (e.fs == 4) ? -1 : 0;
     double* Ls = lamG + s.sbase;
+    long long od[GW], os[GW];
+    double lg[GW][NV], ls[GW][NV];
     for (int g = 1; g <= GW; ++g) {
-      const long long od = at(g), os = off(s, e.is + si * (g - 1), e.js + sj * (g - 1));
+      od[g - 1] = at(g);
+      os[g - 1] = off(s, e.is + si * (g - 1), e.js + sj * (g - 1));
       for (int v = 0; v < NV; ++v) {
-        Ls[v * s.vstride + os] += Lb[v * vs + od];
-        Lb[v * vs + od] = 0.0;
+        lg[g - 1][v] = Lb[v * vs + od[g - 1]];
+        ls[g - 1][v] = Ls[v * s.vstride + os[g - 1]];
       }
     }
+    for (int g = 0; g < GW; ++g)
+      for (int v = 0; v < NV; ++v) {
+        Ls[v * s.vstride + os[g]] = ls[g][v] + lg[g][v];
+        Lb[v * vs + od[g]] = 0.0;
+      }
   } else if (e.type == BC_SYM) {
     // first ghost = the boundary cell with its velocity mirrored in the wall
     const int fi = e.i + (e.f == 2), fj = e.j + (e.f == 4);
@@ -332,33 +368,40 @@ __global__ void k_adj_ghostT(const BlockDesc* blk, const GhostRec* recs, const i
     const double nx = fp[0], ny = fp[vs];
     const long long og = at(1), ob = at(0);
     const double lr = Lb[og], lu = Lb[vs + og], lv = Lb[2 * vs + og], lp = Lb[3 * vs + og];
+    double b[NV];
+    for (int v = 0; v < NV; ++v) b[v] = Lb[v * vs + ob];
     // u' = u - 2 (u.n) n  (transpose of I - 2 n n^T is itself)
     const double dotl = lu * nx + lv * ny;
-    Lb[ob] += lr;
-    Lb[vs + ob] += lu - 2.0 * dotl * nx;
-    Lb[2 * vs + ob] += lv - 2.0 * dotl * ny;
-    Lb[3 * vs + ob] += lp;
+    Lb[ob] = b[0] + lr;
+    Lb[vs + ob] = b[1] + (lu - 2.0 * dotl * nx);
+    Lb[2 * vs + ob] = b[2] + (lv - 2.0 * dotl * ny);
+    Lb[3 * vs + ob] = b[3] + lp;
     for (int g = 1; g <= GW; ++g)
       for (int v = 0; v < NV; ++v) Lb[v * vs + at(g)] = 0.0;
   } else if (e.type == BC_EXTRAP) {
-    // forward: P(g) = 3 P(g-1) - 3 P(g-2) + P(g-3), g = 1, 2 in order
-    for (int g = GW; g >= 1; --g) {
-      const long long od = at(g), oa = at(g - 1), oc = at(g - 2), oe = at(g - 3);
-      for (int v = 0; v < NV; ++v) {
-        const double l = Lb[v * vs + od];
-        Lb[v * vs + od] = 0.0;
-        Lb[v * vs + oa] += 3.0 * l;
-        Lb[v * vs + oc] -= 3.0 * l;
-        Lb[v * vs + oe] += l;
+    // forward: P(g) = 3 P(g-1) - 3 P(g-2) + P(g-3), g = 1, 2 in order;
+    // reverse g = 2 then g = 1 on the five cells g = 2 .. -2
+    for (int v = 0; v < NV; ++v) {
+      double L[5];
+      for (int t = 0; t < 5; ++t) L[t] = Lb[v * vs + at(2 - t)];   // L[t] is cell g = 2 - t
+      for (int g = GW; g >= 1; --g) {
+        const int t = 2 - g;
+        const double l = L[t];
+        L[t] = 0.0;
+        L[t + 1] += 3.0 * l;
+        L[t + 2] -= 3.0 * l;
+        L[t + 3] += l;
       }
+      for (int t = 0; t < 5; ++t) Lb[v * vs + at(2 - t)] = L[t];
     }
   } else {   // zero gradient (0, 405, 406, ...)
     const long long ob = at(0);
-    for (int g = 1; g <= GW; ++g)
-      for (int v = 0; v < NV; ++v) {
-        Lb[v * vs + ob] += Lb[v * vs + at(g)];
-        Lb[v * vs + at(g)] = 0.0;
-      }
+    for (int v = 0; v < NV; ++v) {
+      double acc = Lb[v * vs + ob];
+      for (int g = 1; g <= GW; ++g) acc += Lb[v * vs + at(g)];
+      Lb[v * vs + ob] = acc;
+      for (int g = 1; g <= GW; ++g) Lb[v * vs + at(g)] = 0.0;
+    }
   }
 }
 
@@ -372,37 +415,33 @@ __global__ void k_adj_combine(const BlockDesc* blk, int b, const double* lam_loc
   for (int v = 0; v < NV; ++v) lam_out[o + v * vs] = in ? lam_loc[o + v * vs] + lamG[o + v * vs] : 0.0;
 }
 
-// Deterministic sum of n values into *out (+= when accumulate), one CTA.
-__global__ void k_sum(const double* x, long long n, double* out, int accumulate) {
+// Deterministic sum of n values: pass 1, one partial per CTA over a fixed
+// strided subset; pass 2, one CTA sums the partials into *out (+= when
+// accumulate).  Fixed grid and fixed tree: the same bits every run.
+constexpr int kSumCtas = 296;
+__global__ void k_sum_partial(const double* x, long long n, double* part) {
   __shared__ double s[256];
   double acc = 0.0;
-  for (long long q = threadIdx.x; q < n; q += blockDim.x) acc += x[q];
+  for (long long q = blockIdx.x * 256LL + threadIdx.x; q < n; q += 256LL * gridDim.x) acc += x[q];
   s[threadIdx.x] = acc;
   __syncthreads();
-  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+}
+__global__ void k_sum_final(const double* part, int np, double* out, int accumulate) {
+  __shared__ double s[256];
+  double acc = 0.0;
+  for (int q = threadIdx.x; q < np; q += 256) acc += part[q];
+  s[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
     __syncthreads();
   }
   if (threadIdx.x == 0) *out = accumulate ? *out + s[0] : s[0];
-}
-
-// The cell attaining the step's global dt, in two passes with this
-// kernel's own arithmetic (pass 0: the minimum's bit pattern into arg[1];
-// pass 1: the smallest flat index attaining it into arg[0]), so the choice
-// does not hinge on last-bit agreement with the forward pass's arithmetic.
-template <bool UNI>
-__global__ void k_dt_argmin(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* P, double cfl, int ndir,
-                            unsigned long long* arg, int pass) {
-  const BlockDesc& d = blk[b];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
-  if (i >= d.ni || j >= d.nj) return;
-  const long long o = off(d, i, j);
-  double Q[NV];
-  for (int v = 0; v < NV; ++v) Q[v] = P[d.sbase + o + v * d.vstride];
-  const double dt = cfl_dt<NV, UNI, false>(g, Q, d, m, o, ndir, cfl);
-  const unsigned long long bits = (unsigned long long)__double_as_longlong(dt);
-  if (pass == 0) atomicMin(arg + 1, bits);
-  else if (bits == arg[1]) atomicMin(arg, ((unsigned long long)b << 40) | (unsigned long long)o);
 }
 
 // lam_n[argmin] += (dJ/ddt) d(dt_cell)/dP at the argmin cell.
@@ -477,7 +516,7 @@ void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g,
 void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,
             double* dmach, cudaStream_t s) {
   if (n == 0) return;
-  const int grid = (n + 127) / 128;
+  const int grid = (int)((9LL * n + 127) / 128);
   switch (lim) {
     case 1: k_adj_bc<0, 1><<<grid, 128, 0, s>>>(a, list, n, lamR, Cb, Fbc, dmach); break;
     case 2: k_adj_bc<0, 2><<<grid, 128, 0, s>>>(a, list, n, lamR, Cb, Fbc, dmach); break;
@@ -502,14 +541,11 @@ void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_
                  double* lam_out, cudaStream_t s) {
   k_adj_combine<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, lam_loc, lamG, lam_out);
 }
-void adj_sum(const double* x, long long n, double* out, int accumulate, cudaStream_t s) {
-  k_sum<<<1, 256, 0, s>>>(x, n, out, accumulate);
+void adj_sum(const double* x, long long n, double* out, int accumulate, double* scratch, cudaStream_t s) {
+  k_sum_partial<<<kSumCtas, 256, 0, s>>>(x, n, scratch);
+  k_sum_final<<<1, 256, 0, s>>>(scratch, kSumCtas, out, accumulate);
 }
-void adj_dt_argmin(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P, double cfl,
-                   int ndir, bool uniform, unsigned long long* arg, int pass, cudaStream_t s) {
-  if (uniform) k_dt_argmin<true><<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, P, cfl, ndir, arg, pass);
-  else k_dt_argmin<false><<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, P, cfl, ndir, arg, pass);
-}
+int adj_sum_scratch() { return kSumCtas; }
 void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
             const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s) {
   k_adj_dt<<<1, 32, 0, s>>>(blk, m, g, P, arg, lam_dt, cfl, ndir, lam_n);

@@ -47,9 +47,10 @@ void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* 
                          double* lamG, cudaStream_t s);
 void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,
                  double* lam_out, cudaStream_t s);
-void adj_sum(const double* x, long long n, double* out, int accumulate, cudaStream_t s);
-void adj_dt_argmin(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P, double cfl,
-                   int ndir, bool uniform, unsigned long long* arg, int pass, cudaStream_t s);
+void adj_sum(const double* x, long long n, double* out, int accumulate, double* scratch, cudaStream_t s);
+int adj_sum_scratch();
+void launch_dt_argmin(const BlockDesc* dblk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P,
+                      const double* dtg, double cfl, int ndir, bool uniform, unsigned long long* arg, cudaStream_t s);
 void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
             const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s);
 void adj_objective(const BlockDesc* blk, int b, int f, int n, MetricArgs m, const double* P, double* terms,

@@ -446,6 +446,22 @@ __global__ void k_step_dt_final(const unsigned long long* dtmin_bits, double* dt
   *dtg = v;
   if (advance_time) *time = *time + v;
 }
+// The cell attaining a step's global dt (smallest flat index on ties), for
+// the discrete adjoint.  Built here, with the reference arithmetic of the dt
+// pass, so that the cell's dt equals the recorded dtglobal bit for bit.
+template <bool UNI>
+__global__ void k_dt_argmin(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* P, const double* dtg,
+                            double cfl, int ndir, unsigned long long* arg) {
+  const BlockDesc& d = blk[b];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= d.ni || j >= d.nj) return;
+  const long long o = cell_off2(d, i, j);
+  double Q[4];
+  for (int v = 0; v < 4; ++v) Q[v] = P[d.sbase + o + v * d.vstride];
+  const double dt = cfl_dt<4, UNI, false>(g, Q, d, m, o, ndir, cfl);
+  if (dt == *dtg) atomicMin(arg, ((unsigned long long)b << 40) | (unsigned long long)o);
+}
+
 // Fused-step bookkeeping: dtglobal = the running minimum (from the standalone
 // pass, or from the previous step's last RK stage), time += dtglobal, then
 // the minimum restarts from dt_start for this step's last stage.
@@ -681,6 +697,12 @@ void launch_step_begin(unsigned long long* dtmin_bits, double dt_start, int* ite
 void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time,
                           cudaStream_t s) {
   k_step_dt_final<<<1, 1, 0, s>>>(dtmin_bits, dtg, time, advance_time);
+}
+void launch_dt_argmin(const BlockDesc* dblk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P,
+                      const double* dtg, double cfl, int ndir, bool uniform, unsigned long long* arg, cudaStream_t s) {
+  const dim3 grid((ni + 127) / 128, nj);
+  if (uniform) k_dt_argmin<true><<<grid, 128, 0, s>>>(dblk, b, m, g, P, dtg, cfl, ndir, arg);
+  else k_dt_argmin<false><<<grid, 128, 0, s>>>(dblk, b, m, g, P, dtg, cfl, ndir, arg);
 }
 void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time, double dt_start,
                          int* iter, cudaStream_t s) {

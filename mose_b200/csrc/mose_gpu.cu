@@ -194,11 +194,22 @@ struct mose_gpu_ctx {
   bool adj_init = false;
   int adj_nsteps = 0, adj_interval = 0, adj_block = 0, adj_face = 0;
   std::vector<DevBuf<double>> adj_ckpt;  // P^n at steps 0, K, 2K, ...
-  std::vector<DevBuf<double>> adj_seg;   // stage inputs (ghosts filled) of one segment, [step * 3 + stage]
-  DevBuf<double> adj_segend;             // the state after the segment's last step
+  // the states of one segment as a chain: adj_seg[3 k + s] is the input of
+  // RK stage s + 1 of step k (ghosts filled in place), adj_seg[3 (k + 1)]
+  // the state after step k
+  std::vector<DevBuf<double>> adj_seg;
   DevBuf<double> adj_dts;                // dt of each step of the segment
+  // graphs of a segment's recompute (full segments) and of each reverse step
+  // k, valid for the segment length adj_graph_K; the side stream runs the
+  // boundary faces and the dt argmin beside the interior faces
+  cudaGraphExec_t adj_recgraph = nullptr;
+  std::vector<cudaGraphExec_t> adj_rgraph;
+  int adj_graph_K = 0, adj_rec_kernels = 0, adj_rev_kernels = 0;
+  cudaStream_t adj_aux = nullptr;
+  cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
   DevBuf<double> lam, lam_loc, lam_n, lamR, wdt, lamG, Cx, Cy, Fx, Fy, dtpart, adj_scal, Cb, Fbc, dmach, objt;
   DevBuf<unsigned long long> adj_arg;
+  DevBuf<double> adj_sumscr;             // partial sums of the deterministic reductions
   DevBuf<int4> adj_bclist;               // boundary face cells of faces 1..4, grouped by face
   int adj_bcfirst[5] = {0, 0, 0, 0, 0};  // face f's entries: [adj_bcfirst[f-1], adj_bcfirst[f])
   DevBuf<int> adj_gids;                  // ghost records grouped by face
@@ -270,9 +281,19 @@ int face_index(const HostBlock& h, int f, int i, int j, int k) {
   return i + h.ni * j;
 }
 
+void destroy_adjoint_graphs(mose_gpu_ctx* ctx) {
+  if (ctx->adj_recgraph) cudaGraphExecDestroy(ctx->adj_recgraph);
+  ctx->adj_recgraph = nullptr;
+  for (auto& g : ctx->adj_rgraph)
+    if (g) cudaGraphExecDestroy(g);
+  ctx->adj_rgraph.clear();
+  ctx->adj_graph_K = 0;
+}
+
 void destroy_graphs(mose_gpu_ctx* ctx) {
   for (auto& g : ctx->graph)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  destroy_adjoint_graphs(ctx);
 }
 
 }  // namespace
@@ -343,7 +364,11 @@ void mose_gpu_destroy(mose_gpu_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->cfg.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->adj_aux) cudaStreamSynchronize(ctx->adj_aux);
   destroy_graphs(ctx);
+  if (ctx->adj_fork) cudaEventDestroy(ctx->adj_fork);
+  if (ctx->adj_join) cudaEventDestroy(ctx->adj_join);
+  if (ctx->adj_aux) cudaStreamDestroy(ctx->adj_aux);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -1117,7 +1142,11 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
       ctx->Fy.alloc(4 * m) != cudaSuccess || ctx->dtpart.alloc(m) != cudaSuccess)
     return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
   CU(ctx->adj_scal.alloc(4));
-  CU(ctx->adj_arg.alloc(2));
+  CU(cudaStreamCreateWithFlags(&ctx->adj_aux, cudaStreamNonBlocking));
+  CU(cudaEventCreateWithFlags(&ctx->adj_fork, cudaEventDisableTiming));
+  CU(cudaEventCreateWithFlags(&ctx->adj_join, cudaEventDisableTiming));
+  CU(ctx->adj_arg.alloc(1));
+  CU(ctx->adj_sumscr.alloc(adj_sum_scratch()));
   // boundary face cells of faces 1..4, grouped by face (one launch per face
   // touches each cell at most once)
   std::vector<int4> list;
@@ -1157,97 +1186,153 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
 
 static int adj_segment_buffers(mose_gpu_ctx* ctx, int K) {
   const size_t ns = (size_t)ctx->nv * ctx->marena;
-  if ((int)ctx->adj_seg.size() < 3 * K) {
+  if ((int)ctx->adj_seg.size() < 3 * K + 1) {
     const size_t old = ctx->adj_seg.size();
-    ctx->adj_seg.resize(3 * (size_t)K);
+    ctx->adj_seg.resize(3 * (size_t)K + 1);
     for (size_t q = old; q < ctx->adj_seg.size(); ++q)
       if (ctx->adj_seg[q].alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
   }
-  if (ctx->adj_segend.n < ns && ctx->adj_segend.alloc(ns) != cudaSuccess)
-    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
-  if ((int)ctx->adj_dts.n < K && ctx->adj_dts.alloc(K) != cudaSuccess)
-    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
+  if ((int)ctx->adj_dts.n < K) {
+    destroy_adjoint_graphs(ctx);   // they hold adj_dts
+    if (ctx->adj_dts.alloc(K) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (segment)");
+  }
   return MOSE_OK;
 }
 
-// One Explicit_Step from arena s0 with the standalone Compute_dt, recording
-// every RK stage's input (ghosts filled) in adj_seg[3 k + stage] and the
-// step's dt in adj_dts[k].  Returns the arena of the new state.
-static int record_step(mose_gpu_ctx* ctx, int s0, int k) {
-  const size_t bytes = (size_t)ctx->nv * ctx->marena * sizeof(double);
-  enqueue_dt_pass(ctx, s0);
-  launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
-                      ctx->stream);
-  cudaMemcpyAsync(ctx->adj_dts.p + k, ctx->scal.p, sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
-  int pc = s0;
-  for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
-    const int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
-    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd,
-                       ctx->derr.p, ctx->stream);
-    cudaMemcpyAsync(ctx->adj_seg[3 * (size_t)k + irk - 1].p, ctx->state[pc].p, bytes, cudaMemcpyDeviceToDevice,
-                    ctx->stream);
-    StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-    launch_stage(ctx, a, 0, ctx->cfg.precision, ctx->uniform);
-    pc = pn;
+// Recomputes cnt Explicit_Steps from adj_seg[0] along the chain: the
+// standalone Compute_dt of the first state, the fused CFL minimum of each
+// later one (the last stage of the step before), every RK stage reading its
+// input slot (ghosts filled in place) and writing the next; the steps' dt
+// into adj_dts.  Returns the number of kernels enqueued.
+static int enqueue_record(mose_gpu_ctx* ctx, int cnt) {
+  cudaStream_t st = ctx->stream;
+  launch_step_begin(ctx->dtmin.p, 1e5, nullptr, st);
+  launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->adj_seg[0].p, ctx->margs(), ctx->dtl.p,
+                    ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0, 0, ctx->uniform, st);
+  int kern = 2;
+  const int nrk = ctx->cfg.n_rk;
+  for (int k = 0; k < cnt; ++k) {
+    launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p, st);
+    cudaMemcpyAsync(ctx->adj_dts.p + k, ctx->scal.p, sizeof(double), cudaMemcpyDeviceToDevice, st);
+    ++kern;
+    for (int irk = 1; irk <= nrk; ++irk) {
+      double* Pc = ctx->adj_seg[3 * (size_t)k + irk - 1].p;
+      launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, Pc, ctx->margs(), ctx->nd, ctx->derr.p, st);
+      if (ctx->nghost) ++kern;
+      StageArgs a = stage_args(ctx, 0, 0, -1, irk);
+      a.Pc = Pc;
+      a.Po = ctx->adj_seg[3 * (size_t)k].p;
+      a.Pn = ctx->adj_seg[irk == nrk ? 3 * (size_t)(k + 1) : 3 * (size_t)k + irk].p;
+      const bool fuse = irk == nrk && k + 1 < cnt;
+      if (fuse) fuse_next_dt(ctx, a);
+      kern += launch_stage(ctx, a, fuse ? 2 : 0, ctx->cfg.precision, ctx->uniform);
+    }
   }
-  ctx->launches += 3 + 2 * ctx->cfg.n_rk;
-  return pc;
+  return kern;
 }
 
-// The adjoint of recorded step k: ctx->lam holds dJ/dP^{k+1} on entry and
-// dJ/dP^k on exit; Pnext is P^{k+1}.  dJ/dMach accumulates in adj_scal[1].
-static void adj_reverse_step(mose_gpu_ctx* ctx, int k, const double* Pnext) {
-  cudaStream_t st = ctx->stream;
+// The adjoint of recorded step k of the chain: ctx->lam holds dJ/dP^{k+1}
+// on entry and dJ/dP^k on exit.  dJ/dMach accumulates in adj_scal[1].  The
+// boundary faces and the dt argmin run on the side stream, beside the
+// interior faces.  Returns the number of kernels enqueued.
+static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
+  cudaStream_t st = ctx->stream, aux = ctx->adj_aux;
   const size_t ns = (size_t)ctx->nv * ctx->marena;
-  const double* S[3] = {ctx->adj_seg[3 * (size_t)k].p, ctx->adj_seg[3 * (size_t)k + 1].p,
-                        ctx->adj_seg[3 * (size_t)k + 2].p};
+  const int nrk = ctx->cfg.n_rk;
+  const double* S[4];
+  for (int q = 0; q < nrk; ++q) S[q] = ctx->adj_seg[3 * (size_t)k + q].p;
+  S[nrk] = ctx->adj_seg[3 * (size_t)(k + 1)].p;
   const double* dtg = ctx->adj_dts.p + k;
   const int nb = (int)ctx->hblk.size(), lim = ctx->cfg.limiter;
   const MetricArgs m = ctx->margs();
-  cudaMemsetAsync(ctx->lam_n.p, 0, ns * sizeof(double), st);
-  cudaMemsetAsync(ctx->adj_scal.p, 0, sizeof(double), st);   // dJ/ddt of this step
   const int nlist = ctx->adj_bcfirst[4];
-  for (int irk = ctx->cfg.n_rk; irk >= 1; --irk) {
-    const double* Ps = (irk == ctx->cfg.n_rk) ? Pnext : S[irk];
+  int kern = 0;
+  cudaMemsetAsync(ctx->lam_n.p, 0, ns * sizeof(double), st);
+  cudaMemsetAsync(ctx->dtpart.p, 0, ctx->marena * sizeof(double), st);
+  if (nlist) cudaMemsetAsync(ctx->dmach.p, 0, ctx->dmach.n * sizeof(double), st);
+  // the step's dt = min over cells of the CFL dt of P^k: its argmin cell
+  cudaMemsetAsync(ctx->adj_arg.p, 0xff, sizeof(unsigned long long), st);
+  cudaEventRecord(ctx->adj_fork, st);
+  cudaStreamWaitEvent(aux, ctx->adj_fork, 0);
+  for (int b = 0; b < nb; ++b)
+    launch_dt_argmin(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, S[0], dtg, ctx->cfg.cfl,
+                     ctx->ndir, ctx->uniform, ctx->adj_arg.p, aux);
+  kern += nb;
+  for (int irk = nrk; irk >= 1; --irk) {
+    const double* Ps = S[irk];
     const double* Pprev = S[irk - 1];
     const double c = rk_coeff(ctx, irk);
     for (int b = 0; b < nb; ++b)
       adj_pre(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, Ps, Pprev, S[0], ctx->lam.p,
               ctx->lamR.p, ctx->wdt.p, ctx->lam_loc.p, ctx->lam_n.p, c, dtg, st);
+    if (nlist) {
+      StageArgs a = stage_args(ctx, 0, 0, -1, irk);
+      a.Pc = Pprev;
+      cudaEventRecord(ctx->adj_fork, st);
+      cudaStreamWaitEvent(aux, ctx->adj_fork, 0);
+      adj_bc(a, lim, ctx->adj_bclist.p, nlist, ctx->lamR.p, ctx->Cb.p, ctx->Fbc.p, ctx->dmach.p, aux);
+      ++kern;
+    }
     for (int b = 0; b < nb; ++b) {
       adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cx.p,
                 ctx->Fx.p, 0, st);
       adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cy.p,
                 ctx->Fy.p, 1, st);
     }
-    StageArgs a = stage_args(ctx, 0, 0, -1, irk);
-    a.Pc = Pprev;
-    adj_bc(a, lim, ctx->adj_bclist.p, nlist, ctx->lamR.p, ctx->Cb.p, ctx->Fbc.p, ctx->dmach.p, st);
-    cudaMemsetAsync(ctx->dtpart.p, 0, ctx->marena * sizeof(double), st);
     for (int b = 0; b < nb; ++b)
       adj_gather(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->Cx.p, ctx->Cy.p, ctx->Fx.p, ctx->Fy.p,
                  ctx->wdt.p, ctx->lamG.p, ctx->dtpart.p, st);
-    for (int f = 1; f <= 4; ++f)
-      adj_bc_gather(ctx->d_desc.p, ctx->adj_bclist.p, ctx->adj_bcfirst[f - 1],
-                    ctx->adj_bcfirst[f] - ctx->adj_bcfirst[f - 1], ctx->Cb.p, ctx->Fbc.p, ctx->wdt.p, ctx->lamG.p,
-                    ctx->dtpart.p, st);
-    for (int f = 1; f <= 4; ++f)
-      adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gfirst[f - 1],
-                          ctx->adj_gfirst[f] - ctx->adj_gfirst[f - 1], m, ctx->lamG.p, st);
+    cudaEventRecord(ctx->adj_join, aux);
+    cudaStreamWaitEvent(st, ctx->adj_join, 0);
+    for (int f = 1; f <= 4; ++f) {
+      const int n = ctx->adj_bcfirst[f] - ctx->adj_bcfirst[f - 1];
+      adj_bc_gather(ctx->d_desc.p, ctx->adj_bclist.p, ctx->adj_bcfirst[f - 1], n, ctx->Cb.p, ctx->Fbc.p, ctx->wdt.p,
+                    ctx->lamG.p, ctx->dtpart.p, st);
+      kern += n > 0;
+    }
+    for (int f = 1; f <= 4; ++f) {
+      const int n = ctx->adj_gfirst[f] - ctx->adj_gfirst[f - 1];
+      adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gfirst[f - 1], n, m, ctx->lamG.p,
+                          st);
+      kern += n > 0;
+    }
     for (int b = 0; b < nb; ++b)
       adj_combine(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->lam_loc.p, ctx->lamG.p, ctx->lam.p, st);
-    adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 1, st);
-    adj_sum(ctx->dmach.p, (long long)ctx->dmach.n, ctx->adj_scal.p + 1, 1, st);
+    kern += 5 * nb;
   }
-  // the step's dt = min over cells of the CFL dt of P^k
-  cudaMemsetAsync(ctx->adj_arg.p, 0xff, 2 * sizeof(unsigned long long), st);
-  for (int pass = 0; pass < 2; ++pass)
-    for (int b = 0; b < nb; ++b)
-      adj_dt_argmin(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, S[0], ctx->cfg.cfl, ctx->ndir,
-                    ctx->uniform, ctx->adj_arg.p, pass, st);
+  adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 0, ctx->adj_sumscr.p, st);     // dJ/ddt of this step
+  kern += 2;
+  if (nlist) {
+    adj_sum(ctx->dmach.p, (long long)ctx->dmach.n, ctx->adj_scal.p + 1, 1, ctx->adj_sumscr.p, st);
+    kern += 2;
+  }
   adj_dt(ctx->d_desc.p, m, ctx->gas, S[0], ctx->adj_arg.p, ctx->adj_scal.p, ctx->cfg.cfl, ctx->ndir, ctx->lam_n.p, st);
   adj_axpy(ctx->lam.p, ctx->lam_n.p, (long long)ns, st);
-  ctx->launches += ctx->cfg.n_rk * (5 * nb + 11) + nb + 2;
+  return kern + 2;
+}
+
+// (Re)builds the graphs of a K-step segment: the recompute of a full
+// segment and the reverse of each of its steps (the same buffers serve
+// every segment).
+static int adj_graphs(mose_gpu_ctx* ctx, int K) {
+  if (ctx->adj_graph_K == K) return MOSE_OK;
+  destroy_adjoint_graphs(ctx);
+  cudaGraph_t g;
+  CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  ctx->adj_rec_kernels = enqueue_record(ctx, K);
+  CU(cudaStreamEndCapture(ctx->stream, &g));
+  CU(cudaGraphInstantiate(&ctx->adj_recgraph, g, 0));
+  cudaGraphDestroy(g);
+  ctx->adj_rgraph.assign(K, nullptr);
+  for (int k = 0; k < K; ++k) {
+    CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    ctx->adj_rev_kernels = adj_reverse_step(ctx, k);
+    CU(cudaStreamEndCapture(ctx->stream, &g));
+    CU(cudaGraphInstantiate(&ctx->adj_rgraph[k], g, 0));
+    cudaGraphDestroy(g);
+  }
+  ctx->adj_graph_K = K;
+  return MOSE_OK;
 }
 
 int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
@@ -1281,9 +1366,9 @@ int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval
   if (rc) return rc;
   const size_t ns = (size_t)ctx->nv * ctx->marena;
   const int nck = (nsteps + interval - 1) / interval;
-  if ((int)ctx->adj_ckpt.size() < nck + 1) {
+  if ((int)ctx->adj_ckpt.size() < nck) {
     const size_t old = ctx->adj_ckpt.size();
-    ctx->adj_ckpt.resize(nck + 1);
+    ctx->adj_ckpt.resize(nck);
     for (size_t q = old; q < ctx->adj_ckpt.size(); ++q)
       if (ctx->adj_ckpt[q].alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (checkpoints)");
   }
@@ -1296,15 +1381,13 @@ int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval
     rc = mose_gpu_advance(ctx, cnt, nullptr, nullptr);
     if (rc) return rc;
   }
-  // the final state (restored after the backward sweep) and the objective
-  CU(cudaMemcpyAsync(ctx->adj_ckpt[nck].p, ctx->state[ctx->cur].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
-                     ctx->stream));
+  // the objective on the final state
   const BlockDesc& d = ctx->desc[block - 1];
   const int nf = (face <= 2) ? d.nj : d.ni;
   CU(cudaMemsetAsync(ctx->lam.p, 0, ns * sizeof(double), ctx->stream));
   adj_objective(ctx->d_desc.p, block - 1, face, nf, ctx->margs(), ctx->state[ctx->cur].p, ctx->objt.p, ctx->lam.p,
                 ctx->stream);
-  adj_sum(ctx->objt.p, nf, ctx->adj_scal.p + 2, 0, ctx->stream);
+  adj_sum(ctx->objt.p, nf, ctx->adj_scal.p + 2, 0, ctx->adj_sumscr.p, ctx->stream);
   CU(cudaMemcpyAsync(J, ctx->adj_scal.p + 2, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   ctx->adj_nsteps = nsteps;
@@ -1322,24 +1405,29 @@ int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach) {
   const size_t ns = (size_t)ctx->nv * ctx->marena;
   const int N = ctx->adj_nsteps, K = ctx->adj_interval, nck = (N + K - 1) / K;
   const double h_time = ctx->h_time;
+  rc = adj_graphs(ctx, K);
+  if (rc) return rc;
   CU(cudaMemsetAsync(ctx->adj_scal.p + 1, 0, sizeof(double), ctx->stream));
   for (int mck = nck - 1; mck >= 0; --mck) {
     const int cnt = std::min(K, N - mck * K);
-    // recompute the segment from its checkpoint, recording the stage inputs
-    CU(cudaMemcpyAsync(ctx->state[ctx->cur].p, ctx->adj_ckpt[mck].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+    // recompute the segment from its checkpoint along the chain, then its
+    // steps in reverse (the state arenas keep the forward run's final state)
+    CU(cudaMemcpyAsync(ctx->adj_seg[0].p, ctx->adj_ckpt[mck].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
                        ctx->stream));
-    int pc = ctx->cur;
-    for (int k = 0; k < cnt; ++k) pc = record_step(ctx, pc, k);
-    CU(cudaMemcpyAsync(ctx->adj_segend.p, ctx->state[pc].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
-                       ctx->stream));
-    for (int k = cnt - 1; k >= 0; --k)
-      adj_reverse_step(ctx, k, k == cnt - 1 ? ctx->adj_segend.p : ctx->adj_seg[3 * (size_t)(k + 1)].p);
+    if (cnt == K) {
+      CU(cudaGraphLaunch(ctx->adj_recgraph, ctx->stream));
+      ctx->launches += ctx->adj_rec_kernels;
+    } else {
+      ctx->launches += enqueue_record(ctx, cnt);
+    }
+    for (int k = cnt - 1; k >= 0; --k) {
+      CU(cudaGraphLaunch(ctx->adj_rgraph[k], ctx->stream));
+      ctx->launches += ctx->adj_rev_kernels;
+    }
     rc = check_launch(ctx, "adjoint_backward");
     if (rc) return rc;
   }
-  // back to the forward run's final state and time
-  CU(cudaMemcpyAsync(ctx->state[ctx->cur].p, ctx->adj_ckpt[nck].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
-                     ctx->stream));
+  // the forward run's time (the recompute advanced the device clock)
   ctx->h_time = h_time;
   ctx->dt_valid = false;
   double h = 0.0;
@@ -1360,12 +1448,11 @@ int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach) {
   const size_t ns = (size_t)ctx->nv * ctx->marena;
   const double h_time = ctx->h_time;
   CU(cudaMemsetAsync(ctx->adj_scal.p + 1, 0, sizeof(double), ctx->stream));
-  const int pc = record_step(ctx, ctx->cur, 0);
-  CU(cudaMemcpyAsync(ctx->adj_segend.p, ctx->state[pc].p, ns * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
-  adj_reverse_step(ctx, 0, ctx->adj_segend.p);
-  // the state stays P^n (the recorded first-stage input)
-  CU(cudaMemcpyAsync(ctx->state[ctx->cur].p, ctx->adj_seg[0].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
+  CU(cudaMemcpyAsync(ctx->adj_seg[0].p, ctx->state[ctx->cur].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
                      ctx->stream));
+  ctx->launches += enqueue_record(ctx, 1);
+  ctx->launches += adj_reverse_step(ctx, 0);
+  // the state arenas still hold P^n
   ctx->h_time = h_time;
   ctx->dt_valid = false;
   double h = 0.0;

@@ -147,3 +147,52 @@ def test_autograd_function_matches_direct_api():
     assert J.item() == J_direct
     assert np.array_equal(p.grad.numpy(), g_direct)
     assert float(m.grad) == dM_direct
+
+
+def test_gradient_perturbed_channel_64():
+    """The adjoint configuration's initial state (uniform Mach-0.8 flow with
+    a seeded 5 % cell-wise perturbation) on a 64^2 grid, 30 steps.  Over 30
+    steps the objective is piecewise smooth at the scale of a 1e-6 step
+    (limiter cut-offs where adjacent slopes change sign, HLLC branches), so
+    the differences use a 1e-7 step here."""
+    case = cases.perturbed_channel(64, steps=30, seed=8)
+    mach = case.extra["mach"]
+    s = solver(case)
+    P0 = case.prim[0].copy()
+    n = 30
+    objective(s, P0, mach, n)
+    dM = s.adjoint_backward()
+    grad = interior(s.download_adjoint(1))
+    rng = np.random.default_rng(9)
+    for q in range(3):
+        d = direction(P0.shape, rng)
+        h = 0.1 * H
+        fd = (objective(s, P0 + h * d, mach, n) - objective(s, P0 - h * d, mach, n)) / (2 * h)
+        adj = float((grad * d).sum())
+        assert abs(adj - fd) <= 1e-5 * abs(fd), (q, adj, fd)
+    fdm = (objective(s, P0, mach + H, n) - objective(s, P0, mach - H, n)) / (2 * H)
+    assert abs(dM - fdm) <= 1e-5 * abs(fdm), (dM, fdm)
+
+
+def test_uniform_state_has_no_gradient_in_v():
+    """At v = 0 exactly (every v-slope zero) the one-step map is not
+    differentiable in v: central differences converge to the limiter's
+    one-sided directional derivative, which is not linear in the direction.
+    A ramp in v over five cells gets limited slopes; each of its single-cell
+    parts alone does not, so the differences do not add up."""
+    case = cases.curvilinear_channel(16, steps=1)
+    mach = case.extra["mach"]
+    s = solver(case)
+    P0 = case.prim[0].copy()
+    rng = np.random.default_rng(10)
+    lam1 = direction(P0.shape, rng)
+    g = lambda P: float((lam1 * step_state(s, P, mach, 1)).sum())
+    fd = lambda d: (g(P0 + H * d) - g(P0 - H * d)) / (2 * H)
+    ramp, parts = np.zeros(P0.shape), 0.0
+    for k in range(5):
+        e = np.zeros(P0.shape)
+        e[0, 8, 6 + k, 2] = k + 1.0
+        ramp += e
+        parts += fd(e)
+    whole = fd(ramp)
+    assert abs(whole - parts) > 1e-3 * abs(whole), (whole, parts)
