@@ -54,10 +54,11 @@ __device__ __forceinline__ double face_at(const MetricArgs& m, const BlockDesc& 
 template <int LIM>
 __device__ __forceinline__ void face_vjp(const Gas& g, const double q[4][NV], const double* dl, const double* n,
                                          double A, const double* Fb, double* F, double C[4][NV]) {
-  const double la = 0.5 * (dl[0] + dl[1]), lb = 0.5 * (dl[1] + dl[2]), lc = 0.5 * (dl[2] + dl[3]);
+  const double ila = fast::rcp(0.5 * (dl[0] + dl[1])), ilb = fast::rcp(0.5 * (dl[1] + dl[2])),
+               ilc = fast::rcp(0.5 * (dl[2] + dl[3]));
   double QL[NV], QR[NV], dsLx[NV], dsLy[NV], dsRx[NV], dsRy[NV];
   for (int v = 0; v < NV; ++v) {
-    const double sa = (q[1][v] - q[0][v]) / la, sb = (q[2][v] - q[1][v]) / lb, sc = (q[3][v] - q[2][v]) / lc;
+    const double sa = (q[1][v] - q[0][v]) * ila, sb = (q[2][v] - q[1][v]) * ilb, sc = (q[3][v] - q[2][v]) * ilc;
     const double sL = adj::limiter_grad<LIM>(sb, sa, &dsLx[v], &dsLy[v]);
     const double sR = adj::limiter_grad<LIM>(sc, sb, &dsRx[v], &dsRy[v]);
     QL[v] = q[1][v] + sL * (0.5 * dl[1]);
@@ -76,9 +77,9 @@ __device__ __forceinline__ void face_vjp(const Gas& g, const double q[4][NV], co
     const double sbb = sLb * dsLx[v] + sRb * dsRy[v];   // sb also feeds sR as its upwind slope
     const double sab = sLb * dsLy[v];
     const double scb = sRb * dsRx[v];
-    C[2][v] += sbb / lb; C[1][v] -= sbb / lb;
-    C[1][v] += sab / la; C[0][v] -= sab / la;
-    C[3][v] += scb / lc; C[2][v] -= scb / lc;
+    C[2][v] += sbb * ilb; C[1][v] -= sbb * ilb;
+    C[1][v] += sab * ila; C[0][v] -= sab * ila;
+    C[3][v] += scb * ilc; C[2][v] -= scb * ilc;
   }
 }
 

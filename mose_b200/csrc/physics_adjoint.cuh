@@ -2,6 +2,9 @@
 // the limiters' partial derivatives, Batten HLLC (Lib_Riemann_HLL.f90:147-258,
 // the single-species algebra of physics_fast.cuh) and the primitive <->
 // conservative maps of Newstate_Conservative (Lib_Newstate.f90:134-160).
+// Divisions and square roots use the refined hardware reciprocal and
+// reciprocal square root of physics_fast.cuh (about one ulp): a derivative
+// needs no more than that.
 //
 // Each *_vjp function recomputes its forward values (kept in registers) and
 // then walks the operations in reverse, accumulating the adjoint of every
@@ -12,6 +15,7 @@
 #pragma once
 
 #include "common.cuh"
+#include "physics_fast.cuh"
 
 namespace mose {
 namespace adj {
@@ -27,14 +31,14 @@ __device__ __forceinline__ double limiter_grad(double x, double y, double* dx, d
   } else if constexpr (LIM == 2) {   // van Leer: x (y sg + |y|) / (|x'| + |y|)
     const double xp = x + 1e-30, sg = copysign(1.0, xp), sy = copysign(1.0, y);
     const double N = y * sg + fabs(y), D = fabs(xp) + fabs(y);
-    const double iD = 1.0 / D;
+    const double iD = fast::rcp(D);
     *dx = N * iD - x * N * sg * iD * iD;
     *dy = x * (sg + sy) * iD - x * N * sy * iD * iD;
     return x * N * iD;
   } else if constexpr (LIM == 3) {   // van Albada: x (y^2 + y x') / (x'^2 + y^2)
     const double xp = x + 1e-30;
     const double N = y * (y + xp), D = xp * xp + y * y;
-    const double iD = 1.0 / D;
+    const double iD = fast::rcp(D);
     *dx = N * iD + x * y * iD - 2.0 * x * N * xp * iD * iD;
     *dy = x * (2.0 * y + xp) * iD - 2.0 * x * N * y * iD * iD;
     return x * N * iD;
@@ -51,20 +55,23 @@ __device__ __forceinline__ void hllc_vjp(double gam, double gcp, double gm1, con
   // ---- forward ------------------------------------------------------------
   const double rl = L[0], ul = L[1], vl = L[2], pl = L[3];
   const double rr = R[0], ur = R[1], vr = R[2], pr = R[3];
-  const double srL = sqrt(rl), srR = sqrt(rr);
-  const double irl = 1.0 / rl, irr = 1.0 / rr;
+  const double rsl = fast::rsqrt_(rl), rsr = fast::rsqrt_(rr);
+  const double srL = rl * rsl, srR = rr * rsr;
+  const double irl = rsl * rsl, irr = rsr * rsr;
   const double unl = ul * nx + vl * ny, unr = ur * nx + vr * ny;
   const double pol = pl * irl, por = pr * irr;
-  const double aL = sqrt(gam * pol), aR = sqrt(gam * por);
+  const double raL = fast::rsqrt_(gam * pol), raR = fast::rsqrt_(gam * por);
+  const double aL = gam * pol * raL, aR = gam * por * raR;
   const double h0l = gcp * pol + 0.5 * (ul * ul + vl * vl);
   const double h0r = gcp * por + 0.5 * (ur * ur + vr * vr);
-  const double isr = 1.0 / (srL + srR);
+  const double isr = fast::rcp(srL + srR);
   const double wl = srL * isr, wr = srR * isr;
   const double ur0 = wr * ur + wl * ul, ur1 = wr * vr + wl * vl;
   const double h0roe = wr * h0r + wl * h0l;
   const double vel2 = ur0 * ur0 + ur1 * ur1;
   const double X = gm1 * (h0roe - 0.5 * vel2);
-  const double a_roe = sqrt(X);
+  const double raroe = X > 0.0 ? fast::rsqrt_(X) : 0.0;
+  const double a_roe = X * raroe;
   const double unroe = ur0 * nx + ur1 * ny;
   // S1 = min(min(0, unl - aL), unroe - a_roe); S4 = max(max(0, unr + aR), unroe + a_roe)
   const double s1a = unl - aL, s1b = unroe - a_roe;
@@ -76,7 +83,7 @@ __device__ __forceinline__ void hllc_vjp(double gam, double gcp, double gm1, con
   const double S4 = fmax(m4, s4b);
   const int s4w = (S4 == s4b && s4b > m4) ? 2 : (m4 == s4a && s4a > 0.0) ? 1 : 0;
   const double ml = rl * (S1 - unl), mr = rr * (S4 - unr);
-  const double idn = 1.0 / (ml - mr);
+  const double idn = fast::rcp(ml - mr);
   const double num = pr - pl + ml * unl - mr * unr;
   const double Sstar = num * idn;
   const bool left = (S1 >= 0.0) || (Sstar >= 0.0);
@@ -91,7 +98,7 @@ __device__ __forceinline__ void hllc_vjp(double gam, double gcp, double gm1, con
   const bool corr = left ? (S1 < 0.0) : (S4 > 0.0);
   const double a1 = unl - S1, a2 = unl - Sstar;
   const double pstar = rl * a1 * a2 + pl;
-  const double inv = 1.0 / (SK - Sstar);
+  const double inv = fast::rcp(SK - Sstar);
   const double dp = pstar - pk;
   const double e0k = h0k - pk * irk;
   const double t1 = mk * uk + dp * nx, t2 = mk * vk + dp * ny, t3 = mk * e0k - pk * unk + pstar * Sstar;
@@ -195,7 +202,7 @@ __device__ __forceinline__ void hllc_vjp(double gam, double gcp, double gm1, con
   double ur0b = unroeb * nx, ur1b = unroeb * ny;
   double h0roeb = 0, vel2b = 0;
   {
-    const double Xb = a_roe > 0.0 ? a_roeb * 0.5 / a_roe : 0.0;
+    const double Xb = a_roeb * 0.5 * raroe;
     h0roeb += Xb * gm1;
     vel2b -= Xb * gm1 * 0.5;
   }
@@ -223,8 +230,8 @@ __device__ __forceinline__ void hllc_vjp(double gam, double gcp, double gm1, con
   vlb += h0lb * vl;
   urb += h0rb * ur;
   vrb += h0rb * vr;
-  polb += aLb * gam * 0.5 / aL;
-  porb += aRb * gam * 0.5 / aR;
+  polb += aLb * gam * 0.5 * raL;
+  porb += aRb * gam * 0.5 * raR;
   plb += polb * irl;
   irlb += polb * pl;
   prb += porb * irr;
@@ -235,8 +242,8 @@ __device__ __forceinline__ void hllc_vjp(double gam, double gcp, double gm1, con
   urb += unrb * nx;
   vrb += unrb * ny;
   // 1/rho and sqrt(rho)
-  rlb += -irlb * irl * irl + srLb * 0.5 / srL;
-  rrb += -irrb * irr * irr + srRb * 0.5 / srR;
+  rlb += -irlb * irl * irl + srLb * 0.5 * rsl;
+  rrb += -irrb * irr * irr + srRb * 0.5 * rsr;
   Lb[0] += rlb; Lb[1] += ulb; Lb[2] += vlb; Lb[3] += plb;
   Rb[0] += rrb; Rb[1] += urb; Rb[2] += vrb; Rb[3] += prb;
 }
@@ -254,7 +261,7 @@ __device__ __forceinline__ void p2u_vjp(double igm1, const double* P, const doub
 // U_b = J^T P_b.
 __device__ __forceinline__ void u2p_vjp(double gm1, const double* P, const double* Pb, double* Ub) {
   const double r = P[0], u = P[1], v = P[2];
-  const double ir = 1.0 / r;
+  const double ir = fast::rcp(r);
   Ub[0] = Pb[0] - Pb[1] * u * ir - Pb[2] * v * ir + Pb[3] * gm1 * 0.5 * (u * u + v * v);
   Ub[1] = Pb[1] * ir - Pb[3] * gm1 * u;
   Ub[2] = Pb[2] * ir - Pb[3] * gm1 * v;
