@@ -236,8 +236,11 @@ int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval
 /* Reverse sweep of the preceding mose_gpu_adjoint_forward: each checkpoint
  * segment is recomputed (recording its stage inputs) and differentiated
  * back.  Leaves dJ/dP of the initial state in the context's adjoint state
- * (mose_gpu_download_adjoint) and returns dJ/dMach; the state returns to the
- * forward run's final state. */
+ * (mose_gpu_download_adjoint) and returns dJ/dMach; the state stays the
+ * forward run's final state.  The first call with a given interval captures
+ * the segment's CUDA graphs on the context's stream (call it outside any
+ * stream capture); later calls replay them.  Device memory: 3 * interval + 1
+ * state arenas for the segment plus ceil(nsteps / interval) checkpoints. */
 int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach);
 /* One step of the adjoint at the current state P^n: the adjoint state goes
  * from lambda^{n+1} (uploaded) to lambda^n = (dP^{n+1}/dP^n)^T lambda^{n+1};
