@@ -370,10 +370,36 @@ def extra_configs(local):
     return rep
 
 
+def profile_adjoint(local):
+    """The launches a profiler captures for the adjoint: the configuration-5
+    channel at 512^2 with 16 steps and a checkpoint every 4, forward and
+    backward once to build the graphs, then once more."""
+    from mose_b200 import Solver, cases
+    from mose_b200.cases import to_ref_layout
+    case = cases.perturbed_channel(512, steps=16)
+    s = Solver(case, precision=precision_code("exact"), device=local)
+    for _ in range(2):
+        s.upload_prim(1, to_ref_layout(case.prim[0]))
+        s.set_time(0.0, 0)
+        s.set_inflow_mach(case.extra["mach"])
+        s.adjoint_forward(16, 4, 1, 3)
+        s.adjoint_backward()
+    s.close()
+    return 0
+
+
+# DRAM bytes per cell per stage-kernel launch, averaged over the three RK
+# stages of one step (ncu dram__bytes_read.sum + dram__bytes_write.sum,
+# vortex 2048^2, the benchmark's kernels); None where not captured.
+TRAFFIC_BYTES_PER_CELL = {"fp64": 363.7e6 / 2048 ** 2, "exact": None, "mixed": None}
+
+
 def run_gpu(args):
     world, rank, local = dist_init()
     import torch
     from mose_b200 import Solver
+    if args.profile_adjoint:
+        return profile_adjoint(local)
     case = workload_case(N_CELLS_SIDE, steps=args.steps)
     cells = case.ncells
     peak, peak_kind = peaks()
@@ -433,7 +459,10 @@ def run_gpu(args):
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f64", "data": "synthetic", "config": workload_config(case, args.precision),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None,
+                             "frac": achieved / peak,
+                             "traffic": (TRAFFIC_BYTES_PER_CELL[args.precision] * cells
+                                         if TRAFFIC_BYTES_PER_CELL.get(args.precision) else None),
+                             "traffic_unit": "bytes per launch (ncu, 3-stage average)",
                              "kernel": "k_stage2d (fused residual + RK stage)", "peak_kind": peak_kind,
                              "stage_ms": stage_ms, "step_kernel_ms": step_ms},
                 "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": nbytes,
@@ -467,6 +496,8 @@ def main():
                     help="skip the four-quadrant and 3-D configuration reports")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + K fused steps (the command profiled by ncu); prints nothing")
+    ap.add_argument("--profile-adjoint", action="store_true",
+                    help="only the adjoint's forward + backward on a 16-step channel (profiled by ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
