@@ -16,8 +16,10 @@ struct MetricArgs {
 
 struct StageArgs {
   const BlockDesc* blk;
-  const int4* items;    // (block, first column, first row, last row + 1)
+  const int4* items;    // (block, first column, first row, last row + 1): items touching a boundary face
   int nitems;
+  const int4* items_nb; // items whose block-edge faces are all connections
+  int nitems_nb;
   const double* Pc;     // current state arena
   const double* Po;     // state at the start of the step (Copy_State's PO)
   double* Pn;           // next state (fused mode)

@@ -169,6 +169,8 @@ struct mose_gpu_ctx {
   DevBuf<BcParam> bcp;
   DevBuf<GhostRec> ghosts;
   DevBuf<int4> items;
+  DevBuf<int4> items_nb;      // 2-D items with no physical boundary face
+  int nitems_nb = 0;
   DevBuf<int4> items3[3];     // 3-D sweeps
   int nitems3[3] = {0, 0, 0};
   DevBuf<double> scal;        // [0] dtglobal, [1] time
@@ -660,10 +662,32 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
 
   // ---- work items for the stage kernel -----------------------------------------
-  std::vector<int4> items = plan_stage_items(ctx->hblk, 2 * ctx->nsm);
+  std::vector<int4> all = plan_stage_items(ctx->hblk, 3 * ctx->nsm);
+  // an item runs the boundary-free kernel when every block-edge face its
+  // cells have (column -1 / ni, row -1 / nj) is a connection
+  std::vector<int4> items, items_nb;
+  for (const int4& it : all) {
+    const BlockDesc& d = ctx->desc[it.x];
+    const int c0 = it.y & 0xffff, c1 = it.y >> 16, j0 = it.z, j1 = it.w;
+    bool conn = true;
+    auto check = [&](int f, int lo, int hi) {
+      for (int q = lo; q < hi && conn; ++q) conn = bc_code(bcwords[d.bcoff[f] + q]) == BC_CONN;
+    };
+    if (c0 == 0) check(0, j0, j1);
+    if (c1 == d.ni) check(1, j0, j1);
+    if (j0 == 0) check(2, c0, c1);
+    if (j1 == d.nj) check(3, c0, c1);
+    (conn && ctx->nd == 2 ? items_nb : items).push_back(it);
+  }
   ctx->nitems = (int)items.size();
-  CU(ctx->items.alloc(items.size()));
-  CU(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->nitems_nb = (int)items_nb.size();
+  CU(ctx->items.alloc(std::max<size_t>(items.size(), 1)));
+  CU(ctx->items_nb.alloc(std::max<size_t>(items_nb.size(), 1)));
+  if (!items.empty())
+    CU(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+  if (!items_nb.empty())
+    CU(cudaMemcpyAsync(ctx->items_nb.p, items_nb.data(), items_nb.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                       ctx->stream));
   if (ctx->nd == 3) {
     std::vector<int4> it3[3];
     plan_3d_items(ctx->hblk, it3);
@@ -817,6 +841,8 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   a.blk = ctx->d_desc.p;
   a.items = ctx->items.p;
   a.nitems = ctx->nitems;
+  a.items_nb = ctx->items_nb.p;
+  a.nitems_nb = ctx->nitems_nb;
   a.Pc = ctx->state[pc].p;
   a.Po = ctx->state[po].p;
   a.Pn = pn >= 0 ? ctx->state[pn].p : nullptr;
@@ -846,7 +872,9 @@ static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int pre
     return launch_stage3d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
                ? (ctx->nitems3[0] > 0 ? 3 : 2)
                : 0;
-  return launch_stage2d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream) ? 1 : 0;
+  return launch_stage2d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
+             ? (a.nitems > 0) + (a.nitems_nb > 0)
+             : 0;
 }
 
 int mose_gpu_residual(mose_gpu_ctx* ctx) {

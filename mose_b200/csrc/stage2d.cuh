@@ -44,6 +44,8 @@
 // from the FP64 state.
 #pragma once
 
+#include <type_traits>
+
 #include "arena.cuh"
 #include "physics_exact.cuh"
 #include "physics_fast.cuh"
@@ -259,25 +261,39 @@ constexpr bool stage_fp32_pipeline() {
 }
 
 // NVR ring planes: the NV state variables, plus dl along i and j with metric
-// arrays.  MX: the FP32 pipeline's arrays replace the FP64 slope arrays.
-template <int NV, int NVR, bool MX>
+// arrays.  MX: the FP32 pipeline's arrays replace the FP64 slope arrays.  BC:
+// the items may touch physical boundary faces (their add masks are kept);
+// without, the FP32 pipeline's face fluxes are all FP32 values and are kept
+// as such.  Arrays a variant does not use shrink to one element.
+template <int NV, int NVR, bool MX, bool BC>
 struct StageSmem {
+  using FluxT = typename std::conditional<MX && !BC, float, double>::type;
+  static constexpr int kY = MX ? 1 : SB_Y, kX = MX ? 1 : SB_X, kV = MX ? 1 : NV;
+  static constexpr int mY = MX ? SB_Y : 1, mX = MX ? SB_X : 1, mR = MX ? SB_RING : 1, mS = MX ? SB_RS : 1;
   double ring[NVR][SB_RING][SB_RS];
-  double po[2][NV][SB_Y][SB_X];       // PO of the owned cells (column c - c0), double buffered
-  double f[NV][SB_Y][SB_X];           // F(c + 1/2, j)
-  double g[NV][SB_Y + 1][SB_X];       // G(c, j0 + r - 1/2): row 0 carried from the previous batch
-  int fm[SB_Y][SB_X];                 // add masks of F / G
-  int gm[SB_Y + 1][SB_X];
-  double sx[MX ? 1 : NV][SB_Y][SB_X];       // limited i-slope of cell (c, j)
-  double sy[MX ? 1 : NV][SB_Y + 1][SB_X];   // limited j-slope of row r: 0 = batch base row (carried)
-  float4 r32[MX ? SB_RING : 1][SB_RS];      // FP32 ring of (rho, u, v, p)
-  float4 sx32[MX ? SB_Y : 1][SB_X];
-  float4 sy32[MX ? SB_Y + 1 : 1][SB_X];
+  double po[NV][SB_Y][SB_X];          // PO of the owned cells (column c - c0) of the current batch
+  FluxT f[NV][SB_Y][SB_X];            // F(c + 1/2, j)
+  FluxT g[NV][SB_Y + 1][SB_X];        // G(c, j0 + r - 1/2): row 0 carried from the previous batch
+  int fm[BC ? SB_Y : 1][BC ? SB_X : 1];       // add masks of F / G
+  int gm[BC ? SB_Y + 1 : 1][BC ? SB_X : 1];
+  double sx[kV][kY][kX];              // limited i-slope of cell (c, j)
+  double sy[kV][MX ? 1 : SB_Y + 1][kX];   // limited j-slope of row r: 0 = batch base row (carried)
+  float4 r32[mR][mS];                 // FP32 ring of (rho, u, v, p)
+  float4 sx32[mY][mX];
+  float4 sy32[MX ? SB_Y + 1 : 1][mX];
 };
 
-template <bool UNI, bool MX>
+template <bool UNI, bool MX, bool BC>
 constexpr size_t stage_smem_bytes() {
-  return sizeof(StageSmem<4, UNI ? 4 : 6, MX>);
+  return sizeof(StageSmem<4, UNI ? 4 : 6, MX, BC>);
+}
+
+// Minimum resident CTAs per SM of a kernel variant.  Without boundary faces
+// the uniform-metric kernels fit three CTAs (80 registers, ~71 KB of shared
+// memory); the boundary formulas (a call) and the metric-array ring need two.
+template <bool UNI, bool BC>
+constexpr int stage_min_ctas() {
+  return (UNI && !BC) ? 3 : 2;
 }
 
 __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
@@ -286,6 +302,8 @@ __device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+// all but the most recent commit group of this thread complete
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 __device__ __forceinline__ float4 f4_add(float4 a, float4 b) {
   return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
@@ -298,10 +316,6 @@ __device__ __forceinline__ float4 f4_fma(float s, float4 b, float4 a) {
   return make_float4(fmaf(s, b.x, a.x), fmaf(s, b.y, a.y), fmaf(s, b.z, a.z), fmaf(s, b.w, a.w));
 }
 
-// Minimum resident CTAs per SM the register allocation is sized for.
-#ifndef MOSE_STAGE_MIN_CTAS
-#define MOSE_STAGE_MIN_CTAS 2
-#endif
 
 // FP32 CFL dt of one cell of a uniform 2-D block (the FP32 pipeline's fused
 // Compute_dt): a relative error near 1e-7 in the global dt moves the solution
@@ -319,8 +333,12 @@ __device__ __forceinline__ double cfl_dt32(const Gas& g, const double* Q, const 
 
 // MODE: 0 = fused (residual + RK update, writes Pn), 1 = residual only (writes
 // R), 2 = fused and the next step's Compute_dt on the new state (last stage).
-template <class PH, int RIE, int LIM, bool UNI, int MODE>
-__global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs a) {
+// BC: the kernel of the items that touch a physical boundary face (a.items);
+// without, the items whose block-edge faces are all connections
+// (a.items_nb): no boundary formula, every face flux added whole.  Both add
+// a cell's face terms in the same order, so their results are identical.
+template <class PH, int RIE, int LIM, bool UNI, int MODE, bool BC>
+__global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(StageArgs a) {
   constexpr int NV = 4;
   constexpr int NVR = UNI ? NV : NV + 2;
   constexpr bool MX = stage_fp32_pipeline<PH, RIE, UNI>();
@@ -328,15 +346,17 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
   // so slopes stay in difference units and the half-cell factor is 1/2
   constexpr bool FU = UNI && PH::kFast;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  StageSmem<NV, NVR, MX>& S = *reinterpret_cast<StageSmem<NV, NVR, MX>*>(smem_raw);
+  StageSmem<NV, NVR, MX, BC>& S = *reinterpret_cast<StageSmem<NV, NVR, MX, BC>*>(smem_raw);
+  const int4* items = BC ? a.items : a.items_nb;
+  const int nitems = BC ? a.nitems : a.nitems_nb;
   const int t = threadIdx.x;
   const int tx = t % SB_X, ty = t / SB_X;
   const bool need_po = (MODE != 1) && (a.irk != 1);
   double dtrun = __longlong_as_double(0x7ff0000000000000LL);   // fused dt: running minimum
 
 #pragma unroll 1
-  for (int it = blockIdx.x; it < a.nitems; it += gridDim.x) {
-    const int4 item = a.items[it];
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 item = items[it];
     const int b = item.x, c0 = item.y & 0xffff, c1 = item.y >> 16, j0 = item.z, j1 = item.w;
     const BlockDesc& d = a.blk[b];
     const int ni = d.ni, nj = d.nj, px = d.px;
@@ -462,7 +482,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
         }
       }
     };
-    // PO of batch kk (rows j0 + 4 kk .., owned columns) into po[kk & 1]
+    // PO of batch kk (rows j0 + 4 kk .., owned columns) into po
     auto load_po = [&](int kk) {
       const double* Po = a.Po + d.sbase;
       const int rbase = j0 + SB_Y * kk;
@@ -475,14 +495,13 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
         const int r = rbase + i;
         const int x = c0 + GW + 2 * q;   // padded column of cell c0 + 2q
         if (r >= j1 || x >= px) continue;
-        cp_async16(&S.po[kk & 1][v][i][2 * q], Po + v * vs + (long long)(r + GW) * px + x);
+        cp_async16(&S.po[v][i][2 * q], Po + v * vs + (long long)(r + GW) * px + x);
       }
     };
 
     // ---- prologue: j-slopes of rows j0-1, j0 and the j-face below row j0 --------
     load_unit(0);
     load_unit(1);
-    if (need_po) load_po(0);
     cp_async_commit();
     cp_async_wait_all();
     convert_unit(0);
@@ -523,7 +542,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
       }
       if (!ok && j0 > 0) report(a.err, 4, b, c, j0, 0);
       int mask = ADD_ALL;
-      if (j0 == 0) {
+      if (BC && j0 == 0) {
         const int w = a.bcw[d.bcoff[2] + c];
         if (bc_code(w) == BC_NONE) {
           for (int v = 0; v < NV; ++v) G[v] = 0.0;
@@ -537,14 +556,17 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
       }
 #pragma unroll
       for (int v = 0; v < NV; ++v) S.g[v][SB_Y][tx] = G[v];
-      S.gm[SB_Y][tx] = mask;
+      if constexpr (BC) S.gm[SB_Y][tx] = mask;
     }
 
 #pragma unroll 1
     for (int k = 0; k < nbatch; ++k) {
-      __syncthreads();   // ring units k, k+1 and po[k & 1] visible; batch k-1 done with everything
+      __syncthreads();   // ring units k, k+1 visible; batch k-1 done with everything
+      // two commit groups: this batch's PO (waited for before phase C), then
+      // ring unit k + 2 (waited for at the end of the batch)
+      if (need_po) load_po(k);
+      cp_async_commit();
       if (k + 2 <= nbatch) load_unit(k + 2);
-      if (need_po && k + 1 < nbatch) load_po(k + 1);
       cp_async_commit();
       const int j = j0 + SB_Y * k + ty;
       const bool rowok = j < j1;
@@ -557,7 +579,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
       if (ty == 0 && owns) {   // carry the previous batch's top j-face
 #pragma unroll
         for (int v = 0; v < NV; ++v) S.g[v][0][tx] = S.g[v][SB_Y][tx];
-        S.gm[0][tx] = S.gm[SB_Y][tx];
+        if constexpr (BC) S.gm[0][tx] = S.gm[SB_Y][tx];
       }
       if (rowok) {
         if constexpr (MX) {
@@ -608,7 +630,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           const bool lowb = (c == -1), highb = (c == ni - 1);
           int mask = ADD_ALL;
           if (!ok && !lowb && !highb) report(a.err, 4, b, c, j, 0);
-          if (lowb || highb) {
+          if (BC && (lowb || highb)) {
             const int w = a.bcw[d.bcoff[lowb ? 0 : 1] + j];
             if (bc_code(w) == BC_NONE) {
               for (int v = 0; v < NV; ++v) F[v] = 0.0;
@@ -625,7 +647,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           }
 #pragma unroll
           for (int v = 0; v < NV; ++v) S.f[v][ty][tx] = F[v];
-          S.fm[ty][tx] = mask;
+          if constexpr (BC) S.fm[ty][tx] = mask;
         }
         if (owns) {
           double G[NV], n[3];
@@ -647,7 +669,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           }
           int mask = ADD_ALL;
           if (!ok && j < nj - 1) report(a.err, 4, b, c, j, 0);
-          if (j == nj - 1) {
+          if (BC && j == nj - 1) {
             const int w = a.bcw[d.bcoff[3] + c];
             if (bc_code(w) == BC_NONE) {
               for (int v = 0; v < NV; ++v) G[v] = 0.0;
@@ -662,9 +684,10 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           }
 #pragma unroll
           for (int v = 0; v < NV; ++v) S.g[v][ty + 1][tx] = G[v];
-          S.gm[ty + 1][tx] = mask;
+          if constexpr (BC) S.gm[ty + 1][tx] = mask;
         }
       }
+      cp_async_wait_prev();   // this thread's copies of this batch's PO
       __syncthreads();
 
       // ---- phase C: residual and update ---------------------------------------------
@@ -674,8 +697,8 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           // exact FP64 differences of the FP32 face fluxes, scaled by the areas
 #pragma unroll
           for (int v = 0; v < NV; ++v) {
-            const double dF = S.f[v][ty][tx] - S.f[v][ty][tx - 1];
-            const double dG = S.g[v][ty + 1][tx] - S.g[v][ty][tx];
+            const double dF = (double)S.f[v][ty][tx] - (double)S.f[v][ty][tx - 1];
+            const double dG = (double)S.g[v][ty + 1][tx] - (double)S.g[v][ty][tx];
             Rv[v] = fma(u_Ax, dF, u_Ay * dG);
           }
         } else {
@@ -694,10 +717,18 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           if (!bi1) for (int v = 0; v < NV; ++v) R.add(v, Fp[v]);
           if (!bj0) for (int v = 0; v < NV; ++v) R.add(v, -Gm[v]);
           if (!bj1) for (int v = 0; v < NV; ++v) R.add(v, Gp[v]);
-          if (bi0) add_bc<NV>(R, Fm, -1.0, S.fm[ty][tx - 1]);
-          if (bi1) add_bc<NV>(R, Fp, 1.0, S.fm[ty][tx]);
-          if (bj0) add_bc<NV>(R, Gm, -1.0, S.gm[ty][tx]);
-          if (bj1) add_bc<NV>(R, Gp, 1.0, S.gm[ty + 1][tx]);
+          // block-edge faces last, in face order (connections without BC)
+          if constexpr (BC) {
+            if (bi0) add_bc<NV>(R, Fm, -1.0, S.fm[ty][tx - 1]);
+            if (bi1) add_bc<NV>(R, Fp, 1.0, S.fm[ty][tx]);
+            if (bj0) add_bc<NV>(R, Gm, -1.0, S.gm[ty][tx]);
+            if (bj1) add_bc<NV>(R, Gp, 1.0, S.gm[ty + 1][tx]);
+          } else {
+            if (bi0) add_bc<NV>(R, Fm, -1.0, ADD_ALL);
+            if (bi1) add_bc<NV>(R, Fp, 1.0, ADD_ALL);
+            if (bj0) add_bc<NV>(R, Gm, -1.0, ADD_ALL);
+            if (bj1) add_bc<NV>(R, Gp, 1.0, ADD_ALL);
+          }
 #pragma unroll
           for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
         }
@@ -715,7 +746,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           const bool first = (a.irk == 1);
           if (!first) {
 #pragma unroll
-            for (int v = 0; v < NV; ++v) QO[v] = S.po[k & 1][v][ty][tx - 1];
+            for (int v = 0; v < NV; ++v) QO[v] = S.po[v][ty][tx - 1];
           }
           const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
           if (!ok) report(a.err, 5, b, c, j, 0);
@@ -739,7 +770,7 @@ __global__ void __launch_bounds__(SB_T, MOSE_STAGE_MIN_CTAS) k_stage2d(StageArgs
           for (int v = 0; v < NV; ++v) S.sy[v][0][tx] = S.sy[v][SB_Y][tx];
         }
       }
-      cp_async_wait_all();   // this thread's copies of unit k+2 and po[k+1 & 1]
+      cp_async_wait_all();   // this thread's copies of unit k+2
       if (k + 2 <= nbatch) convert_unit(k + 2);
     }
     __syncthreads();   // the next item refills the ring

@@ -19,20 +19,28 @@ using StagePolicy = typename std::conditional<PREC == 0, PolExact<RIE, LIM>, Pol
 
 // Persistent grid: as many CTAs as the SMs hold at once (registers and the
 // shared-memory ring decide), never more than there are work items.
-template <int PREC, int RIE, int LIM, bool UNI, int MODE>
-static void launch_persistent(const StageArgs& a, int nsm, cudaStream_t s) {
+template <int PREC, int RIE, int LIM, bool UNI, int MODE, bool BC>
+static void launch_persistent_list(const StageArgs& a, int nitems, int nsm, cudaStream_t s) {
   using PH = StagePolicy<PREC, RIE, LIM>;
-  constexpr size_t smem = stage_smem_bytes<UNI, stage_fp32_pipeline<PH, RIE, UNI>()>();
+  constexpr size_t smem = stage_smem_bytes<UNI, stage_fp32_pipeline<PH, RIE, UNI>(), BC>();
   static int occ = 0;   // one per kernel instance
   if (occ == 0) {
-    cudaFuncSetAttribute(k_stage2d<PH, RIE, LIM, UNI, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage2d<PH, RIE, LIM, UNI, MODE>, SB_T, smem) !=
+    cudaFuncSetAttribute(k_stage2d<PH, RIE, LIM, UNI, MODE, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage2d<PH, RIE, LIM, UNI, MODE, BC>, SB_T, smem) !=
             cudaSuccess ||
         occ < 1)
       occ = 1;
   }
-  const int grid = a.nitems < occ * nsm ? a.nitems : occ * nsm;
-  k_stage2d<PH, RIE, LIM, UNI, MODE><<<grid, SB_T, smem, s>>>(a);
+  const int grid = nitems < occ * nsm ? nitems : occ * nsm;
+  k_stage2d<PH, RIE, LIM, UNI, MODE, BC><<<grid, SB_T, smem, s>>>(a);
+}
+
+// The items without physical boundary faces, then those with.
+template <int PREC, int RIE, int LIM, bool UNI, int MODE>
+static void launch_persistent(const StageArgs& a, int nsm, cudaStream_t s) {
+  if (a.nitems_nb > 0) launch_persistent_list<PREC, RIE, LIM, UNI, MODE, false>(a, a.nitems_nb, nsm, s);
+  if (a.nitems > 0) launch_persistent_list<PREC, RIE, LIM, UNI, MODE, true>(a, a.nitems, nsm, s);
 }
 
 template <int PREC, int RIE, int LIM>
