@@ -55,6 +55,9 @@ __device__ __forceinline__ double sqrt_(double x) {
   return x > 0.0 ? s : 0.0;
 }
 __device__ __forceinline__ double div_(double a, double b) { return a * rcp(b); }
+// sqrt(x) = x rsqrt(x) without the residual correction (about 1.5 ulp): the
+// sound speeds of the Riemann solver, where that is far inside the bar
+__device__ __forceinline__ double sqrt1_(double x) { return x > 0.0 ? x * rsqrt_(x) : 0.0; }
 
 // ---- limiters: phi(r) x with r = y/(x + 1e-30), one reciprocal each --------
 // The rational limiters are rewritten over a common denominator, which is
@@ -167,7 +170,7 @@ __device__ __forceinline__ void hllc(const GasF& g, const double* L, const doubl
   const double irl = rsl * rsl, irr = rsr * rsr;        // 1/rho
   const double unl = un<NV>(L, n), unr = un<NV>(R, n);
   const double pol = L[P] * irl, por = R[P] * irr;      // p/rho
-  const double aL = sqrt_(g.gamma * pol), aR = sqrt_(g.gamma * por);
+  const double aL = sqrt1_(g.gamma * pol), aR = sqrt1_(g.gamma * por);
   const double h0l = fma(g.gcp, pol, 0.5 * v2<NV>(L));
   const double h0r = fma(g.gcp, por, 0.5 * v2<NV>(R));
   const double isr = rcp(srL + srR);
@@ -179,7 +182,7 @@ __device__ __forceinline__ void hllc(const GasF& g, const double* L, const doubl
   if constexpr (NV == 5) ur[2] = fma(wr, R[3], wl * L[3]);
   const double h0_roe = fma(wr, h0r, wl * h0l);
   const double vel2 = ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2];
-  const double a_roe = sqrt_(g.gm1 * fma(-0.5, vel2, h0_roe));
+  const double a_roe = sqrt1_(g.gm1 * fma(-0.5, vel2, h0_roe));
   const double un_roe = (NV == 5) ? ur[0] * n[0] + ur[1] * n[1] + ur[2] * n[2] : ur[0] * n[0] + ur[1] * n[1];
   const double S1 = fmin(fmin(0.0, unl - aL), un_roe - a_roe);
   const double S4 = fmax(fmax(0.0, unr + aR), un_roe + a_roe);
