@@ -65,7 +65,14 @@ enum {
   MOSE_RIEMANN_HLLC = 0,
   MOSE_RIEMANN_AUSMP = 1,
   MOSE_RIEMANN_SLAU = 2,
-  MOSE_RIEMANN_SLAU2 = 3
+  MOSE_RIEMANN_SLAU2 = 3,
+  MOSE_RIEMANN_HLLE = 4,       /* 'HLLE'  (Lib_Riemann_HLL.f90:259-317) */
+  MOSE_RIEMANN_HLLEM = 5,      /* 'HLLEM' (Lib_Riemann_HLL.f90:23-146) */
+  MOSE_RIEMANN_LLF = 6,        /* 'LLF', 'Rusanov' (Lib_Riemann_LF.f90:10-45) */
+  MOSE_RIEMANN_PLLF = 7,       /* 'PLLF'  (Lib_Riemann_LF.f90:48-102) */
+  MOSE_RIEMANN_HANEL = 8,      /* 'Hanel' (Lib_Riemann_AUSM.f90:48-117) */
+  MOSE_RIEMANN_AUSMP_UP = 9,   /* 'AUSM+-up'  (Lib_Riemann_AUSM.f90:273-418), needs Minf */
+  MOSE_RIEMANN_AUSMP_UP2 = 10  /* 'AUSM+-up2' (Lib_Riemann_AUSM.f90:455-570), needs Minf */
 };
 
 /* Arithmetic of the face sweeps and of the fused steps' CFL pass.  In the
@@ -226,6 +233,12 @@ int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
  * whole Explicit_Step: every RK stage, the boundary fluxes (405 also in the
  * inflow Mach), the ghost fill and the global CFL dt (through its argmin
  * cell). */
+/* riemann-options-Minf (Register_Numerics.f90:72), the reference Mach number
+ * of AUSM+-up and AUSM+-up2; call before mose_gpu_setup.  Setup rejects
+ * those two solvers while it is 0, as Assign_Setup.f90:96-100 does.  2-D
+ * only: the 3-D sweeps run HLLC and AUSM+. */
+int mose_gpu_set_riemann_minf(mose_gpu_ctx* ctx, double minf);
+
 /* Sets the Mach number of every 405 supersonic-inflow face. */
 int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach);
 /* Runs nsteps fused steps from the current state keeping a checkpoint of the

@@ -25,7 +25,8 @@ NPRIM = 5
 
 # limiter / riemann names as in input.ini (Register_Numerics.f90:57-72)
 LIMITERS = {"first-order": 0, "none": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5}
-RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3}
+RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3, "HLLE": 4, "HLLEM": 5, "LLF": 6, "Rusanov": 6,
+           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10}
 
 
 @dataclass
@@ -40,6 +41,7 @@ class Case:
     time_accurate: bool = True
     limiter: str = "minmod"
     riemann: str = "HLLC"
+    minf: float = 0.0          # riemann-options-Minf (AUSM+-up, AUSM+-up2)
     gamma: float = 1.4
     rgas: float = 1.0
     steps: int = 1

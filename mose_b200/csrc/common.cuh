@@ -49,6 +49,10 @@ struct Gas {
   double gm1;       // gamma - 1
   double gcp;       // gamma / (gamma - 1)
   double igm1;      // 1 / (gamma - 1)
+  // Riemann solver index (MOSE_RIEMANN_*) for the kernels that select the
+  // solver at run time, and riemann-options-Minf of AUSM+-up / AUSM+-up2
+  int rie;
+  double minf;
 };
 
 // Per-block descriptor (device resident).

@@ -77,22 +77,24 @@ namespace mose {
 // Stage kernels: one launcher per (precision p, Riemann solver r) unit.
 #define MOSE_STAGE_DECL(p, r) \
   bool launch_stage2d_p##p##_r##r(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s);
-MOSE_STAGE_DECL(0, 0) MOSE_STAGE_DECL(0, 1) MOSE_STAGE_DECL(0, 2) MOSE_STAGE_DECL(0, 3)
-MOSE_STAGE_DECL(1, 0) MOSE_STAGE_DECL(1, 1) MOSE_STAGE_DECL(1, 2) MOSE_STAGE_DECL(1, 3)
-MOSE_STAGE_DECL(2, 0) MOSE_STAGE_DECL(2, 1) MOSE_STAGE_DECL(2, 2) MOSE_STAGE_DECL(2, 3)
+MOSE_STAGE_DECL(0, 0) MOSE_STAGE_DECL(0, 1) MOSE_STAGE_DECL(0, 2) MOSE_STAGE_DECL(0, 3) MOSE_STAGE_DECL(0, 4)
+MOSE_STAGE_DECL(1, 0) MOSE_STAGE_DECL(1, 1) MOSE_STAGE_DECL(1, 2) MOSE_STAGE_DECL(1, 3) MOSE_STAGE_DECL(1, 4)
+MOSE_STAGE_DECL(2, 0) MOSE_STAGE_DECL(2, 1) MOSE_STAGE_DECL(2, 2) MOSE_STAGE_DECL(2, 3) MOSE_STAGE_DECL(2, 4)
 #undef MOSE_STAGE_DECL
 
 // mode 0: fused residual + RK update; 1: residual only (exact precision);
 // 2: fused, plus the next step's Compute_dt (last RK stage of a fused step).
+// Solvers 4.. (HLLE, HLLEM, LLF, PLLF, Hanel, AUSM+-up, AUSM+-up2) share one
+// unit per precision that selects the solver at run time (Gas::rie).
 inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int prec, int rie, int lim,
                            cudaStream_t s) {
   using L = bool (*)(const StageArgs&, int, int, bool, int, cudaStream_t);
-  static const L table[3][4] = {
-      {launch_stage2d_p0_r0, launch_stage2d_p0_r1, launch_stage2d_p0_r2, launch_stage2d_p0_r3},
-      {launch_stage2d_p1_r0, launch_stage2d_p1_r1, launch_stage2d_p1_r2, launch_stage2d_p1_r3},
-      {launch_stage2d_p2_r0, launch_stage2d_p2_r1, launch_stage2d_p2_r2, launch_stage2d_p2_r3}};
-  if (prec < 0 || prec > 2 || rie < 0 || rie > 3) return false;
-  return table[prec][rie](a, nsm, mode, uni, lim, s);
+  static const L table[3][5] = {
+      {launch_stage2d_p0_r0, launch_stage2d_p0_r1, launch_stage2d_p0_r2, launch_stage2d_p0_r3, launch_stage2d_p0_r4},
+      {launch_stage2d_p1_r0, launch_stage2d_p1_r1, launch_stage2d_p1_r2, launch_stage2d_p1_r3, launch_stage2d_p1_r4},
+      {launch_stage2d_p2_r0, launch_stage2d_p2_r1, launch_stage2d_p2_r2, launch_stage2d_p2_r3, launch_stage2d_p2_r4}};
+  if (prec < 0 || prec > 2 || rie < 0 || rie > 10) return false;
+  return table[prec][rie < 4 ? rie : 4](a, nsm, mode, uni, lim, s);
 }
 
 // 3-D: three directional sweeps per RK stage; HLLC and AUSM+ with minmod,

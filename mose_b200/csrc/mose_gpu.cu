@@ -327,7 +327,7 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   *out = nullptr;
   if (cfg->abi_version != MOSE_GPU_ABI_VERSION) return MOSE_ERR_INVALID;
   if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 || cfg->integration != MOSE_INTEGRATION_CONS ||
-      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > 3 ||
+      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > MOSE_RIEMANN_AUSMP_UP2 ||
       cfg->precision < 0 || cfg->precision > 2 || !(cfg->gamma > 1.0) || !(cfg->rgas > 0.0))
     return MOSE_ERR_UNSUPPORTED;
   ctx = new mose_gpu_ctx();
@@ -358,6 +358,8 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   ctx->gas.gm1 = cfg->gamma - 1.0;
   ctx->gas.gcp = cfg->gamma / (cfg->gamma - 1.0);
   ctx->gas.igm1 = 1.0 / (cfg->gamma - 1.0);
+  ctx->gas.rie = cfg->riemann;
+  ctx->gas.minf = 0.0;
   *out = ctx;
   return MOSE_OK;
 }
@@ -455,6 +457,9 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   else ctx->ndir = 2;
   ctx->nd = (ctx->ndir == 3) ? 3 : 2;
   ctx->nv = (ctx->nd == 3) ? 5 : 4;
+  if ((ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP || ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP2) &&
+      !(ctx->gas.minf > 0.0))
+    return fail(ctx, MOSE_ERR_INVALID, "AUSM+-up solver selected: Minf must be set (mose_gpu_set_riemann_minf)");
   if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: HLLC or AUSM+ with minmod, van Leer or van Albada");
   auto nodeh = [&](const HostBlock& h, int i, int j, int k, int c) {
@@ -1360,6 +1365,14 @@ static int adj_graphs(mose_gpu_ctx* ctx, int K) {
     cudaGraphDestroy(g);
   }
   ctx->adj_graph_K = K;
+  return MOSE_OK;
+}
+
+int mose_gpu_set_riemann_minf(mose_gpu_ctx* ctx, double minf) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_riemann_minf: call before mose_gpu_setup");
+  if (!(minf >= 0.0)) return fail(ctx, MOSE_ERR_INVALID, "set_riemann_minf: Minf must be >= 0");
+  ctx->gas.minf = minf;
   return MOSE_OK;
 }
 

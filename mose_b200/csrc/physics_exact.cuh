@@ -244,12 +244,269 @@ __device__ __forceinline__ void slau(const Gas& g, const double* L, double aL, c
   F[P] = F[0] * ((F[0] >= 0.0) ? H_L : H_R);
 }
 
+// ---- the solvers selected at run time (Gas::rie >= 4) -------------------------
+// They work on three-component velocities and normals, w = 0 and n_z = 0 in
+// 2-D, with every term the reference forms (an exact zero where it vanishes).
+struct St3 { double r, u, v, w, p, a; };
+template <int NV>
+__device__ __forceinline__ St3 st3(const double* q, double a) {
+  constexpr int P = NV - 1;
+  St3 s;
+  s.r = q[0]; s.u = q[1]; s.v = q[2]; s.w = (NV == 5) ? q[3] : 0.0; s.p = q[P]; s.a = a;
+  return s;
+}
+struct Fl5 { double r, u, v, w, E; };
+__device__ __forceinline__ double E0(const Gas& g, double p, double rho, double umag) {
+  double T = p / (rho * g.R);
+  double e = g.cv * T;
+  return e + 0.5 * (umag * umag);
+}
+__device__ __forceinline__ double umag3(const St3& s) { return sqrt(s.u * s.u + s.v * s.v + s.w * s.w); }
+// fluxes(p, r, u, v, w, n), Lib_Riemann_LF.f90:105-126
+__device__ __forceinline__ Fl5 phys3(const Gas& g, const St3& q, double nx, double ny, double nz) {
+  Fl5 F;
+  F.r = q.r * (q.u * nx + q.v * ny + q.w * nz);
+  F.u = F.r * q.u + q.p * nx;
+  F.v = F.r * q.v + q.p * ny;
+  F.w = F.r * q.w + q.p * nz;
+  F.E = F.r * H0(g, q.p, q.r, umag3(q));
+  return F;
+}
+// roe_averages, Lib_Riemann_HLL.f90:550-647 (one calorically perfect species)
+struct Roe { double h0l, h0r, rho, u, v, w, a, h0; };
+__device__ __forceinline__ Roe roe3(const Gas& g, const St3& L, const St3& R) {
+  Roe o;
+  double inv_dltot = 1.0 / L.r, inv_drtot = 1.0 / R.r;
+  double Tl = L.p * inv_dltot / g.R, Tr = R.p * inv_drtot / g.R;
+  double srL = sqrt(L.r), srR = sqrt(R.r);
+  o.rho = srL * srR;
+  double inv_sr = 1.0 / (srL + srR);
+  o.u = (srR * R.u + srL * L.u) * inv_sr;
+  o.v = (srR * R.v + srL * L.v) * inv_sr;
+  o.w = (srR * R.w + srL * L.w) * inv_sr;
+  double R_roe = (srR * g.R + srL * g.R) * inv_sr;
+  double T_roe = (srR * Tr + srL * Tl) * inv_sr;
+  double hl = g.cp * Tl, hr = g.cp * Tr;
+  double el = hl - g.R * Tl, er = hr - g.R * Tr;
+  o.h0l = hl * L.r * inv_dltot;
+  o.h0r = hr * R.r * inv_drtot;
+  double d_roe = (srR * R.r * inv_drtot + srL * L.r * inv_dltot) * inv_sr;
+  double cv_roe = d_roe * g.cpmR;
+  double sum_ei = d_roe * (srR * er + srL * el) * inv_sr;
+  o.h0l = o.h0l + 0.5 * (L.u * L.u + L.v * L.v + L.w * L.w);
+  o.h0r = o.h0r + 0.5 * (R.u * R.u + R.v * R.v + R.w * R.w);
+  o.h0 = (srR * o.h0r + srL * o.h0l) * inv_sr;
+  double gam_roe = 1.0 + R_roe / cv_roe;
+  double vel2 = o.u * o.u + o.v * o.v + o.w * o.w;
+  o.a = sqrt((gam_roe - 1.0) * (o.h0 - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+  return o;
+}
+
+// riemann_HLLE, Lib_Riemann_HLL.f90:259-317
+__device__ __forceinline__ Fl5 hlle3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz) {
+  Fl5 F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  Roe o = roe3(g, L, R);
+  double un_roe = o.u * nx + o.v * ny + o.w * nz;
+  double S1 = fmin(fmin(0.0, unl - L.a), un_roe - o.a);
+  double S4 = fmax(fmax(0.0, unr + R.a), un_roe + o.a);
+  double inv_denom = 1.0 / (S4 - S1);
+  double FrL = L.r * unl, FrR = R.r * unr;
+  F.r = (S4 * FrL - S1 * FrR + S1 * S4 * (R.r - L.r)) * inv_denom;
+  F.u = (S4 * (FrL * L.u + L.p * nx) - S1 * (FrR * R.u + R.p * nx) + S1 * S4 * (R.r * R.u - L.r * L.u)) * inv_denom;
+  F.v = (S4 * (FrL * L.v + L.p * ny) - S1 * (FrR * R.v + R.p * ny) + S1 * S4 * (R.r * R.v - L.r * L.v)) * inv_denom;
+  F.w = (S4 * (FrL * L.w + L.p * nz) - S1 * (FrR * R.w + R.p * nz) + S1 * S4 * (R.r * R.w - L.r * L.w)) * inv_denom;
+  F.E = (S4 * (FrL * o.h0l) - S1 * (FrR * o.h0r) +
+         S1 * S4 * (R.r * (o.h0r - R.p / R.r) - L.r * (o.h0l - L.p / L.r))) * inv_denom;
+  return F;
+}
+
+// riemann_HLLEM, Lib_Riemann_HLL.f90:23-146
+__device__ __forceinline__ Fl5 hllem3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz) {
+  Fl5 F;
+  Roe o = roe3(g, L, R);
+  double un_roe = o.u * nx + o.v * ny + o.w * nz;
+  double S1 = fmin(fmin(0.0, (L.u * nx + L.v * ny + L.w * nz) - L.a), un_roe - o.a);
+  double S4 = fmax(fmax(0.0, (R.u * nx + R.v * ny + R.w * nz) + R.a), un_roe + o.a);
+  Fl5 Fl = phys3(g, L, nx, ny, nz), Fr = phys3(g, R, nx, ny, nz);
+  F.r = (S4 * Fl.r - S1 * Fr.r + S1 * S4 * (R.r - L.r)) / (S4 - S1);
+  F.u = (S4 * Fl.u - S1 * Fr.u + S1 * S4 * (R.r * R.u - L.r * L.u)) / (S4 - S1);
+  F.v = (S4 * Fl.v - S1 * Fr.v + S1 * S4 * (R.r * R.v - L.r * L.v)) / (S4 - S1);
+  F.w = (S4 * Fl.w - S1 * Fr.w + S1 * S4 * (R.r * R.w - L.r * L.w)) / (S4 - S1);
+  F.E = (S4 * Fl.E - S1 * Fr.E + S1 * S4 * (R.r * E0(g, R.p, R.r, umag3(R)) - L.r * E0(g, L.p, L.r, umag3(L)))) /
+        (S4 - S1);
+  if (S1 < 0.0 && S4 > 0.0) {
+    double drho = R.r - L.r, dp = R.p - L.p;
+    double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+    double t1x, t1y, t1z;
+    if (fabs(nx) < 0.9) { t1x = 0.0; t1y = -nz; t1z = ny; }
+    else { t1x = -nz; t1y = 0.0; t1z = nx; }
+    double normt = sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+    t1x = t1x / normt; t1y = t1y / normt; t1z = t1z / normt;
+    double t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
+    double alpha_c = drho - dp / (o.a * o.a);
+    double alpha_s1 = o.rho * (du * t1x + dv * t1y + dw * t1z);
+    double alpha_s2 = o.rho * (du * t2x + dv * t2y + dw * t2z);
+    double delta = o.a / (o.a + fabs(0.5 * (S1 + S4)));
+    double C = (S1 * S4) / (S4 - S1);
+    F.r = F.r - C * delta * alpha_c;
+    F.u = F.u - C * delta * (alpha_c * o.u);
+    F.v = F.v - C * delta * (alpha_c * o.v);
+    F.w = F.w - C * delta * (alpha_c * o.w);
+    F.u = F.u - C * delta * (alpha_s1 * t1x + alpha_s2 * t2x);
+    F.v = F.v - C * delta * (alpha_s1 * t1y + alpha_s2 * t2y);
+    F.w = F.w - C * delta * (alpha_s1 * t1z + alpha_s2 * t2z);
+    F.E = F.E - C * delta * (alpha_c * 0.5 * (o.u * o.u + o.v * o.v + o.w * o.w));
+    F.E = F.E - C * delta * (alpha_s1 * (o.u * t1x + o.v * t1y + o.w * t1z) + alpha_s2 * (o.u * t2x + o.v * t2y + o.w * t2z));
+  }
+  return F;
+}
+
+// 0.5 (F_L + F_R - A (U_R - U_L)), Lib_Riemann_LF.f90:39-44 / :96-101
+__device__ __forceinline__ Fl5 lf3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz,
+                                   double A) {
+  Fl5 Fr = phys3(g, R, nx, ny, nz), Fl = phys3(g, L, nx, ny, nz), F;
+  F.r = 0.5 * (Fl.r + Fr.r - A * (R.r - L.r));
+  F.u = 0.5 * (Fr.u + Fl.u - A * (R.r * R.u - L.r * L.u));
+  F.v = 0.5 * (Fr.v + Fl.v - A * (R.r * R.v - L.r * L.v));
+  F.w = 0.5 * (Fr.w + Fl.w - A * (R.r * R.w - L.r * L.w));
+  F.E = 0.5 * (Fl.E + Fr.E - A * (R.r * E0(g, R.p, R.r, umag3(R)) - L.r * E0(g, L.p, L.r, umag3(L))));
+  return F;
+}
+// riemann_LLF (Rusanov), Lib_Riemann_LF.f90:10-45
+__device__ __forceinline__ Fl5 llf3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz) {
+  double uln = L.u * nx + L.v * ny + L.w * nz;
+  double urn = R.u * nx + R.v * ny + R.w * nz;
+  double A = fmax(fmax(fmax(fabs(uln - L.a), fabs(urn - R.a)), fabs(uln + L.a)), fabs(urn + R.a));
+  return lf3(g, L, R, nx, ny, nz, A);
+}
+// Riemann_PLLF, Lib_Riemann_LF.f90:48-102 (theta_L/R are formed there but unused)
+__device__ __forceinline__ Fl5 pllf3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz) {
+  double uln = L.u * nx + L.v * ny + L.w * nz;
+  double urn = R.u * nx + R.v * ny + R.w * nz;
+  double U_rl = fmax(1e-5 * L.a, fmin(fabs(uln), L.a));
+  double U_rr = fmax(1e-5 * R.a, fmin(fabs(urn), R.a));
+  double betal = 1.0 / (L.a * L.a), betar = 1.0 / (R.a * R.a);
+  double alphal = 0.5 * (1.0 - betal * (U_rl * U_rl));
+  double alphar = 0.5 * (1.0 - betar * (U_rr * U_rr));
+  double ul_mod = fabs(uln * (1.0 - alphal));
+  double ur_mod = fabs(urn * (1.0 - alphar));
+  double al_mod = sqrt((alphal * alphal) * (uln * uln) + U_rl * U_rl);
+  double ar_mod = sqrt((alphar * alphar) * (urn * urn) + U_rr * U_rr);
+  double A = fmax(ul_mod + al_mod, ur_mod + ar_mod);
+  return lf3(g, L, R, nx, ny, nz, A);
+}
+// riemann_Hanel, Lib_Riemann_AUSM.f90:48-117
+__device__ __forceinline__ Fl5 hanel3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz) {
+  Fl5 F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double H_L = H0(g, L.p, L.r, umag3(L));
+  double H_R = H0(g, R.p, R.r, umag3(R));
+  double uLp, uRm, pLp, pRm;
+  if (fabs(unl) <= L.a) uLp = ((unl + L.a) * (unl + L.a)) / (4.0 * L.a);
+  else uLp = 0.5 * (unl + fabs(unl));
+  if (fabs(unr) <= R.a) uRm = (-((unr - R.a) * (unr - R.a))) / (4.0 * R.a);
+  else uRm = 0.5 * (unr - fabs(unr));
+  if (fabs(unl) <= L.a) pLp = L.p * uLp * (2.0 - unl / L.a) / L.a;
+  else pLp = L.p * uLp / unl;
+  if (fabs(unr) <= R.a) pRm = R.p * uRm * (-2.0 - unr / R.a) / R.a;
+  else pRm = R.p * uRm / unr;
+  double phalf = pLp + pRm;
+  F.r = uLp * L.r + uRm * R.r;
+  F.u = uLp * (L.r * L.u) + uRm * (R.r * R.u) + phalf * nx;
+  F.v = uLp * (L.r * L.v) + uRm * (R.r * R.v) + phalf * ny;
+  F.w = uLp * (L.r * L.w) + uRm * (R.r * R.w) + phalf * nz;
+  F.E = uLp * (L.r * H_L) + uRm * (R.r * H_R);
+  return F;
+}
+// riemann_AUSMp_up, Lib_Riemann_AUSM.f90:273-418; riemann_AUSMp_up2, :455-570
+__device__ __forceinline__ Fl5 ausmpup3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz,
+                                        bool up2) {
+  const double Kp = 0.25, Ku = 0.75, sigma = 1.0, beta = 0.125;
+  Fl5 F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double sq_vel = 0.5 * ((L.u * L.u + L.v * L.v + L.w * L.w) + (R.u * R.u + R.v * R.v + R.w * R.w));
+  double H_L = H0(g, L.p, L.r, umag3(L));
+  double H_R = H0(g, R.p, R.r, umag3(R));
+  double astarL2 = 2.0 * (g.gamma - 1.0) / (g.gamma + 1.0) * H_L;
+  double astarR2 = 2.0 * (g.gamma - 1.0) / (g.gamma + 1.0) * H_R;
+  double astarL = sqrt(astarL2), astarR = sqrt(astarR2);
+  double atildeL = astarL2 / fmax(astarL, unl);
+  double atildeR = astarR2 / fmax(astarR, -unr);
+  double aF = fmin(atildeL, atildeR);
+  double mL = unl / aF, mR = unr / aF;
+  double MFsq = 0.5 * (mL * mL + mR * mR);
+  double Mrefsq = fmin(1.0, fmax(MFsq, g.minf * g.minf));
+  double fa = 2.0 * sqrt(Mrefsq) - Mrefsq;
+  double alpha = up2 ? 3.0 / 16.0 * (-4.0 + 5.0 * fa * fa) : 0.1875 * (-4.0 + 5.0 * fa * fa);
+  double mLP, mRM, bLP, bRM;
+  if (fabs(mL) <= 1.0) {
+    double p1 = 0.25 * ((mL + 1.0) * (mL + 1.0));
+    double p2 = (mL * mL - 1.0) * (mL * mL - 1.0);
+    mLP = p1 + beta * p2;
+    bLP = p1 * (2.0 - mL) + alpha * mL * p2;
+  } else {
+    mLP = 0.5 * (mL + fabs(mL));
+    bLP = mLP / mL;
+  }
+  if (fabs(mR) <= 1.0) {
+    double p1 = 0.25 * ((mR - 1.0) * (mR - 1.0));
+    double p2 = (mR * mR - 1.0) * (mR * mR - 1.0);
+    mRM = -p1 - beta * p2;
+    bRM = p1 * (2.0 + mR) - alpha * mR * p2;
+  } else {
+    mRM = 0.5 * (mR - fabs(mR));
+    bRM = mRM / mR;
+  }
+  double rhoF = 0.5 * (L.r + R.r);
+  double Mp = -(Kp / fa) * fmax(0.0, 1.0 - sigma * MFsq) * (R.p - L.p) / (rhoF * aF * aF);
+  double mF = mLP + mRM + Mp;
+  double mdot = aF * (fmax(mF, 0.0) * L.r + fmin(mF, 0.0) * R.r);
+  double phalf;
+  if (!up2) {
+    double Pu = -Ku * fa * bLP * bRM * 2.0 * rhoF * aF * (unr - unl);
+    phalf = bLP * L.p + bRM * R.p + Pu;
+  } else {
+    phalf = 0.5 * (R.p + L.p) + 0.5 * (bLP - bRM) * (L.p - R.p) + sqrt(sq_vel) * (bLP + bRM - 1.0) * rhoF * aF;
+  }
+  const bool up = mF >= 0.0;
+  F.r = mdot;
+  F.u = mdot * (up ? L.u : R.u) + nx * phalf;
+  F.v = mdot * (up ? L.v : R.v) + ny * phalf;
+  F.w = mdot * (up ? L.w : R.w) + nz * phalf;
+  F.E = mdot * (up ? H_L : H_R);
+  return F;
+}
+
+template <int NV>
+__device__ __noinline__ void riemann_rt(const Gas& g, const double* Lq, double aL, const double* Rq, double aR,
+                                        const double* n, double* F) {
+  const St3 L = st3<NV>(Lq, aL), R = st3<NV>(Rq, aR);
+  Fl5 f;
+  switch (g.rie) {
+    case 4: f = hlle3(g, L, R, n[0], n[1], n[2]); break;
+    case 5: f = hllem3(g, L, R, n[0], n[1], n[2]); break;
+    case 6: f = llf3(g, L, R, n[0], n[1], n[2]); break;
+    case 7: f = pllf3(g, L, R, n[0], n[1], n[2]); break;
+    case 8: f = hanel3(g, L, R, n[0], n[1], n[2]); break;
+    case 9: f = ausmpup3(g, L, R, n[0], n[1], n[2], false); break;
+    default: f = ausmpup3(g, L, R, n[0], n[1], n[2], true); break;
+  }
+  F[0] = f.r; F[1] = f.u; F[2] = f.v;
+  if constexpr (NV == 5) { F[3] = f.w; F[4] = f.E; }
+  else F[3] = f.E;
+}
+
 template <int RIE, int NV>
 __device__ __forceinline__ void riemann(const Gas& g, const double* L, double aL, const double* R,
                                         double aR, const double* n, double* F) {
   if constexpr (RIE == 1) ausmp<NV>(g, L, aL, R, aR, n, F);
   else if constexpr (RIE == 2) slau<NV>(g, L, aL, R, aR, n, F, false);
   else if constexpr (RIE == 3) slau<NV>(g, L, aL, R, aR, n, F, true);
+  else if constexpr (RIE == 4) riemann_rt<NV>(g, L, aL, R, aR, n, F);
   else hllc<NV>(g, L, aL, R, aR, n, F);
 }
 

@@ -66,6 +66,8 @@ class Solver:
             raise MoseError(rc, "mose_gpu_create failed (no sm_100 device, or unsupported configuration)")
         self.h = h
         self.case = case
+        if getattr(case, "minf", 0.0):
+            self._check(self.lib.mose_gpu_set_riemann_minf(self.h, float(case.minf)))
         self.dims = []
         for b, nd in enumerate(case.nodes, start=1):
             nk, nj, ni = nd.shape[0] - 1, nd.shape[1] - 1, nd.shape[2] - 1

@@ -22,6 +22,8 @@
 //   T = p / (rho R),  a = sqrt(gamma R T),  h(T) = cp T  (table h_tab)
 //   cp = gamma R / (gamma - 1),  cv = R / (gamma - 1)
 //   H0(p, rho_s, |u|) = h(T) + 0.5 |u|^2
+//   E0(p, rho_s, |u|) = e(T) + 0.5 |u|^2,  e(T) = cv T
+//   f_gamma = gamma,  f_cp = cp
 //   prim2cons: (rho, rho u, rho v, rho w, rho (cv T + 0.5 |u|^2))
 //   cons2prim: u = (rho u)/rho ..., T = (E/rho - 0.5|u|^2)/cv, p = rho R T
 //   check_gas_state: error unless rho_s > 0 and p > 0
@@ -147,6 +149,12 @@ inline double H0(const Thermo& t, double p, double rhos, double umag) {
   double h = (rhos / rho) * (t.cp * T);
   return h + 0.5 * (umag * umag);
 }
+inline double E0(const Thermo& t, double p, double rhos, double umag) {
+  double rho = rhos, R = t.R;
+  double T = p / (rho * R);
+  double e = (rhos / rho) * (t.cv * T);
+  return e + 0.5 * (umag * umag);
+}
 inline double norm2(double a, double b, double c) { return std::sqrt(a * a + b * b + c * c); }
 inline double dot3(const double* a, const double* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 inline int check_gas_state(double rhos, double p) { return (rhos > 0.0 && p > 0.0) ? 0 : 1; }
@@ -256,6 +264,20 @@ inline void roe_averages(const Thermo& t, const RState& L, const RState& Rr, dou
   double gam_roe = 1.0 + R_roe / cv_roe;
   double vel2 = u_roe * u_roe + v_roe * v_roe + w_roe * w_roe;
   a_roe = std::sqrt((gam_roe - 1.0) * (h0_roe - 0.5 * vel2 + cv_roe * T_roe - sum_ei));
+}
+// rho_roe of roe_averages (Lib_Riemann_HLL.f90, roe_averages: rho_roe = srL srR)
+inline double rho_roe_of(const RState& L, const RState& R) { return std::sqrt(L.rho) * std::sqrt(R.rho); }
+
+// fluxes(p, r, u, v, w, n), Lib_Riemann_LF.f90 (and its twin in
+// Lib_Riemann_HLL.f90): the physical flux of one state
+inline RFlux phys_flux(const Thermo& t, const RState& Q, double nx, double ny, double nz) {
+  RFlux F;
+  F.r = Q.d * (Q.u * nx + Q.v * ny + Q.w * nz);
+  F.u = F.r * Q.u + Q.p * nx;
+  F.v = F.r * Q.v + Q.p * ny;
+  F.w = F.r * Q.w + Q.p * nz;
+  F.E = F.r * H0(t, Q.p, Q.d, std::sqrt(Q.u * Q.u + Q.v * Q.v + Q.w * Q.w));
+  return F;
 }
 
 // riemann_HLLC (Batten), Lib_Riemann_HLL.f90:147-258
@@ -412,12 +434,227 @@ inline RFlux riemann_SLAU(const Thermo& t, const RState& L, const RState& R, dou
   return F;
 }
 
+// riemann_HLLE, Lib_Riemann_HLL.f90:259-317 (Batten signal speeds)
+inline RFlux riemann_HLLE(const Thermo& t, const RState& L, const RState& R, double nx, double ny,
+                          double nz) {
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe;
+  roe_averages(t, L, R, h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe);
+  double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  double S1 = std::min(std::min(0.0, unl - L.a), un_roe - a_roe);
+  double S4 = std::max(std::max(0.0, unr + R.a), un_roe + a_roe);
+  double inv_denom = 1.0 / (S4 - S1);
+  double FrL = L.rho * unl, FrR = R.rho * unr;
+  F.r = (S4 * FrL - S1 * FrR + S1 * S4 * (R.rho - L.rho)) * inv_denom;
+  F.u = (S4 * (FrL * L.u + L.p * nx) - S1 * (FrR * R.u + R.p * nx) + S1 * S4 * (R.rho * R.u - L.rho * L.u)) * inv_denom;
+  F.v = (S4 * (FrL * L.v + L.p * ny) - S1 * (FrR * R.v + R.p * ny) + S1 * S4 * (R.rho * R.v - L.rho * L.v)) * inv_denom;
+  F.w = (S4 * (FrL * L.w + L.p * nz) - S1 * (FrR * R.w + R.p * nz) + S1 * S4 * (R.rho * R.w - L.rho * L.w)) * inv_denom;
+  F.E = (S4 * (FrL * h0l) - S1 * (FrR * h0r) +
+         S1 * S4 * (R.rho * (h0r - R.p / R.rho) - L.rho * (h0l - L.p / L.rho))) * inv_denom;
+  return F;
+}
+
+// riemann_HLLEM (Einfeldt et al. 1991), Lib_Riemann_HLL.f90:23-146: HLL flux of
+// the physical fluxes plus the anti-diffusion of the contact and shear waves
+// when S1 < 0 < S4
+inline RFlux riemann_HLLEM(const Thermo& t, const RState& L, const RState& R, double nx, double ny,
+                           double nz) {
+  RFlux F;
+  double h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe;
+  roe_averages(t, L, R, h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe);
+  double rho_roe = rho_roe_of(L, R);
+  double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  double S1 = std::min(std::min(0.0, (L.u * nx + L.v * ny + L.w * nz) - L.a), un_roe - a_roe);
+  double S4 = std::max(std::max(0.0, (R.u * nx + R.v * ny + R.w * nz) + R.a), un_roe + a_roe);
+  RFlux Fl = phys_flux(t, L, nx, ny, nz), Fr = phys_flux(t, R, nx, ny, nz);
+  F.r = (S4 * Fl.r - S1 * Fr.r + S1 * S4 * (R.rho - L.rho)) / (S4 - S1);
+  F.u = (S4 * Fl.u - S1 * Fr.u + S1 * S4 * (R.rho * R.u - L.rho * L.u)) / (S4 - S1);
+  F.v = (S4 * Fl.v - S1 * Fr.v + S1 * S4 * (R.rho * R.v - L.rho * L.v)) / (S4 - S1);
+  F.w = (S4 * Fl.w - S1 * Fr.w + S1 * S4 * (R.rho * R.w - L.rho * L.w)) / (S4 - S1);
+  F.E = (S4 * Fl.E - S1 * Fr.E +
+         S1 * S4 * (R.rho * E0(t, R.p, R.d, std::sqrt(R.u * R.u + R.v * R.v + R.w * R.w)) -
+                    L.rho * E0(t, L.p, L.d, std::sqrt(L.u * L.u + L.v * L.v + L.w * L.w)))) / (S4 - S1);
+  if (S1 < 0.0 && S4 > 0.0) {
+    double drho = R.rho - L.rho, dp = R.p - L.p;
+    double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+    double t1x, t1y, t1z;
+    if (std::fabs(nx) < 0.9) { t1x = 0.0; t1y = -nz; t1z = ny; }
+    else { t1x = -nz; t1y = 0.0; t1z = nx; }
+    double normt = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+    t1x = t1x / normt; t1y = t1y / normt; t1z = t1z / normt;
+    double t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
+    double alpha_c = drho - dp / (a_roe * a_roe);
+    double alpha_s1 = rho_roe * (du * t1x + dv * t1y + dw * t1z);
+    double alpha_s2 = rho_roe * (du * t2x + dv * t2y + dw * t2z);
+    double delta = a_roe / (a_roe + std::fabs(0.5 * (S1 + S4)));
+    double C = (S1 * S4) / (S4 - S1);
+    F.r = F.r - C * delta * alpha_c;
+    F.u = F.u - C * delta * (alpha_c * u_roe);
+    F.v = F.v - C * delta * (alpha_c * v_roe);
+    F.w = F.w - C * delta * (alpha_c * w_roe);
+    F.u = F.u - C * delta * (alpha_s1 * t1x + alpha_s2 * t2x);
+    F.v = F.v - C * delta * (alpha_s1 * t1y + alpha_s2 * t2y);
+    F.w = F.w - C * delta * (alpha_s1 * t1z + alpha_s2 * t2z);
+    F.E = F.E - C * delta * (alpha_c * 0.5 * (u_roe * u_roe + v_roe * v_roe + w_roe * w_roe));
+    F.E = F.E - C * delta * (alpha_s1 * (u_roe * t1x + v_roe * t1y + w_roe * t1z) +
+                             alpha_s2 * (u_roe * t2x + v_roe * t2y + w_roe * t2z));
+  }
+  return F;
+}
+
+// Shared by the Lax-Friedrichs pair: 0.5 (F_L + F_R - A (U_R - U_L)),
+// Lib_Riemann_LF.f90:39-44 / :96-101
+inline RFlux lf_flux(const Thermo& t, const RState& L, const RState& R, double nx, double ny, double nz,
+                     double A) {
+  RFlux Fr = phys_flux(t, R, nx, ny, nz), Fl = phys_flux(t, L, nx, ny, nz), F;
+  F.r = 0.5 * (Fl.r + Fr.r - A * (R.rho - L.rho));
+  F.u = 0.5 * (Fr.u + Fl.u - A * (R.rho * R.u - L.rho * L.u));
+  F.v = 0.5 * (Fr.v + Fl.v - A * (R.rho * R.v - L.rho * L.v));
+  F.w = 0.5 * (Fr.w + Fl.w - A * (R.rho * R.w - L.rho * L.w));
+  F.E = 0.5 * (Fl.E + Fr.E - A * (R.rho * E0(t, R.p, R.d, std::sqrt(R.u * R.u + R.v * R.v + R.w * R.w)) -
+                                  L.rho * E0(t, L.p, L.d, std::sqrt(L.u * L.u + L.v * L.v + L.w * L.w))));
+  return F;
+}
+
+// riemann_LLF (Rusanov), Lib_Riemann_LF.f90:10-45
+inline RFlux riemann_LLF(const Thermo& t, const RState& L, const RState& R, double nx, double ny,
+                         double nz) {
+  double uln = L.u * nx + L.v * ny + L.w * nz;
+  double urn = R.u * nx + R.v * ny + R.w * nz;
+  double A = std::max(std::max(std::max(std::fabs(uln - L.a), std::fabs(urn - R.a)), std::fabs(uln + L.a)),
+                      std::fabs(urn + R.a));
+  return lf_flux(t, L, R, nx, ny, nz, A);
+}
+
+// Riemann_PLLF (preconditioned Rusanov), Lib_Riemann_LF.f90:48-102
+inline RFlux riemann_PLLF(const Thermo& t, const RState& L, const RState& R, double nx, double ny,
+                          double nz) {
+  double uln = L.u * nx + L.v * ny + L.w * nz;
+  double urn = R.u * nx + R.v * ny + R.w * nz;
+  double Tl = L.p / (L.rho * t.R), Tr = R.p / (R.rho * t.R);
+  double rho_Tl = -L.rho / Tl, rho_Tr = -R.rho / Tr;
+  double cpl = t.cp, cpr = t.cp;
+  double U_rl = std::max(1e-5 * L.a, std::min(std::fabs(uln), L.a));
+  double U_rr = std::max(1e-5 * R.a, std::min(std::fabs(urn), R.a));
+  double thetal = 1.0 / (U_rl * U_rl) - rho_Tl / (L.rho * cpl);
+  double thetar = 1.0 / (U_rr * U_rr) - rho_Tr / (R.rho * cpr);
+  (void)thetal;
+  (void)thetar;
+  double betal = 1.0 / (L.a * L.a), betar = 1.0 / (R.a * R.a);
+  double alphal = 0.5 * (1.0 - betal * (U_rl * U_rl));
+  double alphar = 0.5 * (1.0 - betar * (U_rr * U_rr));
+  double ul_mod = std::fabs(uln * (1.0 - alphal));
+  double ur_mod = std::fabs(urn * (1.0 - alphar));
+  double al_mod = std::sqrt((alphal * alphal) * (uln * uln) + U_rl * U_rl);
+  double ar_mod = std::sqrt((alphar * alphar) * (urn * urn) + U_rr * U_rr);
+  double A = std::max(ul_mod + al_mod, ur_mod + ar_mod);
+  return lf_flux(t, L, R, nx, ny, nz, A);
+}
+
+// riemann_Hanel, Lib_Riemann_AUSM.f90:48-117
+inline RFlux riemann_Hanel(const Thermo& t, const RState& L, const RState& R, double nx, double ny,
+                           double nz) {
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double H_L = H0(t, L.p, L.d, std::sqrt(L.u * L.u + L.v * L.v + L.w * L.w));
+  double H_R = H0(t, R.p, R.d, std::sqrt(R.u * R.u + R.v * R.v + R.w * R.w));
+  double uLp, uRm, pLp, pRm;
+  if (std::fabs(unl) <= L.a) uLp = ((unl + L.a) * (unl + L.a)) / (4.0 * L.a);
+  else uLp = 0.5 * (unl + std::fabs(unl));
+  if (std::fabs(unr) <= R.a) uRm = (-((unr - R.a) * (unr - R.a))) / (4.0 * R.a);
+  else uRm = 0.5 * (unr - std::fabs(unr));
+  if (std::fabs(unl) <= L.a) pLp = L.p * uLp * (2.0 - unl / L.a) / L.a;
+  else pLp = L.p * uLp / unl;
+  if (std::fabs(unr) <= R.a) pRm = R.p * uRm * (-2.0 - unr / R.a) / R.a;
+  else pRm = R.p * uRm / unr;
+  double phalf = pLp + pRm;
+  F.r = uLp * L.rho + uRm * R.rho;
+  F.u = uLp * (L.rho * L.u) + uRm * (R.rho * R.u) + phalf * nx;
+  F.v = uLp * (L.rho * L.v) + uRm * (R.rho * R.v) + phalf * ny;
+  F.w = uLp * (L.rho * L.w) + uRm * (R.rho * R.w) + phalf * nz;
+  F.E = uLp * (L.rho * H_L) + uRm * (R.rho * H_R);
+  return F;
+}
+
+// riemann_AUSMp_up (SU2 form), Lib_Riemann_AUSM.f90:273-418, and
+// riemann_AUSMp_up2 (Kitamura-Shima pressure flux), :455-570
+inline RFlux riemann_AUSMp_up(const Thermo& t, const RState& L, const RState& R, double nx, double ny,
+                              double nz, double minf, bool up2) {
+  const double Kp = 0.25, Ku = 0.75, sigma = 1.0, beta = 0.125;
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double sq_vel = 0.5 * ((L.u * L.u + L.v * L.v + L.w * L.w) + (R.u * R.u + R.v * R.v + R.w * R.w));
+  double H_L = H0(t, L.p, L.d, std::sqrt(L.u * L.u + L.v * L.v + L.w * L.w));
+  double H_R = H0(t, R.p, R.d, std::sqrt(R.u * R.u + R.v * R.v + R.w * R.w));
+  double gamma_L = t.gamma, gamma_R = t.gamma;
+  double astarL2 = 2.0 * (gamma_L - 1.0) / (gamma_L + 1.0) * H_L;
+  double astarR2 = 2.0 * (gamma_R - 1.0) / (gamma_R + 1.0) * H_R;
+  double astarL = std::sqrt(astarL2), astarR = std::sqrt(astarR2);
+  double atildeL = astarL2 / std::max(astarL, unl);
+  double atildeR = astarR2 / std::max(astarR, -unr);
+  double aF = std::min(atildeL, atildeR);
+  double mL = unl / aF, mR = unr / aF;
+  double MFsq = 0.5 * (mL * mL + mR * mR);
+  double Mrefsq = std::min(1.0, std::max(MFsq, minf * minf));
+  double fa = 2.0 * std::sqrt(Mrefsq) - Mrefsq;
+  double alpha = up2 ? 3.0 / 16.0 * (-4.0 + 5.0 * fa * fa) : 0.1875 * (-4.0 + 5.0 * fa * fa);
+  double mLP, mRM, bLP, bRM;
+  if (std::fabs(mL) <= 1.0) {
+    double p1 = 0.25 * ((mL + 1.0) * (mL + 1.0));
+    double p2 = (mL * mL - 1.0) * (mL * mL - 1.0);
+    mLP = p1 + beta * p2;
+    bLP = p1 * (2.0 - mL) + alpha * mL * p2;
+  } else {
+    mLP = 0.5 * (mL + std::fabs(mL));
+    bLP = mLP / mL;
+  }
+  if (std::fabs(mR) <= 1.0) {
+    double p1 = 0.25 * ((mR - 1.0) * (mR - 1.0));
+    double p2 = (mR * mR - 1.0) * (mR * mR - 1.0);
+    mRM = -p1 - beta * p2;
+    bRM = p1 * (2.0 + mR) - alpha * mR * p2;
+  } else {
+    mRM = 0.5 * (mR - std::fabs(mR));
+    bRM = mRM / mR;
+  }
+  double rhoF = 0.5 * (L.rho + R.rho);
+  double Mp = -(Kp / fa) * std::max(0.0, 1.0 - sigma * MFsq) * (R.p - L.p) / (rhoF * aF * aF);
+  double mF = mLP + mRM + Mp;
+  double mdot = aF * (std::max(mF, 0.0) * L.rho + std::min(mF, 0.0) * R.rho);
+  double phalf;
+  if (!up2) {
+    double Pu = -Ku * fa * bLP * bRM * 2.0 * rhoF * aF * (unr - unl);
+    phalf = bLP * L.p + bRM * R.p + Pu;
+  } else {
+    phalf = 0.5 * (R.p + L.p) + 0.5 * (bLP - bRM) * (L.p - R.p) + std::sqrt(sq_vel) * (bLP + bRM - 1.0) * rhoF * aF;
+  }
+  const RState& K = (mF >= 0.0) ? L : R;
+  double upwind_H = (mF >= 0.0) ? H_L : H_R;
+  F.r = mdot;
+  F.u = mdot * K.u + nx * phalf;
+  F.v = mdot * K.v + ny * phalf;
+  F.w = mdot * K.w + nz * phalf;
+  F.E = mdot * upwind_H;
+  return F;
+}
+
 inline RFlux Riemann(const orc_domain* d, const RState& L, const RState& R, double nx,
                      double ny, double nz) {
   switch (d->cfg.riemann) {
     case ORC_RIE_AUSMP: return riemann_AUSMp(d->th, L, R, nx, ny, nz);
     case ORC_RIE_SLAU: return riemann_SLAU(d->th, L, R, nx, ny, nz, false);
     case ORC_RIE_SLAU2: return riemann_SLAU(d->th, L, R, nx, ny, nz, true);
+    case ORC_RIE_HLLE: return riemann_HLLE(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_HLLEM: return riemann_HLLEM(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_LLF: return riemann_LLF(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_PLLF: return riemann_PLLF(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_HANEL: return riemann_Hanel(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_AUSMP_UP: return riemann_AUSMp_up(d->th, L, R, nx, ny, nz, d->cfg.minf, false);
+    case ORC_RIE_AUSMP_UP2: return riemann_AUSMp_up(d->th, L, R, nx, ny, nz, d->cfg.minf, true);
     default: return riemann_HLLC(d->th, L, R, nx, ny, nz);
   }
 }

@@ -29,7 +29,9 @@ typedef struct orc_domain orc_domain;
 enum { ORC_LIM_FIRST_ORDER = 0, ORC_LIM_MINMOD = 1, ORC_LIM_VANLEER = 2,
        ORC_LIM_VANALBADA = 3, ORC_LIM_MC = 4, ORC_LIM_SUPERBEE = 5 };
 /* Riemann solvers (Mod_Riemann.f90:43-112). */
-enum { ORC_RIE_HLLC = 0, ORC_RIE_AUSMP = 1, ORC_RIE_SLAU = 2, ORC_RIE_SLAU2 = 3 };
+enum { ORC_RIE_HLLC = 0, ORC_RIE_AUSMP = 1, ORC_RIE_SLAU = 2, ORC_RIE_SLAU2 = 3,
+       ORC_RIE_HLLE = 4, ORC_RIE_HLLEM = 5, ORC_RIE_LLF = 6, ORC_RIE_PLLF = 7,
+       ORC_RIE_HANEL = 8, ORC_RIE_AUSMP_UP = 9, ORC_RIE_AUSMP_UP2 = 10 };
 /* Integration variables (Mod_Newstate.f90:30-44). */
 enum { ORC_INT_CONS = 0, ORC_INT_PRIM = 1 };
 
@@ -45,6 +47,7 @@ typedef struct orc_config {
   double rgas;
   int32_t ramp_iter;     /* cfl-rise-threshold */
   int32_t res_diter;     /* residual output interval */
+  double minf;           /* riemann-options-Minf (AUSM+-up, AUSM+-up2) */
 } orc_config;
 
 /* Error codes: mirror the reference's fatal `stop` sites. */

@@ -20,7 +20,7 @@ class orc_config(C.Structure):
     _fields_ = [("n_rk", C.c_int32), ("cfl", C.c_double), ("time_accurate", C.c_int32),
                 ("limiter", C.c_int32), ("riemann", C.c_int32), ("integration", C.c_int32),
                 ("ndir", C.c_int32), ("gamma", C.c_double), ("rgas", C.c_double),
-                ("ramp_iter", C.c_int32), ("res_diter", C.c_int32)]
+                ("ramp_iter", C.c_int32), ("res_diter", C.c_int32), ("minf", C.c_double)]
 
 
 _LIBS: dict = {}
@@ -78,7 +78,8 @@ def _dp(a: np.ndarray):
 
 
 LIMITERS = {"first-order": 0, "none": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5}
-RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3}
+RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3, "HLLE": 4, "HLLEM": 5, "LLF": 6, "Rusanov": 6,
+           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10}
 
 
 class Oracle:
@@ -88,7 +89,8 @@ class Oracle:
         self.lib = load(omp)
         cfg = orc_config(n_rk=case.n_rk, cfl=case.cfl, time_accurate=int(case.time_accurate),
                          limiter=LIMITERS[case.limiter], riemann=RIEMANN[case.riemann], integration=0,
-                         ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=0, res_diter=1)
+                         ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=0, res_diter=1,
+                         minf=getattr(case, "minf", 0.0))
         self.h = self.lib.orc_create(C.byref(cfg), nthreads)
         self.dims = []
         for nd in case.nodes:
