@@ -73,3 +73,16 @@ def test_ausm_up_requires_minf():
     case = cases.sod(16, riemann="AUSM+-up")
     with pytest.raises(MoseError):
         solver(case)
+
+
+def test_ein91_reference_inputs_bitwise(oracle_mod):
+    """The reference's HLLE case (Ein91, 800 cells) to its final time."""
+    from tests.test_oracle import ein91_case
+    case, _ = ein91_case()
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    while o.time < case.t_end:
+        o.step()
+        s.explicit_step()
+    assert s.time == o.time
+    compare_state(s, o, 1)

@@ -206,3 +206,29 @@ def test_riemann_mirror_symmetry(oracle_mod, riemann):
         o.lib.orc_riemann(o.h, dp(L), dp(R), dp(n.copy()), dp(f1))
         o.lib.orc_riemann(o.h, dp(R.copy()), dp(L.copy()), dp(-n), dp(f2))
         np.testing.assert_allclose(f1, -f2, rtol=1e-11, atol=1e-12)
+
+
+def ein91_case():
+    d = np.load(GOLDEN / "ein91_x8.npz")
+    R = 8314.46 / 28.970418            # test/common/Air
+    cp = 1004.5
+    return Case("ein91", [d["nodes"]], d["bc_rec"], d["bc_data"], [d["prim"]], n_rk=3, cfl=float(d["cfl"]),
+                time_accurate=True, limiter="vanleer", riemann="HLLE", gamma=cp / (cp - R), rgas=R,
+                t_end=float(d["t_end"])), d
+
+
+def test_ein91_reference_case_hlle_passes_reference_check(oracle_mod):
+    """The reference's Ein91 inputs (mesh_x8, ic_x8, bc_x8; its HLLE + van
+    Leer case, CFL 0.9, RK3) meet its verify.py criterion against the exact
+    solution: < 1 % (density, velocity), < 1.5 % (pressure) at cells 80, 160
+    and 240."""
+    case, d = ein91_case()
+    o = oracle_mod.Oracle(case)
+    while o.time < case.t_end:
+        o.step()
+    P = o.get_prim(1)[2, 2, 2:-2]
+    ex = d["exact"]
+    for i in d["probes"]:
+        err = [abs(P[i, 0] - ex[i, 0]) / ex[i, 0] * 100, abs(P[i, 1] - ex[i, 1]) / abs(ex[i, 1] + 1e-10) * 100,
+               abs(P[i, 4] - ex[i, 2]) / ex[i, 2] * 100]
+        assert all(e < t for e, t in zip(err, d["threshold_pct"])), (i, err)
