@@ -492,7 +492,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
                       (ctx->nd == 3 && e.f >= 5 && h.nk < 3);
     if (degenerate && !(e.type == 0 || e.type == 400 || e.type == 406))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "bc type %d on a face of a block thinner than 3 cells", e.type);
-    if (ctx->nd == 2 && e.type == 405 && e.data[4] != 0.0)
+    // (the token 'normal' resolves to atan(0 / ...) = 0 there: 2-D face normals have n_z = 0)
+    if (ctx->nd == 2 && e.type == 405 && e.data[4] != 0.0 && !(e.data[4] >= 0.5 * 1.7976931348623157e308))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
   }
   for (int b = 0; b < nb && ctx->nd == 3; ++b)
@@ -526,6 +527,11 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     }
   }
   ctx->marena = mcur;
+  // 405 records whose direction token is 'normal': their angles follow the
+  // face normal (Compute_Inflow_Direction, Lib_BC_Fluxes_Inflow.f90:479-496)
+  // and are resolved once the device has formed the face metrics
+  struct NormalDir { int pidx, b, f, i, j, k; bool a, be; };
+  std::vector<NormalDir> normal_dirs;
   for (auto& e : ctx->bc) {
     const BlockDesc& d = ctx->desc[e.b - 1];
     const HostBlock& h = ctx->hblk[e.b - 1];
@@ -536,8 +542,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       if (e.type == 405) {
         p.mach = e.data[0]; p.T = e.data[1]; p.p = e.data[2]; p.rel_fac = e.data[5];
         double alpha = e.data[3], beta = e.data[4];
-        if (alpha >= 0.5 * 1.7976931348623157e308 || beta >= 0.5 * 1.7976931348623157e308)
-          return fail(ctx, MOSE_ERR_UNSUPPORTED, "inflow angle 'normal' is not on this path");
+        const bool na = alpha >= 0.5 * 1.7976931348623157e308, nb = beta >= 0.5 * 1.7976931348623157e308;
+        if (na || nb) normal_dirs.push_back(NormalDir{(int)params.size(), e.b - 1, e.f, e.i - 1, e.j - 1, e.k - 1, na, nb});
         p.ca = std::cos(alpha); p.sa = std::sin(alpha); p.cb = std::cos(beta); p.sb = std::sin(beta);
       } else {
         p.pback = e.data[0]; p.rel_fac = e.data[1];
@@ -613,6 +619,40 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     if (rc) return rc;
     rc = poll_device_error(ctx);   // metric failures and index self-checks
     if (rc) return rc;
+  }
+  if (!normal_dirs.empty()) {
+    // the boundary face's normal (nx, ny, nz planes of its direction), then
+    // alpha = atan(N_y / (N_x + 1d-20)), beta = atan(N_z / (N_x + 1d-20)) on
+    // the host, as the reference forms them
+    std::vector<double> nrm(3 * normal_dirs.size());
+    for (size_t q = 0; q < normal_dirs.size(); ++q) {
+      const NormalDir& r = normal_dirs[q];
+      const BlockDesc& d = ctx->desc[r.b];
+      const int dir = (r.f - 1) / 2;
+      const int fi = r.i + (r.f == 2), fj = r.j + (r.f == 4), fk = r.k + (r.f == 6);
+      const long long o = (ctx->nd == 3) ? (long long)(fk + GW) * d.plane + (long long)(fj + GW) * d.px + (fi + GW)
+                                         : (long long)(fj + GW) * d.px + (fi + GW);
+      const double* src = ctx->face.p + 12 * d.mbase + (long long)(4 * dir) * d.vstride + o;
+      CU(cudaMemcpy2DAsync(&nrm[3 * q], sizeof(double), src, d.vstride * sizeof(double), sizeof(double), 3,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CU(cudaStreamSynchronize(ctx->stream));
+    for (size_t q = 0; q < normal_dirs.size(); ++q) {
+      const NormalDir& r = normal_dirs[q];
+      BcParam& p = ctx->hbcp[r.pidx];
+      const double* N = &nrm[3 * q];
+      if (r.a) {
+        const double alpha = std::atan(N[1] / (N[0] + 1e-20));
+        p.ca = std::cos(alpha); p.sa = std::sin(alpha);
+      }
+      if (r.be) {
+        const double beta = std::atan(N[2] / (N[0] + 1e-20));
+        p.cb = std::cos(beta); p.sb = std::sin(beta);
+      }
+    }
+    CU(cudaMemcpyAsync(ctx->bcp.p, ctx->hbcp.data(), ctx->hbcp.size() * sizeof(BcParam), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    CU(cudaStreamSynchronize(ctx->stream));
   }
   // uniformity
   DevBuf<int> flags;

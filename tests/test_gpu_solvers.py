@@ -86,3 +86,20 @@ def test_ein91_reference_inputs_bitwise(oracle_mod):
         s.explicit_step()
     assert s.time == o.time
     compare_state(s, o, 1)
+
+
+def test_inflow_direction_normal_bitwise(oracle_mod):
+    """A 405 inflow whose angles are the token 'normal' (the largest double
+    after parse_dir_tok) takes its direction from each face normal
+    (Compute_Inflow_Direction); on the curvilinear channel the normals vary
+    along the inflow face."""
+    case = cases.curvilinear_channel(24, steps=1)
+    inflow = case.bc_rec[:, 5] == 405
+    case.bc_data[inflow, 3] = np.finfo(np.float64).max
+    case.bc_data[inflow, 4] = np.finfo(np.float64).max
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(6):
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, 1)
