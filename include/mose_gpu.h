@@ -233,6 +233,13 @@ int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
  * whole Explicit_Step: every RK stage, the boundary fluxes (405 also in the
  * inflow Mach), the ghost fill and the global CFL dt (through its argmin
  * cell). */
+/* irs-beta (Register_Numerics.f90): implicit residual smoothing of every RK
+ * stage's residual when beta > 0 (Lib_IRS.f90, Newstate_Conservative's IRS
+ * branch Lib_Newstate.f90:40-72); 0 (the default) disables it.  Call before
+ * mose_gpu_setup.  2-D, exact precision: the stage's residual-only kernel,
+ * then the smoothing kernels, then the update. */
+int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta);
+
 /* riemann-options-Minf (Register_Numerics.f90:72), the reference Mach number
  * of AUSM+-up and AUSM+-up2; call before mose_gpu_setup.  Setup rejects
  * those two solvers while it is 0, as Assign_Setup.f90:96-100 does.  2-D

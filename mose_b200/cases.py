@@ -42,6 +42,7 @@ class Case:
     limiter: str = "minmod"
     riemann: str = "HLLC"
     minf: float = 0.0          # riemann-options-Minf (AUSM+-up, AUSM+-up2)
+    irs_beta: float = 0.0      # irs-beta: implicit residual smoothing when > 0
     gamma: float = 1.4
     rgas: float = 1.0
     steps: int = 1

@@ -92,6 +92,14 @@ struct BcParam {
   double pback;
 };
 
+// One first-layer ghost value of the residual for implicit residual
+// smoothing (Ghost_Residual_Extrapolation, Lib_IRS.f90:130-187): arena
+// offsets of the ghost cell and of its source cell, and their blocks'
+// variable strides.
+struct IrsCopy {
+  long long dst, src, vsd, vss;
+};
+
 // One ghost-fill record (Lib_Ghost.f90 dispatch), 0-based cells.
 struct GhostRec {
   int type;                 // BcCode of the face

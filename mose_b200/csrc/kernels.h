@@ -28,6 +28,14 @@ void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, dou
                           cudaStream_t s);
 void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time, double dt_start,
                          int* iter, cudaStream_t s);
+// Implicit residual smoothing (2-D, conservative integration).
+void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, double* R, MetricArgs m, const double* dtl,
+                      const double* dtg, int use_dtg, cudaStream_t s);
+void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s);
+void launch_irs_jacobi(const BlockDesc* dblk, int nblk, long long maxcell, const double* R, const double* Rs,
+                       double* out, int dir, double beta, cudaStream_t s);
+void launch_irs_update(const BlockDesc* dblk, int nblk, long long maxcell, const double* Pin, const double* PO,
+                       const double* R, double* Pout, Gas g, double c, DevError* err, cudaStream_t s);
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
                      cudaStream_t s);

@@ -503,6 +503,85 @@ __global__ void k_rk_stage(const BlockDesc* blk, double* P, const double* PO, co
 }
 
 // ---------------------------------------------------------------------------
+// Implicit residual smoothing on 2-D blocks (Newstate_Conservative with IRS,
+// Lib_Newstate.f90:40-72, and Lib_IRS.f90), in the reference's arithmetic:
+// scale R to the conservative increment, then per direction the first ghost
+// layer of R and two Jacobi sweeps, then the RK stage on the smoothed
+// increment.
+// ---------------------------------------------------------------------------
+// Scale_Residual_Cons :98-103 (strangcoeff = 1): R = -(R / vol * dt)
+__global__ void k_irs_scale(const BlockDesc* blk, double* R, MetricArgs m, const double* dtl, const double* dtg,
+                            int use_dtg) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
+    const long long o = cell_off2(d, i, j);
+    const double vol = m.vol[d.mbase + o];
+    const double dt = use_dtg ? *dtg : dtl[d.mbase + o];
+    for (int v = 0; v < 4; ++v) {
+      double* r = R + d.sbase + v * vs + o;
+      *r = -(*r / vol * dt);
+    }
+  }
+}
+// Ghost_Residual_Extrapolation :130-187: 101 copies the source cell, every
+// other record its own boundary cell (ghost and source cells are disjoint)
+__global__ void k_irs_ghost(const IrsCopy* list, int n, double* R) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const IrsCopy e = list[q];
+  for (int v = 0; v < 4; ++v) R[e.dst + v * e.vsd] = R[e.src + v * e.vss];
+}
+// One Jacobi sweep along dir (Residual_Smoothing_Blk :64-80):
+// out = (R + beta (Rs(-1) + Rs(+1))) / (1 + 2 beta).  out may be R itself:
+// each cell reads its own R before writing it, neighbours come from Rs.
+__global__ void k_irs_jacobi(const BlockDesc* blk, const double* R, const double* Rs, double* out, int dir,
+                             double beta) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  const long long step = dir == 0 ? 1 : d.px;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
+    const long long o = d.sbase + cell_off2(d, i, j);
+    for (int v = 0; v < 4; ++v) {
+      const long long ov = o + v * vs;
+      const double r = R[ov];
+      out[ov] = (r + beta * (Rs[ov - step] + Rs[ov + step])) / (1.0 + 2.0 * beta);
+    }
+  }
+}
+// Update_State_Cons_IRS :106-131: RK_stage on the smoothed increment, then
+// cons2prim and Check_And_Fix_State.  Pout may be Pin (the phase path).
+__global__ void k_irs_update(const BlockDesc* blk, const double* Pin, const double* PO, const double* R, double* Pout,
+                             Gas g, double c, DevError* err) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
+    const long long o = d.sbase + cell_off2(d, i, j);
+    double Q[4], QO[4], U[4], U0[4];
+    for (int v = 0; v < 4; ++v) { Q[v] = Pin[o + v * vs]; QO[v] = PO[o + v * vs]; }
+    ex::prim2cons<4>(g, QO, U0);
+    ex::prim2cons<4>(g, Q, U);
+    for (int v = 0; v < 4; ++v) {
+      const double r_ = (U[v] - U0[v] + R[o + v * vs]) * c;
+      U[v] = U0[v] + r_;
+    }
+    ex::cons2prim<4>(g, U, Q);
+    bool bad = false;
+    for (int v = 0; v < 4; ++v) bad |= isnan(Q[v]);
+    bad |= (Q[3] < 0.0);
+    if (bad) report(err, 5, b, i, j, 0);
+    if (Q[0] < 1e-20) Q[0] = 1e-20;
+    for (int v = 0; v < 4; ++v) Pout[o + v * vs] = Q[v];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Compute_Residual (Mod_Diagnostic.f90:13-50): per-CTA partial sums of
 // (|d rho|, |du|, |dv|, |dw|, |dp|)^2, reduced in a fixed order afterwards.
 // ---------------------------------------------------------------------------
@@ -719,6 +798,24 @@ void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double*
     if (uniform) k_rk_stage<4, true><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
     else k_rk_stage<4, false><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
   }
+}
+void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, double* R, MetricArgs m, const double* dtl,
+                      const double* dtg, int use_dtg, cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
+  k_irs_scale<<<grid, 256, 0, s>>>(dblk, R, m, dtl, dtg, use_dtg);
+}
+void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s) {
+  if (n > 0) k_irs_ghost<<<(n + 255) / 256, 256, 0, s>>>(list, n, R);
+}
+void launch_irs_jacobi(const BlockDesc* dblk, int nblk, long long maxcell, const double* R, const double* Rs,
+                       double* out, int dir, double beta, cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
+  k_irs_jacobi<<<grid, 256, 0, s>>>(dblk, R, Rs, out, dir, beta);
+}
+void launch_irs_update(const BlockDesc* dblk, int nblk, long long maxcell, const double* Pin, const double* PO,
+                       const double* R, double* Pout, Gas g, double c, DevError* err, cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
+  k_irs_update<<<grid, 256, 0, s>>>(dblk, Pin, PO, R, Pout, g, c, err);
 }
 int norms_partial_count(int nblk, long long maxcell) { return grid_for(maxcell, 256, 148 * 4) * nblk; }
 void launch_residual_norms(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, const double* PO,

@@ -169,6 +169,12 @@ struct mose_gpu_ctx {
   DevBuf<BcParam> bcp;
   DevBuf<GhostRec> ghosts;
   DevBuf<int4> items;
+  // implicit residual smoothing (irs-beta > 0): first-layer ghost records of
+  // R and two work arenas for the Jacobi sweeps
+  double irs_beta = 0.0;
+  DevBuf<IrsCopy> irs_list;
+  int nirs = 0;
+  DevBuf<double> rs1, rs2;
   DevBuf<int4> items_nb;      // 2-D items with no physical boundary face
   int nitems_nb = 0;
   DevBuf<int4> items3[3];     // 3-D sweeps
@@ -460,6 +466,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if ((ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP || ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP2) &&
       !(ctx->gas.minf > 0.0))
     return fail(ctx, MOSE_ERR_INVALID, "AUSM+-up solver selected: Minf must be set (mose_gpu_set_riemann_minf)");
+  if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT))
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");
   if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: HLLC or AUSM+ with minmod, van Leer or van Albada");
   auto nodeh = [&](const HostBlock& h, int i, int j, int k, int c) {
@@ -706,6 +714,32 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
   if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
 
+  // ---- implicit residual smoothing: first-layer ghost records of R ----------------
+  if (ctx->irs_beta > 0.0) {
+    static const int inward[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};   // guide(face, 1:2), faces 1..4
+    std::vector<IrsCopy> il;
+    for (auto& e : ctx->bc) {
+      if (e.f > 4) continue;                      // 2-D: no ghost layer across k
+      const BlockDesc& d = ctx->desc[e.b - 1];
+      const int ig = e.i - 1 - inward[e.f - 1][0], jg = e.j - 1 - inward[e.f - 1][1];
+      const bool conn = e.type == 101;            // 201 takes the zero-gradient branch (Lib_IRS.f90:172-183)
+      const BlockDesc& sd = ctx->desc[conn ? e.bs - 1 : e.b - 1];
+      const int is = conn ? e.is - 1 : e.i - 1, js = conn ? e.js - 1 : e.j - 1;
+      IrsCopy c;
+      c.dst = d.sbase + (long long)(jg + GW) * d.px + (ig + GW);
+      c.src = sd.sbase + (long long)(js + GW) * sd.px + (is + GW);
+      c.vsd = d.vstride;
+      c.vss = sd.vstride;
+      il.push_back(c);
+    }
+    ctx->nirs = (int)il.size();
+    CU(ctx->irs_list.alloc(std::max<size_t>(il.size(), 1)));
+    if (!il.empty())
+      CU(cudaMemcpyAsync(ctx->irs_list.p, il.data(), il.size() * sizeof(IrsCopy), cudaMemcpyHostToDevice, ctx->stream));
+    if (ctx->rs1.alloc((size_t)ctx->nv * mcur) != cudaSuccess || ctx->rs2.alloc((size_t)ctx->nv * mcur) != cudaSuccess)
+      return fail(ctx, MOSE_ERR_CUDA, "out of device memory (residual smoothing)");
+  }
+
   // ---- work items for the stage kernel -----------------------------------------
   std::vector<int4> all = plan_stage_items(ctx->hblk, 3 * ctx->nsm);
   // an item runs the boundary-free kernel when every block-edge face its
@@ -934,12 +968,27 @@ int mose_gpu_residual(mose_gpu_ctx* ctx) {
   return check_launch(ctx, "residual");
 }
 
+static int enqueue_irs_smoothing(mose_gpu_ctx* ctx);
+
 int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (irk < 1 || irk > ctx->cfg.n_rk) return fail(ctx, MOSE_ERR_INVALID, "irk out of range");
   static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
   ctx->dt_valid = false;
+  if (ctx->irs_beta > 0.0) {
+    // RK_Newstate with IRS on the residual of mose_gpu_residual, dt from
+    // dtlocal (Compute_dt / Set_Global_dt of the phase path)
+    const int nb = (int)ctx->hblk.size();
+    launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->scal.p, 0,
+                     ctx->stream);
+    ctx->launches += 1 + enqueue_irs_smoothing(ctx);
+    launch_irs_update(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[ctx->cur].p, ctx->state[ctx->po].p, ctx->resid.p,
+                      ctx->state[ctx->cur].p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->derr.p,
+                      ctx->stream);
+    ctx->launches++;
+    return check_launch(ctx, "rk_stage");
+  }
   launch_rk_stage(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->state[ctx->po].p,
                   ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->nd,
                   ctx->uniform, ctx->derr.p, ctx->stream);
@@ -951,7 +1000,7 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
 // the last RK stage, which holds the new state anyway.  With local time
 // stepping each step keeps its standalone pass, so dtlocal always holds the
 // dt of the step that used it, as in the reference.
-static bool fused_dt(const mose_gpu_ctx* ctx) { return ctx->cfg.time_accurate != 0; }
+static bool fused_dt(const mose_gpu_ctx* ctx) { return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0; }
 static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
   a.dtmin = ctx->dtmin.p;
   a.cfl = ctx->cfg.cfl;
@@ -975,6 +1024,42 @@ static int enqueue_dt_pass(mose_gpu_ctx* ctx, int s0) {
 // stage): publish dtglobal and advance time, then the RK stages; the last
 // stage folds in the CFL minimum of the new state for the next step.
 // Returns the number of kernels enqueued.
+// Residual_Smoothing (Lib_IRS.f90:14-39) of the scaled residual in ctx->resid:
+// per direction the first ghost layer, then two Jacobi sweeps (the second
+// writes R).  Returns the kernel count.
+static int enqueue_irs_smoothing(mose_gpu_ctx* ctx) {
+  const size_t bytes = (size_t)ctx->nv * ctx->marena * sizeof(double);
+  const int nb = (int)ctx->hblk.size();
+  int k = 0;
+  for (int dir = 0; dir < ctx->ndir; ++dir) {
+    launch_irs_ghost(ctx->irs_list.p, ctx->nirs, ctx->resid.p, ctx->stream);
+    cudaMemcpyAsync(ctx->rs1.p, ctx->resid.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    cudaMemcpyAsync(ctx->rs2.p, ctx->resid.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    launch_irs_jacobi(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->rs1.p, ctx->rs2.p, dir, ctx->irs_beta,
+                      ctx->stream);
+    launch_irs_jacobi(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->rs2.p, ctx->resid.p, dir, ctx->irs_beta,
+                      ctx->stream);
+    k += (ctx->nirs > 0) + 2;
+  }
+  return k;
+}
+
+// One RK stage with implicit residual smoothing (Newstate_Conservative with
+// IRS, Lib_Newstate.f90:40-72): the residual-only stage kernel into
+// ctx->resid, Scale_Residual_Cons, the smoothing, Update_State_Cons_IRS from
+// arena pc (PO = arena s0) into arena pn.
+static int enqueue_irs_stage(mose_gpu_ctx* ctx, int pc, int s0, int pn, int irk) {
+  StageArgs a = stage_args(ctx, pc, s0, -1, irk);
+  int k = launch_stage(ctx, a, 1, MOSE_PRECISION_FP64_EXACT, false);
+  const int nb = (int)ctx->hblk.size();
+  launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->scal.p,
+                   ctx->cfg.time_accurate, ctx->stream);
+  k += 1 + enqueue_irs_smoothing(ctx);
+  launch_irs_update(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[pc].p, ctx->state[s0].p, ctx->resid.p,
+                    ctx->state[pn].p, ctx->gas, a.c_rk, ctx->derr.p, ctx->stream);
+  return k + 1;
+}
+
 static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
   int k = 0;
   if (!fused_dt(ctx)) k += enqueue_dt_pass(ctx, s0);
@@ -986,9 +1071,13 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
     launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
                        ctx->stream);
     if (ctx->nghost) ++k;
-    StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-    if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
-    k += launch_stage(ctx, a, a.dtmin ? 2 : 0, ctx->cfg.precision, ctx->uniform);
+    if (ctx->irs_beta > 0.0) {
+      k += enqueue_irs_stage(ctx, pc, s0, pn, irk);
+    } else {
+      StageArgs a = stage_args(ctx, pc, s0, pn, irk);
+      if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
+      k += launch_stage(ctx, a, a.dtmin ? 2 : 0, ctx->cfg.precision, ctx->uniform);
+    }
     pc = pn;
   }
   return k;
@@ -1405,6 +1494,14 @@ static int adj_graphs(mose_gpu_ctx* ctx, int K) {
     cudaGraphDestroy(g);
   }
   ctx->adj_graph_K = K;
+  return MOSE_OK;
+}
+
+int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_irs_beta: call before mose_gpu_setup");
+  if (!(beta >= 0.0)) return fail(ctx, MOSE_ERR_INVALID, "set_irs_beta: beta must be >= 0");
+  ctx->irs_beta = beta;
   return MOSE_OK;
 }
 

@@ -199,8 +199,8 @@ def read_input_ini(path) -> dict:
     unsupported = []
     if rec.upper().endswith("-SD"):
         unsupported.append(f"space-reconstruction = {rec} (shock-detector limiting)")
-    if float(num.get("irs-beta", 0) or 0) > 0:
-        unsupported.append("implicit residual smoothing (irs-beta)")
+    if "irs-beta" in num:
+        kw["irs_beta"] = float(num["irs-beta"])
     kw["unsupported"] = unsupported
     return kw
 
@@ -228,6 +228,6 @@ def load_case(case_dir, resolution: str = "", gamma: float | None = None, rgas: 
         unsupported.append(f"riemann-solver = {kw['riemann']}")
     case = Case(d.name + sfx, nodes, rec, data, prim, gamma=gamma, rgas=rgas,
                 **{k: v for k, v in kw.items() if k in ("cfl", "n_rk", "time_accurate", "riemann", "minf", "limiter",
-                                                        "t_end", "steps")})
+                                                        "t_end", "steps", "irs_beta")})
     case.extra["unsupported"] = unsupported
     return case

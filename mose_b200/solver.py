@@ -68,6 +68,8 @@ class Solver:
         self.case = case
         if getattr(case, "minf", 0.0):
             self._check(self.lib.mose_gpu_set_riemann_minf(self.h, float(case.minf)))
+        if getattr(case, "irs_beta", 0.0):
+            self._check(self.lib.mose_gpu_set_irs_beta(self.h, float(case.irs_beta)))
         self.dims = []
         for b, nd in enumerate(case.nodes, start=1):
             nk, nj, ni = nd.shape[0] - 1, nd.shape[1] - 1, nd.shape[2] - 1

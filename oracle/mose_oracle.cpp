@@ -1653,6 +1653,47 @@ int orc_bc_fluxes(orc_domain* d) {
   return d->err;
 }
 
+// Residual_Smoothing, Lib_IRS.f90:14-39: per direction, the residual's first
+// ghost layer (Ghost_Residual_Extrapolation :130-187: 101 copies the source
+// cell, every other type the boundary cell), then per block two Jacobi
+// sweeps of R* = R + beta (R*(-1) - 2 R* + R*(+1)) along that direction
+// (Residual_Smoothing_Blk :42-103).
+static void residual_smoothing(orc_domain* d, double beta) {
+  const int njacobi = 2;
+  for (int dir = 1; dir <= d->ndir; ++dir) {
+    for (const BCrec& e : d->bc) {
+      Block& B = d->blk[e.b - 1];
+      int ig = e.i - G(e.f, 1), jg = e.j - G(e.f, 2), kg = e.k - G(e.f, 3);
+      const double* src = (e.type == 101) ? d->blk[e.bs - 1].Rc(e.is, e.js, e.ks) : B.Rc(e.i, e.j, e.k);
+      double* dst = B.Rc(ig, jg, kg);
+      for (int v = 0; v < NPRIM; ++v) dst[v] = src[v];
+    }
+    const int di = dir == 1, dj = dir == 2, dk = dir == 3;
+    for (Block& B : d->blk) {
+      std::vector<double> Rs(B.R), Rsn(B.R.size());
+      for (int it = 1; it <= njacobi; ++it) {
+        for (int k = 1; k <= B.nk; ++k)
+          for (int j = 1; j <= B.nj; ++j)
+            for (int i = 1; i <= B.ni; ++i) {
+              const double* r = B.Rc(i, j, k);
+              const double* rm = &Rs[NPRIM * B.cell(i - di, j - dj, k - dk)];
+              const double* rp = &Rs[NPRIM * B.cell(i + di, j + dj, k + dk)];
+              double* o = &Rsn[NPRIM * B.cell(i, j, k)];
+              for (int v = 0; v < NPRIM; ++v) o[v] = (r[v] + beta * (rm[v] + rp[v])) / (1.0 + 2.0 * beta);
+            }
+        for (int k = 1; k <= B.nk; ++k)
+          for (int j = 1; j <= B.nj; ++j)
+            for (int i = 1; i <= B.ni; ++i)
+              for (int v = 0; v < NPRIM; ++v) Rs[NPRIM * B.cell(i, j, k) + v] = Rsn[NPRIM * B.cell(i, j, k) + v];
+      }
+      for (int k = 1; k <= B.nk; ++k)
+        for (int j = 1; j <= B.nj; ++j)
+          for (int i = 1; i <= B.ni; ++i)
+            for (int v = 0; v < NPRIM; ++v) B.Rc(i, j, k)[v] = Rs[NPRIM * B.cell(i, j, k) + v];
+    }
+  }
+}
+
 // RK_Newstate => Newstate_Conservative / Newstate_Primitive, Lib_Newstate.f90
 int orc_rk_newstate(orc_domain* d, int irk) {
   static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};  // Lib_RK.f90:8-11
@@ -1661,6 +1702,43 @@ int orc_rk_newstate(orc_domain* d, int irk) {
   const double strangcoeff = 1.0;
   const Thermo& t = d->th;
   const bool prim_mode = d->cfg.integration == ORC_INT_PRIM;
+  if (d->cfg.irs_beta > 0.0 && !prim_mode) {
+    // Newstate_Conservative with IRS, Lib_Newstate.f90:40-72: scale every
+    // residual (Scale_Residual_Cons), smooth, then Update_State_Cons_IRS
+    for (Block& B : d->blk)
+      for (int k = 1; k <= B.nk; ++k)
+        for (int j = 1; j <= B.nj; ++j)
+          for (int i = 1; i <= B.ni; ++i) {
+            double* res = B.Rc(i, j, k);
+            double dt = B.dtlocal[B.inner(i, j, k)];
+            double volume = B.vol_(i, j, k);
+            for (int v = 0; v < NPRIM; ++v) res[v] = -(res[v] / volume * dt * strangcoeff);
+          }
+    residual_smoothing(d, d->cfg.irs_beta);
+    for (int bi = 0; bi < (int)d->blk.size(); ++bi) {
+      Block& B = d->blk[bi];
+      for (int k = 1; k <= B.nk; ++k)
+        for (int j = 1; j <= B.nj; ++j)
+          for (int i = 1; i <= B.ni; ++i) {
+            double* prim = B.Pc(i, j, k);
+            const double* primold = B.POc(i, j, k);
+            const double* res = B.Rc(i, j, k);
+            double consold[NPRIM], cons[NPRIM];
+            prim2cons(t, primold, consold);
+            prim2cons(t, prim, cons);
+            for (int v = 0; v < NPRIM; ++v) {
+              double r_ = (cons[v] - consold[v] + res[v]) * c;
+              cons[v] = consold[v] + r_;
+            }
+            cons2prim(t, cons, prim);
+            bool nan = false;
+            for (int v = 0; v < NPRIM; ++v) nan |= std::isnan(prim[v]);
+            if (nan || prim[NP] < 0.0) d->fail(ORC_ERR_NAN_OR_NEG_P, bi + 1, i, j, k);
+            if (prim[0] < 1e-20) prim[0] = 1e-20;
+          }
+    }
+    return d->err;
+  }
   for (int bi = 0; bi < (int)d->blk.size(); ++bi) {
     Block& B = d->blk[bi];
 #ifdef _OPENMP

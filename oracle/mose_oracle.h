@@ -48,6 +48,7 @@ typedef struct orc_config {
   int32_t ramp_iter;     /* cfl-rise-threshold */
   int32_t res_diter;     /* residual output interval */
   double minf;           /* riemann-options-Minf (AUSM+-up, AUSM+-up2) */
+  double irs_beta;       /* irs-beta: implicit residual smoothing when > 0 */
 } orc_config;
 
 /* Error codes: mirror the reference's fatal `stop` sites. */

@@ -20,7 +20,8 @@ class orc_config(C.Structure):
     _fields_ = [("n_rk", C.c_int32), ("cfl", C.c_double), ("time_accurate", C.c_int32),
                 ("limiter", C.c_int32), ("riemann", C.c_int32), ("integration", C.c_int32),
                 ("ndir", C.c_int32), ("gamma", C.c_double), ("rgas", C.c_double),
-                ("ramp_iter", C.c_int32), ("res_diter", C.c_int32), ("minf", C.c_double)]
+                ("ramp_iter", C.c_int32), ("res_diter", C.c_int32), ("minf", C.c_double),
+                ("irs_beta", C.c_double)]
 
 
 _LIBS: dict = {}
@@ -90,7 +91,7 @@ class Oracle:
         cfg = orc_config(n_rk=case.n_rk, cfl=case.cfl, time_accurate=int(case.time_accurate),
                          limiter=LIMITERS[case.limiter], riemann=RIEMANN[case.riemann], integration=0,
                          ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=0, res_diter=1,
-                         minf=getattr(case, "minf", 0.0))
+                         minf=getattr(case, "minf", 0.0), irs_beta=getattr(case, "irs_beta", 0.0))
         self.h = self.lib.orc_create(C.byref(cfg), nthreads)
         self.dims = []
         for nd in case.nodes:

@@ -232,3 +232,64 @@ def test_ein91_reference_case_hlle_passes_reference_check(oracle_mod):
         err = [abs(P[i, 0] - ex[i, 0]) / ex[i, 0] * 100, abs(P[i, 1] - ex[i, 1]) / abs(ex[i, 1] + 1e-10) * 100,
                abs(P[i, 4] - ex[i, 2]) / ex[i, 2] * 100]
         assert all(e < t for e, t in zip(err, d["threshold_pct"])), (i, err)
+
+
+def test_irs_stage_matches_numpy_restatement(oracle_mod):
+    """The oracle's RK stage with implicit residual smoothing equals a numpy
+    restatement of Lib_Newstate.f90:40-72 and Lib_IRS.f90 (scale, per
+    direction the first ghost layer and two Jacobi sweeps, then the RK
+    stage) applied to the oracle's own residual, on a two-block case with
+    connection (101) and extrapolation (400) faces."""
+    case = cases.four_quadrant(seed=4, nbx=2, nby=1, nmin=9, nmax=14, steps=1, limiter="minmod", riemann="HLLE",
+                               cfl=0.4)
+    case.irs_beta = 0.6
+    case.time_accurate = False
+    o = oracle_mod.Oracle(case)
+    o.compute_dt()
+    o.copy_state()
+    o.fill_ghost_cell()
+    o.fluxes()
+    o.bc_fluxes()
+    P0 = [o.get_prim(b).copy() for b in (1, 2)]
+    R = [o.get_residual(b).copy() for b in (1, 2)]          # (nk+4, nj+4, ni+4, 5)
+    dt = [o.get_dtlocal(b) for b in (1, 2)]
+    vol = [o.get_metrics(b)[0] for b in (1, 2)]
+    g2 = slice(2, -2)
+    for b in range(2):
+        R[b][g2, g2, g2] = -(R[b][g2, g2, g2] / vol[b][g2, g2, g2][..., None] * dt[b][..., None] * 1.0)
+    beta = case.irs_beta
+    rec = case.bc_rec
+    inward = {1: (1, 0), 2: (-1, 0), 3: (0, 1), 4: (0, -1)}
+    for d in range(2):
+        for r in rec:
+            b, i, j, f, t = r[0] - 1, r[1], r[2], r[4], r[5]
+            if f > 4:
+                continue
+            gi, gj = i - inward[f][0], j - inward[f][1]
+            src = R[r[6] - 1][2, r[8] + 1, r[7] + 1] if t == 101 else R[b][2, j + 1, i + 1]
+            R[b][2, gj + 1, gi + 1] = src
+        for b in range(2):
+            Rs = R[b].copy()
+            for _ in range(2):
+                Rsn = Rs.copy()
+                for k in (2,):
+                    if d == 0:
+                        Rsn[k, g2, g2] = (R[b][k, g2, g2] + beta * (Rs[k, g2, 1:-3] + Rs[k, g2, 3:-1])) / (1.0 + 2.0 * beta)
+                    else:
+                        Rsn[k, g2, g2] = (R[b][k, g2, g2] + beta * (Rs[k, 1:-3, g2] + Rs[k, 3:-1, g2])) / (1.0 + 2.0 * beta)
+                Rs[:, g2, g2] = Rsn[:, g2, g2]
+            R[b][:, g2, g2] = Rs[:, g2, g2]
+    o.rk_newstate(1)
+    gam, Rg = case.gamma, case.rgas
+    cv = Rg / (gam - 1.0)
+    for b in range(2):
+        p = P0[b][2, g2, g2]
+        rho, u, v, w, pr = (p[..., q] for q in range(5))
+        T = pr / (rho * Rg)
+        U = np.stack([rho, rho * u, rho * v, rho * w, rho * (cv * T + 0.5 * (u * u + v * v + w * w))], -1)
+        U = U + (U - U + R[b][2, g2, g2]) * 1.0
+        rho = U[..., 0]
+        u, v, w = U[..., 1] / rho, U[..., 2] / rho, U[..., 3] / rho
+        e = U[..., 4] / rho - 0.5 * (u * u + v * v + w * w)
+        want = np.stack([rho, u, v, w, rho * Rg * (e / cv)], -1)
+        np.testing.assert_allclose(o.get_prim(b + 1)[2, g2, g2], want, rtol=1e-13, atol=1e-14)

@@ -80,7 +80,7 @@ def test_unsupported_numerics_reported(tmp_path):
     ini = tmp_path / "input.ini"
     ini.write_text("[MOSE-Numerics]\nspace-reconstruction = MUSCL-SD\nirs-beta = 0.5\nflux-limiter = mc\n")
     kw = refio.read_input_ini(ini)
-    assert len(kw["unsupported"]) == 2
+    assert len(kw["unsupported"]) == 1 and kw["irs_beta"] == 0.5
 
 
 @pytest.mark.skipif(not REF.exists(), reason="reference tree not present")
