@@ -72,7 +72,9 @@ enum {
   MOSE_RIEMANN_PLLF = 7,       /* 'PLLF'  (Lib_Riemann_LF.f90:48-102) */
   MOSE_RIEMANN_HANEL = 8,      /* 'Hanel' (Lib_Riemann_AUSM.f90:48-117) */
   MOSE_RIEMANN_AUSMP_UP = 9,   /* 'AUSM+-up'  (Lib_Riemann_AUSM.f90:273-418), needs Minf */
-  MOSE_RIEMANN_AUSMP_UP2 = 10  /* 'AUSM+-up2' (Lib_Riemann_AUSM.f90:455-570), needs Minf */
+  MOSE_RIEMANN_AUSMP_UP2 = 10, /* 'AUSM+-up2' (Lib_Riemann_AUSM.f90:455-570), needs Minf */
+  MOSE_RIEMANN_HLLC_SD = 11,   /* 'HLLC+'  (Lib_Riemann_HLL.f90:500-534), shock detector */
+  MOSE_RIEMANN_HLLE_PP = 12    /* 'HLLE++' (Lib_Riemann_HLL.f90:320-464), shock detector */
 };
 
 /* Arithmetic of the face sweeps and of the fused steps' CFL pass.  In the
@@ -233,6 +235,12 @@ int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
  * whole Explicit_Step: every RK stage, the boundary fluxes (405 also in the
  * inflow Mach), the ghost fill and the global CFL dt (through its argmin
  * cell). */
+/* space-reconstruction = MUSCL-SD (Mod_Space.f90:26-31): the limited slopes of
+ * every face scaled by the Tramel shock detector (Lib_Shock_Detector.f90,
+ * Lib_Reconstruction.f90:24-25).  The detector also feeds HLLC+ and HLLE++.
+ * Call before mose_gpu_setup; 2-D blocks of at least 3 x 3 cells. */
+int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on);
+
 /* irs-beta (Register_Numerics.f90): implicit residual smoothing of every RK
  * stage's residual when beta > 0 (Lib_IRS.f90, Newstate_Conservative's IRS
  * branch Lib_Newstate.f90:40-72); 0 (the default) disables it.  Call before

@@ -26,7 +26,7 @@ NPRIM = 5
 # limiter / riemann names as in input.ini (Register_Numerics.f90:57-72)
 LIMITERS = {"first-order": 0, "none": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5}
 RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3, "HLLE": 4, "HLLEM": 5, "LLF": 6, "Rusanov": 6,
-           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10}
+           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10, "HLLC+": 11, "HLLE++": 12}
 
 
 @dataclass
@@ -43,6 +43,8 @@ class Case:
     riemann: str = "HLLC"
     minf: float = 0.0          # riemann-options-Minf (AUSM+-up, AUSM+-up2)
     irs_beta: float = 0.0      # irs-beta: implicit residual smoothing when > 0
+    sd_limiter: bool = False   # space-reconstruction MUSCL-SD (shock-detector scaled slopes)
+    ramp_iter: int = 0         # cfl-rise-threshold: CFL ramped over the first iterations
     gamma: float = 1.4
     rgas: float = 1.0
     steps: int = 1

@@ -53,6 +53,9 @@ struct Gas {
   // solver at run time, and riemann-options-Minf of AUSM+-up / AUSM+-up2
   int rie;
   double minf;
+  // shock detector (SD_Tramel): bit 0 scales the limited slopes (MUSCL-SD),
+  // bit 1 feeds the SD Riemann solvers (HLLC+, HLLE++)
+  int sd;
 };
 
 // Per-block descriptor (device resident).

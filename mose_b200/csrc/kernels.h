@@ -20,7 +20,7 @@ void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, d
                         DevError* err, cudaStream_t s);
 void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,
                        double* dtl, unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
-                       int ramp_iter, int store_local, bool uniform, cudaStream_t s);
+                       int ramp_iter, int store_local, bool uniform, cudaStream_t s, const int* iterp = nullptr);
 void launch_set_global_dt(const BlockDesc* dblk, int nblk, long long maxcell, double* dtl, const double* dtg, int nd,
                           cudaStream_t s);
 void launch_step_begin(unsigned long long* dtmin_bits, double dt_start, int* iter, cudaStream_t s);
@@ -92,8 +92,9 @@ MOSE_STAGE_DECL(2, 0) MOSE_STAGE_DECL(2, 1) MOSE_STAGE_DECL(2, 2) MOSE_STAGE_DEC
 
 // mode 0: fused residual + RK update; 1: residual only (exact precision);
 // 2: fused, plus the next step's Compute_dt (last RK stage of a fused step).
-// Solvers 4.. (HLLE, HLLEM, LLF, PLLF, Hanel, AUSM+-up, AUSM+-up2) share one
-// unit per precision that selects the solver at run time (Gas::rie).
+// Solvers 4.. (HLLE, HLLEM, LLF, PLLF, Hanel, AUSM+-up, AUSM+-up2, HLLC+,
+// HLLE++) share one unit per precision that selects the solver at run time
+// (Gas::rie); with a shock detector (Gas::sd) every solver runs there.
 inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int prec, int rie, int lim,
                            cudaStream_t s) {
   using L = bool (*)(const StageArgs&, int, int, bool, int, cudaStream_t);
@@ -101,8 +102,9 @@ inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int 
       {launch_stage2d_p0_r0, launch_stage2d_p0_r1, launch_stage2d_p0_r2, launch_stage2d_p0_r3, launch_stage2d_p0_r4},
       {launch_stage2d_p1_r0, launch_stage2d_p1_r1, launch_stage2d_p1_r2, launch_stage2d_p1_r3, launch_stage2d_p1_r4},
       {launch_stage2d_p2_r0, launch_stage2d_p2_r1, launch_stage2d_p2_r2, launch_stage2d_p2_r3, launch_stage2d_p2_r4}};
-  if (prec < 0 || prec > 2 || rie < 0 || rie > 10) return false;
-  return table[prec][rie < 4 ? rie : 4](a, nsm, mode, uni, lim, s);
+  if (prec < 0 || prec > 2 || rie < 0 || rie > 12) return false;
+  // the shock detector lives in the run-time solver unit, which serves every solver
+  return table[prec][(rie < 4 && a.g.sd == 0) ? rie : 4](a, nsm, mode, uni, lim, s);
 }
 
 // 3-D: three directional sweeps per RK stage; HLLC and AUSM+ with minmod,

@@ -390,7 +390,8 @@ __global__ void k_fill_ghosts(const BlockDesc* blk, const GhostRec* recs, int nr
 template <int NV, bool UNI>
 __global__ void k_compute_dt(const BlockDesc* blk, int nblk, const double* P, MetricArgs m, double* dtl,
                              unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
-                             int ramp_iter, int store_local) {
+                             int ramp_iter, int store_local, const int* iterp) {
+  if (iterp) iter = *iterp + 1;   // the fused steps' device counter: completed steps + 1
   // blockIdx.y = block; CTAs stride over the block's cell rows (j, k), threads
   // over the cells of a row, so no per-cell index division
   const int b = blockIdx.y;
@@ -754,15 +755,15 @@ void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, d
 }
 void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,
                        double* dtl, unsigned long long* dtmin_bits, Gas g, double cfl, int ndir, int nd, int iter,
-                       int ramp_iter, int store_local, bool uniform, cudaStream_t s) {
+                       int ramp_iter, int store_local, bool uniform, cudaStream_t s, const int* iterp) {
   // one CTA per cell row (rows <= cells), at most 16 per SM
   dim3 grid((unsigned)std::min<long long>(maxcell, 148 * 16), nblk);
   if (nd == 3) {
-    if (uniform) k_compute_dt<5, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
-    else k_compute_dt<5, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
+    if (uniform) k_compute_dt<5, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local, iterp);
+    else k_compute_dt<5, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local, iterp);
   } else {
-    if (uniform) k_compute_dt<4, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
-    else k_compute_dt<4, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local);
+    if (uniform) k_compute_dt<4, true><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local, iterp);
+    else k_compute_dt<4, false><<<grid, 256, 0, s>>>(dblk, nblk, P, m, dtl, dtmin_bits, g, cfl, ndir, nd, iter, ramp_iter, store_local, iterp);
   }
 }
 void launch_set_global_dt(const BlockDesc* dblk, int nblk, long long maxcell, double* dtl, const double* dtg, int nd,

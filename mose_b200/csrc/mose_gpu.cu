@@ -333,7 +333,7 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   *out = nullptr;
   if (cfg->abi_version != MOSE_GPU_ABI_VERSION) return MOSE_ERR_INVALID;
   if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 || cfg->integration != MOSE_INTEGRATION_CONS ||
-      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > MOSE_RIEMANN_AUSMP_UP2 ||
+      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > MOSE_RIEMANN_HLLE_PP ||
       cfg->precision < 0 || cfg->precision > 2 || !(cfg->gamma > 1.0) || !(cfg->rgas > 0.0))
     return MOSE_ERR_UNSUPPORTED;
   ctx = new mose_gpu_ctx();
@@ -366,6 +366,7 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   ctx->gas.igm1 = 1.0 / (cfg->gamma - 1.0);
   ctx->gas.rie = cfg->riemann;
   ctx->gas.minf = 0.0;
+  ctx->gas.sd = (cfg->riemann == MOSE_RIEMANN_HLLC_SD || cfg->riemann == MOSE_RIEMANN_HLLE_PP) ? 2 : 0;
   *out = ctx;
   return MOSE_OK;
 }
@@ -466,6 +467,13 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if ((ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP || ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP2) &&
       !(ctx->gas.minf > 0.0))
     return fail(ctx, MOSE_ERR_INVALID, "AUSM+-up solver selected: Minf must be set (mose_gpu_set_riemann_minf)");
+  if (ctx->gas.sd) {
+    // the detector reads the four face neighbours of every 2-D cell
+    if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector runs on 2-D domains");
+    for (const auto& h : ctx->hblk)
+      if (h.ni < 3 || h.nj < 3)
+        return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector needs blocks of at least 3 x 3 cells");
+  }
   if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");
   if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
@@ -1000,7 +1008,9 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
 // the last RK stage, which holds the new state anyway.  With local time
 // stepping each step keeps its standalone pass, so dtlocal always holds the
 // dt of the step that used it, as in the reference.
-static bool fused_dt(const mose_gpu_ctx* ctx) { return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0; }
+static bool fused_dt(const mose_gpu_ctx* ctx) {
+  return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0;
+}
 static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
   a.dtmin = ctx->dtmin.p;
   a.cfl = ctx->cfg.cfl;
@@ -1013,9 +1023,11 @@ static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
 // accurate.  Returns the number of kernels enqueued.
 static int enqueue_dt_pass(mose_gpu_ctx* ctx, int s0) {
   launch_step_begin(ctx->dtmin.p, 1e5, nullptr, ctx->stream);
+  // the CFL ramp (cfl-rise-threshold) reads the step's iteration on the
+  // device: the completed steps + 1, as Explicit_Step increments iter first
   launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[s0].p, ctx->margs(), ctx->dtl.p,
-                    ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0, ctx->cfg.time_accurate ? 0 : 1,
-                    ctx->uniform, ctx->stream);
+                    ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, ctx->cfg.ramp_iter,
+                    ctx->cfg.time_accurate ? 0 : 1, ctx->uniform, ctx->stream, ctx->iterdev.p);
   return 2;
 }
 
@@ -1093,8 +1105,8 @@ static int step_final_index(const mose_gpu_ctx* ctx, int s0) {
 int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
   int rc = require_ready(ctx);
   if (rc) return rc;
-  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
   CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   int s0 = ctx->cur;
   if (fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, s0);
   ctx->launches += enqueue_step(ctx, s0);
@@ -1117,8 +1129,8 @@ int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (nsteps < 0) return MOSE_ERR_INVALID;
-  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
   CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   if (nsteps > 0 && fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, ctx->cur);
   for (int n = 0; n < nsteps; ++n) {
     int s0 = ctx->cur;
@@ -1188,9 +1200,9 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!ms || !launches || nsteps < 1) return MOSE_ERR_INVALID;
-  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "cfl ramp in the fused step");
   for (int c = 0; c < 3; ++c) { ms[c] = 0.0; launches[c] = 0; }
   CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   std::vector<cudaEvent_t> ev;
   std::vector<int> cls;
   auto mark = [&](int c) {
@@ -1297,6 +1309,8 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
   if (ctx->cfg.riemann != MOSE_RIEMANN_HLLC || ctx->cfg.limiter < 1 || ctx->cfg.limiter > 3)
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: HLLC with minmod, van Leer or van Albada");
   if (!ctx->cfg.time_accurate) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: time-accurate runs only");
+  if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no cfl ramp");
+  if (ctx->irs_beta > 0.0 || ctx->gas.sd) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no IRS or shock detector");
   const size_t ns = (size_t)ctx->nv * ctx->marena, m = (size_t)ctx->marena;
   for (DevBuf<double>* b : {&ctx->lam, &ctx->lam_loc, &ctx->lam_n, &ctx->lamR, &ctx->wdt, &ctx->lamG})
     if (b->alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
@@ -1494,6 +1508,13 @@ static int adj_graphs(mose_gpu_ctx* ctx, int K) {
     cudaGraphDestroy(g);
   }
   ctx->adj_graph_K = K;
+  return MOSE_OK;
+}
+
+int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on) {
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_sd_limiter: call before mose_gpu_setup");
+  ctx->gas.sd = (ctx->gas.sd & ~1) | (on ? 1 : 0);
   return MOSE_OK;
 }
 

@@ -481,12 +481,122 @@ __device__ __forceinline__ Fl5 ausmpup3(const Gas& g, const St3& L, const St3& R
   return F;
 }
 
+// hartenHyman, Lib_Riemann_HLL.f90:537-547
+__device__ __forceinline__ double harten_hyman(double v, double e) {
+  double al = fabs(v);
+  double l = al;
+  if (al <= e) l = (v * v + e * e) / (2.0 * e);
+  return l;
+}
+// riemann_HLLEpp ('HLLE++'), Lib_Riemann_HLL.f90:320-464
+__device__ __forceinline__ Fl5 hllepp3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz,
+                                       double beta) {
+  Fl5 F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  Roe o = roe3(g, L, R);
+  double un_roe = o.u * nx + o.v * ny + o.w * nz;
+  double Sm = fmin(fmin(0.0, unl - L.a), un_roe - o.a);
+  double Sp = fmax(fmax(0.0, unr + R.a), un_roe + o.a);
+  double inv_denom = 1.0 / (Sp - Sm);
+  double lam1_hlle = fabs((Sp + Sm) * un_roe * inv_denom - 2.0 * Sp * Sm * inv_denom);
+  double lam2_hlle = fabs((Sp + Sm) * (un_roe - o.a) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+  double lam3_hlle = fabs((Sp + Sm) * (un_roe + o.a) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+  double eps = 0.3 * (fabs(un_roe) + o.a);
+  double lam1_roe = fabs(un_roe);
+  double lam2_roe = harten_hyman(un_roe - o.a, eps);
+  double lam3_roe = harten_hyman(un_roe + o.a, eps);
+  double lam1_pp = beta * lam1_roe + (1.0 - beta) * lam1_hlle;
+  double lam2_pp = beta * lam2_roe + (1.0 - beta) * lam2_hlle;
+  double lam3_pp = beta * lam3_roe + (1.0 - beta) * lam3_hlle;
+  Fl5 Fl = phys3(g, L, nx, ny, nz), Fr = phys3(g, R, nx, ny, nz);
+  F.r = 0.5 * (Fl.r + Fr.r);
+  F.u = 0.5 * (Fl.u + Fr.u);
+  F.v = 0.5 * (Fl.v + Fr.v);
+  F.w = 0.5 * (Fl.w + Fr.w);
+  F.E = 0.5 * (Fl.E + Fr.E);
+  double drho = R.r - L.r, dp = R.p - L.p;
+  double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w, dun = unr - unl;
+  double t1x, t1y, t1z;
+  if (fabs(nx) < 0.9) { t1x = 0.0; t1y = -nz; t1z = ny; }
+  else { t1x = -nz; t1y = 0.0; t1z = nx; }
+  double normt = sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+  t1x = t1x / normt; t1y = t1y / normt; t1z = t1z / normt;
+  double t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
+  double alpha_m = (dp - o.rho * o.a * dun) / (2.0 * o.a * o.a);
+  double alpha_c = drho - dp / (o.a * o.a);
+  double alpha_s1 = o.rho * (du * t1x + dv * t1y + dw * t1z);
+  double alpha_s2 = o.rho * (du * t2x + dv * t2y + dw * t2z);
+  double alpha_p = (dp + o.rho * o.a * dun) / (2.0 * o.a * o.a);
+  F.r = F.r - 0.5 * (alpha_c * lam1_pp + alpha_m * lam2_pp + alpha_p * lam3_pp);
+  F.u = F.u - 0.5 * (alpha_c * lam1_pp * o.u);
+  F.v = F.v - 0.5 * (alpha_c * lam1_pp * o.v);
+  F.w = F.w - 0.5 * (alpha_c * lam1_pp * o.w);
+  F.u = F.u - 0.5 * lam1_pp * (alpha_s1 * t1x + alpha_s2 * t2x);
+  F.v = F.v - 0.5 * lam1_pp * (alpha_s1 * t1y + alpha_s2 * t2y);
+  F.w = F.w - 0.5 * lam1_pp * (alpha_s1 * t1z + alpha_s2 * t2z);
+  F.u = F.u - 0.5 * (alpha_m * lam2_pp * (o.u - o.a * nx) + alpha_p * lam3_pp * (o.u + o.a * nx));
+  F.v = F.v - 0.5 * (alpha_m * lam2_pp * (o.v - o.a * ny) + alpha_p * lam3_pp * (o.v + o.a * ny));
+  F.w = F.w - 0.5 * (alpha_m * lam2_pp * (o.w - o.a * nz) + alpha_p * lam3_pp * (o.w + o.a * nz));
+  F.E = F.E - 0.5 * lam1_pp * (alpha_c * 0.5 * (o.u * o.u + o.v * o.v + o.w * o.w));
+  F.E = F.E - 0.5 * lam1_pp * (alpha_s1 * (o.u * t1x + o.v * t1y + o.w * t1z) + alpha_s2 * (o.u * t2x + o.v * t2y + o.w * t2z));
+  F.E = F.E - 0.5 * (alpha_m * lam2_pp * (o.h0 - o.a * un_roe) + alpha_p * lam3_pp * (o.h0 + o.a * un_roe));
+  return F;
+}
+
+// SD_Tramel, Lib_Shock_Detector.f90:9-38 (DELTA = 20) over the face
+// neighbours of a 2-D cell; the k pair of the reference is zero-gradient
+// there (2-D k faces are null) and contributes an exact 0 to the maximum.
+__device__ __forceinline__ double sd_tramel2(double p, double p1, double p2, double p3, double p4) {
+  const double DELTA = 20.0;
+  double kp1 = fabs((p2 - 2.0 * p + p1) / (p2 + 2.0 * p + p1));
+  double kp2 = fabs((p4 - 2.0 * p + p3) / (p4 + 2.0 * p + p3));
+  double sw = fmax(kp1, kp2);
+  if (sw < 1.0 / DELTA) {
+    double phi = fmax(sw / DELTA, 0.0);
+    return 1.0 - tanh(10.0 * phi * phi * phi);
+  }
+  return 0.0;
+}
+
+// Every solver selected at run time by Gas::rie (MOSE_RIEMANN_*); beta is
+// the face's shock detector (1 without one).
 template <int NV>
 __device__ __noinline__ void riemann_rt(const Gas& g, const double* Lq, double aL, const double* Rq, double aR,
-                                        const double* n, double* F) {
+                                        const double* n, double* F, double beta) {
+  switch (g.rie) {
+    case 0: hllc<NV>(g, Lq, aL, Rq, aR, n, F); return;
+    case 1: ausmp<NV>(g, Lq, aL, Rq, aR, n, F); return;
+    case 2: slau<NV>(g, Lq, aL, Rq, aR, n, F, false); return;
+    case 3: slau<NV>(g, Lq, aL, Rq, aR, n, F, true); return;
+    case 11: {   // riemann_HLLCSD ('HLLC+'), Lib_Riemann_HLL.f90:500-534
+      if (beta >= 1.0) { hllc<NV>(g, Lq, aL, Rq, aR, n, F); return; }
+      const St3 L = st3<NV>(Lq, aL), R = st3<NV>(Rq, aR);
+      const Fl5 E = hlle3(g, L, R, n[0], n[1], n[2]);
+      if (beta == 0.0) {
+        F[0] = E.r; F[1] = E.u; F[2] = E.v;
+        if constexpr (NV == 5) { F[3] = E.w; F[4] = E.E; } else F[3] = E.E;
+        return;
+      }
+      double C[NV];
+      hllc<NV>(g, Lq, aL, Rq, aR, n, C);
+      F[0] = beta * C[0] + (1.0 - beta) * E.r;
+      F[1] = beta * C[1] + (1.0 - beta) * E.u;
+      F[2] = beta * C[2] + (1.0 - beta) * E.v;
+      if constexpr (NV == 5) {
+        F[3] = beta * C[3] + (1.0 - beta) * E.w;
+        F[4] = beta * C[4] + (1.0 - beta) * E.E;
+      } else {
+        F[3] = beta * C[3] + (1.0 - beta) * E.E;
+      }
+      return;
+    }
+    default: break;
+  }
   const St3 L = st3<NV>(Lq, aL), R = st3<NV>(Rq, aR);
   Fl5 f;
   switch (g.rie) {
+    case 12: f = hllepp3(g, L, R, n[0], n[1], n[2], beta); break;
     case 4: f = hlle3(g, L, R, n[0], n[1], n[2]); break;
     case 5: f = hllem3(g, L, R, n[0], n[1], n[2]); break;
     case 6: f = llf3(g, L, R, n[0], n[1], n[2]); break;
@@ -502,11 +612,11 @@ __device__ __noinline__ void riemann_rt(const Gas& g, const double* Lq, double a
 
 template <int RIE, int NV>
 __device__ __forceinline__ void riemann(const Gas& g, const double* L, double aL, const double* R,
-                                        double aR, const double* n, double* F) {
+                                        double aR, const double* n, double* F, double beta = 1.0) {
   if constexpr (RIE == 1) ausmp<NV>(g, L, aL, R, aR, n, F);
   else if constexpr (RIE == 2) slau<NV>(g, L, aL, R, aR, n, F, false);
   else if constexpr (RIE == 3) slau<NV>(g, L, aL, R, aR, n, F, true);
-  else if constexpr (RIE == 4) riemann_rt<NV>(g, L, aL, R, aR, n, F);
+  else if constexpr (RIE == 4) riemann_rt<NV>(g, L, aL, R, aR, n, F, beta);
   else hllc<NV>(g, L, aL, R, aR, n, F);
 }
 
@@ -516,12 +626,12 @@ __device__ __forceinline__ void riemann(const Gas& g, const double* L, double aL
 // Returns false when check_gas_state rejects either state.
 template <int RIE, int NV>
 __device__ __forceinline__ bool face_flux(const Gas& g, const double* QL, const double* QR,
-                                          const double* n, double area, double* F) {
+                                          const double* n, double area, double* F, double beta = 1.0) {
   constexpr int P = NV - 1;
   bool ok = (QL[0] > 0.0 && QL[P] > 0.0 && QR[0] > 0.0 && QR[P] > 0.0);
   double aL = sound(g, QL[0], QL[P]);
   double aR = sound(g, QR[0], QR[P]);
-  riemann<RIE, NV>(g, QL, aL, QR, aR, n, F);
+  riemann<RIE, NV>(g, QL, aL, QR, aR, n, F, beta);
   for (int v = 0; v < NV; ++v) F[v] = F[v] * area;
   return ok;
 }

@@ -169,8 +169,8 @@ struct PolExact {
   __device__ static double lim(double x, double y) { return ex::limiter<LIM>(x, y); }
   template <int NV>
   __device__ static bool face(const Gas& g, const double* QL, const double* QR, const double* n, double A,
-                              double* F) {
-    return ex::face_flux<RIE, NV>(g, QL, QR, n, A, F);
+                              double* F, double beta = 1.0) {
+    return ex::face_flux<RIE, NV>(g, QL, QR, n, A, F, beta);
   }
   template <int NV>
   __device__ static bool update(const Gas& g, double* Q, const double* QO, const double* R, double vol, double dt,
@@ -192,7 +192,7 @@ struct PolFast {
   }
   template <int NV>
   __device__ static bool face(const Gas& g, const double* QL, const double* QR, const double* n, double A,
-                              double* F) {
+                              double* F, double beta = 1.0) {
     constexpr int P = NV - 1;
     bool ok = (QL[0] > 0.0 && QL[P] > 0.0 && QR[0] > 0.0 && QR[P] > 0.0);
     const fast::GasF gf = fast::gasf(g);
@@ -204,7 +204,7 @@ struct PolFast {
       else fast::ausmp<NV>(gf, QL, QR, n, F);
     } else {
       double aL = ex::sound(g, QL[0], QL[P]), aR = ex::sound(g, QR[0], QR[P]);
-      ex::riemann<RIE, NV>(g, QL, aL, QR, aR, n, F);
+      ex::riemann<RIE, NV>(g, QL, aL, QR, aR, n, F, beta);
     }
     for (int v = 0; v < NV; ++v) F[v] = F[v] * A;
     return ok;
@@ -265,7 +265,7 @@ constexpr bool stage_fp32_pipeline() {
 // the items may touch physical boundary faces (their add masks are kept);
 // without, the FP32 pipeline's face fluxes are all FP32 values and are kept
 // as such.  Arrays a variant does not use shrink to one element.
-template <int NV, int NVR, bool MX, bool BC>
+template <int NV, int NVR, bool MX, bool BC, bool SDV = false>
 struct StageSmem {
   using FluxT = typename std::conditional<MX && !BC, float, double>::type;
   static constexpr int kY = MX ? 1 : SB_Y, kX = MX ? 1 : SB_X, kV = MX ? 1 : NV;
@@ -281,11 +281,12 @@ struct StageSmem {
   float4 r32[mR][mS];                 // FP32 ring of (rho, u, v, p)
   float4 sx32[mY][mX];
   float4 sy32[MX ? SB_Y + 1 : 1][mX];
+  double beta[SDV ? SB_Y : 1][SDV ? SB_X : 1];   // shock detector of cell (c, j) (run-time solver kernels)
 };
 
-template <bool UNI, bool MX, bool BC>
+template <bool UNI, bool MX, bool BC, bool SDV = false>
 constexpr size_t stage_smem_bytes() {
-  return sizeof(StageSmem<4, UNI ? 4 : 6, MX, BC>);
+  return sizeof(StageSmem<4, UNI ? 4 : 6, MX, BC, SDV>);
 }
 
 // Minimum resident CTAs per SM of a kernel variant.  Without boundary faces
@@ -345,8 +346,15 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
   // uniform grid, fast arithmetic: the limiters are homogeneous of degree 1,
   // so slopes stay in difference units and the half-cell factor is 1/2
   constexpr bool FU = UNI && PH::kFast;
+  // the run-time solver kernels carry the shock detector (SD_Tramel) of
+  // Mod_Fluxes.f90:78-85: each face takes its low cell's value (the
+  // boundary cell's at a connection on a low face, Lib_BC_Fluxes_Connection
+  // .f90:58-62), which scales the limited slopes under MUSCL-SD and goes to
+  // the SD Riemann solvers
+  constexpr bool SDV = (RIE == 4);
+  const bool sd = SDV && a.g.sd != 0, sdl = SDV && (a.g.sd & 1) != 0;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  StageSmem<NV, NVR, MX, BC>& S = *reinterpret_cast<StageSmem<NV, NVR, MX, BC>*>(smem_raw);
+  StageSmem<NV, NVR, MX, BC, SDV>& S = *reinterpret_cast<StageSmem<NV, NVR, MX, BC, SDV>*>(smem_raw);
   const int4* items = BC ? a.items : a.items_nb;
   const int nitems = BC ? a.nitems : a.nitems_nb;
   const int t = threadIdx.x;
@@ -416,6 +424,11 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
     // half-cell factor of a face state: 0.5 dl (reference) or 0.5 (difference units)
     auto half = [&](double dl) -> double {
       if constexpr (FU) return 0.5; else return 0.5 * dl;
+    };
+    // shock detector of the cell at ring row rr, column col (rows rm / rp)
+    auto cell_beta = [&](int rm_, int rr_, int rp_, int col_) -> double {
+      return ex::sd_tramel2(S.ring[NV - 1][rr_][col_], S.ring[NV - 1][rr_][col_ - 1], S.ring[NV - 1][rr_][col_ + 1],
+                            S.ring[NV - 1][rm_][col_], S.ring[NV - 1][rp_][col_]);
     };
     // limited j-slope of the cell at ring row rr (rows rm, rr, rp), ring column col
     auto slope_j = [&](int rm, int rr, int rp, int col, double* s) {
@@ -533,12 +546,16 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
         double qm[NV], QL[NV], QR[NV];
         ringQ(1, tx + 1, qm);
         const double lm = half(ring_dly(1, tx + 1)), lp = half(ring_dly(2, tx + 1));
+        // the face below row j0: row j0 - 1's detector, row j0's on the block's low face
+        const double bP = sd ? (j0 == 0 ? cell_beta(1, 2, 3, tx + 1) : cell_beta(0, 1, 2, tx + 1)) : 1.0;
 #pragma unroll
         for (int v = 0; v < NV; ++v) {
-          QL[v] = qm[v] + S.sy[v][1][tx] * lm;
-          QR[v] = q0[v] - S.sy[v][0][tx] * lp;
+          const double sLv = sdl ? bP * S.sy[v][1][tx] : S.sy[v][1][tx];
+          const double sRv = sdl ? bP * S.sy[v][0][tx] : S.sy[v][0][tx];
+          QL[v] = qm[v] + sLv * lm;
+          QR[v] = q0[v] - sRv * lp;
         }
-        ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+        ok = PH::template face<NV>(a.g, QL, QR, n, A, G, bP);
       }
       if (!ok && j0 > 0) report(a.err, 4, b, c, j0, 0);
       int mask = ADD_ALL;
@@ -581,6 +598,9 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
         for (int v = 0; v < NV; ++v) S.g[v][0][tx] = S.g[v][SB_Y][tx];
         if constexpr (BC) S.gm[0][tx] = S.gm[SB_Y][tx];
       }
+      if constexpr (SDV) {
+        if (sd && rowok) S.beta[ty][tx] = cell_beta(rm, rr, rp, col);
+      }
       if (rowok) {
         if constexpr (MX) {
           const float4 qa = S.r32[rr][col - 1], q = S.r32[rr][col], qb = S.r32[rr][col + 1];
@@ -620,12 +640,18 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
           } else {
             double QL[NV], QR[NV];
             const double lm = half(ring_dlx(rr, col)), lp = half(ring_dlx(rr, col + 1));
+            double bF = 1.0;
+            if constexpr (SDV) {
+              if (sd) bF = (c == -1) ? S.beta[ty][tx + 1] : S.beta[ty][tx];
+            }
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-              QL[v] = S.ring[v][rr][col] + S.sx[v][ty][tx] * lm;
-              QR[v] = S.ring[v][rr][col + 1] - S.sx[v][ty][tx + 1] * lp;
+              const double sLv = sdl ? bF * S.sx[v][ty][tx] : S.sx[v][ty][tx];
+              const double sRv = sdl ? bF * S.sx[v][ty][tx + 1] : S.sx[v][ty][tx + 1];
+              QL[v] = S.ring[v][rr][col] + sLv * lm;
+              QR[v] = S.ring[v][rr][col + 1] - sRv * lp;
             }
-            ok = PH::template face<NV>(a.g, QL, QR, n, A, F);
+            ok = PH::template face<NV>(a.g, QL, QR, n, A, F, bF);
           }
           const bool lowb = (c == -1), highb = (c == ni - 1);
           int mask = ADD_ALL;
@@ -660,12 +686,18 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
           } else {
             double QL[NV], QR[NV];
             const double lm = half(ring_dly(rr, col)), lp = half(ring_dly(rp, col));
+            double bG = 1.0;
+            if constexpr (SDV) {
+              if (sd) bG = S.beta[ty][tx];
+            }
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
-              QL[v] = S.ring[v][rr][col] + S.sy[v][ty][tx] * lm;
-              QR[v] = S.ring[v][rp][col] - S.sy[v][ty + 1][tx] * lp;
+              const double sLv = sdl ? bG * S.sy[v][ty][tx] : S.sy[v][ty][tx];
+              const double sRv = sdl ? bG * S.sy[v][ty + 1][tx] : S.sy[v][ty + 1][tx];
+              QL[v] = S.ring[v][rr][col] + sLv * lm;
+              QR[v] = S.ring[v][rp][col] - sRv * lp;
             }
-            ok = PH::template face<NV>(a.g, QL, QR, n, A, G);
+            ok = PH::template face<NV>(a.g, QL, QR, n, A, G, bG);
           }
           int mask = ADD_ALL;
           if (!ok && j < nj - 1) report(a.err, 4, b, c, j, 0);

@@ -22,7 +22,7 @@ using StagePolicy = typename std::conditional<PREC == 0, PolExact<RIE, LIM>, Pol
 template <int PREC, int RIE, int LIM, bool UNI, int MODE, bool BC>
 static void launch_persistent_list(const StageArgs& a, int nitems, int nsm, cudaStream_t s) {
   using PH = StagePolicy<PREC, RIE, LIM>;
-  constexpr size_t smem = stage_smem_bytes<UNI, stage_fp32_pipeline<PH, RIE, UNI>(), BC>();
+  constexpr size_t smem = stage_smem_bytes<UNI, stage_fp32_pipeline<PH, RIE, UNI>(), BC, RIE == 4>();
   static int occ = 0;   // one per kernel instance
   if (occ == 0) {
     cudaFuncSetAttribute(k_stage2d<PH, RIE, LIM, UNI, MODE, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -198,7 +198,9 @@ def read_input_ini(path) -> dict:
         kw["steps"] = int(par["iter-threshold"])
     unsupported = []
     if rec.upper().endswith("-SD"):
-        unsupported.append(f"space-reconstruction = {rec} (shock-detector limiting)")
+        kw["sd_limiter"] = True
+    if "cfl-rise-threshold" in num:
+        kw["ramp_iter"] = int(num["cfl-rise-threshold"])
     if "irs-beta" in num:
         kw["irs_beta"] = float(num["irs-beta"])
     kw["unsupported"] = unsupported
@@ -228,6 +230,6 @@ def load_case(case_dir, resolution: str = "", gamma: float | None = None, rgas: 
         unsupported.append(f"riemann-solver = {kw['riemann']}")
     case = Case(d.name + sfx, nodes, rec, data, prim, gamma=gamma, rgas=rgas,
                 **{k: v for k, v in kw.items() if k in ("cfl", "n_rk", "time_accurate", "riemann", "minf", "limiter",
-                                                        "t_end", "steps", "irs_beta")})
+                                                        "t_end", "steps", "irs_beta", "sd_limiter", "ramp_iter")})
     case.extra["unsupported"] = unsupported
     return case

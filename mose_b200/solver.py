@@ -59,6 +59,7 @@ class Solver:
         cfg.precision = precision
         cfg.gamma = case.gamma
         cfg.rgas = case.rgas
+        cfg.ramp_iter = int(getattr(case, "ramp_iter", 0))
         cfg.device = device
         h = C.c_void_p()
         rc = self.lib.mose_gpu_create(C.byref(cfg), C.byref(h))
@@ -68,6 +69,8 @@ class Solver:
         self.case = case
         if getattr(case, "minf", 0.0):
             self._check(self.lib.mose_gpu_set_riemann_minf(self.h, float(case.minf)))
+        if getattr(case, "sd_limiter", False):
+            self._check(self.lib.mose_gpu_set_sd_limiter(self.h, 1))
         if getattr(case, "irs_beta", 0.0):
             self._check(self.lib.mose_gpu_set_irs_beta(self.h, float(case.irs_beta)))
         self.dims = []

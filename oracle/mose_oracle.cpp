@@ -642,9 +642,118 @@ inline RFlux riemann_AUSMp_up(const Thermo& t, const RState& L, const RState& R,
   return F;
 }
 
+// riemann_HLLCSD ('HLLC+', Tramel), Lib_Riemann_HLL.f90:500-534: HLLE where
+// the shock detector is 0, HLLC where it is >= 1, their blend in between
+inline RFlux riemann_HLLCSD(const Thermo& t, const RState& L, const RState& R, double nx, double ny, double nz,
+                            double beta) {
+  if (beta == 0.0) return riemann_HLLE(t, L, R, nx, ny, nz);
+  if (beta >= 1.0) return riemann_HLLC(t, L, R, nx, ny, nz);
+  RFlux E = riemann_HLLE(t, L, R, nx, ny, nz), C = riemann_HLLC(t, L, R, nx, ny, nz), F;
+  F.r = beta * C.r + (1.0 - beta) * E.r;
+  F.u = beta * C.u + (1.0 - beta) * E.u;
+  F.v = beta * C.v + (1.0 - beta) * E.v;
+  F.w = beta * C.w + (1.0 - beta) * E.w;
+  F.E = beta * C.E + (1.0 - beta) * E.E;
+  return F;
+}
+
+// hartenHyman, Lib_Riemann_HLL.f90:537-547
+inline double hartenHyman(double v, double e) {
+  double al = std::fabs(v);
+  double l = al;
+  if (al <= e) l = (v * v + e * e) / (2.0 * e);
+  return l;
+}
+
+// riemann_HLLEpp ('HLLE++', Tramel), Lib_Riemann_HLL.f90:320-464: central
+// flux with the wave-by-wave dissipation whose eigenvalues blend Roe's
+// (Harten-Hyman fixed) and HLLE's by the shock detector
+inline RFlux riemann_HLLEpp(const Thermo& t, const RState& L, const RState& R, double nx, double ny, double nz,
+                            double beta) {
+  RFlux F;
+  double unl = L.u * nx + L.v * ny + L.w * nz;
+  double unr = R.u * nx + R.v * ny + R.w * nz;
+  double h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe;
+  roe_averages(t, L, R, h0l, h0r, u_roe, v_roe, w_roe, a_roe, h0_roe);
+  double rho_roe = rho_roe_of(L, R);
+  double un_roe = u_roe * nx + v_roe * ny + w_roe * nz;
+  double Sm = std::min(std::min(0.0, unl - L.a), un_roe - a_roe);
+  double Sp = std::max(std::max(0.0, unr + R.a), un_roe + a_roe);
+  double inv_denom = 1.0 / (Sp - Sm);
+  double lam1_hlle = std::fabs((Sp + Sm) * un_roe * inv_denom - 2.0 * Sp * Sm * inv_denom);
+  double lam2_hlle = std::fabs((Sp + Sm) * (un_roe - a_roe) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+  double lam3_hlle = std::fabs((Sp + Sm) * (un_roe + a_roe) * inv_denom - 2.0 * Sp * Sm * inv_denom);
+  double eps = 0.3 * (std::fabs(un_roe) + a_roe);
+  double lam1_roe = std::fabs(un_roe);
+  double lam2_roe = hartenHyman(un_roe - a_roe, eps);
+  double lam3_roe = hartenHyman(un_roe + a_roe, eps);
+  double lam1_pp = beta * lam1_roe + (1.0 - beta) * lam1_hlle;
+  double lam2_pp = beta * lam2_roe + (1.0 - beta) * lam2_hlle;
+  double lam3_pp = beta * lam3_roe + (1.0 - beta) * lam3_hlle;
+  RFlux Fl = phys_flux(t, L, nx, ny, nz), Fr = phys_flux(t, R, nx, ny, nz);
+  F.r = 0.5 * (Fl.r + Fr.r);
+  F.u = 0.5 * (Fl.u + Fr.u);
+  F.v = 0.5 * (Fl.v + Fr.v);
+  F.w = 0.5 * (Fl.w + Fr.w);
+  F.E = 0.5 * (Fl.E + Fr.E);
+  double drho = R.rho - L.rho, dp = R.p - L.p;
+  double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w, dun = unr - unl;
+  double t1x, t1y, t1z;
+  if (std::fabs(nx) < 0.9) { t1x = 0.0; t1y = -nz; t1z = ny; }
+  else { t1x = -nz; t1y = 0.0; t1z = nx; }
+  double normt = std::sqrt(t1x * t1x + t1y * t1y + t1z * t1z);
+  t1x = t1x / normt; t1y = t1y / normt; t1z = t1z / normt;
+  double t2x = ny * t1z - nz * t1y, t2y = nz * t1x - nx * t1z, t2z = nx * t1y - ny * t1x;
+  double alpha_m = (dp - rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+  double alpha_c = drho - dp / (a_roe * a_roe);
+  double alpha_s1 = rho_roe * (du * t1x + dv * t1y + dw * t1z);
+  double alpha_s2 = rho_roe * (du * t2x + dv * t2y + dw * t2z);
+  double alpha_p = (dp + rho_roe * a_roe * dun) / (2.0 * a_roe * a_roe);
+  F.r = F.r - 0.5 * (alpha_c * lam1_pp + alpha_m * lam2_pp + alpha_p * lam3_pp);
+  F.u = F.u - 0.5 * (alpha_c * lam1_pp * u_roe);
+  F.v = F.v - 0.5 * (alpha_c * lam1_pp * v_roe);
+  F.w = F.w - 0.5 * (alpha_c * lam1_pp * w_roe);
+  F.u = F.u - 0.5 * lam1_pp * (alpha_s1 * t1x + alpha_s2 * t2x);
+  F.v = F.v - 0.5 * lam1_pp * (alpha_s1 * t1y + alpha_s2 * t2y);
+  F.w = F.w - 0.5 * lam1_pp * (alpha_s1 * t1z + alpha_s2 * t2z);
+  F.u = F.u - 0.5 * (alpha_m * lam2_pp * (u_roe - a_roe * nx) + alpha_p * lam3_pp * (u_roe + a_roe * nx));
+  F.v = F.v - 0.5 * (alpha_m * lam2_pp * (v_roe - a_roe * ny) + alpha_p * lam3_pp * (v_roe + a_roe * ny));
+  F.w = F.w - 0.5 * (alpha_m * lam2_pp * (w_roe - a_roe * nz) + alpha_p * lam3_pp * (w_roe + a_roe * nz));
+  F.E = F.E - 0.5 * lam1_pp * (alpha_c * 0.5 * (u_roe * u_roe + v_roe * v_roe + w_roe * w_roe));
+  F.E = F.E - 0.5 * lam1_pp * (alpha_s1 * (u_roe * t1x + v_roe * t1y + w_roe * t1z) +
+                               alpha_s2 * (u_roe * t2x + v_roe * t2y + w_roe * t2z));
+  F.E = F.E - 0.5 * (alpha_m * lam2_pp * (h0_roe - a_roe * un_roe) + alpha_p * lam3_pp * (h0_roe + a_roe * un_roe));
+  return F;
+}
+
+// SD_Tramel, Lib_Shock_Detector.f90:9-38 (DELTA = 20): a Jameson-type
+// pressure sensor over the six face neighbours
+inline double SD_Tramel(double p, double p1, double p2, double p3, double p4, double p5, double p6) {
+  const double DELTA = 20.0;
+  double kp1 = std::fabs((p2 - 2.0 * p + p1) / (p2 + 2.0 * p + p1));
+  double kp2 = std::fabs((p4 - 2.0 * p + p3) / (p4 + 2.0 * p + p3));
+  double kp3 = std::fabs((p6 - 2.0 * p + p5) / (p6 + 2.0 * p + p5));
+  double sw = std::max(std::max(kp1, kp2), kp3);
+  if (sw < 1.0 / DELTA) {
+    double phi = std::max(sw / DELTA, 0.0);
+    return 1.0 - std::tanh(10.0 * phi * phi * phi);
+  }
+  return 0.0;
+}
+// the shock-detector solvers (Mod_Riemann.f90:79-87 set obj_riemann%SD)
+inline bool sd_riemann(const orc_domain* d) {
+  return d->cfg.riemann == ORC_RIE_HLLC_SD || d->cfg.riemann == ORC_RIE_HLLE_PP;
+}
+// any shock detector in use (Assign_Setup.f90:43-47)
+inline bool sd_any(const orc_domain* d) { return d->cfg.sd_limiter != 0 || sd_riemann(d); }
+
+// beta: the shock detector of the face (1 at the physical boundary faces,
+// which call Riemann with 1d0)
 inline RFlux Riemann(const orc_domain* d, const RState& L, const RState& R, double nx,
-                     double ny, double nz) {
+                     double ny, double nz, double beta = 1.0) {
   switch (d->cfg.riemann) {
+    case ORC_RIE_HLLC_SD: return riemann_HLLCSD(d->th, L, R, nx, ny, nz, beta);
+    case ORC_RIE_HLLE_PP: return riemann_HLLEpp(d->th, L, R, nx, ny, nz, beta);
     case ORC_RIE_AUSMP: return riemann_AUSMp(d->th, L, R, nx, ny, nz);
     case ORC_RIE_SLAU: return riemann_SLAU(d->th, L, R, nx, ny, nz, false);
     case ORC_RIE_SLAU2: return riemann_SLAU(d->th, L, R, nx, ny, nz, true);
@@ -703,18 +812,19 @@ inline void face_flux(const RFlux& F, double area, const double* p1, double rho1
 // Convective_Flux, Lib_Convective.f90:10-85
 inline bool Convective_Flux(const orc_domain* d, const double* dl /*-1..2*/, const double* N,
                             double area, const double* Pm1, const double* P0, const double* P1,
-                            const double* P2, double* R0, double* R1) {
+                            const double* P2, double* R0, double* R1, double beta) {
   double l0 = 0.5 * (dl[0] + dl[1]);
   double l1 = 0.5 * (dl[1] + dl[2]);
   double l2 = 0.5 * (dl[2] + dl[3]);
   double lm = 0.5 * dl[1];
   double lp = 0.5 * dl[2];
   double Prim1[NPRIM], Prim4[NPRIM];
-  Reconstruction(d->cfg.limiter, Pm1, P0, P1, P2, l0, l1, l2, lm, lp, 1.0, Prim1, Prim4);
+  // :37-42: the limiter scaled by beta under MUSCL-SD, else by 1
+  Reconstruction(d->cfg.limiter, Pm1, P0, P1, P2, l0, l1, l2, lm, lp, d->cfg.sd_limiter ? beta : 1.0, Prim1, Prim4);
   bool bad = false;
   RState L = make_state(d->th, Prim1, bad);
   RState R = make_state(d->th, Prim4, bad);
-  RFlux F = Riemann(d, L, R, N[0], N[1], N[2]);
+  RFlux F = Riemann(d, L, R, N[0], N[1], N[2], beta);
   double Flux[NPRIM];
   face_flux(F, area, Prim1, L.rho, Prim4, R.rho, Flux);
   for (int v = 0; v < NPRIM; ++v) R0[v] = R0[v] + Flux[v];
@@ -1147,11 +1257,15 @@ bool BC_Connection_Eul(const orc_domain* D, int Im, int Jm, int Km, int Fm, Bloc
   double Dist12 = Dl1 + Dl2;
   double Dist34 = Dl3 + Dl4;
   double PL[NPRIM], PR[NPRIM];
-  Reconstruction(D->cfg.limiter, Prim1, Prim2, Prim3, Prim4, Dist12, Dist23, Dist34, Dl2, Dl3, 1.0, PL, PR);
+  // :58-62 / :85-89: the boundary cell's shock detector under MUSCL-SD / an
+  // SD Riemann solver, else 1
+  const double beta_cell = blk.beta[blk.inner(Im, Jm, Km)];
+  Reconstruction(D->cfg.limiter, Prim1, Prim2, Prim3, Prim4, Dist12, Dist23, Dist34, Dl2, Dl3,
+                 D->cfg.sd_limiter ? beta_cell : 1.0, PL, PR);
   bool bad = false;   // the connection flux does not call check_gas_state
   RState L = make_state(D->th, PL, bad);
   RState R = make_state(D->th, PR, bad);
-  RFlux F = Riemann(D, L, R, Normal[0], Normal[1], Normal[2]);
+  RFlux F = Riemann(D, L, R, Normal[0], Normal[1], Normal[2], sd_riemann(D) ? beta_cell : 1.0);
   double su = std::copysign(0.5, F.r);
   double sel_L = 0.5 + su, sel_R = su - 0.5;
   double Fmass = F.r * Area;
@@ -1578,6 +1692,18 @@ int orc_fluxes(orc_domain* d) {
             for (int v = 0; v < NPRIM; ++v) r[v] = 0.0;
             B.beta[B.inner(i, j, k)] = 1.0;
           }
+      // Shock-detector, Mod_Fluxes.f90:78-85
+      if (sd_any(d)) {
+#ifdef _OPENMP
+#pragma omp for collapse(3)
+#endif
+        for (int k = 1; k <= n3; ++k)
+          for (int j = 1; j <= n2; ++j)
+            for (int i = 1; i <= n1; ++i)
+              B.beta[B.inner(i, j, k)] = SD_Tramel(B.Pc(i, j, k)[NP], B.Pc(i - 1, j, k)[NP], B.Pc(i + 1, j, k)[NP],
+                                                   B.Pc(i, j - 1, k)[NP], B.Pc(i, j + 1, k)[NP],
+                                                   B.Pc(i, j, k - 1)[NP], B.Pc(i, j, k + 1)[NP]);
+      }
       // i faces (:89-99)
 #ifdef _OPENMP
 #pragma omp for collapse(2)
@@ -1588,7 +1714,7 @@ int orc_fluxes(orc_domain* d) {
             double dls[4] = {B.dl_(1, i - 1, j, k), B.dl_(1, i, j, k), B.dl_(1, i + 1, j, k), B.dl_(1, i + 2, j, k)};
             size_t f = B.face(1, i, j, k);
             if (!Convective_Flux(d, dls, &B.fN[0][3 * f], B.fA[0][f], B.Pc(i - 1, j, k), B.Pc(i, j, k),
-                                 B.Pc(i + 1, j, k), B.Pc(i + 2, j, k), B.Rc(i, j, k), B.Rc(i + 1, j, k)))
+                                 B.Pc(i + 1, j, k), B.Pc(i + 2, j, k), B.Rc(i, j, k), B.Rc(i + 1, j, k), B.beta[B.inner(i, j, k)]))
               d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
           }
       // j faces (:129-139)
@@ -1601,7 +1727,7 @@ int orc_fluxes(orc_domain* d) {
             double dls[4] = {B.dl_(2, i, j - 1, k), B.dl_(2, i, j, k), B.dl_(2, i, j + 1, k), B.dl_(2, i, j + 2, k)};
             size_t f = B.face(2, i, j, k);
             if (!Convective_Flux(d, dls, &B.fN[1][3 * f], B.fA[1][f], B.Pc(i, j - 1, k), B.Pc(i, j, k),
-                                 B.Pc(i, j + 1, k), B.Pc(i, j + 2, k), B.Rc(i, j, k), B.Rc(i, j + 1, k)))
+                                 B.Pc(i, j + 1, k), B.Pc(i, j + 2, k), B.Rc(i, j, k), B.Rc(i, j + 1, k), B.beta[B.inner(i, j, k)]))
               d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
           }
       // k faces (:169-179)
@@ -1614,7 +1740,7 @@ int orc_fluxes(orc_domain* d) {
             double dls[4] = {B.dl_(3, i, j, k - 1), B.dl_(3, i, j, k), B.dl_(3, i, j, k + 1), B.dl_(3, i, j, k + 2)};
             size_t f = B.face(3, i, j, k);
             if (!Convective_Flux(d, dls, &B.fN[2][3 * f], B.fA[2][f], B.Pc(i, j, k - 1), B.Pc(i, j, k),
-                                 B.Pc(i, j, k + 1), B.Pc(i, j, k + 2), B.Rc(i, j, k), B.Rc(i, j, k + 1)))
+                                 B.Pc(i, j, k + 1), B.Pc(i, j, k + 2), B.Rc(i, j, k), B.Rc(i, j, k + 1), B.beta[B.inner(i, j, k)]))
               d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
           }
     }

@@ -21,7 +21,7 @@ class orc_config(C.Structure):
                 ("limiter", C.c_int32), ("riemann", C.c_int32), ("integration", C.c_int32),
                 ("ndir", C.c_int32), ("gamma", C.c_double), ("rgas", C.c_double),
                 ("ramp_iter", C.c_int32), ("res_diter", C.c_int32), ("minf", C.c_double),
-                ("irs_beta", C.c_double)]
+                ("irs_beta", C.c_double), ("sd_limiter", C.c_int32)]
 
 
 _LIBS: dict = {}
@@ -80,7 +80,7 @@ def _dp(a: np.ndarray):
 
 LIMITERS = {"first-order": 0, "none": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5}
 RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3, "HLLE": 4, "HLLEM": 5, "LLF": 6, "Rusanov": 6,
-           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10}
+           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10, "HLLC+": 11, "HLLE++": 12}
 
 
 class Oracle:
@@ -90,8 +90,10 @@ class Oracle:
         self.lib = load(omp)
         cfg = orc_config(n_rk=case.n_rk, cfl=case.cfl, time_accurate=int(case.time_accurate),
                          limiter=LIMITERS[case.limiter], riemann=RIEMANN[case.riemann], integration=0,
-                         ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=0, res_diter=1,
-                         minf=getattr(case, "minf", 0.0), irs_beta=getattr(case, "irs_beta", 0.0))
+                         ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=int(getattr(case, "ramp_iter", 0)),
+                         res_diter=1,
+                         minf=getattr(case, "minf", 0.0), irs_beta=getattr(case, "irs_beta", 0.0),
+                         sd_limiter=int(getattr(case, "sd_limiter", False)))
         self.h = self.lib.orc_create(C.byref(cfg), nthreads)
         self.dims = []
         for nd in case.nodes:

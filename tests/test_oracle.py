@@ -93,7 +93,8 @@ def test_limiter_known_values(oracle_mod, lim):
         assert f(1.0, 0.5) == pytest.approx(0.75, rel=1e-15)
 
 
-RIEMANN_ALL = ["HLLC", "AUSM+", "SLAU", "SLAU2", "HLLE", "HLLEM", "LLF", "PLLF", "Hanel", "AUSM+-up", "AUSM+-up2"]
+RIEMANN_ALL = ["HLLC", "AUSM+", "SLAU", "SLAU2", "HLLE", "HLLEM", "LLF", "PLLF", "Hanel", "AUSM+-up", "AUSM+-up2",
+               "HLLC+", "HLLE++"]
 
 
 @pytest.mark.parametrize("riemann", RIEMANN_ALL)

@@ -76,11 +76,11 @@ def test_round_trip_two_blocks(tmp_path):
     assert c.extra["unsupported"] == []
 
 
-def test_unsupported_numerics_reported(tmp_path):
+def test_sd_and_irs_numerics_read(tmp_path):
     ini = tmp_path / "input.ini"
     ini.write_text("[MOSE-Numerics]\nspace-reconstruction = MUSCL-SD\nirs-beta = 0.5\nflux-limiter = mc\n")
     kw = refio.read_input_ini(ini)
-    assert len(kw["unsupported"]) == 1 and kw["irs_beta"] == 0.5
+    assert kw["unsupported"] == [] and kw["irs_beta"] == 0.5 and kw["sd_limiter"]
 
 
 @pytest.mark.skipif(not REF.exists(), reason="reference tree not present")
