@@ -18,13 +18,20 @@
  *   bc    : one record per boundary face cell in bc.txt order (block, face
  *           1..6, cell): int32 b,i,j,k,f,type,bs,is,js,ks,fs,d11,d12,d21,d22
  *           (1-based), plus 6 doubles of type data
- *           405: mach, T, p, alpha, beta, rel_fac ; 406: p_back, rel_fac
+ *           401: T0, p0, alpha, beta, rel_fac ; 403: T0, g, alpha, beta,
+ *           rel_fac ; 404: T, g, alpha, beta, rel_fac ; 405: mach, T, p,
+ *           alpha, beta, rel_fac ; 406: p_back, rel_fac ; 407: T0, p0,
+ *           p_back, alpha, beta, rel_fac (g: mass flux per unit area; the
+ *           largest double as alpha or beta is the token 'normal', which
+ *           407 does not take; on 2-D domains beta is 0 or 'normal')
  *
  * State is device resident between calls: host P is stale until
  * mose_gpu_download_prim().  A context is not thread safe and owns one
  * CUDA stream.  On 2-D domains (nk = 1) the transfers of P and R read and
  * write only the k = 1 plane of the reference array: the reference never
- * reads its k ghost planes on this path, and w is identically zero there.
+ * reads its k ghost planes on this path, and w is zero there (the
+ * 401 / 403 / 404 inlets leave rounding-level w in the reference: their
+ * face velocity sums three vectors whose z parts cancel only to rounding).
  */
 #ifndef MOSE_GPU_H
 #define MOSE_GPU_H

@@ -9,7 +9,9 @@ fastest Fortran index last:
   nodes[b] : (nk+1, nj+1, ni+1, 3)  == Fortran node(3, 0:ni, 0:nj, 0:nk)
   prim[b]  : (nk,   nj,   ni,   5)  == interior P(5, 1:ni, 1:nj, 1:nk)
   bc_rec   : (nbound, 15) int32     == b i j k f type bs is js ks fs d11 d12 d21 d22
-  bc_data  : (nbound, 6)  float64   == 405: mach T p alpha beta rel_fac ; 406: p_back rel_fac
+  bc_data  : (nbound, 6)  float64   == 401: T0 p0 alpha beta rel_fac ; 403 / 404: T0 / T g alpha beta
+                                      rel_fac ; 405: mach T p alpha beta rel_fac ; 406: p_back rel_fac ;
+                                      407: T0 p0 p_back alpha beta rel_fac
 
 The five benchmark configurations are built from seeded synthetic inputs of
 the shapes the reference problem statement names; no external dataset is used.

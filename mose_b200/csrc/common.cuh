@@ -34,6 +34,10 @@ enum BcCode : int {
   BC_EXTRAP = 3,    // (400) extrapolation
   BC_SUPIN = 4,     // (405) supersonic inflow (M, T, p)
   BC_OUTFLOW = 5,   // (406) outflow with back pressure
+  BC_STAGIN = 6,    // (401) inlet, total temperature and pressure
+  BC_MFLUX_T0 = 7,  // (403) inlet, total temperature and mass flux
+  BC_MFLUX_T = 8,   // (404) inlet, static temperature and mass flux
+  BC_FARFIELD = 9,  // (407) ambient: total conditions in, back pressure out
 };
 
 // Error word written by kernels (first offender wins).
@@ -88,11 +92,19 @@ __host__ __device__ inline long long cell_off3(const BlockDesc& d, int i, int j,
 __host__ __device__ inline int bc_code(int w) { return w & 0xff; }
 __host__ __device__ inline int bc_param(int w) { return (w >> 8) - 1; }
 
-// Parameters of a 405 / 406 face cell, precomputed on the host.
+// Parameters of a 401 / 403 / 404 / 405 / 406 / 407 face cell, precomputed
+// on the host.  T: the static temperature (404, 405) or the total one (401,
+// 403, 407); p: the static pressure (405), the total pressure (401, 407) or
+// the mass flux g (403, 404); pback: the back pressure (406, 407).
 struct BcParam {
   double mach, T, p, rel_fac;
   double ca, sa, cb, sb;   // cos/sin of the inflow angles (alpha, beta)
   double pback;
+  // 401 / 403 / 404 / 407: the face's unit tangent t (a diagonal between two
+  // of its nodes) and binormal b = n x t / |n x t|, and the ratios E1, E2 of
+  // the t and b velocity components to the normal one that point the inflow
+  // along (alpha, beta) (Lib_BC_Fluxes_Inflow.f90:113-129, 404-420)
+  double tv[3], bv[3], E1, E2;
 };
 
 // One first-layer ghost value of the residual for implicit residual

@@ -276,8 +276,12 @@ int bc_code_of(int type) {
     case 101: case 201: return BC_CONN;
     case 300: return BC_SYM;
     case 400: return BC_EXTRAP;
+    case 401: return BC_STAGIN;
+    case 403: return BC_MFLUX_T0;
+    case 404: return BC_MFLUX_T;
     case 405: return BC_SUPIN;
     case 406: return BC_OUTFLOW;
+    case 407: return BC_FARFIELD;
   }
   return -1;
 }
@@ -511,6 +515,15 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     // (the token 'normal' resolves to atan(0 / ...) = 0 there: 2-D face normals have n_z = 0)
     if (ctx->nd == 2 && e.type == 405 && e.data[4] != 0.0 && !(e.data[4] >= 0.5 * 1.7976931348623157e308))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
+    if (ctx->nd == 2 && (e.type == 401 || e.type == 403 || e.type == 404) && e.data[3] != 0.0 &&
+        !(e.data[3] >= 0.5 * 1.7976931348623157e308))
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
+    // 407 uses its angles as given (Lib_BC_Fluxes_FarField.f90:48-49): the
+    // token 'normal' would enter tan() as the largest double
+    if (e.type == 407 && (e.data[3] >= 0.5 * 1.7976931348623157e308 || e.data[4] >= 0.5 * 1.7976931348623157e308))
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "bc 407 takes numeric inflow angles, not 'normal'");
+    if (ctx->nd == 2 && e.type == 407 && e.data[4] != 0.0)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
   }
   for (int b = 0; b < nb && ctx->nd == 3; ++b)
     if (ctx->hblk[b].nk < 1 || ctx->hblk[b].ni >= 65536)
@@ -548,6 +561,10 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   // and are resolved once the device has formed the face metrics
   struct NormalDir { int pidx, b, f, i, j, k; bool a, be; };
   std::vector<NormalDir> normal_dirs;
+  // 401 / 403 / 404 / 407 records: tangent, binormal and direction
+  // coefficients, formed from the face normal once the device has it
+  struct InletGeo { int pidx, b, f, i, j, k; double alpha, beta; bool raw; };
+  std::vector<InletGeo> inlet_geo;
   for (auto& e : ctx->bc) {
     const BlockDesc& d = ctx->desc[e.b - 1];
     const HostBlock& h = ctx->hblk[e.b - 1];
@@ -564,6 +581,20 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       } else {
         p.pback = e.data[0]; p.rel_fac = e.data[1];
       }
+      pidx = (int)params.size();
+      params.push_back(p);
+    } else if (e.type == 401 || e.type == 403 || e.type == 404 || e.type == 407) {
+      BcParam p{};
+      p.T = e.data[0]; p.p = e.data[1];
+      double alpha = e.data[2], beta = e.data[3];
+      if (e.type == 407) {
+        p.pback = e.data[2]; p.rel_fac = e.data[5];
+        alpha = e.data[3]; beta = e.data[4];
+      } else {
+        p.rel_fac = e.data[4];
+      }
+      inlet_geo.push_back(InletGeo{(int)params.size(), e.b - 1, e.f, e.i - 1, e.j - 1, e.k - 1, alpha, beta,
+                                   e.type == 407});
       pidx = (int)params.size();
       params.push_back(p);
     }
@@ -636,21 +667,28 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     rc = poll_device_error(ctx);   // metric failures and index self-checks
     if (rc) return rc;
   }
-  if (!normal_dirs.empty()) {
+  if (!normal_dirs.empty() || !inlet_geo.empty()) {
     // the boundary face's normal (nx, ny, nz planes of its direction), then
     // alpha = atan(N_y / (N_x + 1d-20)), beta = atan(N_z / (N_x + 1d-20)) on
     // the host, as the reference forms them
-    std::vector<double> nrm(3 * normal_dirs.size());
-    for (size_t q = 0; q < normal_dirs.size(); ++q) {
-      const NormalDir& r = normal_dirs[q];
-      const BlockDesc& d = ctx->desc[r.b];
-      const int dir = (r.f - 1) / 2;
-      const int fi = r.i + (r.f == 2), fj = r.j + (r.f == 4), fk = r.k + (r.f == 6);
+    auto fetch_normal = [&](int b, int f, int i, int j, int k, double* dst) -> cudaError_t {
+      const BlockDesc& d = ctx->desc[b];
+      const int dir = (f - 1) / 2;
+      const int fi = i + (f == 2), fj = j + (f == 4), fk = k + (f == 6);
       const long long o = (ctx->nd == 3) ? (long long)(fk + GW) * d.plane + (long long)(fj + GW) * d.px + (fi + GW)
                                          : (long long)(fj + GW) * d.px + (fi + GW);
       const double* src = ctx->face.p + 12 * d.mbase + (long long)(4 * dir) * d.vstride + o;
-      CU(cudaMemcpy2DAsync(&nrm[3 * q], sizeof(double), src, d.vstride * sizeof(double), sizeof(double), 3,
-                           cudaMemcpyDeviceToHost, ctx->stream));
+      return cudaMemcpy2DAsync(dst, sizeof(double), src, d.vstride * sizeof(double), sizeof(double), 3,
+                               cudaMemcpyDeviceToHost, ctx->stream);
+    };
+    std::vector<double> nrm(3 * normal_dirs.size()), inrm(3 * inlet_geo.size());
+    for (size_t q = 0; q < normal_dirs.size(); ++q) {
+      const NormalDir& r = normal_dirs[q];
+      CU(fetch_normal(r.b, r.f, r.i, r.j, r.k, &nrm[3 * q]));
+    }
+    for (size_t q = 0; q < inlet_geo.size(); ++q) {
+      const InletGeo& r = inlet_geo[q];
+      CU(fetch_normal(r.b, r.f, r.i, r.j, r.k, &inrm[3 * q]));
     }
     CU(cudaStreamSynchronize(ctx->stream));
     for (size_t q = 0; q < normal_dirs.size(); ++q) {
@@ -665,6 +703,42 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
         const double beta = std::atan(N[2] / (N[0] + 1e-20));
         p.cb = std::cos(beta); p.sb = std::sin(beta);
       }
+    }
+    for (size_t q = 0; q < inlet_geo.size(); ++q) {
+      // Setup_Inflow_Geometry's tangent (Lib_BC_Fluxes_Inflow.f90:537-549):
+      // node (Face_i, Face_j, Face_k) less the node one step back along the
+      // face's two other directions, normalised; then Compute_Inflow_Direction
+      // (:479-496) and the binormal and E1, E2 of :404-420
+      const InletGeo& r = inlet_geo[q];
+      const HostBlock& h = ctx->hblk[r.b];
+      BcParam& p = ctx->hbcp[r.pidx];
+      const double* N = &inrm[3 * q];
+      // Face_Index in the reference's indexing: cells from 1, nodes from 0
+      int ci = r.i + 1, cj = r.j + 1, ck = r.k + 1, di = 0, dj = 0, dk = 0;
+      if (r.f <= 2) { ci -= r.f % 2; dj = 1; dk = 1; }
+      else if (r.f <= 4) { cj -= r.f % 2; di = 1; dk = 1; }
+      else { ck -= r.f % 2; di = 1; dj = 1; }
+      double t[3], bv[3];
+      for (int c = 0; c < 3; ++c) t[c] = nodeh(h, ci, cj, ck, c) - nodeh(h, ci - di, cj - dj, ck - dk, c);
+      const double tmod = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+      for (int c = 0; c < 3; ++c) t[c] = t[c] / tmod;
+      double alpha = r.alpha, beta = r.beta;
+      if (!r.raw) {
+        if (alpha >= 0.5 * 1.7976931348623157e308) alpha = std::atan(N[1] / (N[0] + 1e-20));
+        if (beta >= 0.5 * 1.7976931348623157e308) beta = std::atan(N[2] / (N[0] + 1e-20));
+      }
+      bv[0] = N[1] * t[2] - N[2] * t[1];
+      bv[1] = N[2] * t[0] - N[0] * t[2];
+      bv[2] = N[0] * t[1] - N[1] * t[0];
+      const double bmod = std::sqrt(bv[0] * bv[0] + bv[1] * bv[1] + bv[2] * bv[2]);
+      for (int c = 0; c < 3; ++c) bv[c] = bv[c] / bmod;
+      const double ta = std::tan(alpha), tb = std::tan(beta);
+      const double XA = N[1] - N[0] * ta, XB = t[1] - t[0] * ta, XC = bv[1] - bv[0] * ta;
+      const double XD = N[2] - N[0] * tb, XE = t[2] - t[0] * tb, XF = bv[2] - bv[0] * tb;
+      const double check = (XC * XE - XF * XB);
+      p.E1 = (XF * XA - XC * XD) / check;
+      p.E2 = (XD * XB - XE * XA) / check;
+      for (int c = 0; c < 3; ++c) { p.tv[c] = t[c]; p.bv[c] = bv[c]; }
     }
     CU(cudaMemcpyAsync(ctx->bcp.p, ctx->hbcp.data(), ctx->hbcp.size() * sizeof(BcParam), cudaMemcpyHostToDevice,
                        ctx->stream));
@@ -1541,11 +1615,12 @@ int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
   for (auto& e : ctx->bc)
     if (e.type == 405) any = true;
   if (!any) return fail(ctx, MOSE_ERR_INVALID, "no 405 inflow faces");
-  // 405 records keep their parameter slots in bc order; 406 records have rel_fac but no mach
+  // every record with a parameter slot (401, 403 - 407) holds it in bc order;
+  // only 405 has a Mach number
   size_t q = 0;
   for (auto& e : ctx->bc) {
     if (e.type == 405) ctx->hbcp[q].mach = mach;
-    if (e.type == 405 || e.type == 406) ++q;
+    if (e.type == 401 || (e.type >= 403 && e.type <= 407)) ++q;
   }
   CU(cudaMemcpyAsync(ctx->bcp.p, ctx->hbcp.data(), ctx->hbcp.size() * sizeof(BcParam), cudaMemcpyHostToDevice,
                      ctx->stream));

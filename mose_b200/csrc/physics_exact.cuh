@@ -775,6 +775,106 @@ __device__ __forceinline__ void bc_outflow(const Gas& g, const double* Bound, do
   F[P] = BC_mdot * (0.5 * vel_sq<NV>(Face) + Face_Enthalpy);
 }
 
+// ---- inlets 401 / 403 / 404 and the ambient far field 407 --------------------
+// The part of Setup_Inflow_Geometry (Lib_BC_Fluxes_Inflow.f90:502-559) that
+// depends on the state: the boundary cell's normal velocity, sound speed and
+// the Riemann invariant toward the face (the tangent and the direction
+// coefficients come precomputed in BcParam).
+struct InGeo {
+  double Un, sign, sound, riem;
+};
+template <int NV>
+__device__ __forceinline__ InGeo inflow_geo(const Gas& g, const double* Q, const double* n, int face) {
+  InGeo G;
+  G.Un = dot_vel<NV>(Q, n);
+  G.sign = (double)(1 - 2 * (face % 2));
+  G.sound = sound(g, Q[0], Q[NV - 1]);
+  G.riem = G.sound + G.sign * 0.5 * (g.gamma - 1.0) * G.Un;
+  return G;
+}
+
+// Compute_Flux_from_Face (Lib_BC_Fluxes_Inflow.f90:565-587) for a face state
+// of density rho and velocity Un3 (n + E1 t + E2 b).
+template <int NV>
+__device__ __forceinline__ void face_state_flux(const Gas& g, double rho, double p, double Un3, const BcParam& bp,
+                                                const double* n, double area, bool known_un, double* F) {
+  constexpr int P = NV - 1;
+  double Face[NV];
+  Face[0] = rho * 1.0;
+  Face[P] = p;
+  const double Ut3 = Un3 * bp.E1, Ub3 = Un3 * bp.E2;
+  for (int d = 0; d < NV - 2; ++d) Face[1 + d] = Un3 * n[d] + Ut3 * bp.tv[d] + Ub3 * bp.bv[d];
+  // Stagn_Inflow takes Un3 as the face's normal velocity; the mass-flux
+  // inlets dot the face velocity with the normal
+  const double Face_Un = known_un ? Un3 : dot_vel<NV>(Face, n);
+  const double Face_T = Face[P] / (g.R * rho);
+  const double Fmass = rho * Face_Un * area;
+  const double Face_Enthalpy = Face[0] / rho * (g.cp * Face_T);
+  F[0] = Face[0] * Face_Un * area;
+  for (int d = 0; d < NV - 2; ++d) F[1 + d] = Fmass * Face[1 + d] + Face[P] * area * n[d];
+  F[P] = Fmass * (0.5 * vel_sq<NV>(Face) + Face_Enthalpy);
+}
+
+// Stagn_Inflow, Lib_BC_Fluxes_Inflow.f90:388-473: total conditions (bp.T =
+// T0, bp.p = p0); p0 relaxes toward the boundary pressure while the
+// quadratic for the face's normal velocity has no real root, at most 1000
+// times.
+template <int NV>
+__device__ __forceinline__ void stagn_inflow(const Gas& g, const double* Prim, const InGeo& G, const BcParam& bp,
+                                             const double* n, double area, double* F) {
+  constexpr int P = NV - 1;
+  const double Gamma = g.gamma;
+  double Discr = -1.0, p0_try = bp.p, Sound0 = 0.0, Coef_D = 0.0, YA = 0.0, YB = 0.0;
+  int iter = 0;
+  while (Discr < 0.0) {
+    iter = iter + 1;
+    const double Face_Rgas = 1.0 * g.R;
+    Sound0 = sqrt(Gamma * Face_Rgas * bp.T);
+    Coef_D = (1.0 + bp.E1 * bp.E1 + bp.E2 * bp.E2) * (Gamma - 1.0) / 2.0;
+    double Coef_C = pow(p0_try / Prim[P], (Gamma - 1.0) / Gamma);
+    const double ratio = G.sound / Sound0;
+    Coef_C = Coef_C * (ratio * ratio);
+    const double hg = (Gamma - 1.0) / 2.0;
+    YA = hg * hg + Coef_C * Coef_D;
+    YB = G.sign * G.riem * hg;
+    const double YC = G.riem * G.riem - Coef_C * (Sound0 * Sound0);
+    Discr = YB * YB - YA * YC;
+    if (Discr < 0.0 && fabs(Discr) < 1e-2) Discr = 0.0;
+    if (Discr < 0.0 && fabs(Discr) > 1e-2) p0_try = bp.rel_fac * p0_try + (1.0 - bp.rel_fac) * Prim[P];
+    if (iter > 1000) {
+      Discr = 0.0;
+      break;
+    }
+  }
+  const double Un_Sign = copysign(1.0, G.Un);
+  const double Un3 = (YB + Un_Sign * sqrt(Discr)) / YA;
+  const double Sound3 = sqrt(Sound0 * Sound0 - Coef_D * (Un3 * Un3));
+  const double p3 = p0_try * pow(Sound3 / Sound0, 2.0 * Gamma / (Gamma - 1.0));
+  const double rho = Gamma * p3 / (Sound3 * Sound3);
+  face_state_flux<NV>(g, rho, p3, Un3, bp, n, area, true, F);
+}
+
+// BC_Inlet_MassFlux_T0 (403, Lib_BC_Fluxes_Inflow.f90:81-159) and
+// BC_Inlet_MassFlux_T (404, :165-236): mass flux bp.p through the face at the
+// boundary cell's pressure, with the total (403) or static (404)
+// temperature bp.T.
+template <int NV>
+__device__ __forceinline__ void mass_flux_inflow(const Gas& g, const double* Prim, const BcParam& bp, const double* n,
+                                                 double area, bool total, double* F) {
+  const double Rgas3 = 0.0 + 1.0 * g.R;
+  const double p3 = Prim[NV - 1];
+  const double BC_g = bp.p;
+  double T3 = bp.T;
+  if (total) {
+    const double cp3 = 0.0 + 1.0 * g.cp;
+    const double X = BC_g * Rgas3 / p3, Y = p3 / (BC_g * Rgas3);
+    T3 = (-cp3 + sqrt(cp3 * cp3 + 2.0 * cp3 * bp.T * (X * X))) * (Y * Y);
+  }
+  const double rho3 = p3 / (Rgas3 * T3);
+  const double Un3 = BC_g / rho3;
+  face_state_flux<NV>(g, rho3, p3, Un3, bp, n, area, false, F);
+}
+
 // ---- state update: Newstate_Conservative (Lib_Newstate.f90:134-160) --------
 template <int NV>
 __device__ __forceinline__ void prim2cons(const Gas& g, const double* Q, double* U) {

@@ -86,8 +86,25 @@ __device__ __noinline__ int boundary_flux(const StageArgs& a, int w, const doubl
       ex::bc_outflow<NV>(g, Q, Un, n, area, a.bcp[bc_param(w)].pback, face, F);
       return ADD_ALL;
     }
+  } else if (code >= BC_STAGIN && code <= BC_FARFIELD) {
+    // 401 / 403 / 404 take the inflow formula where the boundary cell enters
+    // the domain (its test BC_Sign*Un >= 0 rejects); 407 takes the total
+    // conditions there and the back-pressure outflow elsewhere
+    // (Mod_BC_Fluxes.f90:119-185, Lib_BC_Fluxes_FarField.f90:53-69)
+    const BcParam& bp = a.bcp[bc_param(w)];
+    const ex::InGeo G = ex::inflow_geo<NV>(g, Q, n, face);
+    if (!(G.sign * G.Un >= 0.0)) {
+      if (code == BC_STAGIN || code == BC_FARFIELD) ex::stagn_inflow<NV>(g, Q, G, bp, n, area, F);
+      else ex::mass_flux_inflow<NV>(g, Q, bp, n, area, code == BC_MFLUX_T0, F);
+      return ADD_ALL;
+    }
+    if (code == BC_FARFIELD) {
+      ex::bc_outflow<NV>(g, Q, G.Un, n, area, bp.pback, face, F);
+      return ADD_ALL;
+    }
   }
-  // BC_SYM, and the symmetry fallback of 405 / 406 (Mod_BC_Fluxes.f90:168,173)
+  // BC_SYM, and the symmetry fallback of 401 / 403 / 404 / 405 / 406
+  // (Mod_BC_Fluxes.f90:128,148,157,168,173)
   ex::bc_symmetry<RIE, LIM, NV>(g, Q, Qi, dlB, dlI, n, area, face, F);
   return ADD_MOMENTUM;
 }

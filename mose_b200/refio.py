@@ -6,9 +6,11 @@ the GPU path unchanged.
   cell a record line ``b i j k face type`` and, for the types that carry
   data, one list-directed data line.  The records come back in the layout
   of ``mose_gpu_set_bcs``: int32 (b, i, j, k, f, type, bs, is, js, ks, fs,
-  d11, d12, d21, d22) and six doubles (405: mach, T, p, alpha, beta,
-  rel_fac; 406: p_back, rel_fac).  The direction token ``normal`` becomes
-  the largest double, as parse_dir_tok (IO_BC.f90:443-456) does.
+  d11, d12, d21, d22) and six doubles (401: T0, p0, alpha, beta, rel_fac;
+  403 / 404: T0 / T, mass flux, alpha, beta, rel_fac; 405: mach, T, p, alpha,
+  beta, rel_fac; 406: p_back, rel_fac; 407: T0, p0, p_back, alpha, beta,
+  rel_fac).  The direction token ``normal`` becomes the largest double, as
+  parse_dir_tok (IO_BC.f90:443-456) does.
 * ``read_tecplot`` reads ordered Tecplot ASCII zones with BLOCK data packing
   (the ORION format of MESH/*.tec and INPUT/ic*.tec): node variables on the
   (I, J, K) nodes and, with VARLOCATION, cell-centred variables on the
@@ -76,6 +78,12 @@ def read_bc(path) -> tuple[np.ndarray, np.ndarray]:
         elif t == 406:
             g = _fields(lines[q]); q += 1
             d[0], d[1] = _num(g[0]), _num(g[1])
+        elif t in (401, 403, 404):         # T0 (T), p0 (mass flux), alpha, beta, rel_fac, ci...
+            g = _fields(lines[q]); q += 1
+            d = [_num(g[0]), _num(g[1]), _dir_tok(g[2]), _dir_tok(g[3]), _num(g[4]), 0.0]
+        elif t == 407:                     # T0, p0, p_back, alpha, beta, rel_fac, ci...
+            g = _fields(lines[q]); q += 1
+            d = [_num(g[0]), _num(g[1]), _num(g[2]), _dir_tok(g[3]), _dir_tok(g[4]), _num(g[5])]
         elif t == 102:
             g = _fields(lines[q]); q += 1
             q += int(g[0]) + int(g[1])        # donor lines

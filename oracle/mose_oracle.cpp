@@ -1421,20 +1421,11 @@ bool BC_Inlet_Supersonic(const orc_domain* D, int Im, int Jm, int Km, int Fm, Bl
   return true;
 }
 
-// BC_Outflow + Outflow, Lib_BC_Fluxes_Outflow.f90:12-129.
-bool BC_Outflow(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const double* data) {
-  const Thermo& t = D->th;
-  double BC_pexit = data[0];
-  int modfm, modfm1, modfm2, dir, fi, fj, fk;
-  compute_modfm(Fm, modfm, modfm1, modfm2);
-  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
-  const double* Bound = blk.Pc(Im, Jm, Km);
-  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
-  double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
-  double BC_Sign = (double)modfm2;
+// Outflow, Lib_BC_Fluxes_Outflow.f90:59-129: the face flux of an outflow
+// face with back pressure BC_pexit (0: extrapolation of every variable).
+void Outflow(const Thermo& t, const double* Bound, double BC_Sign, double Un, const double* Normal, double Area,
+             double BC_pexit, double* Flux) {
   double bvel[3] = {Bound[NU], Bound[NV], Bound[NW]};
-  double Un = dot3(bvel, Normal);
-  if (BC_Sign * Un < 0.0) return false;
   double Bound_rho, Bound_Rgas;
   co_rotot_Rtot(t, Bound[0], Bound_rho, Bound_Rgas);
   double Bound_Sound = f_ss(t, Bound[0], Bound[NP], Bound_rho, Bound_Rgas);
@@ -1468,14 +1459,227 @@ bool BC_Outflow(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk,
   (void)Face_Sound;
   double Face_T = Face[NP] / (Face_Rgas * Face_rho);
   double Face_Enthalpy = Face[0] / Face_rho * (t.cp * Face_T);
-  double Flux[NPRIM];
   Flux[0] = Face[0] * Area * Face_Un;
   double BC_mdot = Face_rho * Area * Face_Un;
   for (int q = 0; q < 3; ++q) Flux[NU + q] = Face[NU + q] * BC_mdot + Face[NP] * Area * Normal[q];
   Flux[NP] = BC_mdot * (0.5 * (Face[NU] * Face[NU] + Face[NV] * Face[NV] + Face[NW] * Face[NW]) + Face_Enthalpy);
+}
+
+// BC_Outflow, Lib_BC_Fluxes_Outflow.f90:12-56.  Returns false when
+// BC_Sign*Un < 0 (the caller falls back to symmetry).
+bool BC_Outflow(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const double* data) {
+  int modfm, modfm1, modfm2, dir, fi, fj, fk;
+  compute_modfm(Fm, modfm, modfm1, modfm2);
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const double* Bound = blk.Pc(Im, Jm, Km);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  double BC_Sign = (double)modfm2;
+  double bvel[3] = {Bound[NU], Bound[NV], Bound[NW]};
+  double Un = dot3(bvel, Normal);
+  if (BC_Sign * Un < 0.0) return false;
+  double Flux[NPRIM];
+  Outflow(D->th, Bound, BC_Sign, Un, Normal, Area, data[0], Flux);
   double* r = blk.Rc(Im, Jm, Km);
   for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + (double)modfm2 * Flux[v];
   return true;
+}
+
+// ---- inlets 401 / 403 / 404 and the ambient far field 407 --------------------
+// Setup_Inflow_Geometry, Lib_BC_Fluxes_Inflow.f90:502-559: the boundary face's
+// normal and area, the unit tangent t (the face diagonal between two of its
+// nodes), the boundary cell's state, Un and the Riemann invariant toward the
+// face.
+struct InflowGeo {
+  const double* Normal;
+  double Area, t_Vec[3], BC_Sign, Un, Sound, Gamma, Riem;
+  const double* Bound;
+  int modfm2;
+};
+
+InflowGeo Setup_Inflow_Geometry(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk) {
+  const Thermo& t = D->th;
+  InflowGeo g;
+  int modfm, modfm1, dir, fi, fj, fk;
+  compute_modfm(Fm, modfm, modfm1, g.modfm2);
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  g.Bound = blk.Pc(Im, Jm, Km);
+  g.Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  g.Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  const double* a = blk.nodep(fi, fj, fk);
+  const double* b = (Fm <= 2) ? blk.nodep(fi, fj - 1, fk - 1)
+                  : (Fm <= 4) ? blk.nodep(fi - 1, fj, fk - 1)
+                              : blk.nodep(fi - 1, fj - 1, fk);
+  for (int q = 0; q < 3; ++q) g.t_Vec[q] = a[q] - b[q];
+  double t_Mod = norm2(g.t_Vec[0], g.t_Vec[1], g.t_Vec[2]);
+  for (int q = 0; q < 3; ++q) g.t_Vec[q] = g.t_Vec[q] / t_Mod;
+  g.BC_Sign = (double)g.modfm2;
+  double bvel[3] = {g.Bound[NU], g.Bound[NV], g.Bound[NW]};
+  g.Un = dot3(bvel, g.Normal);
+  double rho, Rgas;
+  co_rotot_Rtot(t, g.Bound[0], rho, Rgas);
+  g.Sound = f_ss(t, g.Bound[0], g.Bound[NP], rho, Rgas);
+  g.Gamma = t.gamma;
+  g.Riem = g.Sound + g.BC_Sign * 0.5 * (g.Gamma - 1.0) * g.Un;
+  return g;
+}
+
+// Compute_Inflow_Direction, Lib_BC_Fluxes_Inflow.f90:479-496: the token
+// 'normal' (read as the largest double) takes the angle of the face normal.
+void inflow_direction(const double* Normal, double alpha_in, double beta_in, double& alpha, double& beta) {
+  alpha = (alpha_in >= 0.5 * 1.7976931348623157e308) ? std::atan(Normal[1] / (Normal[0] + 1e-20)) : alpha_in;
+  beta = (beta_in >= 0.5 * 1.7976931348623157e308) ? std::atan(Normal[2] / (Normal[0] + 1e-20)) : beta_in;
+}
+
+// The binormal b = n x t / |n x t| and the tangential-to-normal velocity
+// ratios E1, E2 that make the face velocity Un (n + E1 t + E2 b) point along
+// (alpha, beta) (Lib_BC_Fluxes_Inflow.f90:113-129, 197-213, 404-420).
+void inflow_E(const double* Normal, const double* t_Vec, double alpha, double beta, double* b_Vec, double& E1,
+              double& E2) {
+  b_Vec[0] = Normal[1] * t_Vec[2] - Normal[2] * t_Vec[1];
+  b_Vec[1] = Normal[2] * t_Vec[0] - Normal[0] * t_Vec[2];
+  b_Vec[2] = Normal[0] * t_Vec[1] - Normal[1] * t_Vec[0];
+  double b_Mod = norm2(b_Vec[0], b_Vec[1], b_Vec[2]);
+  for (int q = 0; q < 3; ++q) b_Vec[q] = b_Vec[q] / b_Mod;
+  double ta = std::tan(alpha), tb = std::tan(beta);
+  double XA = Normal[1] - Normal[0] * ta;
+  double XB = t_Vec[1] - t_Vec[0] * ta;
+  double XC = b_Vec[1] - b_Vec[0] * ta;
+  double XD = Normal[2] - Normal[0] * tb;
+  double XE = t_Vec[2] - t_Vec[0] * tb;
+  double XF = b_Vec[2] - b_Vec[0] * tb;
+  double check = (XC * XE - XF * XB);
+  E1 = (XF * XA - XC * XD) / check;
+  E2 = (XD * XB - XE * XA) / check;
+}
+
+// Compute_Flux_from_Face, Lib_BC_Fluxes_Inflow.f90:565-587 (one species).
+void Flux_from_Face(const Thermo& t, const double* Face, double Face_rho, double Face_Rgas, double Area,
+                    const double* Normal, double* Flux) {
+  double fvel[3] = {Face[NU], Face[NV], Face[NW]};
+  double Face_Un = dot3(fvel, Normal);
+  double Face_T = Face[NP] / (Face_Rgas * Face_rho);
+  double Fmass = Face_rho * Face_Un * Area;
+  double Face_Enthalpy = 0.0 + Face[0] / Face_rho * (t.cp * Face_T);
+  Flux[0] = Face[0] * Face_Un * Area;
+  for (int q = 0; q < 3; ++q) Flux[NU + q] = Fmass * Face[NU + q] + Face[NP] * Area * Normal[q];
+  Flux[NP] = Fmass * (0.5 * (Face[NU] * Face[NU] + Face[NV] * Face[NV] + Face[NW] * Face[NW]) + Face_Enthalpy);
+}
+
+// Stagn_Inflow, Lib_BC_Fluxes_Inflow.f90:388-473: the face state compatible
+// with the interior Riemann invariant and the total conditions (T0, p0); p0
+// relaxes toward the boundary pressure while the quadratic for Un has no
+// real root (at most 1000 tries).
+void Stagn_Inflow(const Thermo& t, const InflowGeo& g, double alpha, double beta, double BC_T0, double BC_p0,
+                  double BC_rel_fac, double* Flux) {
+  const double* Prim = g.Bound;
+  const double Gamma = g.Gamma, Riem = g.Riem, Sound = g.Sound;
+  double b_Vec[3], E1, E2;
+  inflow_E(g.Normal, g.t_Vec, alpha, beta, b_Vec, E1, E2);
+  double Discr = -1.0, BC_p0_try = BC_p0, Face_Rgas = 0.0, Sound0 = 0.0, Coef_D = 0.0, Coef_C, YA = 0.0, YB = 0.0, YC;
+  int iter_discr = 0;
+  while (Discr < 0.0) {
+    iter_discr = iter_discr + 1;
+    Face_Rgas = 1.0 * t.R;                           // sum(BC_ci*Ri_tab), ci = 1
+    Sound0 = std::sqrt(Gamma * Face_Rgas * BC_T0);
+    Coef_D = (1.0 + E1 * E1 + E2 * E2) * (Gamma - 1.0) / 2.0;
+    Coef_C = std::pow(BC_p0_try / Prim[NP], (Gamma - 1.0) / Gamma);
+    Coef_C = Coef_C * ((Sound / Sound0) * (Sound / Sound0));
+    YA = ((Gamma - 1.0) / 2.0) * ((Gamma - 1.0) / 2.0) + Coef_C * Coef_D;
+    YB = g.BC_Sign * Riem * ((Gamma - 1.0) / 2.0);
+    YC = Riem * Riem - Coef_C * (Sound0 * Sound0);
+    Discr = YB * YB - YA * YC;
+    if (Discr < 0.0 && std::fabs(Discr) < 1e-2) Discr = 0.0;
+    if (Discr < 0.0 && std::fabs(Discr) > 1e-2) BC_p0_try = BC_rel_fac * BC_p0_try + (1.0 - BC_rel_fac) * Prim[NP];
+    if (iter_discr > 1000) {
+      Discr = 0.0;
+      break;
+    }
+  }
+  double Un_Sign = std::copysign(1.0, g.Un);
+  double Un3 = (YB + Un_Sign * std::sqrt(Discr)) / YA;
+  double Sound3 = std::sqrt(Sound0 * Sound0 - Coef_D * (Un3 * Un3));
+  double p3 = BC_p0_try * std::pow(Sound3 / Sound0, 2.0 * Gamma / (Gamma - 1.0));
+  double Ut3 = Un3 * E1, Ub3 = Un3 * E2;
+  double Face[NPRIM];
+  Face[NP] = p3;
+  double Face_rho = Gamma * Face[NP] / (Sound3 * Sound3);
+  Face[0] = 1.0 * Face_rho;
+  for (int q = 0; q < 3; ++q) Face[NU + q] = Un3 * g.Normal[q] + Ut3 * g.t_Vec[q] + Ub3 * b_Vec[q];
+  double Face_T = Face[NP] / (Face_Rgas * Face_rho);
+  double Face_Enthalpy = 0.0 + Face[0] / Face_rho * (t.cp * Face_T);
+  Flux[0] = Face[0] * Un3 * g.Area;
+  double Fmass = Face_rho * Un3 * g.Area;
+  for (int q = 0; q < 3; ++q) Flux[NU + q] = Fmass * Face[NU + q] + Face[NP] * g.Area * g.Normal[q];
+  Flux[NP] = Fmass * (0.5 * (Face[NU] * Face[NU] + Face[NV] * Face[NV] + Face[NW] * Face[NW]) + Face_Enthalpy);
+}
+
+void add_bc_flux(Block& blk, int Im, int Jm, int Km, int modfm2, const double* Flux) {
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + (double)modfm2 * Flux[v];
+}
+
+// BC_Inlet_StagnCond, Lib_BC_Fluxes_Inflow.f90:19-75 (no rotating frame).
+// data: T0, p0, alpha, beta, rel_fac.  False when BC_Sign*Un >= 0.
+bool BC_Inlet_StagnCond(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const double* data) {
+  InflowGeo g = Setup_Inflow_Geometry(D, Im, Jm, Km, Fm, blk);
+  if (g.BC_Sign * g.Un >= 0.0) return false;
+  double alpha, beta;
+  inflow_direction(g.Normal, data[2], data[3], alpha, beta);
+  double Flux[NPRIM];
+  Stagn_Inflow(D->th, g, alpha, beta, data[0], data[1], data[4], Flux);
+  add_bc_flux(blk, Im, Jm, Km, g.modfm2, Flux);
+  return true;
+}
+
+// BC_Inlet_MassFlux_T0 (403, :81-159) and BC_Inlet_MassFlux_T (404,
+// :165-236): the mass flux g through the face at the boundary cell's
+// pressure, with the total (403) or static (404) temperature.  data: T0 or T,
+// g, alpha, beta, rel_fac.  False when BC_Sign*Un >= 0.
+bool BC_Inlet_MassFlux(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const double* data,
+                       bool total) {
+  const Thermo& t = D->th;
+  InflowGeo g = Setup_Inflow_Geometry(D, Im, Jm, Km, Fm, blk);
+  if (g.BC_Sign * g.Un >= 0.0) return false;
+  double alpha, beta, b_Vec[3], E1, E2;
+  inflow_direction(g.Normal, data[2], data[3], alpha, beta);
+  inflow_E(g.Normal, g.t_Vec, alpha, beta, b_Vec, E1, E2);
+  const double BC_T = data[0], BC_g = data[1];
+  double Rgas3 = 0.0 + 1.0 * t.R;
+  double p3 = g.Bound[NP];
+  double T3;
+  if (total) {
+    double cp3 = 0.0 + 1.0 * t.cp;
+    double X = BC_g * Rgas3 / p3, Y = p3 / (BC_g * Rgas3);
+    T3 = (-cp3 + std::sqrt(cp3 * cp3 + 2.0 * cp3 * BC_T * (X * X))) * (Y * Y);
+  } else {
+    T3 = BC_T;
+  }
+  double rho3 = p3 / (Rgas3 * T3);
+  double Un3 = BC_g / rho3;
+  double Ut3 = Un3 * E1, Ub3 = Un3 * E2;
+  double Face[NPRIM];
+  Face[0] = rho3 * 1.0;
+  for (int q = 0; q < 3; ++q) Face[NU + q] = Un3 * g.Normal[q] + Ut3 * g.t_Vec[q] + Ub3 * b_Vec[q];
+  Face[NP] = p3;
+  double Flux[NPRIM];
+  Flux_from_Face(t, Face, rho3, Rgas3, g.Area, g.Normal, Flux);
+  add_bc_flux(blk, Im, Jm, Km, g.modfm2, Flux);
+  return true;
+}
+
+// BC_FarField, Lib_BC_Fluxes_FarField.f90:19-73 (no rotating frame): the
+// back-pressure outflow where the boundary cell leaves the domain, the total
+// conditions where it enters (its angles are used as given).  data: T0, p0,
+// p_back, alpha, beta, rel_fac.
+void BC_FarField(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const double* data) {
+  InflowGeo g = Setup_Inflow_Geometry(D, Im, Jm, Km, Fm, blk);
+  double Flux[NPRIM];
+  if (g.BC_Sign * g.Un >= 0.0)
+    Outflow(D->th, g.Bound, g.BC_Sign, g.Un, g.Normal, g.Area, data[2], Flux);
+  else
+    Stagn_Inflow(D->th, g, data[3], data[4], data[0], data[1], data[5], Flux);
+  add_bc_flux(blk, Im, Jm, Km, g.modfm2, Flux);
 }
 
 }  // namespace
@@ -1542,7 +1746,8 @@ int orc_set_bcs(orc_domain* d, const int32_t* rec, const double* data, int nboun
     lastkey = key;
     d->n_bf[key] += 1;
     switch (e.type) {
-      case 0: case 101: case 201: case 300: case 400: case 405: case 406: break;
+      case 0: case 101: case 201: case 300: case 400: case 401: case 403: case 404: case 405: case 406: case 407:
+        break;
       default: return ORC_ERR_UNSUPPORTED;
     }
     if (e.type == 101 || e.type == 201) {
@@ -1772,6 +1977,14 @@ int orc_bc_fluxes(orc_domain* d) {
           case 406:
             if (!BC_Outflow(d, e.i, e.j, e.k, e.f, bm, e.data)) BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
             break;
+          case 401:
+            if (!BC_Inlet_StagnCond(d, e.i, e.j, e.k, e.f, bm, e.data)) BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            break;
+          case 403: case 404:
+            if (!BC_Inlet_MassFlux(d, e.i, e.j, e.k, e.f, bm, e.data, e.type == 403))
+              BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            break;
+          case 407: BC_FarField(d, e.i, e.j, e.k, e.f, bm, e.data); break;
           default: break;
         }
       }

@@ -294,3 +294,49 @@ def test_irs_stage_matches_numpy_restatement(oracle_mod):
         e = U[..., 4] / rho - 0.5 * (u * u + v * v + w * w)
         want = np.stack([rho, u, v, w, rho * Rg * (e / cv)], -1)
         np.testing.assert_allclose(o.get_prim(b + 1)[2, g2, g2], want, rtol=1e-13, atol=1e-14)
+
+
+@pytest.mark.parametrize("btype", [401, 403, 404, 407])
+def test_inlet_boundaries_hold_the_inflow(oracle_mod, btype):
+    """The inlet formulas (401 / 403 / 404 / 407) on the curvilinear Mach-0.8
+    channel, fed with the free stream's own total or static conditions, keep
+    it: after 60 steps the state is finite and the mean density and
+    velocity of the four cell columns next to the inflow face stay within a
+    few percent of the free stream."""
+    g, m = 1.4, 0.8
+    p_inf = 1.0 / g
+    t0 = p_inf * (1 + 0.5 * (g - 1) * m * m)
+    p0 = p_inf * (1 + 0.5 * (g - 1) * m * m) ** (g / (g - 1))
+    data = {401: [t0, p0, 0.0, 0.0, 1.0, 0.0], 403: [t0, m, 0.0, 0.0, 1.0, 0.0],
+            404: [p_inf, m, 0.0, 0.0, 1.0, 0.0], 407: [t0, p0, p_inf, 0.0, 0.0, 1.0]}[btype]
+    case = cases.curvilinear_channel(24, steps=1)
+    f1 = case.bc_rec[:, 5] == 405
+    case.bc_rec[f1, 5] = btype
+    case.bc_data[f1] = data
+    o = oracle_mod.Oracle(case)
+    for _ in range(60):
+        o.step()
+    P = o.get_prim(1)[2, 2:-2, 2:-2]
+    assert np.isfinite(P).all()
+    near = P[:, :4]
+    assert abs(near[..., 0].mean() - 1.0) < 0.05 and abs(near[..., 1].mean() - m) < 0.05 * m, near.mean(axis=(0, 1))
+
+
+def test_far_field_outflow_branch_is_the_406_formula(oracle_mod):
+    """Where the boundary cell leaves the domain, 407 takes the back-pressure
+    outflow of 406 (Lib_BC_Fluxes_FarField.f90:53-55): the same outflow face
+    as 407 or as 406 with the same back pressure gives the same residual."""
+    g = 1.4
+    p_inf = 1.0 / g
+    res = []
+    for rec_type, row in ((406, [p_inf, 1.0, 0.0, 0.0, 0.0, 0.0]), (407, [2.0, 2.0, p_inf, 0.0, 0.0, 1.0])):
+        case = cases.perturbed_channel(16, steps=1, amp=0.02, seed=1)
+        f2 = case.bc_rec[:, 5] == 406
+        case.bc_rec[f2, 5] = rec_type
+        case.bc_data[f2] = row
+        o = oracle_mod.Oracle(case)
+        o.fill_ghost_cell()
+        o.fluxes()
+        o.bc_fluxes()
+        res.append(o.get_residual(1))
+    assert np.array_equal(res[0], res[1])

@@ -94,3 +94,23 @@ def test_reference_inputs_match_fixtures(name, res, fixture):
     assert np.array_equal(c.prim[0], d["prim"])
     assert np.array_equal(c.bc_rec, d["bc_rec"])
     assert c.cfl == float(d["cfl"]) and c.t_end == float(d["t_end"])
+
+
+def test_inlet_records_read(tmp_path):
+    """401 / 403 / 404 / 407 data lines: the numbers in the bc_data layout,
+    the token 'normal' as the largest double, species fractions dropped."""
+    text = "\n".join([
+        "1 1 1 1 1 401", "1.2, 0.95, normal, 0.0, 0.9, 1.0",
+        "1 1 2 1 1 403", "1.15 0.8d0 0.1 normal 1.0 1.0",
+        "1 1 3 1 1 404", "0.71 -0.8 0.0 0.0 1.0 1.0",
+        "1 2 1 1 2 407", "1.2 0.95 0.71 0.05 0.0 0.7 1.0",
+    ]) + "\n"
+    path = tmp_path / "bc.txt"
+    path.write_text(text)
+    rec, data = refio.read_bc(path)
+    huge = np.finfo(np.float64).max
+    assert rec[:, 5].tolist() == [401, 403, 404, 407]
+    np.testing.assert_array_equal(data[0], [1.2, 0.95, huge, 0.0, 0.9, 0.0])
+    np.testing.assert_array_equal(data[1], [1.15, 0.8, 0.1, huge, 1.0, 0.0])
+    np.testing.assert_array_equal(data[2], [0.71, -0.8, 0.0, 0.0, 1.0, 0.0])
+    np.testing.assert_array_equal(data[3], [1.2, 0.95, 0.71, 0.05, 0.0, 0.7])
