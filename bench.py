@@ -163,7 +163,8 @@ def run_reference(args):
     cores = os.cpu_count() or 1
     case = workload_case(N_CELLS_SIDE, steps=1)
     o = pyoracle.Oracle(case, nthreads=cores, omp=True)
-    for _ in range(min(args.warmup, 1)):
+    nwarm = max(1, min(args.warmup, 3))       # CPU steps of ~0.3 s: a few warm the caches and threads
+    for _ in range(nwarm):
         o.step()
     # each step is one full RK3 step of the 2048^2 block; bound the count so the run stays within minutes
     t0 = time.perf_counter()
@@ -175,7 +176,7 @@ def run_reference(args):
     el = time.perf_counter() - t0
     value = case.ncells * steps / el
     line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
-            "n_gpus": world, "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * el / steps,
+            "n_gpus": world, "steps": steps, "warmup": nwarm, "ms_per_step": 1e3 * el / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(case, "fp64 (CPU oracle)"), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "port",
