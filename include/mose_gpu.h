@@ -81,7 +81,9 @@ enum {
   MOSE_RIEMANN_AUSMP_UP = 9,   /* 'AUSM+-up'  (Lib_Riemann_AUSM.f90:273-418), needs Minf */
   MOSE_RIEMANN_AUSMP_UP2 = 10, /* 'AUSM+-up2' (Lib_Riemann_AUSM.f90:455-570), needs Minf */
   MOSE_RIEMANN_HLLC_SD = 11,   /* 'HLLC+'  (Lib_Riemann_HLL.f90:500-534), shock detector */
-  MOSE_RIEMANN_HLLE_PP = 12    /* 'HLLE++' (Lib_Riemann_HLL.f90:320-464), shock detector */
+  MOSE_RIEMANN_HLLE_PP = 12,   /* 'HLLE++' (Lib_Riemann_HLL.f90:320-464), shock detector */
+  MOSE_RIEMANN_HLLC_ROT = 13,  /* 'HLLC Rotated' (Lib_Riemann_HLL.f90:672-755) */
+  MOSE_RIEMANN_EXACT = 14      /* 'exact' (Lib_Riemann_Godunov.f90:10-224) */
 };
 
 /* Arithmetic of the face sweeps and of the fused steps' CFL pass.  In the

@@ -28,7 +28,8 @@ NPRIM = 5
 # limiter / riemann names as in input.ini (Register_Numerics.f90:57-72)
 LIMITERS = {"first-order": 0, "none": 0, "minmod": 1, "vanleer": 2, "vanalbada": 3, "mc": 4, "superbee": 5}
 RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3, "HLLE": 4, "HLLEM": 5, "LLF": 6, "Rusanov": 6,
-           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10, "HLLC+": 11, "HLLE++": 12}
+           "PLLF": 7, "Hanel": 8, "AUSM+-up": 9, "AUSM+-up2": 10, "HLLC+": 11, "HLLE++": 12,
+           "HLLC Rotated": 13, "exact": 14, "Exact": 14}
 
 
 @dataclass

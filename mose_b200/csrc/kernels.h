@@ -95,6 +95,10 @@ MOSE_STAGE_DECL(2, 0) MOSE_STAGE_DECL(2, 1) MOSE_STAGE_DECL(2, 2) MOSE_STAGE_DEC
 // Solvers 4.. (HLLE, HLLEM, LLF, PLLF, Hanel, AUSM+-up, AUSM+-up2, HLLC+,
 // HLLE++) share one unit per precision that selects the solver at run time
 // (Gas::rie); with a shock detector (Gas::sd) every solver runs there.
+// 2-D (and 1-D): every solver index (the compute-time units 0-3, the run-time
+// unit for the rest) in every precision.  Setup refuses what this rejects,
+// so a set-up context always has its stage kernel.
+inline bool stage2d_supported(int rie, int prec) { return prec >= 0 && prec <= 2 && rie >= 0 && rie <= 14; }
 inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int prec, int rie, int lim,
                            cudaStream_t s) {
   using L = bool (*)(const StageArgs&, int, int, bool, int, cudaStream_t);
@@ -102,7 +106,7 @@ inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int 
       {launch_stage2d_p0_r0, launch_stage2d_p0_r1, launch_stage2d_p0_r2, launch_stage2d_p0_r3, launch_stage2d_p0_r4},
       {launch_stage2d_p1_r0, launch_stage2d_p1_r1, launch_stage2d_p1_r2, launch_stage2d_p1_r3, launch_stage2d_p1_r4},
       {launch_stage2d_p2_r0, launch_stage2d_p2_r1, launch_stage2d_p2_r2, launch_stage2d_p2_r3, launch_stage2d_p2_r4}};
-  if (prec < 0 || prec > 2 || rie < 0 || rie > 12) return false;
+  if (!stage2d_supported(rie, prec)) return false;
   // the shock detector lives in the run-time solver unit, which serves every solver
   return table[prec][(rie < 4 && a.g.sd == 0) ? rie : 4](a, nsm, mode, uni, lim, s);
 }

@@ -337,7 +337,7 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   *out = nullptr;
   if (cfg->abi_version != MOSE_GPU_ABI_VERSION) return MOSE_ERR_INVALID;
   if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 || cfg->integration != MOSE_INTEGRATION_CONS ||
-      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > MOSE_RIEMANN_HLLE_PP ||
+      cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > MOSE_RIEMANN_EXACT ||
       cfg->precision < 0 || cfg->precision > 2 || !(cfg->gamma > 1.0) || !(cfg->rgas > 0.0))
     return MOSE_ERR_UNSUPPORTED;
   ctx = new mose_gpu_ctx();
@@ -482,6 +482,9 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");
   if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: HLLC or AUSM+ with minmod, van Leer or van Albada");
+  if (ctx->nd != 3 && !stage2d_supported(ctx->cfg.riemann, ctx->cfg.precision))
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "no stage kernel for riemann %d in precision %d", ctx->cfg.riemann,
+                ctx->cfg.precision);
   auto nodeh = [&](const HostBlock& h, int i, int j, int k, int c) {
     return h.node[3 * ((size_t)i + (size_t)(h.ni + 1) * ((size_t)j + (size_t)(h.nj + 1) * k)) + c];
   };

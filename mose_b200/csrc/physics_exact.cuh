@@ -559,6 +559,153 @@ __device__ __forceinline__ double sd_tramel2(double p, double p1, double p2, dou
   return 0.0;
 }
 
+// riemann_HLLCHLLE ('HLLC Rotated'), Lib_Riemann_HLL.f90:672-755: HLLE along
+// n1, the direction of the velocity jump, and HLLC along n2 = (-n1y, n1x,
+// n1z), weighted by the (non-negative) projections of the face normal on
+// them; HLLC along the normal where the jump is negligible.
+template <int NV>
+__device__ __forceinline__ void hllc_rot(const Gas& g, const double* Lq, double aL, const double* Rq, double aR,
+                                         const double* n, double* F) {
+  const St3 L = st3<NV>(Lq, aL), R = st3<NV>(Rq, aR);
+  const double nx = n[0], ny = n[1], nz = (NV == 5) ? n[2] : 0.0;
+  const double du = R.u - L.u, dv = R.v - L.v, dw = R.w - L.w;
+  const double abs_dv = sqrt(du * du + dv * dv + dw * dw);
+  const double dum = 0.5 * (umag3(L) + umag3(R));
+  if (!(abs_dv / (dum + 1.0e-10) > 1.0e-12)) {
+    hllc<NV>(g, Lq, aL, Rq, aR, n, F);
+    return;
+  }
+  double nx1 = du / abs_dv, ny1 = dv / abs_dv, nz1 = dw / abs_dv;
+  double alfa1 = nx * nx1 + ny * ny1 + nz * nz1;
+  const double s1 = copysign(1.0, alfa1);
+  nx1 = s1 * nx1; ny1 = s1 * ny1; nz1 = s1 * nz1; alfa1 = s1 * alfa1;
+  double n2[3] = {-ny1, nx1, nz1};
+  double alfa2 = nx * n2[0] + ny * n2[1] + nz * n2[2];
+  const double s2 = copysign(1.0, alfa2);
+  n2[0] = s2 * n2[0]; n2[1] = s2 * n2[1]; n2[2] = s2 * n2[2]; alfa2 = s2 * alfa2;
+  if (nz > 0.1) {
+    alfa1 = 0.0;
+    n2[0] = nx; n2[1] = ny; n2[2] = nz;
+    alfa2 = 1.0;
+  }
+  const Fl5 E = hlle3(g, L, R, nx1, ny1, nz1);
+  double C[NV];
+  hllc<NV>(g, Lq, aL, Rq, aR, n2, C);
+  F[0] = E.r * alfa1 + C[0] * alfa2;
+  F[1] = E.u * alfa1 + C[1] * alfa2;
+  F[2] = E.v * alfa1 + C[2] * alfa2;
+  if constexpr (NV == 5) {
+    double fw = E.w * alfa1 + C[3] * alfa2;
+    if (fw != 0.0 && fabs(nz) <= 1.0e-10) fw = 0.0;
+    F[3] = fw;
+    F[4] = E.E * alfa1 + C[4] * alfa2;
+  } else {
+    F[3] = E.E * alfa1 + C[3] * alfa2;
+  }
+}
+
+// riemann_exact ('exact'), Lib_Riemann_Godunov.f90:10-224: Newton iteration
+// on the contact velocity (relative pressure tolerance 1e-5, at most 1001
+// iterations) with the shock or rarefaction relation of each side
+// (shockleft / rareleft / shockright / rareright, :153-224), then the
+// Godunov state sampled at the face.  The sampling reads the wave speeds of
+// the last iteration that set them (0 before).  Its energy flux carries the
+// normal kinetic energy only, H0(p, rho, |u_n|), as the reference's does.
+__device__ __forceinline__ Fl5 exact3(const Gas& g, const St3& L, const St3& R, double nx, double ny, double nz) {
+  const double gam = g.gamma;
+  const double p1 = L.p, a1 = L.a, p4 = R.p, a4 = R.a;
+  const double gm1 = gam - 1.0;
+  const double delta = 0.5 * gm1;
+  const double eta = gam / delta;
+  const double un1 = L.u * nx + L.v * ny + L.w * nz;
+  const double ut1 = L.u - un1 * nx, vt1 = L.v - un1 * ny, wt1 = L.w - un1 * nz;
+  const double un4 = R.u * nx + R.v * ny + R.w * nz;
+  const double ut4 = R.u - un4 * nx, vt4 = R.v - un4 * ny, wt4 = R.w - un4 * nz;
+  const double R2I = un1 + (2.0 / gm1) * a1;
+  const double R1IV = un4 - (2.0 / gm1) * a4;
+  const double dum = gm1 / (2.0 * gam);
+  const double z = (gm1 / gm1) * (a4 / a1) * pow(p1 / p4, dum);
+  double vel = (z * R2I + R1IV) / (1.0 + z);
+  // rareleft / rareright: delta = .5 (gamma - 1), exponent 2 gamma / (gamma - 1)
+  const double rdelta = 0.5 * (gam - 1.0);
+  const double dum1 = 2.0 * gam / (gam - 1.0);
+  double p3 = 1.0, p2 = 2.0 * p3, a2 = 0.0, a3 = 0.0;
+  double swl = 0.0, swr = 0.0, vw1 = 0.0, vw2 = 0.0, vw3 = 0.0, vw4 = 0.0;
+  int iter = 0;
+  while (fabs(1.0 - (p2 / p3)) >= 1e-5 && iter <= 1000) {
+    double dpr, dpl;
+    if (vel < un1) {                 // shockleft(un1, a1, p1, vel, a2, p2, dpr, swl)
+      const double x1 = (gam + 1.0) * (vel - un1) / (4.0 * a1);
+      const double M = x1 - sqrt(1.0 + x1 * x1);
+      const double C1 = gam * p1 / a1;
+      p2 = p1 + C1 * (vel - un1) * M;
+      dpr = 2.0 * C1 * pow(M, 3.0) / (1.0 + M * M);
+      const double rpd = p2 / p1;
+      swl = un1 + a1 * M;
+      a2 = a1 * sqrt((gam + 1.0 + (gam - 1.0) * rpd) / (gam + 1.0 + (gam - 1.0) / rpd));
+    } else {                         // rareleft(p1, a1, un1, vel, p2, a2, dpr, vw1, vw2)
+      a2 = a1 - rdelta * (vel - un1);
+      p2 = p1 * pow(a2 / a1, dum1);
+      dpr = -(gam * p2 / a2);
+      vw1 = un1 - a1;
+      vw2 = vel - a2;
+    }
+    if (vel > un4) {                 // shockright(un4, a4, p4, vel, a3, p3, dpl, swr)
+      const double x4 = (gam + 1.0) * (vel - un4) / (4.0 * a4);
+      const double M = x4 + sqrt(1.0 + x4 * x4);
+      const double C4 = gam * p4 / a4;
+      p3 = p4 + C4 * (vel - un4) * M;
+      dpl = 2.0 * C4 * pow(M, 3.0) / (1.0 + M * M);
+      const double rps = p3 / p4;
+      swr = un4 + a4 * M;
+      a3 = a4 * sqrt((gam + 1.0 + (gam - 1.0) * rps) / (gam + 1.0 + (gam - 1.0) / rps));
+    } else {                         // rareright(p4, a4, un4, vel, p3, a3, dpl, vw3, vw4)
+      a3 = a4 + rdelta * (vel - un4);
+      p3 = p4 * pow(a3 / a4, dum1);
+      dpl = gam * p3 / a3;
+      vw3 = vel + a3;
+      vw4 = un4 + a4;
+    }
+    vel = vel - ((p2 - p3) / (dpr - dpl));
+    iter = iter + 1;
+  }
+  double af, pf, rhof, uf, vf, wf;
+  if (vel > 0.0) {
+    af = a2; pf = p2;
+    if (vel <= un1) {
+      if (swl > 0.0) { af = a1; vel = un1; pf = p1; }
+    } else if (vw1 > 0.0) {
+      vel = un1; af = a1; pf = p1;
+    } else if (vw2 > 0.0) {
+      af = (un1 + a1 / delta) / (1.0 + 1.0 / delta);
+      vel = af;
+      pf = p1 * pow(af / a1, eta);
+    }
+    rhof = gam * pf / (af * af);
+    uf = vel * nx + ut1; vf = vel * ny + vt1; wf = vel * nz + wt1;
+  } else {
+    af = a3; pf = p3;
+    if (vel >= un4) {
+      if (swr < 0.0) { af = a4; vel = un4; pf = p4; }
+    } else if (vw4 < 0.0) {
+      af = a4; vel = un4; pf = p4;
+    } else if (vw3 < 0.0) {
+      af = -(un4 - a4 / delta) / (1.0 + 1.0 / delta);
+      vel = -af;
+      pf = p4 * pow(af / a4, eta);
+    }
+    rhof = gam * pf / (af * af);
+    uf = vel * nx + ut4; vf = vel * ny + vt4; wf = vel * nz + wt4;
+  }
+  Fl5 F;
+  F.r = rhof * vel;
+  F.u = F.r * uf + pf * nx;
+  F.v = F.r * vf + pf * ny;
+  F.w = F.r * wf + pf * nz;
+  F.E = F.r * H0(g, pf, 1.0 * rhof, sqrt(vel * vel));
+  return F;
+}
+
 // Every solver selected at run time by Gas::rie (MOSE_RIEMANN_*); beta is
 // the face's shock detector (1 without one).
 template <int NV>
@@ -591,12 +738,14 @@ __device__ __noinline__ void riemann_rt(const Gas& g, const double* Lq, double a
       }
       return;
     }
+    case 13: hllc_rot<NV>(g, Lq, aL, Rq, aR, n, F); return;
     default: break;
   }
   const St3 L = st3<NV>(Lq, aL), R = st3<NV>(Rq, aR);
   Fl5 f;
   switch (g.rie) {
     case 12: f = hllepp3(g, L, R, n[0], n[1], n[2], beta); break;
+    case 14: f = exact3(g, L, R, n[0], n[1], (NV == 5) ? n[2] : 0.0); break;
     case 4: f = hlle3(g, L, R, n[0], n[1], n[2]); break;
     case 5: f = hllem3(g, L, R, n[0], n[1], n[2]); break;
     case 6: f = llf3(g, L, R, n[0], n[1], n[2]); break;

@@ -747,6 +747,159 @@ inline bool sd_riemann(const orc_domain* d) {
 // any shock detector in use (Assign_Setup.f90:43-47)
 inline bool sd_any(const orc_domain* d) { return d->cfg.sd_limiter != 0 || sd_riemann(d); }
 
+// riemann_HLLCHLLE ('HLLC Rotated'), Lib_Riemann_HLL.f90:672-755: HLLE along
+// n1, the direction of the velocity jump, and HLLC along n2 = (-n1y, n1x,
+// n1z), weighted by the projections of the face normal on them (both made
+// non-negative); HLLC along the normal where the jump is negligible.
+inline RFlux riemann_HLLCrot(const Thermo& t, const RState& L, const RState& R, double nx, double ny, double nz) {
+  double abs_dv = std::sqrt((R.u - L.u) * (R.u - L.u) + (R.v - L.v) * (R.v - L.v) + (R.w - L.w) * (R.w - L.w));
+  double dum = 0.5 * (std::sqrt(L.u * L.u + L.v * L.v + L.w * L.w) + std::sqrt(R.u * R.u + R.v * R.v + R.w * R.w));
+  if (abs_dv / (dum + 1.0e-10) > 1.0e-12) {
+    double nx1 = (R.u - L.u) / abs_dv, ny1 = (R.v - L.v) / abs_dv, nz1 = (R.w - L.w) / abs_dv;
+    double alfa1 = nx * nx1 + ny * ny1 + nz * nz1;
+    double s1 = std::copysign(1.0, alfa1);
+    nx1 = s1 * nx1; ny1 = s1 * ny1; nz1 = s1 * nz1; alfa1 = s1 * alfa1;
+    double nx2 = -ny1, ny2 = nx1, nz2 = nz1;
+    double alfa2 = nx * nx2 + ny * ny2 + nz * nz2;
+    double s2 = std::copysign(1.0, alfa2);
+    nx2 = s2 * nx2; ny2 = s2 * ny2; nz2 = s2 * nz2; alfa2 = s2 * alfa2;
+    if (nz > 0.1) {
+      alfa1 = 0.0;
+      nx2 = nx; ny2 = ny; nz2 = nz;
+      alfa2 = 1.0;
+    }
+    RFlux E = riemann_HLLE(t, L, R, nx1, ny1, nz1);
+    RFlux C = riemann_HLLC(t, L, R, nx2, ny2, nz2);
+    RFlux F;
+    F.r = E.r * alfa1 + C.r * alfa2;
+    F.u = E.u * alfa1 + C.u * alfa2;
+    F.v = E.v * alfa1 + C.v * alfa2;
+    F.w = E.w * alfa1 + C.w * alfa2;
+    if (F.w != 0.0 && std::fabs(nz) <= 1.0e-10) F.w = 0.0;
+    F.E = E.E * alfa1 + C.E * alfa2;
+    return F;
+  }
+  return riemann_HLLC(t, L, R, nx, ny, nz);
+}
+
+// riemann_exact ('exact'), Lib_Riemann_Godunov.f90:10-224: Newton iteration
+// on the contact velocity (relative pressure tolerance 1e-5, at most 1001
+// iterations) with shock or rarefaction relations per side, then the
+// Godunov state sampled at the face.  The wave speeds that the sampling reads
+// (swl, swr, vw1..vw4) keep the value of the last iteration that set them;
+// the reference leaves them undefined before that, here they start at 0.
+struct ExactWaves { double swl = 0.0, swr = 0.0, vw1 = 0.0, vw2 = 0.0, vw3 = 0.0, vw4 = 0.0; };
+inline void exact_rareleft(double ps, double as, double us, double ud, double& pd, double& ad, double& dpr,
+                           double& v1, double& v2, double gamma) {             // :153-169
+  double delta = 0.5 * (gamma - 1.0);
+  double dum1 = 2.0 * gamma / (gamma - 1.0);
+  ad = as - delta * (ud - us);
+  pd = ps * std::pow(ad / as, dum1);
+  dpr = -(gamma * pd / ad);
+  v1 = us - as;
+  v2 = ud - ad;
+}
+inline void exact_rareright(double pd, double ad, double ud, double us, double& ps, double& as, double& dpl,
+                            double& v3, double& v4, double gamma) {            // :172-188
+  double delta = 0.5 * (gamma - 1.0);
+  double dum1 = 2.0 * gamma / (gamma - 1.0);
+  as = ad + delta * (us - ud);
+  ps = pd * std::pow(as / ad, dum1);
+  dpl = gamma * ps / as;
+  v3 = us + as;
+  v4 = ud + ad;
+}
+inline void exact_shockleft(double us, double as, double ps, double ud, double& ad, double& pd, double& dpr,
+                            double& wl, double gamma) {                          // :191-206
+  double x1 = (gamma + 1.0) * (ud - us) / (4.0 * as);
+  double Mlrel = x1 - std::sqrt(1.0 + x1 * x1);
+  double C1 = gamma * ps / as;
+  pd = ps + C1 * (ud - us) * Mlrel;
+  dpr = 2.0 * C1 * std::pow(Mlrel, 3.0) / (1.0 + Mlrel * Mlrel);
+  double rpd = pd / ps;
+  wl = us + as * Mlrel;
+  ad = as * std::sqrt((gamma + 1.0 + (gamma - 1.0) * rpd) / (gamma + 1.0 + (gamma - 1.0) / rpd));
+}
+inline void exact_shockright(double ud, double ad, double pd, double us, double& as, double& ps, double& dpl,
+                             double& wr, double gamma) {                         // :209-224
+  double x4 = (gamma + 1.0) * (us - ud) / (4.0 * ad);
+  double Mrrel = x4 + std::sqrt(1.0 + x4 * x4);
+  double C4 = gamma * pd / ad;
+  ps = pd + C4 * (us - ud) * Mrrel;
+  dpl = 2.0 * C4 * std::pow(Mrrel, 3.0) / (1.0 + Mrrel * Mrrel);
+  double rps = ps / pd;
+  wr = ud + ad * Mrrel;
+  as = ad * std::sqrt((gamma + 1.0 + (gamma - 1.0) * rps) / (gamma + 1.0 + (gamma - 1.0) / rps));
+}
+inline RFlux riemann_exact(const Thermo& t, const RState& L, const RState& R, double nx, double ny, double nz) {
+  const double gam1 = t.gamma, gam4 = t.gamma;                                  // f_gamma
+  const double p1 = L.p, a1 = L.a, p4 = R.p, a4 = R.a;
+  double gm1_1 = gam1 - 1.0, gm1_4 = gam4 - 1.0;
+  double delta1 = 0.5 * gm1_1, delta4 = 0.5 * gm1_4;
+  double eta1 = gam1 / delta1, eta4 = gam4 / delta4;
+  double un1 = L.u * nx + L.v * ny + L.w * nz;
+  double ut1 = L.u - un1 * nx, vt1 = L.v - un1 * ny, wt1 = L.w - un1 * nz;
+  double un4 = R.u * nx + R.v * ny + R.w * nz;
+  double ut4 = R.u - un4 * nx, vt4 = R.v - un4 * ny, wt4 = R.w - un4 * nz;
+  double R2I = un1 + (2.0 / gm1_1) * a1;
+  double R1IV = un4 - (2.0 / gm1_4) * a4;
+  double dum = (p1 < p4) ? gm1_4 / (2.0 * gam4) : gm1_1 / (2.0 * gam1);
+  double z = (gm1_1 / gm1_4) * (a4 / a1) * std::pow(p1 / p4, dum);
+  double u0 = (z * R2I + R1IV) / (1.0 + z);
+  double vel = u0;
+  double p3 = 1.0, p2 = 2.0 * p3, a2 = 0.0, a3 = 0.0, dpr = 0.0, dpl = 0.0;
+  ExactWaves w;
+  int iter = 0;
+  while (std::fabs(1.0 - (p2 / p3)) >= 1e-5 && iter <= 1000) {
+    if (vel < un1) exact_shockleft(un1, a1, p1, vel, a2, p2, dpr, w.swl, gam1);
+    else exact_rareleft(p1, a1, un1, vel, p2, a2, dpr, w.vw1, w.vw2, gam1);
+    if (vel > un4) exact_shockright(un4, a4, p4, vel, a3, p3, dpl, w.swr, gam4);
+    else exact_rareright(p4, a4, un4, vel, p3, a3, dpl, w.vw3, w.vw4, gam4);
+    vel = vel - ((p2 - p3) / (dpr - dpl));
+    iter = iter + 1;
+  }
+  double af, pf, rhof, uf, vf, wf;
+  if (vel > 0.0) {
+    af = a2; pf = p2;
+    if (vel <= un1) {
+      if (w.swl > 0.0) { af = a1; vel = un1; pf = p1; }
+    } else {
+      if (w.vw1 > 0.0) {
+        vel = un1; af = a1; pf = p1;
+      } else if (w.vw2 > 0.0) {
+        af = (un1 + a1 / delta1) / (1.0 + 1.0 / delta1);
+        vel = af;
+        pf = p1 * std::pow(af / a1, eta1);
+      }
+    }
+    rhof = gam1 * pf / (af * af);
+    uf = vel * nx + ut1; vf = vel * ny + vt1; wf = vel * nz + wt1;
+  } else {
+    af = a3; pf = p3;
+    if (vel >= un4) {
+      if (w.swr < 0.0) { af = a4; vel = un4; pf = p4; }
+    } else {
+      if (w.vw4 < 0.0) {
+        af = a4; vel = un4; pf = p4;
+      } else if (w.vw3 < 0.0) {
+        af = -(un4 - a4 / delta4) / (1.0 + 1.0 / delta4);
+        vel = -af;
+        pf = p4 * std::pow(af / a4, eta4);
+      }
+    }
+    rhof = gam4 * pf / (af * af);
+    uf = vel * nx + ut4; vf = vel * ny + vt4; wf = vel * nz + wt4;
+  }
+  double df = 1.0 * rhof;                                   // dl/dltot*rhof, one species
+  RFlux F;
+  F.r = rhof * vel;
+  F.u = F.r * uf + pf * nx;
+  F.v = F.r * vf + pf * ny;
+  F.w = F.r * wf + pf * nz;
+  F.E = F.r * H0(t, pf, df, std::sqrt(vel * vel));
+  return F;
+}
+
 // beta: the shock detector of the face (1 at the physical boundary faces,
 // which call Riemann with 1d0)
 inline RFlux Riemann(const orc_domain* d, const RState& L, const RState& R, double nx,
@@ -764,6 +917,8 @@ inline RFlux Riemann(const orc_domain* d, const RState& L, const RState& R, doub
     case ORC_RIE_HANEL: return riemann_Hanel(d->th, L, R, nx, ny, nz);
     case ORC_RIE_AUSMP_UP: return riemann_AUSMp_up(d->th, L, R, nx, ny, nz, d->cfg.minf, false);
     case ORC_RIE_AUSMP_UP2: return riemann_AUSMp_up(d->th, L, R, nx, ny, nz, d->cfg.minf, true);
+    case ORC_RIE_HLLC_ROT: return riemann_HLLCrot(d->th, L, R, nx, ny, nz);
+    case ORC_RIE_EXACT: return riemann_exact(d->th, L, R, nx, ny, nz);
     default: return riemann_HLLC(d->th, L, R, nx, ny, nz);
   }
 }

@@ -32,7 +32,7 @@ enum { ORC_LIM_FIRST_ORDER = 0, ORC_LIM_MINMOD = 1, ORC_LIM_VANLEER = 2,
 enum { ORC_RIE_HLLC = 0, ORC_RIE_AUSMP = 1, ORC_RIE_SLAU = 2, ORC_RIE_SLAU2 = 3,
        ORC_RIE_HLLE = 4, ORC_RIE_HLLEM = 5, ORC_RIE_LLF = 6, ORC_RIE_PLLF = 7,
        ORC_RIE_HANEL = 8, ORC_RIE_AUSMP_UP = 9, ORC_RIE_AUSMP_UP2 = 10,
-       ORC_RIE_HLLC_SD = 11, ORC_RIE_HLLE_PP = 12 };
+       ORC_RIE_HLLC_SD = 11, ORC_RIE_HLLE_PP = 12, ORC_RIE_HLLC_ROT = 13, ORC_RIE_EXACT = 14 };
 /* Integration variables (Mod_Newstate.f90:30-44). */
 enum { ORC_INT_CONS = 0, ORC_INT_PRIM = 1 };
 
