@@ -18,7 +18,8 @@
  *   bc    : one record per boundary face cell in bc.txt order (block, face
  *           1..6, cell): int32 b,i,j,k,f,type,bs,is,js,ks,fs,d11,d12,d21,d22
  *           (1-based), plus 6 doubles of type data
- *           401: T0, p0, alpha, beta, rel_fac ; 403: T0, g, alpha, beta,
+ *           401: T0, p0, alpha, beta, rel_fac ; 402: T0, time-table id
+ *           (mose_gpu_add_series), alpha, beta, rel_fac ; 403: T0, g, alpha, beta,
  *           rel_fac ; 404: T, g, alpha, beta, rel_fac ; 405: mach, T, p,
  *           alpha, beta, rel_fac ; 406: p_back, rel_fac ; 407: T0, p0,
  *           p_back, alpha, beta, rel_fac (g: mass flux per unit area; the
@@ -136,6 +137,14 @@ int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int
                        const double* node);
 /* Replaces Read_BCfile (io/IO_BC.f90:136-414) with the parsed records. */
 int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, int32_t nbound);
+/* The p0 time table of 402 inlets, replacing time_series_type::initialize
+ * (base/Series_Data_m.f90:20-52): n (time, value) pairs, value in the units
+ * of p0 (the file's bar times 1e5), periodic or not.  Call before
+ * mose_gpu_setup; *id (0, 1, ...) is what a 402 record holds as its second
+ * datum in place of the reference's file name.  At every step the device
+ * evaluates update(time) (Series_Data_m.f90:55-86) at the step's time. */
+int mose_gpu_add_series(mose_gpu_ctx* ctx, const double* time, const double* value, int32_t n, int32_t periodic,
+                        int32_t* id);
 /* Setup_Metrics (numerics/space/Mod_Metrics.f90:8-107) on the device, then the
  * device tables.  Must follow add_block and set_bcs. */
 int mose_gpu_setup(mose_gpu_ctx* ctx);

@@ -52,6 +52,9 @@ class Case:
     rgas: float = 1.0
     steps: int = 1
     t_end: float | None = None
+    # time tables of 402 inlets: (time, value, periodic) each; a 402 record
+    # holds its table's index as its second datum
+    series: list = field(default_factory=list)
     extra: dict = field(default_factory=dict)
 
     @property

@@ -107,6 +107,13 @@ struct BcParam {
   double tv[3], bv[3], E1, E2;
 };
 
+// One 402 face cell: its BcParam slot, and its time table's (time, value)
+// pairs at tv[2 off ..], n pairs, periodic or not (time_series_type,
+// Series_Data_m.f90:7-16).
+struct SeriesRec {
+  int pidx, off, n, periodic;
+};
+
 // One first-layer ghost value of the residual for implicit residual
 // smoothing (Ghost_Residual_Extrapolation, Lib_IRS.f90:130-187): arena
 // offsets of the ghost cell and of its source cell, and their blocks'

@@ -29,6 +29,10 @@ void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, dou
 void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time, double dt_start,
                          int* iter, cudaStream_t s);
 // Implicit residual smoothing (2-D, conservative integration).
+// 402 inlets: p0 of every record from its time table at the device time
+// (update, Series_Data_m.f90:55-86), written into its BcParam.
+void launch_series_p0(const SeriesRec* recs, int n, const double* tv, const double* time, BcParam* bcp,
+                      cudaStream_t s);
 void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, double* R, MetricArgs m, const double* dtl,
                       const double* dtg, int use_dtg, cudaStream_t s);
 void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s);

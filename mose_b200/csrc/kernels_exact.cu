@@ -848,3 +848,49 @@ void launch_faces_to_ref(const BlockDesc* dblk, int b, long long n, MetricArgs m
 }
 
 }  // namespace mose
+
+namespace mose {
+
+// ---- 402 inlets: p0 from the time table (Series_Data_m.f90:55-86) -----------------
+// Linear interpolation at the device time; a periodic table first wraps the
+// time into [t_1, t_n) (Fortran MODULO of reals: fmod, plus the period where
+// the signs differ).  Before t_1 the reference's value is undefined; here it
+// is v_1.  Runs in this --fmad=false unit: the same roundings as the host.
+__global__ void k_series_p0(const SeriesRec* recs, int n, const double* tv, const double* time, BcParam* bcp) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const SeriesRec r = recs[q];
+  const double* T = tv + 2 * (long long)r.off;   // (t, v) pairs
+  double t_ = *time;
+  if (r.periodic) {
+    const double period = T[2 * (r.n - 1)] - T[0];
+    if (period > 0.0) {
+      double m = fmod(t_ - T[0], period);
+      if (m != 0.0 && ((m < 0.0) != (period < 0.0))) m = m + period;
+      t_ = T[0] + m;
+    }
+  }
+  double out = T[1];
+  if (t_ == T[0]) {
+    out = T[1];
+  } else {
+    bool found = false;
+    for (int i = 1; i < r.n && !found; ++i) {
+      const double t0 = T[2 * (i - 1)], t1 = T[2 * i];
+      if (t_ > t0 && t_ <= t1) {
+        const double v0 = T[2 * (i - 1) + 1], v1 = T[2 * i + 1];
+        out = (v1 - v0) / (t1 - t0) * (t_ - t0) + v0;
+        found = true;
+      }
+    }
+    if (!found && t_ > T[2 * (r.n - 1)]) out = T[2 * (r.n - 1) + 1];
+  }
+  bcp[r.pidx].p = out;
+}
+
+void launch_series_p0(const SeriesRec* recs, int n, const double* tv, const double* time, BcParam* bcp,
+                      cudaStream_t s) {
+  if (n <= 0) return;
+  k_series_p0<<<(n + 127) / 128, 128, 0, s>>>(recs, n, tv, time, bcp);
+}
+}  // namespace mose

@@ -223,7 +223,15 @@ struct mose_gpu_ctx {
   DevBuf<int> adj_gids;                  // ghost records grouped by face
   int adj_gfirst[5] = {0, 0, 0, 0, 0};
   bool adj_recorded = false;
-  std::vector<BcParam> hbcp;             // 405 / 406 parameters (host copy)
+  std::vector<BcParam> hbcp;             // 401 / 402 / 403 - 407 parameters (host copy)
+  // 402 time tables: (time, value) pairs of every table, and per table its
+  // first pair, pair count and periodic flag; per 402 record its SeriesRec
+  std::vector<double> hser;
+  struct SerIdx { int off, n, periodic; };
+  std::vector<SerIdx> hser_idx;
+  DevBuf<double> ser_tv;
+  DevBuf<SeriesRec> ser_recs;
+  int nser = 0;
 
   MetricArgs margs() const { return MetricArgs{dl.p, face.p, vol.p, vers.p}; }
 };
@@ -276,7 +284,7 @@ int bc_code_of(int type) {
     case 101: case 201: return BC_CONN;
     case 300: return BC_SYM;
     case 400: return BC_EXTRAP;
-    case 401: return BC_STAGIN;
+    case 401: case 402: return BC_STAGIN;   // 402: p0 from its time table, refreshed every step
     case 403: return BC_MFLUX_T0;
     case 404: return BC_MFLUX_T;
     case 405: return BC_SUPIN;
@@ -412,6 +420,20 @@ int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int
   return MOSE_OK;
 }
 
+int mose_gpu_add_series(mose_gpu_ctx* ctx, const double* time, const double* value, int32_t n, int32_t periodic,
+                        int32_t* id) {
+  if (!ctx || !time || !value || !id || n < 1) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "add_series after setup");
+  mose_gpu_ctx::SerIdx si{(int)(ctx->hser.size() / 2), n, periodic ? 1 : 0};
+  for (int q = 0; q < n; ++q) {
+    ctx->hser.push_back(time[q]);
+    ctx->hser.push_back(value[q]);
+  }
+  ctx->hser_idx.push_back(si);
+  *id = (int32_t)ctx->hser_idx.size() - 1;
+  return MOSE_OK;
+}
+
 int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, int32_t nbound) {
   if (!ctx || !rec) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_bcs after setup");
@@ -518,9 +540,12 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     // (the token 'normal' resolves to atan(0 / ...) = 0 there: 2-D face normals have n_z = 0)
     if (ctx->nd == 2 && e.type == 405 && e.data[4] != 0.0 && !(e.data[4] >= 0.5 * 1.7976931348623157e308))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
-    if (ctx->nd == 2 && (e.type == 401 || e.type == 403 || e.type == 404) && e.data[3] != 0.0 &&
+    if (ctx->nd == 2 && (e.type >= 401 && e.type <= 404) && e.data[3] != 0.0 &&
         !(e.data[3] >= 0.5 * 1.7976931348623157e308))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "2-D inflow with a non-zero out-of-plane angle");
+    if (e.type == 402 && !(e.data[1] >= 0.0 && e.data[1] < (double)ctx->hser_idx.size() &&
+                           e.data[1] == std::floor(e.data[1])))
+      return fail(ctx, MOSE_ERR_INVALID, "bc 402: time table %g was not added", e.data[1]);
     // 407 uses its angles as given (Lib_BC_Fluxes_FarField.f90:48-49): the
     // token 'normal' would enter tan() as the largest double
     if (e.type == 407 && (e.data[3] >= 0.5 * 1.7976931348623157e308 || e.data[4] >= 0.5 * 1.7976931348623157e308))
@@ -568,6 +593,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   // coefficients, formed from the face normal once the device has it
   struct InletGeo { int pidx, b, f, i, j, k; double alpha, beta; bool raw; };
   std::vector<InletGeo> inlet_geo;
+  std::vector<SeriesRec> series_recs;
   for (auto& e : ctx->bc) {
     const BlockDesc& d = ctx->desc[e.b - 1];
     const HostBlock& h = ctx->hblk[e.b - 1];
@@ -586,7 +612,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       }
       pidx = (int)params.size();
       params.push_back(p);
-    } else if (e.type == 401 || e.type == 403 || e.type == 404 || e.type == 407) {
+    } else if (e.type >= 401 && e.type <= 407) {
       BcParam p{};
       p.T = e.data[0]; p.p = e.data[1];
       double alpha = e.data[2], beta = e.data[3];
@@ -598,6 +624,11 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       }
       inlet_geo.push_back(InletGeo{(int)params.size(), e.b - 1, e.f, e.i - 1, e.j - 1, e.k - 1, alpha, beta,
                                    e.type == 407});
+      if (e.type == 402) {
+        const auto& si = ctx->hser_idx[(size_t)e.data[1]];
+        series_recs.push_back(SeriesRec{(int)params.size(), si.off, si.n, si.periodic});
+        p.p = ctx->hser[2 * (size_t)si.off + 1];    // refreshed from the table before every use
+      }
       pidx = (int)params.size();
       params.push_back(p);
     }
@@ -628,6 +659,15 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
   CU(cudaMemcpyAsync(ctx->bcw.p, bcwords.data(), bcwords.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   if (!params.empty()) CU(cudaMemcpyAsync(ctx->bcp.p, params.data(), params.size() * sizeof(BcParam), cudaMemcpyHostToDevice, ctx->stream));
+  ctx->nser = (int)series_recs.size();
+  if (ctx->nser) {
+    CU(ctx->ser_recs.alloc(series_recs.size()));
+    CU(ctx->ser_tv.alloc(ctx->hser.size()));
+    CU(cudaMemcpyAsync(ctx->ser_recs.p, series_recs.data(), series_recs.size() * sizeof(SeriesRec),
+                       cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->ser_tv.p, ctx->hser.data(), ctx->hser.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+  }
   ctx->hbcp = params;
 
   // ---- metrics on the device -------------------------------------------------
@@ -1041,10 +1081,17 @@ static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int pre
              : 0;
 }
 
+static int enqueue_series(mose_gpu_ctx* ctx);
+
 int mose_gpu_residual(mose_gpu_ctx* ctx) {
   int rc = require_ready(ctx);
   if (rc) return rc;
-  // the phase-by-phase path always runs the reference-exact arithmetic
+  // the phase-by-phase path always runs the reference-exact arithmetic; 402
+  // tables are read at the caller's domain time (mose_gpu_set_time)
+  if (ctx->nser) {
+    CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->launches += enqueue_series(ctx);
+  }
   StageArgs a = stage_args(ctx, ctx->cur, ctx->po, -1, 1);
   // the residual-only kernels read the metric arrays
   const int nk = launch_stage(ctx, a, 1, MOSE_PRECISION_FP64_EXACT, false);
@@ -1149,11 +1196,21 @@ static int enqueue_irs_stage(mose_gpu_ctx* ctx, int pc, int s0, int pn, int irk)
   return k + 1;
 }
 
+// 402 inlets: p0 from the time tables at the device time (scal[1]), which
+// Explicit_Step has already advanced to the end of the step when BC_Fluxes
+// reads it (Mod_Explicit.f90:40-48, Mod_BC_Fluxes.f90:129-131).
+static int enqueue_series(mose_gpu_ctx* ctx) {
+  if (!ctx->nser) return 0;
+  launch_series_p0(ctx->ser_recs.p, ctx->nser, ctx->ser_tv.p, ctx->scal.p + 1, ctx->bcp.p, ctx->stream);
+  return 1;
+}
+
 static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
   int k = 0;
   if (!fused_dt(ctx)) k += enqueue_dt_pass(ctx, s0);
   launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
                       ctx->stream); ++k;
+  k += enqueue_series(ctx);
   int pc = s0;
   for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
     int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
@@ -1295,8 +1352,8 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
     if (!fused_dt(ctx) || !ctx->dt_valid) launches[0] += enqueue_dt_pass(ctx, s0);
     launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
                         ctx->stream);
+    launches[0] += 1 + enqueue_series(ctx);
     mark(0);
-    launches[0] += 1;
     int pc = s0;
     for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
       int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
@@ -1388,6 +1445,7 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
   if (!ctx->cfg.time_accurate) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: time-accurate runs only");
   if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no cfl ramp");
   if (ctx->irs_beta > 0.0 || ctx->gas.sd) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no IRS or shock detector");
+  if (ctx->nser) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no time-table (402) inlets");
   const size_t ns = (size_t)ctx->nv * ctx->marena, m = (size_t)ctx->marena;
   for (DevBuf<double>* b : {&ctx->lam, &ctx->lam_loc, &ctx->lam_n, &ctx->lamR, &ctx->wdt, &ctx->lamG})
     if (b->alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
@@ -1618,12 +1676,12 @@ int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
   for (auto& e : ctx->bc)
     if (e.type == 405) any = true;
   if (!any) return fail(ctx, MOSE_ERR_INVALID, "no 405 inflow faces");
-  // every record with a parameter slot (401, 403 - 407) holds it in bc order;
+  // every record with a parameter slot (401 - 407) holds it in bc order;
   // only 405 has a Mach number
   size_t q = 0;
   for (auto& e : ctx->bc) {
     if (e.type == 405) ctx->hbcp[q].mach = mach;
-    if (e.type == 401 || (e.type >= 403 && e.type <= 407)) ++q;
+    if (e.type >= 401 && e.type <= 407) ++q;
   }
   CU(cudaMemcpyAsync(ctx->bcp.p, ctx->hbcp.data(), ctx->hbcp.size() * sizeof(BcParam), cudaMemcpyHostToDevice,
                      ctx->stream));

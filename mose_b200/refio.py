@@ -7,6 +7,7 @@ the GPU path unchanged.
   data, one list-directed data line.  The records come back in the layout
   of ``mose_gpu_set_bcs``: int32 (b, i, j, k, f, type, bs, is, js, ks, fs,
   d11, d12, d21, d22) and six doubles (401: T0, p0, alpha, beta, rel_fac;
+  402: T0, index of its p0 table (``read_series``), alpha, beta, rel_fac;
   403 / 404: T0 / T, mass flux, alpha, beta, rel_fac; 405: mach, T, p, alpha,
   beta, rel_fac; 406: p_back, rel_fac; 407: T0, p0, p_back, alpha, beta,
   rel_fac).  The direction token ``normal`` becomes the largest double, as
@@ -58,8 +59,25 @@ def _num(tok: str) -> float:
     return float(tok.replace("d", "e").replace("D", "e"))
 
 
-def read_bc(path) -> tuple[np.ndarray, np.ndarray]:
-    """bc.txt -> (rec int32 (n, 15), data float64 (n, 6))."""
+def read_series(path) -> tuple[np.ndarray, np.ndarray, bool]:
+    """A 402 p0 table (time_series_type%initialize, Series_Data_m.f90:20-52):
+    lines of ``time value`` in bar, after an optional first line holding
+    ``periodic``; returns (time, value in Pa, periodic)."""
+    lines = [ln for ln in Path(path).read_text().splitlines() if ln.strip()]
+    periodic = any("periodic" in ln for ln in lines)
+    if periodic:
+        lines = lines[1:]
+    rows = [[_num(x) for x in _fields(ln)[:2]] for ln in lines]
+    arr = np.asarray(rows, dtype=np.float64).reshape(-1, 2)
+    return arr[:, 0].copy(), arr[:, 1] * 1e5, periodic
+
+
+def read_bc(path, series: list | None = None, base=None) -> tuple[np.ndarray, np.ndarray]:
+    """bc.txt -> (rec int32 (n, 15), data float64 (n, 6)).  A 402 record's
+    p0 table is read from its file (relative to ``base``, by default the case
+    directory above INPUT/) and appended to ``series``; the record holds its
+    index there."""
+    base = Path(base) if base is not None else Path(path).resolve().parent.parent
     lines = [ln for ln in Path(path).read_text().splitlines() if ln.strip()]
     recs, data = [], []
     q = 0
@@ -78,6 +96,13 @@ def read_bc(path) -> tuple[np.ndarray, np.ndarray]:
         elif t == 406:
             g = _fields(lines[q]); q += 1
             d[0], d[1] = _num(g[0]), _num(g[1])
+        elif t == 402:                     # T0, p0 file, alpha, beta, rel_fac, ci...
+            g = _fields(lines[q]); q += 1
+            if series is None:
+                raise ValueError(f"{path}: a 402 record needs a list for its p0 table")
+            fname = g[1].strip("'\"")
+            series.append(read_series(base / fname))
+            d = [_num(g[0]), float(len(series) - 1), _dir_tok(g[2]), _dir_tok(g[3]), _num(g[4]), 0.0]
         elif t in (401, 403, 404):         # T0 (T), p0 (mass flux), alpha, beta, rel_fac, ci...
             g = _fields(lines[q]); q += 1
             d = [_num(g[0]), _num(g[1]), _dir_tok(g[2]), _dir_tok(g[3]), _num(g[4]), 0.0]
@@ -223,7 +248,8 @@ def load_case(case_dir, resolution: str = "", gamma: float | None = None, rgas: 
     d = Path(case_dir)
     sfx = f"_{resolution}" if resolution else ""
     nodes = read_mesh(d / "MESH" / f"mesh{sfx}.tec")
-    rec, data = read_bc(d / "INPUT" / f"bc{sfx}.txt")
+    series: list = []
+    rec, data = read_bc(d / "INPUT" / f"bc{sfx}.txt", series, base=d)
     prim = read_ic(d / "INPUT" / f"ic{sfx}.tec")
     kw = read_input_ini(d / "input.ini")
     unsupported = kw.pop("unsupported")
@@ -239,5 +265,6 @@ def load_case(case_dir, resolution: str = "", gamma: float | None = None, rgas: 
     case = Case(d.name + sfx, nodes, rec, data, prim, gamma=gamma, rgas=rgas,
                 **{k: v for k, v in kw.items() if k in ("cfl", "n_rk", "time_accurate", "riemann", "minf", "limiter",
                                                         "t_end", "steps", "irs_beta", "sd_limiter", "ramp_iter")})
+    case.series = series
     case.extra["unsupported"] = unsupported
     return case

@@ -78,6 +78,14 @@ class Solver:
             nk, nj, ni = nd.shape[0] - 1, nd.shape[1] - 1, nd.shape[2] - 1
             self.dims.append((ni, nj, nk))
             self._check(self.lib.mose_gpu_add_block(self.h, b, ni, nj, nk, _dp(np.ascontiguousarray(nd))))
+        for t, v, periodic in getattr(case, "series", []):
+            sid = C.c_int32()
+            t = np.ascontiguousarray(t, dtype=np.float64)
+            v = np.ascontiguousarray(v, dtype=np.float64)
+            if t.shape != v.shape or t.ndim != 1:
+                raise ValueError("a time table is two 1-D arrays of equal length")
+            self._check(self.lib.mose_gpu_add_series(self.h, _dp(t), _dp(v), len(t), int(bool(periodic)),
+                                                     C.byref(sid)))
         rec = np.ascontiguousarray(case.bc_rec, dtype=np.int32)
         data = np.ascontiguousarray(case.bc_data, dtype=np.float64)
         self._check(self.lib.mose_gpu_set_bcs(self.h, rec.ctypes.data_as(C.POINTER(C.c_int32)), _dp(data),

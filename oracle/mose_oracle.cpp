@@ -116,6 +116,8 @@ struct orc_domain {
   std::vector<Block> blk;
   std::vector<BCrec> bc;
   std::vector<int> n_bf;                // (nb, 6)
+  struct Series { std::vector<double> t, v; bool periodic = false; };
+  std::vector<Series> series;           // 402 time tables
   double time = 0.0, dtglobal = 0.0;
   int iter = 0, iter_from_call = 0;
   int err = 0, eb = 0, ei = 0, ej = 0, ek = 0;
@@ -1823,6 +1825,29 @@ bool BC_Inlet_MassFlux(const orc_domain* D, int Im, int Jm, int Km, int Fm, Bloc
   return true;
 }
 
+// update, Series_Data_m.f90:55-86: linear interpolation in a time table;
+// a periodic table first wraps time into [t_1, t_n) (Fortran MODULO of
+// reals, restated as fmod plus the period when the signs differ).  The
+// reference leaves the value undefined before t_1; here it is v_1.
+double series_update(const orc_domain::Series& S, double time) {
+  const size_t n = S.t.size();
+  double t_ = time;
+  if (S.periodic) {
+    double period = S.t[n - 1] - S.t[0];
+    if (period > 0.0) {
+      double a = t_ - S.t[0];
+      double m = std::fmod(a, period);
+      if (m != 0.0 && ((m < 0.0) != (period < 0.0))) m = m + period;
+      t_ = S.t[0] + m;
+    }
+  }
+  if (t_ == S.t[0]) return S.v[0];
+  for (size_t i = 1; i < n; ++i)
+    if (t_ > S.t[i - 1] && t_ <= S.t[i]) return (S.v[i] - S.v[i - 1]) / (S.t[i] - S.t[i - 1]) * (t_ - S.t[i - 1]) + S.v[i - 1];
+  if (t_ > S.t[n - 1]) return S.v[n - 1];
+  return S.v[0];
+}
+
 // BC_FarField, Lib_BC_Fluxes_FarField.f90:19-73 (no rotating frame): the
 // back-pressure outflow where the boundary cell leaves the domain, the total
 // conditions where it enters (its angles are used as given).  data: T0, p0,
@@ -1903,6 +1928,10 @@ int orc_set_bcs(orc_domain* d, const int32_t* rec, const double* data, int nboun
     switch (e.type) {
       case 0: case 101: case 201: case 300: case 400: case 401: case 403: case 404: case 405: case 406: case 407:
         break;
+      case 402:
+        if (!(e.data[1] >= 0.0 && e.data[1] < (double)d->series.size() && e.data[1] == std::floor(e.data[1])))
+          return ORC_ERR_INVALID;
+        break;
       default: return ORC_ERR_UNSUPPORTED;
     }
     if (e.type == 101 || e.type == 201) {
@@ -1910,6 +1939,21 @@ int orc_set_bcs(orc_domain* d, const int32_t* rec, const double* data, int nboun
     }
   }
   return ORC_OK;
+}
+
+int orc_add_series(orc_domain* d, const double* time, const double* value, int n, int periodic) {
+  if (!d || !time || !value || n < 1) return -ORC_ERR_INVALID;
+  orc_domain::Series S;
+  S.t.assign(time, time + n);
+  S.v.assign(value, value + n);
+  S.periodic = periodic != 0;
+  d->series.push_back(std::move(S));
+  return (int)d->series.size() - 1;
+}
+
+double orc_series_eval(const orc_domain* d, int id, double time) {
+  if (!d || id < 0 || id >= (int)d->series.size()) return 0.0;
+  return series_update(d->series[id], time);
 }
 
 int orc_setup_metrics(orc_domain* d) {
@@ -2140,6 +2184,13 @@ int orc_bc_fluxes(orc_domain* d) {
               BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
             break;
           case 407: BC_FarField(d, e.i, e.j, e.k, e.f, bm, e.data); break;
+          case 402: {
+            // p0 from the time table at the domain time (Mod_BC_Fluxes.f90:129-140)
+            double dd[6] = {e.data[0], series_update(d->series[(size_t)e.data[1]], d->time), e.data[2], e.data[3],
+                            e.data[4], e.data[5]};
+            if (!BC_Inlet_StagnCond(d, e.i, e.j, e.k, e.f, bm, dd)) BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            break;
+          }
           default: break;
         }
       }

@@ -69,6 +69,12 @@ int orc_add_block(orc_domain* d, int ni, int nj, int nk, const double* node);
  * data: nbound x 6 doubles (mach, T, p, alpha, beta, rel_fac) for 405 and
  * (p_back, rel_fac, 0, 0, 0, 0) for 406; may be NULL. */
 int orc_set_bcs(orc_domain* d, const int32_t* rec, const double* data, int nbound);
+/* Time table of a 402 inlet (time_series_type, Series_Data_m.f90): n pairs
+ * (time, value), values already in the units of p0; returns the table's
+ * index (>= 0), which a 402 record carries as its second datum, or < 0. */
+int orc_add_series(orc_domain* d, const double* time, const double* value, int n, int periodic);
+/* update(time) of table id (Series_Data_m.f90:55-86), for tests. */
+double orc_series_eval(const orc_domain* d, int id, double time);
 
 /* Setup_Metrics (Mod_Metrics.f90:8-107): interior + ghost metrics. */
 int orc_setup_metrics(orc_domain* d);

@@ -69,6 +69,9 @@ def load(omp: bool = False) -> C.CDLL:
     lib.orc_limiter.argtypes = [C.c_int, C.c_double, C.c_double]
     lib.orc_limiter.restype = C.c_double
     lib.orc_riemann.argtypes = [D, dp, dp, dp, dp]
+    lib.orc_add_series.argtypes = [D, dp, dp, C.c_int, C.c_int]
+    lib.orc_series_eval.argtypes = [D, C.c_int, C.c_double]
+    lib.orc_series_eval.restype = C.c_double
     _LIBS[name] = lib
     return lib
 
@@ -102,6 +105,12 @@ class Oracle:
             self.dims.append((ni, nj, nk))
             arr = np.ascontiguousarray(nd, dtype=np.float64)
             self._check(self.lib.orc_add_block(self.h, ni, nj, nk, _dp(arr)), "add_block")
+        for t, v, periodic in getattr(case, "series", []):
+            t = np.ascontiguousarray(t, dtype=np.float64)
+            v = np.ascontiguousarray(v, dtype=np.float64)
+            sid = self.lib.orc_add_series(self.h, _dp(t), _dp(v), len(t), int(periodic))
+            if sid < 0:
+                raise RuntimeError("oracle add_series failed")
         rec = np.ascontiguousarray(case.bc_rec, dtype=np.int32)
         data = np.ascontiguousarray(case.bc_data, dtype=np.float64)
         self._check(self.lib.orc_set_bcs(self.h, rec.ctypes.data_as(C.POINTER(C.c_int32)), _dp(data),
@@ -124,6 +133,9 @@ class Oracle:
     def _shape(self, b):
         ni, nj, nk = self.dims[b - 1]
         return (nk + 2 * GC, nj + 2 * GC, ni + 2 * GC, 5)
+
+    def series_eval(self, sid, time):
+        return self.lib.orc_series_eval(self.h, sid, time)
 
     def set_prim(self, b, P):
         P = np.ascontiguousarray(P, dtype=np.float64)

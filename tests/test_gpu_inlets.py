@@ -150,3 +150,54 @@ def test_far_field_rejects_normal_token():
     case = channel2d((407, [T0, P0, P_INF, NORMAL, 0.0, 1.0]))
     with pytest.raises(MoseError):
         solver(case)
+
+
+RAMP = (np.array([0.0, 0.03, 0.07, 0.2]), np.array([0.97 * P0, 1.04 * P0, 1.01 * P0, 1.06 * P0]), False)
+WAVE = (np.array([0.0, 0.02, 0.05]), np.array([P0, 1.08 * P0, P0]), True)
+
+
+def channel402(table, rel_fac=1.0, alpha=0.0):
+    case = channel2d((402, [T0, 0.0, alpha, 0.0, rel_fac, 0.0]))
+    case.series = [table]
+    return case
+
+
+@pytest.mark.parametrize("name,table", [("ramp", RAMP), ("periodic", WAVE)])
+def test_time_table_inlet_steps(oracle_mod, name, table):
+    """402: p0 from its time table at the step's time (Mod_BC_Fluxes.f90:
+    129-131, Series_Data_m.f90:55-86), through fused steps and
+    graph-replayed steps; the periodic table wraps several times."""
+    case = channel402(table, rel_fac=0.9 if name == "periodic" else 1.0, alpha=NORMAL if name == "ramp" else 0.0)
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(4):
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, 1, exact=False, tol=1e-12)
+    for _ in range(8):
+        o.step()
+    s.advance(8)
+    # the states differ by pow's last bits, so the CFL step may too
+    assert abs(s.time - o.time) <= 1e-14 * o.time and o.time > 0.1
+    compare_state(s, o, 1, exact=False, tol=1e-12)
+
+
+def test_time_table_inlet_phase_path(oracle_mod):
+    """The residual phase reads the table at the caller's domain time."""
+    case = channel402(RAMP)
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for t in (0.0, 0.05, 0.5):
+        o.set_time(t)
+        s.set_time(t)
+        o.fill_ghost_cell(); o.fluxes(); o.bc_fluxes()
+        s.fill_ghost_cell(); s.fluxes_and_bc_fluxes()
+        assert _residual_rel(s, o, 1) <= 1e-12
+
+
+def test_time_table_inlet_needs_its_table():
+    from mose_b200 import MoseError
+    case = channel402(RAMP)
+    case.series = []
+    with pytest.raises(MoseError):
+        solver(case)

@@ -407,3 +407,64 @@ def test_sod79_inputs_with_exact_and_rotated_solvers(oracle_mod, riemann):
     x = 0.5 * (d["nodes"][0, 0, :-1, 0] + d["nodes"][0, 0, 1:, 0])
     err = _probe_errors(P, x, d["exact"], case.gamma, d["probes"])
     assert err.max() < float(d["threshold_pct"]), err
+
+
+def _series_update(t, v, periodic, time):
+    """update of Series_Data_m.f90:55-86 in plain Python (IEEE doubles, the
+    reference's operation order; v_1 where the reference's value is
+    undefined, before t_1)."""
+    import math
+    t_ = time
+    if periodic:
+        period = t[-1] - t[0]
+        if period > 0.0:
+            m = math.fmod(t_ - t[0], period)
+            if m != 0.0 and ((m < 0.0) != (period < 0.0)):
+                m = m + period
+            t_ = t[0] + m
+    if t_ == t[0]:
+        return v[0]
+    for i in range(1, len(t)):
+        if t[i - 1] < t_ <= t[i]:
+            return (v[i] - v[i - 1]) / (t[i] - t[i - 1]) * (t_ - t[i - 1]) + v[i - 1]
+    return v[-1] if t_ > t[-1] else v[0]
+
+
+def test_time_table_update(oracle_mod):
+    """The oracle's time-table update equals the plain-Python restatement bit
+    for bit (interior points, knots, both ends, periodic wrap in both
+    directions) and np.interp to rounding inside the table."""
+    case = cases.sod(8)
+    t = np.array([0.0, 0.1, 0.25, 0.7])
+    v = np.array([1.0, 1.3, 0.8, 1.1])
+    case.series = [(t, v, False), (t, v, True)]
+    o = oracle_mod.Oracle(case)
+    rng = np.random.default_rng(2)
+    times = np.concatenate([rng.uniform(-1.5, 3.0, 200), t, [-0.1, 0.7, 5.0, 0.7 * 3, -0.7]])
+    for x in times:
+        for sid, per in ((0, False), (1, True)):
+            assert o.series_eval(sid, float(x)) == _series_update(t, v, per, float(x)), (sid, x)
+    inside = rng.uniform(0.0, 0.7, 100)
+    np.testing.assert_allclose([o.series_eval(0, float(x)) for x in inside], np.interp(inside, t, v), rtol=1e-14)
+
+
+def test_time_table_inlet_with_constant_table_is_401(oracle_mod):
+    """A 402 inlet whose table holds one p0 at every time gives the 401
+    result with that p0, bit for bit (Mod_BC_Fluxes.f90:119-140)."""
+    g, m = 1.4, 0.8
+    p_inf = 1.0 / g
+    t0 = p_inf * (1 + 0.5 * (g - 1) * m * m)
+    p0 = p_inf * (1 + 0.5 * (g - 1) * m * m) ** (g / (g - 1))
+    out = []
+    for btype in (401, 402):
+        case = cases.perturbed_channel(16, steps=1, amp=0.02, seed=4)
+        f1 = case.bc_rec[:, 5] == 405
+        case.bc_rec[f1, 5] = btype
+        case.bc_data[f1] = [t0, p0 if btype == 401 else 0.0, 0.0, 0.0, 1.0, 0.0]
+        if btype == 402:
+            case.series = [(np.array([0.0, 1.0]), np.array([p0, p0]), False)]
+        o = oracle_mod.Oracle(case)
+        for _ in range(5):
+            o.step()
+        out.append(o.get_prim(1))
+    assert np.array_equal(out[0], out[1])

@@ -114,3 +114,30 @@ def test_inlet_records_read(tmp_path):
     np.testing.assert_array_equal(data[1], [1.15, 0.8, 0.1, huge, 1.0, 0.0])
     np.testing.assert_array_equal(data[2], [0.71, -0.8, 0.0, 0.0, 1.0, 0.0])
     np.testing.assert_array_equal(data[3], [1.2, 0.95, 0.71, 0.05, 0.0, 0.7])
+
+
+def test_time_table_inlet_read(tmp_path):
+    """A 402 record names its p0 table file (Series_Data_m.f90:20-52): the
+    table is read relative to the case directory, bar becomes Pa, a first
+    line holding 'periodic' marks it periodic, and the record carries the
+    table's index."""
+    (tmp_path / "INPUT").mkdir()
+    (tmp_path / "p0.dat").write_text("0.0 1.0\n0.5 1.2\n1.0 1.1\n")
+    (tmp_path / "p0per.dat").write_text("periodic\n0.0 0.9\n0.25 1.0\n")
+    text = "\n".join(["1 1 1 1 1 402", "300.0, p0.dat, 0.0, 0.0, 1.0, 1.0",
+                      "1 1 2 1 1 402", "300.0 'p0per.dat' normal 0.0 0.8 1.0"]) + "\n"
+    (tmp_path / "INPUT" / "bc.txt").write_text(text)
+    series = []
+    rec, data = refio.read_bc(tmp_path / "INPUT" / "bc.txt", series)
+    assert rec[:, 5].tolist() == [402, 402]
+    assert data[0, 1] == 0.0 and data[1, 1] == 1.0
+    assert data[1, 2] == np.finfo(np.float64).max and data[1, 4] == 0.8
+    t, v, per = series[0]
+    np.testing.assert_array_equal(t, [0.0, 0.5, 1.0])
+    np.testing.assert_array_equal(v, np.array([1.0, 1.2, 1.1]) * 1e5)   # var*1d+5, as the reference scales
+    assert not per
+    t, v, per = series[1]
+    np.testing.assert_array_equal(t, [0.0, 0.25])
+    assert per and v[0] == 0.9e5
+    with pytest.raises(ValueError):
+        refio.read_bc(tmp_path / "INPUT" / "bc.txt")
