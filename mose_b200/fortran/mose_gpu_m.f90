@@ -33,7 +33,7 @@ module mose_gpu_m
   end type mose_gpu_config
 
   public :: mose_gpu_default_config, mose_gpu_create, mose_gpu_destroy, mose_gpu_last_error
-  public :: mose_gpu_add_block, mose_gpu_set_bcs, mose_gpu_setup
+  public :: mose_gpu_add_block, mose_gpu_set_bcs, mose_gpu_add_series, mose_gpu_setup
   public :: mose_gpu_upload_prim, mose_gpu_download_prim, mose_gpu_download_residual, mose_gpu_upload_residual
   public :: mose_gpu_compute_dt, mose_gpu_set_global_dt, mose_gpu_copy_state, mose_gpu_fill_ghosts
   public :: mose_gpu_residual, mose_gpu_rk_stage, mose_gpu_step, mose_gpu_residual_norms
@@ -69,6 +69,13 @@ module mose_gpu_m
       integer(c_int32_t), intent(in) :: rec(15, *)
       real(c_double), intent(in) :: dat(6, *)
       integer(c_int32_t), value :: nbound
+    end function
+    integer(c_int) function mose_gpu_add_series(ctx, time, val, n, periodic, id) bind(C, name="mose_gpu_add_series")
+      import :: c_ptr, c_int, c_int32_t, c_double
+      type(c_ptr), value :: ctx
+      real(c_double), intent(in) :: time(*), val(*)
+      integer(c_int32_t), value :: n, periodic
+      integer(c_int32_t), intent(out) :: id
     end function
     integer(c_int) function mose_gpu_setup(ctx) bind(C, name="mose_gpu_setup")
       import :: c_ptr, c_int
