@@ -98,8 +98,10 @@ enum {
   MOSE_PRECISION_MIXED = 2         /* FP32 reconstruction + Riemann, FP64 state/accumulation */
 };
 
-/* integration-variables (Mod_Newstate.f90:30-44); only 'cons' is on this path */
-enum { MOSE_INTEGRATION_CONS = 0 };
+/* integration-variables (Mod_Newstate.f90:30-44): 'cons' (Newstate_Conservative)
+ * or 'prim' (Newstate_Primitive, Lib_Newstate.f90:168-317; reference-exact
+ * precision only) */
+enum { MOSE_INTEGRATION_CONS = 0, MOSE_INTEGRATION_PRIM = 1 };
 
 typedef struct mose_gpu_config {
   int32_t abi_version;     /* MOSE_GPU_ABI_VERSION */
@@ -109,7 +111,7 @@ typedef struct mose_gpu_config {
   int32_t ramp_iter;       /* cfl-rise-threshold */
   int32_t limiter;         /* MOSE_LIMITER_* */
   int32_t riemann;         /* MOSE_RIEMANN_* */
-  int32_t integration;     /* MOSE_INTEGRATION_CONS */
+  int32_t integration;     /* MOSE_INTEGRATION_CONS or _PRIM */
   int32_t precision;       /* MOSE_PRECISION_* */
   int32_t ndir;            /* 0: derived from block 1 as Check_Mesh_Type does */
   int32_t nsc;             /* number of species; must be 1 */

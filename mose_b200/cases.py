@@ -48,6 +48,7 @@ class Case:
     irs_beta: float = 0.0      # irs-beta: implicit residual smoothing when > 0
     sd_limiter: bool = False   # space-reconstruction MUSCL-SD (shock-detector scaled slopes)
     ramp_iter: int = 0         # cfl-rise-threshold: CFL ramped over the first iterations
+    integration: str = "cons"  # integration-variables: 'cons' or 'prim' (primitive RK update)
     gamma: float = 1.4
     rgas: float = 1.0
     steps: int = 1

@@ -60,6 +60,9 @@ struct Gas {
   // shock detector (SD_Tramel): bit 0 scales the limited slopes (MUSCL-SD),
   // bit 1 feeds the SD Riemann solvers (HLLC+, HLLE++)
   int sd;
+  // integration-variables = prim: the exact update advances the primitives
+  // (Newstate_Primitive) instead of the conservatives
+  int prim;
 };
 
 // Per-block descriptor (device resident).

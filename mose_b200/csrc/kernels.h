@@ -33,8 +33,8 @@ void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* ti
 // (update, Series_Data_m.f90:55-86), written into its BcParam.
 void launch_series_p0(const SeriesRec* recs, int n, const double* tv, const double* time, BcParam* bcp,
                       cudaStream_t s);
-void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, double* R, MetricArgs m, const double* dtl,
-                      const double* dtg, int use_dtg, cudaStream_t s);
+void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* R, MetricArgs m,
+                      const double* dtl, const double* dtg, int use_dtg, Gas g, cudaStream_t s);
 void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s);
 void launch_irs_jacobi(const BlockDesc* dblk, int nblk, long long maxcell, const double* R, const double* Rs,
                        double* out, int dir, double beta, cudaStream_t s);

@@ -510,9 +510,11 @@ __global__ void k_rk_stage(const BlockDesc* blk, double* P, const double* PO, co
 // layer of R and two Jacobi sweeps, then the RK stage on the smoothed
 // increment.
 // ---------------------------------------------------------------------------
-// Scale_Residual_Cons :98-103 (strangcoeff = 1): R = -(R / vol * dt)
-__global__ void k_irs_scale(const BlockDesc* blk, double* R, MetricArgs m, const double* dtl, const double* dtg,
-                            int use_dtg) {
+// Scale_Residual_Cons :98-103 (strangcoeff = 1): R = -(R / vol * dt); with
+// integration-variables = prim, Compute_Prim_Residual (:255-302) of the
+// stage's primitives P (Newstate_Primitive's IRS branch, :195-231)
+__global__ void k_irs_scale(const BlockDesc* blk, const double* P, double* R, MetricArgs m, const double* dtl,
+                            const double* dtg, int use_dtg, Gas g) {
   const int b = blockIdx.y;
   const BlockDesc& d = blk[b];
   const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
@@ -521,6 +523,13 @@ __global__ void k_irs_scale(const BlockDesc* blk, double* R, MetricArgs m, const
     const long long o = cell_off2(d, i, j);
     const double vol = m.vol[d.mbase + o];
     const double dt = use_dtg ? *dtg : dtl[d.mbase + o];
+    if (g.prim) {
+      double Q[4], Rv[4];
+      for (int v = 0; v < 4; ++v) { Q[v] = P[d.sbase + v * vs + o]; Rv[v] = R[d.sbase + v * vs + o]; }
+      prim_residual<4>(g, Q, Rv, vol, dt);
+      for (int v = 0; v < 4; ++v) R[d.sbase + v * vs + o] = Rv[v];
+      continue;
+    }
     for (int v = 0; v < 4; ++v) {
       double* r = R + d.sbase + v * vs + o;
       *r = -(*r / vol * dt);
@@ -566,6 +575,13 @@ __global__ void k_irs_update(const BlockDesc* blk, const double* Pin, const doub
     const long long o = d.sbase + cell_off2(d, i, j);
     double Q[4], QO[4], U[4], U0[4];
     for (int v = 0; v < 4; ++v) { Q[v] = Pin[o + v * vs]; QO[v] = PO[o + v * vs]; }
+    if (g.prim) {   // Newstate_Primitive :218-226: RK_stage on the smoothed primitive increment
+      double Rp[4];
+      for (int v = 0; v < 4; ++v) Rp[v] = R[o + v * vs];
+      if (!rk_prim_stage<4>(Q, QO, Rp, c)) report(err, 5, b, i, j, 0);
+      for (int v = 0; v < 4; ++v) Pout[o + v * vs] = Q[v];
+      continue;
+    }
     ex::prim2cons<4>(g, QO, U0);
     ex::prim2cons<4>(g, Q, U);
     for (int v = 0; v < 4; ++v) {
@@ -800,10 +816,10 @@ void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double*
     else k_rk_stage<4, false><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
   }
 }
-void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, double* R, MetricArgs m, const double* dtl,
-                      const double* dtg, int use_dtg, cudaStream_t s) {
+void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* R, MetricArgs m,
+                      const double* dtl, const double* dtg, int use_dtg, Gas g, cudaStream_t s) {
   dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
-  k_irs_scale<<<grid, 256, 0, s>>>(dblk, R, m, dtl, dtg, use_dtg);
+  k_irs_scale<<<grid, 256, 0, s>>>(dblk, P, R, m, dtl, dtg, use_dtg, g);
 }
 void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s) {
   if (n > 0) k_irs_ghost<<<(n + 255) / 256, 256, 0, s>>>(list, n, R);

@@ -344,7 +344,11 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   if (!cfg || !out) return MOSE_ERR_INVALID;
   *out = nullptr;
   if (cfg->abi_version != MOSE_GPU_ABI_VERSION) return MOSE_ERR_INVALID;
-  if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 || cfg->integration != MOSE_INTEGRATION_CONS ||
+  // integration-variables = prim runs in the reference-exact precision
+  if (cfg->integration == MOSE_INTEGRATION_PRIM && cfg->precision != MOSE_PRECISION_FP64_EXACT)
+    return MOSE_ERR_UNSUPPORTED;
+  if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 ||
+      (cfg->integration != MOSE_INTEGRATION_CONS && cfg->integration != MOSE_INTEGRATION_PRIM) ||
       cfg->limiter < 0 || cfg->limiter > 5 || cfg->riemann < 0 || cfg->riemann > MOSE_RIEMANN_EXACT ||
       cfg->precision < 0 || cfg->precision > 2 || !(cfg->gamma > 1.0) || !(cfg->rgas > 0.0))
     return MOSE_ERR_UNSUPPORTED;
@@ -379,6 +383,7 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   ctx->gas.rie = cfg->riemann;
   ctx->gas.minf = 0.0;
   ctx->gas.sd = (cfg->riemann == MOSE_RIEMANN_HLLC_SD || cfg->riemann == MOSE_RIEMANN_HLLE_PP) ? 2 : 0;
+  ctx->gas.prim = cfg->integration == MOSE_INTEGRATION_PRIM ? 1 : 0;
   *out = ctx;
   return MOSE_OK;
 }
@@ -1112,8 +1117,8 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
     // RK_Newstate with IRS on the residual of mose_gpu_residual, dt from
     // dtlocal (Compute_dt / Set_Global_dt of the phase path)
     const int nb = (int)ctx->hblk.size();
-    launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->scal.p, 0,
-                     ctx->stream);
+    launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[ctx->cur].p, ctx->resid.p, ctx->margs(), ctx->dtl.p,
+                     ctx->scal.p, 0, ctx->gas, ctx->stream);
     ctx->launches += 1 + enqueue_irs_smoothing(ctx);
     launch_irs_update(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[ctx->cur].p, ctx->state[ctx->po].p, ctx->resid.p,
                       ctx->state[ctx->cur].p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->derr.p,
@@ -1188,8 +1193,8 @@ static int enqueue_irs_stage(mose_gpu_ctx* ctx, int pc, int s0, int pn, int irk)
   StageArgs a = stage_args(ctx, pc, s0, -1, irk);
   int k = launch_stage(ctx, a, 1, MOSE_PRECISION_FP64_EXACT, false);
   const int nb = (int)ctx->hblk.size();
-  launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->scal.p,
-                   ctx->cfg.time_accurate, ctx->stream);
+  launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[pc].p, ctx->resid.p, ctx->margs(), ctx->dtl.p,
+                   ctx->scal.p, ctx->cfg.time_accurate, ctx->gas, ctx->stream);
   k += 1 + enqueue_irs_smoothing(ctx);
   launch_irs_update(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[pc].p, ctx->state[s0].p, ctx->resid.p,
                     ctx->state[pn].p, ctx->gas, a.c_rk, ctx->derr.p, ctx->stream);
@@ -1446,6 +1451,7 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
   if (ctx->cfg.ramp_iter > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no cfl ramp");
   if (ctx->irs_beta > 0.0 || ctx->gas.sd) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no IRS or shock detector");
   if (ctx->nser) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no time-table (402) inlets");
+  if (ctx->gas.prim) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: conservative integration variables only");
   const size_t ns = (size_t)ctx->nv * ctx->marena, m = (size_t)ctx->marena;
   for (DevBuf<double>* b : {&ctx->lam, &ctx->lam_loc, &ctx->lam_n, &ctx->lamR, &ctx->wdt, &ctx->lamG})
     if (b->alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");

@@ -109,12 +109,68 @@ __device__ __noinline__ int boundary_flux(const StageArgs& a, int w, const doubl
   return ADD_MOMENTUM;
 }
 
-// Newstate_Conservative for one cell (Lib_Newstate.f90:134-160); returns the
-// new primitives in Q.  first_stage: P == PO, so U - U0 is an exact zero.
+// Compute_Prim_Residual (Lib_Newstate.f90:255-302, one calorically perfect
+// species): the conservative residual R of a cell with primitives Q turned,
+// in place, into its primitive increment over dt.  In 2-D the reference's
+// w terms are exact zeros.
+template <int NV>
+__device__ __forceinline__ void prim_residual(const Gas& g, const double* Q, double* R, double vol, double dt) {
+  constexpr int P = NV - 1;
+  const double rho = Q[0];
+  const double temperature = Q[P] / (rho * g.R);
+  const double inv_volume = 1.0 / vol;
+  const double inv_rhovolume = inv_volume / rho;
+  R[0] = -R[0] * inv_volume;
+  const double dwrotot = R[0];
+  for (int d = 0; d < NV - 2; ++d) R[1 + d] = -R[1 + d] * inv_rhovolume - Q[1 + d] / rho * dwrotot;
+  const double dwE = -R[P] * inv_volume;
+  double vr = Q[1] * R[1] + Q[2] * R[2];
+  if constexpr (NV == 5) vr = vr + Q[3] * R[3];
+  const double dwroe = dwE - rho * vr - 0.5 * dwrotot * ex::vel_sq<NV>(Q);
+  const double eiroi = (g.cp * temperature - g.R * temperature) * R[0];
+  const double cv = Q[0] * (g.cp - g.R);
+  const double dwTemp = (dwroe - eiroi) / cv;
+  R[P] = g.R * (temperature * R[0] + Q[0] * dwTemp);
+  for (int v = 0; v < NV; ++v) R[v] = R[v] * dt * 1.0;
+}
+
+// RK_Stage on the primitives and Check_And_Fix_State (Lib_RK.f90:15-27,
+// Lib_Newstate.f90:323-356): Q = QO + c ((Q - QO) + Rp).  first_stage: QO
+// equals Q and is not read (the stage kernels do not load it then).
+template <int NV>
+__device__ __forceinline__ bool rk_prim_stage(double* Q, const double* QO, const double* Rp, double c,
+                                              bool first_stage = false) {
+  constexpr int P = NV - 1;
+  for (int v = 0; v < NV; ++v) {
+    if (first_stage) {
+      const double r_ = (0.0 + Rp[v]) * c;
+      Q[v] = Q[v] + r_;
+    } else {
+      const double r_ = (Q[v] - QO[v] + Rp[v]) * c;
+      Q[v] = QO[v] + r_;
+    }
+  }
+  bool bad = false;
+  for (int v = 0; v < NV; ++v) bad |= isnan(Q[v]);
+  bad |= (Q[P] < 0.0);
+  if (Q[0] < 1e-20) Q[0] = 1e-20;
+  return !bad;
+}
+
+// Newstate_Conservative for one cell (Lib_Newstate.f90:134-160), or
+// Newstate_Primitive's Compute_And_Update_Prim (:305-315) when g.prim;
+// returns the new primitives in Q.  first_stage: P == PO, so U - U0 is an
+// exact zero.
 template <int NV>
 __device__ __forceinline__ bool rk_update(const Gas& g, double* Q, const double* QO, const double* R,
                                           double vol, double dt, double c, bool first_stage) {
   constexpr int P = NV - 1;
+  if (g.prim) {
+    double Rp[NV];
+    for (int v = 0; v < NV; ++v) Rp[v] = R[v];
+    prim_residual<NV>(g, Q, Rp, vol, dt);
+    return rk_prim_stage<NV>(Q, QO, Rp, c, first_stage);
+  }
   double U[NV], U0[NV];
   ex::prim2cons<NV>(g, Q, U);
   if (first_stage) {

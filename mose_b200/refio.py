@@ -236,6 +236,8 @@ def read_input_ini(path) -> dict:
         kw["ramp_iter"] = int(num["cfl-rise-threshold"])
     if "irs-beta" in num:
         kw["irs_beta"] = float(num["irs-beta"])
+    if "integration-variables" in num:
+        kw["integration"] = num["integration-variables"].strip().lower()
     kw["unsupported"] = unsupported
     return kw
 
@@ -260,11 +262,14 @@ def load_case(case_dir, resolution: str = "", gamma: float | None = None, rgas: 
         gamma = cp / (cp - rgas)
     if kw.get("limiter") is not None and kw["limiter"] not in LIMITERS:
         unsupported.append(f"flux-limiter = {kw['limiter']}")
+    if kw.get("integration", "cons") not in ("cons", "prim"):
+        unsupported.append(f"integration-variables = {kw.pop('integration')}")
     if kw.get("riemann") is not None and kw["riemann"] not in RIEMANN:
         unsupported.append(f"riemann-solver = {kw['riemann']}")
     case = Case(d.name + sfx, nodes, rec, data, prim, gamma=gamma, rgas=rgas,
                 **{k: v for k, v in kw.items() if k in ("cfl", "n_rk", "time_accurate", "riemann", "minf", "limiter",
-                                                        "t_end", "steps", "irs_beta", "sd_limiter", "ramp_iter")})
+                                                        "t_end", "steps", "irs_beta", "sd_limiter", "ramp_iter",
+                                                        "integration")})
     case.series = series
     case.extra["unsupported"] = unsupported
     return case

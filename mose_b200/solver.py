@@ -60,6 +60,7 @@ class Solver:
         cfg.gamma = case.gamma
         cfg.rgas = case.rgas
         cfg.ramp_iter = int(getattr(case, "ramp_iter", 0))
+        cfg.integration = {"cons": 0, "prim": 1}[getattr(case, "integration", "cons")]
         cfg.device = device
         h = C.c_void_p()
         rc = self.lib.mose_gpu_create(C.byref(cfg), C.byref(h))

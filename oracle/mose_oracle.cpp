@@ -2239,6 +2239,30 @@ static void residual_smoothing(orc_domain* d, double beta) {
   }
 }
 
+// Compute_Prim_Residual, Lib_Newstate.f90:255-302 (one calorically perfect
+// species): the conservative residual of a cell turned, in place, into the
+// increment of its primitives over dt.
+static void prim_residual(const Thermo& t, const double* prim, double* res, double dt, double volume,
+                          double strangcoeff) {
+  double rho, Rgas;
+  co_rotot_Rtot(t, prim[0], rho, Rgas);
+  double temperature = prim[NP] / (rho * Rgas);
+  double inv_volume = 1.0 / volume;
+  double inv_rhovolume = inv_volume / rho;
+  double velocity[3] = {prim[NU], prim[NV], prim[NW]};
+  res[0] = -res[0] * inv_volume;
+  double dwrotot = res[0];
+  for (int q = 0; q < 3; ++q) res[NU + q] = -res[NU + q] * inv_rhovolume - velocity[q] / rho * dwrotot;
+  double dwE = -res[NP] * inv_volume;
+  double dwroe = dwE - rho * (velocity[0] * res[NU] + velocity[1] * res[NV] + velocity[2] * res[NW]) -
+                 0.5 * dwrotot * (velocity[0] * velocity[0] + velocity[1] * velocity[1] + velocity[2] * velocity[2]);
+  double eiroi = (t.cp * temperature - t.R * temperature) * res[0];
+  double cv = prim[0] * (t.cp - t.R);
+  double dwTemp = (dwroe - eiroi) / cv;
+  res[NP] = t.R * (temperature * res[0] + prim[0] * dwTemp);
+  for (int v = 0; v < NPRIM; ++v) res[v] = res[v] * dt * strangcoeff;
+}
+
 // RK_Newstate => Newstate_Conservative / Newstate_Primitive, Lib_Newstate.f90
 int orc_rk_newstate(orc_domain* d, int irk) {
   static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};  // Lib_RK.f90:8-11
@@ -2247,6 +2271,35 @@ int orc_rk_newstate(orc_domain* d, int irk) {
   const double strangcoeff = 1.0;
   const Thermo& t = d->th;
   const bool prim_mode = d->cfg.integration == ORC_INT_PRIM;
+  if (d->cfg.irs_beta > 0.0 && prim_mode) {
+    // Newstate_Primitive with IRS, Lib_Newstate.f90:195-231: every residual
+    // to primitive increments, smooth, then RK_stage and Check_And_Fix_State
+    for (Block& B : d->blk)
+      for (int k = 1; k <= B.nk; ++k)
+        for (int j = 1; j <= B.nj; ++j)
+          for (int i = 1; i <= B.ni; ++i)
+            prim_residual(t, B.Pc(i, j, k), B.Rc(i, j, k), B.dtlocal[B.inner(i, j, k)], B.vol_(i, j, k), strangcoeff);
+    residual_smoothing(d, d->cfg.irs_beta);
+    for (int bi = 0; bi < (int)d->blk.size(); ++bi) {
+      Block& B = d->blk[bi];
+      for (int k = 1; k <= B.nk; ++k)
+        for (int j = 1; j <= B.nj; ++j)
+          for (int i = 1; i <= B.ni; ++i) {
+            double* prim = B.Pc(i, j, k);
+            const double* primold = B.POc(i, j, k);
+            const double* res = B.Rc(i, j, k);
+            for (int v = 0; v < NPRIM; ++v) {
+              double r_ = (prim[v] - primold[v] + res[v]) * c;
+              prim[v] = primold[v] + r_;
+            }
+            bool nan = false;
+            for (int v = 0; v < NPRIM; ++v) nan |= std::isnan(prim[v]);
+            if (nan || prim[NP] < 0.0) d->fail(ORC_ERR_NAN_OR_NEG_P, bi + 1, i, j, k);
+            if (prim[0] < 1e-20) prim[0] = 1e-20;
+          }
+    }
+    return d->err;
+  }
   if (d->cfg.irs_beta > 0.0 && !prim_mode) {
     // Newstate_Conservative with IRS, Lib_Newstate.f90:40-72: scale every
     // residual (Scale_Residual_Cons), smooth, then Update_State_Cons_IRS
@@ -2313,24 +2366,8 @@ int orc_rk_newstate(orc_domain* d, int irk) {
             (void)temperature;                        // T_guess: closed-form cons2prim
             cons2prim(t, cons, prim);
           } else {
-            // Compute_Prim_Residual :255-302 + RK_Stage (one calorically perfect species)
-            double rho, Rgas;
-            co_rotot_Rtot(t, prim[0], rho, Rgas);
-            double temperature = prim[NP] / (rho * Rgas);
-            double inv_volume = 1.0 / volume;
-            double inv_rhovolume = inv_volume / rho;
-            double velocity[3] = {prim[NU], prim[NV], prim[NW]};
-            res[0] = -res[0] * inv_volume;
-            double dwrotot = res[0];
-            for (int q = 0; q < 3; ++q) res[NU + q] = -res[NU + q] * inv_rhovolume - velocity[q] / rho * dwrotot;
-            double dwE = -res[NP] * inv_volume;
-            double dwroe = dwE - rho * (velocity[0] * res[NU] + velocity[1] * res[NV] + velocity[2] * res[NW]) -
-                           0.5 * dwrotot * (velocity[0] * velocity[0] + velocity[1] * velocity[1] + velocity[2] * velocity[2]);
-            double eiroi = (t.cp * temperature - t.R * temperature) * res[0];
-            double cv = prim[0] * (t.cp - t.R);
-            double dwTemp = (dwroe - eiroi) / cv;
-            res[NP] = t.R * (temperature * res[0] + prim[0] * dwTemp);
-            for (int v = 0; v < NPRIM; ++v) res[v] = res[v] * dt * strangcoeff;
+            // Compute_And_Update_Prim :305-315: Compute_Prim_Residual, then RK_Stage
+            prim_residual(t, prim, res, dt, volume, strangcoeff);
             for (int v = 0; v < NPRIM; ++v) {
               double r_ = (prim[v] - primold[v] + res[v]) * c;
               prim[v] = primold[v] + r_;

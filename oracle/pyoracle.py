@@ -93,7 +93,8 @@ class Oracle:
     def __init__(self, case, nthreads: int = 1, omp: bool = False, ndir: int = 0):
         self.lib = load(omp)
         cfg = orc_config(n_rk=case.n_rk, cfl=case.cfl, time_accurate=int(case.time_accurate),
-                         limiter=LIMITERS[case.limiter], riemann=RIEMANN[case.riemann], integration=0,
+                         limiter=LIMITERS[case.limiter], riemann=RIEMANN[case.riemann],
+                         integration={"cons": 0, "prim": 1}[getattr(case, "integration", "cons")],
                          ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=int(getattr(case, "ramp_iter", 0)),
                          res_diter=1,
                          minf=getattr(case, "minf", 0.0), irs_beta=getattr(case, "irs_beta", 0.0),

@@ -468,3 +468,48 @@ def test_time_table_inlet_with_constant_table_is_401(oracle_mod):
             o.step()
         out.append(o.get_prim(1))
     assert np.array_equal(out[0], out[1])
+
+
+def _one_euler_stage(oracle_mod, make, integration, cfl, irs=0.0):
+    case = make(cfl)
+    case.n_rk = 1
+    case.integration = integration
+    case.irs_beta = irs
+    o = oracle_mod.Oracle(case)
+    P0 = [o.get_prim(b).copy() for b in range(1, len(case.nodes) + 1)]
+    o.step()
+    return P0, [o.get_prim(b) for b in range(1, len(case.nodes) + 1)]
+
+
+def _maxdiff(A, B):
+    return max(np.abs(a - b)[2:-2, 2:-2, 2:-2].max() for a, b in zip(A, B))
+
+
+def test_primitive_update_matches_conservative_to_second_order(oracle_mod):
+    """Newstate_Primitive (Lib_Newstate.f90:168-317) linearises the
+    conservative update: after one forward-Euler stage from the same state
+    the primitive and conservative results differ by O(dt^2), far less than
+    the O(dt) change of the state, and the difference shrinks about 4x when
+    dt halves (four-quadrant blocks)."""
+    make = lambda cfl: cases.four_quadrant(seed=1, nbx=2, nby=2, nmin=12, nmax=20, steps=1, cfl=cfl)
+    gaps = []
+    for cfl in (0.2, 0.1):
+        P0, Pc = _one_euler_stage(oracle_mod, make, "cons", cfl)
+        _, Pp = _one_euler_stage(oracle_mod, make, "prim", cfl)
+        gap, change = _maxdiff(Pp, Pc), _maxdiff(Pc, P0)
+        assert 0.0 < gap < 0.1 * change, (gap, change)
+        gaps.append(gap)
+    assert 3.0 < gaps[0] / gaps[1] < 5.0, gaps
+
+
+def test_primitive_update_with_irs_is_continuous_in_beta(oracle_mod):
+    """The IRS branch of Newstate_Primitive (:195-231: primitive increments,
+    smoothing, RK stage) tends to the plain primitive update as irs-beta
+    goes to 0, linearly in beta."""
+    make = lambda cfl: cases.isentropic_vortex(40, steps=1, cfl=cfl)
+    _, P = _one_euler_stage(oracle_mod, make, "prim", 0.3)
+    d = []
+    for beta in (2e-3, 1e-3):
+        _, Pb = _one_euler_stage(oracle_mod, make, "prim", 0.3, irs=beta)
+        d.append(_maxdiff(Pb, P))
+    assert 0.0 < d[1] < d[0] < 1e-3 and 1.8 < d[0] / d[1] < 2.2, d
