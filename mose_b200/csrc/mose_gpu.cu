@@ -501,9 +501,11 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if (ctx->gas.sd) {
     // the detector reads the four face neighbours of every 2-D cell
     if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector runs on 2-D domains");
+    // (a one-row block, the 1-D cases, reads its j pair from the zero-gradient
+    // ghost rows of its null faces: an exact 0, as in the reference)
     for (const auto& h : ctx->hblk)
-      if (h.ni < 3 || h.nj < 3)
-        return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector needs blocks of at least 3 x 3 cells");
+      if (h.ni < 3 || (h.nj < 3 && h.nj != 1))
+        return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector needs blocks of at least 3 x 3 cells, or 1-D rows");
   }
   if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");

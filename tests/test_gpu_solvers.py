@@ -141,3 +141,40 @@ def test_exact_solver_fp64_within_1e12_per_step(oracle_mod):
     s.explicit_step()
     assert _per_var_rel(s, o, len(case.nodes)) <= 1e-12
     assert _per_var_rel(s, o, len(case.nodes), base=base) <= 1e-12
+
+
+def test_tor99_reference_inputs(oracle_mod):
+    """The reference's Tor99 case (HLLE++ with the shock detector, 800
+    cells) to its final time; the detector calls tanh, hence the 1e-12
+    normwise bar."""
+    from tests.test_oracle import vv_case
+    case, _ = vv_case("tor99_x8")
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    n = 0
+    while o.time < case.t_end:
+        o.step()
+        s.explicit_step()
+        n += 1
+    assert n > 400
+    compare_state(s, o, 1, exact=False, tol=1e-12)
+
+
+def test_noh87_reference_inputs_stop_like_the_oracle(oracle_mod):
+    """Noh87's cold inflow stops the run on the GPU at the same step and with
+    the same code (non-physical interface state) as in the oracle."""
+    from mose_b200 import MoseError
+    from tests.test_oracle import vv_case
+    case, _ = vv_case("noh87_x8")
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for n in range(1000):
+        try:
+            o.step()
+        except RuntimeError:
+            break
+        s.explicit_step()
+    with pytest.raises(MoseError) as ei:
+        s.explicit_step()
+    code, _ = o.last_error()
+    assert ei.value.code == code == 4 and n > 100, (ei.value, code, n)
