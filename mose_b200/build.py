@@ -28,9 +28,9 @@ UNITS = {
     **{f"stage_exact_r{r}.cu": ["--fmad=false"] for r in range(5)},
     **{f"stage_fp64_r{r}.cu": [] for r in range(5)},
     **{f"stage_mixed_r{r}.cu": [] for r in range(5)},
-    **{f"stage3d_exact_r{r}.cu": ["--fmad=false"] for r in range(2)},
-    **{f"stage3d_fp64_r{r}.cu": [] for r in range(2)},
-    **{f"stage3d_mixed_r{r}.cu": [] for r in range(2)},
+    **{f"stage3d_exact_r{r}.cu": ["--fmad=false"] for r in (0, 1, 4)},
+    **{f"stage3d_fp64_r{r}.cu": [] for r in (0, 1, 4)},
+    **{f"stage3d_mixed_r{r}.cu": [] for r in (0, 1, 4)},
     "mose_gpu.cu": [],
     "norms_noalloc.cu": [],
     "fastmath_check.cu": [],

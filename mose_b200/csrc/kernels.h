@@ -115,21 +115,22 @@ inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int 
   return table[prec][(rie < 4 && a.g.sd == 0) ? rie : 4](a, nsm, mode, uni, lim, s);
 }
 
-// 3-D: three directional sweeps per RK stage; HLLC and AUSM+ with minmod,
-// van Leer or van Albada.
+// 3-D: three directional sweeps per RK stage; HLLC and AUSM+ compiled in,
+// every other solver through the run-time solver unit (r4, no shock
+// detector in 3-D); all six limiters.
 #define MOSE_STAGE3_DECL(p, r) \
   bool launch_stage3d_p##p##_r##r(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s);
-MOSE_STAGE3_DECL(0, 0) MOSE_STAGE3_DECL(0, 1) MOSE_STAGE3_DECL(1, 0) MOSE_STAGE3_DECL(1, 1)
-MOSE_STAGE3_DECL(2, 0) MOSE_STAGE3_DECL(2, 1)
+MOSE_STAGE3_DECL(0, 0) MOSE_STAGE3_DECL(0, 1) MOSE_STAGE3_DECL(0, 4) MOSE_STAGE3_DECL(1, 0) MOSE_STAGE3_DECL(1, 1)
+MOSE_STAGE3_DECL(1, 4) MOSE_STAGE3_DECL(2, 0) MOSE_STAGE3_DECL(2, 1) MOSE_STAGE3_DECL(2, 4)
 #undef MOSE_STAGE3_DECL
-inline bool stage3d_supported(int rie, int lim) { return rie >= 0 && rie <= 1 && lim >= 1 && lim <= 3; }
+inline bool stage3d_supported(int rie, int lim) { return rie >= 0 && rie <= 14 && lim >= 0 && lim <= 5; }
 inline bool launch_stage3d(const StageArgs& a, int nsm, int mode, bool uni, int prec, int rie, int lim,
                            cudaStream_t s) {
   using L = bool (*)(const StageArgs&, int, int, bool, int, cudaStream_t);
-  static const L table[3][2] = {{launch_stage3d_p0_r0, launch_stage3d_p0_r1},
-                                {launch_stage3d_p1_r0, launch_stage3d_p1_r1},
-                                {launch_stage3d_p2_r0, launch_stage3d_p2_r1}};
+  static const L table[3][3] = {{launch_stage3d_p0_r0, launch_stage3d_p0_r1, launch_stage3d_p0_r4},
+                                {launch_stage3d_p1_r0, launch_stage3d_p1_r1, launch_stage3d_p1_r4},
+                                {launch_stage3d_p2_r0, launch_stage3d_p2_r1, launch_stage3d_p2_r4}};
   if (prec < 0 || prec > 2 || !stage3d_supported(rie, lim)) return false;
-  return table[prec][rie](a, nsm, mode, uni, lim, s);
+  return table[prec][rie <= 1 ? rie : 2](a, nsm, mode, uni, lim, s);
 }
 }  // namespace mose

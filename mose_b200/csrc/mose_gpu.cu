@@ -510,7 +510,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");
   if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
-    return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: HLLC or AUSM+ with minmod, van Leer or van Albada");
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: no stage kernel for riemann %d, limiter %d",
+                ctx->cfg.riemann, ctx->cfg.limiter);
   if (ctx->nd != 3 && !stage2d_supported(ctx->cfg.riemann, ctx->cfg.precision))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "no stage kernel for riemann %d in precision %d", ctx->cfg.riemann,
                 ctx->cfg.precision);

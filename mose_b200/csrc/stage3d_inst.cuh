@@ -1,7 +1,8 @@
 // stage3d_inst.cuh -- launch dispatch of the 3-D sweeps over arithmetic
 // policy, limiter and metric mode.  Each translation unit
 // stage3d_<precision>_r<solver>.cu instantiates one (precision, Riemann
-// solver) pair for the minmod, van Leer and van Albada limiters.
+// solver) pair for the six limiters (first order, minmod, van Leer, van
+// Albada, MC, superbee).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -58,9 +59,12 @@ static bool stage3d_dispatch_uni(const StageArgs& a, int nsm, int mode, bool uni
 template <int PREC, int RIE>
 static bool stage3d_dispatch_lim(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s) {
   switch (lim) {
+    case 0: return stage3d_dispatch_uni<PREC, RIE, 0>(a, nsm, mode, uni, s);
     case 1: return stage3d_dispatch_uni<PREC, RIE, 1>(a, nsm, mode, uni, s);
     case 2: return stage3d_dispatch_uni<PREC, RIE, 2>(a, nsm, mode, uni, s);
     case 3: return stage3d_dispatch_uni<PREC, RIE, 3>(a, nsm, mode, uni, s);
+    case 4: return stage3d_dispatch_uni<PREC, RIE, 4>(a, nsm, mode, uni, s);
+    case 5: return stage3d_dispatch_uni<PREC, RIE, 5>(a, nsm, mode, uni, s);
   }
   return false;
 }

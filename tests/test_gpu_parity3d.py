@@ -150,3 +150,56 @@ def test_mixed_3d_density_error(oracle_mod, name):
         num += float(((g - r) ** 2).sum())
         den += float((r ** 2).sum())
     assert np.sqrt(num / den) < 1e-6, np.sqrt(num / den)
+
+
+# every solver of the run-time unit and every limiter on the 3-D sweeps
+SOLVERS3 = ["SLAU", "SLAU2", "HLLE", "HLLEM", "LLF", "PLLF", "Hanel", "AUSM+-up", "AUSM+-up2", "HLLC Rotated",
+            "exact"]
+LIMITERS3 = ["first-order", "mc", "superbee"]
+
+
+def _box(riemann="HLLC", limiter="vanleer", seed=5, steps=2):
+    case = cases.periodic_box_3d(sizes=[[6, 7], [7, 5], [5, 6]], seed=seed, steps=steps, limiter=limiter,
+                                 riemann=riemann, amp=5e-2)
+    case.minf = 0.3
+    return case
+
+
+@pytest.mark.parametrize("riemann", SOLVERS3)
+def test_runtime_solvers_3d(oracle_mod, riemann):
+    """The run-time solver unit on the 3-D sweeps: bit for bit, except the
+    exact solver (pow: the 1e-12 normwise bar)."""
+    case = _box(riemann)
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(2):
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, len(case.nodes), exact=riemann != "exact")
+    for _ in range(2):
+        o.step()
+    s.advance(2)
+    compare_state(s, o, len(case.nodes), exact=riemann != "exact")
+
+
+@pytest.mark.parametrize("limiter", LIMITERS3)
+@pytest.mark.parametrize("riemann", ["HLLC", "AUSM+", "HLLE"])
+def test_limiters_3d(oracle_mod, riemann, limiter):
+    case = _box(riemann, limiter)
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(3):
+        o.step()
+        s.explicit_step()
+    compare_state(s, o, len(case.nodes))
+
+
+@pytest.mark.parametrize("riemann", ["HLLE", "exact"])
+def test_runtime_solvers_3d_fp64_within_1e12(oracle_mod, riemann):
+    from mose_b200 import _lib
+    case = _box(riemann, "vanalbada")
+    o = oracle_mod.Oracle(case)
+    s = solver(case, precision=_lib.PRECISION_FP64)
+    o.step()
+    s.explicit_step()
+    compare_state(s, o, len(case.nodes), exact=False, tol=1e-12)
