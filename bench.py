@@ -125,13 +125,21 @@ def barrier(world):
 
 
 def max_over_ranks(x, world):
+    """The maximum of x over the ranks (NCCL on the GPUs, gloo on the host)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(world, cells, steps, ms):
+    """Whole-job throughput: every rank advances its own replica of `cells`
+    cells by `steps` steps; `ms` is the slowest rank's time."""
+    return world * cells * steps / (ms / 1e3)
 
 
 def cpu_baseline(seconds=15.0, n=512):
@@ -155,7 +163,9 @@ def cpu_baseline(seconds=15.0, n=512):
 
 
 def run_reference(args):
-    world, rank, _ = dist_init()
+    # the CPU arm: rank 0 alone times the oracle; no process group is needed
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import pyoracle
@@ -422,7 +432,7 @@ def run_gpu(args):
     clk = ClockSampler(local)
     ms = time_advance(s, stream, args.steps, world, clk)
     launches = s.launch_count - launches0
-    value = world * cells * args.steps / (ms / 1e3)
+    value = aggregate(world, cells, args.steps, ms)
     stage_ms, achieved, step_ms = stage_roofline(s, args.steps, cells)
     # --- end to end through the C ABI with host buffers ----------------------
     shape = (1 + 4, N_CELLS_SIDE + 4, N_CELLS_SIDE + 4, 5)
@@ -450,11 +460,12 @@ def run_gpu(args):
         v.advance(3)
         vms = time_advance(v, vstream, args.steps, world)
         v_stage_ms, v_ach, v_step = stage_roofline(v, args.steps, cells)
-        variants[name] = {"value": world * cells * args.steps / (vms / 1e3), "ms_per_step": vms / args.steps,
+        variants[name] = {"value": aggregate(world, cells, args.steps, vms), "ms_per_step": vms / args.steps,
                           "stage_ms": v_stage_ms, "roofline_frac": v_ach / peak, "step_kernel_ms": v_step}
         v.close()
+    # the reports beside the headline run once, on rank 0 of a one-GPU run
     err = mixed_error(local) if rank == 0 else None
-    extra = extra_configs(local) if (rank == 0 and not args.no_extra_configs) else None
+    extra = extra_configs(local) if (rank == 0 and world == 1 and not args.no_extra_configs) else None
     if rank == 0:
         variants.setdefault("mixed", {})["error_vs_fp64_oracle"] = err
         line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
@@ -477,7 +488,7 @@ def run_gpu(args):
                 "variants": variants}
         if extra is not None:
             line["configs"] = extra
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     if world > 1:
