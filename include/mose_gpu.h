@@ -274,6 +274,23 @@ int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta);
  * only: the 3-D sweeps run HLLC and AUSM+. */
 int mose_gpu_set_riemann_minf(mose_gpu_ctx* ctx, double minf);
 
+/* Tiling of the 2-D work list that the persistent stage kernels walk (no
+ * counterpart in the reference, whose OpenMP loops have no work list):
+ * tiling[0] rows per item (0: the planner's load-balance model), [1] largest
+ * strip width in cells (8..62), [2] item order (0: a block's row bands in
+ * turn, neighbouring strips side by side; 1: its strips in turn), [3] CTAs
+ * per SM of the persistent grid (0: the occupancy limit).  Results do not
+ * depend on the tiling: every face flux and cell update is the same
+ * arithmetic whichever CTA does it. */
+int mose_gpu_set_tiling(mose_gpu_ctx* ctx, const int32_t tiling[4]);
+int mose_gpu_get_tiling(const mose_gpu_ctx* ctx, int32_t tiling[4]);
+/* Autotuner (no counterpart in the reference): times candidate tilings on
+ * the context's own domain, `steps` full steps each from the current state
+ * (restored afterwards), keeps the fastest and returns it with its time per
+ * step and the default's.  Call after the state is uploaded; 2-D only. */
+int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t tiling_out[4], double* best_ms_per_step,
+                      double* default_ms_per_step);
+
 /* Sets the Mach number of every 405 supersonic-inflow face. */
 int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach);
 /* Runs nsteps fused steps from the current state keeping a checkpoint of the

@@ -75,6 +75,9 @@ SIGNATURES = {
     "mose_gpu_set_irs_beta": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_sd_limiter": (C.c_int, [_D, C.c_int32]),
     "mose_gpu_add_series": (C.c_int, [_D, _dp, _dp, C.c_int32, C.c_int32, _ip]),
+    "mose_gpu_set_tiling": (C.c_int, [_D, _ip]),
+    "mose_gpu_get_tiling": (C.c_int, [_D, _ip]),
+    "mose_gpu_autotune": (C.c_int, [_D, C.c_int32, _ip, _dp, _dp]),
     "mose_gpu_adjoint_forward": (C.c_int, [_D, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]),
     "mose_gpu_adjoint_backward": (C.c_int, [_D, _dp]),
     "mose_gpu_adjoint_step": (C.c_int, [_D, _dp]),

@@ -44,6 +44,8 @@ struct StageArgs {
   // 3-D work lists: [0] i-sweep rows, [1] j-march columns, [2] k-march columns
   const int4* items3[3];
   int nitems3[3];
+  // persistent 2-D grid: at most this many CTAs per SM (0: the occupancy limit)
+  int grid_cap;
 };
 
 }  // namespace mose

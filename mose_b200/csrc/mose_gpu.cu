@@ -73,28 +73,34 @@ std::vector<int> split_even(int n, int parts, int q) {
 }
 
 // Work items of the 2-D stage kernel: (block, c0 | c1 << 16, j0, j1).
-// Every block's columns split into ceil(ni / SB_W) strips of nearly equal
-// width starting on even columns (16-byte aligned row copies); its rows into
-// runs of about H rows in whole batches.  H is the candidate whose
-// round-robin assignment over the persistent grid has the smallest makespan,
-// an item costing its batches plus about two for the prologue and the first
-// copies.
-std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int grid) {
+// Every block's columns split into ceil(ni / wmax) strips (wmax <= SB_W) of
+// nearly equal width starting on even columns (16-byte aligned row copies);
+// its rows into runs of about H rows in whole batches.  order 0 lists a
+// block's items row band by row band (neighbouring strips of one band run
+// side by side and share their halo columns in L2), order 1 strip by strip.
+// H = 0 takes the candidate whose round-robin assignment over the
+// persistent grid has the smallest makespan, an item costing its batches
+// plus about two for the prologue and the first copies.
+std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int grid, int Hset = 0, int wmax = SB_W,
+                                   int order = 0) {
   auto build = [&](int H) {
     std::vector<int4> items;
     for (int b = 0; b < (int)blocks.size(); ++b) {
       const HostBlock& h = blocks[b];
-      const int ns = (h.ni + SB_W - 1) / SB_W;
+      const int ns = (h.ni + wmax - 1) / wmax;
       const std::vector<int> cc = split_even(h.ni, ns, 2);
       const int nr = std::max(1, (h.nj + H / 2) / H);
       const std::vector<int> rc = split_even(h.nj, std::min(nr, (h.nj + SB_Y - 1) / SB_Y), SB_Y);
-      for (size_t r = 0; r + 1 < rc.size(); ++r)
-        for (int s = 0; s < ns; ++s)
-          if (rc[r + 1] > rc[r] && cc[s + 1] > cc[s])
-            items.push_back(make_int4(b, cc[s] | (cc[s + 1] << 16), rc[r], rc[r + 1]));
+      const int nrr = (int)rc.size() - 1;
+      for (int o = 0; o < nrr * ns; ++o) {
+        const int r = order == 0 ? o / ns : o % nrr, s = order == 0 ? o % ns : o / nrr;
+        if (rc[r + 1] > rc[r] && cc[s + 1] > cc[s])
+          items.push_back(make_int4(b, cc[s] | (cc[s + 1] << 16), rc[r], rc[r + 1]));
+      }
     }
     return items;
   };
+  if (Hset > 0) return build(Hset);
   auto makespan = [&](const std::vector<int4>& items) {
     std::vector<long long> load(std::max(1, grid), 0);
     for (size_t i = 0; i < items.size(); ++i)
@@ -177,6 +183,11 @@ struct mose_gpu_ctx {
   DevBuf<double> rs1, rs2;
   DevBuf<int4> items_nb;      // 2-D items with no physical boundary face
   int nitems_nb = 0;
+  // 2-D work-list tiling (mose_gpu_set_tiling / mose_gpu_autotune): rows per
+  // item (0: the planner's model), largest strip width, item order, CTAs per
+  // SM (0: the occupancy limit); and the boundary words the planner reads
+  int tile_h = 0, tile_w = SB_W, tile_order = 0, tile_ctas = 0;
+  std::vector<int> hbcw;
   DevBuf<int4> items3[3];     // 3-D sweeps
   int nitems3[3] = {0, 0, 0};
   DevBuf<double> scal;        // [0] dtglobal, [1] time
@@ -479,6 +490,38 @@ int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, 
     if (e.type == 0 && e.f >= 5 && h.nk == 1) continue;
     ctx->bc.push_back(e);
   }
+  return MOSE_OK;
+}
+
+// Plans the 2-D work list with the context's tiling and uploads it: an item
+// runs the boundary-free kernel when every block-edge face its cells have
+// (column -1 / ni, row -1 / nj) is a connection.
+static int install_items(mose_gpu_ctx* ctx) {
+  std::vector<int4> all = plan_stage_items(ctx->hblk, 3 * ctx->nsm, ctx->tile_h, ctx->tile_w, ctx->tile_order);
+  std::vector<int4> items, items_nb;
+  for (const int4& it : all) {
+    const BlockDesc& d = ctx->desc[it.x];
+    const int c0 = it.y & 0xffff, c1 = it.y >> 16, j0 = it.z, j1 = it.w;
+    bool conn = true;
+    auto check = [&](int f, int lo, int hi) {
+      for (int q = lo; q < hi && conn; ++q) conn = bc_code(ctx->hbcw[d.bcoff[f] + q]) == BC_CONN;
+    };
+    if (c0 == 0) check(0, j0, j1);
+    if (c1 == d.ni) check(1, j0, j1);
+    if (j0 == 0) check(2, c0, c1);
+    if (j1 == d.nj) check(3, c0, c1);
+    (conn && ctx->nd == 2 ? items_nb : items).push_back(it);
+  }
+  ctx->nitems = (int)items.size();
+  ctx->nitems_nb = (int)items_nb.size();
+  CU(ctx->items.alloc(std::max<size_t>(items.size(), 1)));
+  CU(ctx->items_nb.alloc(std::max<size_t>(items_nb.size(), 1)));
+  if (!items.empty())
+    CU(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+  if (!items_nb.empty())
+    CU(cudaMemcpyAsync(ctx->items_nb.p, items_nb.data(), items_nb.size() * sizeof(int4), cudaMemcpyHostToDevice,
+                       ctx->stream));
+  CU(cudaStreamSynchronize(ctx->stream));
   return MOSE_OK;
 }
 
@@ -874,32 +917,11 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   }
 
   // ---- work items for the stage kernel -----------------------------------------
-  std::vector<int4> all = plan_stage_items(ctx->hblk, 3 * ctx->nsm);
-  // an item runs the boundary-free kernel when every block-edge face its
-  // cells have (column -1 / ni, row -1 / nj) is a connection
-  std::vector<int4> items, items_nb;
-  for (const int4& it : all) {
-    const BlockDesc& d = ctx->desc[it.x];
-    const int c0 = it.y & 0xffff, c1 = it.y >> 16, j0 = it.z, j1 = it.w;
-    bool conn = true;
-    auto check = [&](int f, int lo, int hi) {
-      for (int q = lo; q < hi && conn; ++q) conn = bc_code(bcwords[d.bcoff[f] + q]) == BC_CONN;
-    };
-    if (c0 == 0) check(0, j0, j1);
-    if (c1 == d.ni) check(1, j0, j1);
-    if (j0 == 0) check(2, c0, c1);
-    if (j1 == d.nj) check(3, c0, c1);
-    (conn && ctx->nd == 2 ? items_nb : items).push_back(it);
+  ctx->hbcw = bcwords;
+  {
+    int rc = install_items(ctx);
+    if (rc) return rc;
   }
-  ctx->nitems = (int)items.size();
-  ctx->nitems_nb = (int)items_nb.size();
-  CU(ctx->items.alloc(std::max<size_t>(items.size(), 1)));
-  CU(ctx->items_nb.alloc(std::max<size_t>(items_nb.size(), 1)));
-  if (!items.empty())
-    CU(cudaMemcpyAsync(ctx->items.p, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
-  if (!items_nb.empty())
-    CU(cudaMemcpyAsync(ctx->items_nb.p, items_nb.data(), items_nb.size() * sizeof(int4), cudaMemcpyHostToDevice,
-                       ctx->stream));
   if (ctx->nd == 3) {
     std::vector<int4> it3[3];
     plan_3d_items(ctx->hblk, it3);
@@ -1073,6 +1095,7 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
     a.items3[q] = ctx->items3[q].p;
     a.nitems3[q] = ctx->nitems3[q];
   }
+  a.grid_cap = ctx->tile_ctas;
   return a;
 }
 
@@ -1814,5 +1837,128 @@ int mose_gpu_upload_adjoint(mose_gpu_ctx* ctx, int32_t b, const double* lam) {
   return prim_io(ctx, b, const_cast<double*>(lam), -2, true);
 }
 int mose_gpu_download_adjoint(mose_gpu_ctx* ctx, int32_t b, double* lam) { return prim_io(ctx, b, lam, -2, false); }
+
+// ---- 2-D work-list tiling and its autotuner ------------------------------------
+int mose_gpu_get_tiling(const mose_gpu_ctx* ctx, int32_t* tiling) {
+  if (!ctx || !tiling) return MOSE_ERR_INVALID;
+  tiling[0] = ctx->tile_h; tiling[1] = ctx->tile_w; tiling[2] = ctx->tile_order; tiling[3] = ctx->tile_ctas;
+  return MOSE_OK;
+}
+
+static int apply_tiling(mose_gpu_ctx* ctx, int h, int w, int order, int ctas) {
+  CU(cudaStreamSynchronize(ctx->stream));
+  destroy_graphs(ctx);   // the captured steps hold the old work lists
+  ctx->tile_h = h; ctx->tile_w = w; ctx->tile_order = order; ctx->tile_ctas = ctas;
+  return install_items(ctx);
+}
+
+int mose_gpu_set_tiling(mose_gpu_ctx* ctx, const int32_t* tiling) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (!tiling) return MOSE_ERR_INVALID;
+  if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "the tiling applies to the 2-D work list");
+  if (tiling[0] < 0 || tiling[0] > (1 << 20) || tiling[1] < 8 || tiling[1] > SB_W || tiling[2] < 0 || tiling[2] > 1 ||
+      tiling[3] < 0 || tiling[3] > 32)
+    return fail(ctx, MOSE_ERR_INVALID, "tiling out of range (rows >= 0, 8 <= width <= %d, order 0/1, ctas 0..32)",
+                SB_W);
+  return apply_tiling(ctx, tiling[0], tiling[1], tiling[2], tiling[3]);
+}
+
+// Times candidate tilings of the 2-D work list on the context's own domain
+// and keeps the fastest: each trial restores the state, runs one untimed
+// step, then `steps` timed steps (CUDA events on the context's stream), and
+// the state is restored at the end.  Coordinate search: rows per item, then
+// strip width, item order and CTAs per SM, then rows per item again; a
+// candidate replaces the best one only when more than 1 % faster.
+int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, double* best_ms, double* default_ms) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "the autotuner tunes the 2-D work list");
+  if (steps < 1) steps = 3;
+  CU(cudaStreamSynchronize(ctx->stream));
+  const size_t n = (size_t)ctx->nv * ctx->marena;
+  DevBuf<double> snap;
+  if (snap.alloc(n) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (autotune snapshot)");
+  const int cur0 = ctx->cur, po0 = ctx->po;
+  const bool valid0 = ctx->dt_valid;
+  CU(cudaMemcpyAsync(snap.p, ctx->state[cur0].p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+  const long long launches0 = ctx->launches;
+  cudaEvent_t e0, e1;
+  CU(cudaEventCreate(&e0));
+  CU(cudaEventCreate(&e1));
+  auto restore = [&]() -> int {
+    CU(cudaMemcpyAsync(ctx->state[cur0].p, snap.p, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->cur = cur0;
+    ctx->po = po0;
+    ctx->dt_valid = false;
+    return MOSE_OK;
+  };
+  auto one_step = [&]() {
+    const int s0 = ctx->cur;
+    if (fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, s0);
+    ctx->launches += enqueue_step(ctx, s0);
+    ctx->dt_valid = fused_dt(ctx);
+    ctx->po = s0;
+    ctx->cur = step_final_index(ctx, s0);
+  };
+  auto trial = [&](int h, int w, int order, int ctas, double& ms) -> int {
+    int r = apply_tiling(ctx, h, w, order, ctas);
+    if (r) return r;
+    if ((r = restore())) return r;
+    one_step();
+    CU(cudaEventRecord(e0, ctx->stream));
+    for (int q = 0; q < steps; ++q) one_step();
+    CU(cudaEventRecord(e1, ctx->stream));
+    CU(cudaEventSynchronize(e1));
+    float t = 0.0f;
+    CU(cudaEventElapsedTime(&t, e0, e1));
+    ms = (double)t / steps;
+    return poll_device_error(ctx);
+  };
+  int best[4] = {0, SB_W, 0, 0};
+  double tbest = 0.0;
+  rc = trial(best[0], best[1], best[2], best[3], tbest);
+  const double t0 = tbest;
+  static const int Hs[] = {16, 32, 64, 128, 256, 512, 0};
+  static const int Ws[] = {SB_W, 46, 30};
+  static const int Os[] = {0, 1};
+  static const int Cs[] = {0, 2, 1};
+  auto sweep = [&](int knob, const int* vals, int nv) -> int {
+    for (int q = 0; q < nv && !rc; ++q) {
+      int c[4] = {best[0], best[1], best[2], best[3]};
+      c[knob] = vals[q];
+      if (c[knob] == best[knob]) continue;
+      double t = 0.0;
+      int r = trial(c[0], c[1], c[2], c[3], t);
+      if (r) return r;
+      if (t < 0.99 * tbest) {
+        tbest = t;
+        for (int z = 0; z < 4; ++z) best[z] = c[z];
+      }
+    }
+    return MOSE_OK;
+  };
+  if (!rc) rc = sweep(0, Hs, 7);
+  if (!rc) rc = sweep(1, Ws, 3);
+  if (!rc) rc = sweep(2, Os, 2);
+  if (!rc) rc = sweep(3, Cs, 3);
+  if (!rc) rc = sweep(0, Hs, 7);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  rc = apply_tiling(ctx, best[0], best[1], best[2], best[3]);
+  if (rc) return rc;
+  if ((rc = restore())) return rc;
+  ctx->dt_valid = false;
+  (void)valid0;
+  CU(cudaStreamSynchronize(ctx->stream));
+  ctx->launches = launches0;   // the trials are not the caller's steps
+  if (tiling_out) for (int z = 0; z < 4; ++z) tiling_out[z] = best[z];
+  if (best_ms) *best_ms = tbest;
+  if (default_ms) *default_ms = t0;
+  return MOSE_OK;
+}
 
 }  // extern "C"

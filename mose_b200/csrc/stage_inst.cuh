@@ -32,7 +32,8 @@ static void launch_persistent_list(const StageArgs& a, int nitems, int nsm, cuda
         occ < 1)
       occ = 1;
   }
-  const int grid = nitems < occ * nsm ? nitems : occ * nsm;
+  const int per_sm = (a.grid_cap > 0 && a.grid_cap < occ) ? a.grid_cap : occ;
+  const int grid = nitems < per_sm * nsm ? nitems : per_sm * nsm;
   k_stage2d<PH, RIE, LIM, UNI, MODE, BC><<<grid, SB_T, smem, s>>>(a);
 }
 

@@ -232,6 +232,29 @@ class Solver:
         self._check(self.lib.mose_gpu_residual_norms(self.h, _dp(out)))
         return out
 
+    # ---- 2-D work-list tiling -----------------------------------------------
+    TILING_KEYS = ("rows_per_item", "strip_width", "order", "ctas_per_sm")
+
+    def tiling(self) -> dict:
+        t = (C.c_int32 * 4)()
+        self._check(self.lib.mose_gpu_get_tiling(self.h, t))
+        return dict(zip(self.TILING_KEYS, list(t)))
+
+    def set_tiling(self, rows_per_item=0, strip_width=62, order=0, ctas_per_sm=0):
+        t = (C.c_int32 * 4)(rows_per_item, strip_width, order, ctas_per_sm)
+        self._check(self.lib.mose_gpu_set_tiling(self.h, t))
+
+    def autotune(self, steps: int = 3) -> dict:
+        """Times candidate tilings of the 2-D work list on this domain and
+        keeps the fastest; the state is unchanged.  Returns the tiling and
+        the measured ms per step of it and of the default."""
+        t = (C.c_int32 * 4)()
+        best, default = C.c_double(), C.c_double()
+        self._check(self.lib.mose_gpu_autotune(self.h, steps, t, C.byref(best), C.byref(default)))
+        out = dict(zip(self.TILING_KEYS, list(t)))
+        out.update(ms_per_step=best.value, default_ms_per_step=default.value)
+        return out
+
     def set_time(self, time: float, it: int = 0):
         self._check(self.lib.mose_gpu_set_time(self.h, time, it))
 
