@@ -252,6 +252,30 @@ def mixed_error(local, steps=100):
             "against": "reference-exact GPU path (bit-identical to the FP64 oracle)"}
 
 
+def warm_up(s, stream, seconds=0.5):
+    """Steps until about `seconds` of GPU time have passed: a new context
+    runs slower for its first few hundred steps."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    done = 0.0
+    n = 4
+    while done < seconds * 1e3:
+        e0.record(stream)
+        s.advance(n)
+        e1.record(stream)
+        e1.synchronize()
+        done += e0.elapsed_time(e1)
+        n = min(2 * n, 256)
+
+
+def autotune(s, case):
+    """The project's autotuner on a 2-D solver (work-list tiling, measured on
+    this domain before any timing); None for 3-D, whose sweeps are not tuned."""
+    if any(nd.shape[0] > 2 for nd in case.nodes):
+        return None
+    return s.autotune(steps=3)
+
+
 def config_report(name, make_case, local, steps, precisions=PRECISIONS):
     """Throughput of each precision (graph-replayed steps, CUDA events) on one
     configuration, and the mixed precision's density error against the
@@ -266,9 +290,12 @@ def config_report(name, make_case, local, steps, precisions=PRECISIONS):
     for prec in precisions:
         s = Solver(case, precision=precision_code(prec), device=local)
         stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
-        s.advance(2)
+        tuned = autotune(s, case)
+        warm_up(s, stream)
         ms = time_advance(s, stream, steps, 1)
         out[prec] = {"value": case.ncells * steps / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / steps}
+        if tuned is not None:
+            out[prec]["autotune"] = tuned
         s.close()
         # error run from the initial state
         s = Solver(case, precision=precision_code(prec), device=local)
@@ -418,7 +445,10 @@ def run_gpu(args):
     peak, peak_kind = peaks()
     s = Solver(case, precision=precision_code(args.precision), device=local)
     stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
+    tuned = autotune(s, case) if not args.profile else None
     s.advance(max(args.warmup, 3))
+    if not args.profile:
+        warm_up(s, stream)
     torch.cuda.synchronize()
     if args.profile:
         # the launches a profiler captures: warm-up above, then K plain steps
@@ -457,11 +487,14 @@ def run_gpu(args):
             continue
         v = Solver(case, precision=precision_code(name), device=local)
         vstream = torch.cuda.ExternalStream(v.stream_handle, device=torch.device("cuda", local))
+        vtuned = autotune(v, case)
         v.advance(3)
+        warm_up(v, vstream)
         vms = time_advance(v, vstream, args.steps, world)
         v_stage_ms, v_ach, v_step = stage_roofline(v, args.steps, cells)
         variants[name] = {"value": aggregate(world, cells, args.steps, vms), "ms_per_step": vms / args.steps,
-                          "stage_ms": v_stage_ms, "roofline_frac": v_ach / peak, "step_kernel_ms": v_step}
+                          "stage_ms": v_stage_ms, "roofline_frac": v_ach / peak, "step_kernel_ms": v_step,
+                          "autotune": vtuned}
         v.close()
     # the reports beside the headline run once, on rank 0 of a one-GPU run
     err = mixed_error(local) if rank == 0 else None
@@ -471,7 +504,8 @@ def run_gpu(args):
         line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f64", "data": "synthetic", "config": workload_config(case, args.precision),
+                "dtype": "f64", "data": "synthetic",
+                "config": dict(workload_config(case, args.precision), autotune=tuned),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak,
                              "traffic": (TRAFFIC_BYTES_PER_CELL[args.precision] * cells

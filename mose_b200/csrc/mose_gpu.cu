@@ -1290,12 +1290,9 @@ int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
   return rc;
 }
 
-int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double* time) {
-  int rc = require_ready(ctx);
-  if (rc) return rc;
-  if (nsteps < 0) return MOSE_ERR_INVALID;
-  CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+// Enqueues nsteps graph-replayed steps (one graph per starting arena,
+// captured on first use); the device time and iteration are already set.
+static int enqueue_graph_steps(mose_gpu_ctx* ctx, int nsteps) {
   if (nsteps > 0 && fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, ctx->cur);
   for (int n = 0; n < nsteps; ++n) {
     int s0 = ctx->cur;
@@ -1314,6 +1311,17 @@ int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double
     ctx->po = s0;
     ctx->cur = step_final_index(ctx, s0);
   }
+  return MOSE_OK;
+}
+
+int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double* time) {
+  int rc = require_ready(ctx);
+  if (rc) return rc;
+  if (nsteps < 0) return MOSE_ERR_INVALID;
+  CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+  CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  rc = enqueue_graph_steps(ctx, nsteps);
+  if (rc) return rc;
   double h[2];
   CU(cudaMemcpyAsync(h, ctx->scal.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   rc = poll_device_error(ctx);
@@ -1865,11 +1873,15 @@ int mose_gpu_set_tiling(mose_gpu_ctx* ctx, const int32_t* tiling) {
 }
 
 // Times candidate tilings of the 2-D work list on the context's own domain
-// and keeps the fastest: each trial restores the state, runs one untimed
-// step, then `steps` timed steps (CUDA events on the context's stream), and
-// the state is restored at the end.  Coordinate search: rows per item, then
-// strip width, item order and CTAs per SM, then rows per item again; a
-// candidate replaces the best one only when more than 1 % faster.
+// and keeps the fastest.  Every trial runs the path mose_gpu_advance runs
+// (graph-replayed steps): it restores the state, runs one untimed step, then
+// twice `steps` timed steps (CUDA events on the context's stream), keeping
+// the faster.  Default-tiling steps come first until the timing has settled
+// (a new context runs slower for its first few hundred steps); coordinate search over rows per item, then strip width, item
+// order and CTAs per SM, then rows per item again, a candidate replacing
+// the best one only when more than 1 % faster; finally the default and the
+// best are timed again, alternately, three times, and the best is kept only
+// if still more than 1 % faster.  The state is restored at the end.
 int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, double* best_ms, double* default_ms) {
   int rc = require_ready(ctx);
   if (rc) return rc;
@@ -1895,32 +1907,35 @@ int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, dou
     ctx->dt_valid = false;
     return MOSE_OK;
   };
-  auto one_step = [&]() {
-    const int s0 = ctx->cur;
-    if (fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, s0);
-    ctx->launches += enqueue_step(ctx, s0);
-    ctx->dt_valid = fused_dt(ctx);
-    ctx->po = s0;
-    ctx->cur = step_final_index(ctx, s0);
-  };
   auto trial = [&](int h, int w, int order, int ctas, double& ms) -> int {
     int r = apply_tiling(ctx, h, w, order, ctas);
     if (r) return r;
     if ((r = restore())) return r;
-    one_step();
-    CU(cudaEventRecord(e0, ctx->stream));
-    for (int q = 0; q < steps; ++q) one_step();
-    CU(cudaEventRecord(e1, ctx->stream));
-    CU(cudaEventSynchronize(e1));
-    float t = 0.0f;
-    CU(cudaEventElapsedTime(&t, e0, e1));
-    ms = (double)t / steps;
+    if ((r = enqueue_graph_steps(ctx, 1))) return r;
+    ms = 0.0;
+    for (int rep = 0; rep < 2; ++rep) {
+      CU(cudaEventRecord(e0, ctx->stream));
+      if ((r = enqueue_graph_steps(ctx, steps))) return r;
+      CU(cudaEventRecord(e1, ctx->stream));
+      CU(cudaEventSynchronize(e1));
+      float t = 0.0f;
+      CU(cudaEventElapsedTime(&t, e0, e1));
+      if (rep == 0 || (double)t / steps < ms) ms = (double)t / steps;
+    }
     return poll_device_error(ctx);
   };
   int best[4] = {0, SB_W, 0, 0};
   double tbest = 0.0;
-  rc = trial(best[0], best[1], best[2], best[3], tbest);
-  const double t0 = tbest;
+  // warm-up with the default tiling until two successive trials agree within
+  // 1 % after at least 0.5 s of steps (at most about 4 s): a new context runs
+  // slower for its first few hundred steps
+  double warm = 0.0, prev = -1.0;
+  for (int q = 0; q < 400 && !rc && warm < 4000.0; ++q) {
+    rc = trial(best[0], best[1], best[2], best[3], tbest);
+    warm += tbest * (2 * steps + 1);
+    if (warm >= 500.0 && prev > 0.0 && std::fabs(tbest - prev) <= 0.01 * prev) break;
+    prev = tbest;
+  }
   static const int Hs[] = {16, 32, 64, 128, 256, 512, 0};
   static const int Ws[] = {SB_W, 46, 30};
   static const int Os[] = {0, 1};
@@ -1945,6 +1960,24 @@ int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, dou
   if (!rc) rc = sweep(2, Os, 2);
   if (!rc) rc = sweep(3, Cs, 3);
   if (!rc) rc = sweep(0, Hs, 7);
+  // the decision: default and best measured again, alternately, three times
+  double tdef = 0.0, tb = 0.0;
+  const bool moved = best[0] != 0 || best[1] != SB_W || best[2] != 0 || best[3] != 0;
+  for (int q = 0; q < 3 && !rc; ++q) {
+    double t = 0.0;
+    rc = trial(0, SB_W, 0, 0, t);
+    if (!rc) tdef = (q == 0 || t < tdef) ? t : tdef;
+    if (!rc && moved) {
+      rc = trial(best[0], best[1], best[2], best[3], t);
+      if (!rc) tb = (q == 0 || t < tb) ? t : tb;
+    }
+  }
+  if (!moved || !(tb < 0.99 * tdef)) {
+    best[0] = 0; best[1] = SB_W; best[2] = 0; best[3] = 0;
+    tb = tdef;
+  }
+  tbest = tb;
+  const double t0 = tdef;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
