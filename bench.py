@@ -253,8 +253,10 @@ def mixed_error(local, steps=100):
 
 
 def warm_up(s, stream, seconds=0.5):
-    """Steps until about `seconds` of GPU time have passed: a new context
-    runs slower for its first few hundred steps."""
+    """Steps until about `seconds` of GPU time have passed: the first few
+    hundred steps from the initial state run slower than the later ones, so
+    the autotuner (which measures on the state it is given and restores it)
+    and the timed region both start from the warmed flow."""
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     done = 0.0
@@ -270,7 +272,8 @@ def warm_up(s, stream, seconds=0.5):
 
 def autotune(s, case):
     """The project's autotuner on a 2-D solver (work-list tiling, measured on
-    this domain before any timing); None for 3-D, whose sweeps are not tuned."""
+    this domain's warmed flow before any timing); None for 3-D, whose sweeps
+    are not tuned."""
     if any(nd.shape[0] > 2 for nd in case.nodes):
         return None
     return s.autotune(steps=3)
@@ -290,8 +293,8 @@ def config_report(name, make_case, local, steps, precisions=PRECISIONS):
     for prec in precisions:
         s = Solver(case, precision=precision_code(prec), device=local)
         stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
-        tuned = autotune(s, case)
         warm_up(s, stream)
+        tuned = autotune(s, case)
         ms = time_advance(s, stream, steps, 1)
         out[prec] = {"value": case.ncells * steps / (ms / 1e3), "unit": "cell-updates/s", "ms_per_step": ms / steps}
         if tuned is not None:
@@ -383,7 +386,7 @@ def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0):
     fdm = (J(P0, mach + h) - J(P0, mach - h)) / (2 * h)
     s.close()
     return {"adjoint_curvilinear_512^2_200_steps": {
-        "cells": case.ncells, "steps": nsteps, "checkpoint_interval": K, "J": float(Jt), "J_direct": J0,
+        "cells": case.ncells, "steps": nsteps, "checkpoint_interval": K, "J": float(Jt.detach()), "J_direct": J0,
         "forward_ms": fwd_ms, "plain_forward_ms": plain_ms, "backward_ms": bwd_ms,
         "adjoint_over_forward": bwd_ms / plain_ms,
         "gradient_vs_fd": {"directions": ndir, "kind": "seeded cell-wise N(0,1) on rho, u, v, p", "step": h,
@@ -445,10 +448,11 @@ def run_gpu(args):
     peak, peak_kind = peaks()
     s = Solver(case, precision=precision_code(args.precision), device=local)
     stream = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
-    tuned = autotune(s, case) if not args.profile else None
     s.advance(max(args.warmup, 3))
+    tuned = None
     if not args.profile:
         warm_up(s, stream)
+        tuned = autotune(s, case)
     torch.cuda.synchronize()
     if args.profile:
         # the launches a profiler captures: warm-up above, then K plain steps
@@ -487,9 +491,9 @@ def run_gpu(args):
             continue
         v = Solver(case, precision=precision_code(name), device=local)
         vstream = torch.cuda.ExternalStream(v.stream_handle, device=torch.device("cuda", local))
-        vtuned = autotune(v, case)
         v.advance(3)
         warm_up(v, vstream)
+        vtuned = autotune(v, case)
         vms = time_advance(v, vstream, args.steps, world)
         v_stage_ms, v_ach, v_step = stage_roofline(v, args.steps, cells)
         variants[name] = {"value": aggregate(world, cells, args.steps, vms), "ms_per_step": vms / args.steps,

@@ -15,7 +15,7 @@ void launch_face_metrics(const BlockDesc* dblk, int b, long long nface, NodeView
 void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, const NodeView* nodes, MetricArgs m,
                           int nd, int ndir, DevError* err, cudaStream_t s);
 void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir, int* flags,
-                          double* firsts, cudaStream_t s);
+                          double* firsts, double tol, cudaStream_t s);
 void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, double* P, MetricArgs m, int nd,
                         DevError* err, cudaStream_t s);
 void launch_compute_dt(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, MetricArgs m,

@@ -266,10 +266,15 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
 }
 
 // Uniformity check: flags[b] bit p set when plane p differs from its first
-// valid value somewhere in its valid region.
+// valid value somewhere in its valid region.  tol = 0 asks for bitwise
+// equality; tol > 0 accepts values within tol relative to the first one
+// (last-bit differences of nodes placed by floating-point arithmetic).
 __global__ void k_uniform_check(const BlockDesc* blk, int b, MetricArgs m, int nd, int ndir, int* flags,
-                                double* firsts) {
+                                double* firsts, double tol) {
   const BlockDesc& d = blk[b];
+  auto ne = [tol](double a, double a0) -> bool {
+    return tol == 0.0 ? (a != a0) : !(fabs(a - a0) <= tol * fabs(a0));
+  };
   const long long vs = d.vstride, mb = d.mbase;
   // reference values: cell (0,0,0) metrics; faces of cell (0,0,0)
   long long o0 = (nd == 3) ? cell_off3(d, 0, 0, 0) : cell_off2(d, 0, 0);
@@ -281,20 +286,20 @@ __global__ void k_uniform_check(const BlockDesc* blk, int b, MetricArgs m, int n
     long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
     int f = 0;
     // dl along each active direction on that direction's ghosted line
-    if (in_j && in_k && m.dl[3 * mb + 0 * vs + o] != m.dl[3 * mb + 0 * vs + o0]) f |= 1;
-    if (in_i && in_k && m.dl[3 * mb + 1 * vs + o] != m.dl[3 * mb + 1 * vs + o0]) f |= 2;
-    if (nd == 3 && in_i && in_j && m.dl[3 * mb + 2 * vs + o] != m.dl[3 * mb + 2 * vs + o0]) f |= 4;
+    if (in_j && in_k && ne(m.dl[3 * mb + 0 * vs + o], m.dl[3 * mb + 0 * vs + o0])) f |= 1;
+    if (in_i && in_k && ne(m.dl[3 * mb + 1 * vs + o], m.dl[3 * mb + 1 * vs + o0])) f |= 2;
+    if (nd == 3 && in_i && in_j && ne(m.dl[3 * mb + 2 * vs + o], m.dl[3 * mb + 2 * vs + o0])) f |= 4;
     if (in_i && in_j && in_k) {
-      if (m.vol[mb + o] != m.vol[mb + o0]) f |= 8;
+      if (ne(m.vol[mb + o], m.vol[mb + o0])) f |= 8;
       for (int p = 0; p < 3 * ndir; ++p)
-        if (m.vers[9 * mb + p * vs + o] != m.vers[9 * mb + p * vs + o0]) f |= 16;
+        if (ne(m.vers[9 * mb + p * vs + o], m.vers[9 * mb + p * vs + o0])) f |= 16;
     }
     for (int dir = 0; dir < nd; ++dir) {
       bool in = (dir == 0 ? (i >= 0 && i <= d.ni) : in_i) && (dir == 1 ? (j >= 0 && j <= d.nj) : in_j) &&
                 (nd == 2 || (dir == 2 ? (k >= 0 && k <= d.nk) : in_k));
       if (!in) continue;
       for (int p = 0; p < 4; ++p)
-        if (m.face[12 * mb + (4 * dir + p) * vs + o] != m.face[12 * mb + (4 * dir + p) * vs + o0]) f |= 32 << dir;
+        if (ne(m.face[12 * mb + (4 * dir + p) * vs + o], m.face[12 * mb + (4 * dir + p) * vs + o0])) f |= 32 << dir;
     }
     if (f) atomicOr(&flags[b], f);
   }
@@ -760,8 +765,8 @@ void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, con
                                                      const_cast<double*>(m.dl), nd, ndir, err);
 }
 void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir,
-                          int* flags, double* firsts, cudaStream_t s) {
-  k_uniform_check<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, m, nd, ndir, flags, firsts);
+                          int* flags, double* firsts, double tol, cudaStream_t s) {
+  k_uniform_check<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, m, nd, ndir, flags, firsts, tol);
 }
 void launch_fill_ghosts(const BlockDesc* dblk, const GhostRec* recs, int nrec, double* P, MetricArgs m, int nd,
                         DevError* err, cudaStream_t s) {
