@@ -443,7 +443,11 @@ def run_gpu(args):
     from mose_b200 import Solver
     if args.profile_adjoint:
         return profile_adjoint(local)
-    case = workload_case(N_CELLS_SIDE, steps=args.steps)
+    if args.profile and args.profile_case == "quadrant":
+        from mose_b200 import cases
+        case = cases.four_quadrant(seed=0, steps=args.steps)
+    else:
+        case = workload_case(N_CELLS_SIDE, steps=args.steps)
     cells = case.ncells
     peak, peak_kind = peaks()
     s = Solver(case, precision=precision_code(args.precision), device=local)
@@ -548,6 +552,8 @@ def main():
                     help="skip the four-quadrant and 3-D configuration reports")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + K fused steps (the command profiled by ncu); prints nothing")
+    ap.add_argument("--profile-case", default="vortex", choices=["vortex", "quadrant"],
+                    help="with --profile: the 2048^2 vortex or the 64-block four-quadrant domain (seed 0)")
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="only the adjoint's forward + backward on a 16-step channel (profiled by ncu)")
     args = ap.parse_args()
