@@ -226,6 +226,10 @@ struct mose_gpu_ctx {
   int adj_graph_K = 0, adj_rec_kernels = 0, adj_rev_kernels = 0;
   cudaStream_t adj_aux = nullptr;
   cudaEvent_t adj_fork = nullptr, adj_join = nullptr;
+  // 2-D stages with both item lists: the boundary items' launch runs on
+  // stage_aux beside the boundary-free items' launch
+  cudaStream_t stage_aux = nullptr;
+  cudaEvent_t stage_fork = nullptr, stage_join = nullptr;
   DevBuf<double> lam, lam_loc, lam_n, lamR, wdt, lamG, Cx, Cy, Fx, Fy, dtpart, adj_scal, Cb, Fbc, dmach, objt;
   DevBuf<unsigned long long> adj_arg;
   DevBuf<double> adj_sumscr;             // partial sums of the deterministic reductions
@@ -378,8 +382,11 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
     return MOSE_ERR_CUDA;   // built for sm_100a only
   }
   ctx->nsm = prop.multiProcessorCount;
-  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-    delete ctx;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->stage_aux, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->stage_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->stage_join, cudaEventDisableTiming) != cudaSuccess) {
+    mose_gpu_destroy(ctx);
     return MOSE_ERR_CUDA;
   }
   // thermodynamic constants of the restated FLINT closure
@@ -404,10 +411,14 @@ void mose_gpu_destroy(mose_gpu_ctx* ctx) {
   cudaSetDevice(ctx->cfg.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->adj_aux) cudaStreamSynchronize(ctx->adj_aux);
+  if (ctx->stage_aux) cudaStreamSynchronize(ctx->stage_aux);
   destroy_graphs(ctx);
   if (ctx->adj_fork) cudaEventDestroy(ctx->adj_fork);
   if (ctx->adj_join) cudaEventDestroy(ctx->adj_join);
   if (ctx->adj_aux) cudaStreamDestroy(ctx->adj_aux);
+  if (ctx->stage_fork) cudaEventDestroy(ctx->stage_fork);
+  if (ctx->stage_join) cudaEventDestroy(ctx->stage_join);
+  if (ctx->stage_aux) cudaStreamDestroy(ctx->stage_aux);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -1112,6 +1123,27 @@ static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int pre
     return launch_stage3d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
                ? (ctx->nitems3[0] > 0 ? 3 : 2)
                : 0;
+  if (a.nitems > 0 && a.nitems_nb > 0) {
+    // The boundary-free items and the boundary items write disjoint cells
+    // and meet only in atomics (the fused dt minimum, the error word), so the
+    // two persistent launches run side by side: the boundary items on
+    // stage_aux, forked from and joined back into the context's stream (also
+    // inside graph capture).  Serialised, a small domain paid one item's
+    // march twice per stage.
+    StageArgs anb = a, abc = a;
+    anb.nitems = 0;
+    abc.nitems_nb = 0;
+    if (cudaEventRecord(ctx->stage_fork, ctx->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(ctx->stage_aux, ctx->stage_fork, 0) != cudaSuccess)
+      return 0;
+    const bool ok = launch_stage2d(abc, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stage_aux) &&
+                    launch_stage2d(anb, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream);
+    // the join is recorded whatever happened, so a capture never ends forked
+    if (cudaEventRecord(ctx->stage_join, ctx->stage_aux) != cudaSuccess ||
+        cudaStreamWaitEvent(ctx->stream, ctx->stage_join, 0) != cudaSuccess)
+      return 0;
+    return ok ? 2 : 0;
+  }
   return launch_stage2d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
              ? (a.nitems > 0) + (a.nitems_nb > 0)
              : 0;

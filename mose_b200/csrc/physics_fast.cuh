@@ -425,6 +425,100 @@ __device__ __forceinline__ void ausmp32(const GasF32& g, float4 L, float4 R, flo
   F[3] = fmaf(mp, HL, mm * HR);
 }
 
+// ---- FP32 solvers over NV-variable arrays -----------------------------------
+// hllc32 / ausmp32 above for (rho, u, ..., p) arrays of NV values and a
+// three-component normal (the 3-D sweeps of the mixed precision).  The upwind
+// side is chosen per value with selects, so the arrays stay in registers.
+template <int NV>
+__device__ __forceinline__ float un32(const float* q, const float* n) {
+  if constexpr (NV == 5) return fmaf(q[1], n[0], fmaf(q[2], n[1], q[3] * n[2]));
+  else return fmaf(q[1], n[0], q[2] * n[1]);
+}
+template <int NV>
+__device__ __forceinline__ float v2_32(const float* q) {
+  if constexpr (NV == 5) return fmaf(q[1], q[1], fmaf(q[2], q[2], q[3] * q[3]));
+  else return fmaf(q[1], q[1], q[2] * q[2]);
+}
+
+template <int NV>
+__device__ __forceinline__ void hllc32n(const GasF32& g, const float* L, const float* R, const float* n, float* F) {
+  constexpr int P = NV - 1, D = NV - 2;
+  const float rsl = frsq(L[0]), rsr = frsq(R[0]);
+  const float srL = L[0] * rsl, srR = R[0] * rsr;          // sqrt(rho)
+  const float irl = rsl * rsl, irr = rsr * rsr;            // 1 / rho
+  const float unl = un32<NV>(L, n), unr = un32<NV>(R, n);
+  const float pol = L[P] * irl, por = R[P] * irr;          // p / rho
+  const float aL = fsqrtp(g.gamma * pol), aR = fsqrtp(g.gamma * por);
+  const float h0l = fmaf(g.gcp, pol, 0.5f * v2_32<NV>(L));
+  const float h0r = fmaf(g.gcp, por, 0.5f * v2_32<NV>(R));
+  const float isr = frcp(srL + srR);
+  const float wl = srL * isr, wr = srR * isr;
+  float vel2 = 0.0f, un_roe = 0.0f;
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float ur = fmaf(wr, R[1 + d], wl * L[1 + d]);
+    vel2 = fmaf(ur, ur, vel2);
+    un_roe = fmaf(ur, n[d], un_roe);
+  }
+  const float h0_roe = fmaf(wr, h0r, wl * h0l);
+  const float a2 = g.gm1 * fmaf(-0.5f, vel2, h0_roe);
+  const float a_roe = fsqrtp(fmaxf(a2, 1.17549435e-38f));
+  const float S1 = fminf(fminf(0.0f, unl - aL), un_roe - a_roe);
+  const float S4 = fmaxf(fmaxf(0.0f, unr + aR), un_roe + a_roe);
+  const float ml = L[0] * (S1 - unl), mr = R[0] * (S4 - unr);
+  const float Sstar = (R[P] - L[P] + ml * unl - mr * unr) * frcp(ml - mr);
+  const bool left = (S1 >= 0.0f) || (Sstar >= 0.0f);
+  const float rk = left ? L[0] : R[0], pk = left ? L[P] : R[P];
+  const float unk = left ? unl : unr, h0k = left ? h0l : h0r, irk = left ? irl : irr;
+  const float SK = left ? S1 : S4, mk = left ? ml : mr;
+  const float m = rk * unk;
+  // star correction, applied when K's outer wave is subsonic in the face frame
+  const bool corr = left ? (S1 < 0.0f) : (S4 > 0.0f);
+  const float sc = corr ? SK : 0.0f;
+  const float pstar = fmaf(L[0] * (unl - S1), unl - Sstar, L[P]);
+  const float inv = frcp(SK - Sstar);
+  const float dp = pstar - pk;
+  const float e0k = h0k - pk * irk;
+  F[0] = fmaf(sc, fmaf(mk, inv, -rk), m);
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float uk = left ? L[1 + d] : R[1 + d];
+    F[1 + d] = fmaf(sc, fmaf(fmaf(mk, uk, dp * n[d]), inv, -rk * uk), fmaf(m, uk, pk * n[d]));
+  }
+  F[P] = fmaf(sc, fmaf(fmaf(mk, e0k, fmaf(-pk, unk, pstar * Sstar)), inv, -rk * e0k), m * h0k);
+}
+
+template <int NV>
+__device__ __forceinline__ void ausmp32n(const GasF32& g, const float* L, const float* R, const float* n, float* F) {
+  constexpr int P = NV - 1, D = NV - 2;
+  const float beta = 0.125f, alpha = 0.1875f;
+  const float irl = frcp(L[0]), irr = frcp(R[0]);
+  const float unl = un32<NV>(L, n), unr = un32<NV>(R, n);
+  const float pol = L[P] * irl, por = R[P] * irr;
+  const float a_half = fsqrtp(g.gamma * fsqrtp(pol * por));   // sqrt(aL aR)
+  const float ia = frcp(a_half);
+  const float ML = unl * ia, MR = unr * ia;
+  const float mL2 = fmaf(ML, ML, -1.0f), mR2 = fmaf(MR, MR, -1.0f);
+  const bool sl = fabsf(ML) < 1.0f, sr = fabsf(MR) < 1.0f;
+  const float lp1 = ML + 1.0f, rm1 = MR - 1.0f;
+  const float MplusL = sl ? fmaf(0.25f * lp1, lp1, beta * mL2 * mL2) : 0.5f * (ML + fabsf(ML));
+  const float pplusL = sl ? fmaf(0.25f * lp1 * lp1, 2.0f - ML, alpha * ML * mL2 * mL2)
+                          : 0.5f * (1.0f + copysignf(1.0f, ML));
+  const float MminusR = sr ? -fmaf(0.25f * rm1, rm1, beta * mR2 * mR2) : 0.5f * (MR - fabsf(MR));
+  const float pminusR = sr ? fmaf(0.25f * rm1 * rm1, 2.0f + MR, -alpha * MR * mR2 * mR2)
+                           : 0.5f * (1.0f - copysignf(1.0f, MR));
+  const float Mhalf = MplusL + MminusR;
+  const float phalf = fmaf(pplusL, L[P], pminusR * R[P]);
+  const float mp = L[0] * a_half * 0.5f * (Mhalf + fabsf(Mhalf));
+  const float mm = R[0] * a_half * 0.5f * (Mhalf - fabsf(Mhalf));
+  const float HL = fmaf(g.gcp, pol, 0.5f * v2_32<NV>(L));
+  const float HR = fmaf(g.gcp, por, 0.5f * v2_32<NV>(R));
+  F[0] = mp + mm;
+#pragma unroll
+  for (int d = 0; d < D; ++d) F[1 + d] = fmaf(mp, L[1 + d], fmaf(mm, R[1 + d], n[d] * phalf));
+  F[P] = fmaf(mp, HL, mm * HR);
+}
+
 // ---- state update (Newstate_Conservative restated, one species) -----------
 // U = (rho, rho u, ..., p/(gamma-1) + rho |u|^2 / 2); p = (gamma-1)(E - rho |u|^2 / 2)
 template <int NV>

@@ -237,6 +237,7 @@ struct PolExact {
   static constexpr bool kFast = false;
   static constexpr bool kCompensated = false;
   static constexpr bool kMixed = false;
+  static constexpr bool kFace32 = false;
   __device__ static double inv_len(double l) { return 0.0; }
   __device__ static double slope(double dq, double l, double) { return dq / l; }
   __device__ static double lim(double x, double y) { return ex::limiter<LIM>(x, y); }
@@ -257,6 +258,9 @@ struct PolFast {
   static constexpr bool kFast = true;
   static constexpr bool kCompensated = MIXED;
   static constexpr bool kMixed = MIXED;
+  // face states and Riemann solve in FP32 (face32): the mixed precision with
+  // a solver that has an FP32 form
+  static constexpr bool kFace32 = MIXED && RIE <= 1;
   __device__ static double inv_len(double l) { return fast::rcp(l); }
   __device__ static double slope(double dq, double, double il) { return dq * il; }
   __device__ static double lim(double x, double y) {
@@ -280,6 +284,22 @@ struct PolFast {
       ex::riemann<RIE, NV>(g, QL, aL, QR, aR, n, F, beta);
     }
     for (int v = 0; v < NV; ++v) F[v] = F[v] * A;
+    return ok;
+  }
+  // FP32 face states QL, QR (rho, velocity, p): the FP32 solve, its flux per
+  // unit area widened to FP64 (exactly) and scaled by the face area
+  template <int NV>
+  __device__ static bool face32(const Gas& g, const float* QL, const float* QR, const double* n, double A,
+                                double* F) {
+    constexpr int P = NV - 1;
+    const bool ok = (QL[0] > 0.0f && QL[P] > 0.0f && QR[0] > 0.0f && QR[P] > 0.0f);
+    const fast::GasF32 gf = fast::gasf32(g);
+    const float nf[3] = {(float)n[0], (float)n[1], (float)n[2]};
+    float f[NV];
+    if constexpr (RIE == 0) fast::hllc32n<NV>(gf, QL, QR, nf, f);
+    else fast::ausmp32n<NV>(gf, QL, QR, nf, f);
+#pragma unroll
+    for (int v = 0; v < NV; ++v) F[v] = (double)f[v] * A;
     return ok;
   }
   template <int NV>

@@ -79,6 +79,17 @@ template <class PH, bool UNI>
 __device__ __forceinline__ bool face(const Gas& g, const double* PL, const double* sL, double dL, const double* PR,
                                      const double* sR, double dR, const double* n, double A, double* F) {
   constexpr bool FU = UNI && PH::kFast;
+  if constexpr (FU && PH::kFace32) {
+    // mixed precision on uniform grids: face states and the solve in FP32
+    // (slopes in difference units, half-cell offsets of 1/2)
+    float QL[NV], QR[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+      QL[v] = fmaf((float)sL[v], 0.5f, (float)PL[v]);
+      QR[v] = fmaf((float)sR[v], -0.5f, (float)PR[v]);
+    }
+    return PH::template face32<NV>(g, QL, QR, n, A, F);
+  }
   const double hm = FU ? 0.5 : 0.5 * dL, hp = FU ? 0.5 : 0.5 * dR;
   double QL[NV], QR[NV];
 #pragma unroll
