@@ -228,7 +228,8 @@ void* mose_gpu_stream(const mose_gpu_ctx* ctx);
  * launches[c] counts the launches of each class.  Advances the solution. */
 int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t* launches);
 /* 1 when every metric of every block is uniform and the constant-metric
- * kernels are used. */
+ * kernels are used: bitwise uniform for the exact and fp64 precisions, within
+ * 1e-9 relative of each block's first cell for the mixed precision. */
 int mose_gpu_uniform_metrics(const mose_gpu_ctx* ctx);
 /* Number of kernel launches this context issued since creation. */
 int64_t mose_gpu_launch_count(const mose_gpu_ctx* ctx);
