@@ -142,6 +142,21 @@ def aggregate(world, cells, steps, ms):
     return world * cells * steps / (ms / 1e3)
 
 
+def fp64_ceiling(device):
+    """Measured issue ceilings of FP64 FMA, IEEE division and IEEE square root
+    on this GPU (mose_gpu_fp64_peak): the compute roofline of the fp64 and
+    exact stage kernels, beside the HBM copy bandwidth."""
+    import ctypes as C
+    from mose_b200 import _lib
+    lib = _lib.load()
+    out = np.zeros(6)
+    if lib.mose_gpu_fp64_peak(device, out.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+        return None
+    return {"dfma_tflops": float(out[0]), "ddiv_g_per_s": float(out[1]), "dsqrt_g_per_s": float(out[2]),
+            "method": "independent FMA / division / square-root chains per thread, 1024 threads per SM, "
+                      "CUDA events around the second of two launches"}
+
+
 def cpu_baseline(seconds=15.0, n=512):
     """The oracle's OpenMP build on a bounded sample: the same problem on a
     512 x 512 block, steps until ~`seconds` of CPU work."""
@@ -530,6 +545,8 @@ def run_gpu(args):
                 "variants": variants}
         if extra is not None:
             line["configs"] = extra
+        if world == 1:
+            line["fp64_ceiling"] = fp64_ceiling(local)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)

@@ -70,6 +70,7 @@ SIGNATURES = {
     "mose_gpu_download_metrics": (C.c_int, [_D, C.c_int32, _dp, _dp]),
     "mose_gpu_download_faces": (C.c_int, [_D, C.c_int32, C.c_int32, _dp, _dp]),
     "mose_gpu_check_fast_math": (C.c_int, [C.c_int64, C.c_uint64, _dp]),
+    "mose_gpu_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "mose_gpu_set_inflow_mach": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_riemann_minf": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_irs_beta": (C.c_int, [_D, C.c_double]),

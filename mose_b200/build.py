@@ -34,6 +34,7 @@ UNITS = {
     "mose_gpu.cu": [],
     "norms_noalloc.cu": [],
     "fastmath_check.cu": [],
+    "fp64_peak.cu": [],
     "adjoint.cu": [],
 }
 

@@ -23,3 +23,19 @@ def test_fast_reciprocals_within_one_ulp():
     assert rsq <= 2.0, out
     assert sq <= 2.0, out
     assert ulp_sqrt <= 1.0, out
+
+
+def test_fp64_issue_ceilings():
+    """The FP64 ceiling microbenchmark returns finite rates in a plausible
+    range for one B200 (FMA tens of TFLOP/s; division and square root
+    slower than FMA) and timed launches of a few milliseconds."""
+    from mose_b200 import _lib
+    lib = _lib.load()
+    out = np.zeros(6)
+    assert lib.mose_gpu_fp64_peak(0, out.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    fma_tf, div_g, sqrt_g = out[:3]
+    assert np.all(np.isfinite(out)) and np.all(out > 0), out
+    assert 5.0 < fma_tf < 200.0, out
+    fma_g = fma_tf * 1e3 / 2.0           # FMAs per ns
+    assert div_g < fma_g and sqrt_g < fma_g, out
+    assert np.all(out[3:] < 1000.0), out
