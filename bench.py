@@ -450,6 +450,10 @@ def profile_adjoint(local):
 # reads; ~45 MB of each launch's output is still in L2 when it ends, so the
 # write count is below the state written.
 TRAFFIC_BYTES_PER_CELL = {"fp64": 330.3e6 / 2048 ** 2, "mixed": 330.1e6 / 2048 ** 2, "exact": None}
+# FP64-pipe lane slots per cell per stage of the stage kernel on the 2048^2
+# vortex (ncu sm__inst_executed_pipe_fp64.sum x 32 / cells, 3-stage average;
+# profiles/stage2d_vortex2048_fp64_ops.md)
+FP64_SLOTS_PER_CELL = {"fp64": 492.2, "exact": 1156.0}
 
 
 def run_gpu(args):
@@ -546,7 +550,18 @@ def run_gpu(args):
         if extra is not None:
             line["configs"] = extra
         if world == 1:
-            line["fp64_ceiling"] = fp64_ceiling(local)
+            ceil = fp64_ceiling(local)
+            line["fp64_ceiling"] = ceil
+            slots = FP64_SLOTS_PER_CELL.get(args.precision)
+            if ceil is not None and slots:
+                # the stage kernel against the FP64 pipe: lane operations per
+                # second over the measured FMA issue rate (2 flops per FMA)
+                ach = slots * cells / (stage_ms * 1e-3) / 1e12
+                pk = ceil["dfma_tflops"] / 2.0
+                line["fp64_roofline"] = {"kernel": "k_stage2d", "achieved": ach, "peak": pk,
+                                         "unit": "T FP64 lane-ops/s", "frac": ach / pk,
+                                         "slots_per_cell_stage": slots,
+                                         "slots_source": "ncu sm__inst_executed_pipe_fp64.sum x 32 / cells"}
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
