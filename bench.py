@@ -562,6 +562,11 @@ def run_gpu(args):
                                          "unit": "T FP64 lane-ops/s", "frac": ach / pk,
                                          "slots_per_cell_stage": slots,
                                          "slots_source": "ncu sm__inst_executed_pipe_fp64.sum x 32 / cells"}
+            for name, vv in variants.items():
+                sl = FP64_SLOTS_PER_CELL.get(name)
+                if ceil is not None and sl and vv.get("stage_ms"):
+                    vv["fp64_roofline_frac"] = (sl * cells / (vv["stage_ms"] * 1e-3) / 1e12
+                                                / (ceil["dfma_tflops"] / 2.0))
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
