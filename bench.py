@@ -465,6 +465,9 @@ def run_gpu(args):
     if args.profile and args.profile_case == "quadrant":
         from mose_b200 import cases
         case = cases.four_quadrant(seed=0, steps=args.steps)
+    elif args.profile and args.profile_case in ("box3d", "box3d_small"):
+        from mose_b200 import cases
+        case = cases.periodic_box_3d(128 if args.profile_case == "box3d" else 64, steps=args.steps)
     else:
         case = workload_case(N_CELLS_SIDE, steps=args.steps)
     cells = case.ncells
@@ -589,8 +592,9 @@ def main():
                     help="skip the four-quadrant and 3-D configuration reports")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + K fused steps (the command profiled by ncu); prints nothing")
-    ap.add_argument("--profile-case", default="vortex", choices=["vortex", "quadrant"],
-                    help="with --profile: the 2048^2 vortex or the 64-block four-quadrant domain (seed 0)")
+    ap.add_argument("--profile-case", default="vortex", choices=["vortex", "quadrant", "box3d", "box3d_small"],
+                    help="with --profile: the 2048^2 vortex, the 64-block four-quadrant domain (seed 0), "
+                         "the 3-D periodic box of 8 x 128^3 or of 8 x 64^3 cells")
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="only the adjoint's forward + backward on a 16-step channel (profiled by ncu)")
     args = ap.parse_args()
