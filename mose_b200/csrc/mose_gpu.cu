@@ -123,7 +123,9 @@ std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int gri
 // Work items of the 3-D sweeps.  [0] i-sweep: (block, c0 | c1 << 16, r0, r1)
 // over rows r = j + nj k, strips as in 2-D, runs of up to 64 rows; [1] j-march
 // and [2] k-march: (block, q0, m0, m1), 256 consecutive columns q of the
-// block's (i, k) or (i, j) plane marching m over runs of at most 64 cells.
+// block's (i, k) or (i, j) plane marching m over runs of at most 32 cells
+// (the marches are latency-bound: shorter runs give more items per wave of
+// the persistent grid and a shorter tail, for one extra face flux per run).
 void plan_3d_items(const std::vector<HostBlock>& blocks, std::vector<int4> out[3]) {
   for (int q = 0; q < 3; ++q) out[q].clear();
   for (int b = 0; b < (int)blocks.size(); ++b) {
@@ -139,7 +141,7 @@ void plan_3d_items(const std::vector<HostBlock>& blocks, std::vector<int4> out[3
     for (int dir = 1; dir <= 2; ++dir) {
       const int nl = dir == 1 ? h.nj : h.nk, nother = dir == 1 ? h.nk : h.nj;
       const int ncol = h.ni * nother;
-      const std::vector<int> mc = split_even(nl, (nl + 63) / 64, 1);
+      const std::vector<int> mc = split_even(nl, (nl + 31) / 32, 1);
       for (size_t r = 0; r + 1 < mc.size(); ++r)
         for (int q0 = 0; q0 < ncol; q0 += SB_T)
           if (mc[r + 1] > mc[r]) out[dir].push_back(make_int4(b, q0, mc[r], mc[r + 1]));
