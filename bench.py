@@ -35,7 +35,10 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 N_CELLS_SIDE = 2048
-BYTES_PER_CELL_STEP = 256          # 8 * nv * 8 B with nv = 4
+# 8 arrays of nv = 4 doubles per cell and RK3 step: stage 1 reads P^n and
+# writes P^1; stages 2 and 3 read their input and P^n and write their output
+# (the fused CFL pass works on the state the last stage has just written)
+BYTES_PER_CELL_STEP = 256
 STAGE_BYTES_PER_CELL = (64 + 96 + 96) / 3.0   # stage 1 reads P^n, writes P^1; stages 2,3 also read P^n
 FALLBACK_HBM_GBS = 6650.0
 
@@ -451,8 +454,8 @@ def profile_adjoint(local):
 # write count is below the state written.
 TRAFFIC_BYTES_PER_CELL = {"fp64": 330.3e6 / 2048 ** 2, "mixed": 330.1e6 / 2048 ** 2, "exact": None}
 # FP64-pipe lane slots per cell per stage of the stage kernel on the 2048^2
-# vortex (ncu sm__inst_executed_pipe_fp64.sum x 32 / cells, 3-stage average;
-# profiles/stage2d_vortex2048_fp64_ops.md)
+# vortex (ncu sm__inst_executed_pipe_fp64.sum x 32 / cells, average of the
+# three RK stages of one step)
 FP64_SLOTS_PER_CELL = {"fp64": 492.2, "exact": 1156.0}
 
 
