@@ -147,13 +147,13 @@ def aggregate(world, cells, steps, ms):
 
 def fp64_ceiling(device):
     """Measured issue ceilings of FP64 FMA, IEEE division and IEEE square root
-    on this GPU (mose_gpu_fp64_peak): the compute roofline of the fp64 and
+    on this GPU (mose_probe_fp64_peak, libmose_probe.so): the compute roofline of the fp64 and
     exact stage kernels, beside the HBM copy bandwidth."""
     import ctypes as C
     from mose_b200 import _lib
-    lib = _lib.load()
+    lib = _lib.load_probe()
     out = np.zeros(6)
-    if lib.mose_gpu_fp64_peak(device, out.ctypes.data_as(C.POINTER(C.c_double))) != 0:
+    if lib.mose_probe_fp64_peak(device, out.ctypes.data_as(C.POINTER(C.c_double))) != 0:
         return None
     return {"dfma_tflops": float(out[0]), "ddiv_g_per_s": float(out[1]), "dsqrt_g_per_s": float(out[2]),
             "method": "independent FMA / division / square-root chains per thread, 1024 threads per SM, "

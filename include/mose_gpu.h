@@ -249,15 +249,6 @@ int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N
  * rounded one.  No context needed; synchronous. */
 int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
 
-/* Issue ceilings of the FP64 operations the stage kernels are made of, on
- * the given device (no reference counterpart: the compute roofline of this
- * path, which has no dense contraction).  out[0]: FP64 fused multiply-add,
- * TFLOP/s (two flops each); out[1]: IEEE FP64 divisions, G/s; out[2]: IEEE
- * FP64 square roots, G/s; out[3..5]: the timed launches' durations in ms.
- * Independent dependency chains per thread, 1024 threads per SM, CUDA events
- * around the second of two identical launches.  Synchronous; about 0.1 s. */
-int mose_gpu_fp64_peak(int32_t device, double* out);
-
 /* ---- Discrete adjoint (2-D, HLLC with minmod / van Leer / van Albada,
  * time-accurate SSP-RK).  The objective is the pressure integral over one
  * block face, J = sum over the face cells of p * A (the wall-pressure

@@ -70,7 +70,6 @@ SIGNATURES = {
     "mose_gpu_download_metrics": (C.c_int, [_D, C.c_int32, _dp, _dp]),
     "mose_gpu_download_faces": (C.c_int, [_D, C.c_int32, C.c_int32, _dp, _dp]),
     "mose_gpu_check_fast_math": (C.c_int, [C.c_int64, C.c_uint64, _dp]),
-    "mose_gpu_fp64_peak": (C.c_int, [C.c_int32, _dp]),
     "mose_gpu_set_inflow_mach": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_riemann_minf": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_irs_beta": (C.c_int, [_D, C.c_double]),
@@ -88,6 +87,24 @@ SIGNATURES = {
 
 
 _lib = None
+_probe = None
+
+# the measurement-only library (FP64 issue ceilings), not part of the ABI
+PROBE_PATH = _HERE / "lib" / "libmose_probe.so"
+
+
+def load_probe() -> C.CDLL:
+    """Loads libmose_probe.so (bench and tests only); raises if not built."""
+    global _probe
+    if _probe is not None:
+        return _probe
+    if not PROBE_PATH.exists():
+        raise RuntimeError(f"{PROBE_PATH} is missing: build it with `python -m mose_b200.build`")
+    lib = C.CDLL(str(PROBE_PATH))
+    lib.mose_probe_fp64_peak.restype = C.c_int
+    lib.mose_probe_fp64_peak.argtypes = [C.c_int32, _dp]
+    _probe = lib
+    return lib
 
 
 def load() -> C.CDLL:

@@ -17,6 +17,9 @@ CSRC = HERE / "csrc"
 LIBDIR = HERE / "lib"
 OBJDIR = HERE / "_build"
 LIBNAME = "libmose_gpu.so"
+# measurement-only probes, linked into their own library beside the product
+PROBE_DIR = HERE / "probe"
+PROBE_LIB = "libmose_probe.so"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -34,7 +37,6 @@ UNITS = {
     "mose_gpu.cu": [],
     "norms_noalloc.cu": [],
     "fastmath_check.cu": [],
-    "fp64_peak.cu": [],
     "adjoint.cu": [],
 }
 
@@ -88,6 +90,13 @@ def build(verbose: bool = False, force: bool = False, out_dir: Path | None = Non
     lib = LIBDIR / LIBNAME
     if force or _stale(lib, objs):
         cmd = [cc] + ARCH + ["-shared", "-cudart=static", "-o", str(lib)] + [str(o) for o in objs]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    probe = LIBDIR / PROBE_LIB
+    psrc = sorted(PROBE_DIR.glob("*.cu"))
+    if psrc and (force or _stale(probe, psrc)):
+        cmd = [cc] + COMMON + ["-shared", "-cudart=static", "-o", str(probe)] + [str(x) for x in psrc]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

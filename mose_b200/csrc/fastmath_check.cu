@@ -10,6 +10,8 @@
 // rounded one (__dsqrt_rn).
 #include <cuda_runtime.h>
 
+#include "nvtx.cuh"
+
 #include <cstdint>
 #include <cstring>
 
@@ -58,6 +60,7 @@ __global__ void k_check_fast_math(long long n, uint64_t seed, unsigned long long
 }  // namespace
 
 extern "C" int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out) {
+  MOSE_NVTX_RANGE("mose_gpu_check_fast_math");
   if (n <= 0 || !out) return MOSE_ERR_INVALID;
   unsigned long long* d = nullptr;
   if (cudaMalloc(&d, 4 * sizeof(unsigned long long)) != cudaSuccess) return MOSE_ERR_CUDA;

@@ -6,6 +6,8 @@
 // return values to the host.
 #include <cuda_runtime.h>
 
+#include "nvtx.cuh"
+
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
@@ -156,6 +158,10 @@ struct mose_gpu_ctx {
   Gas gas;
   std::string err;
   int devcode = 0, eb = 0, ei = 0, ej = 0, ek = 0;
+  // the first failed enqueue that returns no status of its own (a copy
+  // inside a step's sequence), reported by the next check_launch
+  cudaError_t enq_err = cudaSuccess;
+  const char* enq_what = "";
   cudaStream_t stream = nullptr;
   int nsm = 148;
   bool ready = false;
@@ -274,6 +280,12 @@ int fail(mose_gpu_ctx* c, int code, const char* fmt, ...) {
   } while (0)
 
 int check_launch(mose_gpu_ctx* ctx, const char* what) {
+  if (ctx->enq_err != cudaSuccess) {
+    const cudaError_t q = ctx->enq_err;
+    ctx->enq_err = cudaSuccess;
+    cudaGetLastError();
+    return fail(ctx, MOSE_ERR_CUDA, "%s: %s: %s", what, ctx->enq_what, cudaGetErrorString(q));
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "%s launch: %s", what, cudaGetErrorString(e));
   return MOSE_OK;
@@ -357,6 +369,7 @@ void mose_gpu_default_config(mose_gpu_config* cfg) {
 }
 
 int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
+  MOSE_NVTX_RANGE("mose_gpu_create");
   mose_gpu_ctx* ctx = nullptr;
   if (!cfg || !out) return MOSE_ERR_INVALID;
   *out = nullptr;
@@ -409,6 +422,7 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
 }
 
 void mose_gpu_destroy(mose_gpu_ctx* ctx) {
+  MOSE_NVTX_RANGE("mose_gpu_destroy");
   if (!ctx) return;
   cudaSetDevice(ctx->cfg.device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
@@ -437,6 +451,7 @@ int mose_gpu_error_location(const mose_gpu_ctx* ctx, int32_t* b, int32_t* i, int
 }
 
 int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int32_t nk, const double* node) {
+  MOSE_NVTX_RANGE("mose_gpu_add_block");
   if (!ctx || !node) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "add_block after setup");
   if (b != (int)ctx->hblk.size() + 1) return fail(ctx, MOSE_ERR_INVALID, "blocks must be added in order 1..nb");
@@ -451,6 +466,7 @@ int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int
 
 int mose_gpu_add_series(mose_gpu_ctx* ctx, const double* time, const double* value, int32_t n, int32_t periodic,
                         int32_t* id) {
+  MOSE_NVTX_RANGE("mose_gpu_add_series");
   if (!ctx || !time || !value || !id || n < 1) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "add_series after setup");
   mose_gpu_ctx::SerIdx si{(int)(ctx->hser.size() / 2), n, periodic ? 1 : 0};
@@ -464,6 +480,7 @@ int mose_gpu_add_series(mose_gpu_ctx* ctx, const double* time, const double* val
 }
 
 int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, int32_t nbound) {
+  MOSE_NVTX_RANGE("mose_gpu_set_bcs");
   if (!ctx || !rec) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_bcs after setup");
   int nb = (int)ctx->hblk.size();
@@ -539,6 +556,7 @@ static int install_items(mose_gpu_ctx* ctx) {
 }
 
 int mose_gpu_setup(mose_gpu_ctx* ctx) {
+  MOSE_NVTX_RANGE("mose_gpu_setup");
   if (!ctx) return MOSE_ERR_INVALID;
   if (ctx->hblk.empty() || ctx->bc.empty()) return fail(ctx, MOSE_ERR_NOT_READY, "no blocks or no boundary records");
   CU(cudaSetDevice(ctx->cfg.device));
@@ -993,16 +1011,20 @@ static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool uplo
 }
 
 int mose_gpu_upload_prim(mose_gpu_ctx* ctx, int32_t b, const double* P) {
+  MOSE_NVTX_RANGE("mose_gpu_upload_prim");
   return prim_io(ctx, b, const_cast<double*>(P), ctx ? ctx->cur : 0, true);
 }
 int mose_gpu_download_prim(mose_gpu_ctx* ctx, int32_t b, double* P) {
+  MOSE_NVTX_RANGE("mose_gpu_download_prim");
   return prim_io(ctx, b, P, ctx ? ctx->cur : 0, false);
 }
 int mose_gpu_upload_prim_old(mose_gpu_ctx* ctx, int32_t b, const double* PO) {
+  MOSE_NVTX_RANGE("mose_gpu_upload_prim_old");
   return prim_io(ctx, b, const_cast<double*>(PO), ctx ? ctx->po : 1, true);
 }
 int mose_gpu_download_residual(mose_gpu_ctx* ctx, int32_t b, double* R) { return prim_io(ctx, b, R, -1, false); }
 int mose_gpu_upload_residual(mose_gpu_ctx* ctx, int32_t b, const double* R) {
+  MOSE_NVTX_RANGE("mose_gpu_download_residual");
   return prim_io(ctx, b, const_cast<double*>(R), -1, true);
 }
 
@@ -1029,6 +1051,7 @@ static int dt_io(mose_gpu_ctx* ctx, int32_t b, double* dt, bool upload) {
 }
 int mose_gpu_download_dt(mose_gpu_ctx* ctx, int32_t b, double* dt) { return dt_io(ctx, b, dt, false); }
 int mose_gpu_upload_dt(mose_gpu_ctx* ctx, int32_t b, const double* dt) {
+  MOSE_NVTX_RANGE("mose_gpu_download_dt");
   return dt_io(ctx, b, const_cast<double*>(dt), true);
 }
 
@@ -1041,6 +1064,7 @@ static int require_ready(mose_gpu_ctx* ctx) {
 }
 
 int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ramp_iter, double* dtglobal) {
+  MOSE_NVTX_RANGE("mose_gpu_compute_dt");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!dtglobal) return MOSE_ERR_INVALID;
@@ -1057,6 +1081,7 @@ int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ram
 }
 
 int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
+  MOSE_NVTX_RANGE("mose_gpu_set_global_dt");
   int rc = require_ready(ctx);
   if (rc) return rc;
   ctx->dt_valid = false;
@@ -1069,6 +1094,7 @@ int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
 }
 
 int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
+  MOSE_NVTX_RANGE("mose_gpu_copy_state");
   int rc = require_ready(ctx);
   if (rc) return rc;
   ctx->dt_valid = false;
@@ -1079,6 +1105,7 @@ int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
 }
 
 int mose_gpu_fill_ghosts(mose_gpu_ctx* ctx) {
+  MOSE_NVTX_RANGE("mose_gpu_fill_ghosts");
   int rc = require_ready(ctx);
   if (rc) return rc;
   launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[ctx->cur].p, ctx->margs(), ctx->nd, ctx->derr.p,
@@ -1154,6 +1181,7 @@ static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int pre
 static int enqueue_series(mose_gpu_ctx* ctx);
 
 int mose_gpu_residual(mose_gpu_ctx* ctx) {
+  MOSE_NVTX_RANGE("mose_gpu_residual");
   int rc = require_ready(ctx);
   if (rc) return rc;
   // the phase-by-phase path always runs the reference-exact arithmetic; 402
@@ -1173,6 +1201,7 @@ int mose_gpu_residual(mose_gpu_ctx* ctx) {
 static int enqueue_irs_smoothing(mose_gpu_ctx* ctx);
 
 int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
+  MOSE_NVTX_RANGE("mose_gpu_rk_stage");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (irk < 1 || irk > ctx->cfg.n_rk) return fail(ctx, MOSE_ERR_INVALID, "irk out of range");
@@ -1239,8 +1268,15 @@ static int enqueue_irs_smoothing(mose_gpu_ctx* ctx) {
   int k = 0;
   for (int dir = 0; dir < ctx->ndir; ++dir) {
     launch_irs_ghost(ctx->irs_list.p, ctx->nirs, ctx->resid.p, ctx->stream);
-    cudaMemcpyAsync(ctx->rs1.p, ctx->resid.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
-    cudaMemcpyAsync(ctx->rs2.p, ctx->resid.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+    // the Jacobi sweeps read both copies: a failed copy is reported by the
+    // step's check_launch instead of smoothing stale data silently
+    for (double* dst : {ctx->rs1.p, ctx->rs2.p}) {
+      const cudaError_t e = cudaMemcpyAsync(dst, ctx->resid.p, bytes, cudaMemcpyDeviceToDevice, ctx->stream);
+      if (e != cudaSuccess && ctx->enq_err == cudaSuccess) {
+        ctx->enq_err = e;
+        ctx->enq_what = "IRS residual copy";
+      }
+    }
     launch_irs_jacobi(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->rs1.p, ctx->rs2.p, dir, ctx->irs_beta,
                       ctx->stream);
     launch_irs_jacobi(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->rs2.p, ctx->resid.p, dir, ctx->irs_beta,
@@ -1307,6 +1343,7 @@ static int step_final_index(const mose_gpu_ctx* ctx, int s0) {
 }
 
 int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
+  MOSE_NVTX_RANGE("mose_gpu_step");
   int rc = require_ready(ctx);
   if (rc) return rc;
   CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
@@ -1340,6 +1377,10 @@ static int enqueue_graph_steps(mose_gpu_ctx* ctx, int nsteps) {
       CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
       int k = enqueue_step(ctx, s0);
       CU(cudaStreamEndCapture(ctx->stream, &g));
+      if (int rc = check_launch(ctx, "step capture")) {
+        cudaGraphDestroy(g);
+        return rc;
+      }
       CU(cudaGraphInstantiate(&ctx->graph[s0], g, 0));
       cudaGraphDestroy(g);
       ctx->graph_kernels = k;
@@ -1354,6 +1395,7 @@ static int enqueue_graph_steps(mose_gpu_ctx* ctx, int nsteps) {
 }
 
 int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double* time) {
+  MOSE_NVTX_RANGE("mose_gpu_advance");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (nsteps < 0) return MOSE_ERR_INVALID;
@@ -1372,6 +1414,7 @@ int mose_gpu_advance(mose_gpu_ctx* ctx, int32_t nsteps, double* dtglobal, double
 }
 
 int mose_gpu_residual_norms(mose_gpu_ctx* ctx, double* total) {
+  MOSE_NVTX_RANGE("mose_gpu_residual_norms");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!total) return MOSE_ERR_INVALID;
@@ -1384,6 +1427,7 @@ int mose_gpu_residual_norms(mose_gpu_ctx* ctx, double* total) {
 }
 
 int mose_gpu_set_time(mose_gpu_ctx* ctx, double time, int32_t iter) {
+  MOSE_NVTX_RANGE("mose_gpu_set_time");
   if (!ctx) return MOSE_ERR_INVALID;
   ctx->h_time = time;
   ctx->h_iter = iter;
@@ -1398,6 +1442,7 @@ int mose_gpu_get_time(mose_gpu_ctx* ctx, double* time, int32_t* iter) {
 }
 
 int mose_gpu_synchronize(mose_gpu_ctx* ctx) {
+  MOSE_NVTX_RANGE("mose_gpu_synchronize");
   int rc = require_ready(ctx);
   if (rc) return rc;
   CU(cudaStreamSynchronize(ctx->stream));
@@ -1409,6 +1454,7 @@ int mose_gpu_synchronize(mose_gpu_ctx* ctx) {
 void* mose_gpu_stream(const mose_gpu_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
 int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t* launches) {
+  MOSE_NVTX_RANGE("mose_gpu_time_kernels");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!ms || !launches || nsteps < 1) return MOSE_ERR_INVALID;
@@ -1473,6 +1519,7 @@ int mose_gpu_uniform_metrics(const mose_gpu_ctx* ctx) { return ctx && ctx->unifo
 int64_t mose_gpu_launch_count(const mose_gpu_ctx* ctx) { return ctx ? ctx->launches : -1; }
 
 int mose_gpu_download_metrics(mose_gpu_ctx* ctx, int32_t b, double* vol, double* dl) {
+  MOSE_NVTX_RANGE("mose_gpu_download_metrics");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (b < 1 || b > (int)ctx->hblk.size()) return fail(ctx, MOSE_ERR_INVALID, "bad block");
@@ -1490,6 +1537,7 @@ int mose_gpu_download_metrics(mose_gpu_ctx* ctx, int32_t b, double* vol, double*
 }
 
 int mose_gpu_download_faces(mose_gpu_ctx* ctx, int32_t b, int32_t dir, double* N, double* A) {
+  MOSE_NVTX_RANGE("mose_gpu_download_faces");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (b < 1 || b > (int)ctx->hblk.size() || dir < 1 || dir > ctx->nd) return fail(ctx, MOSE_ERR_INVALID, "bad args");
@@ -1726,6 +1774,7 @@ static int adj_graphs(mose_gpu_ctx* ctx, int K) {
 }
 
 int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on) {
+  MOSE_NVTX_RANGE("mose_gpu_set_sd_limiter");
   if (!ctx) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_sd_limiter: call before mose_gpu_setup");
   ctx->gas.sd = (ctx->gas.sd & ~1) | (on ? 1 : 0);
@@ -1733,6 +1782,7 @@ int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on) {
 }
 
 int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta) {
+  MOSE_NVTX_RANGE("mose_gpu_set_irs_beta");
   if (!ctx) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_irs_beta: call before mose_gpu_setup");
   if (!(beta >= 0.0)) return fail(ctx, MOSE_ERR_INVALID, "set_irs_beta: beta must be >= 0");
@@ -1741,6 +1791,7 @@ int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta) {
 }
 
 int mose_gpu_set_riemann_minf(mose_gpu_ctx* ctx, double minf) {
+  MOSE_NVTX_RANGE("mose_gpu_set_riemann_minf");
   if (!ctx) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_riemann_minf: call before mose_gpu_setup");
   if (!(minf >= 0.0)) return fail(ctx, MOSE_ERR_INVALID, "set_riemann_minf: Minf must be >= 0");
@@ -1749,6 +1800,7 @@ int mose_gpu_set_riemann_minf(mose_gpu_ctx* ctx, double minf) {
 }
 
 int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
+  MOSE_NVTX_RANGE("mose_gpu_set_inflow_mach");
   int rc = require_ready(ctx);
   if (rc) return rc;
   bool any = false;
@@ -1771,6 +1823,7 @@ int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
 
 int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval, int32_t block, int32_t face,
                              double* J) {
+  MOSE_NVTX_RANGE("mose_gpu_adjoint_forward");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (nsteps < 1 || interval < 1 || !J) return fail(ctx, MOSE_ERR_INVALID, "adjoint_forward: bad arguments");
@@ -1813,6 +1866,7 @@ int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval
 }
 
 int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach) {
+  MOSE_NVTX_RANGE("mose_gpu_adjoint_backward");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!ctx->adj_recorded) return fail(ctx, MOSE_ERR_INVALID, "adjoint_backward needs a preceding adjoint_forward");
@@ -1853,6 +1907,7 @@ int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach) {
 }
 
 int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach) {
+  MOSE_NVTX_RANGE("mose_gpu_adjoint_step");
   int rc = require_ready(ctx);
   if (rc) return rc;
   rc = adj_prepare(ctx);
@@ -1877,6 +1932,7 @@ int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach) {
 }
 
 int mose_gpu_upload_adjoint(mose_gpu_ctx* ctx, int32_t b, const double* lam) {
+  MOSE_NVTX_RANGE("mose_gpu_upload_adjoint");
   int rc = require_ready(ctx);
   if (rc) return rc;
   rc = adj_prepare(ctx);
@@ -1887,6 +1943,7 @@ int mose_gpu_download_adjoint(mose_gpu_ctx* ctx, int32_t b, double* lam) { retur
 
 // ---- 2-D work-list tiling and its autotuner ------------------------------------
 int mose_gpu_get_tiling(const mose_gpu_ctx* ctx, int32_t* tiling) {
+  MOSE_NVTX_RANGE("mose_gpu_download_adjoint");
   if (!ctx || !tiling) return MOSE_ERR_INVALID;
   tiling[0] = ctx->tile_h; tiling[1] = ctx->tile_w; tiling[2] = ctx->tile_order; tiling[3] = ctx->tile_ctas;
   return MOSE_OK;
@@ -1900,6 +1957,7 @@ static int apply_tiling(mose_gpu_ctx* ctx, int h, int w, int order, int ctas) {
 }
 
 int mose_gpu_set_tiling(mose_gpu_ctx* ctx, const int32_t* tiling) {
+  MOSE_NVTX_RANGE("mose_gpu_set_tiling");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (!tiling) return MOSE_ERR_INVALID;
@@ -1922,6 +1980,7 @@ int mose_gpu_set_tiling(mose_gpu_ctx* ctx, const int32_t* tiling) {
 // best are timed again, alternately, three times, and the best is kept only
 // if still more than 1 % faster.  The state is restored at the end.
 int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, double* best_ms, double* default_ms) {
+  MOSE_NVTX_RANGE("mose_gpu_autotune");
   int rc = require_ready(ctx);
   if (rc) return rc;
   if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "the autotuner tunes the 2-D work list");

@@ -9,6 +9,8 @@
 // the process exits.
 #include <cuda_runtime.h>
 
+#include "nvtx.cuh"
+
 #include <cstdio>
 #include <mutex>
 
@@ -79,6 +81,7 @@ __global__ void k_norm_finish(const double* partial, int nchunks, double* total)
 
 extern "C" int mose_gpu_residual_norms_noalloc(const double* P, const double* PO, int32_t ni, int32_t nj,
                                                int32_t nk, double* total, void* stream) {
+  MOSE_NVTX_RANGE("mose_gpu_residual_norms_noalloc");
   if (!P || !PO || !total) return fail(MOSE_ERR_INVALID, "null array");
   if (ni < 1 || nj < 1 || nk < 1) return fail(MOSE_ERR_INVALID, "bad block dimensions");
   const long long ncell = (long long)ni * nj * nk;
@@ -93,10 +96,20 @@ extern "C" int mose_gpu_residual_norms_noalloc(const double* P, const double* PO
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(MOSE_ERR_CUDA, "no current CUDA device");
   double* scratch = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
   {
     std::lock_guard<std::mutex> lock(g_mu);
     if (!g_scratch_addr[dev]) {
-      // first call on this device (it is current): look up the array's address
+      // first call on this device (it is current): look up the array's
+      // address.  The lookup may load the module, which a stream capture in
+      // progress does not allow, so a first call inside a capture is refused.
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return fail(MOSE_ERR_INVALID,
+                    "the first call on a device must come before any stream capture (it looks up the scratch "
+                    "array's address)");
+      }
       cudaError_t e = cudaGetSymbolAddress((void**)&g_scratch_addr[dev], g_norm_scratch);
       if (e != cudaSuccess) {
         g_scratch_addr[dev] = nullptr;
@@ -106,7 +119,6 @@ extern "C" int mose_gpu_residual_norms_noalloc(const double* P, const double* PO
     }
     scratch = g_scratch_addr[dev];
   }
-  cudaStream_t s = (cudaStream_t)stream;
   k_norm_chunks<<<(unsigned)nchunks, kThreads, 0, s>>>(P, PO, ni, nj, ncell, scratch);
   k_norm_finish<<<1, 32, 0, s>>>(scratch, (int)nchunks, total);
   cudaError_t e = cudaGetLastError();

@@ -8,11 +8,16 @@
 // values stay bounded, and the result is kept live through one conditional
 // store, so nothing is optimised away.  Timed with CUDA events around the
 // second of two identical launches.
+//
+// Measurement only: built into libmose_probe.so beside the product library
+// (libmose_gpu.so), whose C ABI does not carry it.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 
-#include "../../include/mose_gpu.h"
+// status codes of this probe: 0 = ok, 1 = bad argument, 3 = CUDA failure
+// (the values of MOSE_OK, MOSE_ERR_INVALID, MOSE_ERR_CUDA in mose_gpu.h)
+enum { MOSE_OK = 0, MOSE_ERR_INVALID = 1, MOSE_ERR_CUDA = 3 };
 
 namespace {
 
@@ -87,7 +92,10 @@ int time_ms(L launch, float* ms) {
 
 }  // namespace
 
-extern "C" int mose_gpu_fp64_peak(int32_t device, double* out) {
+// out[0]: FP64 fused multiply-add, TFLOP/s (two flops each); out[1]: IEEE
+// FP64 divisions, G/s; out[2]: IEEE FP64 square roots, G/s; out[3..5]: the
+// timed launches' durations in ms.  Synchronous; about 0.1 s.
+extern "C" int mose_probe_fp64_peak(int32_t device, double* out) {
   if (!out) return MOSE_ERR_INVALID;
   cudaDeviceProp prop;
   if (cudaSetDevice(device) != cudaSuccess || cudaGetDeviceProperties(&prop, device) != cudaSuccess)

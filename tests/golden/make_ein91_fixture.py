@@ -1,7 +1,7 @@
 """Builds tests/golden/ein91_x8.npz from the reference's own Ein91 test case
 (the HLLE case of its 1-D suite).
 
-Reads, from the MOSE source tree (default /root/reference, or argv[1]):
+Reads, from the MOSE source tree (argv[1], or the MOSE_SOURCE_DIR environment variable):
   test/1D/Ein91/MESH/mesh_x8.tec    node coordinates (Tecplot ASCII, BLOCK)
   test/1D/Ein91/INPUT/ic_x8.tec     initial primitives (cell centred)
   test/1D/Ein91/INPUT/bc_x8.txt     boundary list (bc.txt format)
@@ -21,6 +21,9 @@ import sys
 from pathlib import Path
 
 import numpy as np
+
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from _source import source_tree  # noqa: E402
 
 
 def _numbers(lines):
@@ -81,7 +84,8 @@ def exact_riemann(WL, WR, g, xi):
     return out
 
 
-def main(root: str = "/root/reference") -> Path:
+def main(root: str | None = None) -> Path:
+    root = source_tree(root)
     case = Path(root) / "test" / "1D" / "Ein91"
     mesh = (case / "MESH" / "mesh_x8.tec").read_text().splitlines()
     ni1, nj1, nk1 = 801, 2, 2

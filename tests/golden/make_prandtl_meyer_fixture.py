@@ -17,8 +17,12 @@ import numpy as np
 sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
 from mose_b200 import refio  # noqa: E402
 
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from _source import source_tree  # noqa: E402
 
-def main(root: str = "/root/reference") -> Path:
+
+def main(root: str | None = None) -> Path:
+    root = source_tree(root)
     c = refio.load_case(Path(root) / "test" / "2D" / "euler" / "prandtl-meyer")
     assert c.extra["unsupported"] == [], c.extra["unsupported"]
     out = Path(__file__).resolve().parent / "prandtl_meyer.npz"

@@ -1,6 +1,6 @@
 """Builds tests/golden/sod79_x4.npz from the reference's own Sod79 test case.
 
-Reads, from the MOSE source tree (default /root/reference, or argv[1]):
+Reads, from the MOSE source tree (argv[1], or the MOSE_SOURCE_DIR environment variable):
   test/1D/Sod79/MESH/mesh_x4.tec    node coordinates (Tecplot ASCII, BLOCK)
   test/1D/Sod79/INPUT/ic_x4.tec     initial primitives (cell centred)
   test/1D/Sod79/INPUT/bc_x4.txt     boundary list (bc.txt format)
@@ -17,12 +17,16 @@ from pathlib import Path
 
 import numpy as np
 
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from _source import source_tree  # noqa: E402
+
 
 def _numbers(lines):
     return np.array(" ".join(lines).split(), dtype=np.float64)
 
 
-def main(root: str = "/root/reference") -> Path:
+def main(root: str | None = None) -> Path:
+    root = source_tree(root)
     case = Path(root) / "test" / "1D" / "Sod79"
     mesh = (case / "MESH" / "mesh_x4.tec").read_text().splitlines()
     ni1, nj1, nk1 = 401, 2, 2

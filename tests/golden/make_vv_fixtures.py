@@ -1,7 +1,7 @@
 """Builds tests/golden/tor99_x8.npz from one more of the reference's 1-D
 verification cases (and, for the record, noh87_x8.npz; see below).
 
-Reads, from the MOSE source tree (default /root/reference, or argv[1]),
+Reads, from the MOSE source tree (argv[1], or the MOSE_SOURCE_DIR environment variable),
 through mose_b200.refio: test/1D/<case>/MESH/mesh_x8.tec,
 INPUT/ic_x8.tec, INPUT/bc_x8.txt and input.ini (the gas is test/common/Air,
 which both cases' MOSE.sh link).
@@ -41,6 +41,9 @@ sys.path.insert(0, str(HERE))
 from make_ein91_fixture import exact_riemann   # noqa: E402
 from mose_b200 import refio                     # noqa: E402
 
+sys.path.insert(0, str(Path(__file__).resolve().parent))
+from _source import source_tree  # noqa: E402
+
 
 def _save(name, case, exact, probes, thresholds, extra):
     out = HERE / f"{name}.npz"
@@ -51,7 +54,8 @@ def _save(name, case, exact, probes, thresholds, extra):
     return out
 
 
-def main(root: str = "/root/reference"):
+def main(root: str | None = None):
+    root = source_tree(root)
     outs = []
     case = refio.load_case(Path(root) / "test" / "1D" / "Tor99", "x8")
     x = 0.5 * (case.nodes[0][0, 0, :-1, 0] + case.nodes[0][0, 0, 1:, 0])

@@ -31,6 +31,14 @@ def test_every_declared_symbol_is_exported(lib):
     assert not missing, missing
 
 
+def test_measurement_probe_stays_out_of_the_product(lib):
+    """The FP64 issue-ceiling probe is a benchmark tool: it lives in its own
+    library, not in the ABI a Fortran solver links."""
+    from mose_b200 import _lib
+    assert not hasattr(lib, "mose_gpu_fp64_peak")
+    assert hasattr(_lib.load_probe(), "mose_probe_fp64_peak")
+
+
 def test_binding_covers_the_header(lib):
     from mose_b200 import _lib
     assert set(_lib.SIGNATURES) == set(declared_functions())

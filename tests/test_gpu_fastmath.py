@@ -30,9 +30,9 @@ def test_fp64_issue_ceilings():
     range for one B200 (FMA tens of TFLOP/s; division and square root
     slower than FMA) and timed launches of a few milliseconds."""
     from mose_b200 import _lib
-    lib = _lib.load()
+    lib = _lib.load_probe()
     out = np.zeros(6)
-    assert lib.mose_gpu_fp64_peak(0, out.ctypes.data_as(C.POINTER(C.c_double))) == 0
+    assert lib.mose_probe_fp64_peak(0, out.ctypes.data_as(C.POINTER(C.c_double))) == 0
     fma_tf, div_g, sqrt_g = out[:3]
     assert np.all(np.isfinite(out)) and np.all(out > 0), out
     assert 5.0 < fma_tf < 200.0, out

@@ -2,6 +2,7 @@
 files written in the reference's formats (Tecplot ASCII BLOCK zones,
 bc.txt two-line records, input.ini), and, where the reference tree is
 present, its own Sod79 and Ein91 inputs against the committed fixtures."""
+import os
 from pathlib import Path
 
 import numpy as np
@@ -10,7 +11,8 @@ import pytest
 from mose_b200 import cases, refio
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-REF = Path("/root/reference/test")
+# the reference's own test inputs, when MOSE_SOURCE_DIR names a MOSE source tree
+REF = Path(os.environ.get("MOSE_SOURCE_DIR", "/nonexistent")) / "test"
 
 
 def write_tecplot(path, zones, names, ncell_vars=0):
@@ -83,7 +85,7 @@ def test_sd_and_irs_numerics_read(tmp_path):
     assert kw["unsupported"] == [] and kw["irs_beta"] == 0.5 and kw["sd_limiter"]
 
 
-@pytest.mark.skipif(not REF.exists(), reason="reference tree not present")
+@pytest.mark.skipif(not REF.exists(), reason="MOSE_SOURCE_DIR does not name a MOSE source tree")
 @pytest.mark.parametrize("name,res,fixture", [("1D/Sod79", "x4", "sod79_x4.npz"), ("1D/Ein91", "x8", "ein91_x8.npz")])
 def test_reference_inputs_match_fixtures(name, res, fixture):
     """The readers give, from the reference's own files, exactly the arrays

@@ -28,7 +28,11 @@ def _run(case):
     s.explicit_step()
     after = [np.ascontiguousarray(s.download_prim(b)) for b in range(1, nb + 1)]
     expect = s.compute_residual()            # the existing entry point: sums over blocks
-    assert np.all(expect[[0, 1, 2, 4]] > 0) and expect[3] == 0.0     # 2-D: w is identically zero
+    assert np.all(expect[[0, 1, 2, 4]] > 0)
+    if all(d[2] == 1 for d in s.dims):
+        assert expect[3] == 0.0              # 2-D: w is identically zero
+    else:
+        assert expect[3] > 0.0               # 3-D: the w sums and the k-plane offsets are exercised
     dev = torch.device("cuda", 0)
     P = [torch.from_numpy(a).to(dev) for a in after]
     PO = [torch.from_numpy(a).to(dev) for a in before]
@@ -55,6 +59,11 @@ def test_noalloc_norms_single_block():
 
 def test_noalloc_norms_multi_block_accumulates():
     _run(cases.four_quadrant(seed=4, nbx=2, nby=2, nmin=20, nmax=60, steps=1))
+
+
+def test_noalloc_norms_3d_blocks():
+    # two 3-D blocks: the arrays carry k ghost planes (offsets over nk > 1)
+    _run(cases.periodic_box_3d(12, nb=(2, 1, 1), sizes=[[12, 8], [10], [6]], steps=1, seed=1))
 
 
 def test_noalloc_rejects_blocks_beyond_the_limit():
