@@ -11,8 +11,10 @@ RK3 step of one cell; N GPUs run N independent replicas (weak scaling).
 Precisions: value is the "fp64" path (the reference algorithm in restated
 FP64 arithmetic, within 1e-12 of the reference arithmetic per step); the
 reference-exact path and the mixed FP32/FP64 path are timed in the same run
-under "variants", with the mixed path's density error after 100 steps
-against the reference-exact path.
+under "variants"; "errors_vs_oracle" holds every precision's density error
+after 100 steps against the FP64 oracle itself (run in a spawned process
+beside the device-timed reports).  The line's last key, "summary", repeats
+the figures a reader needs in a few hundred characters.
 
 --impl reference times the CPU oracle (the C++/OpenMP restatement of the
 reference's Fortran algorithm; the Fortran build itself cannot be compiled
@@ -160,24 +162,64 @@ def fp64_ceiling(device):
                       "CUDA events around the second of two launches"}
 
 
-def cpu_baseline(seconds=15.0, n=512):
-    """The oracle's OpenMP build on a bounded sample: the same problem on a
-    512 x 512 block, steps until ~`seconds` of CPU work."""
+def host_cores():
+    """The host threads this process may use (its CPU affinity)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def time_oracle_build(path, case, cores, runs=5, steps_per_run=2, warmup=1):
+    """One oracle build on the workload: `warmup` untimed steps, then the
+    median of `runs` wall-clock runs of `steps_per_run` RK3 steps each."""
     from oracle import pyoracle
-    pyoracle.build()
-    cores = os.cpu_count() or 1
-    case = workload_case(n, steps=1)
-    o = pyoracle.Oracle(case, nthreads=cores, omp=True)
-    o.step()                                   # warm-up
-    t0 = time.perf_counter()
-    steps = 0
-    while time.perf_counter() - t0 < seconds or steps < 2:
+    o = pyoracle.Oracle(case, nthreads=cores, omp=True, lib_path=path)
+    for _ in range(warmup):
         o.step()
-        steps += 1
-    dt = time.perf_counter() - t0
-    return {"value": case.ncells * steps / dt, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-            "sample": f"{n}x{n} block of the same vortex problem, {steps} RK3 steps, {dt:.1f} s wall on "
-                      f"{cores} threads (C++/OpenMP restatement of the reference Fortran)"}
+    per = []
+    for _ in range(runs):
+        t0 = time.perf_counter()
+        for _ in range(steps_per_run):
+            o.step()
+        per.append((time.perf_counter() - t0) / steps_per_run)
+    del o
+    return case.ncells / statistics.median(per), per
+
+
+def cpu_baseline(runs=5, steps_per_run=2):
+    """The oracle on the box's host cores, on the 2048^2 workload itself, in
+    two builds made on this host: -O3 -march=native (IEEE, bit-identical to
+    the serial oracle) and -O3 -march=native -ffast-math (the reference's
+    RELEASE flags).  Each: one warm-up step, then the median of `runs` runs
+    of `steps_per_run` steps.  The value is the faster build's."""
+    import tempfile
+    from oracle import pyoracle
+    cores = host_cores()
+    case = workload_case(N_CELLS_SIDE, steps=1)
+    builds = pyoracle.build_native(tempfile.mkdtemp(prefix="mose_oracle_"))
+    res = {}
+    for name, path in builds.items():
+        v, per = time_oracle_build(path, case, cores, runs, steps_per_run)
+        res[name] = {"value": v, "ms_per_step_runs": [1e3 * x for x in per]}
+    best = max(res, key=lambda k: res[k]["value"])
+    return {"value": res[best]["value"], "unit": "cell-updates/s", "cores": cores, "kind": "port",
+            "sample": f"the {N_CELLS_SIDE}x{N_CELLS_SIDE} workload itself: 1 warm-up step, then the median of "
+                      f"{runs} runs of {steps_per_run} RK3 steps, {cores} OpenMP threads, per build; value = "
+                      f"the faster build ({best}); C++/OpenMP restatement of the reference Fortran",
+            "cpu_model": cpu_model(), "builds": {k: {"value": v["value"], "flags": (
+                "-O3 -march=native -fopenmp -ffp-contract=off" if k == "native" else
+                "-O3 -march=native -ffast-math -fomit-frame-pointer -fopenmp")} for k, v in res.items()}}
 
 
 def run_reference(args):
@@ -186,30 +228,40 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    import tempfile
     from oracle import pyoracle
-    pyoracle.build()
-    cores = os.cpu_count() or 1
+    cores = host_cores()
     case = workload_case(N_CELLS_SIDE, steps=1)
-    o = pyoracle.Oracle(case, nthreads=cores, omp=True)
-    nwarm = max(1, min(args.warmup, 3))       # CPU steps of ~0.3 s: a few warm the caches and threads
-    for _ in range(nwarm):
-        o.step()
-    # each step is one full RK3 step of the 2048^2 block; bound the count so the run stays within minutes
-    t0 = time.perf_counter()
-    steps = 0
-    budget = 90.0
-    while steps < args.steps and (time.perf_counter() - t0) < budget:
-        o.step()
-        steps += 1
-    el = time.perf_counter() - t0
-    value = case.ncells * steps / el
+    builds = pyoracle.build_native(tempfile.mkdtemp(prefix="mose_oracle_"))
+    nwarm = max(args.warmup, 3)               # the GPU arm's warm-up count
+    # each timed step is one full RK3 step of the 2048^2 block; both builds
+    # run, the faster one is the arm's value; the count is bounded so the run
+    # stays within minutes
+    budget = 60.0
+    res = {}
+    for name, path in builds.items():
+        o = pyoracle.Oracle(case, nthreads=cores, omp=True, lib_path=path)
+        for _ in range(nwarm):
+            o.step()
+        t0 = time.perf_counter()
+        steps = 0
+        while steps < args.steps and (time.perf_counter() - t0) < budget:
+            o.step()
+            steps += 1
+        el = time.perf_counter() - t0
+        res[name] = (case.ncells * steps / el, steps, el)
+        del o
+    best = max(res, key=lambda k: res[k][0])
+    value, steps, el = res[best]
     line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
             "n_gpus": world, "steps": steps, "warmup": nwarm, "ms_per_step": 1e3 * el / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(case, "fp64 (CPU oracle)"), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "cell-updates/s", "cores": cores, "kind": "port",
-                             "sample": f"{steps} of the requested {args.steps} steps of the 2048^2 workload "
-                                       f"({el:.1f} s on {cores} threads)"},
+                             "sample": f"{steps} of the requested {args.steps} steps of the 2048^2 workload after "
+                                       f"{nwarm} warm-up steps ({el:.1f} s on {cores} threads), build {best}",
+                             "cpu_model": cpu_model(),
+                             "builds": {k: v[0] for k, v in res.items()}},
             "e2e": {"value": value, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -251,23 +303,53 @@ def stage_roofline(s, steps, cells):
                                 "stage": stage_ms}
 
 
-def mixed_error(local, steps=100):
-    """Density error of the mixed precision against the reference-exact
-    path (bit-identical to the FP64 oracle) after `steps` RK3 steps of the
-    workload."""
+def _oracle_density(out_path, steps, cores, n=N_CELLS_SIDE):
+    """(Run in a spawned process.)  The FP64 oracle on the n x n workload
+    (2048^2) for `steps` RK3 steps; saves the final interior density."""
+    from mose_b200.cases import GC
+    from oracle import pyoracle
+    case = workload_case(n, steps=steps)
+    o = pyoracle.Oracle(case, nthreads=cores, omp=True)
+    for _ in range(steps):
+        o.step()
+    np.save(out_path, o.get_prim(1)[GC:-GC, GC:-GC, GC:-GC, 0])
+
+
+def start_oracle_density(steps=100, n=N_CELLS_SIDE):
+    """Starts the oracle run of _oracle_density in a fresh (spawned) process,
+    so that it overlaps the device-timed reports; returns (process, path)."""
+    import multiprocessing as mp
+    import tempfile
+    path = os.path.join(tempfile.mkdtemp(prefix="mose_oracle_"), "density.npy")
+    proc = mp.get_context("spawn").Process(target=_oracle_density, args=(path, steps, host_cores(), n))
+    proc.start()
+    return proc, path
+
+
+def errors_vs_oracle(local, proc, path, steps=100):
+    """Density error of every precision against the FP64 oracle itself after
+    `steps` RK3 steps of the 2048^2 workload from the same initial state: L2
+    (relative, over all cells) and normwise L-infinity; for the
+    reference-exact precision also whether it is bit-identical."""
     from mose_b200 import Solver
     from mose_b200.cases import GC
+    proc.join()
+    if proc.exitcode != 0 or not os.path.exists(path):
+        return {"error": f"oracle run failed (exit code {proc.exitcode})"}
+    r = np.load(path)
     case = workload_case(N_CELLS_SIDE, steps=steps)
-    out = {}
-    for name in ("exact", "mixed"):
+    out = {"steps": steps, "against": "FP64 oracle (C++ restatement of the reference, OpenMP build)"}
+    for name in PRECISIONS:
         s = Solver(case, precision=precision_code(name), device=local)
         s.advance(steps)
-        out[name] = s.download_prim(1)[GC:-GC, GC:-GC, GC:-GC, 0].copy()
+        g = s.download_prim(1)[GC:-GC, GC:-GC, GC:-GC, 0]
         s.close()
-    r, g = out["exact"], out["mixed"]
-    return {"density_l2": float(np.sqrt(((g - r) ** 2).sum() / (r ** 2).sum())),
-            "density_linf": float(np.abs(g - r).max() / np.abs(r).max()), "steps": steps,
-            "against": "reference-exact GPU path (bit-identical to the FP64 oracle)"}
+        e = {"density_l2": float(np.sqrt(((g - r) ** 2).sum() / (r ** 2).sum())),
+             "density_linf": float(np.abs(g - r).max() / np.abs(r).max())}
+        if name == "exact":
+            e["bitwise"] = bool(np.array_equal(g, r))
+        out[name] = e
+    return out
 
 
 def warm_up(s, stream, seconds=0.5):
@@ -382,6 +464,22 @@ def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0):
     s.upload_prim(1, to_ref_layout(P0))
     s.set_inflow_mach(mach)
     _, plain_ms = timed(lambda: s.advance(nsteps))
+    # the same forward in the fp64 precision (the fastest FP64 forward): the
+    # cost ratios are quoted against it as well
+    f = Solver(case, precision=precision_code("fp64"), device=local)
+    f.set_inflow_mach(mach)
+    f.advance(nsteps)                                     # warm-up (graph capture)
+    f.upload_prim(1, to_ref_layout(P0))
+    f.set_time(0.0, 0)
+    fst = torch.cuda.ExternalStream(f.stream_handle, device=torch.device("cuda", local))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(fst)
+    f.advance(nsteps)
+    e1.record(fst)
+    torch.cuda.synchronize()
+    fp64_ms = e0.elapsed_time(e1)
+    f.close()
     s.upload_prim(1, to_ref_layout(P0))
     s.set_time(0.0, 0)
     J0, fwd_ms = timed(lambda: s.adjoint_forward(nsteps, K, 1, 3))
@@ -405,8 +503,13 @@ def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0):
     s.close()
     return {"adjoint_curvilinear_512^2_200_steps": {
         "cells": case.ncells, "steps": nsteps, "checkpoint_interval": K, "J": float(Jt.detach()), "J_direct": J0,
-        "forward_ms": fwd_ms, "plain_forward_ms": plain_ms, "backward_ms": bwd_ms,
-        "adjoint_over_forward": bwd_ms / plain_ms,
+        "forward_ms": fwd_ms, "plain_forward_ms": plain_ms, "fp64_forward_ms": fp64_ms, "backward_ms": bwd_ms,
+        "backward_over_exact_forward": bwd_ms / plain_ms, "backward_over_fp64_forward": bwd_ms / fp64_ms,
+        "gradient_over_exact_forward": (fwd_ms + bwd_ms) / plain_ms,
+        "gradient_over_fp64_forward": (fwd_ms + bwd_ms) / fp64_ms,
+        "ratios": "backward = the reverse sweep (segment recompute + adjoint steps); gradient = the "
+                  "checkpointing forward + the backward; each over a plain graph-replayed forward of the "
+                  "same 200 steps in the reference-exact or the fp64 precision",
         "gradient_vs_fd": {"directions": ndir, "kind": "seeded cell-wise N(0,1) on rho, u, v, p", "step": h,
                            "max_rel_err": max(errs), "median_rel_err": float(np.median(errs)),
                            "below_1e-5": int(sum(e < 1e-5 for e in errs)),
@@ -513,6 +616,8 @@ def run_gpu(args):
     e2e = world * cells * n_e2e / e2e_s
     nbytes = int(np.prod(shape[1:])) * 8      # 2-D: the k = 1 plane of the reference array crosses the bus
     s.close()
+    # --- the oracle's 100 steps run beside the device-timed reports ----------
+    oracle_job = start_oracle_density() if (rank == 0 and world == 1 and not args.no_extra_configs) else None
     # --- the other precisions on the same workload ---------------------------
     variants = {}
     for name in PRECISIONS:
@@ -530,10 +635,9 @@ def run_gpu(args):
                           "autotune": vtuned}
         v.close()
     # the reports beside the headline run once, on rank 0 of a one-GPU run
-    err = mixed_error(local) if rank == 0 else None
-    extra = extra_configs(local) if (rank == 0 and world == 1 and not args.no_extra_configs) else None
+    extra = extra_configs(local) if oracle_job is not None else None
+    errs = errors_vs_oracle(local, *oracle_job) if oracle_job is not None else None
     if rank == 0:
-        variants.setdefault("mixed", {})["error_vs_fp64_oracle"] = err
         line = {"metric": "cell-updates/s MUSCL+HLLC RK3 FP64", "value": value, "unit": "cell-updates/s",
                 "n_gpus": world, "steps": args.steps, "warmup": max(args.warmup, 3),
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -553,6 +657,8 @@ def run_gpu(args):
                 "step_bytes_per_cell": BYTES_PER_CELL_STEP,
                 "hbm_frac_whole_step": BYTES_PER_CELL_STEP * cells * args.steps / (ms / 1e3 / world) / 1e9 / peak,
                 "variants": variants}
+        if errs is not None:
+            line["errors_vs_oracle"] = errs
         if extra is not None:
             line["configs"] = extra
         if world == 1:
@@ -575,11 +681,48 @@ def run_gpu(args):
                                                 / (ceil["dfma_tflops"] / 2.0))
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline()
+        line["summary"] = summary(line, args.precision)
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def _g(x, digits=4):
+    """x rounded to `digits` significant digits (compact report numbers)."""
+    return float(f"{x:.{digits - 1}e}") if isinstance(x, (int, float)) and x == x and x != 0 else x
+
+
+def summary(line, headline):
+    """The figures a reader needs, in a few hundred characters: the JSON line's
+    last key, so that a kept tail of the output holds them."""
+    out = {headline: _g(line["value"])}
+    for name, v in line.get("variants", {}).items():
+        out[name] = _g(v["value"])
+    out["hbm_frac"] = _g(line["roofline"]["frac"], 3)
+    if "fp64_roofline" in line:
+        out["fp64_pipe_frac"] = _g(line["fp64_roofline"]["frac"], 3)
+    e = line.get("errors_vs_oracle") or {}
+    for name in PRECISIONS:
+        if isinstance(e.get(name), dict):
+            out[f"{name}_rho_l2_vs_oracle"] = _g(e[name]["density_l2"], 2)
+    if isinstance(e.get("exact"), dict):
+        out["exact_bitwise_vs_oracle"] = e["exact"]["bitwise"]
+    for cname, c in (line.get("configs") or {}).items():
+        short = cname.split("_")[0]
+        if "adjoint" in cname:
+            out["adjoint"] = {k: _g(c[k], 3) for k in ("backward_over_fp64_forward", "gradient_over_fp64_forward",
+                                                        "backward_over_exact_forward") if k in c}
+            g = c.get("gradient_vs_fd", {})
+            out["adjoint"]["fd_max_rel_err"] = _g(g.get("max_rel_err", float("nan")), 2)
+            out["adjoint"]["fd_below_1e-5"] = g.get("below_1e-5")
+            continue
+        out[short] = {p: _g(c[p]["value"], 3) for p in PRECISIONS if isinstance(c.get(p), dict)}
+    if "cpu_baseline" in line:
+        out["cpu"] = {k: _g(v["value"], 3) for k, v in line["cpu_baseline"].get("builds", {}).items()}
+    out["e2e"] = _g(line["e2e"]["value"], 3)
+    return out
 
 
 def main():

@@ -173,7 +173,9 @@ int mose_gpu_copy_state(mose_gpu_ctx* ctx);
 /* Fill_Ghost_Cell (numerics/space/Lib_Ghost.f90:11-137). */
 int mose_gpu_fill_ghosts(mose_gpu_ctx* ctx);
 /* Fluxes (numerics/fluxes/Mod_Fluxes.f90:10-209) followed by BC_Fluxes
- * (numerics/fluxes/bc/Mod_BC_Fluxes.f90:10-218): R on the device. */
+ * (numerics/fluxes/bc/Mod_BC_Fluxes.f90:10-218): R on the device.  In the
+ * reference-exact arithmetic, or in the fp64 precision's when the context
+ * computes in it (the mixed precision's phases run the exact arithmetic). */
 int mose_gpu_residual(mose_gpu_ctx* ctx);
 /* RK_Newstate => Newstate_Conservative (numerics/time/explicit/Lib_Newstate.f90:13-160). */
 int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk);

@@ -1184,15 +1184,20 @@ int mose_gpu_residual(mose_gpu_ctx* ctx) {
   MOSE_NVTX_RANGE("mose_gpu_residual");
   int rc = require_ready(ctx);
   if (rc) return rc;
-  // the phase-by-phase path always runs the reference-exact arithmetic; 402
-  // tables are read at the caller's domain time (mose_gpu_set_time)
+  // the residual phase runs the reference-exact arithmetic, or the fp64
+  // precision's restated arithmetic when the context computes in it (the
+  // same face physics as its fused stages); 402 tables are read at the
+  // caller's domain time (mose_gpu_set_time)
   if (ctx->nser) {
     CU(cudaMemcpyAsync(ctx->scal.p + 1, &ctx->h_time, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     ctx->launches += enqueue_series(ctx);
   }
   StageArgs a = stage_args(ctx, ctx->cur, ctx->po, -1, 1);
-  // the residual-only kernels read the metric arrays
-  const int nk = launch_stage(ctx, a, 1, MOSE_PRECISION_FP64_EXACT, false);
+  // the exact residual-only kernels read the metric arrays; the fp64 ones
+  // take the constant metrics of uniform grids like the fused stages
+  const bool fp64 = ctx->cfg.precision == MOSE_PRECISION_FP64;
+  const int nk = launch_stage(ctx, a, 1, fp64 ? MOSE_PRECISION_FP64 : MOSE_PRECISION_FP64_EXACT,
+                              fp64 && ctx->uniform);
   if (!nk) return fail(ctx, MOSE_ERR_UNSUPPORTED, "no kernel for this solver / limiter");
   ctx->launches += nk;
   return check_launch(ctx, "residual");

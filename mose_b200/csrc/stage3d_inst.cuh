@@ -40,8 +40,15 @@ static void launch3d(const StageArgs& a, int nsm, cudaStream_t s) {
 template <int PREC, int RIE, int LIM>
 static bool stage3d_dispatch_uni(const StageArgs& a, int nsm, int mode, bool uni, cudaStream_t s) {
   if (mode == 1) {
+    // residual only: the reference-exact policy with metric arrays, and the
+    // fp64 policy in both metric modes (its residual is checked against the
+    // oracle's per evaluation)
     if constexpr (PREC == 0) {
       launch3d<PREC, RIE, LIM, false, 1>(a, nsm, s);
+      return true;
+    } else if constexpr (PREC == 1) {
+      if (uni) launch3d<PREC, RIE, LIM, true, 1>(a, nsm, s);
+      else launch3d<PREC, RIE, LIM, false, 1>(a, nsm, s);
       return true;
     }
     return false;

@@ -2,8 +2,8 @@
 // policy, limiter, metric mode and kernel mode.  Each translation unit
 // stage_<precision>_r<solver>.cu instantiates one (precision, Riemann solver)
 // pair.  The residual-only mode (the phase-by-phase C-ABI path) exists for the
-// reference-exact policy with metric arrays; the fused mode has
-// constant-metric variants for uniform grids.
+// reference-exact policy with metric arrays and for the fp64 policy; the
+// fused mode has constant-metric variants for uniform grids.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -47,8 +47,15 @@ static void launch_persistent(const StageArgs& a, int nsm, cudaStream_t s) {
 template <int PREC, int RIE, int LIM>
 static bool stage2d_dispatch_uni(const StageArgs& a, int nsm, int mode, bool uni, cudaStream_t s) {
   if (mode == 1) {
+    // residual only: the reference-exact policy with metric arrays, and the
+    // fp64 policy in both metric modes (its residual is checked against the
+    // oracle's per evaluation)
     if constexpr (PREC == 0) {
       launch_persistent<PREC, RIE, LIM, false, 1>(a, nsm, s);
+      return true;
+    } else if constexpr (PREC == 1) {
+      if (uni) launch_persistent<PREC, RIE, LIM, true, 1>(a, nsm, s);
+      else launch_persistent<PREC, RIE, LIM, false, 1>(a, nsm, s);
       return true;
     }
     return false;

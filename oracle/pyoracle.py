@@ -32,11 +32,18 @@ def build() -> None:
     subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
 
 
-def load(omp: bool = False) -> C.CDLL:
-    name = "liboracle_omp.so" if omp else "liboracle.so"
+def build_native(dest: str | os.PathLike) -> dict:
+    """Builds the host-tuned timing builds (-march=native, IEEE and
+    -ffast-math) into dest on the machine that runs them; returns their paths."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_DIR={dest}"], check=True)
+    return {"native": Path(dest) / "liboracle_native.so", "fastmath": Path(dest) / "liboracle_fastmath.so"}
+
+
+def load(omp: bool = False, path: str | os.PathLike | None = None) -> C.CDLL:
+    name = str(path) if path is not None else ("liboracle_omp.so" if omp else "liboracle.so")
     if name in _LIBS:
         return _LIBS[name]
-    path = HERE / name
+    path = Path(path) if path is not None else HERE / name
     if not path.exists():
         build()
     lib = C.CDLL(str(path))
@@ -90,8 +97,8 @@ RIEMANN = {"HLLC": 0, "AUSM+": 1, "SLAU": 2, "SLAU2": 3, "HLLE": 4, "HLLEM": 5, 
 class Oracle:
     """One oracle domain built from a mose_b200.cases.Case (or the same fields)."""
 
-    def __init__(self, case, nthreads: int = 1, omp: bool = False, ndir: int = 0):
-        self.lib = load(omp)
+    def __init__(self, case, nthreads: int = 1, omp: bool = False, ndir: int = 0, lib_path=None):
+        self.lib = load(omp, lib_path)
         cfg = orc_config(n_rk=case.n_rk, cfl=case.cfl, time_accurate=int(case.time_accurate),
                          limiter=LIMITERS[case.limiter], riemann=RIEMANN[case.riemann],
                          integration={"cons": 0, "prim": 1}[getattr(case, "integration", "cons")],

@@ -1,0 +1,176 @@
+"""GPU parity at the benchmark configurations' own sizes, against the oracle's
+OpenMP build (bit-identical to its serial build) on all host cores.
+
+* 2-D vortex, one periodic 2048 x 2048 block (van Albada + HLLC): one
+  residual evaluation (Fill_Ghost_Cell + Fluxes + BC_Fluxes) and one RK3 step,
+  bit for bit in the reference-exact precision and within the normwise
+  relative L-infinity bar of 1e-12 in the fp64 precision, on the residual, the
+  state and the state change.
+* Four-quadrant problem, the seed-0 domain of 64 uneven blocks (17.6 M cells,
+  AUSM+ + minmod): the same residual and step checks.
+* 3-D periodic box of 8 blocks of 128^3 (van Leer + HLLC): one RK3 step, bit
+  for bit in the exact precision and within 1e-12 in fp64.
+* Curvilinear channel, 512 x 512 with the 405 inflow, 406 outflow and 300
+  walls (van Albada + HLLC), from its seeded perturbed state: the 200-step
+  reference-exact forward the adjoint differentiates, final state and the
+  wall-pressure objective J.  The 406 outflow calls pow, whose glibc and CUDA
+  results may differ by an ulp, so this case is held to the 1e-12 normwise
+  bar (J to 1e-12 relative) instead of bit equality.
+
+The normwise bar is max over cells |gpu - oracle| / max over cells |oracle|,
+per variable (rho, u, v, [w,] p), worst variable.  These tests need host
+memory for the oracle's reference-layout arrays (ghosts in every direction)
+and skip with the figure when the host lacks it."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from mose_b200 import cases
+from mose_b200.cases import GC
+
+pytestmark = pytest.mark.gpu
+
+THREADS = os.cpu_count() or 1
+TOL = 1e-12
+
+
+def need_host_memory(gib):
+    import psutil
+    avail = psutil.virtual_memory().available / 2 ** 30
+    if avail < gib:
+        pytest.skip(f"the oracle needs about {gib} GiB of host memory here, {avail:.0f} GiB available")
+
+
+def interior(P):
+    return P[GC:-GC, GC:-GC, GC:-GC]
+
+
+def vars_of(case):
+    return (0, 1, 2, 3, 4) if any(nd.shape[0] > 2 for nd in case.nodes) else (0, 1, 2, 4)
+
+
+def oracle(mod, case):
+    return mod.Oracle(case, nthreads=THREADS, omp=True)
+
+
+def normwise(get_a, get_b, nblk, vars_, base=None):
+    """Worst per-variable normwise relative L-infinity of a against b over all
+    blocks (with base: of the changes a - base and b - base)."""
+    num = dict.fromkeys(vars_, 0.0)
+    den = dict.fromkeys(vars_, 0.0)
+    for b in range(1, nblk + 1):
+        x, y = interior(get_a(b)), interior(get_b(b))
+        if base is not None:
+            x = x - base[b - 1]
+            y = y - base[b - 1]
+        for v in vars_:
+            num[v] = max(num[v], float(np.abs(x[..., v] - y[..., v]).max()))
+            den[v] = max(den[v], float(np.abs(y[..., v]).max()))
+    return max(num[v] / den[v] if den[v] > 0 else num[v] for v in vars_)
+
+
+def assert_bitwise(get_a, get_b, nblk, vars_):
+    for b in range(1, nblk + 1):
+        x, y = interior(get_a(b))[..., list(vars_)], interior(get_b(b))[..., list(vars_)]
+        assert np.array_equal(x, y), f"block {b}: max |diff| {np.abs(x - y).max()}"
+
+
+def residual_checks(oracle_mod, case):
+    """One residual evaluation: exact bit for bit, fp64 within the bar."""
+    from mose_b200 import Solver, _lib
+    nb, vs = len(case.nodes), vars_of(case)
+    o = oracle(oracle_mod, case)
+    o.fill_ghost_cell()
+    o.fluxes()
+    o.bc_fluxes()
+    for prec in (_lib.PRECISION_FP64_EXACT, _lib.PRECISION_FP64):
+        s = Solver(case, precision=prec)
+        s.fill_ghost_cell()
+        s.fluxes_and_bc_fluxes()
+        if prec == _lib.PRECISION_FP64_EXACT:
+            assert_bitwise(s.download_residual, o.get_residual, nb, vs)
+        else:
+            err = normwise(s.download_residual, o.get_residual, nb, vs)
+            assert err <= TOL, f"fp64 residual: normwise relative error {err:.3e}"
+        s.close()
+    del o
+
+
+def step_checks(oracle_mod, case, precisions=("exact", "fp64")):
+    """One RK3 step from identical inputs: exact bit for bit (dt too), fp64
+    within the bar on the state and on the state change."""
+    from mose_b200 import Solver, _lib
+    nb, vs = len(case.nodes), vars_of(case)
+    o = oracle(oracle_mod, case)
+    base = [interior(o.get_prim(b)).copy() for b in range(1, nb + 1)]
+    dto, to = o.step()
+    codes = {"exact": _lib.PRECISION_FP64_EXACT, "fp64": _lib.PRECISION_FP64}
+    for name in precisions:
+        s = Solver(case, precision=codes[name])
+        dtg, tg = s.explicit_step()
+        assert dtg == dto and tg == to       # the first step's dt pass is the reference arithmetic
+        if name == "exact":
+            assert_bitwise(s.download_prim, o.get_prim, nb, vs)
+        else:
+            err = normwise(s.download_prim, o.get_prim, nb, vs)
+            derr = normwise(s.download_prim, o.get_prim, nb, vs, base=base)
+            assert err <= TOL and derr <= TOL, f"fp64 step: state {err:.3e}, state change {derr:.3e}"
+        s.close()
+    del o
+
+
+def test_vortex_2048_residual_exact_and_fp64(oracle_mod):
+    need_host_memory(16)
+    residual_checks(oracle_mod, cases.isentropic_vortex(2048, steps=1, limiter="vanalbada", riemann="HLLC",
+                                                        cfl=0.8))
+
+
+def test_vortex_2048_step_exact_and_fp64(oracle_mod):
+    need_host_memory(16)
+    step_checks(oracle_mod, cases.isentropic_vortex(2048, steps=1, limiter="vanalbada", riemann="HLLC", cfl=0.8))
+
+
+def test_quadrant_64_blocks_seed0_residual_and_step(oracle_mod):
+    need_host_memory(64)
+    case = cases.four_quadrant(seed=0, steps=1)
+    assert len(case.nodes) == 64 and case.ncells > 10_000_000
+    residual_checks(oracle_mod, case)
+    step_checks(oracle_mod, case)
+
+
+def test_box3d_8x128_step_exact_and_fp64(oracle_mod):
+    need_host_memory(40)
+    case = cases.periodic_box_3d(128, steps=1, seed=0)
+    assert len(case.nodes) == 8 and case.ncells == 256 ** 3
+    step_checks(oracle_mod, case)
+
+
+def test_channel_512_200_steps_exact_forward(oracle_mod):
+    """The adjoint configuration's forward: 200 RK3 steps of the 512^2
+    curvilinear channel in the reference-exact precision, graph-replayed on
+    the GPU, against 200 oracle steps; then the checkpointing forward's J
+    against the oracle's wall-pressure integral."""
+    from mose_b200 import Solver
+    from mose_b200.cases import to_ref_layout
+    need_host_memory(8)
+    nsteps = 200
+    case = cases.perturbed_channel(512, steps=nsteps, seed=0)
+    o = oracle(oracle_mod, case)
+    for _ in range(nsteps):
+        o.step()
+    s = Solver(case)
+    dtg, tg = s.advance(nsteps)
+    assert tg == o.time
+    err = normwise(s.download_prim, o.get_prim, 1, (0, 1, 2, 4))
+    assert err <= TOL, f"state after {nsteps} steps: {err:.3e}"
+    # J = sum over the bottom-wall (face 3) cells of p * A, in any summation order
+    _, A = o.get_faces(1, 2)                         # j-faces: A[k, j, i], j = 0 is face 3
+    p = interior(o.get_prim(1))[0, 0, :, 4]
+    J_oracle = math.fsum(float(x) for x in p * A[0, 0, :])
+    s.upload_prim(1, to_ref_layout(case.prim[0]))
+    s.set_time(0.0, 0)
+    J_gpu = s.adjoint_forward(nsteps, 14, 1, 3)
+    assert abs(J_gpu - J_oracle) <= TOL * abs(J_oracle), (J_gpu, J_oracle)
+    s.close()
