@@ -215,6 +215,22 @@ def test_fp64_precision_within_1e12_per_step(oracle_mod, name):
     # the state change of the step, which the residual drives, to the same bar
     derr = _per_var_rel(s, o, len(case.nodes), base=base)
     assert derr <= 1e-12, derr
+    # one residual evaluation (the residual phase runs the fp64 arithmetic)
+    o2 = oracle_mod.Oracle(case)
+    s2 = solver(case, precision=_lib.PRECISION_FP64)
+    o2.fill_ghost_cell()
+    o2.fluxes()
+    o2.bc_fluxes()
+    s2.fill_ghost_cell()
+    s2.fluxes_and_bc_fluxes()
+    num, den = np.zeros(4), np.zeros(4)
+    for b in range(1, len(case.nodes) + 1):
+        rg = interior(s2.download_residual(b))[..., [0, 1, 2, 4]]
+        ro = interior(o2.get_residual(b))[..., [0, 1, 2, 4]]
+        num = np.maximum(num, np.abs(rg - ro).reshape(-1, 4).max(axis=0))
+        den = np.maximum(den, np.abs(ro).reshape(-1, 4).max(axis=0))
+    rerr = float((num / np.where(den > 0, den, 1.0)).max())
+    assert rerr <= 1e-12, rerr
 
 
 @pytest.mark.parametrize("name", ["vortex", "quadrant", "sod"])
