@@ -24,7 +24,8 @@
  *           alpha, beta, rel_fac ; 406: p_back, rel_fac ; 407: T0, p0,
  *           p_back, alpha, beta, rel_fac (g: mass flux per unit area; the
  *           largest double as alpha or beta is the token 'normal', which
- *           407 does not take; on 2-D domains beta is 0 or 'normal')
+ *           407 does not take; on 2-D domains beta is 0 or 'normal') ;
+ *           301: qw ; 302: Tw (walls, see mose_gpu_set_viscous)
  *
  * State is device resident between calls: host P is stale until
  * mose_gpu_download_prim().  A context is not thread safe and owns one
@@ -270,6 +271,20 @@ int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on);
  * mose_gpu_setup.  2-D, exact precision: the stage's residual-only kernel,
  * then the smoothing kernels, then the update. */
 int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta);
+
+/* equations = navier-stokes (Global_m model): model 1 adds the laminar
+ * diffusive fluxes of Lib_Diffusive.f90 (Diffusive_Flux, Compute_Diffusive_Flux,
+ * called from Mod_Fluxes.f90:101-206 when model > 0), their boundary terms
+ * (BC_Connection_Visc for 101 / 201, BC_Symmetry_Visc for 300, BC_Wall_Heat
+ * for 301 with qw as the record's first datum, BC_Wall_Temperature for 302
+ * with Tw) and the VNN time-step limit (Mod_dt.f90:87-103); model 0 (the
+ * default) is the Euler path.  mu and kappa are the laminar viscosity and
+ * conductivity (one species, constant-property transport tables, for which
+ * FLINT's table interpolation and Wilke mixing return the constants), vnn the
+ * von Neumann number.  Call before mose_gpu_setup.  2-D domains, exact
+ * precision, conservative integration, no IRS or shock detector; without
+ * model 1, 301 and 302 faces are symmetry walls, as in the reference. */
+int mose_gpu_set_viscous(mose_gpu_ctx* ctx, int32_t model, double mu, double kappa, double vnn);
 
 /* riemann-options-Minf (Register_Numerics.f90:72), the reference Mach number
  * of AUSM+-up and AUSM+-up2; call before mose_gpu_setup.  Setup rejects

@@ -73,6 +73,7 @@ SIGNATURES = {
     "mose_gpu_set_inflow_mach": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_riemann_minf": (C.c_int, [_D, C.c_double]),
     "mose_gpu_set_irs_beta": (C.c_int, [_D, C.c_double]),
+    "mose_gpu_set_viscous": (C.c_int, [_D, C.c_int32, C.c_double, C.c_double, C.c_double]),
     "mose_gpu_set_sd_limiter": (C.c_int, [_D, C.c_int32]),
     "mose_gpu_add_series": (C.c_int, [_D, _dp, _dp, C.c_int32, C.c_int32, _ip]),
     "mose_gpu_set_tiling": (C.c_int, [_D, _ip]),

@@ -28,6 +28,7 @@ COMMON = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--exp
 # translation unit -> extra flags
 UNITS = {
     "kernels_exact.cu": ["--fmad=false"],
+    "viscous2d.cu": ["--fmad=false"],
     **{f"stage_exact_r{r}.cu": ["--fmad=false"] for r in range(5)},
     **{f"stage_fp64_r{r}.cu": [] for r in range(5)},
     **{f"stage_mixed_r{r}.cu": [] for r in range(5)},

@@ -49,6 +49,10 @@ class Case:
     sd_limiter: bool = False   # space-reconstruction MUSCL-SD (shock-detector scaled slopes)
     ramp_iter: int = 0         # cfl-rise-threshold: CFL ramped over the first iterations
     integration: str = "cons"  # integration-variables: 'cons' or 'prim' (primitive RK update)
+    model: int = 0             # 0: Euler, 1: laminar Navier-Stokes
+    mu: float = 0.0            # laminar viscosity (constant transport properties)
+    kappa: float = 0.0         # laminar conductivity
+    vnn: float = 0.5           # von Neumann number of the viscous time-step limit
     gamma: float = 1.4
     rgas: float = 1.0
     steps: int = 1
@@ -414,3 +418,65 @@ def channel_3d(n: int = 16, steps: int = 10, mach: float = 0.8, amp: float = 0.0
     return Case("channel3d", [np.ascontiguousarray(nodes)], rec, data, [prim], n_rk=3, cfl=cfl,
                 time_accurate=True, limiter=limiter, riemann=riemann, gamma=gamma, rgas=1.0, steps=steps,
                 extra={"mach": mach})
+
+
+def shear_layer(n: int = 64, nbx: int = 1, nby: int = 1, steps: int = 10, mu: float = 0.01, prandtl: float = 0.72,
+                u0: float = 0.5, amp: float = 0.02, seed: int = 0, tw: float | None = None, top: str = "adiabatic",
+                warp: float = 0.0, limiter="vanleer", riemann="HLLC", cfl=0.5, vnn=0.5, gamma=1.4) -> Case:
+    """2-D laminar Navier-Stokes channel on [0, 2] x [0, 1]: a shear layer
+    u = u0 sin(pi y) between walls, periodic in x, decaying by viscosity;
+    rho = 1, p = 1/gamma (sound speed 1) plus seeded cell-wise perturbations
+    of relative amplitude `amp` on rho, u, v and p so every gradient term is
+    exercised.  Bottom wall (face 3 of the bottom blocks): 302 at temperature
+    `tw` (default: the free-stream temperature); top: 301 adiabatic (qw = 0),
+    or 300 symmetry with top='symmetry'.  nbx x nby blocks of 2n x n cells
+    (101 interfaces, the periodic wrap in x is 201); constant transport
+    properties mu and kappa = mu cp / Pr.  warp > 0 moves the nodes to
+    y = eta + warp sin(pi xi) sin(pi eta) (walls stay flat, the wrap stays
+    periodic), so the metric tensor has off-diagonal terms."""
+    rng = np.random.default_rng(seed)
+    Nx, Ny = 2 * n * nbx, n * nby
+    rgas = 1.0
+    p_inf = 1.0 / gamma
+    T_inf = p_inf / (1.0 * rgas)
+    tw = T_inf if tw is None else tw
+    cp = gamma * rgas / (gamma - 1.0)
+    nodes, prims, dims = [], [], []
+    for by in range(nby):
+        for bx in range(nbx):
+            ni, nj = 2 * n, n
+            nd = cartesian_nodes(ni, nj, 1, (0.0, 0.0, 0.0), (2.0, 1.0, 1.0), offs=(ni * bx, nj * by, 0),
+                                 ntot=(Nx, Ny, 1))
+            if warp:
+                nd[..., 1] = nd[..., 1] + warp * np.sin(np.pi * nd[..., 0]) * np.sin(np.pi * nd[..., 1])
+            c = cell_centres(nd)
+            p = np.zeros((1, nj, ni, NPRIM))
+            shape = p.shape[:-1]
+            p[..., 0] = 1.0 * (1 + amp * rng.standard_normal(shape))
+            p[..., 1] = u0 * np.sin(np.pi * c[..., 1]) * (1 + amp * rng.standard_normal(shape))
+            p[..., 2] = amp * u0 * rng.standard_normal(shape)
+            p[..., 4] = p_inf * (1 + amp * rng.standard_normal(shape))
+            nodes.append(nd)
+            prims.append(p)
+            dims.append((ni, nj, 1))
+
+    def spec(b, f):
+        bx, by = (b - 1) % nbx, (b - 1) // nbx
+        if f >= 5:
+            return ("bc", 0, [0.0] * 6)
+        if f in (1, 2):   # x: neighbours, the wrap is periodic (201)
+            nbx_ = (bx - 1) % nbx if f == 1 else (bx + 1) % nbx
+            wrap = (f == 1 and bx == 0) or (f == 2 and bx == nbx - 1)
+            return ("conn", 201 if wrap else 101, by * nbx + nbx_ + 1, 2 if f == 1 else 1)
+        if f == 3 and by > 0:
+            return ("conn", 101, (by - 1) * nbx + bx + 1, 4)
+        if f == 4 and by < nby - 1:
+            return ("conn", 101, (by + 1) * nbx + bx + 1, 3)
+        if f == 3:
+            return ("bc", 302, [tw, 0.0, 0.0, 0.0, 0.0, 0.0])
+        return ("bc", 300, [0.0] * 6) if top == "symmetry" else ("bc", 301, [0.0] * 6)
+
+    rec, data = build_bcs(dims, spec)
+    return Case("shear2d", nodes, rec, data, prims, n_rk=3, cfl=cfl, time_accurate=True, limiter=limiter,
+                riemann=riemann, gamma=gamma, rgas=rgas, steps=steps, model=1, mu=mu, kappa=mu * cp / prandtl,
+                vnn=vnn, extra={"u0": u0, "tw": tw})

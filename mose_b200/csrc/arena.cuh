@@ -12,6 +12,10 @@ struct MetricArgs {
   const double* face;   // 12 planes per block: for dir d: nx, ny, nz, A of the low face of each cell
   const double* vol;    // 1 plane
   const double* vers;   // 9 planes: versor of direction d, component q at plane 3 d + q
+  // Navier-Stokes only (null otherwise): 4 planes of the 2-D metric tensor
+  // M(r, s) = d xi_r / d x_s, r, s = 1, 2, at plane (r - 1) + 2 (s - 1); held
+  // for the interior cells and the first ghost layer
+  const double* Mt;
 };
 
 struct StageArgs {
@@ -46,6 +50,9 @@ struct StageArgs {
   int nitems3[3];
   // persistent 2-D grid: at most this many CTAs per SM (0: the occupancy limit)
   int grid_cap;
+  // Navier-Stokes connection faces: per 101 / 201 face cell the source stencil
+  // of its viscous flux (VConn), indexed by the boundary word's parameter
+  const int* vconn;
 };
 
 }  // namespace mose

@@ -38,6 +38,8 @@ enum BcCode : int {
   BC_MFLUX_T0 = 7,  // (403) inlet, total temperature and mass flux
   BC_MFLUX_T = 8,   // (404) inlet, static temperature and mass flux
   BC_FARFIELD = 9,  // (407) ambient: total conditions in, back pressure out
+  BC_WALL_Q = 10,   // (301) wall with prescribed heat flux (BcParam::p = qw)
+  BC_WALL_T = 11,   // (302) wall at prescribed temperature (BcParam::T = Tw)
 };
 
 // Error word written by kernels (first offender wins).
@@ -63,6 +65,18 @@ struct Gas {
   // integration-variables = prim: the exact update advances the primitives
   // (Newstate_Primitive) instead of the conservatives
   int prim;
+  // Navier-Stokes (model = 1, laminar): constant transport properties mu and
+  // kappa (one species, constant-property tables) and the von Neumann number
+  // of the viscous time-step limit
+  int model;
+  double mu, kappa, vnn;
+};
+
+// Source stencil of a viscous connection face cell (2-D, 0-based cells): the
+// source block bs, the source cell (is, js) on its face fs, and the
+// orientation d11 of the tangential direction (Fill_BC_Ghost_Connection).
+struct VConn {
+  int bs, is, js, fs, d11;
 };
 
 // Per-block descriptor (device resident).

@@ -43,6 +43,14 @@ void launch_irs_update(const BlockDesc* dblk, int nblk, long long maxcell, const
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
                      cudaStream_t s);
+// The same update from Pin into Pout, dt from *dtg when given, else dtl.
+void launch_rk_stage_to(const BlockDesc* dblk, int nblk, long long maxcell, const double* Pin, const double* PO,
+                        const double* R, MetricArgs m, const double* dtl, const double* dtg, double* Pout, Gas g,
+                        double c, int nd, bool uniform, DevError* err, cudaStream_t s);
+// Navier-Stokes residual of 2-D blocks (viscous2d.cu): a.Pc with filled
+// ghosts -> a.R, every convective, diffusive and boundary term in the
+// reference's order.  False for an unknown limiter.
+bool launch_visc_residual2d(const StageArgs& a, int nblk, long long maxcell, int lim, cudaStream_t s);
 // Discrete adjoint (2-D, HLLC; adjoint.cu).
 void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* Ps, const double* Pprev,
              const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc, double* lam_n, double c,

@@ -16,7 +16,7 @@ namespace mose {
 // ---------------------------------------------------------------------------
 // Interior cells: Compute_Metric_Tensor -> dl, vol, CFL versors.
 __global__ void k_cell_metrics(const BlockDesc* blk, int b, NodeView nv, double* dl, double* vol,
-                               double* vers, int nd, int ndir, DevError* err) {
+                               double* vers, double* Mt, int nd, int ndir, DevError* err) {
   const BlockDesc& d = blk[b];
   long long n = (long long)d.ni * d.nj * d.nk;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
@@ -31,6 +31,10 @@ __global__ void k_cell_metrics(const BlockDesc* blk, int b, NodeView nv, double*
     long long vs = d.vstride, mb = d.mbase;
     for (int h = 0; h < 3; ++h) dl[3 * mb + h * vs + o] = l[h];
     vol[mb + o] = v;
+    // the 2-D metric tensor of the viscous fluxes: M(r,s) at plane (r-1) + 2(s-1)
+    if (Mt)
+      for (int r = 0; r < 2; ++r)
+        for (int c = 0; c < 2; ++c) Mt[4 * mb + (r + 2 * c) * vs + o] = M[r + 3 * c];
     // versor = M(d,:)/norm2(M(d,:))  (Mod_dt.f90:78-80)
     for (int dd = 0; dd < ndir; ++dd) {
       double m0 = M[dd + 0], m1 = M[dd + 3], m2 = M[dd + 6];
@@ -83,8 +87,23 @@ __device__ void store_ghost_dl(const BlockDesc* blk, double* dl, int b, int nd, 
   dl[3 * d.mbase + dir * d.vstride + o] = val;
 }
 
+// The metric tensor of the first ghost layer (viscous fluxes; Mt null otherwise).
+__device__ void store_ghost_M(const BlockDesc* blk, double* Mt, int b, int nd, int I, int J, int K, const double* M,
+                              DevError* err) {
+  if (!Mt || nd != 2) return;
+  const BlockDesc& d = blk[b];
+  const bool in = I - 1 >= -GW && I - 1 < d.ni + GW && J - 1 >= -GW && J - 1 < d.nj + GW;
+  if (!in) {
+    if (atomicCAS(&err->code, 0, 1) == 0) { err->b = b + 1; err->i = I; err->j = J; err->k = K; }
+    return;
+  }
+  const long long o = cell_off2(d, I - 1, J - 1);
+  for (int r = 0; r < 2; ++r)
+    for (int c = 0; c < 2; ++c) Mt[4 * d.mbase + (r + 2 * c) * d.vstride + o] = M[r + 3 * c];
+}
+
 __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs, int nrec,
-                                const NodeView* nodes, double* dl, int nd, int ndir, DevError* err) {
+                                const NodeView* nodes, double* dl, double* Mt, int nd, int ndir, DevError* err) {
   int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= nrec) return;
   const GhostMetricRec e = recs[q];
@@ -116,6 +135,12 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
       long long so = (nd == 3) ? cell_off3(bm, si - 1, sj - 1, sk - 1) : cell_off2(bm, si - 1, sj - 1);
       double val = dl[3 * bm.mbase + dir * bm.vstride + so];
       store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, val, err);
+      if (g == 1 && Mt && nd == 2) {
+        double Ms[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int r = 0; r < 2; ++r)
+          for (int c = 0; c < 2; ++c) Ms[r + 3 * c] = Mt[4 * bm.mbase + (r + 2 * c) * bm.vstride + so];
+        store_ghost_M(blk, Mt, e.b, nd, gi, gj, gk, Ms, err);
+      }
     }
     return;
   }
@@ -173,6 +198,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
         case 6: ok &= metric_tensor(N[1][g - 1], N[1][g], N[3][g - 1], N[3][g], N[5][g - 1], N[5][g], N[7][g - 1], N[7][g], M, l, &v); gk = Km + g; break;
       }
       store_ghost_dl(blk, dl, e.b, nd, gi, gj, gk, dir, l[dir], err);
+      if (g == 1) store_ghost_M(blk, Mt, e.b, nd, gi, gj, gk, M, err);
     }
   } else {
     // BC_Extrapolate_Metrics (delthe = 0 branches)
@@ -187,6 +213,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           for (int s = 0; s < 4; ++s) at(s, g) = v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3));
           ok &= metric_tensor(at(0, g), at(1, g), at(2, g), at(3, g), at(0, g + 1), at(1, g + 1), at(2, g + 1), at(3, g + 1), M, l, &v);
           store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir], err);
+          if (g == -1 || g == 1) store_ghost_M(blk, Mt, e.b, nd, Im + g, Jm, Km, M, err);
         }
         break;
       case 2:
@@ -198,6 +225,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           for (int s = 4; s < 8; ++s) at(s, g) = v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3));
           ok &= metric_tensor(at(4, g - 1), at(5, g - 1), at(6, g - 1), at(7, g - 1), at(4, g), at(5, g), at(6, g), at(7, g), M, l, &v);
           store_ghost_dl(blk, dl, e.b, nd, Im + g, Jm, Km, dir, l[dir], err);
+          if (g == -1 || g == 1) store_ghost_M(blk, Mt, e.b, nd, Im + g, Jm, Km, M, err);
         }
         break;
       case 3: {
@@ -212,6 +240,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3)) : v3lin2(at(s, g + 1), at(s, g + 2));
           ok &= metric_tensor(at(0, g), at(1, g), at(0, g + 1), at(1, g + 1), at(4, g), at(5, g), at(4, g + 1), at(5, g + 1), M, l, &v);
           store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir], err);
+          if (g == -1 || g == 1) store_ghost_M(blk, Mt, e.b, nd, Im, Jm + g, Km, M, err);
         }
         break;
       }
@@ -227,6 +256,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3)) : v3lin2(at(s, g - 1), at(s, g - 2));
           ok &= metric_tensor(at(2, g - 1), at(3, g - 1), at(2, g), at(3, g), at(6, g - 1), at(7, g - 1), at(6, g), at(7, g), M, l, &v);
           store_ghost_dl(blk, dl, e.b, nd, Im, Jm + g, Km, dir, l[dir], err);
+          if (g == -1 || g == 1) store_ghost_M(blk, Mt, e.b, nd, Im, Jm + g, Km, M, err);
         }
         break;
       }
@@ -242,6 +272,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g + 1), at(s, g + 2), at(s, g + 3)) : v3lin2(at(s, g + 1), at(s, g + 2));
           ok &= metric_tensor(at(0, g), at(0, g + 1), at(2, g), at(2, g + 1), at(4, g), at(4, g + 1), at(6, g), at(6, g + 1), M, l, &v);
           store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir], err);
+          if (g == -1 || g == 1) store_ghost_M(blk, Mt, e.b, nd, Im, Jm, Km + g, M, err);
         }
         break;
       }
@@ -257,6 +288,7 @@ __global__ void k_ghost_metrics(const BlockDesc* blk, const GhostMetricRec* recs
           for (int s : sl) at(s, g) = cubic ? v3lin3(at(s, g - 1), at(s, g - 2), at(s, g - 3)) : v3lin2(at(s, g - 1), at(s, g - 2));
           ok &= metric_tensor(at(1, g - 1), at(1, g), at(3, g - 1), at(3, g), at(5, g - 1), at(5, g), at(7, g - 1), at(7, g), M, l, &v);
           store_ghost_dl(blk, dl, e.b, nd, Im, Jm, Km + g, dir, l[dir], err);
+          if (g == -1 || g == 1) store_ghost_M(blk, Mt, e.b, nd, Im, Jm, Km + g, M, err);
         }
         break;
       }
@@ -412,6 +444,16 @@ __global__ void k_compute_dt(const BlockDesc* blk, int nblk, const double* P, Me
     double Q[NV];
     for (int v = 0; v < NV; ++v) Q[v] = Pb[v * vs + o];
     double dtcell = cfl_dt<NV, UNI, false>(g, Q, d, m, o, ndir, cfl);
+    if (g.model > 0) {
+      // VNN condition (Mod_dt.f90:87-103), laminar: mi = 0 + mil
+      const double mi = 0.0 + g.mu;
+      for (int dd = 0; dd < ndir; ++dd) {
+        double dlv;
+        if constexpr (UNI) dlv = d.u_dl[dd]; else dlv = m.dl[3 * mb + dd * vs + o];
+        const double dtv = (Q[0] * (dlv * dlv) * g.vnn) / mi;
+        dtcell = fmin(dtv, dtcell);
+      }
+    }
     if (ramp_iter > 0 && iter < ramp_iter) dtcell = dtcell * (double)iter / (double)ramp_iter;
     if (store_local) dtl[mb + o] = dtcell;
     local_min = fmin(local_min, dtcell);
@@ -483,9 +525,12 @@ __global__ void k_step_dt_take(unsigned long long* dtmin_bits, double* dtg, doub
 // ---------------------------------------------------------------------------
 // RK_Newstate pointwise (phase path): P <- update(P, PO, R)
 // ---------------------------------------------------------------------------
+// Pout = RK stage of Pin (in place when Pout == Pin); dt from *dtg when
+// given (time accurate), else the local dt plane.
 template <int NV, bool UNI>
-__global__ void k_rk_stage(const BlockDesc* blk, double* P, const double* PO, const double* R, MetricArgs m,
-                           const double* dtl, Gas g, double c, int nd, DevError* err) {
+__global__ void k_rk_stage(const BlockDesc* blk, const double* P, const double* PO, const double* R, MetricArgs m,
+                           const double* dtl, const double* dtg, double* Pout, Gas g, double c, int nd,
+                           DevError* err) {
   const int b = blockIdx.y;
   const BlockDesc& d = blk[b];
   long long ncell = (long long)d.ni * d.nj * d.nk;
@@ -501,10 +546,10 @@ __global__ void k_rk_stage(const BlockDesc* blk, double* P, const double* PO, co
     }
     double vol;
     if constexpr (UNI) vol = d.u_vol; else vol = m.vol[mb + o];
-    double dt = dtl[mb + o];
+    double dt = dtg ? *dtg : dtl[mb + o];
     bool ok = rk_update<NV>(g, Q, QO, Rv, vol, dt, c, false);
     if (!ok) report(err, 5, b, i, j, k);
-    for (int v = 0; v < NV; ++v) P[d.sbase + v * vs + o] = Q[v];
+    for (int v = 0; v < NV; ++v) Pout[d.sbase + v * vs + o] = Q[v];
   }
 }
 
@@ -752,7 +797,7 @@ void launch_cell_metrics(const BlockDesc* dblk, int b, long long ncell, NodeView
                          int ndir, DevError* err, cudaStream_t s) {
   k_cell_metrics<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, nv, const_cast<double*>(m.dl),
                                                        const_cast<double*>(m.vol), const_cast<double*>(m.vers),
-                                                       nd, ndir, err);
+                                                       const_cast<double*>(m.Mt), nd, ndir, err);
 }
 void launch_face_metrics(const BlockDesc* dblk, int b, long long nface, NodeView nv, MetricArgs m, int nd,
                          int dir, cudaStream_t s) {
@@ -762,7 +807,8 @@ void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, con
                           int nd, int ndir, DevError* err, cudaStream_t s) {
   if (nrec == 0) return;
   k_ghost_metrics<<<(nrec + 127) / 128, 128, 0, s>>>(dblk, (const GhostMetricRec*)recs, nrec, nodes,
-                                                     const_cast<double*>(m.dl), nd, ndir, err);
+                                                     const_cast<double*>(m.dl), const_cast<double*>(m.Mt), nd, ndir,
+                                                     err);
 }
 void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir,
                           int* flags, double* firsts, double tol, cudaStream_t s) {
@@ -812,13 +858,18 @@ void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* ti
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
                      cudaStream_t s) {
+  launch_rk_stage_to(dblk, nblk, maxcell, P, PO, R, m, dtl, nullptr, P, g, c, nd, uniform, err, s);
+}
+void launch_rk_stage_to(const BlockDesc* dblk, int nblk, long long maxcell, const double* Pin, const double* PO,
+                        const double* R, MetricArgs m, const double* dtl, const double* dtg, double* Pout, Gas g,
+                        double c, int nd, bool uniform, DevError* err, cudaStream_t s) {
   dim3 grid(grid_for(maxcell, 256, 148 * 8), nblk);
   if (nd == 3) {
-    if (uniform) k_rk_stage<5, true><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
-    else k_rk_stage<5, false><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
+    if (uniform) k_rk_stage<5, true><<<grid, 256, 0, s>>>(dblk, Pin, PO, R, m, dtl, dtg, Pout, g, c, nd, err);
+    else k_rk_stage<5, false><<<grid, 256, 0, s>>>(dblk, Pin, PO, R, m, dtl, dtg, Pout, g, c, nd, err);
   } else {
-    if (uniform) k_rk_stage<4, true><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
-    else k_rk_stage<4, false><<<grid, 256, 0, s>>>(dblk, P, PO, R, m, dtl, g, c, nd, err);
+    if (uniform) k_rk_stage<4, true><<<grid, 256, 0, s>>>(dblk, Pin, PO, R, m, dtl, dtg, Pout, g, c, nd, err);
+    else k_rk_stage<4, false><<<grid, 256, 0, s>>>(dblk, Pin, PO, R, m, dtl, dtg, Pout, g, c, nd, err);
   }
 }
 void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* R, MetricArgs m,

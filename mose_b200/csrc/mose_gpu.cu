@@ -179,6 +179,8 @@ struct mose_gpu_ctx {
   DevBuf<double> state[3];
   DevBuf<double> resid;
   DevBuf<double> dl, face, vol, vers, dtl;
+  DevBuf<double> Mt;          // Navier-Stokes: 2-D metric tensor planes (null otherwise)
+  DevBuf<int> vconn;          // Navier-Stokes: VConn stencils of the connection face cells
   DevBuf<int> bcw;
   DevBuf<BcParam> bcp;
   DevBuf<GhostRec> ghosts;
@@ -256,7 +258,7 @@ struct mose_gpu_ctx {
   DevBuf<SeriesRec> ser_recs;
   int nser = 0;
 
-  MetricArgs margs() const { return MetricArgs{dl.p, face.p, vol.p, vers.p}; }
+  MetricArgs margs() const { return MetricArgs{dl.p, face.p, vol.p, vers.p, Mt.p}; }
 };
 
 namespace {
@@ -319,6 +321,8 @@ int bc_code_of(int type) {
     case 405: return BC_SUPIN;
     case 406: return BC_OUTFLOW;
     case 407: return BC_FARFIELD;
+    case 301: return BC_WALL_Q;   // walls: the symmetry flux, plus the viscous wall flux with model = 1
+    case 302: return BC_WALL_T;
   }
   return -1;
 }
@@ -417,6 +421,9 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   ctx->gas.minf = 0.0;
   ctx->gas.sd = (cfg->riemann == MOSE_RIEMANN_HLLC_SD || cfg->riemann == MOSE_RIEMANN_HLLE_PP) ? 2 : 0;
   ctx->gas.prim = cfg->integration == MOSE_INTEGRATION_PRIM ? 1 : 0;
+  ctx->gas.model = 0;   // Euler until mose_gpu_set_viscous
+  ctx->gas.mu = ctx->gas.kappa = 0.0;
+  ctx->gas.vnn = 0.5;
   *out = ctx;
   return MOSE_OK;
 }
@@ -583,6 +590,16 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   }
   if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");
+  if (ctx->gas.model > 0) {
+    if (ctx->nd != 2 || ctx->ndir != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT ||
+        ctx->cfg.integration != MOSE_INTEGRATION_CONS || ctx->irs_beta > 0.0 || ctx->gas.sd != 0)
+      return fail(ctx, MOSE_ERR_UNSUPPORTED,
+                  "Navier-Stokes runs on 2-D domains in the exact precision, conservative integration, without "
+                  "implicit residual smoothing or the shock detector");
+    for (int b = 0; b < nb; ++b)
+      if (ctx->hblk[b].nj < 3 || ctx->hblk[b].ni < 3)
+        return fail(ctx, MOSE_ERR_UNSUPPORTED, "Navier-Stokes: block %d needs at least 3 x 3 cells", b + 1);
+  }
   if (ctx->nd == 3 && !stage3d_supported(ctx->cfg.riemann, ctx->cfg.limiter))
     return fail(ctx, MOSE_ERR_UNSUPPORTED, "3-D blocks: no stage kernel for riemann %d, limiter %d",
                 ctx->cfg.riemann, ctx->cfg.limiter);
@@ -676,6 +693,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   struct InletGeo { int pidx, b, f, i, j, k; double alpha, beta; bool raw; };
   std::vector<InletGeo> inlet_geo;
   std::vector<SeriesRec> series_recs;
+  std::vector<VConn> vconn;
   for (auto& e : ctx->bc) {
     const BlockDesc& d = ctx->desc[e.b - 1];
     const HostBlock& h = ctx->hblk[e.b - 1];
@@ -714,6 +732,22 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       pidx = (int)params.size();
       params.push_back(p);
     }
+    if (e.type == 301 || e.type == 302) {
+      BcParam p{};
+      if (e.type == 301) p.p = e.data[0];   // qw
+      else p.T = e.data[0];                 // Tw
+      pidx = (int)params.size();
+      params.push_back(p);
+    }
+    if (ctx->gas.model > 0 && (e.type == 101 || e.type == 201) && e.f <= 4) {
+      // the viscous flux's source stencil (Fill_BC_Ghost_Connection); 2-D
+      // orientations: d11 = +-1 along the face, d22 = +-1 across k
+      if (e.d12 != 0 || e.d21 != 0 || (e.d11 != 1 && e.d11 != -1) || (e.d22 != 1 && e.d22 != -1) || e.fs > 4)
+        return fail(ctx, MOSE_ERR_UNSUPPORTED, "Navier-Stokes: connection orientation d11..d22 = %d %d %d %d",
+                    e.d11, e.d12, e.d21, e.d22);
+      pidx = (int)vconn.size();
+      vconn.push_back(VConn{e.bs - 1, e.is - 1, e.js - 1, e.fs, e.d11});
+    }
     bcwords[d.bcoff[e.f - 1] + face_index(h, e.f, e.i - 1, e.j - 1, e.k - 1)] = code | ((pidx + 1) << 8);
   }
 
@@ -729,6 +763,14 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       ctx->face.alloc(12 * (size_t)mcur) != cudaSuccess || ctx->vol.alloc((size_t)mcur) != cudaSuccess ||
       ctx->vers.alloc(9 * (size_t)mcur) != cudaSuccess || ctx->dtl.alloc((size_t)mcur) != cudaSuccess)
     return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
+  if (ctx->gas.model > 0) {
+    if (ctx->Mt.alloc(4 * (size_t)mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
+    CU(cudaMemsetAsync(ctx->Mt.p, 0, 4 * (size_t)mcur * sizeof(double), ctx->stream));
+    CU(ctx->vconn.alloc(std::max<size_t>(vconn.size(), 1)));
+    if (!vconn.empty())
+      CU(cudaMemcpyAsync(ctx->vconn.p, vconn.data(), vconn.size() * sizeof(VConn), cudaMemcpyHostToDevice,
+                         ctx->stream));
+  }
   CU(ctx->d_desc.alloc(nb));
   CU(ctx->bcw.alloc(bcwords.size()));
   CU(ctx->bcp.alloc(std::max<size_t>(params.size(), 1)));
@@ -918,6 +960,7 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     // faces of degenerate directions have no ghost layer on the device
     if ((e.f == 3 || e.f == 4) && h.nj < 3) continue;
     int t = bc_code_of(e.type);
+    if (t == BC_WALL_Q || t == BC_WALL_T) t = BC_EXTRAP;   // walls: Ghost_Extrapolate (the dispatch's default)
     GhostRec g{t, e.b - 1, e.i - 1, e.j - 1, e.k - 1, e.f, e.bs - 1, e.is - 1, e.js - 1, e.ks - 1, e.fs};
     gr.push_back(g);
   }
@@ -1141,6 +1184,7 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
     a.nitems3[q] = ctx->nitems3[q];
   }
   a.grid_cap = ctx->tile_ctas;
+  a.vconn = ctx->vconn.p;
   return a;
 }
 
@@ -1193,6 +1237,12 @@ int mose_gpu_residual(mose_gpu_ctx* ctx) {
     ctx->launches += enqueue_series(ctx);
   }
   StageArgs a = stage_args(ctx, ctx->cur, ctx->po, -1, 1);
+  if (ctx->gas.model > 0) {
+    if (!launch_visc_residual2d(a, (int)ctx->hblk.size(), ctx->maxcell, ctx->cfg.limiter, ctx->stream))
+      return fail(ctx, MOSE_ERR_UNSUPPORTED, "no viscous kernel for limiter %d", ctx->cfg.limiter);
+    ctx->launches++;
+    return check_launch(ctx, "residual");
+  }
   // the exact residual-only kernels read the metric arrays; the fp64 ones
   // take the constant metrics of uniform grids like the fused stages
   const bool fp64 = ctx->cfg.precision == MOSE_PRECISION_FP64;
@@ -1237,7 +1287,7 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
 // stepping each step keeps its standalone pass, so dtlocal always holds the
 // dt of the step that used it, as in the reference.
 static bool fused_dt(const mose_gpu_ctx* ctx) {
-  return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0;
+  return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0 && ctx->gas.model == 0;
 }
 static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
   a.dtmin = ctx->dtmin.p;
@@ -1330,6 +1380,14 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
     if (ctx->nghost) ++k;
     if (ctx->irs_beta > 0.0) {
       k += enqueue_irs_stage(ctx, pc, s0, pn, irk);
+    } else if (ctx->gas.model > 0) {
+      // Navier-Stokes: the residual of every term, then Newstate_Conservative
+      StageArgs a = stage_args(ctx, pc, s0, pn, irk);
+      launch_visc_residual2d(a, (int)ctx->hblk.size(), ctx->maxcell, ctx->cfg.limiter, ctx->stream);
+      launch_rk_stage_to(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[pc].p, ctx->state[s0].p,
+                         ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->cfg.time_accurate ? ctx->scal.p : nullptr,
+                         ctx->state[pn].p, ctx->gas, a.c_rk, ctx->nd, ctx->uniform, ctx->derr.p, ctx->stream);
+      k += 2;
     } else {
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
       if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
@@ -1578,6 +1636,7 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
   if (ctx->irs_beta > 0.0 || ctx->gas.sd) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no IRS or shock detector");
   if (ctx->nser) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: no time-table (402) inlets");
   if (ctx->gas.prim) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: conservative integration variables only");
+  if (ctx->gas.model > 0) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: the Euler step only");
   const size_t ns = (size_t)ctx->nv * ctx->marena, m = (size_t)ctx->marena;
   for (DevBuf<double>* b : {&ctx->lam, &ctx->lam_loc, &ctx->lam_n, &ctx->lamR, &ctx->wdt, &ctx->lamG})
     if (b->alloc(ns) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (adjoint)");
@@ -1783,6 +1842,25 @@ int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on) {
   if (!ctx) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_sd_limiter: call before mose_gpu_setup");
   ctx->gas.sd = (ctx->gas.sd & ~1) | (on ? 1 : 0);
+  return MOSE_OK;
+}
+
+int mose_gpu_set_viscous(mose_gpu_ctx* ctx, int32_t model, double mu, double kappa, double vnn) {
+  MOSE_NVTX_RANGE("mose_gpu_set_viscous");
+  if (!ctx) return MOSE_ERR_INVALID;
+  if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "set_viscous must precede setup");
+  if (model == 0) {
+    ctx->gas.model = 0;
+    return MOSE_OK;
+  }
+  if (model != 1) return fail(ctx, MOSE_ERR_UNSUPPORTED, "model %d: only 0 (Euler) and 1 (laminar) are on this path", model);
+  if (!(mu > 0.0) || !(kappa >= 0.0) || !(vnn > 0.0) || !std::isfinite(mu) || !std::isfinite(kappa) ||
+      !std::isfinite(vnn))
+    return fail(ctx, MOSE_ERR_INVALID, "viscous constants: need mu > 0, kappa >= 0, vnn > 0");
+  ctx->gas.model = 1;
+  ctx->gas.mu = mu;
+  ctx->gas.kappa = kappa;
+  ctx->gas.vnn = vnn;
   return MOSE_OK;
 }
 

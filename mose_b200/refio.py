@@ -10,7 +10,7 @@ the GPU path unchanged.
   402: T0, index of its p0 table (``read_series``), alpha, beta, rel_fac;
   403 / 404: T0 / T, mass flux, alpha, beta, rel_fac; 405: mach, T, p, alpha,
   beta, rel_fac; 406: p_back, rel_fac; 407: T0, p0, p_back, alpha, beta,
-  rel_fac).  The direction token ``normal`` becomes the largest double, as
+  rel_fac; 301: qw; 302: Tw).  The direction token ``normal`` becomes the largest double, as
   parse_dir_tok (IO_BC.f90:443-456) does.
 * ``read_tecplot`` reads ordered Tecplot ASCII zones with BLOCK data packing
   (the ORION format of MESH/*.tec and INPUT/ic*.tec): node variables on the
@@ -109,6 +109,9 @@ def read_bc(path, series: list | None = None, base=None) -> tuple[np.ndarray, np
         elif t == 407:                     # T0, p0, p_back, alpha, beta, rel_fac, ci...
             g = _fields(lines[q]); q += 1
             d = [_num(g[0]), _num(g[1]), _num(g[2]), _dir_tok(g[3]), _dir_tok(g[4]), _num(g[5])]
+        elif t in (301, 302):              # qw (Tw), k_rough, eps_wall (IO_BC.f90:241-252)
+            g = _fields(lines[q]); q += 1
+            d[0] = _num(g[0])
         elif t == 102:
             g = _fields(lines[q]); q += 1
             q += int(g[0]) + int(g[1])        # donor lines

@@ -74,6 +74,9 @@ class Solver:
             self._check(self.lib.mose_gpu_set_sd_limiter(self.h, 1))
         if getattr(case, "irs_beta", 0.0):
             self._check(self.lib.mose_gpu_set_irs_beta(self.h, float(case.irs_beta)))
+        if getattr(case, "model", 0):
+            self._check(self.lib.mose_gpu_set_viscous(self.h, int(case.model), float(case.mu), float(case.kappa),
+                                                      float(case.vnn)))
         self.dims = []
         for b, nd in enumerate(case.nodes, start=1):
             nk, nj, ni = nd.shape[0] - 1, nd.shape[1] - 1, nd.shape[2] - 1

@@ -31,6 +31,13 @@
 // Parity at this boundary is therefore against the restated closure; the
 // FLINT table path (1 K tables, int(T) index) cannot be reproduced without
 // its source.
+//
+// Transport closure (Navier-Stokes, model = 1).  FLINT's laminar transport
+// (co_k_mi_lam_Wilke_expr, f_laminarViscosity) interpolates mu(T) and k(T)
+// in 1 K tables and mixes species by Wilke's rule.  For one species Wilke's
+// weight is 1, and the reference's viscous tables are constant
+// (test/common/Air-viscous/transport.dat), so both interpolations return the
+// table's constant exactly: mu and kappa are configuration constants here.
 
 #include "mose_oracle.h"
 
@@ -1771,6 +1778,321 @@ void Stagn_Inflow(const Thermo& t, const InflowGeo& g, double alpha, double beta
   Flux[NP] = Fmass * (0.5 * (Face[NU] * Face[NU] + Face[NV] * Face[NV] + Face[NW] * Face[NW]) + Face_Enthalpy);
 }
 
+// ---------------------------------------------------------------------------
+// Navier-Stokes diffusive fluxes (model = 1, laminar): Lib_Diffusive.f90,
+// Lib_BC_Fluxes_Connection.f90:117-224, Lib_BC_Fluxes_Symmetry.f90:128-247,
+// Lib_BC_Fluxes_Wall_Heat.f90, Lib_BC_Fluxes_Wall_Temperature.f90 and the
+// standard stress vector Stress_Vector_Std (Lib_Fluid.f90:23-46).  One
+// species: the concentration gradient is an exact zero, so the species
+// diffusion and its enthalpy flux vanish exactly; the eddy viscosity is 0.
+// Gradients are G[v][c], v over the nprim visc variables (Y, u, v, w, T),
+// c over the three directions; matmul(G, M) sums over the index direction
+// in order 1, 2, 3.
+// ---------------------------------------------------------------------------
+
+// matmul(Gradient(nprim,3), M(3,3)) with M stored c(r,s) at r + 3 s
+inline void grad_matmul(double G[NPRIM][3], const double* M) {
+  double out[NPRIM][3];
+  for (int v = 0; v < NPRIM; ++v)
+    for (int c = 0; c < 3; ++c) {
+      double s = 0.0;
+      for (int d = 0; d < 3; ++d) s = s + G[v][d] * M[d + 3 * c];
+      out[v][c] = s;
+    }
+  for (int v = 0; v < NPRIM; ++v)
+    for (int c = 0; c < 3; ++c) G[v][c] = out[v][c];
+}
+
+// Stress_Vector_Std(Gradvel, Normal, mi_l, mi_t): Gradvel(r, c) = d u_r / d x_c
+inline void stress_vector(const double Gv[3][3], const double* n, double mi_l, double mi_t, double* S) {
+  const double negativetwothird = -2.0 / 3.0;
+  double mi = mi_l + mi_t;
+  double lam = negativetwothird * mi;
+  double Divervel = Gv[0][0] + Gv[1][1] + Gv[2][2];
+  double lamDivervel = lam * Divervel;
+  double Txx = lamDivervel + 2.0 * mi * Gv[0][0];
+  double Tyy = lamDivervel + 2.0 * mi * Gv[1][1];
+  double Tzz = lamDivervel + 2.0 * mi * Gv[2][2];
+  double Txy = mi * (Gv[0][1] + Gv[1][0]);
+  double Txz = mi * (Gv[0][2] + Gv[2][0]);
+  double Tyz = mi * (Gv[1][2] + Gv[2][1]);
+  S[0] = Txx * n[0] + Txy * n[1] + Txz * n[2];
+  S[1] = Txy * n[0] + Tyy * n[1] + Tyz * n[2];
+  S[2] = Txz * n[0] + Tyz * n[1] + Tzz * n[2];
+}
+
+inline void vel_grad(const double G[NPRIM][3], double Gv[3][3]) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) Gv[r][c] = G[NU + r][c];
+}
+
+// Compute_Diffusive_Flux (Lib_Diffusive.f90:90-172), laminar, one species
+inline void Compute_Diffusive_Flux(const orc_domain* D, const double* Prim, double G[NPRIM][3], double area,
+                                   const double* normal, double* Flux) {
+  const Thermo& t = D->th;
+  double rho, Rgas;
+  co_rotot_Rtot(t, Prim[0], rho, Rgas);
+  const double mil = D->cfg.mu, kl = D->cfg.kappa, mie = 0.0;
+  const double Sc = 1.0;   // obj_rans%Sc; multiplies an exact zero gradient
+  double Dm = (mil / Sc + 0.0) / rho;
+  double kappa = kl + mie * t.cp / 0.85;
+  double Gv[3][3];
+  vel_grad(G, Gv);
+  double Stress[3];
+  stress_vector(Gv, normal, mil, mie, Stress);
+  double DiffHFlux = 0.0;
+  for (int v = 0; v < NPRIM; ++v) Flux[v] = 0.0;
+  double DmGradYi = Dm * (G[0][0] * normal[0] + G[0][1] * normal[1] + G[0][2] * normal[2]);
+  Flux[0] = rho * area * DmGradYi;
+  double T = Prim[NP] / (rho * Rgas);
+  DiffHFlux = DiffHFlux + DmGradYi * (t.cp * T);
+  Flux[0] = Flux[0] - Flux[0] * Prim[0] / rho;
+  Flux[NU] = area * Stress[0];
+  Flux[NV] = area * Stress[1];
+  Flux[NW] = area * Stress[2];
+  Flux[NP] = area * ((Stress[0] * Prim[NU] + Stress[1] * Prim[NV] + Stress[2] * Prim[NW]) +
+                     kappa * (G[NP][0] * normal[0] + G[NP][1] * normal[1] + G[NP][2] * normal[2]) + DiffHFlux * rho);
+}
+
+// Visc_Variables: (rho_s / rho, u, v, w, T)
+inline void visc_vars(const Thermo& t, const double* P, double* V) {
+  double rho, Rgas;
+  co_rotot_Rtot(t, P[0], rho, Rgas);
+  V[0] = P[0] / rho;
+  V[NU] = P[NU];
+  V[NV] = P[NV];
+  V[NW] = P[NW];
+  V[NP] = P[NP] / (rho * Rgas);
+}
+
+// Tangential_Gradient (Lib_Diffusive.f90:55-87)
+inline void Tangential_Gradient(const Thermo& t, const double* P1, const double* P2, const double* P3, const double* P4,
+                                double G[NPRIM][3], int c) {
+  double V1[NPRIM], V2[NPRIM], V3[NPRIM], V4[NPRIM];
+  visc_vars(t, P1, V1);
+  visc_vars(t, P2, V2);
+  visc_vars(t, P3, V3);
+  visc_vars(t, P4, V4);
+  for (int v = 0; v < NPRIM; ++v) G[v][c] = (V2[v] - V1[v] + V4[v] - V3[v]) * 0.25;
+}
+
+// Diffusive_Flux (Lib_Diffusive.f90:10-52): face between cells 1 and 2 along
+// direction a (1-based), tangential stencils 3-6 along b and 7-10 along c
+void Diffusive_Flux(const orc_domain* D, const double* normal, double area, const double* P1, const double* P2,
+                    const double* P3, const double* P4, const double* P5, const double* P6, const double* P7,
+                    const double* P8, const double* P9, const double* P10, const double* M1, const double* M2,
+                    double* Res1, double* Res2, int a, int b, int c) {
+  const Thermo& t = D->th;
+  double G[NPRIM][3];
+  for (int v = 0; v < NPRIM; ++v) G[v][0] = G[v][1] = G[v][2] = 0.0;
+  double rho1, R1, rho2, R2;
+  co_rotot_Rtot(t, P1[0], rho1, R1);
+  double T1 = P1[NP] / (rho1 * R1);
+  co_rotot_Rtot(t, P2[0], rho2, R2);
+  double T2 = P2[NP] / (rho2 * R2);
+  G[0][a - 1] = P2[0] / rho2 - P1[0] / rho1;
+  G[NP][a - 1] = T2 - T1;
+  for (int v = NU; v <= NW; ++v) G[v][a - 1] = P2[v] - P1[v];
+  Tangential_Gradient(t, P3, P4, P5, P6, G, b - 1);
+  Tangential_Gradient(t, P7, P8, P9, P10, G, c - 1);
+  double M[9];
+  for (int q = 0; q < 9; ++q) M[q] = 0.5 * (M1[q] + M2[q]);
+  grad_matmul(G, M);
+  double Prim[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) Prim[v] = 0.5 * (P1[v] + P2[v]);
+  double Flux[NPRIM];
+  Compute_Diffusive_Flux(D, Prim, G, area, normal, Flux);
+  for (int v = 0; v < NPRIM; ++v) {
+    Res1[v] = Res1[v] - Flux[v];
+    Res2[v] = Res2[v] + Flux[v];
+  }
+}
+
+// BC_Connection_Visc (Lib_BC_Fluxes_Connection.f90:117-224).  The ghost stencil
+// Pg(:,1) is the first ghost layer; Pg(:,3:6) are the source block's cells
+// that Fill_BC_Ghost_Connection (Lib_Ghost.f90:405-460) picks with d11..d22.
+void BC_Connection_Visc(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, const Block& bs, int Is,
+                        int Js, int Ks, int Fs, int d11, int d12, int d21, int d22) {
+  const Thermo& t = D->th;
+  int dir, fi, fj, fk;
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const int modfm2 = 1 - 2 * (Fm % 2);
+  const int Ig = Im - G(Fm, 1), Jg = Jm - G(Fm, 2), Kg = Km - G(Fm, 3);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  const double area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  double M[9];
+  for (int q = 0; q < 9; ++q) M[q] = 0.5 * ((&blk.M_(1, 1, Im, Jm, Km))[q] + (&blk.M_(1, 1, Ig, Jg, Kg))[q]);
+  int i1, j1, k1, i2, j2, k2, i3, j3, k3, i4, j4, k4;
+  if (Fs <= 2) {
+    i1 = Is; j1 = Js - d11; k1 = Ks - d12; i2 = Is; j2 = Js + d11; k2 = Ks + d12;
+    i3 = Is; j3 = Js - d21; k3 = Ks - d22; i4 = Is; j4 = Js + d21; k4 = Ks + d22;
+  } else if (Fs <= 4) {
+    i1 = Is - d11; j1 = Js; k1 = Ks - d12; i2 = Is + d11; j2 = Js; k2 = Ks + d12;
+    i3 = Is - d21; j3 = Js; k3 = Ks - d22; i4 = Is + d21; j4 = Js; k4 = Ks + d22;
+  } else {
+    i1 = Is - d11; j1 = Js - d12; k1 = Ks; i2 = Is + d11; j2 = Js + d12; k2 = Ks;
+    i3 = Is - d21; j3 = Js - d22; k3 = Ks; i4 = Is + d21; j4 = Js + d22; k4 = Ks;
+  }
+  const double* Prim_loc = blk.Pc(Im, Jm, Km);
+  const double* Prim_ghost = blk.Pc(Ig, Jg, Kg);
+  double Vl[NPRIM], Vip[NPRIM], Vim[NPRIM], Vjp[NPRIM], Vjm[NPRIM], Vkp[NPRIM], Vkm[NPRIM];
+  double Vg[NPRIM], Vg3[NPRIM], Vg4[NPRIM], Vg5[NPRIM], Vg6[NPRIM];
+  visc_vars(t, Prim_loc, Vl);
+  visc_vars(t, blk.Pc(Im + 1, Jm, Km), Vip);
+  visc_vars(t, blk.Pc(Im - 1, Jm, Km), Vim);
+  visc_vars(t, blk.Pc(Im, Jm + 1, Km), Vjp);
+  visc_vars(t, blk.Pc(Im, Jm - 1, Km), Vjm);
+  visc_vars(t, blk.Pc(Im, Jm, Km + 1), Vkp);
+  visc_vars(t, blk.Pc(Im, Jm, Km - 1), Vkm);
+  visc_vars(t, Prim_ghost, Vg);
+  visc_vars(t, &bs.P[NPRIM * bs.cell(i1, j1, k1)], Vg3);
+  visc_vars(t, &bs.P[NPRIM * bs.cell(i2, j2, k2)], Vg4);
+  visc_vars(t, &bs.P[NPRIM * bs.cell(i3, j3, k3)], Vg5);
+  visc_vars(t, &bs.P[NPRIM * bs.cell(i4, j4, k4)], Vg6);
+  double Gl[NPRIM][3], Gg[NPRIM][3];
+  for (int v = 0; v < NPRIM; ++v) {
+    const double across_l = (Vg[v] - Vl[v]) * (double)modfm2;
+    const double across_g = (Vl[v] - Vg[v]) * (double)(-modfm2);
+    const double g34 = (Vg4[v] - Vg3[v]) * 0.5, g56 = (Vg6[v] - Vg5[v]) * 0.5;
+    if (Fm <= 2) {
+      Gl[v][0] = across_l; Gl[v][1] = (Vjp[v] - Vjm[v]) * 0.5; Gl[v][2] = (Vkp[v] - Vkm[v]) * 0.5;
+      Gg[v][0] = across_g; Gg[v][1] = g34; Gg[v][2] = g56;
+    } else if (Fm <= 4) {
+      Gl[v][0] = (Vip[v] - Vim[v]) * 0.5; Gl[v][1] = across_l; Gl[v][2] = (Vkp[v] - Vkm[v]) * 0.5;
+      Gg[v][0] = g34; Gg[v][1] = across_g; Gg[v][2] = g56;
+    } else {
+      Gl[v][0] = (Vip[v] - Vim[v]) * 0.5; Gl[v][1] = (Vjp[v] - Vjm[v]) * 0.5; Gl[v][2] = across_l;
+      Gg[v][0] = g34; Gg[v][1] = g56; Gg[v][2] = across_g;
+    }
+  }
+  grad_matmul(Gl, M);
+  grad_matmul(Gg, M);
+  double Prim[NPRIM];
+  for (int v = 0; v < NPRIM; ++v) Prim[v] = (Prim_loc[v] + Prim_ghost[v]) * 0.5;
+  double Fl[NPRIM], Fg[NPRIM];
+  Compute_Diffusive_Flux(D, Prim, Gl, area, Normal, Fl);
+  Compute_Diffusive_Flux(D, Prim, Gg, area, Normal, Fg);
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] - 0.5 * (double)modfm2 * (Fl[v] + Fg[v]);
+}
+
+// BC_Symmetry_Visc (Lib_BC_Fluxes_Symmetry.f90:128-247), no RSM
+void BC_Symmetry_Visc(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk) {
+  int dir, fi, fj, fk;
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const int modfm2 = 1 - 2 * (Fm % 2);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  const double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  const double* M = &blk.M_(1, 1, Im, Jm, Km);
+  const double mil = D->cfg.mu, mie = 0.0;
+  auto vel = [&](int i, int j, int k, double* V) {
+    const double* p = blk.Pc(i, j, k);
+    V[0] = p[NU]; V[1] = p[NV]; V[2] = p[NW];
+  };
+  double V1[3], V3[3], V4[3], V7[3], V8[3];
+  int a, b, c;
+  vel(Im, Jm, Km, V1);
+  if (Fm <= 2) {
+    vel(Im, Jm - 1, Km, V3); vel(Im, Jm + 1, Km, V4); vel(Im, Jm, Km - 1, V7); vel(Im, Jm, Km + 1, V8);
+    a = 0; b = 1; c = 2;
+  } else if (Fm <= 4) {
+    vel(Im - 1, Jm, Km, V3); vel(Im + 1, Jm, Km, V4); vel(Im, Jm, Km - 1, V7); vel(Im, Jm, Km + 1, V8);
+    a = 1; b = 0; c = 2;
+  } else {
+    vel(Im - 1, Jm, Km, V3); vel(Im + 1, Jm, Km, V4); vel(Im, Jm - 1, Km, V7); vel(Im, Jm + 1, Km, V8);
+    a = 2; b = 0; c = 1;
+  }
+  auto mirror = [&](const double* V, double* W) {
+    const double dn = V[0] * Normal[0] + V[1] * Normal[1] + V[2] * Normal[2];
+    for (int q = 0; q < 3; ++q) W[q] = V[q] - 2.0 * dn * Normal[q];
+  };
+  double V2[3], V5[3], V6[3], V9[3], V10[3];
+  mirror(V1, V2); mirror(V3, V5); mirror(V4, V6); mirror(V7, V9); mirror(V8, V10);
+  double Gr[NPRIM][3];
+  for (int v = 0; v < NPRIM; ++v) Gr[v][0] = Gr[v][1] = Gr[v][2] = 0.0;
+  for (int q = 0; q < 3; ++q) {
+    Gr[NU + q][a] = (V2[q] - V1[q]) * (double)modfm2;
+    Gr[NU + q][b] = (V4[q] - V3[q] + V6[q] - V5[q]) * 0.25;
+    Gr[NU + q][c] = (V8[q] - V7[q] + V10[q] - V9[q]) * 0.25;
+  }
+  grad_matmul(Gr, M);
+  double Gv[3][3];
+  vel_grad(Gr, Gv);
+  double Stress[3];
+  stress_vector(Gv, Normal, mil, mie, Stress);
+  double Vel[3];
+  for (int q = 0; q < 3; ++q) Vel[q] = 0.5 * (V1[q] + V2[q]);
+  double Flux[NPRIM] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  Flux[NU] = Area * Stress[0];
+  Flux[NV] = Area * Stress[1];
+  Flux[NW] = Area * Stress[2];
+  Flux[NP] = Area * (Vel[0] * Stress[0] + Vel[1] * Stress[1] + Vel[2] * Stress[2]);
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = NU; v <= NP; ++v) r[v] = r[v] - (double)modfm2 * Flux[v];
+}
+
+// the wall routines' common part: velocity gradient across the face from the
+// no-slip wall (Gradient(nu:nw, Dir) = Prim(nu:nw) * modfm3), the given
+// temperature gradient across it, then matmul and the stress
+inline void wall_stress(const orc_domain* D, const double* Prim, int dir, int modfm3, double Tgrad, const double* M,
+                        const double* Normal, double G[NPRIM][3], double* Stress) {
+  for (int v = 0; v < NPRIM; ++v) G[v][0] = G[v][1] = G[v][2] = 0.0;
+  for (int v = NU; v <= NW; ++v) G[v][dir - 1] = Prim[v] * (double)modfm3;
+  G[NP][dir - 1] = Tgrad;
+  grad_matmul(G, M);
+  double Gv[3][3];
+  vel_grad(G, Gv);
+  stress_vector(Gv, Normal, D->cfg.mu, 0.0, Stress);
+}
+
+// BC_Wall_Heat (Lib_BC_Fluxes_Wall_Heat.f90:13-116): prescribed heat flux qw
+void BC_Wall_Heat(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, double Heat_Flux) {
+  int dir, fi, fj, fk;
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const int modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  const double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  const double* M = &blk.M_(1, 1, Im, Jm, Km);
+  const double* Prim = blk.Pc(Im, Jm, Km);
+  const double kl = D->cfg.kappa;
+  const double mdotn = M[(dir - 1) + 0] * Normal[0] + M[(dir - 1) + 3] * Normal[1] + M[(dir - 1) + 6] * Normal[2];
+  const double Tgrad = -Heat_Flux / (2.0 * kl * mdotn) * (double)modfm2;
+  double G[NPRIM][3], Stress[3];
+  wall_stress(D, Prim, dir, modfm3, Tgrad, M, Normal, G, Stress);
+  double Flux[NPRIM] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  Flux[NU] = Stress[0] * Area;
+  Flux[NV] = Stress[1] * Area;
+  Flux[NW] = Stress[2] * Area;
+  Flux[NP] = Area * Heat_Flux;
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] - (double)modfm2 * Flux[v];
+}
+
+// BC_Wall_Temperature (Lib_BC_Fluxes_Wall_Temperature.f90:12-100): wall at T_wall
+void BC_Wall_Temperature(const orc_domain* D, int Im, int Jm, int Km, int Fm, Block& blk, double T_wall) {
+  const Thermo& t = D->th;
+  int dir, fi, fj, fk;
+  Face_Index(Fm, Im, Jm, Km, dir, fi, fj, fk);
+  const int modfm = Fm % 2, modfm2 = 1 - 2 * modfm, modfm3 = 2 * (2 * modfm - 1);
+  const double* Normal = &blk.fN[dir - 1][3 * blk.face(dir, fi, fj, fk)];
+  const double Area = blk.fA[dir - 1][blk.face(dir, fi, fj, fk)];
+  const double* M = &blk.M_(1, 1, Im, Jm, Km);
+  const double* Prim = blk.Pc(Im, Jm, Km);
+  double rho, Rgas;
+  co_rotot_Rtot(t, Prim[0], rho, Rgas);
+  const double T = Prim[NP] / (rho * Rgas);
+  const double kl = D->cfg.kappa;
+  double G[NPRIM][3], Stress[3];
+  wall_stress(D, Prim, dir, modfm3, (T - T_wall) * (double)modfm3, M, Normal, G, Stress);
+  double Flux[NPRIM] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  Flux[NU] = Stress[0] * Area;
+  Flux[NV] = Stress[1] * Area;
+  Flux[NW] = Stress[2] * Area;
+  Flux[NP] = Area * kl * (G[NP][0] * Normal[0] + G[NP][1] * Normal[1] + G[NP][2] * Normal[2]);
+  double* r = blk.Rc(Im, Jm, Km);
+  for (int v = 0; v < NPRIM; ++v) r[v] = r[v] - (double)modfm2 * Flux[v];
+}
+
 void add_bc_flux(Block& blk, int Im, int Jm, int Km, int modfm2, const double* Flux) {
   double* r = blk.Rc(Im, Jm, Km);
   for (int v = 0; v < NPRIM; ++v) r[v] = r[v] + (double)modfm2 * Flux[v];
@@ -1927,6 +2249,8 @@ int orc_set_bcs(orc_domain* d, const int32_t* rec, const double* data, int nboun
     d->n_bf[key] += 1;
     switch (e.type) {
       case 0: case 101: case 201: case 300: case 400: case 401: case 403: case 404: case 405: case 406: case 407:
+        break;
+      case 301: case 302:   // walls: prescribed heat flux (data[0] = qw) / temperature (data[0] = Tw)
         break;
       case 402:
         if (!(e.data[1] >= 0.0 && e.data[1] < (double)d->series.size() && e.data[1] == std::floor(e.data[1])))
@@ -2121,6 +2445,20 @@ int orc_fluxes(orc_domain* d) {
                                  B.Pc(i + 1, j, k), B.Pc(i + 2, j, k), B.Rc(i, j, k), B.Rc(i + 1, j, k), B.beta[B.inner(i, j, k)]))
               d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
           }
+      if (d->cfg.model > 0) {   // diffusive i faces (:101-126)
+#ifdef _OPENMP
+#pragma omp for collapse(2)
+#endif
+        for (int k = 1; k <= n3; ++k)
+          for (int j = 1; j <= n2; ++j)
+            for (int i = 1; i <= n1 - 1; ++i) {
+              size_t f = B.face(1, i, j, k);
+              Diffusive_Flux(d, &B.fN[0][3 * f], B.fA[0][f], B.Pc(i, j, k), B.Pc(i + 1, j, k), B.Pc(i, j - 1, k),
+                             B.Pc(i, j + 1, k), B.Pc(i + 1, j - 1, k), B.Pc(i + 1, j + 1, k), B.Pc(i, j, k - 1),
+                             B.Pc(i, j, k + 1), B.Pc(i + 1, j, k - 1), B.Pc(i + 1, j, k + 1), &B.M_(1, 1, i, j, k),
+                             &B.M_(1, 1, i + 1, j, k), B.Rc(i, j, k), B.Rc(i + 1, j, k), 1, 2, 3);
+            }
+      }
       // j faces (:129-139)
 #ifdef _OPENMP
 #pragma omp for collapse(2)
@@ -2134,6 +2472,20 @@ int orc_fluxes(orc_domain* d) {
                                  B.Pc(i, j + 1, k), B.Pc(i, j + 2, k), B.Rc(i, j, k), B.Rc(i, j + 1, k), B.beta[B.inner(i, j, k)]))
               d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
           }
+      if (d->cfg.model > 0) {   // diffusive j faces (:141-166)
+#ifdef _OPENMP
+#pragma omp for collapse(2)
+#endif
+        for (int k = 1; k <= n3; ++k)
+          for (int i = 1; i <= n1; ++i)
+            for (int j = 1; j <= n2 - 1; ++j) {
+              size_t f = B.face(2, i, j, k);
+              Diffusive_Flux(d, &B.fN[1][3 * f], B.fA[1][f], B.Pc(i, j, k), B.Pc(i, j + 1, k), B.Pc(i - 1, j, k),
+                             B.Pc(i + 1, j, k), B.Pc(i - 1, j + 1, k), B.Pc(i + 1, j + 1, k), B.Pc(i, j, k - 1),
+                             B.Pc(i, j, k + 1), B.Pc(i, j + 1, k - 1), B.Pc(i, j + 1, k + 1), &B.M_(1, 1, i, j, k),
+                             &B.M_(1, 1, i, j + 1, k), B.Rc(i, j, k), B.Rc(i, j + 1, k), 2, 1, 3);
+            }
+      }
       // k faces (:169-179)
 #ifdef _OPENMP
 #pragma omp for collapse(2)
@@ -2147,6 +2499,20 @@ int orc_fluxes(orc_domain* d) {
                                  B.Pc(i, j, k + 1), B.Pc(i, j, k + 2), B.Rc(i, j, k), B.Rc(i, j, k + 1), B.beta[B.inner(i, j, k)]))
               d->fail(ORC_ERR_INTERFACE_STATE, bi + 1, i, j, k);
           }
+      if (d->cfg.model > 0) {   // diffusive k faces (:181-206)
+#ifdef _OPENMP
+#pragma omp for collapse(2)
+#endif
+        for (int j = 1; j <= n2; ++j)
+          for (int i = 1; i <= n1; ++i)
+            for (int k = 1; k <= n3 - 1; ++k) {
+              size_t f = B.face(3, i, j, k);
+              Diffusive_Flux(d, &B.fN[2][3 * f], B.fA[2][f], B.Pc(i, j, k), B.Pc(i, j, k + 1), B.Pc(i - 1, j, k),
+                             B.Pc(i + 1, j, k), B.Pc(i - 1, j, k + 1), B.Pc(i + 1, j, k + 1), B.Pc(i, j - 1, k),
+                             B.Pc(i, j + 1, k), B.Pc(i, j - 1, k + 1), B.Pc(i, j + 1, k + 1), &B.M_(1, 1, i, j, k),
+                             &B.M_(1, 1, i, j, k + 1), B.Rc(i, j, k), B.Rc(i, j, k + 1), 3, 1, 2);
+            }
+      }
     }
   }
   return d->err;
@@ -2167,8 +2533,24 @@ int orc_bc_fluxes(orc_domain* d) {
         const BCrec& e = d->bc[q];
         Block& bm = d->blk[e.b - 1];
         switch (e.type) {
-          case 101: case 201: BC_Connection_Eul(d, e.i, e.j, e.k, e.f, bm); break;
-          case 300: BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm); break;
+          case 101: case 201:
+            BC_Connection_Eul(d, e.i, e.j, e.k, e.f, bm);
+            if (d->cfg.model > 0)
+              BC_Connection_Visc(d, e.i, e.j, e.k, e.f, bm, d->blk[e.bs - 1], e.is, e.js, e.ks, e.fs, e.d11, e.d12,
+                                 e.d21, e.d22);
+            break;
+          case 300:
+            BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            if (d->cfg.model > 0) BC_Symmetry_Visc(d, e.i, e.j, e.k, e.f, bm);
+            break;
+          case 301:   // Mod_BC_Fluxes.f90:87-95 (no rotating frame)
+            BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            if (d->cfg.model > 0) BC_Wall_Heat(d, e.i, e.j, e.k, e.f, bm, e.data[0]);
+            break;
+          case 302:   // Mod_BC_Fluxes.f90:97-104
+            BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
+            if (d->cfg.model > 0) BC_Wall_Temperature(d, e.i, e.j, e.k, e.f, bm, e.data[0]);
+            break;
           case 400: BC_Extrapolation(d, e.i, e.j, e.k, e.f, bm); break;
           case 405:
             if (!BC_Inlet_Supersonic(d, e.i, e.j, e.k, e.f, bm, e.data)) BC_Symmetry_Eul(d, e.i, e.j, e.k, e.f, bm);
@@ -2427,6 +2809,14 @@ int orc_compute_dt(orc_domain* d, double* dtglobal_out) {
             double lambda = vel_ + Sound;
             double dt = B.dl_(dd, i, j, k) / lambda * cfl;
             dtmin = std::min(dt, dtmin);
+          }
+          if (d->cfg.model > 0) {   // VNN condition, Mod_dt.f90:87-103 (laminar: mi = 0 + mil)
+            const double mi = 0.0 + d->cfg.mu;
+            for (int dd = 1; dd <= ndir; ++dd) {
+              const double dlv = B.dl_(dd, i, j, k);
+              double dt = (rho * (dlv * dlv) * d->cfg.vnn) / mi;
+              dtmin = std::min(dt, dtmin);
+            }
           }
           double dtcell = dtmin;
           if (d->iter < d->cfg.ramp_iter) dtcell = dtcell * (double)d->iter / (double)d->cfg.ramp_iter;

@@ -51,6 +51,10 @@ typedef struct orc_config {
   double minf;           /* riemann-options-Minf (AUSM+-up, AUSM+-up2) */
   double irs_beta;       /* irs-beta: implicit residual smoothing when > 0 */
   int32_t sd_limiter;    /* space-reconstruction MUSCL-SD: slopes scaled by the shock detector */
+  int32_t model;         /* 0: Euler, 1: laminar Navier-Stokes (Global_m model) */
+  double mu;             /* laminar viscosity (constant-property transport table) */
+  double kappa;          /* laminar conductivity (constant-property transport table) */
+  double vnn;            /* von Neumann number of the viscous time-step limit (Mod_dt.f90:98-103) */
 } orc_config;
 
 /* Error codes: mirror the reference's fatal `stop` sites. */

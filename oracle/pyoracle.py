@@ -21,7 +21,8 @@ class orc_config(C.Structure):
                 ("limiter", C.c_int32), ("riemann", C.c_int32), ("integration", C.c_int32),
                 ("ndir", C.c_int32), ("gamma", C.c_double), ("rgas", C.c_double),
                 ("ramp_iter", C.c_int32), ("res_diter", C.c_int32), ("minf", C.c_double),
-                ("irs_beta", C.c_double), ("sd_limiter", C.c_int32)]
+                ("irs_beta", C.c_double), ("sd_limiter", C.c_int32), ("model", C.c_int32), ("mu", C.c_double),
+                ("kappa", C.c_double), ("vnn", C.c_double)]
 
 
 _LIBS: dict = {}
@@ -105,7 +106,9 @@ class Oracle:
                          ndir=ndir, gamma=case.gamma, rgas=case.rgas, ramp_iter=int(getattr(case, "ramp_iter", 0)),
                          res_diter=1,
                          minf=getattr(case, "minf", 0.0), irs_beta=getattr(case, "irs_beta", 0.0),
-                         sd_limiter=int(getattr(case, "sd_limiter", False)))
+                         sd_limiter=int(getattr(case, "sd_limiter", False)), model=int(getattr(case, "model", 0)),
+                         mu=float(getattr(case, "mu", 0.0)), kappa=float(getattr(case, "kappa", 0.0)),
+                         vnn=float(getattr(case, "vnn", 0.5)))
         self.h = self.lib.orc_create(C.byref(cfg), nthreads)
         self.dims = []
         for nd in case.nodes:

@@ -39,6 +39,17 @@ def test_measurement_probe_stays_out_of_the_product(lib):
     assert hasattr(_lib.load_probe(), "mose_probe_fp64_peak")
 
 
+def test_fortran_module_binds_every_entry_point():
+    """mose_b200/fortran/mose_gpu_m.f90 has an ISO_C_BINDING interface, bound
+    by name, for every entry point the header declares (no Fortran compiler
+    is on these machines, so this is a text check of the module)."""
+    f90 = (ROOT / "mose_b200" / "fortran" / "mose_gpu_m.f90").read_text()
+    bound = set(re.findall(r'bind\(C, name="(mose_gpu_\w+)"\)', f90))
+    public = set(re.findall(r"\b(mose_gpu_\w+)\b", " ".join(l for l in f90.splitlines() if "public ::" in l)))
+    assert bound == set(declared_functions())
+    assert public >= bound
+
+
 def test_binding_covers_the_header(lib):
     from mose_b200 import _lib
     assert set(_lib.SIGNATURES) == set(declared_functions())
