@@ -416,39 +416,22 @@ def config_report(name, make_case, local, steps, precisions=PRECISIONS):
     return {name: out}
 
 
-def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0):
-    """Configuration 5: the wall-pressure objective on the curvilinear 512^2
-    channel after 200 RK3 steps (van Albada + HLLC, FP64 reference-exact
-    forward), its gradient with respect to the initial state and the inflow
-    Mach by the discrete adjoint with sqrt(N) checkpointing through the
-    torch.autograd.Function, the cost ratio backward / forward (device time
-    of the C ABI calls), and the gradient against central differences (step
-    1e-6, and 1e-7 beside it) on 32 seeded cell-wise random directions.  The
-    objective is piecewise smooth (the limiters' cut-off where adjacent
-    slopes change sign, the branches of the HLLC wave selection): a
-    difference step can straddle kinks, whose share falls with the step.
-    The initial state is the
-    uniform Mach-0.8 flow with a seeded 5 % cell-wise perturbation
-    (cases.perturbed_channel): at the exactly uniform state every limited
-    slope vanishes and the objective has no gradient."""
-    import math
+def _adjoint_timing(local, case, prec, nsteps, K):
+    """Device times (ms) on one context of the given precision: a plain
+    graph-replayed forward of nsteps, the checkpointing forward and the
+    reverse sweep (after a warm-up of each, which captures the graphs)."""
     import torch
-    from mose_b200 import Solver, cases
-    from mose_b200.adjoint import wall_pressure
-    from mose_b200.cases import GC, to_ref_layout
-    case = cases.perturbed_channel(n, steps=nsteps, seed=seed)
-    rng = np.random.default_rng(seed + 1)
+    from mose_b200 import Solver
+    from mose_b200.cases import to_ref_layout
     P0 = case.prim[0].copy()
     mach = case.extra["mach"]
-    s = Solver(case, precision=precision_code("exact"), device=local)
+    s = Solver(case, precision=precision_code(prec), device=local)
     st = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
-    K = max(1, int(round(math.sqrt(nsteps))))
 
-    def J(P, M):
-        s.upload_prim(1, to_ref_layout(P))
+    def reset():
+        s.upload_prim(1, to_ref_layout(P0))
         s.set_time(0.0, 0)
-        s.set_inflow_mach(M)
-        return s.adjoint_forward(nsteps, K, 1, 3)
+        s.set_inflow_mach(mach)
 
     def timed(fn):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -459,31 +442,59 @@ def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0):
         torch.cuda.synchronize()
         return r, e0.elapsed_time(e1)
 
-    J(P0, mach)
-    s.adjoint_backward()                                  # warm-up (graphs, buffers)
-    s.upload_prim(1, to_ref_layout(P0))
-    s.set_inflow_mach(mach)
+    reset()
+    s.advance(nsteps)                                     # warm-up (graph capture)
+    reset()
     _, plain_ms = timed(lambda: s.advance(nsteps))
-    # the same forward in the fp64 precision (the fastest FP64 forward): the
-    # cost ratios are quoted against it as well
-    f = Solver(case, precision=precision_code("fp64"), device=local)
-    f.set_inflow_mach(mach)
-    f.advance(nsteps)                                     # warm-up (graph capture)
-    f.upload_prim(1, to_ref_layout(P0))
-    f.set_time(0.0, 0)
-    fst = torch.cuda.ExternalStream(f.stream_handle, device=torch.device("cuda", local))
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(fst)
-    f.advance(nsteps)
-    e1.record(fst)
-    torch.cuda.synchronize()
-    fp64_ms = e0.elapsed_time(e1)
-    f.close()
-    s.upload_prim(1, to_ref_layout(P0))
-    s.set_time(0.0, 0)
+    reset()
+    s.adjoint_forward(nsteps, K, 1, 3)
+    s.adjoint_backward()                                  # warm-up (graphs, buffers)
+    reset()
     J0, fwd_ms = timed(lambda: s.adjoint_forward(nsteps, K, 1, 3))
     _, bwd_ms = timed(lambda: s.adjoint_backward())
+    s.close()
+    return {"plain_forward_ms": plain_ms, "forward_ms": fwd_ms, "backward_ms": bwd_ms, "J_direct": J0,
+            "backward_over_forward": bwd_ms / plain_ms, "gradient_over_forward": (fwd_ms + bwd_ms) / plain_ms}
+
+
+def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0, precision="fp64"):
+    """Configuration 5: the wall-pressure objective on the curvilinear 512^2
+    channel after 200 RK3 steps (van Albada + HLLC, FP64), its gradient with
+    respect to the initial state and the inflow Mach by the discrete adjoint
+    with sqrt(N) checkpointing through the torch.autograd.Function, and the
+    gradient against central differences (step 1e-6, and 1e-7 beside it) on
+    32 seeded cell-wise random directions.  The forward runs in the fp64
+    precision (the fastest FP64 forward; within rounding of the reference
+    arithmetic); the cost ratios are the device times of the C ABI calls over
+    a plain graph-replayed forward of the same 200 steps in the same
+    precision, and beside them the same ratios in the reference-exact
+    precision.  backward = the reverse sweep (segment recompute + adjoint
+    steps); gradient = the checkpointing forward + the backward.  The
+    objective is piecewise smooth (the limiters' cut-off where adjacent
+    slopes change sign, the branches of the HLLC wave selection): a
+    difference step can straddle kinks, whose share falls with the step.  The
+    initial state is the uniform Mach-0.8 flow with a seeded 5 % cell-wise
+    perturbation (cases.perturbed_channel): at the exactly uniform state
+    every limited slope vanishes and the objective has no gradient."""
+    import math
+    import torch
+    from mose_b200 import Solver, cases
+    from mose_b200.adjoint import wall_pressure
+    from mose_b200.cases import to_ref_layout
+    case = cases.perturbed_channel(n, steps=nsteps, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    P0 = case.prim[0].copy()
+    mach = case.extra["mach"]
+    K = max(1, int(round(math.sqrt(nsteps))))
+    times = {prec: _adjoint_timing(local, case, prec, nsteps, K) for prec in (precision, "exact")}
+    s = Solver(case, precision=precision_code(precision), device=local)
+
+    def J(P, M):
+        s.upload_prim(1, to_ref_layout(P))
+        s.set_time(0.0, 0)
+        s.set_inflow_mach(M)
+        return s.adjoint_forward(nsteps, K, 1, 3)
+
     p = torch.tensor(P0, requires_grad=True)
     m = torch.tensor(mach, dtype=torch.float64, requires_grad=True)
     Jt = wall_pressure(p, m, s, nsteps, K, 1, 3)
@@ -501,15 +512,17 @@ def adjoint_report(local, n=512, nsteps=200, ndir=32, seed=0):
         errs7.append(abs(adj - fd7) / abs(fd7))
     fdm = (J(P0, mach + h) - J(P0, mach - h)) / (2 * h)
     s.close()
+    t = times[precision]
     return {"adjoint_curvilinear_512^2_200_steps": {
-        "cells": case.ncells, "steps": nsteps, "checkpoint_interval": K, "J": float(Jt.detach()), "J_direct": J0,
-        "forward_ms": fwd_ms, "plain_forward_ms": plain_ms, "fp64_forward_ms": fp64_ms, "backward_ms": bwd_ms,
-        "backward_over_exact_forward": bwd_ms / plain_ms, "backward_over_fp64_forward": bwd_ms / fp64_ms,
-        "gradient_over_exact_forward": (fwd_ms + bwd_ms) / plain_ms,
-        "gradient_over_fp64_forward": (fwd_ms + bwd_ms) / fp64_ms,
+        "cells": case.ncells, "steps": nsteps, "checkpoint_interval": K, "precision": precision,
+        "J": float(Jt.detach()), "J_direct": t["J_direct"],
+        "forward_ms": t["forward_ms"], "plain_forward_ms": t["plain_forward_ms"], "backward_ms": t["backward_ms"],
+        "backward_over_fp64_forward": t["backward_over_forward"],
+        "gradient_over_fp64_forward": t["gradient_over_forward"],
+        "exact": times["exact"],
         "ratios": "backward = the reverse sweep (segment recompute + adjoint steps); gradient = the "
                   "checkpointing forward + the backward; each over a plain graph-replayed forward of the "
-                  "same 200 steps in the reference-exact or the fp64 precision",
+                  "same 200 steps in the same precision",
         "gradient_vs_fd": {"directions": ndir, "kind": "seeded cell-wise N(0,1) on rho, u, v, p", "step": h,
                            "max_rel_err": max(errs), "median_rel_err": float(np.median(errs)),
                            "below_1e-5": int(sum(e < 1e-5 for e in errs)),
@@ -712,8 +725,10 @@ def summary(line, headline):
     for cname, c in (line.get("configs") or {}).items():
         short = cname.split("_")[0]
         if "adjoint" in cname:
-            out["adjoint"] = {k: _g(c[k], 3) for k in ("backward_over_fp64_forward", "gradient_over_fp64_forward",
-                                                        "backward_over_exact_forward") if k in c}
+            out["adjoint"] = {k: _g(c[k], 3) for k in ("backward_over_fp64_forward", "gradient_over_fp64_forward")
+                              if k in c}
+            if "exact" in c:
+                out["adjoint"]["exact_gradient_over_forward"] = _g(c["exact"]["gradient_over_forward"], 3)
             g = c.get("gradient_vs_fd", {})
             out["adjoint"]["fd_max_rel_err"] = _g(g.get("max_rel_err", float("nan")), 2)
             out["adjoint"]["fd_below_1e-5"] = g.get("below_1e-5")

@@ -89,6 +89,10 @@ struct BlockDesc {
   long long mbase;      // offset of this block in the one-plane arenas
   int bcoff[6];         // offset of face f's per-cell BC words in the BC table
   int bcn[6];           // number of face cells on face f
+  // 2-D connection images: offset of face f's entries in the image table
+  // (one per face cell: the ghosts of a connected block that copy it), -1
+  // when no connection reads this face
+  int imgoff[4];
   // Uniform metrics (valid when the context runs the constant-metric kernels)
   double u_dl[3];
   double u_n[3][3];     // face normal per direction

@@ -209,8 +209,23 @@ struct mose_gpu_ctx {
   int nghost = 0, nitems = 0;
   int cur = 0, po = 0;        // state arena holding P, and PO
 
-  cudaGraphExec_t graph[3] = {nullptr, nullptr, nullptr};
-  int graph_kernels = 0;
+  // step graphs per starting arena, [1] with the standalone dt pass forced
+  // (the adjoint's forward in a non-exact precision, below)
+  cudaGraphExec_t graph[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};
+  int graph_kernels[2] = {0, 0};
+  // The adjoint's forward and recompute in the fp64 / mixed precisions take
+  // every step's dt from the standalone (reference-arithmetic) pass instead
+  // of the fused one, so the dt argmin of the reverse sweep finds the cell
+  // that set it.
+  bool adj_dt_standalone = false;
+  // Connection images (2-D fused stages): the stage kernels write the ghosts
+  // that 101 / 201 records copy; the ghost-fill kernel then runs only the
+  // other records (ghosts_nc).  ghost_valid: the current state's connection
+  // ghosts were written with it.
+  bool img_ok = false, ghost_valid = false;
+  DevBuf<int4> img;
+  DevBuf<GhostRec> ghosts_nc;
+  int nghost_nc = 0;
   // dtmin holds the CFL minimum of state[cur], folded in by the last RK stage
   // of the previous fused step; cleared by every call that changes the state
   bool dt_valid = false;
@@ -344,8 +359,9 @@ void destroy_adjoint_graphs(mose_gpu_ctx* ctx) {
 }
 
 void destroy_graphs(mose_gpu_ctx* ctx) {
-  for (auto& g : ctx->graph)
-    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  for (auto& gs : ctx->graph)
+    for (auto& g : gs)
+      if (g) { cudaGraphExecDestroy(g); g = nullptr; }
   destroy_adjoint_graphs(ctx);
 }
 
@@ -766,7 +782,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if (ctx->gas.model > 0) {
     if (ctx->Mt.alloc(4 * (size_t)mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
     CU(cudaMemsetAsync(ctx->Mt.p, 0, 4 * (size_t)mcur * sizeof(double), ctx->stream));
-    CU(ctx->vconn.alloc(std::max<size_t>(vconn.size(), 1)));
+    static_assert(sizeof(VConn) == 5 * sizeof(int), "VConn is five ints");
+    CU(ctx->vconn.alloc(5 * std::max<size_t>(vconn.size(), 1)));
     if (!vconn.empty())
       CU(cudaMemcpyAsync(ctx->vconn.p, vconn.data(), vconn.size() * sizeof(VConn), cudaMemcpyHostToDevice,
                          ctx->stream));
@@ -969,6 +986,50 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
   if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
 
+  // ---- connection images of the 2-D fused stages -------------------------------
+  // Each connection ghost g = 1, 2 of a record copies the source cell g - 1
+  // steps inward from the source face; indexed by the source face cell, the
+  // table names the two ghosts.  Used when every source face cell feeds at
+  // most one record, for the fused (not IRS, not viscous) stages.
+  {
+    for (auto& d : ctx->desc)
+      for (int f = 0; f < 4; ++f) d.imgoff[f] = -1;
+    ctx->img_ok = false;
+    std::vector<int4> table;
+    std::vector<GhostRec> nc;
+    bool ok = ctx->nd == 2 && ctx->irs_beta == 0.0 && ctx->gas.model == 0;
+    for (const GhostRec& g : gr) {
+      if (g.type != BC_CONN) { nc.push_back(g); continue; }
+      if (!ok) continue;
+      BlockDesc& sd = ctx->desc[g.bs];
+      if (g.fs > 4) { ok = false; continue; }
+      if (sd.imgoff[g.fs - 1] < 0) {
+        sd.imgoff[g.fs - 1] = (int)table.size();
+        table.resize(table.size() + ((g.fs <= 2) ? sd.nj : sd.ni), int4{-1, 0, 0, 0});
+      }
+      const int pos = (g.fs <= 2) ? g.js : g.is;
+      int4& t = table[sd.imgoff[g.fs - 1] + pos];
+      if (t.x >= 0) { ok = false; continue; }   // a face cell feeding two records
+      const BlockDesc& td = ctx->desc[g.b];
+      const int gi = (g.f == 1) ? 1 : (g.f == 2) ? -1 : 0, gj = (g.f == 3) ? 1 : (g.f == 4) ? -1 : 0;
+      t = int4{g.b, (int)cell_off2(td, g.i - gi, g.j - gj), (int)cell_off2(td, g.i - 2 * gi, g.j - 2 * gj), 0};
+    }
+    if (ok && !table.empty()) {
+      ctx->img_ok = true;
+      CU(ctx->img.alloc(table.size()));
+      CU(cudaMemcpyAsync(ctx->img.p, table.data(), table.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
+      ctx->nghost_nc = (int)nc.size();
+      CU(ctx->ghosts_nc.alloc(std::max<size_t>(nc.size(), 1)));
+      if (!nc.empty())
+        CU(cudaMemcpyAsync(ctx->ghosts_nc.p, nc.data(), nc.size() * sizeof(GhostRec), cudaMemcpyHostToDevice,
+                           ctx->stream));
+    } else {
+      for (auto& d : ctx->desc)
+        for (int f = 0; f < 4; ++f) d.imgoff[f] = -1;
+    }
+    CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
+  }
+
   // ---- implicit residual smoothing: first-layer ghost records of R ----------------
   if (ctx->irs_beta > 0.0) {
     static const int inward[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};   // guide(face, 1:2), faces 1..4
@@ -1041,6 +1102,7 @@ static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool uplo
   if (arena == -2 && !ctx->lam.p) return fail(ctx, MOSE_ERR_NOT_READY, "no adjoint state yet");
   if (upload) {
     ctx->dt_valid = false;
+    ctx->ghost_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, P, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_ref_to_soa(ctx->d_desc.p, b - 1, n, ctx->staging.p, dst, ctx->nv, ctx->nd, ctx->stream);
     ctx->launches++;
@@ -1082,6 +1144,7 @@ static int dt_io(mose_gpu_ctx* ctx, int32_t b, double* dt, bool upload) {
   if (rc) return rc;
   if (upload) {
     ctx->dt_valid = false;
+    ctx->ghost_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, dt, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_plane_io(ctx->d_desc.p, b - 1, n, ctx->dtl.p, ctx->staging.p, ctx->nd, 0, ctx->stream);
   } else {
@@ -1112,6 +1175,7 @@ int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ram
   if (rc) return rc;
   if (!dtglobal) return MOSE_ERR_INVALID;
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   launch_step_begin(ctx->dtmin.p, *dtglobal, nullptr, ctx->stream);
   launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->margs(),
                     ctx->dtl.p, ctx->dtmin.p, ctx->gas, cfl, ctx->ndir, ctx->nd, iter, ramp_iter, 1, ctx->uniform,
@@ -1128,6 +1192,7 @@ int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
   int rc = require_ready(ctx);
   if (rc) return rc;
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   CU(cudaMemcpyAsync(ctx->scal.p, &dtglobal, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   launch_set_global_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->dtl.p, ctx->scal.p, ctx->nd,
                        ctx->stream);
@@ -1141,6 +1206,7 @@ int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
   int rc = require_ready(ctx);
   if (rc) return rc;
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   ctx->po = (ctx->cur + 1) % 3;
   CU(cudaMemcpyAsync(ctx->state[ctx->po].p, ctx->state[ctx->cur].p, ctx->state[0].n * sizeof(double),
                      cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1185,7 +1251,23 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   }
   a.grid_cap = ctx->tile_ctas;
   a.vconn = ctx->vconn.p;
+  a.img = ctx->img_ok ? ctx->img.p : nullptr;
   return a;
+}
+
+// The ghost layers of the stage input pc: every record, or, when the stages
+// write their connection images and pc's connection ghosts were written with
+// it, the other records only.  Returns the number of kernels enqueued.
+static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc, bool conn_valid) {
+  if (ctx->img_ok && conn_valid) {
+    if (!ctx->nghost_nc) return 0;
+    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts_nc.p, ctx->nghost_nc, ctx->state[pc].p, ctx->margs(), ctx->nd,
+                       ctx->derr.p, ctx->stream);
+    return 1;
+  }
+  launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
+                     ctx->stream);
+  return ctx->nghost ? 1 : 0;
 }
 
 // One RK stage (mode 0 / 2) or one residual evaluation (mode 1) on every
@@ -1262,6 +1344,7 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
   if (irk < 1 || irk > ctx->cfg.n_rk) return fail(ctx, MOSE_ERR_INVALID, "irk out of range");
   static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   if (ctx->irs_beta > 0.0) {
     // RK_Newstate with IRS on the residual of mose_gpu_residual, dt from
     // dtlocal (Compute_dt / Set_Global_dt of the phase path)
@@ -1287,7 +1370,8 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
 // stepping each step keeps its standalone pass, so dtlocal always holds the
 // dt of the step that used it, as in the reference.
 static bool fused_dt(const mose_gpu_ctx* ctx) {
-  return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0 && ctx->gas.model == 0;
+  return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0 && ctx->gas.model == 0 &&
+         !ctx->adj_dt_standalone;
 }
 static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
   a.dtmin = ctx->dtmin.p;
@@ -1366,7 +1450,7 @@ static int enqueue_series(mose_gpu_ctx* ctx) {
   return 1;
 }
 
-static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
+static int enqueue_step(mose_gpu_ctx* ctx, int s0, bool ghosts_valid) {
   int k = 0;
   if (!fused_dt(ctx)) k += enqueue_dt_pass(ctx, s0);
   launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
@@ -1375,9 +1459,8 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
   int pc = s0;
   for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
     int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
-    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
-                       ctx->stream);
-    if (ctx->nghost) ++k;
+    // the stages after the first read the images the stage before wrote
+    k += enqueue_stage_ghosts(ctx, pc, irk == 1 ? ghosts_valid : true);
     if (ctx->irs_beta > 0.0) {
       k += enqueue_irs_stage(ctx, pc, s0, pn, irk);
     } else if (ctx->gas.model > 0) {
@@ -1413,10 +1496,11 @@ int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
   CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   int s0 = ctx->cur;
   if (fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, s0);
-  ctx->launches += enqueue_step(ctx, s0);
+  ctx->launches += enqueue_step(ctx, s0, ctx->ghost_valid);
   rc = check_launch(ctx, "step");
   if (rc) return rc;
   ctx->dt_valid = fused_dt(ctx);
+  ctx->ghost_valid = ctx->img_ok;
   ctx->po = s0;
   ctx->cur = step_final_index(ctx, s0);
   double h[2];
@@ -1433,24 +1517,28 @@ int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
 // captured on first use); the device time and iteration are already set.
 static int enqueue_graph_steps(mose_gpu_ctx* ctx, int nsteps) {
   if (nsteps > 0 && fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, ctx->cur);
+  // the graphs start from current connection ghosts
+  if (nsteps > 0 && ctx->img_ok && !ctx->ghost_valid) ctx->launches += enqueue_stage_ghosts(ctx, ctx->cur, false);
   for (int n = 0; n < nsteps; ++n) {
     int s0 = ctx->cur;
-    if (!ctx->graph[s0]) {
+    const int gv = ctx->adj_dt_standalone ? 1 : 0;
+    if (!ctx->graph[gv][s0]) {
       cudaGraph_t g;
       CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      int k = enqueue_step(ctx, s0);
+      int k = enqueue_step(ctx, s0, true);
       CU(cudaStreamEndCapture(ctx->stream, &g));
       if (int rc = check_launch(ctx, "step capture")) {
         cudaGraphDestroy(g);
         return rc;
       }
-      CU(cudaGraphInstantiate(&ctx->graph[s0], g, 0));
+      CU(cudaGraphInstantiate(&ctx->graph[gv][s0], g, 0));
       cudaGraphDestroy(g);
-      ctx->graph_kernels = k;
+      ctx->graph_kernels[gv] = k;
     }
-    CU(cudaGraphLaunch(ctx->graph[s0], ctx->stream));
-    ctx->launches += ctx->graph_kernels;
+    CU(cudaGraphLaunch(ctx->graph[gv][s0], ctx->stream));
+    ctx->launches += ctx->graph_kernels[gv];
     ctx->dt_valid = fused_dt(ctx);
+    ctx->ghost_valid = ctx->img_ok;
     ctx->po = s0;
     ctx->cur = step_final_index(ctx, s0);
   }
@@ -1544,11 +1632,10 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
     int pc = s0;
     for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
       int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
-      if (ctx->nghost) {
-        launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
-                           ctx->stream);
+      const int ng = enqueue_stage_ghosts(ctx, pc, irk == 1 ? ctx->ghost_valid : true);
+      if (ng) {
         mark(1);
-        launches[1] += 1;
+        launches[1] += ng;
       }
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
       if (irk == ctx->cfg.n_rk && fused_dt(ctx)) fuse_next_dt(ctx, a);
@@ -1557,6 +1644,7 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
       pc = pn;
     }
     ctx->dt_valid = fused_dt(ctx);
+    ctx->ghost_valid = ctx->img_ok;
     ctx->po = s0;
     ctx->cur = pc;
   }
@@ -1713,7 +1801,17 @@ static int enqueue_record(mose_gpu_ctx* ctx, int cnt) {
                     ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0, 0, ctx->uniform, st);
   int kern = 2;
   const int nrk = ctx->cfg.n_rk;
+  // the exact precision folds each next dt into the last stage; the others
+  // take it from the standalone pass, as their forward did
+  const bool fuse_ok = ctx->cfg.precision == MOSE_PRECISION_FP64_EXACT;
   for (int k = 0; k < cnt; ++k) {
+    if (k > 0 && !fuse_ok) {
+      launch_step_begin(ctx->dtmin.p, 1e5, nullptr, st);
+      launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->adj_seg[3 * (size_t)k].p,
+                        ctx->margs(), ctx->dtl.p, ctx->dtmin.p, ctx->gas, ctx->cfg.cfl, ctx->ndir, ctx->nd, 0, 0, 0,
+                        ctx->uniform, st);
+      kern += 2;
+    }
     launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p, st);
     cudaMemcpyAsync(ctx->adj_dts.p + k, ctx->scal.p, sizeof(double), cudaMemcpyDeviceToDevice, st);
     ++kern;
@@ -1725,7 +1823,7 @@ static int enqueue_record(mose_gpu_ctx* ctx, int cnt) {
       a.Pc = Pc;
       a.Po = ctx->adj_seg[3 * (size_t)k].p;
       a.Pn = ctx->adj_seg[irk == nrk ? 3 * (size_t)(k + 1) : 3 * (size_t)k + irk].p;
-      const bool fuse = irk == nrk && k + 1 < cnt;
+      const bool fuse = fuse_ok && irk == nrk && k + 1 < cnt;
       if (fuse) fuse_next_dt(ctx, a);
       kern += launch_stage(ctx, a, fuse ? 2 : 0, ctx->cfg.precision, ctx->uniform);
     }
@@ -1901,6 +1999,7 @@ int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
                      ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   return MOSE_OK;
 }
 
@@ -1924,13 +2023,20 @@ int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval
   }
   rc = adj_segment_buffers(ctx, interval);
   if (rc) return rc;
+  ctx->adj_dt_standalone = ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT;
   for (int mck = 0; mck < nck; ++mck) {
     CU(cudaMemcpyAsync(ctx->adj_ckpt[mck].p, ctx->state[ctx->cur].p, ns * sizeof(double), cudaMemcpyDeviceToDevice,
                        ctx->stream));
     const int cnt = std::min(interval, nsteps - mck * interval);
     rc = mose_gpu_advance(ctx, cnt, nullptr, nullptr);
-    if (rc) return rc;
+    if (rc) {
+      ctx->adj_dt_standalone = false;
+      return rc;
+    }
   }
+  ctx->adj_dt_standalone = false;
+  ctx->dt_valid = false;   // the next fused step starts from the standalone pass
+  ctx->ghost_valid = false;
   // the objective on the final state
   const BlockDesc& d = ctx->desc[block - 1];
   const int nf = (face <= 2) ? d.nj : d.ni;
@@ -1981,6 +2087,7 @@ int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach) {
   // the forward run's time (the recompute advanced the device clock)
   ctx->h_time = h_time;
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   double h = 0.0;
   CU(cudaMemcpyAsync(&h, ctx->adj_scal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   rc = poll_device_error(ctx);
@@ -2007,6 +2114,7 @@ int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach) {
   // the state arenas still hold P^n
   ctx->h_time = h_time;
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   double h = 0.0;
   CU(cudaMemcpyAsync(&h, ctx->adj_scal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   rc = poll_device_error(ctx);
@@ -2086,6 +2194,7 @@ int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, dou
     ctx->cur = cur0;
     ctx->po = po0;
     ctx->dt_valid = false;
+    ctx->ghost_valid = false;
     return MOSE_OK;
   };
   auto trial = [&](int h, int w, int order, int ctas, double& ms) -> int {
@@ -2166,6 +2275,7 @@ int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, dou
   if (rc) return rc;
   if ((rc = restore())) return rc;
   ctx->dt_valid = false;
+  ctx->ghost_valid = false;
   (void)valid0;
   CU(cudaStreamSynchronize(ctx->stream));
   ctx->launches = launches0;   // the trials are not the caller's steps

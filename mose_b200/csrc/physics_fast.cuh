@@ -55,9 +55,14 @@ __device__ __forceinline__ double sqrt_(double x) {
   return x > 0.0 ? s : 0.0;
 }
 __device__ __forceinline__ double div_(double a, double b) { return a * rcp(b); }
+// Sign tests on the high word, on the integer pipe instead of the FP64 one
+// (the stage kernels are bound by the FP64 pipe): sgn_neg(x) for x < 0 or
+// -0 (or a NaN with the sign bit set), pos_(x) for x > 0 (or a positive NaN).
+__device__ __forceinline__ bool sgn_neg(double x) { return __double2hiint(x) < 0; }
+__device__ __forceinline__ bool pos_(double x) { return __double_as_longlong(x) > 0; }
 // sqrt(x) = x rsqrt(x) without the residual correction (about 1.5 ulp): the
 // sound speeds of the Riemann solver, where that is far inside the bar
-__device__ __forceinline__ double sqrt1_(double x) { return x > 0.0 ? x * rsqrt_(x) : 0.0; }
+__device__ __forceinline__ double sqrt1_(double x) { return pos_(x) ? x * rsqrt_(x) : 0.0; }
 
 // ---- limiters: phi(r) x with r = y/(x + 1e-30), one reciprocal each --------
 // The rational limiters are rewritten over a common denominator, which is
@@ -184,13 +189,17 @@ __device__ __forceinline__ void hllc(const GasF& g, const double* L, const doubl
   const double vel2 = ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2];
   const double a_roe = sqrt1_(g.gm1 * fma(-0.5, vel2, h0_roe));
   const double un_roe = (NV == 5) ? ur[0] * n[0] + ur[1] * n[1] + ur[2] * n[2] : ur[0] * n[0] + ur[1] * n[1];
-  const double S1 = fmin(fmin(0.0, unl - aL), un_roe - a_roe);
-  const double S4 = fmax(fmax(0.0, unr + aR), un_roe + a_roe);
+  // min(0, unl - aL, un_roe - a_roe) and max(0, unr + aR, un_roe + a_roe),
+  // the comparisons with 0 as sign tests
+  const double t1 = unl - aL, t4 = unr + aR;
+  const double S1 = fmin(sgn_neg(t1) ? t1 : 0.0, un_roe - a_roe);
+  const double S4 = fmax(sgn_neg(t4) ? 0.0 : t4, un_roe + a_roe);
   const double ml = rl * (S1 - unl), mr = rr * (S4 - unr);
   const double idn = rcp(ml - mr);
   const double Sstar = (R[P] - L[P] + ml * unl - mr * unr) * idn;
-  // upwind side K: left when S1 >= 0 or Sstar >= 0
-  const bool left = (S1 >= 0.0) || (Sstar >= 0.0);
+  // upwind side K: left when S1 >= 0 or Sstar >= 0 (a -0 takes the other
+  // branch, to which the flux is continuous)
+  const bool left = !sgn_neg(S1) || !sgn_neg(Sstar);
   const double* K = left ? L : R;
   const double rk = left ? rl : rr, unk = left ? unl : unr, h0k = left ? h0l : h0r;
   const double SK = left ? S1 : S4;
@@ -200,7 +209,7 @@ __device__ __forceinline__ void hllc(const GasF& g, const double* L, const doubl
   for (int d = 0; d < NV - 2; ++d) F[1 + d] = fma(F[0], K[1 + d], pk * n[d]);
   F[P] = F[0] * h0k;
   // star correction, applied when K's outer wave is subsonic in the face frame
-  const bool corr = left ? (S1 < 0.0) : (S4 > 0.0);
+  const bool corr = left ? sgn_neg(S1) : pos_(S4);
   const double mk = left ? ml : mr;                        // rho_K (S_K - un_K)
   const double pstar = fma(rl * (unl - S1), unl - Sstar, L[P]);
   const double inv = rcp(SK - Sstar);
@@ -546,8 +555,11 @@ __device__ __forceinline__ bool rk_update(const GasF& g, double* Q, const double
   }
   Q[P] = g.gm1 * fma(-0.5, ke, U[P]);
   // A NaN in any conserved variable reaches p (through 1/rho, the velocities
-  // or E), so one ordered compare finds NaN or p < 0 (Lib_Newstate.f90:334-338).
-  const bool bad = !(Q[P] >= 0.0);
+  // or E), so one test finds NaN or p < 0 (Lib_Newstate.f90:334-338): as an
+  // unsigned integer, every bit pattern above +inf is a negative number or a
+  // NaN (-0 excepted, which is not below 0).
+  const unsigned long long pb = (unsigned long long)__double_as_longlong(Q[P]);
+  const bool bad = pb > 0x7ff0000000000000ULL && pb != 0x8000000000000000ULL;
   if (Q[0] < 1e-20) Q[0] = 1e-20;
   return !bad;
 }

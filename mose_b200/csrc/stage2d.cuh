@@ -271,7 +271,12 @@ struct PolFast {
   __device__ static bool face(const Gas& g, const double* QL, const double* QR, const double* n, double A,
                               double* F, double beta = 1.0) {
     constexpr int P = NV - 1;
-    bool ok = (QL[0] > 0.0 && QL[P] > 0.0 && QR[0] > 0.0 && QR[P] > 0.0);
+    // check_gas_state (x > 0) on the integer pipe: x in (0, +inf] as bit
+    // patterns, which leaves out -0, negatives and NaNs
+    auto pos_fin = [](double x) {
+      return (unsigned long long)(__double_as_longlong(x) - 1) < 0x7ff0000000000000ULL;
+    };
+    bool ok = pos_fin(QL[0]) && pos_fin(QL[P]) && pos_fin(QR[0]) && pos_fin(QR[P]);
     const fast::GasF gf = fast::gasf(g);
     if constexpr (RIE == 0) {
       if constexpr (MIXED) fast::hllc_mixed<NV>(gf, QL, QR, n, F);
@@ -878,6 +883,25 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
           double* Pn = a.Pn + d.sbase;
 #pragma unroll
           for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
+          if (a.img) {
+            // the ghosts of connected blocks that copy this cell (Ghost_Connection,
+            // Lib_Ghost.f90:140-160), written with the new state so the next
+            // stage needs no ghost-fill pass for them
+            auto put = [&](int f, int pos, int delta) {
+              const int base = d.imgoff[f];
+              if (base < 0) return;
+              const int4 t = a.img[base + pos];
+              if (t.x < 0) return;
+              const BlockDesc& bt = a.blk[t.x];
+              double* dst = a.Pn + bt.sbase + (delta == 0 ? t.y : t.z);
+#pragma unroll
+              for (int v = 0; v < NV; ++v) dst[v * bt.vstride] = Q[v];
+            };
+            if (c < 2) put(0, j, c);
+            if (c >= ni - 2) put(1, j, ni - 1 - c);
+            if (j < 2) put(2, c, j);
+            if (j >= nj - 2) put(3, c, nj - 1 - j);
+          }
           if constexpr (MODE == 2) {   // Compute_dt of the next step on the new state
             double dtc;
             if constexpr (MX) dtc = cfl_dt32(a.g, Q, d, a.ndir, a.cfl);
