@@ -268,8 +268,9 @@ int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on);
 /* irs-beta (Register_Numerics.f90): implicit residual smoothing of every RK
  * stage's residual when beta > 0 (Lib_IRS.f90, Newstate_Conservative's IRS
  * branch Lib_Newstate.f90:40-72); 0 (the default) disables it.  Call before
- * mose_gpu_setup.  2-D, exact precision: the stage's residual-only kernel,
- * then the smoothing kernels, then the update. */
+ * mose_gpu_setup.  2-D, exact or fp64 precision: the stage's residual-only
+ * kernel in that precision, then the smoothing kernels and the update in
+ * the reference's arithmetic. */
 int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta);
 
 /* equations = navier-stokes (Global_m model): model 1 adds the laminar

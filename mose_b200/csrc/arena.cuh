@@ -53,12 +53,6 @@ struct StageArgs {
   // Navier-Stokes connection faces: per 101 / 201 face cell the source stencil
   // of its viscous flux (VConn), indexed by the boundary word's parameter
   const int* vconn;
-  // Connection images (2-D fused stages; null: the ghost-fill kernel fills
-  // every ghost).  Entry BlockDesc::imgoff[f] + p of a cell at position p
-  // along face f: (target block, offset in its plane of the first ghost
-  // layer that copies the face cell, offset of the second one, which copies
-  // the next cell inward; target block -1: none).
-  const int4* img;
 };
 
 }  // namespace mose

@@ -25,6 +25,10 @@ constexpr int SB_X = 64;
 constexpr int SB_Y = 4;
 constexpr int SB_T = SB_X * SB_Y;
 constexpr int SB_W = SB_X - 2;
+// Fused 3-D stage tiling: a CTA of SB_T threads owns T3X x T3Y cells of a
+// block's (i, j) plane and marches in k.
+constexpr int T3X = 32;
+constexpr int T3Y = SB_T / T3X;
 
 // Internal boundary codes (reference bc.txt types in parentheses).
 enum BcCode : int {
@@ -89,10 +93,6 @@ struct BlockDesc {
   long long mbase;      // offset of this block in the one-plane arenas
   int bcoff[6];         // offset of face f's per-cell BC words in the BC table
   int bcn[6];           // number of face cells on face f
-  // 2-D connection images: offset of face f's entries in the image table
-  // (one per face cell: the ghosts of a connected block that copy it), -1
-  // when no connection reads this face
-  int imgoff[4];
   // Uniform metrics (valid when the context runs the constant-metric kernels)
   double u_dl[3];
   double u_n[3][3];     // face normal per direction

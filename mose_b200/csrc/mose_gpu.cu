@@ -122,32 +122,19 @@ std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int gri
   return best;
 }
 
-// Work items of the 3-D sweeps.  [0] i-sweep: (block, c0 | c1 << 16, r0, r1)
-// over rows r = j + nj k, strips as in 2-D, runs of up to 64 rows; [1] j-march
-// and [2] k-march: (block, q0, m0, m1), 256 consecutive columns q of the
-// block's (i, k) or (i, j) plane marching m over runs of at most 32 cells
-// (the marches are latency-bound: shorter runs give more items per wave of
-// the persistent grid and a shorter tail, for one extra face flux per run).
+// Work items of the fused 3-D stage: (block, i0 | j0 << 16, k0, k1), tiles
+// of T3X x T3Y cells of the block's (i, j) plane marching k over runs of at
+// most 32 planes (shorter runs give more items per wave of the persistent
+// grid and a shorter tail, for one extra k-face flux and two slopes per run).
 void plan_3d_items(const std::vector<HostBlock>& blocks, std::vector<int4> out[3]) {
   for (int q = 0; q < 3; ++q) out[q].clear();
   for (int b = 0; b < (int)blocks.size(); ++b) {
     const HostBlock& h = blocks[b];
-    const int ns = (h.ni + SB_W - 1) / SB_W;
-    const std::vector<int> cc = split_even(h.ni, ns, 2);
-    const int rows = h.nj * h.nk;
-    const std::vector<int> rc = split_even(rows, (rows + 63) / 64, SB_Y);
-    for (size_t r = 0; r + 1 < rc.size(); ++r)
-      for (int s = 0; s < ns; ++s)
-        if (rc[r + 1] > rc[r] && cc[s + 1] > cc[s])
-          out[0].push_back(make_int4(b, cc[s] | (cc[s + 1] << 16), rc[r], rc[r + 1]));
-    for (int dir = 1; dir <= 2; ++dir) {
-      const int nl = dir == 1 ? h.nj : h.nk, nother = dir == 1 ? h.nk : h.nj;
-      const int ncol = h.ni * nother;
-      const std::vector<int> mc = split_even(nl, (nl + 31) / 32, 1);
-      for (size_t r = 0; r + 1 < mc.size(); ++r)
-        for (int q0 = 0; q0 < ncol; q0 += SB_T)
-          if (mc[r + 1] > mc[r]) out[dir].push_back(make_int4(b, q0, mc[r], mc[r + 1]));
-    }
+    const std::vector<int> kc = split_even(h.nk, (h.nk + 31) / 32, 1);
+    for (size_t r = 0; r + 1 < kc.size(); ++r)
+      for (int j0 = 0; j0 < h.nj; j0 += T3Y)
+        for (int i0 = 0; i0 < h.ni; i0 += T3X)
+          if (kc[r + 1] > kc[r]) out[0].push_back(make_int4(b, i0 | (j0 << 16), kc[r], kc[r + 1]));
   }
 }
 
@@ -218,14 +205,7 @@ struct mose_gpu_ctx {
   // of the fused one, so the dt argmin of the reverse sweep finds the cell
   // that set it.
   bool adj_dt_standalone = false;
-  // Connection images (2-D fused stages): the stage kernels write the ghosts
-  // that 101 / 201 records copy; the ghost-fill kernel then runs only the
-  // other records (ghosts_nc).  ghost_valid: the current state's connection
-  // ghosts were written with it.
-  bool img_ok = false, ghost_valid = false;
-  DevBuf<int4> img;
-  DevBuf<GhostRec> ghosts_nc;
-  int nghost_nc = 0;
+
   // dtmin holds the CFL minimum of state[cur], folded in by the last RK stage
   // of the previous fused step; cleared by every call that changes the state
   bool dt_valid = false;
@@ -604,8 +584,9 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       if (h.ni < 3 || (h.nj < 3 && h.nj != 1))
         return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector needs blocks of at least 3 x 3 cells, or 1-D rows");
   }
-  if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT))
-    return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs on 2-D domains in the exact precision");
+  if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision == MOSE_PRECISION_MIXED))
+    return fail(ctx, MOSE_ERR_UNSUPPORTED,
+                "implicit residual smoothing runs on 2-D domains in the exact and fp64 precisions");
   if (ctx->gas.model > 0) {
     if (ctx->nd != 2 || ctx->ndir != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT ||
         ctx->cfg.integration != MOSE_INTEGRATION_CONS || ctx->irs_beta > 0.0 || ctx->gas.sd != 0)
@@ -986,49 +967,6 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
   if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
 
-  // ---- connection images of the 2-D fused stages -------------------------------
-  // Each connection ghost g = 1, 2 of a record copies the source cell g - 1
-  // steps inward from the source face; indexed by the source face cell, the
-  // table names the two ghosts.  Used when every source face cell feeds at
-  // most one record, for the fused (not IRS, not viscous) stages.
-  {
-    for (auto& d : ctx->desc)
-      for (int f = 0; f < 4; ++f) d.imgoff[f] = -1;
-    ctx->img_ok = false;
-    std::vector<int4> table;
-    std::vector<GhostRec> nc;
-    bool ok = ctx->nd == 2 && ctx->irs_beta == 0.0 && ctx->gas.model == 0;
-    for (const GhostRec& g : gr) {
-      if (g.type != BC_CONN) { nc.push_back(g); continue; }
-      if (!ok) continue;
-      BlockDesc& sd = ctx->desc[g.bs];
-      if (g.fs > 4) { ok = false; continue; }
-      if (sd.imgoff[g.fs - 1] < 0) {
-        sd.imgoff[g.fs - 1] = (int)table.size();
-        table.resize(table.size() + ((g.fs <= 2) ? sd.nj : sd.ni), int4{-1, 0, 0, 0});
-      }
-      const int pos = (g.fs <= 2) ? g.js : g.is;
-      int4& t = table[sd.imgoff[g.fs - 1] + pos];
-      if (t.x >= 0) { ok = false; continue; }   // a face cell feeding two records
-      const BlockDesc& td = ctx->desc[g.b];
-      const int gi = (g.f == 1) ? 1 : (g.f == 2) ? -1 : 0, gj = (g.f == 3) ? 1 : (g.f == 4) ? -1 : 0;
-      t = int4{g.b, (int)cell_off2(td, g.i - gi, g.j - gj), (int)cell_off2(td, g.i - 2 * gi, g.j - 2 * gj), 0};
-    }
-    if (ok && !table.empty()) {
-      ctx->img_ok = true;
-      CU(ctx->img.alloc(table.size()));
-      CU(cudaMemcpyAsync(ctx->img.p, table.data(), table.size() * sizeof(int4), cudaMemcpyHostToDevice, ctx->stream));
-      ctx->nghost_nc = (int)nc.size();
-      CU(ctx->ghosts_nc.alloc(std::max<size_t>(nc.size(), 1)));
-      if (!nc.empty())
-        CU(cudaMemcpyAsync(ctx->ghosts_nc.p, nc.data(), nc.size() * sizeof(GhostRec), cudaMemcpyHostToDevice,
-                           ctx->stream));
-    } else {
-      for (auto& d : ctx->desc)
-        for (int f = 0; f < 4; ++f) d.imgoff[f] = -1;
-    }
-    CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
-  }
 
   // ---- implicit residual smoothing: first-layer ghost records of R ----------------
   if (ctx->irs_beta > 0.0) {
@@ -1102,7 +1040,6 @@ static int prim_io(mose_gpu_ctx* ctx, int32_t b, double* P, int arena, bool uplo
   if (arena == -2 && !ctx->lam.p) return fail(ctx, MOSE_ERR_NOT_READY, "no adjoint state yet");
   if (upload) {
     ctx->dt_valid = false;
-    ctx->ghost_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, P, 5 * n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_ref_to_soa(ctx->d_desc.p, b - 1, n, ctx->staging.p, dst, ctx->nv, ctx->nd, ctx->stream);
     ctx->launches++;
@@ -1144,7 +1081,6 @@ static int dt_io(mose_gpu_ctx* ctx, int32_t b, double* dt, bool upload) {
   if (rc) return rc;
   if (upload) {
     ctx->dt_valid = false;
-    ctx->ghost_valid = false;
     CU(cudaMemcpyAsync(ctx->staging.p, dt, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     launch_plane_io(ctx->d_desc.p, b - 1, n, ctx->dtl.p, ctx->staging.p, ctx->nd, 0, ctx->stream);
   } else {
@@ -1175,7 +1111,6 @@ int mose_gpu_compute_dt(mose_gpu_ctx* ctx, double cfl, int32_t iter, int32_t ram
   if (rc) return rc;
   if (!dtglobal) return MOSE_ERR_INVALID;
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   launch_step_begin(ctx->dtmin.p, *dtglobal, nullptr, ctx->stream);
   launch_compute_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[ctx->cur].p, ctx->margs(),
                     ctx->dtl.p, ctx->dtmin.p, ctx->gas, cfl, ctx->ndir, ctx->nd, iter, ramp_iter, 1, ctx->uniform,
@@ -1192,7 +1127,6 @@ int mose_gpu_set_global_dt(mose_gpu_ctx* ctx, double dtglobal) {
   int rc = require_ready(ctx);
   if (rc) return rc;
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   CU(cudaMemcpyAsync(ctx->scal.p, &dtglobal, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   launch_set_global_dt(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->dtl.p, ctx->scal.p, ctx->nd,
                        ctx->stream);
@@ -1206,7 +1140,6 @@ int mose_gpu_copy_state(mose_gpu_ctx* ctx) {
   int rc = require_ready(ctx);
   if (rc) return rc;
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   ctx->po = (ctx->cur + 1) % 3;
   CU(cudaMemcpyAsync(ctx->state[ctx->po].p, ctx->state[ctx->cur].p, ctx->state[0].n * sizeof(double),
                      cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1251,20 +1184,12 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   }
   a.grid_cap = ctx->tile_ctas;
   a.vconn = ctx->vconn.p;
-  a.img = ctx->img_ok ? ctx->img.p : nullptr;
   return a;
 }
 
-// The ghost layers of the stage input pc: every record, or, when the stages
-// write their connection images and pc's connection ghosts were written with
-// it, the other records only.  Returns the number of kernels enqueued.
-static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc, bool conn_valid) {
-  if (ctx->img_ok && conn_valid) {
-    if (!ctx->nghost_nc) return 0;
-    launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts_nc.p, ctx->nghost_nc, ctx->state[pc].p, ctx->margs(), ctx->nd,
-                       ctx->derr.p, ctx->stream);
-    return 1;
-  }
+// The ghost layers of the stage input pc (Fill_Ghost_Cell).  Returns the
+// number of kernels enqueued.
+static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc) {
   launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
                      ctx->stream);
   return ctx->nghost ? 1 : 0;
@@ -1276,7 +1201,7 @@ static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc, bool conn_valid) {
 static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int prec, bool uni) {
   if (ctx->nd == 3)
     return launch_stage3d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
-               ? (ctx->nitems3[0] > 0 ? 3 : 2)
+               ? (ctx->nitems3[0] > 0 ? 1 : 0)
                : 0;
   if (a.nitems > 0 && a.nitems_nb > 0) {
     // The boundary-free items and the boundary items write disjoint cells
@@ -1344,7 +1269,6 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
   if (irk < 1 || irk > ctx->cfg.n_rk) return fail(ctx, MOSE_ERR_INVALID, "irk out of range");
   static const double RKcoeff[3][3] = {{1.0, 0.0, 0.0}, {1.0, 0.50, 0.0}, {1.0, 0.25, 2.0 / 3.0}};
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   if (ctx->irs_beta > 0.0) {
     // RK_Newstate with IRS on the residual of mose_gpu_residual, dt from
     // dtlocal (Compute_dt / Set_Global_dt of the phase path)
@@ -1431,7 +1355,11 @@ static int enqueue_irs_smoothing(mose_gpu_ctx* ctx) {
 // arena pc (PO = arena s0) into arena pn.
 static int enqueue_irs_stage(mose_gpu_ctx* ctx, int pc, int s0, int pn, int irk) {
   StageArgs a = stage_args(ctx, pc, s0, -1, irk);
-  int k = launch_stage(ctx, a, 1, MOSE_PRECISION_FP64_EXACT, false);
+  // the residual in the context's arithmetic (exact, or fp64 with the
+  // constant metrics of uniform grids); the smoothing and the update in the
+  // reference's
+  const bool fp64 = ctx->cfg.precision == MOSE_PRECISION_FP64;
+  int k = launch_stage(ctx, a, 1, fp64 ? MOSE_PRECISION_FP64 : MOSE_PRECISION_FP64_EXACT, fp64 && ctx->uniform);
   const int nb = (int)ctx->hblk.size();
   launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[pc].p, ctx->resid.p, ctx->margs(), ctx->dtl.p,
                    ctx->scal.p, ctx->cfg.time_accurate, ctx->gas, ctx->stream);
@@ -1450,7 +1378,7 @@ static int enqueue_series(mose_gpu_ctx* ctx) {
   return 1;
 }
 
-static int enqueue_step(mose_gpu_ctx* ctx, int s0, bool ghosts_valid) {
+static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
   int k = 0;
   if (!fused_dt(ctx)) k += enqueue_dt_pass(ctx, s0);
   launch_step_dt_take(ctx->dtmin.p, ctx->scal.p, ctx->scal.p + 1, ctx->cfg.time_accurate, 1e5, ctx->iterdev.p,
@@ -1459,8 +1387,7 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0, bool ghosts_valid) {
   int pc = s0;
   for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
     int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
-    // the stages after the first read the images the stage before wrote
-    k += enqueue_stage_ghosts(ctx, pc, irk == 1 ? ghosts_valid : true);
+    k += enqueue_stage_ghosts(ctx, pc);
     if (ctx->irs_beta > 0.0) {
       k += enqueue_irs_stage(ctx, pc, s0, pn, irk);
     } else if (ctx->gas.model > 0) {
@@ -1496,11 +1423,10 @@ int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
   CU(cudaMemcpyAsync(ctx->iterdev.p, &ctx->h_iter, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
   int s0 = ctx->cur;
   if (fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, s0);
-  ctx->launches += enqueue_step(ctx, s0, ctx->ghost_valid);
+  ctx->launches += enqueue_step(ctx, s0);
   rc = check_launch(ctx, "step");
   if (rc) return rc;
   ctx->dt_valid = fused_dt(ctx);
-  ctx->ghost_valid = ctx->img_ok;
   ctx->po = s0;
   ctx->cur = step_final_index(ctx, s0);
   double h[2];
@@ -1517,15 +1443,13 @@ int mose_gpu_step(mose_gpu_ctx* ctx, double* dtglobal, double* time) {
 // captured on first use); the device time and iteration are already set.
 static int enqueue_graph_steps(mose_gpu_ctx* ctx, int nsteps) {
   if (nsteps > 0 && fused_dt(ctx) && !ctx->dt_valid) ctx->launches += enqueue_dt_pass(ctx, ctx->cur);
-  // the graphs start from current connection ghosts
-  if (nsteps > 0 && ctx->img_ok && !ctx->ghost_valid) ctx->launches += enqueue_stage_ghosts(ctx, ctx->cur, false);
   for (int n = 0; n < nsteps; ++n) {
     int s0 = ctx->cur;
     const int gv = ctx->adj_dt_standalone ? 1 : 0;
     if (!ctx->graph[gv][s0]) {
       cudaGraph_t g;
       CU(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-      int k = enqueue_step(ctx, s0, true);
+      int k = enqueue_step(ctx, s0);
       CU(cudaStreamEndCapture(ctx->stream, &g));
       if (int rc = check_launch(ctx, "step capture")) {
         cudaGraphDestroy(g);
@@ -1538,7 +1462,6 @@ static int enqueue_graph_steps(mose_gpu_ctx* ctx, int nsteps) {
     CU(cudaGraphLaunch(ctx->graph[gv][s0], ctx->stream));
     ctx->launches += ctx->graph_kernels[gv];
     ctx->dt_valid = fused_dt(ctx);
-    ctx->ghost_valid = ctx->img_ok;
     ctx->po = s0;
     ctx->cur = step_final_index(ctx, s0);
   }
@@ -1632,7 +1555,7 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
     int pc = s0;
     for (int irk = 1; irk <= ctx->cfg.n_rk; ++irk) {
       int pn = (irk == 1) ? (s0 + 1) % 3 : (pc == (s0 + 1) % 3 ? (s0 + 2) % 3 : (s0 + 1) % 3);
-      const int ng = enqueue_stage_ghosts(ctx, pc, irk == 1 ? ctx->ghost_valid : true);
+      const int ng = enqueue_stage_ghosts(ctx, pc);
       if (ng) {
         mark(1);
         launches[1] += ng;
@@ -1644,7 +1567,6 @@ int mose_gpu_time_kernels(mose_gpu_ctx* ctx, int32_t nsteps, double* ms, int32_t
       pc = pn;
     }
     ctx->dt_valid = fused_dt(ctx);
-    ctx->ghost_valid = ctx->img_ok;
     ctx->po = s0;
     ctx->cur = pc;
   }
@@ -1999,7 +1921,6 @@ int mose_gpu_set_inflow_mach(mose_gpu_ctx* ctx, double mach) {
                      ctx->stream));
   CU(cudaStreamSynchronize(ctx->stream));
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   return MOSE_OK;
 }
 
@@ -2036,7 +1957,6 @@ int mose_gpu_adjoint_forward(mose_gpu_ctx* ctx, int32_t nsteps, int32_t interval
   }
   ctx->adj_dt_standalone = false;
   ctx->dt_valid = false;   // the next fused step starts from the standalone pass
-  ctx->ghost_valid = false;
   // the objective on the final state
   const BlockDesc& d = ctx->desc[block - 1];
   const int nf = (face <= 2) ? d.nj : d.ni;
@@ -2087,7 +2007,6 @@ int mose_gpu_adjoint_backward(mose_gpu_ctx* ctx, double* dJ_dmach) {
   // the forward run's time (the recompute advanced the device clock)
   ctx->h_time = h_time;
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   double h = 0.0;
   CU(cudaMemcpyAsync(&h, ctx->adj_scal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   rc = poll_device_error(ctx);
@@ -2114,7 +2033,6 @@ int mose_gpu_adjoint_step(mose_gpu_ctx* ctx, double* dJ_dmach) {
   // the state arenas still hold P^n
   ctx->h_time = h_time;
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   double h = 0.0;
   CU(cudaMemcpyAsync(&h, ctx->adj_scal.p + 1, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
   rc = poll_device_error(ctx);
@@ -2194,7 +2112,6 @@ int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, dou
     ctx->cur = cur0;
     ctx->po = po0;
     ctx->dt_valid = false;
-    ctx->ghost_valid = false;
     return MOSE_OK;
   };
   auto trial = [&](int h, int w, int order, int ctas, double& ms) -> int {
@@ -2275,7 +2192,6 @@ int mose_gpu_autotune(mose_gpu_ctx* ctx, int32_t steps, int32_t* tiling_out, dou
   if (rc) return rc;
   if ((rc = restore())) return rc;
   ctx->dt_valid = false;
-  ctx->ghost_valid = false;
   (void)valid0;
   CU(cudaStreamSynchronize(ctx->stream));
   ctx->launches = launches0;   // the trials are not the caller's steps

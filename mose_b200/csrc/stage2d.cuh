@@ -883,25 +883,6 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
           double* Pn = a.Pn + d.sbase;
 #pragma unroll
           for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
-          if (a.img) {
-            // the ghosts of connected blocks that copy this cell (Ghost_Connection,
-            // Lib_Ghost.f90:140-160), written with the new state so the next
-            // stage needs no ghost-fill pass for them
-            auto put = [&](int f, int pos, int delta) {
-              const int base = d.imgoff[f];
-              if (base < 0) return;
-              const int4 t = a.img[base + pos];
-              if (t.x < 0) return;
-              const BlockDesc& bt = a.blk[t.x];
-              double* dst = a.Pn + bt.sbase + (delta == 0 ? t.y : t.z);
-#pragma unroll
-              for (int v = 0; v < NV; ++v) dst[v * bt.vstride] = Q[v];
-            };
-            if (c < 2) put(0, j, c);
-            if (c >= ni - 2) put(1, j, ni - 1 - c);
-            if (j < 2) put(2, c, j);
-            if (j >= nj - 2) put(3, c, nj - 1 - j);
-          }
           if constexpr (MODE == 2) {   // Compute_dt of the next step on the new state
             double dtc;
             if constexpr (MX) dtc = cfl_dt32(a.g, Q, d, a.ndir, a.cfl);

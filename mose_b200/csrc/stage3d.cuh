@@ -147,6 +147,230 @@ __device__ __noinline__ int bc_face(const StageArgs& a, int b, int f, int i, int
 
 }  // namespace s3
 
+// ---- fused stage -----------------------------------------------------------------
+// One kernel per RK stage: a CTA of T3X x T3Y threads owns a tile of cells
+// (i0 .. i0 + T3X - 1, j0 .. j0 + T3Y - 1) of one block and marches up a run of
+// k planes.  Per plane it stages the tile and a two-cell halo ring in i and j
+// in shared memory, forms the limited i- and j-slopes and every i- and j-face
+// flux of the tile (halo faces included) there, while each thread marches its
+// own column in k with the stencil P(k), P(k+1), P(k+2), the k-slope and the
+// lower k-face flux in registers.  Each cell's residual stays in registers in
+// the reference's order: interior i-faces, j-faces, k-faces, then the
+// boundary faces in face order 1..6, then Newstate (or R in residual mode)
+// and the next step's CFL dt.  R never goes through HBM.
+constexpr int H3X = T3X + 4, H3Y = T3Y + 4;  // plane region: the tile and two halo cells per side
+
+template <int NVS>
+struct Stage3dSmem {
+  double P[NVS][H3Y][H3X];          // plane k (region cells; the four corners are not used)
+  double dx[T3Y][H3X];              // dl along i on the tile rows (metric arrays only)
+  double dy[H3Y][T3X];              // dl along j on the tile columns
+  double sx[NVS][T3Y][T3X + 2];     // limited i-slope of cells i0 - 1 .. i0 + T3X
+  double sy[NVS][T3Y + 2][T3X];     // limited j-slope of cells j0 - 1 .. j0 + T3Y
+  double F[NVS][T3Y][T3X + 1];      // F(i0 - 1 + x + 1/2)
+  double G[NVS][T3Y + 1][T3X];      // G(j0 - 1 + y + 1/2)
+};
+constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5>); }
+
+// Items: (block, i0 | j0 << 16, k0, k1).
+template <class PH, int RIE, int LIM, bool UNI, int MODE>
+__global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* items, int nitems) {
+  using namespace s3;
+  extern __shared__ __align__(16) unsigned char smem3[];
+  Stage3dSmem<NV>& S = *reinterpret_cast<Stage3dSmem<NV>*>(smem3);
+  const int t = threadIdx.x, tx = t % T3X, ty = t / T3X;
+  double dtrun = __longlong_as_double(0x7ff0000000000000LL);
+#pragma unroll 1
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 item = items[it];
+    const int b = item.x, i0 = item.y & 0xffff, j0 = item.y >> 16, k0 = item.z, k1 = item.w;
+    const BlockDesc& d = a.blk[b];
+    const int ni = d.ni, nj = d.nj, nk = d.nk;
+    const long long vs = d.vstride;
+    const double* P = a.Pc + d.sbase;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool mine = i < ni && j < nj;
+    // ---- the k march of this thread's column: P(k+1), slope(k), H(k - 1/2) in
+    // registers; P(k) is the cell's own value in the staged plane
+    double p1[NV], s0[NV], Hm[NV];
+    double d0 = 0.0, d1 = 0.0;
+    auto ok3 = [&](int kk) { return off3(d, i, j, kk); };
+    if (mine) {
+      double pm2[NV], pm1[NV], sm1[NV], p0[NV];
+      loadQ(P, vs, ok3(k0 - 2), pm2);
+      loadQ(P, vs, ok3(k0 - 1), pm1);
+      loadQ(P, vs, ok3(k0), p0);
+      loadQ(P, vs, ok3(k0 + 1), p1);
+      const double dm2 = dl_at<UNI>(a, d, 2, ok3(k0 - 2)), dm1 = dl_at<UNI>(a, d, 2, ok3(k0 - 1));
+      d0 = dl_at<UNI>(a, d, 2, ok3(k0));
+      d1 = dl_at<UNI>(a, d, 2, ok3(k0 + 1));
+      lslope<PH, UNI>(pm2, pm1, p0, dm2, dm1, d0, sm1);
+      lslope<PH, UNI>(pm1, p0, p1, dm1, d0, d1, s0);
+      if (k0 > 0) {
+        double n[3];
+        const double A = face_at<UNI>(a, d, 2, ok3(k0), n);
+        const bool ok = face<PH, UNI>(a.g, pm1, sm1, dm1, p0, s0, d0, n, A, Hm);
+        if (!ok) report(a.err, 4, b, i, j, k0);
+      }
+    }
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+      __syncthreads();   // the previous plane's readers are done
+      // ---- stage plane k: rows j0 .. j0 + T3Y - 1 over columns i0 - 2 .. i0 + T3X + 1,
+      //      and columns i0 .. i0 + T3X - 1 over rows j0 - 2, j0 - 1, j0 + T3Y, j0 + T3Y + 1
+      for (int e = t; e < T3Y * H3X + 4 * T3X; e += SB_T) {
+        int cx, ry;
+        if (e < T3Y * H3X) { cx = e % H3X; ry = 2 + e / H3X; }
+        else { const int q = e - T3Y * H3X; cx = 2 + q % T3X; const int r = q / T3X; ry = r < 2 ? r : T3Y + r; }
+        const int ci = i0 - 2 + cx, cj = j0 - 2 + ry;
+        if (ci > ni + 1 || cj > nj + 1) continue;   // beyond a partial tile's ghosts
+        const long long o = off3(d, ci, cj, k);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) S.P[v][ry][cx] = P[v * vs + o];
+        if constexpr (!UNI) {
+          if (ry >= 2 && ry < T3Y + 2) S.dx[ry - 2][cx] = a.m.dl[3 * d.mbase + 0 * vs + o];
+          if (cx >= 2 && cx < T3X + 2) S.dy[ry][cx - 2] = a.m.dl[3 * d.mbase + 1 * vs + o];
+        }
+      }
+      __syncthreads();
+      auto dxat = [&](int y, int cx) -> double { if constexpr (UNI) return d.u_dl[0]; else return S.dx[y][cx]; };
+      auto dyat = [&](int ry, int x) -> double { if constexpr (UNI) return d.u_dl[1]; else return S.dy[ry][x]; };
+      // ---- limited slopes: i-slopes of cells i0 - 1 .. i0 + T3X (columns 1 .. T3X + 2),
+      //      j-slopes of cells j0 - 1 .. j0 + T3Y (rows 1 .. T3Y + 2)
+      for (int e = t; e < T3Y * (T3X + 2); e += SB_T) {
+        const int x = e % (T3X + 2), y = e / (T3X + 2);
+        const int ci = i0 - 1 + x, cj = j0 + y;
+        if (ci > ni || cj >= nj) continue;
+        double qa[NV], q[NV], qb[NV], sl[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y + 2][x]; q[v] = S.P[v][y + 2][x + 1]; qb[v] = S.P[v][y + 2][x + 2]; }
+        lslope<PH, UNI>(qa, q, qb, dxat(y, x), dxat(y, x + 1), dxat(y, x + 2), sl);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) S.sx[v][y][x] = sl[v];
+      }
+      for (int e = t; e < (T3Y + 2) * T3X; e += SB_T) {
+        const int x = e % T3X, y = e / T3X;
+        const int ci = i0 + x, cj = j0 - 1 + y;
+        if (ci >= ni || cj > nj) continue;
+        double qa[NV], q[NV], qb[NV], sl[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y][x + 2]; q[v] = S.P[v][y + 1][x + 2]; qb[v] = S.P[v][y + 2][x + 2]; }
+        lslope<PH, UNI>(qa, q, qb, dyat(y, x), dyat(y + 1, x), dyat(y + 2, x), sl);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) S.sy[v][y][x] = sl[v];
+      }
+      __syncthreads();
+      // ---- interior face fluxes of the tile: i-faces (i0 - 1 + x) + 1/2, j-faces (j0 - 1 + y) + 1/2
+      for (int e = t; e < T3Y * (T3X + 1); e += SB_T) {
+        const int x = e % (T3X + 1), y = e / (T3X + 1);
+        const int cl = i0 - 1 + x, cj = j0 + y;
+        if (cl < 0 || cl > ni - 2 || cj >= nj) continue;
+        double PL[NV], PR[NV], sL[NV], sR[NV], F[NV], n[3];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          PL[v] = S.P[v][y + 2][x + 1]; PR[v] = S.P[v][y + 2][x + 2];
+          sL[v] = S.sx[v][y][x]; sR[v] = S.sx[v][y][x + 1];
+        }
+        const double A = face_at<UNI>(a, d, 0, off3(d, cl + 1, cj, k), n);
+        const bool ok = face<PH, UNI>(a.g, PL, sL, dxat(y, x + 1), PR, sR, dxat(y, x + 2), n, A, F);
+        if (!ok) report(a.err, 4, b, cl, cj, k);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) S.F[v][y][x] = F[v];
+      }
+      for (int e = t; e < (T3Y + 1) * T3X; e += SB_T) {
+        const int x = e % T3X, y = e / T3X;
+        const int ci = i0 + x, cl = j0 - 1 + y;
+        if (ci >= ni || cl < 0 || cl > nj - 2) continue;
+        double PL[NV], PR[NV], sL[NV], sR[NV], G[NV], n[3];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+          PL[v] = S.P[v][y + 1][x + 2]; PR[v] = S.P[v][y + 2][x + 2];
+          sL[v] = S.sy[v][y][x]; sR[v] = S.sy[v][y + 1][x];
+        }
+        const double A = face_at<UNI>(a, d, 1, off3(d, ci, cl + 1, k), n);
+        const bool ok = face<PH, UNI>(a.g, PL, sL, dyat(y + 1, x), PR, sR, dyat(y + 2, x), n, A, G);
+        if (!ok) report(a.err, 4, b, ci, cl, k);
+#pragma unroll
+        for (int v = 0; v < NV; ++v) S.G[v][y][x] = G[v];
+      }
+      __syncthreads();
+      if (!mine) continue;
+      // ---- the k face above, then the residual of cell (i, j, k) in the reference's order
+      double p0[NV], p2[NV], s1[NV], Hp[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) p0[v] = S.P[v][ty + 2][tx + 2];
+      loadQ(P, vs, ok3(k + 2), p2);
+      const double d2 = dl_at<UNI>(a, d, 2, ok3(k + 2));
+      lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
+      if (k <= nk - 2) {
+        double n[3];
+        const double A = face_at<UNI>(a, d, 2, ok3(k + 1), n);
+        const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Hp);
+        if (!ok) report(a.err, 4, b, i, j, k);
+      }
+      const long long o = ok3(k);
+      ResAcc<NV, PH::kCompensated> R;
+      R.init();
+      if (i > 0) for (int v = 0; v < NV; ++v) R.add(v, -S.F[v][ty][tx]);
+      if (i < ni - 1) for (int v = 0; v < NV; ++v) R.add(v, S.F[v][ty][tx + 1]);
+      if (j > 0) for (int v = 0; v < NV; ++v) R.add(v, -S.G[v][ty][tx]);
+      if (j < nj - 1) for (int v = 0; v < NV; ++v) R.add(v, S.G[v][ty + 1][tx]);
+      if (k > 0) for (int v = 0; v < NV; ++v) R.add(v, -Hm[v]);
+      if (k < nk - 1) for (int v = 0; v < NV; ++v) R.add(v, Hp[v]);
+      // boundary faces in face order 1..6
+      if (i == 0 || i == ni - 1 || j == 0 || j == nj - 1 || k == 0 || k == nk - 1) {
+#pragma unroll 1
+        for (int f = 1; f <= 6; ++f) {
+          const bool on = (f == 1) ? i == 0 : (f == 2) ? i == ni - 1 : (f == 3) ? j == 0 : (f == 4) ? j == nj - 1
+                          : (f == 5) ? k == 0 : k == nk - 1;
+          if (!on) continue;
+          double F[NV];
+          const int mask = bc_face<PH, RIE, LIM, UNI>(a, b, f, i, j, k, F);
+          add_bc<NV>(R, F, (f % 2) ? -1.0 : 1.0, mask);
+        }
+      }
+      double Rv[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
+      if constexpr (MODE == 1) {
+        double* Rb = a.R + d.sbase;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Rb[v * vs + o] = Rv[v];
+      } else {
+        double vol;
+        if constexpr (UNI) vol = d.u_vol; else vol = a.m.vol[d.mbase + o];
+        const double dt = a.time_accurate ? *a.dtg : a.dtl[d.mbase + o];
+        double Q[NV], QO[NV];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Q[v] = p0[v];
+        const bool first = (a.irk == 1);
+        if (!first) loadQ(a.Po + d.sbase, vs, o, QO);
+        const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
+        if (!ok) report(a.err, 5, b, i, j, k);
+        double* Pn = a.Pn + d.sbase;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
+        if constexpr (MODE == 2) dtrun = fmin(dtrun, cfl_dt<NV, UNI, PH::kFast>(a.g, Q, d, a.m, o, a.ndir, a.cfl));
+      }
+#pragma unroll
+      for (int v = 0; v < NV; ++v) { p1[v] = p2[v]; s0[v] = s1[v]; Hm[v] = Hp[v]; }
+      d0 = d1;
+      d1 = d2;
+    }
+  }
+  if constexpr (MODE == 2) {
+    __shared__ double red[SB_T / 32];
+    for (int s = 16; s > 0; s >>= 1) dtrun = fmin(dtrun, __shfl_xor_sync(0xffffffffu, dtrun, s));
+    if ((t & 31) == 0) red[t >> 5] = dtrun;
+    __syncthreads();
+    if (t == 0) {
+      double v = red[0];
+      for (int w = 1; w < SB_T / 32; ++w) v = fmin(v, red[w]);
+      atomicMin(a.dtmin, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
 // ---- i-sweep ------------------------------------------------------------------
 // Items: (block, c0 | c1 << 16, r0, r1) with rows r = j + nj k.  A CTA takes
 // SB_Y rows at a time, SB_X thread columns on cells c0 - 1 .. c0 + 62.

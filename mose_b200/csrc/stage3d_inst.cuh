@@ -12,29 +12,24 @@
 
 namespace mose {
 
-template <class K>
-static int occupancy_grid(K kernel, int nitems, int nsm, int& occ) {
-  if (occ == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, SB_T, 0) != cudaSuccess || occ < 1) occ = 1;
-  }
-  const int g = occ * nsm;
-  return nitems < g ? nitems : g;
-}
-
-// One RK stage (or one residual evaluation, MODE 1): the i-sweep, the
-// j-march, then the k-march that finishes the residual.
+// One RK stage (or one residual evaluation, MODE 1): the fused tile march
+// over the block tiles of items3[0].
 template <int PREC, int RIE, int LIM, bool UNI, int MODE>
 static void launch3d(const StageArgs& a, int nsm, cudaStream_t s) {
   using PH = StagePolicy<PREC, RIE, LIM>;
-  static int occ[3] = {0, 0, 0};
-  if (a.nitems3[0] > 0) {
-    auto k0 = k_sweep3d_i<PH, RIE, LIM, UNI>;
-    k0<<<occupancy_grid(k0, a.nitems3[0], nsm, occ[0]), SB_T, 0, s>>>(a, a.items3[0], a.nitems3[0]);
+  constexpr size_t smem = stage3d_smem_bytes();
+  static int occ = 0;   // one per kernel instance
+  if (occ == 0) {
+    cudaFuncSetAttribute(k_stage3d<PH, RIE, LIM, UNI, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage3d<PH, RIE, LIM, UNI, MODE>, SB_T, smem) !=
+            cudaSuccess ||
+        occ < 1)
+      occ = 1;
   }
-  auto k1 = k_march3d<PH, RIE, LIM, UNI, 1, 3>;
-  k1<<<occupancy_grid(k1, a.nitems3[1], nsm, occ[1]), SB_T, 0, s>>>(a, a.items3[1], a.nitems3[1]);
-  auto k2 = k_march3d<PH, RIE, LIM, UNI, 2, MODE>;
-  k2<<<occupancy_grid(k2, a.nitems3[2], nsm, occ[2]), SB_T, 0, s>>>(a, a.items3[2], a.nitems3[2]);
+  const int n = a.nitems3[0];
+  if (n <= 0) return;
+  const int grid = n < occ * nsm ? n : occ * nsm;
+  k_stage3d<PH, RIE, LIM, UNI, MODE><<<grid, SB_T, smem, s>>>(a, a.items3[0], n);
 }
 
 template <int PREC, int RIE, int LIM>

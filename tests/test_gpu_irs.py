@@ -95,3 +95,19 @@ def test_prandtl_meyer_reference_inputs_bitwise(oracle_mod):
     s.advance(40)
     compare_state(s, o, 1)
     assert np.isfinite(s.compute_residual()).all()
+
+
+@pytest.mark.parametrize("name", ["quadrant_steady", "vortex_periodic"])
+def test_irs_fp64_precision(oracle_mod, name):
+    """IRS with the residual in the fp64 precision (the smoothing and the
+    update keep the reference's arithmetic): the states stay within the
+    normwise relative L-infinity bar of 1e-12 of the oracle over 3 steps."""
+    from mose_b200 import _lib
+    from tests.test_gpu_parity import _per_var_rel
+    case = IRS_CASES[name]()
+    o = oracle_mod.Oracle(case)
+    s = solver(case, precision=_lib.PRECISION_FP64)
+    for _ in range(3):
+        o.step()
+        s.explicit_step()
+    assert _per_var_rel(s, o, len(case.nodes)) <= 1e-12

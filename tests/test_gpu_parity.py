@@ -300,31 +300,3 @@ def test_device_error_reports_location(oracle_mod):
     with pytest.raises(MoseError) as ei:
         s.explicit_step()
     assert ei.value.code in (4, 5)
-
-
-def test_connection_ghosts_written_by_the_stages(oracle_mod):
-    """On a periodic block every ghost is a connection ghost, which the stage
-    kernels write with their new state: a graph-replayed step launches the
-    dt publish and one stage kernel per RK stage, and no ghost-fill kernel;
-    the states stay bit-identical to the oracle through uploads, phase calls
-    and further steps (each of which makes the next step refill the ghosts)."""
-    case = cases.isentropic_vortex(48, steps=4)
-    o = oracle_mod.Oracle(case)
-    s = solver(case)
-    s.advance(2)
-    n0 = s.launch_count
-    s.advance(3)
-    assert (s.launch_count - n0) == 3 * (1 + 3)
-    for _ in range(5):
-        o.step()
-    compare_state(s, o, 1)
-    s.upload_prim(1, s.download_prim(1))
-    o.step()
-    s.explicit_step()
-    compare_state(s, o, 1)
-    dto = o.step()[0]
-    assert s.run_phases() == dto
-    compare_state(s, o, 1)
-    o.step()
-    s.advance(1)
-    compare_state(s, o, 1)
