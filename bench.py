@@ -542,7 +542,45 @@ def extra_configs(local):
     rep.update(config_report("box3d_8x128^3_hllc_vanleer",
                              lambda: cases.periodic_box_3d(128, steps=50, seed=0), local, 50))
     rep.update(adjoint_report(local))
+    rep.update(viscous_report(local))
     return rep
+
+
+def viscous_report(local, n=512, steps=50):
+    """The Navier-Stokes path (model 1, laminar) on the shear layer between
+    walls, 2 x 2 blocks of 1024 x 512 cells on a warped mesh (2.1 M cells):
+    throughput of graph-replayed steps in the reference-exact precision (the
+    only one the viscous terms run in), and whether `steps` steps are bit
+    for bit those of the oracle's OpenMP build on the same inputs."""
+    import torch
+    from mose_b200 import Solver, cases
+    from mose_b200.cases import GC
+    from oracle import pyoracle
+    case = cases.shear_layer(n, nbx=2, nby=2, warp=0.05, mu=0.002, steps=steps, seed=0)
+    s = Solver(case, precision=precision_code("exact"), device=local)
+    st = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
+    s.advance(3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    s.advance(steps)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    s.close()
+    s = Solver(case, precision=precision_code("exact"), device=local)
+    s.advance(steps)
+    o = pyoracle.Oracle(case, nthreads=host_cores(), omp=True)
+    for _ in range(steps):
+        o.step()
+    same = all(np.array_equal(s.download_prim(b)[GC:-GC, GC:-GC, GC:-GC][..., [0, 1, 2, 4]],
+                              o.get_prim(b)[GC:-GC, GC:-GC, GC:-GC][..., [0, 1, 2, 4]]) for b in range(1, 5))
+    s.close()
+    return {"navier_stokes_shear_layer_2x2_blocks_1024x512": {
+        "cells": case.ncells, "steps": steps, "exact": {"value": case.ncells / (ms * 1e-3), "unit": "cell-updates/s",
+                                                        "ms_per_step": ms},
+        "bitwise_vs_oracle_after_steps": bool(same),
+        "terms": "HLLC + van Leer convective, laminar diffusive fluxes, 302 / 301 walls, 101 / 201 connections"}}
 
 
 def profile_adjoint(local):
@@ -724,6 +762,9 @@ def summary(line, headline):
         out["exact_bitwise_vs_oracle"] = e["exact"]["bitwise"]
     for cname, c in (line.get("configs") or {}).items():
         short = cname.split("_")[0]
+        if "navier" in cname:
+            out["navier_stokes"] = {"exact": _g(c["exact"]["value"], 3), "bitwise": c["bitwise_vs_oracle_after_steps"]}
+            continue
         if "adjoint" in cname:
             out["adjoint"] = {k: _g(c[k], 3) for k in ("backward_over_fp64_forward", "gradient_over_fp64_forward")
                               if k in c}

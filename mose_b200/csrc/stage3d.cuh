@@ -1,25 +1,13 @@
-// stage3d.cuh -- residual + RK-stage kernels for 3-D blocks: three directional
-// sweeps per RK stage over every block.
+// stage3d.cuh -- the fused residual + RK-stage kernel of 3-D blocks, one
+// launch per RK stage over every block (k_stage3d below).
 //
 // The reference accumulates a cell's residual in a fixed order: the interior
 // i-faces (low then high), the interior j-faces, the interior k-faces
 // (Mod_Fluxes.f90:89-179), then the boundary faces in face order 1..6
-// (BC_Fluxes walks the bc list, Mod_BC_Fluxes.f90:52-216).  The 3-D path keeps
-// that order with one kernel per direction and the residual in HBM between
-// them (FP64, so the round trip is exact):
-//   k_sweep3d_i:  R  = -F(i-1/2) + F(i+1/2)     (interior i-faces)
-//   k_march3d<1>: R += -G(j-1/2) + G(j+1/2)     (interior j-faces)
-//   k_march3d<2>: R += -H(k-1/2) + H(k+1/2), then the boundary-face terms of
-//                 faces 1..6, then Newstate (or R itself in residual mode) and
-//                 the next step's CFL dt on the new state.
-// The i-sweep exchanges slopes and face fluxes through shared memory along
-// rows of 62 cells (one halo column each side).  The j- and k-sweeps march:
-// each thread walks one column along j (or k) with the three-cell stencil, the
-// limited slope and the lower face flux in registers, so every interior face
-// flux is formed once and loads are coalesced across threads in i.
-// Boundary faces are formed only for boundary cells, in the last sweep: the
-// interior formula with the ghosts for connections (101/201, as
-// BC_Connection_Eul does), boundary_flux() for the other types.
+// (BC_Fluxes walks the bc list, Mod_BC_Fluxes.f90:52-216).  The kernel keeps
+// that order with the residual in registers.  Boundary faces are formed only
+// for boundary cells: the interior formula with the ghosts for connections
+// (101/201, as BC_Connection_Eul does), boundary_flux() for the other types.
 #pragma once
 
 #include "stage2d.cuh"
@@ -162,13 +150,16 @@ constexpr int H3X = T3X + 4, H3Y = T3Y + 4;  // plane region: the tile and two h
 
 template <int NVS>
 struct Stage3dSmem {
-  double P[NVS][H3Y][H3X];          // plane k (region cells; the four corners are not used)
+  double P[2][NVS][H3Y][H3X];       // planes k and k + 1 (in flight): region cells, corners unused
   double dx[T3Y][H3X];              // dl along i on the tile rows (metric arrays only)
   double dy[H3Y][T3X];              // dl along j on the tile columns
   double sx[NVS][T3Y][T3X + 2];     // limited i-slope of cells i0 - 1 .. i0 + T3X
   double sy[NVS][T3Y + 2][T3X];     // limited j-slope of cells j0 - 1 .. j0 + T3Y
   double F[NVS][T3Y][T3X + 1];      // F(i0 - 1 + x + 1/2)
   double G[NVS][T3Y + 1][T3X];      // G(j0 - 1 + y + 1/2)
+  double PO[2][NVS][T3Y][T3X];      // PO of the tile cells, planes k and k + 1
+  // the block's uniform metrics: dl (3), face normals (3 x 3), areas (3), volume
+  double um[16];
 };
 constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5>); }
 
@@ -190,6 +181,21 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
     const double* P = a.Pc + d.sbase;
     const int i = i0 + tx, j = j0 + ty;
     const bool mine = i < ni && j < nj;
+    const bool need_po = (MODE != 1) && (a.irk != 1);
+    const double dtg = (MODE != 1 && a.time_accurate) ? *a.dtg : 0.0;
+    // the face metric of the low face along dir of cell o: the uniform
+    // constants (shared memory) or the metric arrays
+    auto facek = [&](int dir, long long o, double* n) -> double {
+      if constexpr (UNI) {
+        n[0] = S.um[3 + 3 * dir]; n[1] = S.um[4 + 3 * dir]; n[2] = S.um[5 + 3 * dir];
+        return S.um[12 + dir];
+      } else {
+        return face_at<false>(a, d, dir, o, n);
+      }
+    };
+    auto dlk = [&](long long o) -> double {
+      if constexpr (UNI) return S.um[2]; else return a.m.dl[3 * d.mbase + 2 * vs + o];
+    };
     // ---- the k march of this thread's column: P(k+1), slope(k), H(k - 1/2) in
     // registers; P(k) is the cell's own value in the staged plane
     double p1[NV], s0[NV], Hm[NV];
@@ -213,98 +219,144 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
         if (!ok) report(a.err, 4, b, i, j, k0);
       }
     }
-#pragma unroll 1
-    for (int k = k0; k < k1; ++k) {
-      __syncthreads();   // the previous plane's readers are done
-      // ---- stage plane k: rows j0 .. j0 + T3Y - 1 over columns i0 - 2 .. i0 + T3X + 1,
-      //      and columns i0 .. i0 + T3X - 1 over rows j0 - 2, j0 - 1, j0 + T3Y, j0 + T3Y + 1
-      for (int e = t; e < T3Y * H3X + 4 * T3X; e += SB_T) {
+    // plane kk into buffer bf with 16-byte copies (two cells per copy; the
+    // region's rows start on even columns and the padded rows keep every copy
+    // inside the block's plane): rows j0 .. j0 + T3Y - 1 over columns
+    // i0 - 2 .. i0 + T3X + 1, and columns i0 .. i0 + T3X - 1 over rows j0 - 2,
+    // j0 - 1, j0 + T3Y, j0 + T3Y + 1
+    auto stage_plane = [&](int kk, int bf) {
+      constexpr int CA = H3X / 2, CB = T3X / 2;   // chunks per row
+      for (int e = t; e < T3Y * CA + 4 * CB; e += SB_T) {
         int cx, ry;
-        if (e < T3Y * H3X) { cx = e % H3X; ry = 2 + e / H3X; }
-        else { const int q = e - T3Y * H3X; cx = 2 + q % T3X; const int r = q / T3X; ry = r < 2 ? r : T3Y + r; }
+        if (e < T3Y * CA) { cx = 2 * (e % CA); ry = 2 + e / CA; }
+        else { const int q = e - T3Y * CA; cx = 2 + 2 * (q % CB); const int r = q / CB; ry = r < 2 ? r : T3Y + r; }
         const int ci = i0 - 2 + cx, cj = j0 - 2 + ry;
         if (ci > ni + 1 || cj > nj + 1) continue;   // beyond a partial tile's ghosts
-        const long long o = off3(d, ci, cj, k);
+        const long long o = off3(d, ci, cj, kk);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) S.P[v][ry][cx] = P[v * vs + o];
-        if constexpr (!UNI) {
+        for (int v = 0; v < NV; ++v) cp_async16(&S.P[bf][v][ry][cx], P + v * vs + o);
+      }
+      if (need_po) {
+        const double* Po = a.Po + d.sbase;
+        for (int e = t; e < T3Y * CB; e += SB_T) {
+          const int cx = 2 * (e % CB), y = e / CB;
+          const int ci = i0 + cx, cj = j0 + y;
+          if (ci >= ni || cj >= nj) continue;
+          const long long o = off3(d, ci, cj, kk);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) cp_async16(&S.PO[bf][v][y][cx], Po + v * vs + o);
+        }
+      }
+      cp_async_commit();
+    };
+    __syncthreads();   // the previous item's readers are done with both buffers
+    if constexpr (UNI) {
+      if (t < 3) S.um[t] = d.u_dl[t];
+      else if (t < 12) S.um[t] = d.u_n[(t - 3) / 3][(t - 3) % 3];
+      else if (t < 15) S.um[t] = d.u_A[t - 12];
+      else if (t == 15) S.um[15] = d.u_vol;
+    }
+    stage_plane(k0, 0);
+#pragma unroll 1
+    for (int k = k0; k < k1; ++k) {
+      const int bf = (k - k0) & 1;
+      __syncthreads();   // the previous plane's readers are done with buffer bf ^ 1
+      if (k + 1 < k1) stage_plane(k + 1, bf ^ 1);
+      else cp_async_commit();   // an empty group keeps the wait count uniform
+      // the column's P(k + 2), loaded early so its latency overlaps the plane's work
+      double p2[NV];
+      if (mine) loadQ(P, vs, ok3(k + 2), p2);
+      if constexpr (!UNI) {
+        for (int e = t; e < T3Y * H3X + 4 * T3X; e += SB_T) {
+          int cx, ry;
+          if (e < T3Y * H3X) { cx = e % H3X; ry = 2 + e / H3X; }
+          else { const int q = e - T3Y * H3X; cx = 2 + q % T3X; const int r = q / T3X; ry = r < 2 ? r : T3Y + r; }
+          const int ci = i0 - 2 + cx, cj = j0 - 2 + ry;
+          if (ci > ni + 1 || cj > nj + 1) continue;
+          const long long o = off3(d, ci, cj, k);
           if (ry >= 2 && ry < T3Y + 2) S.dx[ry - 2][cx] = a.m.dl[3 * d.mbase + 0 * vs + o];
           if (cx >= 2 && cx < T3X + 2) S.dy[ry][cx - 2] = a.m.dl[3 * d.mbase + 1 * vs + o];
         }
       }
+      cp_async_wait_prev();   // this thread's copies of plane k
       __syncthreads();
-      auto dxat = [&](int y, int cx) -> double { if constexpr (UNI) return d.u_dl[0]; else return S.dx[y][cx]; };
-      auto dyat = [&](int ry, int x) -> double { if constexpr (UNI) return d.u_dl[1]; else return S.dy[ry][x]; };
+      auto dxat = [&](int y, int cx) -> double { if constexpr (UNI) return S.um[0]; else return S.dx[y][cx]; };
+      auto dyat = [&](int ry, int x) -> double { if constexpr (UNI) return S.um[1]; else return S.dy[ry][x]; };
       // ---- limited slopes: i-slopes of cells i0 - 1 .. i0 + T3X (columns 1 .. T3X + 2),
       //      j-slopes of cells j0 - 1 .. j0 + T3Y (rows 1 .. T3Y + 2)
-      for (int e = t; e < T3Y * (T3X + 2); e += SB_T) {
-        const int x = e % (T3X + 2), y = e / (T3X + 2);
-        const int ci = i0 - 1 + x, cj = j0 + y;
-        if (ci > ni || cj >= nj) continue;
+      // (one index space for both, so the items beyond one per thread spread
+      // over different threads)
+      constexpr int NSX = T3Y * (T3X + 2), NSY = (T3Y + 2) * T3X;
+      for (int e = t; e < NSX + NSY; e += SB_T) {
         double qa[NV], q[NV], qb[NV], sl[NV];
+        if (e < NSX) {
+          const int x = e % (T3X + 2), y = e / (T3X + 2);
+          const int ci = i0 - 1 + x, cj = j0 + y;
+          if (ci > ni || cj >= nj) continue;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y + 2][x]; q[v] = S.P[v][y + 2][x + 1]; qb[v] = S.P[v][y + 2][x + 2]; }
-        lslope<PH, UNI>(qa, q, qb, dxat(y, x), dxat(y, x + 1), dxat(y, x + 2), sl);
+          for (int v = 0; v < NV; ++v) { qa[v] = S.P[bf][v][y + 2][x]; q[v] = S.P[bf][v][y + 2][x + 1]; qb[v] = S.P[bf][v][y + 2][x + 2]; }
+          lslope<PH, UNI>(qa, q, qb, dxat(y, x), dxat(y, x + 1), dxat(y, x + 2), sl);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) S.sx[v][y][x] = sl[v];
-      }
-      for (int e = t; e < (T3Y + 2) * T3X; e += SB_T) {
-        const int x = e % T3X, y = e / T3X;
-        const int ci = i0 + x, cj = j0 - 1 + y;
-        if (ci >= ni || cj > nj) continue;
-        double qa[NV], q[NV], qb[NV], sl[NV];
+          for (int v = 0; v < NV; ++v) S.sx[v][y][x] = sl[v];
+        } else {
+          const int e2 = e - NSX;
+          const int x = e2 % T3X, y = e2 / T3X;
+          const int ci = i0 + x, cj = j0 - 1 + y;
+          if (ci >= ni || cj > nj) continue;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y][x + 2]; q[v] = S.P[v][y + 1][x + 2]; qb[v] = S.P[v][y + 2][x + 2]; }
-        lslope<PH, UNI>(qa, q, qb, dyat(y, x), dyat(y + 1, x), dyat(y + 2, x), sl);
+          for (int v = 0; v < NV; ++v) { qa[v] = S.P[bf][v][y][x + 2]; q[v] = S.P[bf][v][y + 1][x + 2]; qb[v] = S.P[bf][v][y + 2][x + 2]; }
+          lslope<PH, UNI>(qa, q, qb, dyat(y, x), dyat(y + 1, x), dyat(y + 2, x), sl);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) S.sy[v][y][x] = sl[v];
+          for (int v = 0; v < NV; ++v) S.sy[v][y][x] = sl[v];
+        }
       }
       __syncthreads();
       // ---- interior face fluxes of the tile: i-faces (i0 - 1 + x) + 1/2, j-faces (j0 - 1 + y) + 1/2
-      for (int e = t; e < T3Y * (T3X + 1); e += SB_T) {
-        const int x = e % (T3X + 1), y = e / (T3X + 1);
-        const int cl = i0 - 1 + x, cj = j0 + y;
-        if (cl < 0 || cl > ni - 2 || cj >= nj) continue;
+      constexpr int NFX = T3Y * (T3X + 1), NFY = (T3Y + 1) * T3X;
+      for (int e = t; e < NFX + NFY; e += SB_T) {
         double PL[NV], PR[NV], sL[NV], sR[NV], F[NV], n[3];
+        if (e < NFX) {
+          const int x = e % (T3X + 1), y = e / (T3X + 1);
+          const int cl = i0 - 1 + x, cj = j0 + y;
+          if (cl < 0 || cl > ni - 2 || cj >= nj) continue;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          PL[v] = S.P[v][y + 2][x + 1]; PR[v] = S.P[v][y + 2][x + 2];
-          sL[v] = S.sx[v][y][x]; sR[v] = S.sx[v][y][x + 1];
+          for (int v = 0; v < NV; ++v) {
+            PL[v] = S.P[bf][v][y + 2][x + 1]; PR[v] = S.P[bf][v][y + 2][x + 2];
+            sL[v] = S.sx[v][y][x]; sR[v] = S.sx[v][y][x + 1];
+          }
+          const double A = facek(0, off3(d, cl + 1, cj, k), n);
+          const bool ok = face<PH, UNI>(a.g, PL, sL, dxat(y, x + 1), PR, sR, dxat(y, x + 2), n, A, F);
+          if (!ok) report(a.err, 4, b, cl, cj, k);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) S.F[v][y][x] = F[v];
+        } else {
+          const int e2 = e - NFX;
+          const int x = e2 % T3X, y = e2 / T3X;
+          const int ci = i0 + x, cl = j0 - 1 + y;
+          if (ci >= ni || cl < 0 || cl > nj - 2) continue;
+#pragma unroll
+          for (int v = 0; v < NV; ++v) {
+            PL[v] = S.P[bf][v][y + 1][x + 2]; PR[v] = S.P[bf][v][y + 2][x + 2];
+            sL[v] = S.sy[v][y][x]; sR[v] = S.sy[v][y + 1][x];
+          }
+          const double A = facek(1, off3(d, ci, cl + 1, k), n);
+          const bool ok = face<PH, UNI>(a.g, PL, sL, dyat(y + 1, x), PR, sR, dyat(y + 2, x), n, A, F);
+          if (!ok) report(a.err, 4, b, ci, cl, k);
+#pragma unroll
+          for (int v = 0; v < NV; ++v) S.G[v][y][x] = F[v];
         }
-        const double A = face_at<UNI>(a, d, 0, off3(d, cl + 1, cj, k), n);
-        const bool ok = face<PH, UNI>(a.g, PL, sL, dxat(y, x + 1), PR, sR, dxat(y, x + 2), n, A, F);
-        if (!ok) report(a.err, 4, b, cl, cj, k);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) S.F[v][y][x] = F[v];
-      }
-      for (int e = t; e < (T3Y + 1) * T3X; e += SB_T) {
-        const int x = e % T3X, y = e / T3X;
-        const int ci = i0 + x, cl = j0 - 1 + y;
-        if (ci >= ni || cl < 0 || cl > nj - 2) continue;
-        double PL[NV], PR[NV], sL[NV], sR[NV], G[NV], n[3];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          PL[v] = S.P[v][y + 1][x + 2]; PR[v] = S.P[v][y + 2][x + 2];
-          sL[v] = S.sy[v][y][x]; sR[v] = S.sy[v][y + 1][x];
-        }
-        const double A = face_at<UNI>(a, d, 1, off3(d, ci, cl + 1, k), n);
-        const bool ok = face<PH, UNI>(a.g, PL, sL, dyat(y + 1, x), PR, sR, dyat(y + 2, x), n, A, G);
-        if (!ok) report(a.err, 4, b, ci, cl, k);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) S.G[v][y][x] = G[v];
       }
       __syncthreads();
       if (!mine) continue;
       // ---- the k face above, then the residual of cell (i, j, k) in the reference's order
-      double p0[NV], p2[NV], s1[NV], Hp[NV];
+      double p0[NV], s1[NV], Hp[NV];
 #pragma unroll
-      for (int v = 0; v < NV; ++v) p0[v] = S.P[v][ty + 2][tx + 2];
-      loadQ(P, vs, ok3(k + 2), p2);
-      const double d2 = dl_at<UNI>(a, d, 2, ok3(k + 2));
+      for (int v = 0; v < NV; ++v) p0[v] = S.P[bf][v][ty + 2][tx + 2];
+      const double d2 = dlk(ok3(k + 2));
       lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
       if (k <= nk - 2) {
         double n[3];
-        const double A = face_at<UNI>(a, d, 2, ok3(k + 1), n);
+        const double A = facek(2, ok3(k + 1), n);
         const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Hp);
         if (!ok) report(a.err, 4, b, i, j, k);
       }
@@ -338,13 +390,16 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
         for (int v = 0; v < NV; ++v) Rb[v * vs + o] = Rv[v];
       } else {
         double vol;
-        if constexpr (UNI) vol = d.u_vol; else vol = a.m.vol[d.mbase + o];
-        const double dt = a.time_accurate ? *a.dtg : a.dtl[d.mbase + o];
+        if constexpr (UNI) vol = S.um[15]; else vol = a.m.vol[d.mbase + o];
+        const double dt = a.time_accurate ? dtg : a.dtl[d.mbase + o];
         double Q[NV], QO[NV];
 #pragma unroll
         for (int v = 0; v < NV; ++v) Q[v] = p0[v];
         const bool first = (a.irk == 1);
-        if (!first) loadQ(a.Po + d.sbase, vs, o, QO);
+        if (!first) {
+#pragma unroll
+          for (int v = 0; v < NV; ++v) QO[v] = S.PO[bf][v][ty][tx];
+        }
         const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
         if (!ok) report(a.err, 5, b, i, j, k);
         double* Pn = a.Pn + d.sbase;
@@ -360,204 +415,6 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
   }
   if constexpr (MODE == 2) {
     __shared__ double red[SB_T / 32];
-    for (int s = 16; s > 0; s >>= 1) dtrun = fmin(dtrun, __shfl_xor_sync(0xffffffffu, dtrun, s));
-    if ((t & 31) == 0) red[t >> 5] = dtrun;
-    __syncthreads();
-    if (t == 0) {
-      double v = red[0];
-      for (int w = 1; w < SB_T / 32; ++w) v = fmin(v, red[w]);
-      atomicMin(a.dtmin, (unsigned long long)__double_as_longlong(v));
-    }
-  }
-}
-
-// ---- i-sweep ------------------------------------------------------------------
-// Items: (block, c0 | c1 << 16, r0, r1) with rows r = j + nj k.  A CTA takes
-// SB_Y rows at a time, SB_X thread columns on cells c0 - 1 .. c0 + 62.
-template <class PH, int RIE, int LIM, bool UNI>
-__global__ void __launch_bounds__(SB_T, 2) k_sweep3d_i(StageArgs a, const int4* items, int nitems) {
-  using namespace s3;
-  __shared__ double sP[NV][SB_Y][SB_X + 2];
-  __shared__ double sD[SB_Y][SB_X + 2];
-  __shared__ double sS[NV][SB_Y][SB_X];
-  __shared__ double sF[NV][SB_Y][SB_X];
-  const int t = threadIdx.x, tx = t % SB_X, ty = t / SB_X;
-#pragma unroll 1
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int4 item = items[it];
-    const int b = item.x, c0 = item.y & 0xffff, c1 = item.y >> 16, r0 = item.z, r1 = item.w;
-    const BlockDesc& d = a.blk[b];
-    const int ni = d.ni, nj = d.nj;
-    const long long vs = d.vstride;
-    const double* P = a.Pc + d.sbase;
-    const int c = c0 - 1 + tx;
-#pragma unroll 1
-    for (int rb = r0; rb < r1; rb += SB_Y) {
-      const int r = rb + ty;
-      const bool rowok = r < r1;
-      const int j = rowok ? r % nj : 0, k = rowok ? r / nj : 0;
-      __syncthreads();
-      if (rowok) {
-        auto put = [&](int cc, int col) {
-          if (cc > ni + 1) return;
-          const long long o = off3(d, cc, j, k);
-#pragma unroll
-          for (int v = 0; v < NV; ++v) sP[v][ty][col] = P[v * vs + o];
-          sD[ty][col] = dl_at<UNI>(a, d, 0, o);
-        };
-        put(c, tx + 1);
-        if (tx == 0) put(c0 - 2, 0);
-        if (tx == SB_X - 1) put(c0 + SB_X - 1, SB_X + 1);
-      }
-      __syncthreads();
-      if (rowok && c <= ni) {
-        double qa[NV], q[NV], qb[NV], s[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) { qa[v] = sP[v][ty][tx]; q[v] = sP[v][ty][tx + 1]; qb[v] = sP[v][ty][tx + 2]; }
-        lslope<PH, UNI>(qa, q, qb, sD[ty][tx], sD[ty][tx + 1], sD[ty][tx + 2], s);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) sS[v][ty][tx] = s[v];
-      }
-      __syncthreads();
-      // interior face c + 1/2, 0 <= c <= ni - 2
-      if (rowok && tx < SB_X - 1 && c >= 0 && c <= ni - 2 && c <= c1 - 1) {
-        double PL[NV], PR[NV], sL[NV], sR[NV], F[NV], n[3];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) {
-          PL[v] = sP[v][ty][tx + 1]; PR[v] = sP[v][ty][tx + 2];
-          sL[v] = sS[v][ty][tx]; sR[v] = sS[v][ty][tx + 1];
-        }
-        const double A = face_at<UNI>(a, d, 0, off3(d, c + 1, j, k), n);
-        const bool ok = face<PH, UNI>(a.g, PL, sL, sD[ty][tx + 1], PR, sR, sD[ty][tx + 2], n, A, F);
-        if (!ok) report(a.err, 4, b, c, j, k);
-#pragma unroll
-        for (int v = 0; v < NV; ++v) sF[v][ty][tx] = F[v];
-      }
-      __syncthreads();
-      if (rowok && tx >= 1 && c < c1) {
-        ResAcc<NV, PH::kCompensated> R;
-        R.init();
-        if (c > 0) for (int v = 0; v < NV; ++v) R.add(v, -sF[v][ty][tx - 1]);
-        if (c < ni - 1) for (int v = 0; v < NV; ++v) R.add(v, sF[v][ty][tx]);
-        const long long o = off3(d, c, j, k);
-        double* Rb = a.R + d.sbase;
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Rb[v * vs + o] = R.get(v);
-      }
-    }
-  }
-}
-
-// ---- j- and k-sweeps ------------------------------------------------------------
-// DIR = 1 (j) or 2 (k).  Items: (block, q0, m0, m1): threads q0 .. q0 + 255 of
-// the block's columns q = i + ni * other (other = k for DIR 1, j for DIR 2)
-// march m = j (or k) over [m0, m1).  MODE: 3 = add the interior faces to R
-// (j-sweep); 0 = last sweep, fused Newstate; 1 = last sweep, residual only;
-// 2 = last sweep, fused Newstate and the next step's CFL dt.
-template <class PH, int RIE, int LIM, bool UNI, int DIR, int MODE>
-__global__ void __launch_bounds__(SB_T, 2) k_march3d(StageArgs a, const int4* items, int nitems) {
-  using namespace s3;
-  double dtrun = __longlong_as_double(0x7ff0000000000000LL);
-#pragma unroll 1
-  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-    const int4 item = items[it];
-    const int b = item.x, m0 = item.z, m1 = item.w;
-    const BlockDesc& d = a.blk[b];
-    const int ni = d.ni, nj = d.nj, nk = d.nk;
-    const int nl = (DIR == 1) ? nj : nk, nother = (DIR == 1) ? nk : nj;
-    const int q = item.y + threadIdx.x;
-    if (q >= ni * nother) continue;
-    const int i = q % ni, other = q / ni;
-    const long long vs = d.vstride;
-    const long long S = (DIR == 1) ? (long long)d.px : d.plane;   // stride along the march
-    const double* P = a.Pc + d.sbase;
-    double* Rb = a.R + d.sbase;
-    const long long obase = (DIR == 1) ? off3(d, i, 0, other) : off3(d, i, other, 0);   // cell m = 0
-    auto om = [&](int m) { return obase + (long long)m * S; };
-    // march state: P(m), P(m+1), slope(m), lower face flux G(m-1/2)
-    double p0[NV], p1[NV], p2[NV], s0[NV], s1[NV], Gm[NV], Gp[NV];
-    double d0, d1, d2;
-    {
-      double pm2[NV], pm1[NV], sm1[NV];
-      loadQ(P, vs, om(m0 - 2), pm2);
-      loadQ(P, vs, om(m0 - 1), pm1);
-      loadQ(P, vs, om(m0), p0);
-      loadQ(P, vs, om(m0 + 1), p1);
-      const double dm2 = dl_at<UNI>(a, d, DIR, om(m0 - 2)), dm1 = dl_at<UNI>(a, d, DIR, om(m0 - 1));
-      d0 = dl_at<UNI>(a, d, DIR, om(m0));
-      d1 = dl_at<UNI>(a, d, DIR, om(m0 + 1));
-      lslope<PH, UNI>(pm2, pm1, p0, dm2, dm1, d0, sm1);
-      lslope<PH, UNI>(pm1, p0, p1, dm1, d0, d1, s0);
-      if (m0 > 0) {
-        double n[3];
-        const double A = face_at<UNI>(a, d, DIR, om(m0), n);
-        const bool ok = face<PH, UNI>(a.g, pm1, sm1, dm1, p0, s0, d0, n, A, Gm);
-        const int jj = (DIR == 1) ? m0 : other, kk = (DIR == 1) ? other : m0;
-        if (!ok) report(a.err, 4, b, i, jj, kk);
-      }
-    }
-#pragma unroll 1
-    for (int m = m0; m < m1; ++m) {
-      loadQ(P, vs, om(m + 2), p2);
-      d2 = dl_at<UNI>(a, d, DIR, om(m + 2));
-      lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
-      const int j = (DIR == 1) ? m : other, k = (DIR == 1) ? other : m;
-      if (m <= nl - 2) {
-        double n[3];
-        const double A = face_at<UNI>(a, d, DIR, om(m + 1), n);
-        const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Gp);
-        if (!ok) report(a.err, 4, b, i, j, k);
-      }
-      const long long o = om(m);
-      ResAcc<NV, PH::kCompensated> R;
-      R.init();
-#pragma unroll
-      for (int v = 0; v < NV; ++v) R.s[v] = Rb[v * vs + o];
-      if (m > 0) for (int v = 0; v < NV; ++v) R.add(v, -Gm[v]);
-      if (m < nl - 1) for (int v = 0; v < NV; ++v) R.add(v, Gp[v]);
-      if constexpr (MODE == 3) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Rb[v * vs + o] = R.get(v);
-      } else {
-        // boundary faces in face order 1..6
-        const bool on[6] = {i == 0, i == ni - 1, j == 0, j == nj - 1, k == 0, k == nk - 1};
-        for (int f = 1; f <= 6; ++f) {
-          if (!on[f - 1]) continue;
-          double F[NV];
-          const int mask = bc_face<PH, RIE, LIM, UNI>(a, b, f, i, j, k, F);
-          add_bc<NV>(R, F, (f % 2) ? -1.0 : 1.0, mask);
-        }
-        double Rv[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Rv[v] = R.get(v);
-        if constexpr (MODE == 1) {
-#pragma unroll
-          for (int v = 0; v < NV; ++v) Rb[v * vs + o] = Rv[v];
-        } else {
-          double vol;
-          if constexpr (UNI) vol = d.u_vol; else vol = a.m.vol[d.mbase + o];
-          const double dt = a.time_accurate ? *a.dtg : a.dtl[d.mbase + o];
-          double Q[NV], QO[NV];
-#pragma unroll
-          for (int v = 0; v < NV; ++v) Q[v] = p0[v];
-          const bool first = (a.irk == 1);
-          if (!first) loadQ(a.Po + d.sbase, vs, o, QO);
-          const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
-          if (!ok) report(a.err, 5, b, i, j, k);
-          double* Pn = a.Pn + d.sbase;
-#pragma unroll
-          for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
-          if constexpr (MODE == 2) dtrun = fmin(dtrun, cfl_dt<NV, UNI, PH::kFast>(a.g, Q, d, a.m, o, a.ndir, a.cfl));
-        }
-      }
-#pragma unroll
-      for (int v = 0; v < NV; ++v) { p0[v] = p1[v]; p1[v] = p2[v]; s0[v] = s1[v]; Gm[v] = Gp[v]; }
-      d0 = d1; d1 = d2;
-    }
-  }
-  if constexpr (MODE == 2) {
-    __shared__ double red[SB_T / 32];
-    const int t = threadIdx.x;
     for (int s = 16; s > 0; s >>= 1) dtrun = fmin(dtrun, __shfl_xor_sync(0xffffffffu, dtrun, s));
     if ((t & 31) == 0) red[t >> 5] = dtrun;
     __syncthreads();
