@@ -372,8 +372,8 @@ def warm_up(s, stream, seconds=0.5):
 
 def autotune(s, case):
     """The project's autotuner on a 2-D solver (work-list tiling, measured on
-    this domain's warmed flow before any timing); None for 3-D, whose sweeps
-    are not tuned."""
+    this domain's warmed flow before any timing); None for 3-D, whose tiles
+    and k runs are planned at setup."""
     if any(nd.shape[0] > 2 for nd in case.nodes):
         return None
     return s.autotune(steps=3)

@@ -88,7 +88,7 @@ enum {
   MOSE_RIEMANN_EXACT = 14      /* 'exact' (Lib_Riemann_Godunov.f90:10-224) */
 };
 
-/* Arithmetic of the face sweeps and of the fused steps' CFL pass.  In the
+/* Arithmetic of the face fluxes and of the fused steps' CFL pass.  In the
  * fused step (mose_gpu_step / mose_gpu_advance) the last RK stage also forms
  * the next step's Compute_dt on the state it writes; the first fused step
  * after any call that changes the state runs the standalone (reference
@@ -289,8 +289,8 @@ int mose_gpu_set_viscous(mose_gpu_ctx* ctx, int32_t model, double mu, double kap
 
 /* riemann-options-Minf (Register_Numerics.f90:72), the reference Mach number
  * of AUSM+-up and AUSM+-up2; call before mose_gpu_setup.  Setup rejects
- * those two solvers while it is 0, as Assign_Setup.f90:96-100 does.  2-D
- * only: the 3-D sweeps run HLLC and AUSM+. */
+ * those two solvers while it is 0, as Assign_Setup.f90:96-100 does (2-D
+ * and 3-D). */
 int mose_gpu_set_riemann_minf(mose_gpu_ctx* ctx, double minf);
 
 /* Tiling of the 2-D work list that the persistent stage kernels walk (no

@@ -329,13 +329,14 @@ def perturbed_channel(n: int = 512, steps: int = 200, amp: float = 0.05, seed: i
 
 def periodic_box_3d(n: int = 128, nb=(2, 2, 2), sizes=None, steps: int = 50, seed: int = 0,
                     limiter="vanleer", riemann="HLLC", cfl=0.3, gamma=1.4, mach=0.3, amp=1e-2,
-                    nmodes: int = 16, kmax: int = 8) -> Case:
+                    nmodes: int = 16, kmax: int = 8, ywalls: bool = False) -> Case:
     """3-D periodic box [0,1]^3 of nb[0] x nb[1] x nb[2] blocks (n^3 cells each, or
     per-direction block sizes `sizes`), uniform state rho = 1, p = 1/gamma
     (sound speed 1), Mach 0.3 along x, plus `nmodes` seeded Fourier modes with
     integer wavevectors of norm in [1, kmax] and random phases on rho, u, v, w,
     their sum scaled to amplitude `amp`.  Block interfaces are 101 connections,
     the periodic wrap is 201 (connection with extrapolated ghost metrics).
+    ywalls: the domain's y ends (faces 3 and 4) are 300 slip walls instead.
     [0,1] with a power-of-two cell count gives dyadic, exactly uniform metrics."""
     rng = np.random.default_rng(seed)
     sizes = sizes or [[n] * nb[0], [n] * nb[1], [n] * nb[2]]
@@ -379,6 +380,8 @@ def periodic_box_3d(n: int = 128, nb=(2, 2, 2), sizes=None, steps: int = 50, see
         nbk = list(key)
         nbk[d] += step
         wrap = not (0 <= nbk[d] < nb[d])
+        if wrap and ywalls and d == 1:
+            return ("bc", 300, [0.0] * 6)
         nbk[d] %= nb[d]
         fs = f + 1 if f % 2 == 1 else f - 1
         return ("conn", 201 if wrap else 101, index[tuple(nbk)], fs)

@@ -28,6 +28,7 @@ struct StageArgs {
   const double* Po;     // state at the start of the step (Copy_State's PO)
   double* Pn;           // next state (fused mode)
   double* R;            // residual arena (residual-only mode)
+  double* Hk;           // 3-D: interior k-face flux H(k + 1/2) at cell (i, j, k), a state-shaped arena
   MetricArgs m;
   double* dtl;          // local dt plane arena (one plane per block), or null
   const double* dtg;    // device scalar dtglobal (time-accurate)
@@ -45,7 +46,7 @@ struct StageArgs {
   double cfl;
   int ndir;
   int dt_local;
-  // 3-D work lists: [0] i-sweep rows, [1] j-march columns, [2] k-march columns
+  // 3-D work list in [0]: (block, i0 | j0 << 16, k0, k1) tiles marching k
   const int4* items3[3];
   int nitems3[3];
   // persistent 2-D grid: at most this many CTAs per SM (0: the occupancy limit)

@@ -122,19 +122,75 @@ std::vector<int4> plan_stage_items(const std::vector<HostBlock>& blocks, int gri
   return best;
 }
 
-// Work items of the fused 3-D stage: (block, i0 | j0 << 16, k0, k1), tiles
-// of T3X x T3Y cells of the block's (i, j) plane marching k over runs of at
-// most 32 planes (shorter runs give more items per wave of the persistent
-// grid and a shorter tail, for one extra k-face flux and two slopes per run).
-void plan_3d_items(const std::vector<HostBlock>& blocks, std::vector<int4> out[3]) {
+// The k-run length of the 3-D work items on a persistent grid of `slots`
+// CTAs: the runs of at most L planes that minimise the grid's time, modelled
+// as its waves (items over slots, rounded up) times the longest run plus 1.5
+// planes of per-item setup (the first plane's copy, the march's extra
+// slope).  Ties go to the longer runs.
+int choose_k_run(const std::vector<HostBlock>& blocks, int slots) {
+  int nkmax = 1;
+  for (const HostBlock& h : blocks) nkmax = std::max(nkmax, h.nk);
+  int best = nkmax;
+  double bcost = 1e300;
+  for (int L = nkmax; L >= std::min(4, nkmax); --L) {
+    long long n = 0;
+    int lmax = 0;
+    for (const HostBlock& h : blocks) {
+      const int runs = (h.nk + L - 1) / L;
+      n += (long long)((h.ni + T3X - 1) / T3X) * ((h.nj + T3Y - 1) / T3Y) * runs;
+      lmax = std::max(lmax, (h.nk + runs - 1) / runs);
+    }
+    const double cost = (double)((n + slots - 1) / slots) * (lmax + 1.5);
+    if (cost < bcost - 1e-9) {
+      bcost = cost;
+      best = L;
+    }
+  }
+  return best;
+}
+
+// Work items of the 3-D stage: (block, i0 | j0 << 16, k0, k1), tiles of T3X
+// x T3Y cells of the block's (i, j) plane marching k over runs of at most
+// run_s planes for the plane stage and run_k planes for the k-face march
+// (their grids differ in CTAs per SM).  out[0]: the plane-stage tiles whose
+// block-edge faces (the faces 1..6 their cells touch) are all connections;
+// out[1]: the other plane-stage tiles; out[2]: the k-face march's tiles.
+void plan_3d_items(const std::vector<HostBlock>& blocks, const std::vector<BlockDesc>& desc,
+                   const std::vector<int>& bcw, int run_s, int run_k, std::vector<int4> out[3]) {
   for (int q = 0; q < 3; ++q) out[q].clear();
-  for (int b = 0; b < (int)blocks.size(); ++b) {
-    const HostBlock& h = blocks[b];
-    const std::vector<int> kc = split_even(h.nk, (h.nk + 31) / 32, 1);
-    for (size_t r = 0; r + 1 < kc.size(); ++r)
-      for (int j0 = 0; j0 < h.nj; j0 += T3Y)
-        for (int i0 = 0; i0 < h.ni; i0 += T3X)
-          if (kc[r + 1] > kc[r]) out[0].push_back(make_int4(b, i0 | (j0 << 16), kc[r], kc[r + 1]));
+  for (int pass = 0; pass < 2; ++pass) {
+    const int L = pass == 0 ? run_s : run_k;
+    for (int b = 0; b < (int)blocks.size(); ++b) {
+      const HostBlock& h = blocks[b];
+      const BlockDesc& d = desc[b];
+      const std::vector<int> kc = split_even(h.nk, (h.nk + L - 1) / L, 1);
+      for (size_t r = 0; r + 1 < kc.size(); ++r)
+        for (int j0 = 0; j0 < h.nj; j0 += T3Y)
+          for (int i0 = 0; i0 < h.ni; i0 += T3X) {
+            const int k0 = kc[r], k1 = kc[r + 1];
+            if (k1 <= k0) continue;
+            const int4 it = make_int4(b, i0 | (j0 << 16), k0, k1);
+            if (pass == 1) {
+              out[2].push_back(it);
+              continue;
+            }
+            const int i1 = std::min(i0 + T3X, h.ni), j1 = std::min(j0 + T3Y, h.nj);
+            bool conn = true;
+            // face f (1..6) over the index ranges [a0, a1) x [b0, b1) of its
+            // words (word index a + na * b)
+            auto check = [&](int f, int a0, int a1, int na, int b0, int b1) {
+              for (int y = b0; y < b1 && conn; ++y)
+                for (int x = a0; x < a1 && conn; ++x) conn = bc_code(bcw[d.bcoff[f - 1] + x + na * y]) == BC_CONN;
+            };
+            if (i0 == 0) check(1, j0, j1, h.nj, k0, k1);
+            if (i1 == h.ni) check(2, j0, j1, h.nj, k0, k1);
+            if (j0 == 0) check(3, i0, i1, h.ni, k0, k1);
+            if (j1 == h.nj) check(4, i0, i1, h.ni, k0, k1);
+            if (k0 == 0) check(5, i0, i1, h.ni, j0, j1);
+            if (k1 == h.nk) check(6, i0, i1, h.ni, j0, j1);
+            out[conn ? 0 : 1].push_back(it);
+          }
+    }
   }
 }
 
@@ -165,6 +221,7 @@ struct mose_gpu_ctx {
   DevBuf<BlockDesc> d_desc;
   DevBuf<double> state[3];
   DevBuf<double> resid;
+  DevBuf<double> hk;          // 3-D: the k-face flux arena of the stage kernels
   DevBuf<double> dl, face, vol, vers, dtl;
   DevBuf<double> Mt;          // Navier-Stokes: 2-D metric tensor planes (null otherwise)
   DevBuf<int> vconn;          // Navier-Stokes: VConn stencils of the connection face cells
@@ -185,7 +242,7 @@ struct mose_gpu_ctx {
   // SM (0: the occupancy limit); and the boundary words the planner reads
   int tile_h = 0, tile_w = SB_W, tile_order = 0, tile_ctas = 0;
   std::vector<int> hbcw;
-  DevBuf<int4> items3[3];     // 3-D sweeps
+  DevBuf<int4> items3[3];     // 3-D tiles: connection-only, with a physical boundary face, all
   int nitems3[3] = {0, 0, 0};
   DevBuf<double> scal;        // [0] dtglobal, [1] time
   DevBuf<unsigned long long> dtmin;
@@ -760,6 +817,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
       ctx->face.alloc(12 * (size_t)mcur) != cudaSuccess || ctx->vol.alloc((size_t)mcur) != cudaSuccess ||
       ctx->vers.alloc(9 * (size_t)mcur) != cudaSuccess || ctx->dtl.alloc((size_t)mcur) != cudaSuccess)
     return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
+  if (ctx->nd == 3 && ctx->hk.alloc((size_t)ctx->nv * mcur) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (k-face arena)");
   if (ctx->gas.model > 0) {
     if (ctx->Mt.alloc(4 * (size_t)mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
     CU(cudaMemsetAsync(ctx->Mt.p, 0, 4 * (size_t)mcur * sizeof(double), ctx->stream));
@@ -1002,7 +1061,9 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   }
   if (ctx->nd == 3) {
     std::vector<int4> it3[3];
-    plan_3d_items(ctx->hblk, it3);
+    // the plane stage runs three CTAs per SM, the k-face march two
+    plan_3d_items(ctx->hblk, ctx->desc, ctx->hbcw, choose_k_run(ctx->hblk, 3 * ctx->nsm),
+                  choose_k_run(ctx->hblk, 2 * ctx->nsm), it3);
     for (int q = 0; q < 3; ++q) {
       ctx->nitems3[q] = (int)it3[q].size();
       CU(ctx->items3[q].alloc(std::max<size_t>(it3[q].size(), 1)));
@@ -1168,6 +1229,7 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   a.Po = ctx->state[po].p;
   a.Pn = pn >= 0 ? ctx->state[pn].p : nullptr;
   a.R = ctx->resid.p;
+  a.Hk = ctx->hk.p;
   a.m = ctx->margs();
   a.dtl = ctx->dtl.p;
   a.dtg = ctx->scal.p;
@@ -1196,13 +1258,33 @@ static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc) {
 }
 
 // One RK stage (mode 0 / 2) or one residual evaluation (mode 1) on every
-// block: the 2-D kernel, or the three 3-D sweeps.  Returns the kernel count
-// (0: no kernel for this configuration).
+// block: the 2-D kernel, or the 3-D k-face march and plane stage.  Returns
+// the kernel count (0: no kernel for this configuration).
 static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int prec, bool uni) {
-  if (ctx->nd == 3)
+  if (ctx->nd == 3) {
+    if (a.nitems3[0] > 0 && a.nitems3[1] > 0) {
+      // the k-face march, then the two plane stages side by side (disjoint
+      // cells, as the 2-D kernels below): the boundary tiles on stage_aux
+      StageArgs ak = a, anb = a, abc = a;
+      ak.nitems3[0] = ak.nitems3[1] = 0;
+      anb.nitems3[1] = anb.nitems3[2] = 0;
+      abc.nitems3[0] = abc.nitems3[2] = 0;
+      if (!launch_stage3d(ak, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)) return 0;
+      if (cudaEventRecord(ctx->stage_fork, ctx->stream) != cudaSuccess ||
+          cudaStreamWaitEvent(ctx->stage_aux, ctx->stage_fork, 0) != cudaSuccess)
+        return 0;
+      const bool ok =
+          launch_stage3d(abc, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stage_aux) &&
+          launch_stage3d(anb, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream);
+      if (cudaEventRecord(ctx->stage_join, ctx->stage_aux) != cudaSuccess ||
+          cudaStreamWaitEvent(ctx->stream, ctx->stage_join, 0) != cudaSuccess)
+        return 0;
+      return ok ? 3 : 0;
+    }
     return launch_stage3d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
-               ? (ctx->nitems3[0] > 0 ? 1 : 0)
+               ? (a.nitems3[2] > 0) + (a.nitems3[0] > 0) + (a.nitems3[1] > 0)
                : 0;
+  }
   if (a.nitems > 0 && a.nitems_nb > 0) {
     // The boundary-free items and the boundary items write disjoint cells
     // and meet only in atomics (the fused dt minimum, the error word), so the

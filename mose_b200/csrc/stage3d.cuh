@@ -1,13 +1,15 @@
-// stage3d.cuh -- the fused residual + RK-stage kernel of 3-D blocks, one
-// launch per RK stage over every block (k_stage3d below).
+// stage3d.cuh -- one RK stage (or one residual evaluation) of 3-D blocks in
+// two launches over every block: the k-face march (k_kface3d) and the plane
+// stage (k_stage3d) that forms the i- and j-faces and updates the cells.
 //
 // The reference accumulates a cell's residual in a fixed order: the interior
 // i-faces (low then high), the interior j-faces, the interior k-faces
 // (Mod_Fluxes.f90:89-179), then the boundary faces in face order 1..6
-// (BC_Fluxes walks the bc list, Mod_BC_Fluxes.f90:52-216).  The kernel keeps
-// that order with the residual in registers.  Boundary faces are formed only
-// for boundary cells: the interior formula with the ghosts for connections
-// (101/201, as BC_Connection_Eul does), boundary_flux() for the other types.
+// (BC_Fluxes walks the bc list, Mod_BC_Fluxes.f90:52-216).  The plane stage
+// keeps that order with the residual in registers.  Boundary faces are formed
+// only for boundary cells: the interior formula with the ghosts for
+// connections (101/201, as BC_Connection_Eul does), boundary_flux() for the
+// other types.
 #pragma once
 
 #include "stage2d.cuh"
@@ -135,40 +137,129 @@ __device__ __noinline__ int bc_face(const StageArgs& a, int b, int f, int i, int
 
 }  // namespace s3
 
-// ---- fused stage -----------------------------------------------------------------
-// One kernel per RK stage: a CTA of T3X x T3Y threads owns a tile of cells
-// (i0 .. i0 + T3X - 1, j0 .. j0 + T3Y - 1) of one block and marches up a run of
-// k planes.  Per plane it stages the tile and a two-cell halo ring in i and j
-// in shared memory, forms the limited i- and j-slopes and every i- and j-face
-// flux of the tile (halo faces included) there, while each thread marches its
-// own column in k with the stencil P(k), P(k+1), P(k+2), the k-slope and the
-// lower k-face flux in registers.  Each cell's residual stays in registers in
-// the reference's order: interior i-faces, j-faces, k-faces, then the
-// boundary faces in face order 1..6, then Newstate (or R in residual mode)
-// and the next step's CFL dt.  R never goes through HBM.
+// ---- k-face march ----------------------------------------------------------------
+// k_kface3d: each thread marches one (i, j) column of a work item's tile up its
+// run of k planes with P(k), P(k + 1), P(k + 2), the k-slopes and the next
+// plane's load in registers, and stores the interior k-face flux H(k + 1/2)
+// (0 <= k <= nk - 2) at cell (i, j, k) of the k-face arena; a connection face
+// at either k end of the block takes the same formula with the ghosts.  No shared memory
+// and no barrier: the march is a register pipeline, and the plane stage below
+// reads H(k - 1/2) and H(k + 1/2) back as two coalesced loads per cell.  The
+// flux is the interior formula of Mod_Fluxes.f90:155-179 (the k loop), so
+// the plane stage adds exactly the value the reference adds.  Two CTAs per
+// SM: the march holds four states and two slopes across the face, which at
+// the three-CTA budget of 80 registers spills to local memory.
+template <class PH, int RIE, int LIM, bool UNI>
+__global__ void __launch_bounds__(SB_T, 2) k_kface3d(StageArgs a, const int4* items, int nitems) {
+  using namespace s3;
+  const int t = threadIdx.x, tx = t % T3X, ty = t / T3X;
+#pragma unroll 1
+  for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+    const int4 item = items[it];
+    const int b = item.x, i = (item.y & 0xffff) + tx, j = (item.y >> 16) + ty, k0 = item.z;
+    const BlockDesc& d = a.blk[b];
+    if (ty >= T3Y || i >= d.ni || j >= d.nj) continue;
+    // faces k + 1/2 for kb <= k < ke: the interior faces of the run, and a
+    // connection face at the block's k = 0 or k = nk end (its ghosts are the
+    // source block's cells), stored at the ghost slot k = -1 or at k = nk - 1
+    auto conn = [&](int f) { return bc_code(a.bcw[d.bcoff[f - 1] + i + d.ni * j]) == BC_CONN; };
+    const int kb = (k0 == 0 && conn(5)) ? -1 : k0;
+    const int ke = (item.w == d.nk && conn(6)) ? d.nk : (item.w < d.nk - 1 ? item.w : d.nk - 1);
+    if (kb >= ke) continue;
+    const long long vs = d.vstride;
+    const double* P = a.Pc + d.sbase;
+    double* H = a.Hk + d.sbase;
+    double un[3] = {0.0, 0.0, 0.0}, uA = 0.0, udl = 0.0;
+    if constexpr (UNI) {
+      un[0] = d.u_n[2][0]; un[1] = d.u_n[2][1]; un[2] = d.u_n[2][2];
+      uA = d.u_A[2];
+      udl = d.u_dl[2];
+    }
+    auto ok3 = [&](int kk) { return off3(d, i, j, kk); };
+    auto dlk = [&](long long o) -> double {
+      if constexpr (UNI) return udl; else return a.m.dl[3 * d.mbase + 2 * vs + o];
+    };
+    double p0[NV], p1[NV], pn[NV], s0[NV];
+    double d0, d1;
+    {
+      double pm[NV];
+      loadQ(P, vs, ok3(kb - 1), pm);
+      loadQ(P, vs, ok3(kb), p0);
+      loadQ(P, vs, ok3(kb + 1), p1);
+      const double dm = dlk(ok3(kb - 1));
+      d0 = dlk(ok3(kb));
+      d1 = dlk(ok3(kb + 1));
+      lslope<PH, UNI>(pm, p0, p1, dm, d0, d1, s0);
+    }
+    loadQ(P, vs, ok3(kb + 2), pn);
+#pragma unroll 1
+    for (int k = kb; k < ke; ++k) {
+      double p2[NV];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) p2[v] = pn[v];
+      // the next plane's P(k + 2), in flight during this face
+      if (k + 1 < ke) loadQ(P, vs, ok3(k + 3), pn);
+      const double d2 = dlk(ok3(k + 2));
+      double s1[NV], Hf[NV], n[3], A;
+      lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
+      if constexpr (UNI) { n[0] = un[0]; n[1] = un[1]; n[2] = un[2]; A = uA; }
+      else A = face_at<false>(a, d, 2, ok3(k + 1), n);
+      const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Hf);
+      if (!ok) report(a.err, 4, b, i, j, k);
+      const long long o = ok3(k);
+#pragma unroll
+      for (int v = 0; v < NV; ++v) H[v * vs + o] = Hf[v];
+#pragma unroll
+      for (int v = 0; v < NV; ++v) { p0[v] = p1[v]; p1[v] = p2[v]; s0[v] = s1[v]; }
+      d0 = d1;
+      d1 = d2;
+    }
+  }
+}
+
+// ---- plane stage -----------------------------------------------------------------
+// k_stage3d: a CTA of T3X x T3Y threads owns a tile of cells (i0 .. i0 + T3X -
+// 1, j0 .. j0 + T3Y - 1) of one block and marches up a run of k planes.  Per
+// plane it stages the tile and a two-cell halo ring in i and j in shared
+// memory, forms the limited i- and j-slopes and every i- and j-face flux of
+// the tile (halo faces included) there, then each thread adds its cell's
+// terms in the reference's order: interior i-faces, j-faces, the k-faces from
+// the k-face arena, then the boundary faces in face order 1..6, and applies
+// Newstate (or stores R in residual mode) and the next step's CFL dt.  R
+// never goes through HBM.  The next plane's copy is issued once the faces
+// are formed, so it lands during the cell updates; with no k-march state in
+// registers three CTAs fit on an SM.
 constexpr int H3X = T3X + 4, H3Y = T3Y + 4;  // plane region: the tile and two halo cells per side
 
-template <int NVS>
+template <int NVS, bool UNI>
 struct Stage3dSmem {
-  double P[2][NVS][H3Y][H3X];       // planes k and k + 1 (in flight): region cells, corners unused
-  double dx[T3Y][H3X];              // dl along i on the tile rows (metric arrays only)
-  double dy[H3Y][T3X];              // dl along j on the tile columns
+  double P[NVS][H3Y][H3X];          // plane k: region cells, corners unused
+  double dx[UNI ? 1 : T3Y][UNI ? 1 : H3X];   // dl along i on the tile rows (metric arrays only)
+  double dy[UNI ? 1 : H3Y][UNI ? 1 : T3X];   // dl along j on the tile columns
   double sx[NVS][T3Y][T3X + 2];     // limited i-slope of cells i0 - 1 .. i0 + T3X
   double sy[NVS][T3Y + 2][T3X];     // limited j-slope of cells j0 - 1 .. j0 + T3Y
   double F[NVS][T3Y][T3X + 1];      // F(i0 - 1 + x + 1/2)
   double G[NVS][T3Y + 1][T3X];      // G(j0 - 1 + y + 1/2)
-  double PO[2][NVS][T3Y][T3X];      // PO of the tile cells, planes k and k + 1
   // the block's uniform metrics: dl (3), face normals (3 x 3), areas (3), volume
   double um[16];
 };
-constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5>); }
+template <bool UNI>
+constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5, UNI>); }
 
-// Items: (block, i0 | j0 << 16, k0, k1).
-template <class PH, int RIE, int LIM, bool UNI, int MODE>
-__global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* items, int nitems) {
+// Items: (block, i0 | j0 << 16, k0, k1).  BC: the items with a physical
+// boundary face (the boundary formulas, a call, hold the kernel to two CTAs
+// per SM); without, every block-edge face of the items' cells is a
+// connection, formed here from the staged ghosts (i, j) or by the k-face
+// march (k) and added in its boundary-face position.  Both add a cell's terms
+// in the same order, so their results are identical.
+template <bool BC>
+constexpr int stage3d_min_ctas() { return BC ? 2 : 3; }
+
+template <class PH, int RIE, int LIM, bool UNI, int MODE, bool BC>
+__global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageArgs a, const int4* items, int nitems) {
   using namespace s3;
   extern __shared__ __align__(16) unsigned char smem3[];
-  Stage3dSmem<NV>& S = *reinterpret_cast<Stage3dSmem<NV>*>(smem3);
+  Stage3dSmem<NV, UNI>& S = *reinterpret_cast<Stage3dSmem<NV, UNI>*>(smem3);
   const int t = threadIdx.x, tx = t % T3X, ty = t / T3X;
   double dtrun = __longlong_as_double(0x7ff0000000000000LL);
 #pragma unroll 1
@@ -180,8 +271,7 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
     const long long vs = d.vstride;
     const double* P = a.Pc + d.sbase;
     const int i = i0 + tx, j = j0 + ty;
-    const bool mine = i < ni && j < nj;
-    const bool need_po = (MODE != 1) && (a.irk != 1);
+    const bool mine = ty < T3Y && i < ni && j < nj;
     const double dtg = (MODE != 1 && a.time_accurate) ? *a.dtg : 0.0;
     // the face metric of the low face along dir of cell o: the uniform
     // constants (shared memory) or the metric arrays
@@ -193,38 +283,13 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
         return face_at<false>(a, d, dir, o, n);
       }
     };
-    auto dlk = [&](long long o) -> double {
-      if constexpr (UNI) return S.um[2]; else return a.m.dl[3 * d.mbase + 2 * vs + o];
-    };
-    // ---- the k march of this thread's column: P(k+1), slope(k), H(k - 1/2) in
-    // registers; P(k) is the cell's own value in the staged plane
-    double p1[NV], s0[NV], Hm[NV];
-    double d0 = 0.0, d1 = 0.0;
     auto ok3 = [&](int kk) { return off3(d, i, j, kk); };
-    if (mine) {
-      double pm2[NV], pm1[NV], sm1[NV], p0[NV];
-      loadQ(P, vs, ok3(k0 - 2), pm2);
-      loadQ(P, vs, ok3(k0 - 1), pm1);
-      loadQ(P, vs, ok3(k0), p0);
-      loadQ(P, vs, ok3(k0 + 1), p1);
-      const double dm2 = dl_at<UNI>(a, d, 2, ok3(k0 - 2)), dm1 = dl_at<UNI>(a, d, 2, ok3(k0 - 1));
-      d0 = dl_at<UNI>(a, d, 2, ok3(k0));
-      d1 = dl_at<UNI>(a, d, 2, ok3(k0 + 1));
-      lslope<PH, UNI>(pm2, pm1, p0, dm2, dm1, d0, sm1);
-      lslope<PH, UNI>(pm1, p0, p1, dm1, d0, d1, s0);
-      if (k0 > 0) {
-        double n[3];
-        const double A = face_at<UNI>(a, d, 2, ok3(k0), n);
-        const bool ok = face<PH, UNI>(a.g, pm1, sm1, dm1, p0, s0, d0, n, A, Hm);
-        if (!ok) report(a.err, 4, b, i, j, k0);
-      }
-    }
-    // plane kk into buffer bf with 16-byte copies (two cells per copy; the
-    // region's rows start on even columns and the padded rows keep every copy
-    // inside the block's plane): rows j0 .. j0 + T3Y - 1 over columns
-    // i0 - 2 .. i0 + T3X + 1, and columns i0 .. i0 + T3X - 1 over rows j0 - 2,
-    // j0 - 1, j0 + T3Y, j0 + T3Y + 1
-    auto stage_plane = [&](int kk, int bf) {
+    // plane kk with 16-byte copies (two cells per copy; the region's rows
+    // start on even columns and the padded rows keep every copy inside the
+    // block's plane): rows j0 .. j0 + T3Y - 1 over columns i0 - 2 .. i0 + T3X
+    // + 1, and columns i0 .. i0 + T3X - 1 over rows j0 - 2, j0 - 1, j0 + T3Y,
+    // j0 + T3Y + 1
+    auto stage_plane = [&](int kk) {
       constexpr int CA = H3X / 2, CB = T3X / 2;   // chunks per row
       for (int e = t; e < T3Y * CA + 4 * CB; e += SB_T) {
         int cx, ry;
@@ -234,38 +299,20 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
         if (ci > ni + 1 || cj > nj + 1) continue;   // beyond a partial tile's ghosts
         const long long o = off3(d, ci, cj, kk);
 #pragma unroll
-        for (int v = 0; v < NV; ++v) cp_async16(&S.P[bf][v][ry][cx], P + v * vs + o);
-      }
-      if (need_po) {
-        const double* Po = a.Po + d.sbase;
-        for (int e = t; e < T3Y * CB; e += SB_T) {
-          const int cx = 2 * (e % CB), y = e / CB;
-          const int ci = i0 + cx, cj = j0 + y;
-          if (ci >= ni || cj >= nj) continue;
-          const long long o = off3(d, ci, cj, kk);
-#pragma unroll
-          for (int v = 0; v < NV; ++v) cp_async16(&S.PO[bf][v][y][cx], Po + v * vs + o);
-        }
+        for (int v = 0; v < NV; ++v) cp_async16(&S.P[v][ry][cx], P + v * vs + o);
       }
       cp_async_commit();
     };
-    __syncthreads();   // the previous item's readers are done with both buffers
+    __syncthreads();   // the previous item's readers are done with the plane and the constants
     if constexpr (UNI) {
       if (t < 3) S.um[t] = d.u_dl[t];
       else if (t < 12) S.um[t] = d.u_n[(t - 3) / 3][(t - 3) % 3];
       else if (t < 15) S.um[t] = d.u_A[t - 12];
       else if (t == 15) S.um[15] = d.u_vol;
     }
-    stage_plane(k0, 0);
+    stage_plane(k0);
 #pragma unroll 1
     for (int k = k0; k < k1; ++k) {
-      const int bf = (k - k0) & 1;
-      __syncthreads();   // the previous plane's readers are done with buffer bf ^ 1
-      if (k + 1 < k1) stage_plane(k + 1, bf ^ 1);
-      else cp_async_commit();   // an empty group keeps the wait count uniform
-      // the column's P(k + 2), loaded early so its latency overlaps the plane's work
-      double p2[NV];
-      if (mine) loadQ(P, vs, ok3(k + 2), p2);
       if constexpr (!UNI) {
         for (int e = t; e < T3Y * H3X + 4 * T3X; e += SB_T) {
           int cx, ry;
@@ -278,8 +325,8 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
           if (cx >= 2 && cx < T3X + 2) S.dy[ry][cx - 2] = a.m.dl[3 * d.mbase + 1 * vs + o];
         }
       }
-      cp_async_wait_prev();   // this thread's copies of plane k
-      __syncthreads();
+      cp_async_wait_all();   // this thread's copies of plane k
+      __syncthreads();       // everyone's copies; the previous plane's cell updates are done with F and G
       auto dxat = [&](int y, int cx) -> double { if constexpr (UNI) return S.um[0]; else return S.dx[y][cx]; };
       auto dyat = [&](int ry, int x) -> double { if constexpr (UNI) return S.um[1]; else return S.dy[ry][x]; };
       // ---- limited slopes: i-slopes of cells i0 - 1 .. i0 + T3X (columns 1 .. T3X + 2),
@@ -294,7 +341,7 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
           const int ci = i0 - 1 + x, cj = j0 + y;
           if (ci > ni || cj >= nj) continue;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) { qa[v] = S.P[bf][v][y + 2][x]; q[v] = S.P[bf][v][y + 2][x + 1]; qb[v] = S.P[bf][v][y + 2][x + 2]; }
+          for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y + 2][x]; q[v] = S.P[v][y + 2][x + 1]; qb[v] = S.P[v][y + 2][x + 2]; }
           lslope<PH, UNI>(qa, q, qb, dxat(y, x), dxat(y, x + 1), dxat(y, x + 2), sl);
 #pragma unroll
           for (int v = 0; v < NV; ++v) S.sx[v][y][x] = sl[v];
@@ -304,7 +351,7 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
           const int ci = i0 + x, cj = j0 - 1 + y;
           if (ci >= ni || cj > nj) continue;
 #pragma unroll
-          for (int v = 0; v < NV; ++v) { qa[v] = S.P[bf][v][y][x + 2]; q[v] = S.P[bf][v][y + 1][x + 2]; qb[v] = S.P[bf][v][y + 2][x + 2]; }
+          for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y][x + 2]; q[v] = S.P[v][y + 1][x + 2]; qb[v] = S.P[v][y + 2][x + 2]; }
           lslope<PH, UNI>(qa, q, qb, dyat(y, x), dyat(y + 1, x), dyat(y + 2, x), sl);
 #pragma unroll
           for (int v = 0; v < NV; ++v) S.sy[v][y][x] = sl[v];
@@ -318,10 +365,10 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
         if (e < NFX) {
           const int x = e % (T3X + 1), y = e / (T3X + 1);
           const int cl = i0 - 1 + x, cj = j0 + y;
-          if (cl < 0 || cl > ni - 2 || cj >= nj) continue;
+          if (cl < (BC ? 0 : -1) || cl > (BC ? ni - 2 : ni - 1) || cj >= nj) continue;
 #pragma unroll
           for (int v = 0; v < NV; ++v) {
-            PL[v] = S.P[bf][v][y + 2][x + 1]; PR[v] = S.P[bf][v][y + 2][x + 2];
+            PL[v] = S.P[v][y + 2][x + 1]; PR[v] = S.P[v][y + 2][x + 2];
             sL[v] = S.sx[v][y][x]; sR[v] = S.sx[v][y][x + 1];
           }
           const double A = facek(0, off3(d, cl + 1, cj, k), n);
@@ -333,10 +380,10 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
           const int e2 = e - NFX;
           const int x = e2 % T3X, y = e2 / T3X;
           const int ci = i0 + x, cl = j0 - 1 + y;
-          if (ci >= ni || cl < 0 || cl > nj - 2) continue;
+          if (ci >= ni || cl < (BC ? 0 : -1) || cl > (BC ? nj - 2 : nj - 1)) continue;
 #pragma unroll
           for (int v = 0; v < NV; ++v) {
-            PL[v] = S.P[bf][v][y + 1][x + 2]; PR[v] = S.P[bf][v][y + 2][x + 2];
+            PL[v] = S.P[v][y + 1][x + 2]; PR[v] = S.P[v][y + 2][x + 2];
             sL[v] = S.sy[v][y][x]; sR[v] = S.sy[v][y + 1][x];
           }
           const double A = facek(1, off3(d, ci, cl + 1, k), n);
@@ -346,21 +393,24 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
           for (int v = 0; v < NV; ++v) S.G[v][y][x] = F[v];
         }
       }
-      __syncthreads();
-      if (!mine) continue;
-      // ---- the k face above, then the residual of cell (i, j, k) in the reference's order
-      double p0[NV], s1[NV], Hp[NV];
-#pragma unroll
-      for (int v = 0; v < NV; ++v) p0[v] = S.P[bf][v][ty + 2][tx + 2];
-      const double d2 = dlk(ok3(k + 2));
-      lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
-      if (k <= nk - 2) {
-        double n[3];
-        const double A = facek(2, ok3(k + 1), n);
-        const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Hp);
-        if (!ok) report(a.err, 4, b, i, j, k);
-      }
+      // the cell's own state, and its k-face fluxes and stage-start state
+      // from HBM: issued before the barrier, so the loads are in flight while
+      // the last faces of the plane are formed
       const long long o = ok3(k);
+      const bool first = (a.irk == 1);
+      double p0[NV], Hm[NV], Hp[NV], QO[NV];
+      if (mine) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) p0[v] = S.P[v][ty + 2][tx + 2];
+        const double* Hk = a.Hk + d.sbase;
+        if (!BC || k > 0) loadQ(Hk, vs, ok3(k - 1), Hm);
+        if (!BC || k < nk - 1) loadQ(Hk, vs, o, Hp);
+        if (MODE != 1 && !first) loadQ(a.Po + d.sbase, vs, o, QO);
+      }
+      __syncthreads();   // faces formed, the plane read: the next plane may land
+      if (k + 1 < k1) stage_plane(k + 1);
+      if (!mine) continue;
+      // ---- the residual of cell (i, j, k) in the reference's order
       ResAcc<NV, PH::kCompensated> R;
       R.init();
       if (i > 0) for (int v = 0; v < NV; ++v) R.add(v, -S.F[v][ty][tx]);
@@ -370,7 +420,27 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
       if (k > 0) for (int v = 0; v < NV; ++v) R.add(v, -Hm[v]);
       if (k < nk - 1) for (int v = 0; v < NV; ++v) R.add(v, Hp[v]);
       // boundary faces in face order 1..6
-      if (i == 0 || i == ni - 1 || j == 0 || j == nj - 1 || k == 0 || k == nk - 1) {
+      if constexpr (!BC) {
+        double Fe[NV];
+        if (i == 0) {
+          for (int v = 0; v < NV; ++v) Fe[v] = S.F[v][ty][tx];
+          add_bc<NV>(R, Fe, -1.0, ADD_ALL);
+        }
+        if (i == ni - 1) {
+          for (int v = 0; v < NV; ++v) Fe[v] = S.F[v][ty][tx + 1];
+          add_bc<NV>(R, Fe, 1.0, ADD_ALL);
+        }
+        if (j == 0) {
+          for (int v = 0; v < NV; ++v) Fe[v] = S.G[v][ty][tx];
+          add_bc<NV>(R, Fe, -1.0, ADD_ALL);
+        }
+        if (j == nj - 1) {
+          for (int v = 0; v < NV; ++v) Fe[v] = S.G[v][ty + 1][tx];
+          add_bc<NV>(R, Fe, 1.0, ADD_ALL);
+        }
+        if (k == 0) add_bc<NV>(R, Hm, -1.0, ADD_ALL);
+        if (k == nk - 1) add_bc<NV>(R, Hp, 1.0, ADD_ALL);
+      } else if (i == 0 || i == ni - 1 || j == 0 || j == nj - 1 || k == 0 || k == nk - 1) {
 #pragma unroll 1
         for (int f = 1; f <= 6; ++f) {
           const bool on = (f == 1) ? i == 0 : (f == 2) ? i == ni - 1 : (f == 3) ? j == 0 : (f == 4) ? j == nj - 1
@@ -392,25 +462,13 @@ __global__ void __launch_bounds__(SB_T, 2) k_stage3d(StageArgs a, const int4* it
         double vol;
         if constexpr (UNI) vol = S.um[15]; else vol = a.m.vol[d.mbase + o];
         const double dt = a.time_accurate ? dtg : a.dtl[d.mbase + o];
-        double Q[NV], QO[NV];
-#pragma unroll
-        for (int v = 0; v < NV; ++v) Q[v] = p0[v];
-        const bool first = (a.irk == 1);
-        if (!first) {
-#pragma unroll
-          for (int v = 0; v < NV; ++v) QO[v] = S.PO[bf][v][ty][tx];
-        }
-        const bool ok = PH::template update<NV>(a.g, Q, QO, Rv, vol, dt, a.c_rk, first);
+        const bool ok = PH::template update<NV>(a.g, p0, QO, Rv, vol, dt, a.c_rk, first);
         if (!ok) report(a.err, 5, b, i, j, k);
         double* Pn = a.Pn + d.sbase;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) Pn[v * vs + o] = Q[v];
-        if constexpr (MODE == 2) dtrun = fmin(dtrun, cfl_dt<NV, UNI, PH::kFast>(a.g, Q, d, a.m, o, a.ndir, a.cfl));
+        for (int v = 0; v < NV; ++v) Pn[v * vs + o] = p0[v];
+        if constexpr (MODE == 2) dtrun = fmin(dtrun, cfl_dt<NV, UNI, PH::kFast>(a.g, p0, d, a.m, o, a.ndir, a.cfl));
       }
-#pragma unroll
-      for (int v = 0; v < NV; ++v) { p1[v] = p2[v]; s0[v] = s1[v]; Hm[v] = Hp[v]; }
-      d0 = d1;
-      d1 = d2;
     }
   }
   if constexpr (MODE == 2) {

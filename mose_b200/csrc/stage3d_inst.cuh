@@ -1,5 +1,5 @@
-// stage3d_inst.cuh -- launch dispatch of the 3-D sweeps over arithmetic
-// policy, limiter and metric mode.  Each translation unit
+// stage3d_inst.cuh -- launch dispatch of the 3-D stage kernels over
+// arithmetic policy, limiter and metric mode.  Each translation unit
 // stage3d_<precision>_r<solver>.cu instantiates one (precision, Riemann
 // solver) pair for the six limiters (first order, minmod, van Leer, van
 // Albada, MC, superbee).
@@ -12,24 +12,42 @@
 
 namespace mose {
 
-// One RK stage (or one residual evaluation, MODE 1): the fused tile march
-// over the block tiles of items3[0].
+// The persistent grid of a kernel instance: one CTA per resident slot, at
+// most one per item.
+template <class K>
+static int persistent_grid(K kernel, size_t smem, int nsm, int n, int& occ) {
+  if (occ == 0) {
+    if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, SB_T, smem) != cudaSuccess || occ < 1) occ = 1;
+  }
+  return n < occ * nsm ? n : occ * nsm;
+}
+
+// One RK stage (or one residual evaluation, MODE 1): the k-face march over
+// every tile (items3[2]), then the plane stage over the connection-only tiles
+// (items3[0]) and over the tiles with a physical boundary face (items3[1]).
+// A list with no items launches nothing, so a caller may pass each part on
+// its own stream.
 template <int PREC, int RIE, int LIM, bool UNI, int MODE>
 static void launch3d(const StageArgs& a, int nsm, cudaStream_t s) {
   using PH = StagePolicy<PREC, RIE, LIM>;
-  constexpr size_t smem = stage3d_smem_bytes();
-  static int occ = 0;   // one per kernel instance
-  if (occ == 0) {
-    cudaFuncSetAttribute(k_stage3d<PH, RIE, LIM, UNI, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_stage3d<PH, RIE, LIM, UNI, MODE>, SB_T, smem) !=
-            cudaSuccess ||
-        occ < 1)
-      occ = 1;
+  constexpr size_t smem = stage3d_smem_bytes<UNI>();
+  static int occ_k = 0, occ_n = 0, occ_b = 0;   // one set per kernel instance
+  if (a.nitems3[2] > 0) {
+    const int n = a.nitems3[2];
+    const int g = persistent_grid(k_kface3d<PH, RIE, LIM, UNI>, 0, nsm, n, occ_k);
+    k_kface3d<PH, RIE, LIM, UNI><<<g, SB_T, 0, s>>>(a, a.items3[2], n);
   }
-  const int n = a.nitems3[0];
-  if (n <= 0) return;
-  const int grid = n < occ * nsm ? n : occ * nsm;
-  k_stage3d<PH, RIE, LIM, UNI, MODE><<<grid, SB_T, smem, s>>>(a, a.items3[0], n);
+  if (a.nitems3[0] > 0) {
+    const int n = a.nitems3[0];
+    const int g = persistent_grid(k_stage3d<PH, RIE, LIM, UNI, MODE, false>, smem, nsm, n, occ_n);
+    k_stage3d<PH, RIE, LIM, UNI, MODE, false><<<g, SB_T, smem, s>>>(a, a.items3[0], n);
+  }
+  if (a.nitems3[1] > 0) {
+    const int n = a.nitems3[1];
+    const int g = persistent_grid(k_stage3d<PH, RIE, LIM, UNI, MODE, true>, smem, nsm, n, occ_b);
+    k_stage3d<PH, RIE, LIM, UNI, MODE, true><<<g, SB_T, smem, s>>>(a, a.items3[1], n);
+  }
 }
 
 template <int PREC, int RIE, int LIM>
