@@ -551,12 +551,16 @@ def viscous_report(local, n=512, steps=50):
     walls, 2 x 2 blocks of 1024 x 512 cells on a warped mesh (2.1 M cells):
     throughput of graph-replayed steps in the reference-exact precision (the
     only one the viscous terms run in), and whether `steps` steps are bit
-    for bit those of the oracle's OpenMP build on the same inputs."""
+    for bit those of the oracle's OpenMP build on the same inputs.  mu =
+    1e-4: with the case's seeded cell-wise perturbations, a viscosity of
+    2e-3 at this resolution puts the heat-diffusion number (gamma / Pr times
+    the momentum one the reference's VNN limit bounds) past RK3's stability
+    bound, and the oracle itself stops with p < 0 in the first step."""
     import torch
     from mose_b200 import Solver, cases
     from mose_b200.cases import GC
     from oracle import pyoracle
-    case = cases.shear_layer(n, nbx=2, nby=2, warp=0.05, mu=0.002, steps=steps, seed=0)
+    case = cases.shear_layer(n, nbx=2, nby=2, warp=0.05, mu=1e-4, steps=steps, seed=0)
     s = Solver(case, precision=precision_code("exact"), device=local)
     st = torch.cuda.ExternalStream(s.stream_handle, device=torch.device("cuda", local))
     s.advance(3)
@@ -606,11 +610,11 @@ def profile_adjoint(local):
 # vortex 2048^2, the benchmark's kernels).  Reads equal the algorithmic
 # reads; ~45 MB of each launch's output is still in L2 when it ends, so the
 # write count is below the state written.
-TRAFFIC_BYTES_PER_CELL = {"fp64": 330.3e6 / 2048 ** 2, "mixed": 330.1e6 / 2048 ** 2, "exact": None}
+TRAFFIC_BYTES_PER_CELL = {"fp64": 329.3e6 / 2048 ** 2, "mixed": 330.1e6 / 2048 ** 2, "exact": None}
 # FP64-pipe lane slots per cell per stage of the stage kernel on the 2048^2
 # vortex (ncu sm__inst_executed_pipe_fp64.sum x 32 / cells, average of the
 # three RK stages of one step)
-FP64_SLOTS_PER_CELL = {"fp64": 492.2, "exact": 1156.0}
+FP64_SLOTS_PER_CELL = {"fp64": 463.4, "exact": 1156.0}
 
 
 def run_gpu(args):
