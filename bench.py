@@ -626,9 +626,13 @@ def run_gpu(args):
     if args.profile and args.profile_case == "quadrant":
         from mose_b200 import cases
         case = cases.four_quadrant(seed=0, steps=args.steps)
-    elif args.profile and args.profile_case in ("box3d", "box3d_small"):
+    elif args.profile and args.profile_case in ("box3d", "box3d_medium", "box3d_small"):
         from mose_b200 import cases
-        case = cases.periodic_box_3d(128 if args.profile_case == "box3d" else 64, steps=args.steps)
+        # 8 x 128^3, 4 x 4 x 2 blocks of 64^3 or 8 x 64^3 cells: power-of-two
+        # cells per unit length in every direction, so all run the uniform-grid kernels
+        n3, nb3 = {"box3d": (128, (2, 2, 2)), "box3d_medium": (64, (4, 4, 2)),
+                   "box3d_small": (64, (2, 2, 2))}[args.profile_case]
+        case = cases.periodic_box_3d(n3, nb=nb3, steps=args.steps)
     else:
         case = workload_case(N_CELLS_SIDE, steps=args.steps)
     cells = case.ncells
@@ -798,9 +802,10 @@ def main():
                     help="skip the four-quadrant and 3-D configuration reports")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + K fused steps (the command profiled by ncu); prints nothing")
-    ap.add_argument("--profile-case", default="vortex", choices=["vortex", "quadrant", "box3d", "box3d_small"],
+    ap.add_argument("--profile-case", default="vortex",
+                    choices=["vortex", "quadrant", "box3d", "box3d_medium", "box3d_small"],
                     help="with --profile: the 2048^2 vortex, the 64-block four-quadrant domain (seed 0), "
-                         "the 3-D periodic box of 8 x 128^3 or of 8 x 64^3 cells")
+                         "the 3-D periodic box of 8 x 128^3, 32 x 64^3 or 8 x 64^3 cells")
     ap.add_argument("--profile-adjoint", action="store_true",
                     help="only the adjoint's forward + backward on a 16-step channel (profiled by ncu)")
     args = ap.parse_args()

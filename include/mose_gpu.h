@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define MOSE_GPU_ABI_VERSION 1
+#define MOSE_GPU_ABI_VERSION 2
 
 /* Status codes.  The nonzero codes mirror the reference's fatal `stop`s. */
 enum {
@@ -100,8 +100,8 @@ enum {
 };
 
 /* integration-variables (Mod_Newstate.f90:30-44): 'cons' (Newstate_Conservative)
- * or 'prim' (Newstate_Primitive, Lib_Newstate.f90:168-317; reference-exact
- * precision only) */
+ * or 'prim' (Newstate_Primitive, Lib_Newstate.f90:168-317; the reference-exact
+ * and fp64 precisions, mose_gpu_create refuses it with the mixed one) */
 enum { MOSE_INTEGRATION_CONS = 0, MOSE_INTEGRATION_PRIM = 1 };
 
 typedef struct mose_gpu_config {
@@ -135,9 +135,28 @@ const char* mose_gpu_last_error(const mose_gpu_ctx* ctx);
 /* Offending (b,i,j,k) of the last device-detected failure (1-based). */
 int mose_gpu_error_location(const mose_gpu_ctx* ctx, int32_t* b, int32_t* i, int32_t* j, int32_t* k);
 
-/* Geometry and boundaries.  Blocks are added in order b = 1..nb. */
+/* Geometry and boundaries.  Blocks are added in order b = 1..nb.
+ * node: block_type%node(0:ni, 0:nj, 0:nk)%c(3) in its Fortran memory order
+ * (Advanced_Types_m.f90:16).  The device forms the metrics from the nodes at
+ * setup, bit for bit as Setup_Metrics does (Mod_Metrics.f90:8-107).
+ * metrics (optional, NULL: formed from the nodes) hands in the block's own
+ * Setup_Metrics output instead: the block_type arrays allocated by
+ * Allocate_Block (driver/Mod_Allocate_Data.f90:105-110), one after another,
+ * each in its Fortran memory order, ghost layers included (gc = 2 in every
+ * direction; NG = (ni+4)(nj+4)(nk+4)):
+ *   vol(1-gc:ni+gc, 1-gc:nj+gc, 1-gc:nk+gc)       NG doubles
+ *   dl(...)%c(3)                                  3 NG
+ *   M(...)%c(3,3)                                 9 NG
+ *   dir(1)%f(0:ni, nj, nk)%(N(3), A)              4 (ni+1) nj nk
+ *   dir(2)%f(ni, 0:nj, nk)%(N(3), A)              4 ni (nj+1) nk
+ *   dir(3)%f(ni, nj, 0:nk)%(N(3), A)              4 ni nj (nk+1)
+ * The device takes vol, dl and the CFL versors M(d,:)/norm2(M(d,:)) of the
+ * interior cells (and M(1:2,1:2) for the viscous terms), dl along each
+ * boundary's normal in the ghost layers (and M in the first layer), and every
+ * face's N and A; the nodes still give the inlet tangents.  The array is
+ * copied before the call returns. */
 int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int32_t nk,
-                       const double* node);
+                       const double* node, const double* metrics);
 /* Replaces Read_BCfile (io/IO_BC.f90:136-414) with the parsed records. */
 int mose_gpu_set_bcs(mose_gpu_ctx* ctx, const int32_t* rec, const double* data, int32_t nbound);
 /* The p0 time table of 402 inlets, replacing time_series_type::initialize

@@ -12,7 +12,7 @@ _HERE = Path(__file__).resolve().parent
 # MOSE_GPU_LIB selects another build of the same library (e.g. a tuning variant)
 LIB_PATH = Path(os.environ.get("MOSE_GPU_LIB", _HERE / "lib" / "libmose_gpu.so"))
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 ERR_INVALID, ERR_UNSUPPORTED, ERR_CUDA, ERR_INTERFACE_STATE, ERR_NAN_OR_NEG_P, ERR_METRICS, ERR_TIMEOUT, \
@@ -39,7 +39,7 @@ SIGNATURES = {
     "mose_gpu_destroy": (None, [_D]),
     "mose_gpu_last_error": (C.c_char_p, [_D]),
     "mose_gpu_error_location": (C.c_int, [_D, _ip, _ip, _ip, _ip]),
-    "mose_gpu_add_block": (C.c_int, [_D, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp]),
+    "mose_gpu_add_block": (C.c_int, [_D, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _dp, _dp]),
     "mose_gpu_set_bcs": (C.c_int, [_D, _ip, _dp, C.c_int32]),
     "mose_gpu_setup": (C.c_int, [_D]),
     "mose_gpu_upload_prim": (C.c_int, [_D, C.c_int32, _dp]),

@@ -12,6 +12,10 @@ void launch_cell_metrics(const BlockDesc* dblk, int b, long long ncell, NodeView
                          int ndir, DevError* err, cudaStream_t s);
 void launch_face_metrics(const BlockDesc* dblk, int b, long long nface, NodeView nv, MetricArgs m, int nd, int dir,
                          cudaStream_t s);
+// mose_gpu_add_block's precomputed metrics (reference layout, see the header)
+// over block b's metric planes; dims = (ni, nj, nk)
+void launch_metrics_from_ref(const BlockDesc* dblk, int b, const int* dims, const double* src, MetricArgs m, int nd,
+                             int ndir, cudaStream_t s);
 void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, const NodeView* nodes, MetricArgs m,
                           int nd, int ndir, DevError* err, cudaStream_t s);
 void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir, int* flags,

@@ -70,6 +70,71 @@ __global__ void k_face_metrics(const BlockDesc* blk, int b, NodeView nv, double*
   }
 }
 
+// Precomputed metrics of block b handed to mose_gpu_add_block: the
+// reference's Setup_Metrics arrays in their Fortran memory order (vol, dl%c(3),
+// M%c(3,3) over 1-gc:n+gc in every direction, then dir(1..3)%f as (N(3), A)),
+// laid over the planes the node kernels above formed.  Interior cells take
+// vol, dl and the CFL versors M(d,:)/norm2(M(d,:)) (and M(1:2,1:2) for the
+// viscous terms); the ghost layers take dl along their boundary's normal (and
+// M in the first layer), as the ghost-metric kernel stores them.
+__global__ void k_metrics_from_ref(const BlockDesc* blk, int b, const double* src, double* dl, double* vol,
+                                   double* vers, double* Mt, int nd, int ndir) {
+  const BlockDesc& d = blk[b];
+  const int ni = d.ni, nj = d.nj, nk = d.nk;
+  const long long gi = ni + 4, gj = nj + 4, gk = nk + 4, NG = gi * gj * gk;
+  const double* rvol = src;
+  const double* rdl = src + NG;
+  const double* rM = src + 4 * NG;
+  const long long n = gi * gj * (nd == 3 ? gk : 1);
+  const long long vs = d.vstride, mb = d.mbase;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % gi) - 2, j = (int)((q / gi) % gj) - 2, k = nd == 3 ? (int)(q / (gi * gj)) - 2 : 0;
+    const bool oi = i < 0 || i >= ni, oj = j < 0 || j >= nj, ok = nd == 3 && (k < 0 || k >= nk);
+    if ((int)oi + (int)oj + (int)ok > 1) continue;   // corners: not metric cells
+    const long long r = (i + 2) + gi * ((j + 2) + gj * (long long)(k + 2));   // reference linear index
+    const long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    const double* M = rM + 9 * r;   // M(a, c) at (a - 1) + 3 (c - 1)
+    if (!oi && !oj && !ok) {
+      vol[mb + o] = rvol[r];
+      for (int h = 0; h < 3; ++h) dl[3 * mb + h * vs + o] = rdl[3 * r + h];
+      if (Mt)
+        for (int a = 0; a < 2; ++a)
+          for (int c = 0; c < 2; ++c) Mt[4 * mb + (a + 2 * c) * vs + o] = M[a + 3 * c];
+      for (int dd = 0; dd < ndir; ++dd) {
+        double m0 = M[dd + 0], m1 = M[dd + 3], m2 = M[dd + 6];
+        double nrm = sqrt(m0 * m0 + m1 * m1 + m2 * m2);
+        vers[9 * mb + (3 * dd + 0) * vs + o] = m0 / nrm;
+        vers[9 * mb + (3 * dd + 1) * vs + o] = m1 / nrm;
+        vers[9 * mb + (3 * dd + 2) * vs + o] = m2 / nrm;
+      }
+    } else {
+      const int dir = oi ? 0 : oj ? 1 : 2;
+      dl[3 * mb + dir * vs + o] = rdl[3 * r + dir];
+      const bool first = (oi && (i == -1 || i == ni)) || (oj && (j == -1 || j == nj));
+      if (Mt && nd == 2 && first)
+        for (int a = 0; a < 2; ++a)
+          for (int c = 0; c < 2; ++c) Mt[4 * mb + (a + 2 * c) * vs + o] = M[a + 3 * c];
+    }
+  }
+}
+
+// The face part of the same input: dir(dir+1)%f, (N(3), A) per face, onto the
+// low-face planes (the face of reference index I along i is the low face of
+// 0-based cell I).
+__global__ void k_faces_from_ref(const BlockDesc* blk, int b, const double* src, double* face, int nd, int dir) {
+  const BlockDesc& d = blk[b];
+  const int ei = d.ni + (dir == 0), ej = d.nj + (dir == 1), ek = d.nk + (dir == 2);
+  const long long n = (long long)ei * ej * ek;
+  const long long vs = d.vstride, mb = d.mbase;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % ei), j = (int)((q / ei) % ej), k = (int)(q / ((long long)ei * ej));
+    const long long o = (nd == 3) ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
+    const double* f = src + 4 * q;
+    double* g = face + 12 * mb + (4 * dir) * vs + o;
+    g[0] = f[0]; g[vs] = f[1]; g[2 * vs] = f[2]; g[3 * vs] = f[3];
+  }
+}
+
 // Ghost dl along the face direction for each boundary record:
 // BC_Connect_Metrics (101), BC_Symmetry_Metrics (300), BC_Extrapolate_Metrics
 // (everything else), Lib_Metrics.f90:535-1092.
@@ -809,6 +874,22 @@ void launch_ghost_metrics(const BlockDesc* dblk, const void* recs, int nrec, con
   k_ghost_metrics<<<(nrec + 127) / 128, 128, 0, s>>>(dblk, (const GhostMetricRec*)recs, nrec, nodes,
                                                      const_cast<double*>(m.dl), const_cast<double*>(m.Mt), nd, ndir,
                                                      err);
+}
+void launch_metrics_from_ref(const BlockDesc* dblk, int b, const int* dims, const double* src, MetricArgs m, int nd,
+                             int ndir, cudaStream_t s) {
+  const int ni = dims[0], nj = dims[1], nk = dims[2];
+  const long long ncell = (long long)(ni + 4) * (nj + 4) * (nd == 3 ? nk + 4 : 1);
+  k_metrics_from_ref<<<grid_for(ncell, 256), 256, 0, s>>>(dblk, b, src, const_cast<double*>(m.dl),
+                                                           const_cast<double*>(m.vol), const_cast<double*>(m.vers),
+                                                           const_cast<double*>(m.Mt), nd, ndir);
+  const long long NG = (long long)(ni + 4) * (nj + 4) * (nk + 4);
+  const double* f = src + 13 * NG;
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long nf = (long long)(ni + (dir == 0)) * (nj + (dir == 1)) * (nk + (dir == 2));
+    if (dir < nd)
+      k_faces_from_ref<<<grid_for(nf, 256), 256, 0, s>>>(dblk, b, f, const_cast<double*>(m.face), nd, dir);
+    f += 4 * nf;
+  }
 }
 void launch_uniform_check(const BlockDesc* dblk, int b, long long ncell, MetricArgs m, int nd, int ndir,
                           int* flags, double* firsts, double tol, cudaStream_t s) {

@@ -26,7 +26,15 @@ namespace {
 struct HostBlock {
   int ni, nj, nk;
   std::vector<double> node;
+  std::vector<double> metrics;   // precomputed Setup_Metrics output (reference layout), or empty
 };
+
+// Doubles of mose_gpu_add_block's precomputed metrics: vol, dl%c(3), M%c(3,3)
+// over the ghosted cells, then the (N(3), A) of the i-, j- and k-faces.
+size_t ref_metrics_size(int ni, int nj, int nk) {
+  const size_t NG = (size_t)(ni + 4) * (nj + 4) * (nk + 4);
+  return 13 * NG + 4 * ((size_t)(ni + 1) * nj * nk + (size_t)ni * (nj + 1) * nk + (size_t)ni * nj * (nk + 1));
+}
 
 struct BcRecord {
   int b, i, j, k, f, type, bs, is, js, ks, fs, d11, d12, d21, d22;
@@ -431,8 +439,9 @@ int mose_gpu_create(const mose_gpu_config* cfg, mose_gpu_ctx** out) {
   if (!cfg || !out) return MOSE_ERR_INVALID;
   *out = nullptr;
   if (cfg->abi_version != MOSE_GPU_ABI_VERSION) return MOSE_ERR_INVALID;
-  // integration-variables = prim runs in the reference-exact precision
-  if (cfg->integration == MOSE_INTEGRATION_PRIM && cfg->precision != MOSE_PRECISION_FP64_EXACT)
+  // integration-variables = prim runs in the reference-exact and fp64
+  // precisions (the mixed precision's FP32 face states are not kept with it)
+  if (cfg->integration == MOSE_INTEGRATION_PRIM && cfg->precision == MOSE_PRECISION_MIXED)
     return MOSE_ERR_UNSUPPORTED;
   if (cfg->n_rk < 1 || cfg->n_rk > 3 || cfg->nsc != 1 ||
       (cfg->integration != MOSE_INTEGRATION_CONS && cfg->integration != MOSE_INTEGRATION_PRIM) ||
@@ -510,7 +519,8 @@ int mose_gpu_error_location(const mose_gpu_ctx* ctx, int32_t* b, int32_t* i, int
   return ctx->devcode;
 }
 
-int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int32_t nk, const double* node) {
+int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int32_t nk, const double* node,
+                       const double* metrics) {
   MOSE_NVTX_RANGE("mose_gpu_add_block");
   if (!ctx || !node) return MOSE_ERR_INVALID;
   if (ctx->ready) return fail(ctx, MOSE_ERR_INVALID, "add_block after setup");
@@ -520,6 +530,7 @@ int mose_gpu_add_block(mose_gpu_ctx* ctx, int32_t b, int32_t ni, int32_t nj, int
   h.ni = ni; h.nj = nj; h.nk = nk;
   size_t n = 3 * (size_t)(ni + 1) * (nj + 1) * (nk + 1);
   h.node.assign(node, node + n);
+  if (metrics) h.metrics.assign(metrics, metrics + ref_metrics_size(ni, nj, nk));
   ctx->hblk.push_back(std::move(h));
   return MOSE_OK;
 }
@@ -889,6 +900,20 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     int rc = check_launch(ctx, "metrics");
     if (rc) return rc;
     rc = poll_device_error(ctx);   // metric failures and index self-checks
+    if (rc) return rc;
+  }
+  // precomputed metrics handed to add_block replace the node-derived ones
+  for (int b = 0; b < nb; ++b) {
+    const HostBlock& h = ctx->hblk[b];
+    if (h.metrics.empty()) continue;
+    DevBuf<double> src;
+    CU(src.alloc(h.metrics.size()));
+    CU(cudaMemcpyAsync(src.p, h.metrics.data(), h.metrics.size() * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    const int dims[3] = {h.ni, h.nj, h.nk};
+    launch_metrics_from_ref(ctx->d_desc.p, b, dims, src.p, m, ctx->nd, ctx->ndir, ctx->stream);
+    CU(cudaStreamSynchronize(ctx->stream));   // src is freed at the end of this scope
+    int rc = check_launch(ctx, "precomputed metrics");
     if (rc) return rc;
   }
   if (!normal_dirs.empty() || !inlet_geo.empty()) {
@@ -1375,9 +1400,15 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
 // the last RK stage, which holds the new state anyway.  With local time
 // stepping each step keeps its standalone pass, so dtlocal always holds the
 // dt of the step that used it, as in the reference.
+// integration-variables = prim in the fp64 precision: each stage is the fp64
+// residual kernel and Newstate_Primitive in its own kernel (the fused fp64
+// stage kernels carry the conservative update only)
+static bool prim_phased(const mose_gpu_ctx* ctx) {
+  return ctx->gas.prim != 0 && ctx->cfg.precision == MOSE_PRECISION_FP64;
+}
 static bool fused_dt(const mose_gpu_ctx* ctx) {
   return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0 && ctx->gas.model == 0 &&
-         !ctx->adj_dt_standalone;
+         !ctx->adj_dt_standalone && !prim_phased(ctx);
 }
 static void fuse_next_dt(mose_gpu_ctx* ctx, StageArgs& a) {
   a.dtmin = ctx->dtmin.p;
@@ -1472,10 +1503,14 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
     k += enqueue_stage_ghosts(ctx, pc);
     if (ctx->irs_beta > 0.0) {
       k += enqueue_irs_stage(ctx, pc, s0, pn, irk);
-    } else if (ctx->gas.model > 0) {
-      // Navier-Stokes: the residual of every term, then Newstate_Conservative
+    } else if (ctx->gas.model > 0 || prim_phased(ctx)) {
+      // Navier-Stokes: the residual of every term; primitive integration in
+      // fp64: the fp64 residual kernel; then Newstate
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-      launch_visc_residual2d(a, (int)ctx->hblk.size(), ctx->maxcell, ctx->cfg.limiter, ctx->stream);
+      if (ctx->gas.model > 0)
+        launch_visc_residual2d(a, (int)ctx->hblk.size(), ctx->maxcell, ctx->cfg.limiter, ctx->stream);
+      else
+        k += launch_stage(ctx, a, 1, MOSE_PRECISION_FP64, ctx->uniform) - 1;
       launch_rk_stage_to(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[pc].p, ctx->state[s0].p,
                          ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->cfg.time_accurate ? ctx->scal.p : nullptr,
                          ctx->state[pn].p, ctx->gas, a.c_rk, ctx->nd, ctx->uniform, ctx->derr.p, ctx->stream);

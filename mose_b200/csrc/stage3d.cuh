@@ -230,6 +230,14 @@ __global__ void __launch_bounds__(SB_T, 2) k_kface3d(StageArgs a, const int4* it
 // are formed, so it lands during the cell updates; with no k-march state in
 // registers three CTAs fit on an SM.
 constexpr int H3X = T3X + 4, H3Y = T3Y + 4;  // plane region: the tile and two halo cells per side
+// Threads of a plane-stage CTA.  The fast policies: one per tile cell (256),
+// three CTAs per SM at 80 registers.  The reference-exact policy: 320, so
+// that the slope (592 per plane) and face (552) phases take two rounds each
+// instead of three, at two CTAs per SM; its IEEE divisions and square roots
+// make each round long enough for that to pay (1.07 against 1.02 G
+// cell-updates/s on 8 x 128^3, where the fast policies lose 5-8 % with it).
+template <class PH>
+constexpr int s3_threads() { return PH::kFast ? T3X * T3Y : 320; }
 
 template <int NVS, bool UNI>
 struct Stage3dSmem {
@@ -252,11 +260,13 @@ constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5, UNI>); }
 // connection, formed here from the staged ghosts (i, j) or by the k-face
 // march (k) and added in its boundary-face position.  Both add a cell's terms
 // in the same order, so their results are identical.
-template <bool BC>
-constexpr int stage3d_min_ctas() { return BC ? 2 : 3; }
+template <class PH, bool BC>
+constexpr int stage3d_min_ctas() { return (BC || !PH::kFast) ? 2 : 3; }
 
 template <class PH, int RIE, int LIM, bool UNI, int MODE, bool BC>
-__global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageArgs a, const int4* items, int nitems) {
+__global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
+    k_stage3d(StageArgs a, const int4* items, int nitems) {
+  constexpr int S3_T = s3_threads<PH>();
   using namespace s3;
   extern __shared__ __align__(16) unsigned char smem3[];
   Stage3dSmem<NV, UNI>& S = *reinterpret_cast<Stage3dSmem<NV, UNI>*>(smem3);
@@ -291,7 +301,7 @@ __global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageA
     // j0 + T3Y + 1
     auto stage_plane = [&](int kk) {
       constexpr int CA = H3X / 2, CB = T3X / 2;   // chunks per row
-      for (int e = t; e < T3Y * CA + 4 * CB; e += SB_T) {
+      for (int e = t; e < T3Y * CA + 4 * CB; e += S3_T) {
         int cx, ry;
         if (e < T3Y * CA) { cx = 2 * (e % CA); ry = 2 + e / CA; }
         else { const int q = e - T3Y * CA; cx = 2 + 2 * (q % CB); const int r = q / CB; ry = r < 2 ? r : T3Y + r; }
@@ -314,7 +324,7 @@ __global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageA
 #pragma unroll 1
     for (int k = k0; k < k1; ++k) {
       if constexpr (!UNI) {
-        for (int e = t; e < T3Y * H3X + 4 * T3X; e += SB_T) {
+        for (int e = t; e < T3Y * H3X + 4 * T3X; e += S3_T) {
           int cx, ry;
           if (e < T3Y * H3X) { cx = e % H3X; ry = 2 + e / H3X; }
           else { const int q = e - T3Y * H3X; cx = 2 + q % T3X; const int r = q / T3X; ry = r < 2 ? r : T3Y + r; }
@@ -334,7 +344,7 @@ __global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageA
       // (one index space for both, so the items beyond one per thread spread
       // over different threads)
       constexpr int NSX = T3Y * (T3X + 2), NSY = (T3Y + 2) * T3X;
-      for (int e = t; e < NSX + NSY; e += SB_T) {
+      for (int e = t; e < NSX + NSY; e += S3_T) {
         double qa[NV], q[NV], qb[NV], sl[NV];
         if (e < NSX) {
           const int x = e % (T3X + 2), y = e / (T3X + 2);
@@ -360,7 +370,7 @@ __global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageA
       __syncthreads();
       // ---- interior face fluxes of the tile: i-faces (i0 - 1 + x) + 1/2, j-faces (j0 - 1 + y) + 1/2
       constexpr int NFX = T3Y * (T3X + 1), NFY = (T3Y + 1) * T3X;
-      for (int e = t; e < NFX + NFY; e += SB_T) {
+      for (int e = t; e < NFX + NFY; e += S3_T) {
         double PL[NV], PR[NV], sL[NV], sR[NV], F[NV], n[3];
         if (e < NFX) {
           const int x = e % (T3X + 1), y = e / (T3X + 1);
@@ -393,23 +403,31 @@ __global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageA
           for (int v = 0; v < NV; ++v) S.G[v][y][x] = F[v];
         }
       }
-      // the cell's own state, and its k-face fluxes and stage-start state
-      // from HBM: issued before the barrier, so the loads are in flight while
-      // the last faces of the plane are formed
+      // the cell's own state from the plane, its k-face fluxes and
+      // stage-start state from HBM.  The mixed policy issues the HBM loads
+      // before the barrier, in flight while the last faces of the plane are
+      // formed (2.99 against 2.81 G cell-updates/s on 8 x 128^3); the FP64
+      // policies after it, where the 15 loaded values are not live across
+      // the barrier and the next plane's copy (16 against 88 B of spills at
+      // 80 registers; 3.08 against 2.91 G in fp64)
       const long long o = ok3(k);
       const bool first = (a.irk == 1);
       double p0[NV], Hm[NV], Hp[NV], QO[NV];
-      if (mine) {
-#pragma unroll
-        for (int v = 0; v < NV; ++v) p0[v] = S.P[v][ty + 2][tx + 2];
+      auto load_cell = [&]() {
         const double* Hk = a.Hk + d.sbase;
         if (!BC || k > 0) loadQ(Hk, vs, ok3(k - 1), Hm);
         if (!BC || k < nk - 1) loadQ(Hk, vs, o, Hp);
         if (MODE != 1 && !first) loadQ(a.Po + d.sbase, vs, o, QO);
+      };
+      if (mine) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) p0[v] = S.P[v][ty + 2][tx + 2];
+        if constexpr (PH::kMixed) load_cell();
       }
       __syncthreads();   // faces formed, the plane read: the next plane may land
       if (k + 1 < k1) stage_plane(k + 1);
       if (!mine) continue;
+      if constexpr (!PH::kMixed) load_cell();
       // ---- the residual of cell (i, j, k) in the reference's order
       ResAcc<NV, PH::kCompensated> R;
       R.init();
@@ -472,13 +490,13 @@ __global__ void __launch_bounds__(SB_T, stage3d_min_ctas<BC>()) k_stage3d(StageA
     }
   }
   if constexpr (MODE == 2) {
-    __shared__ double red[SB_T / 32];
+    __shared__ double red[S3_T / 32];
     for (int s = 16; s > 0; s >>= 1) dtrun = fmin(dtrun, __shfl_xor_sync(0xffffffffu, dtrun, s));
     if ((t & 31) == 0) red[t >> 5] = dtrun;
     __syncthreads();
     if (t == 0) {
       double v = red[0];
-      for (int w = 1; w < SB_T / 32; ++w) v = fmin(v, red[w]);
+      for (int w = 1; w < S3_T / 32; ++w) v = fmin(v, red[w]);
       atomicMin(a.dtmin, (unsigned long long)__double_as_longlong(v));
     }
   }

@@ -15,10 +15,11 @@ namespace mose {
 // The persistent grid of a kernel instance: one CTA per resident slot, at
 // most one per item.
 template <class K>
-static int persistent_grid(K kernel, size_t smem, int nsm, int n, int& occ) {
+static int persistent_grid(K kernel, int threads, size_t smem, int nsm, int n, int& occ) {
   if (occ == 0) {
     if (smem > 0) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, SB_T, smem) != cudaSuccess || occ < 1) occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess || occ < 1)
+      occ = 1;
   }
   return n < occ * nsm ? n : occ * nsm;
 }
@@ -35,18 +36,18 @@ static void launch3d(const StageArgs& a, int nsm, cudaStream_t s) {
   static int occ_k = 0, occ_n = 0, occ_b = 0;   // one set per kernel instance
   if (a.nitems3[2] > 0) {
     const int n = a.nitems3[2];
-    const int g = persistent_grid(k_kface3d<PH, RIE, LIM, UNI>, 0, nsm, n, occ_k);
+    const int g = persistent_grid(k_kface3d<PH, RIE, LIM, UNI>, SB_T, 0, nsm, n, occ_k);
     k_kface3d<PH, RIE, LIM, UNI><<<g, SB_T, 0, s>>>(a, a.items3[2], n);
   }
   if (a.nitems3[0] > 0) {
     const int n = a.nitems3[0];
-    const int g = persistent_grid(k_stage3d<PH, RIE, LIM, UNI, MODE, false>, smem, nsm, n, occ_n);
-    k_stage3d<PH, RIE, LIM, UNI, MODE, false><<<g, SB_T, smem, s>>>(a, a.items3[0], n);
+    const int g = persistent_grid(k_stage3d<PH, RIE, LIM, UNI, MODE, false>, s3_threads<PH>(), smem, nsm, n, occ_n);
+    k_stage3d<PH, RIE, LIM, UNI, MODE, false><<<g, s3_threads<PH>(), smem, s>>>(a, a.items3[0], n);
   }
   if (a.nitems3[1] > 0) {
     const int n = a.nitems3[1];
-    const int g = persistent_grid(k_stage3d<PH, RIE, LIM, UNI, MODE, true>, smem, nsm, n, occ_b);
-    k_stage3d<PH, RIE, LIM, UNI, MODE, true><<<g, SB_T, smem, s>>>(a, a.items3[1], n);
+    const int g = persistent_grid(k_stage3d<PH, RIE, LIM, UNI, MODE, true>, s3_threads<PH>(), smem, nsm, n, occ_b);
+    k_stage3d<PH, RIE, LIM, UNI, MODE, true><<<g, s3_threads<PH>(), smem, s>>>(a, a.items3[1], n);
   }
 }
 

@@ -15,7 +15,7 @@ module mose_gpu_m
   implicit none
   private
 
-  integer(c_int32_t), parameter, public :: MOSE_GPU_ABI_VERSION = 1
+  integer(c_int32_t), parameter, public :: MOSE_GPU_ABI_VERSION = 2
   integer(c_int), parameter, public :: MOSE_OK = 0
 
   type, bind(C), public :: mose_gpu_config
@@ -76,7 +76,9 @@ module mose_gpu_m
       integer(c_int32_t), intent(out) :: j
       integer(c_int32_t), intent(out) :: k
     end function
-    integer(c_int) function mose_gpu_add_block(ctx, b, ni, nj, nk, node) bind(C, name="mose_gpu_add_block")
+    ! metrics: c_loc of the packed Setup_Metrics arrays (layout in mose_gpu.h),
+    ! or c_null_ptr to form them on the device from the nodes
+    integer(c_int) function mose_gpu_add_block(ctx, b, ni, nj, nk, node, metrics) bind(C, name="mose_gpu_add_block")
       import :: c_ptr, c_int, c_int32_t, c_double
       type(c_ptr), value :: ctx
       integer(c_int32_t), value :: b
@@ -84,6 +86,7 @@ module mose_gpu_m
       integer(c_int32_t), value :: nj
       integer(c_int32_t), value :: nk
       real(c_double), intent(in) :: node(*)
+      type(c_ptr), value :: metrics
     end function
     integer(c_int) function mose_gpu_set_bcs(ctx, rec, dat, nbound) bind(C, name="mose_gpu_set_bcs")
       import :: c_ptr, c_int, c_int32_t, c_double

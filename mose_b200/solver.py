@@ -43,11 +43,27 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def pack_metrics(vol, dl, M, faces) -> np.ndarray:
+    """A block's Setup_Metrics output in the layout mose_gpu_add_block takes:
+    vol, dl%c(3) and M%c(3,3) over the ghosted cells (each in its Fortran
+    memory order: arrays shaped (nk+4, nj+4, ni+4[, ...]) C-contiguous), then
+    for each direction d = 1..3 the faces dir(d)%f as (N(3), A) per face;
+    faces = [(N_d, A_d)] with N_d shaped A_d.shape + (3,)."""
+    parts = [np.ascontiguousarray(x, dtype=np.float64).ravel() for x in (vol, dl, M)]
+    for N, A in faces:
+        N = np.asarray(N, dtype=np.float64).reshape(-1, 3)
+        A = np.asarray(A, dtype=np.float64).reshape(-1, 1)
+        parts.append(np.concatenate([N, A], axis=1).ravel())
+    return np.ascontiguousarray(np.concatenate(parts))
+
+
 class Solver:
-    """A GPU context holding one multi-block domain."""
+    """A GPU context holding one multi-block domain.  metrics: optional, per
+    block a pack_metrics() array (or None) of precomputed metrics to use
+    instead of the ones the device forms from the nodes."""
 
     def __init__(self, case: Case, precision: int = _lib.PRECISION_FP64_EXACT, device: int = 0,
-                 upload: bool = True):
+                 upload: bool = True, metrics=None):
         self.lib = _lib.load()
         cfg = _lib.Config()
         self.lib.mose_gpu_default_config(C.byref(cfg))
@@ -81,7 +97,15 @@ class Solver:
         for b, nd in enumerate(case.nodes, start=1):
             nk, nj, ni = nd.shape[0] - 1, nd.shape[1] - 1, nd.shape[2] - 1
             self.dims.append((ni, nj, nk))
-            self._check(self.lib.mose_gpu_add_block(self.h, b, ni, nj, nk, _dp(np.ascontiguousarray(nd))))
+            mb = metrics[b - 1] if metrics is not None else None
+            if mb is not None:
+                mb = np.ascontiguousarray(mb, dtype=np.float64)
+                NG = (ni + 4) * (nj + 4) * (nk + 4)
+                want = 13 * NG + 4 * ((ni + 1) * nj * nk + ni * (nj + 1) * nk + ni * nj * (nk + 1))
+                if mb.size != want:
+                    raise ValueError(f"block {b}: precomputed metrics hold {mb.size} values, the layout {want}")
+            self._check(self.lib.mose_gpu_add_block(self.h, b, ni, nj, nk, _dp(np.ascontiguousarray(nd)),
+                                                    _dp(mb) if mb is not None else None))
         for t, v, periodic in getattr(case, "series", []):
             sid = C.c_int32()
             t = np.ascontiguousarray(t, dtype=np.float64)

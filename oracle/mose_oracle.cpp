@@ -2378,6 +2378,24 @@ int orc_get_faces(const orc_domain* d, int b, int dir, double* N, double* A) {
   return ORC_OK;
 }
 
+// Replaces the block's metrics (tests: precomputed metrics handed to the
+// device must be the ones both sides step with).  Same layouts as the getters.
+int orc_set_metrics(orc_domain* d, int b, const double* vol, const double* dl, const double* M) {
+  if (check_block(d, b)) return ORC_ERR_INVALID;
+  Block& B = d->blk[b - 1];
+  if (vol) std::memcpy(B.vol.data(), vol, B.vol.size() * sizeof(double));
+  if (dl) std::memcpy(B.dl.data(), dl, B.dl.size() * sizeof(double));
+  if (M) std::memcpy(B.M.data(), M, B.M.size() * sizeof(double));
+  return ORC_OK;
+}
+int orc_set_faces(orc_domain* d, int b, int dir, const double* N, const double* A) {
+  if (check_block(d, b) || dir < 1 || dir > 3) return ORC_ERR_INVALID;
+  Block& B = d->blk[b - 1];
+  if (N) std::memcpy(B.fN[dir - 1].data(), N, B.fN[dir - 1].size() * sizeof(double));
+  if (A) std::memcpy(B.fA[dir - 1].data(), A, B.fA[dir - 1].size() * sizeof(double));
+  return ORC_OK;
+}
+
 // Fill_Ghost_Cell, Lib_Ghost.f90:11-137 (single rank: every block is local).
 int orc_fill_ghost_cell(orc_domain* d) {
   int n = (int)d->bc.size();

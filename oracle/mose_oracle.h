@@ -95,6 +95,8 @@ int orc_set_dtlocal(orc_domain* d, int b, const double* dt);
  * faces for direction dir (1..3) over the reference's dir(d)%f bounds. */
 int orc_get_metrics(const orc_domain* d, int b, double* vol, double* dl, double* M);
 int orc_get_faces(const orc_domain* d, int b, int dir, double* N, double* A);
+int orc_set_metrics(orc_domain* d, int b, const double* vol, const double* dl, const double* M);
+int orc_set_faces(orc_domain* d, int b, int dir, const double* N, const double* A);
 
 /* The phases of Explicit_Step (Mod_Explicit.f90:40-85). */
 int orc_fill_ghost_cell(orc_domain* d);

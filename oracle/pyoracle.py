@@ -63,6 +63,8 @@ def load(omp: bool = False, path: str | os.PathLike | None = None) -> C.CDLL:
         getattr(lib, f).argtypes = [D, C.c_int, dp]
     lib.orc_get_metrics.argtypes = [D, C.c_int, dp, dp, dp]
     lib.orc_get_faces.argtypes = [D, C.c_int, C.c_int, dp, dp]
+    lib.orc_set_metrics.argtypes = [D, C.c_int, dp, dp, dp]
+    lib.orc_set_faces.argtypes = [D, C.c_int, C.c_int, dp, dp]
     for f in ("orc_fill_ghost_cell", "orc_fluxes", "orc_bc_fluxes", "orc_copy_state", "orc_set_global_dt"):
         getattr(lib, f).argtypes = [D]
     lib.orc_rk_newstate.argtypes = [D, C.c_int]
@@ -193,6 +195,19 @@ class Oracle:
         A = np.empty(shape)
         self._check(self.lib.orc_get_faces(self.h, b, direction, _dp(N), _dp(A)), "get_faces")
         return N, A
+
+    def set_metrics(self, b, vol, dl, M):
+        ni, nj, nk = self.dims[b - 1]
+        g = (nk + 4, nj + 4, ni + 4)
+        arrs = [np.ascontiguousarray(x, dtype=np.float64) for x in (vol, dl, M)]
+        assert arrs[0].shape == g and arrs[1].shape == g + (3,) and arrs[2].shape == g + (3, 3)
+        self._check(self.lib.orc_set_metrics(self.h, b, *(_dp(x) for x in arrs)), "set_metrics")
+
+    def set_faces(self, b, direction, N, A):
+        N = np.ascontiguousarray(N, dtype=np.float64)
+        A = np.ascontiguousarray(A, dtype=np.float64)
+        assert N.shape == A.shape + (3,)
+        self._check(self.lib.orc_set_faces(self.h, b, direction, _dp(N), _dp(A)), "set_faces")
 
     # phases of Explicit_Step
     def fill_ghost_cell(self):
