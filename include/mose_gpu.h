@@ -281,15 +281,16 @@ int mose_gpu_check_fast_math(int64_t n, uint64_t seed, double* out);
 /* space-reconstruction = MUSCL-SD (Mod_Space.f90:26-31): the limited slopes of
  * every face scaled by the Tramel shock detector (Lib_Shock_Detector.f90,
  * Lib_Reconstruction.f90:24-25).  The detector also feeds HLLC+ and HLLE++.
- * Call before mose_gpu_setup; 2-D blocks of at least 3 x 3 cells. */
+ * Call before mose_gpu_setup; 2-D blocks of at least 3 x 3 cells, or 3-D
+ * blocks of any size. */
 int mose_gpu_set_sd_limiter(mose_gpu_ctx* ctx, int32_t on);
 
 /* irs-beta (Register_Numerics.f90): implicit residual smoothing of every RK
  * stage's residual when beta > 0 (Lib_IRS.f90, Newstate_Conservative's IRS
  * branch Lib_Newstate.f90:40-72); 0 (the default) disables it.  Call before
- * mose_gpu_setup.  2-D, exact or fp64 precision: the stage's residual-only
- * kernel in that precision, then the smoothing kernels and the update in
- * the reference's arithmetic. */
+ * mose_gpu_setup.  2-D and 3-D, exact or fp64 precision: the stage's
+ * residual-only kernel in that precision, then the smoothing kernels and the
+ * update in the reference's arithmetic. */
 int mose_gpu_set_irs_beta(mose_gpu_ctx* ctx, double beta);
 
 /* equations = navier-stokes (Global_m model): model 1 adds the laminar

@@ -32,18 +32,23 @@ void launch_step_dt_final(const unsigned long long* dtmin_bits, double* dtg, dou
                           cudaStream_t s);
 void launch_step_dt_take(unsigned long long* dtmin_bits, double* dtg, double* time, int advance_time, double dt_start,
                          int* iter, cudaStream_t s);
-// Implicit residual smoothing (2-D, conservative integration).
 // 402 inlets: p0 of every record from its time table at the device time
 // (update, Series_Data_m.f90:55-86), written into its BcParam.
 void launch_series_p0(const SeriesRec* recs, int n, const double* tv, const double* time, BcParam* bcp,
                       cudaStream_t s);
+// The 3-D shock detector of every cell into the beta plane arena (from the
+// stage input P, ghosts filled).
+void launch_sd_beta3d(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* beta,
+                      cudaStream_t s);
+// Implicit residual smoothing on 2-D and 3-D blocks (nd), conservative or
+// primitive integration.
 void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* R, MetricArgs m,
-                      const double* dtl, const double* dtg, int use_dtg, Gas g, cudaStream_t s);
-void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s);
+                      const double* dtl, const double* dtg, int use_dtg, Gas g, int nd, cudaStream_t s);
+void launch_irs_ghost(const IrsCopy* list, int n, double* R, int nd, cudaStream_t s);
 void launch_irs_jacobi(const BlockDesc* dblk, int nblk, long long maxcell, const double* R, const double* Rs,
-                       double* out, int dir, double beta, cudaStream_t s);
+                       double* out, int dir, double beta, int nd, cudaStream_t s);
 void launch_irs_update(const BlockDesc* dblk, int nblk, long long maxcell, const double* Pin, const double* PO,
-                       const double* R, double* Pout, Gas g, double c, DevError* err, cudaStream_t s);
+                       const double* R, double* Pout, Gas g, double c, DevError* err, int nd, cudaStream_t s);
 void launch_rk_stage(const BlockDesc* dblk, int nblk, long long maxcell, double* P, const double* PO, const double* R,
                      MetricArgs m, const double* dtl, Gas g, double c, int nd, bool uniform, DevError* err,
                      cudaStream_t s);
@@ -127,9 +132,9 @@ inline bool launch_stage2d(const StageArgs& a, int nsm, int mode, bool uni, int 
   return table[prec][(rie < 4 && a.g.sd == 0) ? rie : 4](a, nsm, mode, uni, lim, s);
 }
 
-// 3-D: three directional sweeps per RK stage; HLLC and AUSM+ compiled in,
-// every other solver through the run-time solver unit (r4, no shock
-// detector in 3-D); all six limiters.
+// 3-D: the k-face march and the plane stage per RK stage; HLLC and AUSM+
+// compiled in, every other solver, and every solver under the shock
+// detector, through the run-time solver unit (r4); all six limiters.
 #define MOSE_STAGE3_DECL(p, r) \
   bool launch_stage3d_p##p##_r##r(const StageArgs& a, int nsm, int mode, bool uni, int lim, cudaStream_t s);
 MOSE_STAGE3_DECL(0, 0) MOSE_STAGE3_DECL(0, 1) MOSE_STAGE3_DECL(0, 4) MOSE_STAGE3_DECL(1, 0) MOSE_STAGE3_DECL(1, 1)
@@ -143,6 +148,6 @@ inline bool launch_stage3d(const StageArgs& a, int nsm, int mode, bool uni, int 
                                 {launch_stage3d_p1_r0, launch_stage3d_p1_r1, launch_stage3d_p1_r4},
                                 {launch_stage3d_p2_r0, launch_stage3d_p2_r1, launch_stage3d_p2_r4}};
   if (prec < 0 || prec > 2 || !stage3d_supported(rie, lim)) return false;
-  return table[prec][rie <= 1 ? rie : 2](a, nsm, mode, uni, lim, s);
+  return table[prec][(rie <= 1 && a.g.sd == 0) ? rie : 2](a, nsm, mode, uni, lim, s);
 }
 }  // namespace mose

@@ -619,33 +619,34 @@ __global__ void k_rk_stage(const BlockDesc* blk, const double* P, const double* 
 }
 
 // ---------------------------------------------------------------------------
-// Implicit residual smoothing on 2-D blocks (Newstate_Conservative with IRS,
+// Implicit residual smoothing (Newstate_Conservative with IRS,
 // Lib_Newstate.f90:40-72, and Lib_IRS.f90), in the reference's arithmetic:
 // scale R to the conservative increment, then per direction the first ghost
 // layer of R and two Jacobi sweeps, then the RK stage on the smoothed
-// increment.
+// increment.  NV = 4: 2-D blocks (ni x nj); NV = 5: 3-D (ni x nj x nk).
 // ---------------------------------------------------------------------------
 // Scale_Residual_Cons :98-103 (strangcoeff = 1): R = -(R / vol * dt); with
 // integration-variables = prim, Compute_Prim_Residual (:255-302) of the
 // stage's primitives P (Newstate_Primitive's IRS branch, :195-231)
+template <int NV>
 __global__ void k_irs_scale(const BlockDesc* blk, const double* P, double* R, MetricArgs m, const double* dtl,
                             const double* dtg, int use_dtg, Gas g) {
   const int b = blockIdx.y;
   const BlockDesc& d = blk[b];
-  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  const long long ncell = (long long)d.ni * d.nj * (NV == 5 ? d.nk : 1), vs = d.vstride;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
-    const long long o = cell_off2(d, i, j);
+    const int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    const long long o = NV == 5 ? cell_off3(d, i, j, k) : cell_off2(d, i, j);
     const double vol = m.vol[d.mbase + o];
     const double dt = use_dtg ? *dtg : dtl[d.mbase + o];
     if (g.prim) {
-      double Q[4], Rv[4];
-      for (int v = 0; v < 4; ++v) { Q[v] = P[d.sbase + v * vs + o]; Rv[v] = R[d.sbase + v * vs + o]; }
-      prim_residual<4>(g, Q, Rv, vol, dt);
-      for (int v = 0; v < 4; ++v) R[d.sbase + v * vs + o] = Rv[v];
+      double Q[NV], Rv[NV];
+      for (int v = 0; v < NV; ++v) { Q[v] = P[d.sbase + v * vs + o]; Rv[v] = R[d.sbase + v * vs + o]; }
+      prim_residual<NV>(g, Q, Rv, vol, dt);
+      for (int v = 0; v < NV; ++v) R[d.sbase + v * vs + o] = Rv[v];
       continue;
     }
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < NV; ++v) {
       double* r = R + d.sbase + v * vs + o;
       *r = -(*r / vol * dt);
     }
@@ -653,25 +654,28 @@ __global__ void k_irs_scale(const BlockDesc* blk, const double* P, double* R, Me
 }
 // Ghost_Residual_Extrapolation :130-187: 101 copies the source cell, every
 // other record its own boundary cell (ghost and source cells are disjoint)
+template <int NV>
 __global__ void k_irs_ghost(const IrsCopy* list, int n, double* R) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n) return;
   const IrsCopy e = list[q];
-  for (int v = 0; v < 4; ++v) R[e.dst + v * e.vsd] = R[e.src + v * e.vss];
+  for (int v = 0; v < NV; ++v) R[e.dst + v * e.vsd] = R[e.src + v * e.vss];
 }
-// One Jacobi sweep along dir (Residual_Smoothing_Blk :64-80):
-// out = (R + beta (Rs(-1) + Rs(+1))) / (1 + 2 beta).  out may be R itself:
-// each cell reads its own R before writing it, neighbours come from Rs.
+// One Jacobi sweep along dir (Residual_Smoothing_Blk :64-80, the i, j and k
+// loops alike): out = (R + beta (Rs(-1) + Rs(+1))) / (1 + 2 beta).  out may
+// be R itself: each cell reads its own R before writing it, neighbours come
+// from Rs.
+template <int NV>
 __global__ void k_irs_jacobi(const BlockDesc* blk, const double* R, const double* Rs, double* out, int dir,
                              double beta) {
   const int b = blockIdx.y;
   const BlockDesc& d = blk[b];
-  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
-  const long long step = dir == 0 ? 1 : d.px;
+  const long long ncell = (long long)d.ni * d.nj * (NV == 5 ? d.nk : 1), vs = d.vstride;
+  const long long step = dir == 0 ? 1 : dir == 1 ? d.px : d.plane;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
-    const long long o = d.sbase + cell_off2(d, i, j);
-    for (int v = 0; v < 4; ++v) {
+    const int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    const long long o = d.sbase + (NV == 5 ? cell_off3(d, i, j, k) : cell_off2(d, i, j));
+    for (int v = 0; v < NV; ++v) {
       const long long ov = o + v * vs;
       const double r = R[ov];
       out[ov] = (r + beta * (Rs[ov - step] + Rs[ov + step])) / (1.0 + 2.0 * beta);
@@ -680,36 +684,55 @@ __global__ void k_irs_jacobi(const BlockDesc* blk, const double* R, const double
 }
 // Update_State_Cons_IRS :106-131: RK_stage on the smoothed increment, then
 // cons2prim and Check_And_Fix_State.  Pout may be Pin (the phase path).
+template <int NV>
 __global__ void k_irs_update(const BlockDesc* blk, const double* Pin, const double* PO, const double* R, double* Pout,
                              Gas g, double c, DevError* err) {
+  constexpr int P = NV - 1;
   const int b = blockIdx.y;
   const BlockDesc& d = blk[b];
-  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  const long long ncell = (long long)d.ni * d.nj * (NV == 5 ? d.nk : 1), vs = d.vstride;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
-    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
-    const long long o = d.sbase + cell_off2(d, i, j);
-    double Q[4], QO[4], U[4], U0[4];
-    for (int v = 0; v < 4; ++v) { Q[v] = Pin[o + v * vs]; QO[v] = PO[o + v * vs]; }
+    const int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    const long long o = d.sbase + (NV == 5 ? cell_off3(d, i, j, k) : cell_off2(d, i, j));
+    double Q[NV], QO[NV], U[NV], U0[NV];
+    for (int v = 0; v < NV; ++v) { Q[v] = Pin[o + v * vs]; QO[v] = PO[o + v * vs]; }
     if (g.prim) {   // Newstate_Primitive :218-226: RK_stage on the smoothed primitive increment
-      double Rp[4];
-      for (int v = 0; v < 4; ++v) Rp[v] = R[o + v * vs];
-      if (!rk_prim_stage<4>(Q, QO, Rp, c)) report(err, 5, b, i, j, 0);
-      for (int v = 0; v < 4; ++v) Pout[o + v * vs] = Q[v];
+      double Rp[NV];
+      for (int v = 0; v < NV; ++v) Rp[v] = R[o + v * vs];
+      if (!rk_prim_stage<NV>(Q, QO, Rp, c)) report(err, 5, b, i, j, k);
+      for (int v = 0; v < NV; ++v) Pout[o + v * vs] = Q[v];
       continue;
     }
-    ex::prim2cons<4>(g, QO, U0);
-    ex::prim2cons<4>(g, Q, U);
-    for (int v = 0; v < 4; ++v) {
+    ex::prim2cons<NV>(g, QO, U0);
+    ex::prim2cons<NV>(g, Q, U);
+    for (int v = 0; v < NV; ++v) {
       const double r_ = (U[v] - U0[v] + R[o + v * vs]) * c;
       U[v] = U0[v] + r_;
     }
-    ex::cons2prim<4>(g, U, Q);
+    ex::cons2prim<NV>(g, U, Q);
     bool bad = false;
-    for (int v = 0; v < 4; ++v) bad |= isnan(Q[v]);
-    bad |= (Q[3] < 0.0);
-    if (bad) report(err, 5, b, i, j, 0);
+    for (int v = 0; v < NV; ++v) bad |= isnan(Q[v]);
+    bad |= (Q[P] < 0.0);
+    if (bad) report(err, 5, b, i, j, k);
     if (Q[0] < 1e-20) Q[0] = 1e-20;
-    for (int v = 0; v < 4; ++v) Pout[o + v * vs] = Q[v];
+    for (int v = 0; v < NV; ++v) Pout[o + v * vs] = Q[v];
+  }
+}
+
+// The shock detector of every cell of the 3-D blocks (Fluxes_blk's SD_Tramel
+// pass, Mod_Fluxes.f90:78-85) into the beta plane arena, from the pressures
+// of the cell and its six face neighbours (ghosts at the block edges).
+__global__ void k_sd_beta3d(const BlockDesc* blk, const double* P, double* beta) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = blk[b];
+  const long long ncell = (long long)d.ni * d.nj * d.nk, vs = d.vstride;
+  const double* p = P + d.sbase + 4 * vs;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell; q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % d.ni), j = (int)((q / d.ni) % d.nj), k = (int)(q / ((long long)d.ni * d.nj));
+    const long long o = cell_off3(d, i, j, k);
+    beta[d.mbase + o] = ex::sd_tramel3(p[o], p[cell_off3(d, i - 1, j, k)], p[cell_off3(d, i + 1, j, k)],
+                                       p[cell_off3(d, i, j - 1, k)], p[cell_off3(d, i, j + 1, k)],
+                                       p[cell_off3(d, i, j, k - 1)], p[cell_off3(d, i, j, k + 1)]);
   }
 }
 
@@ -954,22 +977,32 @@ void launch_rk_stage_to(const BlockDesc* dblk, int nblk, long long maxcell, cons
   }
 }
 void launch_irs_scale(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* R, MetricArgs m,
-                      const double* dtl, const double* dtg, int use_dtg, Gas g, cudaStream_t s) {
+                      const double* dtl, const double* dtg, int use_dtg, Gas g, int nd, cudaStream_t s) {
   dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
-  k_irs_scale<<<grid, 256, 0, s>>>(dblk, P, R, m, dtl, dtg, use_dtg, g);
+  if (nd == 3) k_irs_scale<5><<<grid, 256, 0, s>>>(dblk, P, R, m, dtl, dtg, use_dtg, g);
+  else k_irs_scale<4><<<grid, 256, 0, s>>>(dblk, P, R, m, dtl, dtg, use_dtg, g);
 }
-void launch_irs_ghost(const IrsCopy* list, int n, double* R, cudaStream_t s) {
-  if (n > 0) k_irs_ghost<<<(n + 255) / 256, 256, 0, s>>>(list, n, R);
+void launch_irs_ghost(const IrsCopy* list, int n, double* R, int nd, cudaStream_t s) {
+  if (n <= 0) return;
+  if (nd == 3) k_irs_ghost<5><<<(n + 255) / 256, 256, 0, s>>>(list, n, R);
+  else k_irs_ghost<4><<<(n + 255) / 256, 256, 0, s>>>(list, n, R);
 }
 void launch_irs_jacobi(const BlockDesc* dblk, int nblk, long long maxcell, const double* R, const double* Rs,
-                       double* out, int dir, double beta, cudaStream_t s) {
+                       double* out, int dir, double beta, int nd, cudaStream_t s) {
   dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
-  k_irs_jacobi<<<grid, 256, 0, s>>>(dblk, R, Rs, out, dir, beta);
+  if (nd == 3) k_irs_jacobi<5><<<grid, 256, 0, s>>>(dblk, R, Rs, out, dir, beta);
+  else k_irs_jacobi<4><<<grid, 256, 0, s>>>(dblk, R, Rs, out, dir, beta);
 }
 void launch_irs_update(const BlockDesc* dblk, int nblk, long long maxcell, const double* Pin, const double* PO,
-                       const double* R, double* Pout, Gas g, double c, DevError* err, cudaStream_t s) {
+                       const double* R, double* Pout, Gas g, double c, DevError* err, int nd, cudaStream_t s) {
   dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
-  k_irs_update<<<grid, 256, 0, s>>>(dblk, Pin, PO, R, Pout, g, c, err);
+  if (nd == 3) k_irs_update<5><<<grid, 256, 0, s>>>(dblk, Pin, PO, R, Pout, g, c, err);
+  else k_irs_update<4><<<grid, 256, 0, s>>>(dblk, Pin, PO, R, Pout, g, c, err);
+}
+void launch_sd_beta3d(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, double* beta,
+                      cudaStream_t s) {
+  dim3 grid(grid_for(maxcell, 256, 148 * 4), nblk);
+  k_sd_beta3d<<<grid, 256, 0, s>>>(dblk, P, beta);
 }
 int norms_partial_count(int nblk, long long maxcell) { return grid_for(maxcell, 256, 148 * 4) * nblk; }
 void launch_residual_norms(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, const double* PO,

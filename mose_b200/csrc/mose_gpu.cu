@@ -230,6 +230,7 @@ struct mose_gpu_ctx {
   DevBuf<double> state[3];
   DevBuf<double> resid;
   DevBuf<double> hk;          // 3-D: the k-face flux arena of the stage kernels
+  DevBuf<double> sdbeta;      // 3-D with the shock detector: beta of every cell (one plane per block)
   DevBuf<double> dl, face, vol, vers, dtl;
   DevBuf<double> Mt;          // Navier-Stokes: 2-D metric tensor planes (null otherwise)
   DevBuf<int> vconn;          // Navier-Stokes: VConn stencils of the connection face cells
@@ -643,18 +644,18 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   if ((ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP || ctx->cfg.riemann == MOSE_RIEMANN_AUSMP_UP2) &&
       !(ctx->gas.minf > 0.0))
     return fail(ctx, MOSE_ERR_INVALID, "AUSM+-up solver selected: Minf must be set (mose_gpu_set_riemann_minf)");
-  if (ctx->gas.sd) {
-    // the detector reads the four face neighbours of every 2-D cell
-    if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector runs on 2-D domains");
-    // (a one-row block, the 1-D cases, reads its j pair from the zero-gradient
-    // ghost rows of its null faces: an exact 0, as in the reference)
+  if (ctx->gas.sd && ctx->nd == 2) {
+    // the 2-D stage kernel reads the four face neighbours of every cell from
+    // its ring (a one-row block, the 1-D cases, reads its j pair from the
+    // zero-gradient ghost rows of its null faces: an exact 0, as in the
+    // reference); 3-D blocks take the detector from its own pass over the
+    // ghosted state
     for (const auto& h : ctx->hblk)
       if (h.ni < 3 || (h.nj < 3 && h.nj != 1))
         return fail(ctx, MOSE_ERR_UNSUPPORTED, "the shock detector needs blocks of at least 3 x 3 cells, or 1-D rows");
   }
-  if (ctx->irs_beta > 0.0 && (ctx->nd != 2 || ctx->cfg.precision == MOSE_PRECISION_MIXED))
-    return fail(ctx, MOSE_ERR_UNSUPPORTED,
-                "implicit residual smoothing runs on 2-D domains in the exact and fp64 precisions");
+  if (ctx->irs_beta > 0.0 && ctx->cfg.precision == MOSE_PRECISION_MIXED)
+    return fail(ctx, MOSE_ERR_UNSUPPORTED, "implicit residual smoothing runs in the exact and fp64 precisions");
   if (ctx->gas.model > 0) {
     if (ctx->nd != 2 || ctx->ndir != 2 || ctx->cfg.precision != MOSE_PRECISION_FP64_EXACT ||
         ctx->cfg.integration != MOSE_INTEGRATION_CONS || ctx->irs_beta > 0.0 || ctx->gas.sd != 0)
@@ -830,6 +831,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
   if (ctx->nd == 3 && ctx->hk.alloc((size_t)ctx->nv * mcur) != cudaSuccess)
     return fail(ctx, MOSE_ERR_CUDA, "out of device memory (k-face arena)");
+  if (ctx->nd == 3 && ctx->gas.sd && ctx->sdbeta.alloc((size_t)mcur) != cudaSuccess)
+    return fail(ctx, MOSE_ERR_CUDA, "out of device memory (shock detector)");
   if (ctx->gas.model > 0) {
     if (ctx->Mt.alloc(4 * (size_t)mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
     CU(cudaMemsetAsync(ctx->Mt.p, 0, 4 * (size_t)mcur * sizeof(double), ctx->stream));
@@ -1054,18 +1057,25 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
 
   // ---- implicit residual smoothing: first-layer ghost records of R ----------------
   if (ctx->irs_beta > 0.0) {
-    static const int inward[4][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}};   // guide(face, 1:2), faces 1..4
+    // guide(face, 1:3), faces 1..6
+    static const int inward[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
     std::vector<IrsCopy> il;
+    // 0-based cell (i, j, k) of a block: its offset in the block's planes
+    auto cell = [&](const BlockDesc& d, int i, int j, int k) -> long long {
+      return ctx->nd == 3 ? (long long)(k + GW) * d.plane + (long long)(j + GW) * d.px + (i + GW)
+                          : (long long)(j + GW) * d.px + (i + GW);
+    };
     for (auto& e : ctx->bc) {
-      if (e.f > 4) continue;                      // 2-D: no ghost layer across k
+      if (e.f > 2 * ctx->nd) continue;            // 2-D: no ghost layer across k
       const BlockDesc& d = ctx->desc[e.b - 1];
-      const int ig = e.i - 1 - inward[e.f - 1][0], jg = e.j - 1 - inward[e.f - 1][1];
+      const int* g = inward[e.f - 1];
+      const int ig = e.i - 1 - g[0], jg = e.j - 1 - g[1], kg = e.k - 1 - g[2];
       const bool conn = e.type == 101;            // 201 takes the zero-gradient branch (Lib_IRS.f90:172-183)
       const BlockDesc& sd = ctx->desc[conn ? e.bs - 1 : e.b - 1];
-      const int is = conn ? e.is - 1 : e.i - 1, js = conn ? e.js - 1 : e.j - 1;
+      const int is = conn ? e.is - 1 : e.i - 1, js = conn ? e.js - 1 : e.j - 1, ks = conn ? e.ks - 1 : e.k - 1;
       IrsCopy c;
-      c.dst = d.sbase + (long long)(jg + GW) * d.px + (ig + GW);
-      c.src = sd.sbase + (long long)(js + GW) * sd.px + (is + GW);
+      c.dst = d.sbase + cell(d, ig, jg, kg);
+      c.src = sd.sbase + cell(sd, is, js, ks);
       c.vsd = d.vstride;
       c.vss = sd.vstride;
       il.push_back(c);
@@ -1255,6 +1265,7 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   a.Pn = pn >= 0 ? ctx->state[pn].p : nullptr;
   a.R = ctx->resid.p;
   a.Hk = ctx->hk.p;
+  a.beta = ctx->sdbeta.p;
   a.m = ctx->margs();
   a.dtl = ctx->dtl.p;
   a.dtg = ctx->scal.p;
@@ -1287,6 +1298,12 @@ static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc) {
 // the kernel count (0: no kernel for this configuration).
 static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int prec, bool uni) {
   if (ctx->nd == 3) {
+    int ksd = 0;
+    if (ctx->gas.sd) {
+      // the shock detector of every cell of the stage input first
+      launch_sd_beta3d(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, a.Pc, ctx->sdbeta.p, ctx->stream);
+      ksd = 1;
+    }
     if (a.nitems3[0] > 0 && a.nitems3[1] > 0) {
       // the k-face march, then the two plane stages side by side (disjoint
       // cells, as the 2-D kernels below): the boundary tiles on stage_aux
@@ -1304,10 +1321,10 @@ static int launch_stage(mose_gpu_ctx* ctx, const StageArgs& a, int mode, int pre
       if (cudaEventRecord(ctx->stage_join, ctx->stage_aux) != cudaSuccess ||
           cudaStreamWaitEvent(ctx->stream, ctx->stage_join, 0) != cudaSuccess)
         return 0;
-      return ok ? 3 : 0;
+      return ok ? 3 + ksd : 0;
     }
     return launch_stage3d(a, ctx->nsm, mode, uni, prec, ctx->cfg.riemann, ctx->cfg.limiter, ctx->stream)
-               ? (a.nitems3[2] > 0) + (a.nitems3[0] > 0) + (a.nitems3[1] > 0)
+               ? ksd + (a.nitems3[2] > 0) + (a.nitems3[0] > 0) + (a.nitems3[1] > 0)
                : 0;
   }
   if (a.nitems > 0 && a.nitems_nb > 0) {
@@ -1381,10 +1398,10 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
     // dtlocal (Compute_dt / Set_Global_dt of the phase path)
     const int nb = (int)ctx->hblk.size();
     launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[ctx->cur].p, ctx->resid.p, ctx->margs(), ctx->dtl.p,
-                     ctx->scal.p, 0, ctx->gas, ctx->stream);
+                     ctx->scal.p, 0, ctx->gas, ctx->nd, ctx->stream);
     ctx->launches += 1 + enqueue_irs_smoothing(ctx);
     launch_irs_update(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[ctx->cur].p, ctx->state[ctx->po].p, ctx->resid.p,
-                      ctx->state[ctx->cur].p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->derr.p,
+                      ctx->state[ctx->cur].p, ctx->gas, RKcoeff[ctx->cfg.n_rk - 1][irk - 1], ctx->derr.p, ctx->nd,
                       ctx->stream);
     ctx->launches++;
     return check_launch(ctx, "rk_stage");
@@ -1396,16 +1413,16 @@ int mose_gpu_rk_stage(mose_gpu_ctx* ctx, int32_t irk) {
   return check_launch(ctx, "rk_stage");
 }
 
-// Time-accurate runs fold the next step's Compute_dt (the CFL minimum) into
-// the last RK stage, which holds the new state anyway.  With local time
-// stepping each step keeps its standalone pass, so dtlocal always holds the
-// dt of the step that used it, as in the reference.
 // integration-variables = prim in the fp64 precision: each stage is the fp64
 // residual kernel and Newstate_Primitive in its own kernel (the fused fp64
 // stage kernels carry the conservative update only)
 static bool prim_phased(const mose_gpu_ctx* ctx) {
   return ctx->gas.prim != 0 && ctx->cfg.precision == MOSE_PRECISION_FP64;
 }
+// Time-accurate runs fold the next step's Compute_dt (the CFL minimum) into
+// the last RK stage, which holds the new state anyway.  With local time
+// stepping each step keeps its standalone pass, so dtlocal always holds the
+// dt of the step that used it, as in the reference.
 static bool fused_dt(const mose_gpu_ctx* ctx) {
   return ctx->cfg.time_accurate != 0 && ctx->irs_beta == 0.0 && ctx->cfg.ramp_iter <= 0 && ctx->gas.model == 0 &&
          !ctx->adj_dt_standalone && !prim_phased(ctx);
@@ -1443,7 +1460,7 @@ static int enqueue_irs_smoothing(mose_gpu_ctx* ctx) {
   const int nb = (int)ctx->hblk.size();
   int k = 0;
   for (int dir = 0; dir < ctx->ndir; ++dir) {
-    launch_irs_ghost(ctx->irs_list.p, ctx->nirs, ctx->resid.p, ctx->stream);
+    launch_irs_ghost(ctx->irs_list.p, ctx->nirs, ctx->resid.p, ctx->nd, ctx->stream);
     // the Jacobi sweeps read both copies: a failed copy is reported by the
     // step's check_launch instead of smoothing stale data silently
     for (double* dst : {ctx->rs1.p, ctx->rs2.p}) {
@@ -1454,9 +1471,9 @@ static int enqueue_irs_smoothing(mose_gpu_ctx* ctx) {
       }
     }
     launch_irs_jacobi(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->rs1.p, ctx->rs2.p, dir, ctx->irs_beta,
-                      ctx->stream);
+                      ctx->nd, ctx->stream);
     launch_irs_jacobi(ctx->d_desc.p, nb, ctx->maxcell, ctx->resid.p, ctx->rs2.p, ctx->resid.p, dir, ctx->irs_beta,
-                      ctx->stream);
+                      ctx->nd, ctx->stream);
     k += (ctx->nirs > 0) + 2;
   }
   return k;
@@ -1475,10 +1492,10 @@ static int enqueue_irs_stage(mose_gpu_ctx* ctx, int pc, int s0, int pn, int irk)
   int k = launch_stage(ctx, a, 1, fp64 ? MOSE_PRECISION_FP64 : MOSE_PRECISION_FP64_EXACT, fp64 && ctx->uniform);
   const int nb = (int)ctx->hblk.size();
   launch_irs_scale(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[pc].p, ctx->resid.p, ctx->margs(), ctx->dtl.p,
-                   ctx->scal.p, ctx->cfg.time_accurate, ctx->gas, ctx->stream);
+                   ctx->scal.p, ctx->cfg.time_accurate, ctx->gas, ctx->nd, ctx->stream);
   k += 1 + enqueue_irs_smoothing(ctx);
   launch_irs_update(ctx->d_desc.p, nb, ctx->maxcell, ctx->state[pc].p, ctx->state[s0].p, ctx->resid.p,
-                    ctx->state[pn].p, ctx->gas, a.c_rk, ctx->derr.p, ctx->stream);
+                    ctx->state[pn].p, ctx->gas, a.c_rk, ctx->derr.p, ctx->nd, ctx->stream);
   return k + 1;
 }
 

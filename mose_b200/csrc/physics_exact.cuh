@@ -559,6 +559,22 @@ __device__ __forceinline__ double sd_tramel2(double p, double p1, double p2, dou
   return 0.0;
 }
 
+// SD_Tramel over the six face neighbours of a 3-D cell (p1/p2 along i, p3/p4
+// along j, p5/p6 along k).
+__device__ __forceinline__ double sd_tramel3(double p, double p1, double p2, double p3, double p4, double p5,
+                                             double p6) {
+  const double DELTA = 20.0;
+  double kp1 = fabs((p2 - 2.0 * p + p1) / (p2 + 2.0 * p + p1));
+  double kp2 = fabs((p4 - 2.0 * p + p3) / (p4 + 2.0 * p + p3));
+  double kp3 = fabs((p6 - 2.0 * p + p5) / (p6 + 2.0 * p + p5));
+  double sw = fmax(fmax(kp1, kp2), kp3);
+  if (sw < 1.0 / DELTA) {
+    double phi = fmax(sw / DELTA, 0.0);
+    return 1.0 - tanh(10.0 * phi * phi * phi);
+  }
+  return 0.0;
+}
+
 // riemann_HLLCHLLE ('HLLC Rotated'), Lib_Riemann_HLL.f90:672-755: HLLE along
 // n1, the direction of the velocity jump, and HLLC along n2 = (-n1y, n1x,
 // n1z), weighted by the (non-negative) projections of the face normal on

@@ -65,9 +65,13 @@ __device__ __forceinline__ void lslope(const double* qa, const double* q, const 
 
 // Face flux between cells L (state PL, slope sL, dl dL) and R from the
 // reconstructed states; n, A the face metric.  false: check_gas_state rejects.
+// beta: the face's shock detector (its low cell's), which scales both slopes
+// under MUSCL-SD (sdl, Lib_Reconstruction.f90:24-25) and goes to the SD
+// Riemann solvers.
 template <class PH, bool UNI>
 __device__ __forceinline__ bool face(const Gas& g, const double* PL, const double* sL, double dL, const double* PR,
-                                     const double* sR, double dR, const double* n, double A, double* F) {
+                                     const double* sR, double dR, const double* n, double A, double* F,
+                                     double beta = 1.0, bool sdl = false) {
   constexpr bool FU = UNI && PH::kFast;
   if constexpr (FU && PH::kFace32) {
     // mixed precision on uniform grids: face states and the solve in FP32
@@ -84,10 +88,11 @@ __device__ __forceinline__ bool face(const Gas& g, const double* PL, const doubl
   double QL[NV], QR[NV];
 #pragma unroll
   for (int v = 0; v < NV; ++v) {
-    QL[v] = PL[v] + sL[v] * hm;
-    QR[v] = PR[v] - sR[v] * hp;
+    const double sl = sdl ? beta * sL[v] : sL[v], sr = sdl ? beta * sR[v] : sR[v];
+    QL[v] = PL[v] + sl * hm;
+    QR[v] = PR[v] - sr * hp;
   }
-  return PH::template face<NV>(g, QL, QR, n, A, F);
+  return PH::template face<NV>(g, QL, QR, n, A, F, beta);
 }
 
 // Boundary-face term of face f (1..6) of boundary cell (i, j, k) of block b:
@@ -125,7 +130,15 @@ __device__ __noinline__ int bc_face(const StageArgs& a, int b, int f, int i, int
     double sL[NV], sR[NV];
     lslope<PH, UNI>(q[0], q[1], q[2], dl[0], dl[1], dl[2], sL);
     lslope<PH, UNI>(q[1], q[2], q[3], dl[1], dl[2], dl[3], sR);
-    face<PH, UNI>(a.g, q[1], sL, dl[1], q[2], sR, dl[2], n, A, F);
+    // the shock detector of a connection face is the boundary cell's
+    // (Lib_BC_Fluxes_Connection.f90:58-62)
+    double bF = 1.0;
+    bool sdl = false;
+    if constexpr (RIE == 4) {
+      if (a.g.sd) bF = a.beta[d.mbase + cell(0)];
+      sdl = (a.g.sd & 1) != 0;
+    }
+    face<PH, UNI>(a.g, q[1], sL, dl[1], q[2], sR, dl[2], n, A, F, bF, sdl);
     return ADD_ALL;
   }
   double Q[NV], Qi[NV];
@@ -169,6 +182,10 @@ __global__ void __launch_bounds__(SB_T, 2) k_kface3d(StageArgs a, const int4* it
     const long long vs = d.vstride;
     const double* P = a.Pc + d.sbase;
     double* H = a.Hk + d.sbase;
+    // the run-time solver kernels carry the shock detector: a face takes its
+    // low cell's beta (a connection face at k = 0, the boundary cell's)
+    constexpr bool SDV = (RIE == 4);
+    const bool sd = SDV && a.g.sd != 0, sdl = SDV && (a.g.sd & 1) != 0;
     double un[3] = {0.0, 0.0, 0.0}, uA = 0.0, udl = 0.0;
     if constexpr (UNI) {
       un[0] = d.u_n[2][0]; un[1] = d.u_n[2][1]; un[2] = d.u_n[2][2];
@@ -204,7 +221,11 @@ __global__ void __launch_bounds__(SB_T, 2) k_kface3d(StageArgs a, const int4* it
       lslope<PH, UNI>(p0, p1, p2, d0, d1, d2, s1);
       if constexpr (UNI) { n[0] = un[0]; n[1] = un[1]; n[2] = un[2]; A = uA; }
       else A = face_at<false>(a, d, 2, ok3(k + 1), n);
-      const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Hf);
+      double bF = 1.0;
+      if constexpr (SDV) {
+        if (sd) bF = a.beta[d.mbase + ok3(k < 0 ? 0 : k)];
+      }
+      const bool ok = face<PH, UNI>(a.g, p0, s0, d0, p1, s1, d1, n, A, Hf, bF, sdl);
       if (!ok) report(a.err, 4, b, i, j, k);
       const long long o = ok3(k);
 #pragma unroll
@@ -271,6 +292,8 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
   extern __shared__ __align__(16) unsigned char smem3[];
   Stage3dSmem<NV, UNI>& S = *reinterpret_cast<Stage3dSmem<NV, UNI>*>(smem3);
   const int t = threadIdx.x, tx = t % T3X, ty = t / T3X;
+  constexpr bool SDV = (RIE == 4);   // the shock detector (run-time solver kernels)
+  const bool sd = SDV && a.g.sd != 0, sdl = SDV && (a.g.sd & 1) != 0;
   double dtrun = __longlong_as_double(0x7ff0000000000000LL);
 #pragma unroll 1
   for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -382,7 +405,11 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
             sL[v] = S.sx[v][y][x]; sR[v] = S.sx[v][y][x + 1];
           }
           const double A = facek(0, off3(d, cl + 1, cj, k), n);
-          const bool ok = face<PH, UNI>(a.g, PL, sL, dxat(y, x + 1), PR, sR, dxat(y, x + 2), n, A, F);
+          double bF = 1.0;
+          if constexpr (SDV) {
+            if (sd) bF = a.beta[d.mbase + off3(d, cl < 0 ? 0 : cl, cj, k)];
+          }
+          const bool ok = face<PH, UNI>(a.g, PL, sL, dxat(y, x + 1), PR, sR, dxat(y, x + 2), n, A, F, bF, sdl);
           if (!ok) report(a.err, 4, b, cl, cj, k);
 #pragma unroll
           for (int v = 0; v < NV; ++v) S.F[v][y][x] = F[v];
@@ -397,7 +424,11 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
             sL[v] = S.sy[v][y][x]; sR[v] = S.sy[v][y + 1][x];
           }
           const double A = facek(1, off3(d, ci, cl + 1, k), n);
-          const bool ok = face<PH, UNI>(a.g, PL, sL, dyat(y + 1, x), PR, sR, dyat(y + 2, x), n, A, F);
+          double bF = 1.0;
+          if constexpr (SDV) {
+            if (sd) bF = a.beta[d.mbase + off3(d, ci, cl < 0 ? 0 : cl, k)];
+          }
+          const bool ok = face<PH, UNI>(a.g, PL, sL, dyat(y + 1, x), PR, sR, dyat(y + 2, x), n, A, F, bF, sdl);
           if (!ok) report(a.err, 4, b, ci, cl, k);
 #pragma unroll
           for (int v = 0; v < NV; ++v) S.G[v][y][x] = F[v];
