@@ -59,6 +59,7 @@ void launch_rk_stage_to(const BlockDesc* dblk, int nblk, long long maxcell, cons
 // Navier-Stokes residual of 2-D blocks (viscous2d.cu): a.Pc with filled
 // ghosts -> a.R, every convective, diffusive and boundary term in the
 // reference's order.  False for an unknown limiter.
+// (two launches: the interior face fluxes into a.Fv, then each cell's residual)
 bool launch_visc_residual2d(const StageArgs& a, int nblk, long long maxcell, int lim, cudaStream_t s);
 // Discrete adjoint (2-D, HLLC; adjoint.cu).
 void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* Ps, const double* Pprev,

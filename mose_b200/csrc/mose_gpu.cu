@@ -234,6 +234,7 @@ struct mose_gpu_ctx {
   DevBuf<double> dl, face, vol, vers, dtl;
   DevBuf<double> Mt;          // Navier-Stokes: 2-D metric tensor planes (null otherwise)
   DevBuf<int> vconn;          // Navier-Stokes: VConn stencils of the connection face cells
+  DevBuf<double> vface;       // Navier-Stokes: the interior face fluxes of the residual (14 planes)
   DevBuf<int> bcw;
   DevBuf<BcParam> bcp;
   DevBuf<GhostRec> ghosts;
@@ -835,6 +836,8 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     return fail(ctx, MOSE_ERR_CUDA, "out of device memory (shock detector)");
   if (ctx->gas.model > 0) {
     if (ctx->Mt.alloc(4 * (size_t)mcur) != cudaSuccess) return fail(ctx, MOSE_ERR_CUDA, "out of device memory (metrics)");
+    if (ctx->vface.alloc(14 * (size_t)mcur) != cudaSuccess)
+      return fail(ctx, MOSE_ERR_CUDA, "out of device memory (viscous face fluxes)");
     CU(cudaMemsetAsync(ctx->Mt.p, 0, 4 * (size_t)mcur * sizeof(double), ctx->stream));
     static_assert(sizeof(VConn) == 5 * sizeof(int), "VConn is five ints");
     CU(ctx->vconn.alloc(5 * std::max<size_t>(vconn.size(), 1)));
@@ -1266,6 +1269,7 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   a.R = ctx->resid.p;
   a.Hk = ctx->hk.p;
   a.beta = ctx->sdbeta.p;
+  a.Fv = ctx->vface.p;
   a.m = ctx->margs();
   a.dtl = ctx->dtl.p;
   a.dtg = ctx->scal.p;
@@ -1371,7 +1375,7 @@ int mose_gpu_residual(mose_gpu_ctx* ctx) {
   if (ctx->gas.model > 0) {
     if (!launch_visc_residual2d(a, (int)ctx->hblk.size(), ctx->maxcell, ctx->cfg.limiter, ctx->stream))
       return fail(ctx, MOSE_ERR_UNSUPPORTED, "no viscous kernel for limiter %d", ctx->cfg.limiter);
-    ctx->launches++;
+    ctx->launches += 2;
     return check_launch(ctx, "residual");
   }
   // the exact residual-only kernels read the metric arrays; the fp64 ones
@@ -1524,9 +1528,10 @@ static int enqueue_step(mose_gpu_ctx* ctx, int s0) {
       // Navier-Stokes: the residual of every term; primitive integration in
       // fp64: the fp64 residual kernel; then Newstate
       StageArgs a = stage_args(ctx, pc, s0, pn, irk);
-      if (ctx->gas.model > 0)
+      if (ctx->gas.model > 0) {
         launch_visc_residual2d(a, (int)ctx->hblk.size(), ctx->maxcell, ctx->cfg.limiter, ctx->stream);
-      else
+        ++k;   // the face pass and the cell pass
+      } else
         k += launch_stage(ctx, a, 1, MOSE_PRECISION_FP64, ctx->uniform) - 1;
       launch_rk_stage_to(ctx->d_desc.p, (int)ctx->hblk.size(), ctx->maxcell, ctx->state[pc].p, ctx->state[s0].p,
                          ctx->resid.p, ctx->margs(), ctx->dtl.p, ctx->cfg.time_accurate ? ctx->scal.p : nullptr,

@@ -260,20 +260,27 @@ constexpr int H3X = T3X + 4, H3Y = T3Y + 4;  // plane region: the tile and two h
 template <class PH>
 constexpr int s3_threads() { return PH::kFast ? T3X * T3Y : 320; }
 
-template <int NVS, bool UNI>
+// F32: the mixed policy on uniform grids, whose limited slopes and per-area
+// face fluxes are FP32 values: held as such (the face area is applied when a
+// cell adds the flux, the same product as before), half the bytes.
+template <int NVS, bool UNI, bool F32 = false>
 struct Stage3dSmem {
+  using T = typename std::conditional<F32, float, double>::type;
   double P[NVS][H3Y][H3X];          // plane k: region cells, corners unused
   double dx[UNI ? 1 : T3Y][UNI ? 1 : H3X];   // dl along i on the tile rows (metric arrays only)
   double dy[UNI ? 1 : H3Y][UNI ? 1 : T3X];   // dl along j on the tile columns
-  double sx[NVS][T3Y][T3X + 2];     // limited i-slope of cells i0 - 1 .. i0 + T3X
-  double sy[NVS][T3Y + 2][T3X];     // limited j-slope of cells j0 - 1 .. j0 + T3Y
-  double F[NVS][T3Y][T3X + 1];      // F(i0 - 1 + x + 1/2)
-  double G[NVS][T3Y + 1][T3X];      // G(j0 - 1 + y + 1/2)
+  T sx[NVS][T3Y][T3X + 2];          // limited i-slope of cells i0 - 1 .. i0 + T3X
+  T sy[NVS][T3Y + 2][T3X];          // limited j-slope of cells j0 - 1 .. j0 + T3Y
+  T F[NVS][T3Y][T3X + 1];           // F(i0 - 1 + x + 1/2) (F32: per unit area)
+  T G[NVS][T3Y + 1][T3X];           // G(j0 - 1 + y + 1/2)
   // the block's uniform metrics: dl (3), face normals (3 x 3), areas (3), volume
   double um[16];
 };
-template <bool UNI>
-constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5, UNI>); }
+template <bool UNI, bool F32 = false>
+constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5, UNI, F32>); }
+// the FP32 shared-memory variant of a policy
+template <class PH, bool UNI>
+constexpr bool stage3d_f32() { return UNI && PH::kFace32; }
 
 // Items: (block, i0 | j0 << 16, k0, k1).  BC: the items with a physical
 // boundary face (the boundary formulas, a call, hold the kernel to two CTAs
@@ -281,16 +288,17 @@ constexpr size_t stage3d_smem_bytes() { return sizeof(Stage3dSmem<5, UNI>); }
 // connection, formed here from the staged ghosts (i, j) or by the k-face
 // march (k) and added in its boundary-face position.  Both add a cell's terms
 // in the same order, so their results are identical.
-template <class PH, bool BC>
-constexpr int stage3d_min_ctas() { return (BC || !PH::kFast) ? 2 : 3; }
+template <class PH, bool BC, bool F32>
+constexpr int stage3d_min_ctas() { return (BC || !PH::kFast) ? 2 : F32 ? 4 : 3; }
 
 template <class PH, int RIE, int LIM, bool UNI, int MODE, bool BC>
-__global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
+__global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC, stage3d_f32<PH, UNI>()>())
     k_stage3d(StageArgs a, const int4* items, int nitems) {
   constexpr int S3_T = s3_threads<PH>();
+  constexpr bool F32 = stage3d_f32<PH, UNI>();
   using namespace s3;
   extern __shared__ __align__(16) unsigned char smem3[];
-  Stage3dSmem<NV, UNI>& S = *reinterpret_cast<Stage3dSmem<NV, UNI>*>(smem3);
+  Stage3dSmem<NV, UNI, F32>& S = *reinterpret_cast<Stage3dSmem<NV, UNI, F32>*>(smem3);
   const int t = threadIdx.x, tx = t % T3X, ty = t / T3X;
   constexpr bool SDV = (RIE == 4);   // the shock detector (run-time solver kernels)
   const bool sd = SDV && a.g.sd != 0, sdl = SDV && (a.g.sd & 1) != 0;
@@ -377,7 +385,7 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
           for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y + 2][x]; q[v] = S.P[v][y + 2][x + 1]; qb[v] = S.P[v][y + 2][x + 2]; }
           lslope<PH, UNI>(qa, q, qb, dxat(y, x), dxat(y, x + 1), dxat(y, x + 2), sl);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) S.sx[v][y][x] = sl[v];
+          for (int v = 0; v < NV; ++v) S.sx[v][y][x] = (typename Stage3dSmem<NV, UNI, F32>::T)sl[v];
         } else {
           const int e2 = e - NSX;
           const int x = e2 % T3X, y = e2 / T3X;
@@ -387,7 +395,7 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
           for (int v = 0; v < NV; ++v) { qa[v] = S.P[v][y][x + 2]; q[v] = S.P[v][y + 1][x + 2]; qb[v] = S.P[v][y + 2][x + 2]; }
           lslope<PH, UNI>(qa, q, qb, dyat(y, x), dyat(y + 1, x), dyat(y + 2, x), sl);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) S.sy[v][y][x] = sl[v];
+          for (int v = 0; v < NV; ++v) S.sy[v][y][x] = (typename Stage3dSmem<NV, UNI, F32>::T)sl[v];
         }
       }
       __syncthreads();
@@ -404,7 +412,9 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
             PL[v] = S.P[v][y + 2][x + 1]; PR[v] = S.P[v][y + 2][x + 2];
             sL[v] = S.sx[v][y][x]; sR[v] = S.sx[v][y][x + 1];
           }
-          const double A = facek(0, off3(d, cl + 1, cj, k), n);
+          // F32: the flux per unit area (an FP32 value, held exactly)
+          const double A = F32 ? 1.0 : facek(0, off3(d, cl + 1, cj, k), n);
+          if constexpr (F32) facek(0, off3(d, cl + 1, cj, k), n);
           double bF = 1.0;
           if constexpr (SDV) {
             if (sd) bF = a.beta[d.mbase + off3(d, cl < 0 ? 0 : cl, cj, k)];
@@ -412,7 +422,7 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
           const bool ok = face<PH, UNI>(a.g, PL, sL, dxat(y, x + 1), PR, sR, dxat(y, x + 2), n, A, F, bF, sdl);
           if (!ok) report(a.err, 4, b, cl, cj, k);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) S.F[v][y][x] = F[v];
+          for (int v = 0; v < NV; ++v) S.F[v][y][x] = (typename Stage3dSmem<NV, UNI, F32>::T)F[v];
         } else {
           const int e2 = e - NFX;
           const int x = e2 % T3X, y = e2 / T3X;
@@ -423,7 +433,9 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
             PL[v] = S.P[v][y + 1][x + 2]; PR[v] = S.P[v][y + 2][x + 2];
             sL[v] = S.sy[v][y][x]; sR[v] = S.sy[v][y + 1][x];
           }
-          const double A = facek(1, off3(d, ci, cl + 1, k), n);
+          // F32: the flux per unit area (an FP32 value, held exactly)
+          const double A = F32 ? 1.0 : facek(1, off3(d, ci, cl + 1, k), n);
+          if constexpr (F32) facek(1, off3(d, ci, cl + 1, k), n);
           double bF = 1.0;
           if constexpr (SDV) {
             if (sd) bF = a.beta[d.mbase + off3(d, ci, cl < 0 ? 0 : cl, k)];
@@ -431,7 +443,7 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
           const bool ok = face<PH, UNI>(a.g, PL, sL, dyat(y + 1, x), PR, sR, dyat(y + 2, x), n, A, F, bF, sdl);
           if (!ok) report(a.err, 4, b, ci, cl, k);
 #pragma unroll
-          for (int v = 0; v < NV; ++v) S.G[v][y][x] = F[v];
+          for (int v = 0; v < NV; ++v) S.G[v][y][x] = (typename Stage3dSmem<NV, UNI, F32>::T)F[v];
         }
       }
       // the cell's own state from the plane, its k-face fluxes and
@@ -462,29 +474,36 @@ __global__ void __launch_bounds__(s3_threads<PH>(), stage3d_min_ctas<PH, BC>())
       // ---- the residual of cell (i, j, k) in the reference's order
       ResAcc<NV, PH::kCompensated> R;
       R.init();
-      if (i > 0) for (int v = 0; v < NV; ++v) R.add(v, -S.F[v][ty][tx]);
-      if (i < ni - 1) for (int v = 0; v < NV; ++v) R.add(v, S.F[v][ty][tx + 1]);
-      if (j > 0) for (int v = 0; v < NV; ++v) R.add(v, -S.G[v][ty][tx]);
-      if (j < nj - 1) for (int v = 0; v < NV; ++v) R.add(v, S.G[v][ty + 1][tx]);
+      // a face flux as the face solve gave it: F32 holds it per unit area
+      auto fx = [&](int v, int x) -> double {
+        if constexpr (F32) return (double)S.F[v][ty][x] * S.um[12]; else return S.F[v][ty][x];
+      };
+      auto gy = [&](int v, int y) -> double {
+        if constexpr (F32) return (double)S.G[v][y][tx] * S.um[13]; else return S.G[v][y][tx];
+      };
+      if (i > 0) for (int v = 0; v < NV; ++v) R.add(v, -fx(v, tx));
+      if (i < ni - 1) for (int v = 0; v < NV; ++v) R.add(v, fx(v, tx + 1));
+      if (j > 0) for (int v = 0; v < NV; ++v) R.add(v, -gy(v, ty));
+      if (j < nj - 1) for (int v = 0; v < NV; ++v) R.add(v, gy(v, ty + 1));
       if (k > 0) for (int v = 0; v < NV; ++v) R.add(v, -Hm[v]);
       if (k < nk - 1) for (int v = 0; v < NV; ++v) R.add(v, Hp[v]);
       // boundary faces in face order 1..6
       if constexpr (!BC) {
         double Fe[NV];
         if (i == 0) {
-          for (int v = 0; v < NV; ++v) Fe[v] = S.F[v][ty][tx];
+          for (int v = 0; v < NV; ++v) Fe[v] = fx(v, tx);
           add_bc<NV>(R, Fe, -1.0, ADD_ALL);
         }
         if (i == ni - 1) {
-          for (int v = 0; v < NV; ++v) Fe[v] = S.F[v][ty][tx + 1];
+          for (int v = 0; v < NV; ++v) Fe[v] = fx(v, tx + 1);
           add_bc<NV>(R, Fe, 1.0, ADD_ALL);
         }
         if (j == 0) {
-          for (int v = 0; v < NV; ++v) Fe[v] = S.G[v][ty][tx];
+          for (int v = 0; v < NV; ++v) Fe[v] = gy(v, ty);
           add_bc<NV>(R, Fe, -1.0, ADD_ALL);
         }
         if (j == nj - 1) {
-          for (int v = 0; v < NV; ++v) Fe[v] = S.G[v][ty + 1][tx];
+          for (int v = 0; v < NV; ++v) Fe[v] = gy(v, ty + 1);
           add_bc<NV>(R, Fe, 1.0, ADD_ALL);
         }
         if (k == 0) add_bc<NV>(R, Hm, -1.0, ADD_ALL);

@@ -32,7 +32,7 @@ static int persistent_grid(K kernel, int threads, size_t smem, int nsm, int n, i
 template <int PREC, int RIE, int LIM, bool UNI, int MODE>
 static void launch3d(const StageArgs& a, int nsm, cudaStream_t s) {
   using PH = StagePolicy<PREC, RIE, LIM>;
-  constexpr size_t smem = stage3d_smem_bytes<UNI>();
+  constexpr size_t smem = stage3d_smem_bytes<UNI, stage3d_f32<PH, UNI>()>();
   static int occ_k = 0, occ_n = 0, occ_b = 0;   // one set per kernel instance
   if (a.nitems3[2] > 0) {
     const int n = a.nitems3[2];

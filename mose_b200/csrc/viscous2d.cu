@@ -3,18 +3,18 @@
 // operation order, compiled with --fmad=false like every reference-exact
 // unit, so it matches the oracle bit for bit.
 //
-// One thread per interior cell forms the cell's whole residual, in the order
-// the reference accumulates it (Mod_Fluxes.f90:86-206, then BC_Fluxes by
-// block and face, Mod_BC_Fluxes.f90:52-216):
+// Two launches per residual.  k_visc_faces2d forms every interior face's
+// convective (4 values) and diffusive (3 values) flux once, one thread per
+// cell for its i+1/2 and j+1/2 faces, into the viscous face arena.  Then one
+// thread per cell forms the cell's whole residual, in the order the reference
+// accumulates it (Mod_Fluxes.f90:86-206, then BC_Fluxes by block and face,
+// Mod_BC_Fluxes.f90:52-216):
 //   convective i-faces (i-1/2, i+1/2), diffusive i-faces, convective j-faces,
-//   diffusive j-faces, then the block-edge faces in face order 1..4, each with
-//   its Euler flux followed by its viscous one (101/201: BC_Connection_Eul +
-//   BC_Connection_Visc; 300: symmetry + BC_Symmetry_Visc; 301: symmetry +
-//   BC_Wall_Heat; 302: symmetry + BC_Wall_Temperature; the others inviscid).
-// Every interior face flux is formed by both of its cells, with the same
-// operations, so each cell sees the values the reference adds to it.  This
-// unit is the correctness path of the viscous terms; the inviscid headline
-// kernels (stage2d.cuh) form each face once.
+//   diffusive j-faces (from the arena), then the block-edge faces in face
+//   order 1..4, each with its Euler flux followed by its viscous one (101/201:
+//   BC_Connection_Eul + BC_Connection_Visc; 300: symmetry + BC_Symmetry_Visc;
+//   301: symmetry + BC_Wall_Heat; 302: symmetry + BC_Wall_Temperature; the
+//   others inviscid).
 //
 // 2-D specialisation of Lib_Diffusive.f90: the out-of-plane gradients are
 // exact zeros in the reference (its k ghost planes are zero-gradient copies,
@@ -323,55 +323,74 @@ __device__ __forceinline__ void add_masked(double* R, const double* F, double sg
   }
 }
 
+// The viscous face arena: 14 planes per block (offset 14 mbase), at the low
+// cell of each interior face: the convective i-face flux (planes 0-3), the
+// diffusive one (4-6), then the same for the j-face (7-10, 11-13).
+constexpr int kVisc_CX = 0, kVisc_DX = 4, kVisc_CY = 7, kVisc_DY = 11;
+
+template <int LIM>
+__global__ void __launch_bounds__(128) k_visc_faces2d(StageArgs a) {
+  const int b = blockIdx.y;
+  const BlockDesc& d = a.blk[b];
+  const Cell2 c{d, a, a.Pc + d.sbase};
+  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  double* Fv = a.Fv + 14 * d.mbase;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell;
+       q += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % d.ni), j = (int)(q / d.ni);
+    const long long o = c.off(i, j);
+    double F[NV];
+    bool ok = true;
+    if (i < d.ni - 1) {
+      ok &= conv_face<LIM>(c, 0, i, j, F);
+      for (int v = 0; v < NV; ++v) Fv[(kVisc_CX + v) * vs + o] = F[v];
+      diff_face(c, 0, i, j, F);
+      for (int v = 0; v < 3; ++v) Fv[(kVisc_DX + v) * vs + o] = F[v];
+    }
+    if (d.nj > 1 && j < d.nj - 1) {
+      ok &= conv_face<LIM>(c, 1, i, j, F);
+      for (int v = 0; v < NV; ++v) Fv[(kVisc_CY + v) * vs + o] = F[v];
+      diff_face(c, 1, i, j, F);
+      for (int v = 0; v < 3; ++v) Fv[(kVisc_DY + v) * vs + o] = F[v];
+    }
+    if (!ok) report(a.err, 4, b, i, j, 0);
+  }
+}
+
 template <int LIM>
 __global__ void __launch_bounds__(128) k_visc_residual2d(StageArgs a) {
   const int b = blockIdx.y;
   const BlockDesc& d = a.blk[b];
   const Cell2 c{d, a, a.Pc + d.sbase};
-  const long long ncell = (long long)d.ni * d.nj;
+  const long long ncell = (long long)d.ni * d.nj, vs = d.vstride;
+  const double* Fv = a.Fv + 14 * d.mbase;
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < ncell;
        q += (long long)gridDim.x * blockDim.x) {
     const int i = (int)(q % d.ni), j = (int)(q / d.ni);
     double R[NV] = {0.0, 0.0, 0.0, 0.0};
     double F[NV];
-    bool ok = true;
+    // plane p of the face whose low cell is (ii, jj)
+    auto fv = [&](int p, int ii, int jj) { return Fv[p * vs + c.off(ii, jj)]; };
     // convective i faces, diffusive i faces (Mod_Fluxes.f90:89-126)
-    if (i > 0) {
-      ok &= conv_face<LIM>(c, 0, i - 1, j, F);
-      for (int v = 0; v < NV; ++v) R[v] = R[v] - F[v];
-    }
-    if (i < d.ni - 1) {
-      ok &= conv_face<LIM>(c, 0, i, j, F);
-      for (int v = 0; v < NV; ++v) R[v] = R[v] + F[v];
-    }
-    if (i > 0) {
-      diff_face(c, 0, i - 1, j, F);
-      for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] + F[v];
-    }
-    if (i < d.ni - 1) {
-      diff_face(c, 0, i, j, F);
-      for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] - F[v];
-    }
+    if (i > 0)
+      for (int v = 0; v < NV; ++v) R[v] = R[v] - fv(kVisc_CX + v, i - 1, j);
+    if (i < d.ni - 1)
+      for (int v = 0; v < NV; ++v) R[v] = R[v] + fv(kVisc_CX + v, i, j);
+    if (i > 0)
+      for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] + fv(kVisc_DX + v, i - 1, j);
+    if (i < d.ni - 1)
+      for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] - fv(kVisc_DX + v, i, j);
     // convective j faces, diffusive j faces (:129-166)
     if (d.nj > 1) {
-      if (j > 0) {
-        ok &= conv_face<LIM>(c, 1, i, j - 1, F);
-        for (int v = 0; v < NV; ++v) R[v] = R[v] - F[v];
-      }
-      if (j < d.nj - 1) {
-        ok &= conv_face<LIM>(c, 1, i, j, F);
-        for (int v = 0; v < NV; ++v) R[v] = R[v] + F[v];
-      }
-      if (j > 0) {
-        diff_face(c, 1, i, j - 1, F);
-        for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] + F[v];
-      }
-      if (j < d.nj - 1) {
-        diff_face(c, 1, i, j, F);
-        for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] - F[v];
-      }
+      if (j > 0)
+        for (int v = 0; v < NV; ++v) R[v] = R[v] - fv(kVisc_CY + v, i, j - 1);
+      if (j < d.nj - 1)
+        for (int v = 0; v < NV; ++v) R[v] = R[v] + fv(kVisc_CY + v, i, j);
+      if (j > 0)
+        for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] + fv(kVisc_DY + v, i, j - 1);
+      if (j < d.nj - 1)
+        for (int v = 0; v < 3; ++v) R[1 + v] = R[1 + v] - fv(kVisc_DY + v, i, j);
     }
-    if (!ok) report(a.err, 4, b, i, j, 0);
     // block-edge faces in face order, Euler part then viscous part
     for (int f = 1; f <= 4; ++f) {
       const bool on = (f == 1 && i == 0) || (f == 2 && i == d.ni - 1) || (f == 3 && j == 0) ||
@@ -410,12 +429,18 @@ __global__ void __launch_bounds__(128) k_visc_residual2d(StageArgs a) {
 bool launch_visc_residual2d(const StageArgs& a, int nblk, long long maxcell, int lim, cudaStream_t s) {
   const dim3 grid((unsigned)std::min<long long>((maxcell + 127) / 128, 148 * 8), (unsigned)nblk);
   switch (lim) {
-    case 0: k_visc_residual2d<0><<<grid, 128, 0, s>>>(a); return true;
-    case 1: k_visc_residual2d<1><<<grid, 128, 0, s>>>(a); return true;
-    case 2: k_visc_residual2d<2><<<grid, 128, 0, s>>>(a); return true;
-    case 3: k_visc_residual2d<3><<<grid, 128, 0, s>>>(a); return true;
-    case 4: k_visc_residual2d<4><<<grid, 128, 0, s>>>(a); return true;
-    case 5: k_visc_residual2d<5><<<grid, 128, 0, s>>>(a); return true;
+#define MOSE_VISC_LIM(L)                                      \
+  case L:                                                      \
+    k_visc_faces2d<L><<<grid, 128, 0, s>>>(a);                 \
+    k_visc_residual2d<L><<<grid, 128, 0, s>>>(a);              \
+    return true;
+    MOSE_VISC_LIM(0)
+    MOSE_VISC_LIM(1)
+    MOSE_VISC_LIM(2)
+    MOSE_VISC_LIM(3)
+    MOSE_VISC_LIM(4)
+    MOSE_VISC_LIM(5)
+#undef MOSE_VISC_LIM
   }
   return false;
 }
