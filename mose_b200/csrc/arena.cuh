@@ -31,6 +31,9 @@ struct StageArgs {
   double* Hk;           // 3-D: interior k-face flux H(k + 1/2) at cell (i, j, k), a state-shaped arena
   const double* beta;   // 3-D shock detector of every cell (one plane per block), or null
   double* Fv;           // Navier-Stokes: interior face fluxes, 14 planes per block (null otherwise)
+  // 2-D: the stage kernels read the ghost cells of remapped connection edges
+  // (BlockDesc::rm_*) from their source cells, so their ghost fill is not needed
+  int remap;
   MetricArgs m;
   double* dtl;          // local dt plane arena (one plane per block), or null
   const double* dtg;    // device scalar dtglobal (time-accurate)

@@ -99,6 +99,15 @@ struct BlockDesc {
   double u_A[3];        // face area per direction
   double u_vol;
   double u_vers[3][3];  // CFL versor per direction
+  // 2-D connection edges read in place (StageArgs::remap): per face f = 1..4
+  // (index f - 1) the source block (-1: the ghost layer is filled), and the
+  // source cells of the ghost chunks: faces 1 / 2, column rm_at (of the
+  // ghost chunk's first cell) and row j + rm_off; faces 3 / 4, column
+  // i + rm_off and row rm_at + r (face 3, ghost rows r = -2, -1) or
+  // rm_at + r - nj (face 4)
+  int rm_src[4];
+  int rm_at[4];
+  int rm_off[4];
 };
 
 // Cell offset inside one plane of block d (i, j, k 0-based, ghosts negative).

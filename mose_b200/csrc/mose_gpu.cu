@@ -238,6 +238,9 @@ struct mose_gpu_ctx {
   DevBuf<int> bcw;
   DevBuf<BcParam> bcp;
   DevBuf<GhostRec> ghosts;
+  DevBuf<GhostRec> ghosts_nc;   // the records of edges not read in place (fused steps)
+  int nghost_nc = 0;
+  bool remap = false;           // some 2-D connection edge is read in place
   DevBuf<int4> items;
   // implicit residual smoothing (irs-beta > 0): first-layer ghost records of
   // R and two work arenas for the Jacobi sweeps
@@ -1038,6 +1041,62 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
     for (int dd = 0; dd < 3; ++dd)
       for (int q = 0; q < 3; ++q) d.u_vers[dd][q] = f[16 + 3 * dd + q];
   }
+  // ---- connection edges read in place (2-D, inviscid) ----------------------------
+  // A block edge whose face cells are all 101 / 201 connections to one source
+  // block's opposite face, aligned (the source column, or row, a fixed offset
+  // from the face cell's), on an even-sized block with 16-byte-aligned source
+  // chunks: the stage kernels read its ghost cells from the source cells
+  // Ghost_Connection copies there (Lib_Ghost.f90:140-160), so the fused
+  // steps fill only the other ghost records.
+  for (BlockDesc& d : ctx->desc)
+    for (int f = 0; f < 4; ++f) {
+      d.rm_src[f] = -1;
+      d.rm_at[f] = 0;
+      d.rm_off[f] = 0;
+    }
+  ctx->remap = false;
+  if (ctx->nd == 2 && ctx->gas.model == 0) {
+    std::vector<std::vector<const BcRecord*>> recs(4 * (size_t)nb);
+    for (const BcRecord& e : ctx->bc)
+      if (e.f <= 4) recs[4 * (size_t)(e.b - 1) + (e.f - 1)].push_back(&e);
+    for (int b = 0; b < nb; ++b) {
+      const HostBlock& h = ctx->hblk[b];
+      if (h.ni % 2 != 0) continue;   // the ghost chunk of face 2 starts at cell ni
+      for (int f = 0; f < 4; ++f) {
+        const std::vector<const BcRecord*>& L = recs[4 * (size_t)b + f];
+        if (f >= 2 && h.nj < 3) continue;   // j-faces without a ghost layer
+        if ((int)L.size() != (f < 2 ? h.nj : h.ni)) continue;
+        const int want_fs = (f == 0) ? 2 : (f == 1) ? 1 : (f == 2) ? 4 : 3;
+        bool ok = true;
+        int src = -1, at = 0, off = 0;
+        for (size_t q = 0; q < L.size() && ok; ++q) {
+          const BcRecord& e = *L[q];
+          if ((e.type != 101 && e.type != 201) || e.fs != want_fs) {
+            ok = false;
+            break;
+          }
+          const int c = f < 2 ? e.j - 1 : e.i - 1, is = e.is - 1, js = e.js - 1;
+          const int a_ = f == 0 ? is - 1 : f == 1 ? is : f == 2 ? js + 1 : js;
+          const int o_ = f < 2 ? js - c : is - c;
+          if (q == 0) {
+            src = e.bs - 1;
+            at = a_;
+            off = o_;
+          } else if (e.bs - 1 != src || a_ != at || o_ != off) {
+            ok = false;
+          }
+        }
+        // 16-byte source chunks: an even first column
+        if (ok && (f < 2 ? at : off) % 2 != 0) ok = false;
+        if (!ok) continue;
+        BlockDesc& d = ctx->desc[b];
+        d.rm_src[f] = src;
+        d.rm_at[f] = at;
+        d.rm_off[f] = off;
+        ctx->remap = true;
+      }
+    }
+  }
   CU(cudaMemcpyAsync(ctx->d_desc.p, ctx->desc.data(), nb * sizeof(BlockDesc), cudaMemcpyHostToDevice, ctx->stream));
 
   // ---- ghost-fill records (Fill_Ghost_Cell dispatch, Lib_Ghost.f90:50-73) ------
@@ -1056,6 +1115,17 @@ int mose_gpu_setup(mose_gpu_ctx* ctx) {
   ctx->hghost = gr;
   CU(ctx->ghosts.alloc(std::max<size_t>(gr.size(), 1)));
   if (!gr.empty()) CU(cudaMemcpyAsync(ctx->ghosts.p, gr.data(), gr.size() * sizeof(GhostRec), cudaMemcpyHostToDevice, ctx->stream));
+  // the records the fused steps still fill: all but those of edges read in place
+  {
+    std::vector<GhostRec> nc;
+    for (const GhostRec& g : gr)
+      if (!(g.type == BC_CONN && g.f <= 4 && ctx->desc[g.b].rm_src[g.f - 1] >= 0)) nc.push_back(g);
+    ctx->nghost_nc = (int)nc.size();
+    CU(ctx->ghosts_nc.alloc(std::max<size_t>(nc.size(), 1)));
+    if (!nc.empty())
+      CU(cudaMemcpyAsync(ctx->ghosts_nc.p, nc.data(), nc.size() * sizeof(GhostRec), cudaMemcpyHostToDevice,
+                         ctx->stream));
+  }
 
 
   // ---- implicit residual smoothing: first-layer ghost records of R ----------------
@@ -1270,6 +1340,7 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   a.Hk = ctx->hk.p;
   a.beta = ctx->sdbeta.p;
   a.Fv = ctx->vface.p;
+  a.remap = ctx->remap ? 1 : 0;
   a.m = ctx->margs();
   a.dtl = ctx->dtl.p;
   a.dtg = ctx->scal.p;
@@ -1289,12 +1360,15 @@ static StageArgs stage_args(mose_gpu_ctx* ctx, int pc, int po, int pn, int irk) 
   return a;
 }
 
-// The ghost layers of the stage input pc (Fill_Ghost_Cell).  Returns the
-// number of kernels enqueued.
+// The ghost layers of the stage input pc (Fill_Ghost_Cell) that the fused
+// steps' stage kernels read from memory: every record, less those of the
+// connection edges they read in place.  Returns the number of kernels
+// enqueued.
 static int enqueue_stage_ghosts(mose_gpu_ctx* ctx, int pc) {
-  launch_fill_ghosts(ctx->d_desc.p, ctx->ghosts.p, ctx->nghost, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p,
-                     ctx->stream);
-  return ctx->nghost ? 1 : 0;
+  const GhostRec* recs = ctx->remap ? ctx->ghosts_nc.p : ctx->ghosts.p;
+  const int n = ctx->remap ? ctx->nghost_nc : ctx->nghost;
+  launch_fill_ghosts(ctx->d_desc.p, recs, n, ctx->state[pc].p, ctx->margs(), ctx->nd, ctx->derr.p, ctx->stream);
+  return n ? 1 : 0;
 }
 
 // One RK stage (mode 0 / 2) or one residual evaluation (mode 1) on every

@@ -557,21 +557,56 @@ __global__ void __launch_bounds__(SB_T, stage_min_ctas<UNI, BC>()) k_stage2d(Sta
       }
     };
 
+    // the item reads ghost chunks of an edge read in place only when it
+    // touches a block edge
+    const bool edge_item = a.remap && (c0 == 0 || c1 >= ni || j0 == 0 || j1 >= nj);
     // unit u = rows j0 - 2 + 4u .. + 3 into ring rows 4 (u % 3) ..; each
     // thread copies all planes of its (row, 2-cell chunk) pairs
     auto load_unit = [&](int u) {
       const int slot = (u % 3) * SB_Y;
       const int rbase = j0 - 2 + SB_Y * u;
+      if (!edge_item) {
+        for (int e = t; e < SB_Y * SB_CH; e += SB_T) {
+          const int i = e / SB_CH, q = e - i * SB_CH;
+          const int r = rbase + i;
+          const int x = c0 + 2 * q;   // padded column of cell c0 - 2 + 2q
+          if (r > nj + 1 || x >= px) continue;
+          const long long o = (long long)(r + GW) * px + x;
+#pragma unroll
+          for (int pv = 0; pv < NVR; ++pv) {
+            const double* plane = pv < NV ? Pc + pv * vs : a.m.dl + 3 * mb + (pv - NV) * vs;
+            cp_async16(&S.ring[pv][slot + i][2 * q], plane + o);
+          }
+        }
+        return;
+      }
       for (int e = t; e < SB_Y * SB_CH; e += SB_T) {
         const int i = e / SB_CH, q = e - i * SB_CH;
         const int r = rbase + i;
-        const int x = c0 + 2 * q;   // padded column of cell c0 - 2 + 2q
+        const int x = c0 + 2 * q;
         if (r > nj + 1 || x >= px) continue;
         const long long o = (long long)(r + GW) * px + x;
+        // the state's source: this block's cells, or, for a ghost chunk of
+        // an edge read in place, the source block's cells that
+        // Ghost_Connection would copy there (corner chunks stay as they are:
+        // no stencil reads them)
+        const double* src = Pc + o;
+        long long svs = vs;
+        const int cell = x - GW;
+        const int gc = cell < 0 ? 0 : cell >= ni ? 1 : -1;
+        const int gr = r < 0 ? 2 : r >= nj ? 3 : -1;
+        const int f = (gc >= 0) == (gr >= 0) ? -1 : (gc >= 0 ? gc : gr);
+        if (f >= 0 && d.rm_src[f] >= 0) {
+          const BlockDesc& sb = a.blk[d.rm_src[f]];
+          const int si = f < 2 ? d.rm_at[f] : cell + d.rm_off[f];
+          const int sj = f < 2 ? r + d.rm_off[f] : d.rm_at[f] + (f == 2 ? r : r - nj);
+          src = a.Pc + sb.sbase + cell_off2(sb, si, sj);
+          svs = sb.vstride;
+        }
 #pragma unroll
         for (int pv = 0; pv < NVR; ++pv) {
-          const double* plane = pv < NV ? Pc + pv * vs : a.m.dl + 3 * mb + (pv - NV) * vs;
-          cp_async16(&S.ring[pv][slot + i][2 * q], plane + o);
+          const double* g = pv < NV ? src + pv * svs : a.m.dl + 3 * mb + (pv - NV) * vs + o;
+          cp_async16(&S.ring[pv][slot + i][2 * q], g);
         }
       }
     };

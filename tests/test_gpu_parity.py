@@ -124,6 +124,28 @@ def test_fused_steps_bitwise(oracle_mod, name):
     np.testing.assert_allclose(ng, no, rtol=1e-12, atol=0)
 
 
+@pytest.mark.parametrize("n, in_place", [(64, True), (63, False)])
+def test_connection_edges_read_in_place(oracle_mod, n, in_place):
+    """On an even-sized periodic block the stage kernels read the four 201
+    edges' ghost cells from the source cells Ghost_Connection copies there,
+    so the fused steps launch no ghost fill; an odd-sized block keeps it.
+    Both step bit for bit with the oracle, fused and graph-replayed."""
+    case = cases.isentropic_vortex(n, steps=3)
+    o = oracle_mod.Oracle(case)
+    s = solver(case)
+    for _ in range(2):
+        dto, to = o.step()
+        dtg, tg = s.explicit_step()
+        assert dtg == dto and tg == to
+    compare_state(s, o, 1)
+    for _ in range(3):
+        o.step()
+    s.advance(3)
+    compare_state(s, o, 1)
+    _, launches = s.time_kernels(2)
+    assert (launches[1] == 0) == in_place, launches
+
+
 def test_sod_to_final_time_bitwise(oracle_mod):
     """Configuration 1 at 1000 cells integrated to t >= 0.2."""
     case = cases.sod(1000)
