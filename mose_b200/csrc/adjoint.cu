@@ -115,12 +115,15 @@ __global__ void k_adj_pre(const BlockDesc* blk, int b, MetricArgs m, Gas g, cons
   }
 }
 
-// ---- interior faces along dir ----------------------------------------------------
+// ---- interior faces, both directions in one launch (dir = blockIdx.z) --------------
 // Face between cells (i, j) and its dir-neighbour, stored at (i, j): the four
 // stencil contributions in C (16 planes per direction) and the flux in F.
 template <int LIM>
 __global__ void k_adj_faces(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* P, const double* lamR,
-                            double* C, double* F, int dir) {
+                            double* Cx, double* Fx, double* Cy, double* Fy) {
+  const int dir = blockIdx.z;
+  double* C = dir ? Cy : Cx;
+  double* F = dir ? Fy : Fx;
   const BlockDesc& d = blk[b];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   const int di = dir == 0, dj = dir == 1;
@@ -506,12 +509,13 @@ void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, c
   k_adj_pre<<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, Ps, Pprev, Pn, lam, lamR, wdt, lam_loc, lam_n, c, dtg);
 }
 void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, int lim, const double* P,
-               const double* lamR, double* C, double* F, int dir, cudaStream_t s) {
-  const dim3 grid = adjl::cells(ni, nj, false);
+               const double* lamR, double* Cx, double* Fx, double* Cy, double* Fy, cudaStream_t s) {
+  dim3 grid = adjl::cells(ni, nj, false);
+  grid.z = 2;
   switch (lim) {
-    case 1: k_adj_faces<1><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, C, F, dir); break;
-    case 2: k_adj_faces<2><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, C, F, dir); break;
-    default: k_adj_faces<3><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, C, F, dir); break;
+    case 1: k_adj_faces<1><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, Cx, Fx, Cy, Fy); break;
+    case 2: k_adj_faces<2><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, Cx, Fx, Cy, Fy); break;
+    default: k_adj_faces<3><<<grid, 128, 0, s>>>(blk, b, m, g, P, lamR, Cx, Fx, Cy, Fy); break;
   }
 }
 void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,

@@ -66,7 +66,7 @@ void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, c
              const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc, double* lam_n, double c,
              const double* dtg, cudaStream_t s);
 void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, int lim, const double* P,
-               const double* lamR, double* C, double* F, int dir, cudaStream_t s);
+               const double* lamR, double* Cx, double* Fx, double* Cy, double* Fy, cudaStream_t s);
 void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,
             double* dmach, cudaStream_t s);
 void adj_gather(const BlockDesc* blk, int b, int ni, int nj, const double* Cx, const double* Cy, const double* Fx,

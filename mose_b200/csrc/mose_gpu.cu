@@ -13,6 +13,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
+#include <iterator>
 #include <string>
 #include <vector>
 
@@ -317,6 +319,9 @@ struct mose_gpu_ctx {
   int adj_bcfirst[5] = {0, 0, 0, 0, 0};  // face f's entries: [adj_bcfirst[f-1], adj_bcfirst[f])
   DevBuf<int> adj_gids;                  // ghost records grouped by face
   int adj_gfirst[5] = {0, 0, 0, 0, 0};
+  // launches of the boundary gather and of the ghost transpose: runs of
+  // consecutive faces whose entries touch disjoint cells, as entry ranges
+  std::vector<int> adj_bcpass, adj_gpass;
   bool adj_recorded = false;
   std::vector<BcParam> hbcp;             // 401 / 402 / 403 - 407 parameters (host copy)
   // 402 time tables: (time, value) pairs of every table, and per table its
@@ -1907,6 +1912,44 @@ static double rk_coeff(const mose_gpu_ctx* ctx, int irk) {
 }
 
 // Buffers and work lists of the adjoint, made on first use.
+// Splits the face groups first[0..4] into launches: a face joins the current
+// launch when none of the cells its entries touch (cells(q) of entry q) is
+// touched by the faces already in it, so every cell sees the same updates in
+// the same order as with one launch per face.  Returns the entry offsets at
+// which launches start, followed by first[4].
+static std::vector<int> face_passes(const int first[5],
+                                    const std::function<void(int, std::vector<long long>&)>& cells) {
+  std::vector<int> pass{first[0]};
+  std::vector<long long> in_pass, face, c;
+  for (int f = 0; f < 4; ++f) {
+    face.clear();
+    for (int q = first[f]; q < first[f + 1]; ++q) {
+      c.clear();
+      cells(q, c);
+      face.insert(face.end(), c.begin(), c.end());
+    }
+    std::sort(face.begin(), face.end());
+    face.erase(std::unique(face.begin(), face.end()), face.end());
+    bool overlap = false;
+    for (long long x : face)
+      if (std::binary_search(in_pass.begin(), in_pass.end(), x)) { overlap = true; break; }
+    if (overlap) {
+      pass.push_back(first[f]);
+      in_pass.clear();
+    }
+    std::vector<long long> u;
+    std::merge(in_pass.begin(), in_pass.end(), face.begin(), face.end(), std::back_inserter(u));
+    in_pass.swap(u);
+  }
+  pass.push_back(first[4]);
+  return pass;
+}
+
+// (block, i, j) as one key; i and j lie within GW of the block.
+static long long cell_key(int b, int i, int j) {
+  return ((long long)b << 40) | ((long long)(i + 16) << 20) | (long long)(j + 16);
+}
+
 static int adj_prepare(mose_gpu_ctx* ctx) {
   if (ctx->adj_init) return MOSE_OK;
   if (ctx->nd != 2) return fail(ctx, MOSE_ERR_UNSUPPORTED, "adjoint: 2-D domains only");
@@ -1959,6 +2002,31 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
       if (ctx->hghost[q].f == f) gids.push_back(q);
   }
   ctx->adj_gfirst[4] = (int)gids.size();
+  ctx->adj_bcpass = face_passes(ctx->adj_bcfirst, [&](int q, std::vector<long long>& c) {
+    // the four cells along the normal that k_adj_bc_gather updates
+    const int4 e = list[q];
+    const BlockDesc& d = ctx->desc[e.x];
+    const int dir = (e.y - 1) / 2;
+    const bool high = e.y % 2 == 0;
+    const int i = dir == 0 ? (high ? d.ni - 1 : 0) : e.z, j = dir == 1 ? (high ? d.nj - 1 : 0) : e.z;
+    for (int s = 0; s < 4; ++s) {
+      const int t = high ? s - 1 : s - 2;
+      c.push_back(cell_key(e.x, i + (dir == 0) * t, j + (dir == 1) * t));
+    }
+  });
+  ctx->adj_gpass = face_passes(ctx->adj_gfirst, [&](int q, std::vector<long long>& c) {
+    // the cells k_adj_ghostT reads and writes for the record
+    const GhostRec& e = ctx->hghost[gids[q]];
+    const int gi = (e.f == 1) ? 1 : (e.f == 2) ? -1 : 0;
+    const int gj = (e.f == 3) ? 1 : (e.f == 4) ? -1 : 0;
+    const int lo = e.type == BC_CONN ? 1 : e.type == BC_EXTRAP ? -GW : 0;
+    for (int g = lo; g <= GW; ++g) c.push_back(cell_key(e.b, e.i - gi * g, e.j - gj * g));
+    if (e.type == BC_CONN) {
+      const int si = (e.fs == 1) ? 1 : (e.fs == 2) ? -1 : 0;
+      const int sj = (e.fs == 3) ? 1 : (e.fs == 4) ? -1 : 0;
+      for (int g = 1; g <= GW; ++g) c.push_back(cell_key(e.bs, e.is + si * (g - 1), e.js + sj * (g - 1)));
+    }
+  });
   CU(ctx->adj_gids.alloc(std::max<size_t>(gids.size(), 1)));
   if (!gids.empty())
     CU(cudaMemcpyAsync(ctx->adj_gids.p, gids.data(), gids.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
@@ -2065,32 +2133,28 @@ static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
       adj_bc(a, lim, ctx->adj_bclist.p, nlist, ctx->lamR.p, ctx->Cb.p, ctx->Fbc.p, ctx->dmach.p, aux);
       ++kern;
     }
-    for (int b = 0; b < nb; ++b) {
+    for (int b = 0; b < nb; ++b)
       adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cx.p,
-                ctx->Fx.p, 0, st);
-      adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cy.p,
-                ctx->Fy.p, 1, st);
-    }
+                ctx->Fx.p, ctx->Cy.p, ctx->Fy.p, st);
     for (int b = 0; b < nb; ++b)
       adj_gather(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->Cx.p, ctx->Cy.p, ctx->Fx.p, ctx->Fy.p,
                  ctx->wdt.p, ctx->lamG.p, ctx->dtpart.p, st);
     cudaEventRecord(ctx->adj_join, aux);
     cudaStreamWaitEvent(st, ctx->adj_join, 0);
-    for (int f = 1; f <= 4; ++f) {
-      const int n = ctx->adj_bcfirst[f] - ctx->adj_bcfirst[f - 1];
-      adj_bc_gather(ctx->d_desc.p, ctx->adj_bclist.p, ctx->adj_bcfirst[f - 1], n, ctx->Cb.p, ctx->Fbc.p, ctx->wdt.p,
+    for (size_t q = 0; q + 1 < ctx->adj_bcpass.size(); ++q) {
+      const int n = ctx->adj_bcpass[q + 1] - ctx->adj_bcpass[q];
+      adj_bc_gather(ctx->d_desc.p, ctx->adj_bclist.p, ctx->adj_bcpass[q], n, ctx->Cb.p, ctx->Fbc.p, ctx->wdt.p,
                     ctx->lamG.p, ctx->dtpart.p, st);
       kern += n > 0;
     }
-    for (int f = 1; f <= 4; ++f) {
-      const int n = ctx->adj_gfirst[f] - ctx->adj_gfirst[f - 1];
-      adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gfirst[f - 1], n, m, ctx->lamG.p,
-                          st);
+    for (size_t q = 0; q + 1 < ctx->adj_gpass.size(); ++q) {
+      const int n = ctx->adj_gpass[q + 1] - ctx->adj_gpass[q];
+      adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gpass[q], n, m, ctx->lamG.p, st);
       kern += n > 0;
     }
     for (int b = 0; b < nb; ++b)
       adj_combine(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->lam_loc.p, ctx->lamG.p, ctx->lam.p, st);
-    kern += 5 * nb;
+    kern += 4 * nb;   // pre, faces, gather, combine
   }
   adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 0, ctx->adj_sumscr.p, st);     // dJ/ddt of this step
   kern += 2;
