@@ -258,7 +258,8 @@ __global__ void k_adj_bc(StageArgs a, const int4* list, int nlist, const double*
 // Ghosted cells: lamG = sum of the interior-face contributions that reach the
 // cell; interior cells also form R . wdt of the interior faces (dt partial).
 __global__ void k_adj_gather(const BlockDesc* blk, int b, const double* Cx, const double* Cy, const double* Fx,
-                             const double* Fy, const double* wdt, double* lamG, double* dtpart) {
+                             const double* Fy, const double* __restrict__ Cb, const double* __restrict__ Fbc,
+                             const double* wdt, double* lamG, double* dtpart) {
   const BlockDesc& d = blk[b];
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - GW, j = (int)blockIdx.y - GW;
   if (i >= d.ni + GW || j >= d.nj + GW) return;
@@ -279,6 +280,26 @@ __global__ void k_adj_gather(const BlockDesc* blk, int b, const double* Cx, cons
       const long long base = 16 * d.mbase + off(d, i, f);
       for (int v = 0; v < NV; ++v) acc[v] += Cy[base + (4 * s + v) * vs];
     }
+  // then the boundary faces' stencil contributions (k_adj_bc), faces 1..4 in
+  // order: face f's entry idx touches the four cells along its normal, slot s
+  // (the boundary cell is slot 2 on a low face, 1 on a high one)
+  double bsum[4];
+  int nbs = 0;
+  if (Cb != nullptr && (i < 2 || i >= d.ni - 2 || j < 2 || j >= d.nj - 2))
+    for (int f = 1; f <= 4; ++f) {
+      const int dir = (f - 1) / 2;
+      const bool high = (f % 2) == 0;
+      const int x = dir == 0 ? i : j, idx = dir == 0 ? j : i, n = dir == 0 ? d.ni : d.nj;
+      const int s = high ? x - n + 2 : x + 2;
+      if (s < 0 || s > 3 || idx < 0 || idx >= d.bcn[f - 1]) continue;
+      const size_t ent = (size_t)(d.bcoff[f - 1] + idx);
+      for (int v = 0; v < NV; ++v) acc[v] += Cb[ent * 16 + 4 * s + v];
+      if (s == (high ? 1 : 2)) {
+        double sum = 0.0;
+        for (int v = 0; v < NV; ++v) sum += Fbc[ent * 4 + v] * wdt[d.sbase + oc + v * vs];
+        bsum[nbs++] = sum;
+      }
+    }
   for (int v = 0; v < NV; ++v) lamG[d.sbase + oc + v * vs] = acc[v];
   if (i >= 0 && i < d.ni && j >= 0 && j < d.nj) {
     double R[NV] = {0, 0, 0, 0};
@@ -289,45 +310,10 @@ __global__ void k_adj_gather(const BlockDesc* blk, int b, const double* Cx, cons
     if (j < d.nj - 1) for (int v = 0; v < NV; ++v) R[v] += Fy[o4 + oc + v * vs];
     double s = 0.0;
     for (int v = 0; v < NV; ++v) s += R[v] * wdt[d.sbase + oc + v * vs];
-    dtpart[d.mbase + oc] += s;
+    double dp = dtpart[d.mbase + oc] + s;
+    for (int q = 0; q < nbs; ++q) dp = dp + bsum[q];
+    dtpart[d.mbase + oc] = dp;
   }
-}
-
-// Boundary-face contributions of face f (entries of one face touch distinct cells).
-__global__ void k_adj_bc_gather(const BlockDesc* blk, const int4* __restrict__ list, int first, int n,
-                                const double* __restrict__ Cb, const double* __restrict__ Fbc,
-                                const double* __restrict__ wdt, double* __restrict__ lamG,
-                                double* __restrict__ dtpart) {
-  const int q = blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= n) return;
-  const int4 e = list[first + q];
-  const int b = e.x, f = e.y, idx = e.z, ent = e.w;
-  const BlockDesc& d = blk[b];
-  const int dir = (f - 1) / 2;
-  const bool high = (f % 2) == 0;
-  const int i = dir == 0 ? (high ? d.ni - 1 : 0) : idx, j = dir == 1 ? (high ? d.nj - 1 : 0) : idx;
-  const int di = dir == 0, dj = dir == 1;
-  const long long vs = d.vstride;
-  // all loads first: the sixteen read-modify-writes are independent
-  long long o[4];
-  double l[4][NV], c[4][NV];
-  for (int s = 0; s < 4; ++s) {
-    const int t = high ? s - 1 : s - 2;
-    o[s] = d.sbase + off(d, i + di * t, j + dj * t);
-    for (int v = 0; v < NV; ++v) {
-      l[s][v] = lamG[o[s] + v * vs];
-      c[s][v] = Cb[(size_t)ent * 16 + 4 * s + v];
-    }
-  }
-  const long long ob = off(d, i, j);
-  double w[NV], F[NV];
-  for (int v = 0; v < NV; ++v) { w[v] = wdt[d.sbase + ob + v * vs]; F[v] = Fbc[(size_t)ent * 4 + v]; }
-  const double dp = dtpart[d.mbase + ob];
-  for (int s = 0; s < 4; ++s)
-    for (int v = 0; v < NV; ++v) lamG[o[s] + v * vs] = l[s][v] + c[s][v];
-  double sum = 0.0;
-  for (int v = 0; v < NV; ++v) sum += F[v] * w[v];
-  dtpart[d.mbase + ob] = dp + sum;
 }
 
 // Transpose of Fill_Ghost_Cell for the ghost records of one face.
@@ -529,13 +515,9 @@ void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* 
   }
 }
 void adj_gather(const BlockDesc* blk, int b, int ni, int nj, const double* Cx, const double* Cy,
-                const double* Fx, const double* Fy, const double* wdt, double* lamG, double* dtpart, cudaStream_t s) {
-  k_adj_gather<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, Cx, Cy, Fx, Fy, wdt, lamG, dtpart);
-}
-void adj_bc_gather(const BlockDesc* blk, const int4* list, int first, int n, const double* Cb, const double* Fbc,
-                   const double* wdt, double* lamG, double* dtpart, cudaStream_t s) {
-  if (n == 0) return;
-  k_adj_bc_gather<<<(n + 127) / 128, 128, 0, s>>>(blk, list, first, n, Cb, Fbc, wdt, lamG, dtpart);
+                const double* Fx, const double* Fy, const double* Cb, const double* Fbc, const double* wdt,
+                double* lamG, double* dtpart, cudaStream_t s) {
+  k_adj_gather<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, Cx, Cy, Fx, Fy, Cb, Fbc, wdt, lamG, dtpart);
 }
 void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
                          double* lamG, cudaStream_t s) {

@@ -69,10 +69,11 @@ void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g,
                const double* lamR, double* Cx, double* Fx, double* Cy, double* Fy, cudaStream_t s);
 void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,
             double* dmach, cudaStream_t s);
+// Cb / Fbc: the boundary faces' stencil contributions and fluxes (k_adj_bc),
+// added after the interior faces'; nullptr when the domain has none
 void adj_gather(const BlockDesc* blk, int b, int ni, int nj, const double* Cx, const double* Cy, const double* Fx,
-                const double* Fy, const double* wdt, double* lamG, double* dtpart, cudaStream_t s);
-void adj_bc_gather(const BlockDesc* blk, const int4* list, int first, int n, const double* Cb, const double* Fbc,
-                   const double* wdt, double* lamG, double* dtpart, cudaStream_t s);
+                const double* Fy, const double* Cb, const double* Fbc, const double* wdt, double* lamG,
+                double* dtpart, cudaStream_t s);
 void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
                          double* lamG, cudaStream_t s);
 void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,

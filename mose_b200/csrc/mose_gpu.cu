@@ -319,9 +319,9 @@ struct mose_gpu_ctx {
   int adj_bcfirst[5] = {0, 0, 0, 0, 0};  // face f's entries: [adj_bcfirst[f-1], adj_bcfirst[f])
   DevBuf<int> adj_gids;                  // ghost records grouped by face
   int adj_gfirst[5] = {0, 0, 0, 0, 0};
-  // launches of the boundary gather and of the ghost transpose: runs of
-  // consecutive faces whose entries touch disjoint cells, as entry ranges
-  std::vector<int> adj_bcpass, adj_gpass;
+  // launches of the ghost transpose: runs of consecutive faces whose records
+  // touch disjoint cells, as record ranges
+  std::vector<int> adj_gpass;
   bool adj_recorded = false;
   std::vector<BcParam> hbcp;             // 401 / 402 / 403 - 407 parameters (host copy)
   // 402 time tables: (time, value) pairs of every table, and per table its
@@ -1973,8 +1973,8 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
   CU(cudaEventCreateWithFlags(&ctx->adj_join, cudaEventDisableTiming));
   CU(ctx->adj_arg.alloc(1));
   CU(ctx->adj_sumscr.alloc(adj_sum_scratch()));
-  // boundary face cells of faces 1..4, grouped by face (one launch per face
-  // touches each cell at most once)
+  // boundary face cells of faces 1..4, grouped by face: one k_adj_bc entry
+  // each, whose stencil contributions k_adj_gather adds per cell
   std::vector<int4> list;
   size_t nent = 0, maxface = 1;
   for (const BlockDesc& d : ctx->desc) {
@@ -2002,18 +2002,6 @@ static int adj_prepare(mose_gpu_ctx* ctx) {
       if (ctx->hghost[q].f == f) gids.push_back(q);
   }
   ctx->adj_gfirst[4] = (int)gids.size();
-  ctx->adj_bcpass = face_passes(ctx->adj_bcfirst, [&](int q, std::vector<long long>& c) {
-    // the four cells along the normal that k_adj_bc_gather updates
-    const int4 e = list[q];
-    const BlockDesc& d = ctx->desc[e.x];
-    const int dir = (e.y - 1) / 2;
-    const bool high = e.y % 2 == 0;
-    const int i = dir == 0 ? (high ? d.ni - 1 : 0) : e.z, j = dir == 1 ? (high ? d.nj - 1 : 0) : e.z;
-    for (int s = 0; s < 4; ++s) {
-      const int t = high ? s - 1 : s - 2;
-      c.push_back(cell_key(e.x, i + (dir == 0) * t, j + (dir == 1) * t));
-    }
-  });
   ctx->adj_gpass = face_passes(ctx->adj_gfirst, [&](int q, std::vector<long long>& c) {
     // the cells k_adj_ghostT reads and writes for the record
     const GhostRec& e = ctx->hghost[gids[q]];
@@ -2136,17 +2124,13 @@ static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
     for (int b = 0; b < nb; ++b)
       adj_faces(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, lim, Pprev, ctx->lamR.p, ctx->Cx.p,
                 ctx->Fx.p, ctx->Cy.p, ctx->Fy.p, st);
-    for (int b = 0; b < nb; ++b)
-      adj_gather(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->Cx.p, ctx->Cy.p, ctx->Fx.p, ctx->Fy.p,
-                 ctx->wdt.p, ctx->lamG.p, ctx->dtpart.p, st);
     cudaEventRecord(ctx->adj_join, aux);
     cudaStreamWaitEvent(st, ctx->adj_join, 0);
-    for (size_t q = 0; q + 1 < ctx->adj_bcpass.size(); ++q) {
-      const int n = ctx->adj_bcpass[q + 1] - ctx->adj_bcpass[q];
-      adj_bc_gather(ctx->d_desc.p, ctx->adj_bclist.p, ctx->adj_bcpass[q], n, ctx->Cb.p, ctx->Fbc.p, ctx->wdt.p,
-                    ctx->lamG.p, ctx->dtpart.p, st);
-      kern += n > 0;
-    }
+    // interior and boundary faces' contributions, per cell
+    for (int b = 0; b < nb; ++b)
+      adj_gather(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->Cx.p, ctx->Cy.p, ctx->Fx.p, ctx->Fy.p,
+                 nlist ? ctx->Cb.p : nullptr, nlist ? ctx->Fbc.p : nullptr, ctx->wdt.p, ctx->lamG.p, ctx->dtpart.p,
+                 st);
     for (size_t q = 0; q + 1 < ctx->adj_gpass.size(); ++q) {
       const int n = ctx->adj_gpass[q + 1] - ctx->adj_gpass[q];
       adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gpass[q], n, m, ctx->lamG.p, st);
