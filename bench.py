@@ -587,14 +587,15 @@ def viscous_report(local, n=512, steps=50):
         "terms": "HLLC + van Leer convective, laminar diffusive fluxes, 302 / 301 walls, 101 / 201 connections"}}
 
 
-def profile_adjoint(local):
+def profile_adjoint(local, precision="fp64"):
     """The launches a profiler captures for the adjoint: the configuration-5
     channel at 512^2 with 16 steps and a checkpoint every 4, forward and
-    backward once to build the graphs, then once more."""
+    backward once to build the graphs, then once more (forward in the given
+    precision)."""
     from mose_b200 import Solver, cases
     from mose_b200.cases import to_ref_layout
     case = cases.perturbed_channel(512, steps=16)
-    s = Solver(case, precision=precision_code("exact"), device=local)
+    s = Solver(case, precision=precision_code(precision), device=local)
     for _ in range(2):
         s.upload_prim(1, to_ref_layout(case.prim[0]))
         s.set_time(0.0, 0)
@@ -622,7 +623,7 @@ def run_gpu(args):
     import torch
     from mose_b200 import Solver
     if args.profile_adjoint:
-        return profile_adjoint(local)
+        return profile_adjoint(local, args.precision)
     if args.profile and args.profile_case == "quadrant":
         from mose_b200 import cases
         case = cases.four_quadrant(seed=0, steps=args.steps)

@@ -88,15 +88,20 @@ __device__ __forceinline__ void face_vjp(const Gas& g, const double q[4][NV], co
 // ---- per-cell pre-step ---------------------------------------------------------
 // lam (adjoint of P_s) -> lamR = -(dt/vol) c lam_V, wdt = -(c/vol) lam_V,
 // lam_loc = J_P2U(P_{s-1})^T c lam_V, lam_n += J_P2U(P^n)^T (1-c) lam_V.
+// lamG == nullptr: the stage output's adjoint is lam; else it is the later
+// stage's lam_loc + lamG (that stage's k_adj_combine, folded in here)
 __global__ void k_adj_pre(const BlockDesc* blk, int b, MetricArgs m, Gas g, const double* Ps, const double* Pprev,
-                          const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc,
-                          double* lam_n, double c, const double* dtg) {
+                          const double* Pn, const double* lam, const double* lamG, double* lamR, double* wdt,
+                          double* lam_loc, double* lam_n, double c, const double* dtg) {
   const BlockDesc& d = blk[b];
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= d.ni || j >= d.nj) return;
   const long long vs = d.vstride, o = d.sbase + off(d, i, j), om = d.mbase + off(d, i, j);
   double P[NV], L[NV], V[NV];
-  for (int v = 0; v < NV; ++v) { P[v] = Ps[o + v * vs]; L[v] = lam[o + v * vs]; }
+  for (int v = 0; v < NV; ++v) {
+    P[v] = Ps[o + v * vs];
+    L[v] = lamG ? lam_loc[o + v * vs] + lamG[o + v * vs] : lam[o + v * vs];
+  }
   adj::u2p_vjp(g.gm1, P, L, V);
   const double vol = m.vol[om], dt = *dtg;
   double Q[NV], Ub[NV], loc[NV] = {0, 0, 0, 0}, acc[NV] = {0, 0, 0, 0};
@@ -395,14 +400,19 @@ __global__ void k_adj_ghostT(const BlockDesc* blk, const GhostRec* __restrict__ 
   }
 }
 
-// lam_out = lam_loc + lamG on interior cells, 0 on ghosts.
-__global__ void k_adj_combine(const BlockDesc* blk, int b, const double* lam_loc, const double* lamG, double* lam_out) {
+// lam_out = (lam_loc + lamG on interior cells, 0 on ghosts) + lam_n: the
+// step's first stage and the direct terms of P^n.
+__global__ void k_adj_combine(const BlockDesc* blk, int b, const double* lam_loc, const double* lamG,
+                              const double* lam_n, double* lam_out) {
   const BlockDesc& d = blk[b];
   const int i = (int)(blockIdx.x * blockDim.x + threadIdx.x) - GW, j = (int)blockIdx.y - GW;
   if (i >= d.ni + GW || j >= d.nj + GW) return;
   const long long vs = d.vstride, o = d.sbase + off(d, i, j);
   const bool in = i >= 0 && i < d.ni && j >= 0 && j < d.nj;
-  for (int v = 0; v < NV; ++v) lam_out[o + v * vs] = in ? lam_loc[o + v * vs] + lamG[o + v * vs] : 0.0;
+  for (int v = 0; v < NV; ++v) {
+    const double x = in ? lam_loc[o + v * vs] + lamG[o + v * vs] : 0.0;
+    lam_out[o + v * vs] = x + lam_n[o + v * vs];
+  }
 }
 
 // Deterministic sum of n values: pass 1, one partial per CTA over a fixed
@@ -490,9 +500,10 @@ static dim3 cells(int ni, int nj, bool ghosted) {
 }  // namespace adjl
 
 void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* Ps,
-             const double* Pprev, const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc,
-             double* lam_n, double c, const double* dtg, cudaStream_t s) {
-  k_adj_pre<<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, Ps, Pprev, Pn, lam, lamR, wdt, lam_loc, lam_n, c, dtg);
+             const double* Pprev, const double* Pn, const double* lam, const double* lamG, double* lamR, double* wdt,
+             double* lam_loc, double* lam_n, double c, const double* dtg, cudaStream_t s) {
+  k_adj_pre<<<adjl::cells(ni, nj, false), 128, 0, s>>>(blk, b, m, g, Ps, Pprev, Pn, lam, lamG, lamR, wdt, lam_loc,
+                                                       lam_n, c, dtg);
 }
 void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, int lim, const double* P,
                const double* lamR, double* Cx, double* Fx, double* Cy, double* Fy, cudaStream_t s) {
@@ -525,8 +536,8 @@ void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* 
   k_adj_ghostT<<<(n + 127) / 128, 128, 0, s>>>(blk, recs, ids, n, m, lamG);
 }
 void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,
-                 double* lam_out, cudaStream_t s) {
-  k_adj_combine<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, lam_loc, lamG, lam_out);
+                 const double* lam_n, double* lam_out, cudaStream_t s) {
+  k_adj_combine<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, lam_loc, lamG, lam_n, lam_out);
 }
 void adj_sum(const double* x, long long n, double* out, int accumulate, double* scratch, cudaStream_t s) {
   k_sum_partial<<<kSumCtas, 256, 0, s>>>(x, n, scratch);
@@ -536,14 +547,6 @@ int adj_sum_scratch() { return kSumCtas; }
 void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
             const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s) {
   k_adj_dt<<<1, 32, 0, s>>>(blk, m, g, P, arg, lam_dt, cfl, ndir, lam_n);
-}
-__global__ void k_axpy(double* y, const double* x, long long n) {
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-    y[q] += x[q];
-}
-void adj_axpy(double* y, const double* x, long long n, cudaStream_t s) {
-  const long long g = (n + 255) / 256;
-  k_axpy<<<(unsigned)(g < 148 * 8 ? g : 148 * 8), 256, 0, s>>>(y, x, n);
 }
 void adj_objective(const BlockDesc* blk, int b, int f, int n, MetricArgs m, const double* P, double* terms,
                    double* lam, cudaStream_t s) {

@@ -63,8 +63,8 @@ void launch_rk_stage_to(const BlockDesc* dblk, int nblk, long long maxcell, cons
 bool launch_visc_residual2d(const StageArgs& a, int nblk, long long maxcell, int lim, cudaStream_t s);
 // Discrete adjoint (2-D, HLLC; adjoint.cu).
 void adj_pre(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, const double* Ps, const double* Pprev,
-             const double* Pn, const double* lam, double* lamR, double* wdt, double* lam_loc, double* lam_n, double c,
-             const double* dtg, cudaStream_t s);
+             const double* Pn, const double* lam, const double* lamG, double* lamR, double* wdt, double* lam_loc,
+             double* lam_n, double c, const double* dtg, cudaStream_t s);
 void adj_faces(const BlockDesc* blk, int b, int ni, int nj, MetricArgs m, Gas g, int lim, const double* P,
                const double* lamR, double* Cx, double* Fx, double* Cy, double* Fy, cudaStream_t s);
 void adj_bc(const StageArgs& a, int lim, const int4* list, int n, const double* lamR, double* Cb, double* Fbc,
@@ -77,7 +77,7 @@ void adj_gather(const BlockDesc* blk, int b, int ni, int nj, const double* Cx, c
 void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* ids, int n, MetricArgs m,
                          double* lamG, cudaStream_t s);
 void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,
-                 double* lam_out, cudaStream_t s);
+                 const double* lam_n, double* lam_out, cudaStream_t s);
 void adj_sum(const double* x, long long n, double* out, int accumulate, double* scratch, cudaStream_t s);
 int adj_sum_scratch();
 void launch_dt_argmin(const BlockDesc* dblk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P,
@@ -86,7 +86,6 @@ void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const un
             const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s);
 void adj_objective(const BlockDesc* blk, int b, int f, int n, MetricArgs m, const double* P, double* terms,
                    double* lam, cudaStream_t s);
-void adj_axpy(double* y, const double* x, long long n, cudaStream_t s);
 
 int norms_partial_count(int nblk, long long maxcell);
 void launch_residual_norms(const BlockDesc* dblk, int nblk, long long maxcell, const double* P, const double* PO,

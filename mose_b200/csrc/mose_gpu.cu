@@ -2110,9 +2110,11 @@ static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
     const double* Ps = S[irk];
     const double* Pprev = S[irk - 1];
     const double c = rk_coeff(ctx, irk);
+    // the adjoint of stage irk's output: lam for the last stage, else the
+    // later stage's lam_loc + lamG
     for (int b = 0; b < nb; ++b)
       adj_pre(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, m, ctx->gas, Ps, Pprev, S[0], ctx->lam.p,
-              ctx->lamR.p, ctx->wdt.p, ctx->lam_loc.p, ctx->lam_n.p, c, dtg, st);
+              irk == nrk ? nullptr : ctx->lamG.p, ctx->lamR.p, ctx->wdt.p, ctx->lam_loc.p, ctx->lam_n.p, c, dtg, st);
     if (nlist) {
       StageArgs a = stage_args(ctx, 0, 0, -1, irk);
       a.Pc = Pprev;
@@ -2136,9 +2138,7 @@ static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
       adj_ghost_transpose(ctx->d_desc.p, ctx->ghosts.p, ctx->adj_gids.p + ctx->adj_gpass[q], n, m, ctx->lamG.p, st);
       kern += n > 0;
     }
-    for (int b = 0; b < nb; ++b)
-      adj_combine(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->lam_loc.p, ctx->lamG.p, ctx->lam.p, st);
-    kern += 4 * nb;   // pre, faces, gather, combine
+    kern += 3 * nb;   // pre, faces, gather
   }
   adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 0, ctx->adj_sumscr.p, st);     // dJ/ddt of this step
   kern += 2;
@@ -2147,8 +2147,11 @@ static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
     kern += 2;
   }
   adj_dt(ctx->d_desc.p, m, ctx->gas, S[0], ctx->adj_arg.p, ctx->adj_scal.p, ctx->cfg.cfl, ctx->ndir, ctx->lam_n.p, st);
-  adj_axpy(ctx->lam.p, ctx->lam_n.p, (long long)ns, st);
-  return kern + 2;
+  // lam = the first stage's lam_loc + lamG, plus the direct terms of P^n
+  for (int b = 0; b < nb; ++b)
+    adj_combine(ctx->d_desc.p, b, ctx->hblk[b].ni, ctx->hblk[b].nj, ctx->lam_loc.p, ctx->lamG.p, ctx->lam_n.p,
+                ctx->lam.p, st);
+  return kern + 1 + nb;
 }
 
 // (Re)builds the graphs of a K-step segment: the recompute of a full
