@@ -419,8 +419,19 @@ __global__ void k_adj_combine(const BlockDesc* blk, int b, const double* lam_loc
 // strided subset; pass 2, one CTA sums the partials into *out (+= when
 // accumulate).  Fixed grid and fixed tree: the same bits every run.
 constexpr int kSumCtas = 296;
-__global__ void k_sum_partial(const double* x, long long n, double* part) {
+// Up to two independent sums in one launch pair: sum blockIdx.y reads
+// job[blockIdx.y] and writes its partials at part + blockIdx.y * kSumCtas.
+struct SumJobs {
+  const double* x[2];
+  long long n[2];
+  double* out[2];
+  int accumulate[2];
+};
+__global__ void k_sum_partial(SumJobs jb, double* part) {
   __shared__ double s[256];
+  const int y = blockIdx.y;
+  const double* x = jb.x[y];
+  const long long n = jb.n[y];
   double acc = 0.0;
   for (long long q = blockIdx.x * 256LL + threadIdx.x; q < n; q += 256LL * gridDim.x) acc += x[q];
   s[threadIdx.x] = acc;
@@ -429,19 +440,20 @@ __global__ void k_sum_partial(const double* x, long long n, double* part) {
     if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) part[blockIdx.x] = s[0];
+  if (threadIdx.x == 0) part[y * kSumCtas + blockIdx.x] = s[0];
 }
-__global__ void k_sum_final(const double* part, int np, double* out, int accumulate) {
+__global__ void k_sum_final(SumJobs jb, const double* part) {
   __shared__ double s[256];
+  const int y = blockIdx.x;
   double acc = 0.0;
-  for (int q = threadIdx.x; q < np; q += 256) acc += part[q];
+  for (int q = threadIdx.x; q < kSumCtas; q += 256) acc += part[y * kSumCtas + q];
   s[threadIdx.x] = acc;
   __syncthreads();
   for (int w = 128; w > 0; w >>= 1) {
     if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
     __syncthreads();
   }
-  if (threadIdx.x == 0) *out = accumulate ? *out + s[0] : s[0];
+  if (threadIdx.x == 0) *jb.out[y] = jb.accumulate[y] ? *jb.out[y] + s[0] : s[0];
 }
 
 // lam_n[argmin] += (dJ/ddt) d(dt_cell)/dP at the argmin cell.
@@ -540,10 +552,17 @@ void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_
   k_adj_combine<<<adjl::cells(ni, nj, true), 128, 0, s>>>(blk, b, lam_loc, lamG, lam_n, lam_out);
 }
 void adj_sum(const double* x, long long n, double* out, int accumulate, double* scratch, cudaStream_t s) {
-  k_sum_partial<<<kSumCtas, 256, 0, s>>>(x, n, scratch);
-  k_sum_final<<<1, 256, 0, s>>>(scratch, kSumCtas, out, accumulate);
+  SumJobs jb{{x, nullptr}, {n, 0}, {out, nullptr}, {accumulate, 0}};
+  k_sum_partial<<<dim3(kSumCtas, 1), 256, 0, s>>>(jb, scratch);
+  k_sum_final<<<1, 256, 0, s>>>(jb, scratch);
 }
-int adj_sum_scratch() { return kSumCtas; }
+void adj_sum2(const double* x0, long long n0, double* out0, int acc0, const double* x1, long long n1, double* out1,
+              int acc1, double* scratch, cudaStream_t s) {
+  SumJobs jb{{x0, x1}, {n0, n1}, {out0, out1}, {acc0, acc1}};
+  k_sum_partial<<<dim3(kSumCtas, 2), 256, 0, s>>>(jb, scratch);
+  k_sum_final<<<2, 256, 0, s>>>(jb, scratch);
+}
+int adj_sum_scratch() { return 2 * kSumCtas; }
 void adj_dt(const BlockDesc* blk, MetricArgs m, Gas g, const double* P, const unsigned long long* arg,
             const double* lam_dt, double cfl, int ndir, double* lam_n, cudaStream_t s) {
   k_adj_dt<<<1, 32, 0, s>>>(blk, m, g, P, arg, lam_dt, cfl, ndir, lam_n);

@@ -79,6 +79,9 @@ void adj_ghost_transpose(const BlockDesc* blk, const GhostRec* recs, const int* 
 void adj_combine(const BlockDesc* blk, int b, int ni, int nj, const double* lam_loc, const double* lamG,
                  const double* lam_n, double* lam_out, cudaStream_t s);
 void adj_sum(const double* x, long long n, double* out, int accumulate, double* scratch, cudaStream_t s);
+// two sums in one launch pair, each in the same order as adj_sum's
+void adj_sum2(const double* x0, long long n0, double* out0, int acc0, const double* x1, long long n1, double* out1,
+              int acc1, double* scratch, cudaStream_t s);
 int adj_sum_scratch();
 void launch_dt_argmin(const BlockDesc* dblk, int b, int ni, int nj, MetricArgs m, Gas g, const double* P,
                       const double* dtg, double cfl, int ndir, bool uniform, unsigned long long* arg, cudaStream_t s);

@@ -2140,12 +2140,13 @@ static int adj_reverse_step(mose_gpu_ctx* ctx, int k) {
     }
     kern += 3 * nb;   // pre, faces, gather
   }
-  adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 0, ctx->adj_sumscr.p, st);     // dJ/ddt of this step
+  // dJ/ddt of this step; dJ/dMach accumulates over the steps
+  if (nlist)
+    adj_sum2(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 0, ctx->dmach.p, (long long)ctx->dmach.n,
+             ctx->adj_scal.p + 1, 1, ctx->adj_sumscr.p, st);
+  else
+    adj_sum(ctx->dtpart.p, ctx->marena, ctx->adj_scal.p, 0, ctx->adj_sumscr.p, st);
   kern += 2;
-  if (nlist) {
-    adj_sum(ctx->dmach.p, (long long)ctx->dmach.n, ctx->adj_scal.p + 1, 1, ctx->adj_sumscr.p, st);
-    kern += 2;
-  }
   adj_dt(ctx->d_desc.p, m, ctx->gas, S[0], ctx->adj_arg.p, ctx->adj_scal.p, ctx->cfg.cfl, ctx->ndir, ctx->lam_n.p, st);
   // lam = the first stage's lam_loc + lamG, plus the direct terms of P^n
   for (int b = 0; b < nb; ++b)
